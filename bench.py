@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the finite-volume step (cell-updates/s) on one or more GPUs.
+
+Default workload (the config the metric is quoted on): 2048 x 2048 periodic
+cells, smooth seeded Fourier data, second order (LSM gradients + van Albada
+limiting + HLLC), CFL 0.4, FP64.  One step = SmFluid::update on every cell.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--scheme pc|heun] [--workload fourier2048|riemann256]
+
+Multi-GPU (torchrun): every rank runs an independent replica of the whole
+workload (weak scaling); the timed region is bracketed by a barrier and a
+device synchronise, and the time is the maximum over ranks.
+
+Output: one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC_FILE = ROOT / "profiles" / "traffic_per_cell.txt"
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes per cell and launch (the model: each pass reads the
+# persistent state it needs once and writes its result once; 2-D conserved
+# state = 4 doubles).  Kernels that the model folds into others carry 0.
+B_ALG_KERNEL = {"dt": 0, "flux1": 64, "grad": 0, "stage1": 64, "stage2": 96, "heun_a": 64, "heun_b": 96,
+                "flags": 0}
+B_ALG_STEP = {1: 64, 2: 160}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["fourier2048", "riemann256"], default="fourier2048")
+    ap.add_argument("--scheme", choices=["pc", "heun"], default="pc")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name):
+    from zephyr_b200.workloads import fourier_smooth, riemann2d_case3
+    if name == "fourier2048":
+        return fourier_smooth(2048), dict(acc=2, lim="van Albada", CFL=0.4, lim_id=5, bounds=(3, 3, 3, 3))
+    return riemann2d_case3(256), dict(acc=1, lim="MC", CFL=0.4, lim_id=3, bounds=(2, 2, 2, 2))
+
+
+def config_of(args, w, cfg, n_gpus):
+    return {
+        "workload": f"{w.name} {w.gen.nx()}x{w.gen.ny()}",
+        "cells": w.gen.nx() * w.gen.ny(),
+        "accuracy": cfg["acc"],
+        "scheme": "predictor-corrector (reference)" if args.scheme == "pc" else "heun (extension)",
+        "flux": "HLLC",
+        "limiter": cfg["lim"],
+        "CFL": cfg["CFL"],
+        "boundaries": "periodic" if cfg["bounds"][0] == 3 else "transmissive (ZOE)",
+        "l2": "working set larger than L2 (no flush)",
+        "parallelism": f"replicas x{n_gpus}",
+    }
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def hbm_peak():
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_cell(kernel):
+    """dram read+write bytes per cell of `kernel` from the committed ncu summary."""
+    try:
+        for ln in TRAFFIC_FILE.read_text().splitlines():
+            parts = ln.split()
+            if len(parts) >= 2 and parts[0] == kernel and not ln.startswith("#"):
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(w, cfg, scheme, budget_s=12.0):
+    """The oracle (CPU restatement of the reference step) on this host's cores."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    gen = w.gen
+    om = O.Mesh(gen.nx(), gen.ny(), gen.x_min, gen.x_max, gen.y_min, gen.y_max, cfg["bounds"])
+    osv = O.Solver(om, gamma=1.4, flux=O.FLUX_HLLC, limiter=cfg["lim_id"], accuracy=cfg["acc"],
+                   scheme=0 if scheme == "pc" else 1, CFL=cfg["CFL"], threads=threads)
+    osv.set_state(*w.state)
+    t0 = time.perf_counter()
+    osv.step()
+    t1 = time.perf_counter()
+    steps = 1
+    per = t1 - t0
+    extra = max(0, min(20, int(budget_s / max(per, 1e-3)) - 1))
+    if extra:
+        t0 = time.perf_counter()
+        osv.steps(extra)
+        t1 = time.perf_counter()
+        steps = extra
+        per = (t1 - t0) / extra
+    cells = gen.nx() * gen.ny()
+    return {"value": cells / per, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{steps} step(s) of the full {gen.nx()}x{gen.ny()} workload after 1 untimed step, "
+                      f"oracle restatement, {threads} std::threads"}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    w, cfg = workload(args.workload)
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    gen = w.gen
+    om = O.Mesh(gen.nx(), gen.ny(), gen.x_min, gen.x_max, gen.y_min, gen.y_max, cfg["bounds"])
+    osv = O.Solver(om, gamma=1.4, flux=O.FLUX_HLLC, limiter=cfg["lim_id"], accuracy=cfg["acc"],
+                   scheme=0 if args.scheme == "pc" else 1, CFL=cfg["CFL"], threads=threads)
+    osv.set_state(*w.state)
+    for _ in range(args.warmup):
+        osv.step()
+    t0 = time.perf_counter()
+    osv.steps(args.steps)
+    t1 = time.perf_counter()
+    cells = gen.nx() * gen.ny()
+    sec = t1 - t0
+    value = cells * args.steps / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(args, w, cfg, 1),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full steps of the {gen.nx()}x{gen.ny()} workload on the "
+                                   f"oracle restatement (std::threads={threads})"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference cannot be built here (Eigen3/Boost absent); its algorithm is timed through the "
+                "oracle restatement on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import zephyr_b200 as Z
+    from zephyr_b200._lib import KERNEL_KINDS
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    lib = Z.load()
+
+    w, cfg = workload(args.workload)
+    cells = w.gen.nx() * w.gen.ny()
+    mesh = Z.EuMesh(w.gen, device=local_rank, stream=stream.cuda_stream)
+    solver = Z.SmFluid(w.eos)
+    solver.set_accuracy(cfg["acc"])
+    solver.set_CFL(cfg["CFL"])
+    solver.set_limiter(cfg["lim"])
+    solver.set_method(Z.Fluxes.HLLC)
+    solver.set_scheme(Z.Scheme.HEUN if args.scheme == "heun" else Z.Scheme.PREDICTOR_CORRECTOR)
+    solver.add_types(mesh)
+    mesh.set_state(*w.state)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # warm-up
+    solver.update(mesh, steps=max(args.warmup, 3))
+    mesh.synchronize()
+
+    # ---- device-resident timed region -----------------------------------
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    lib.zg_set_timing(mesh.ctx, 1)
+    n0 = mesh.launch_count()
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.update(mesh, steps=args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = mesh.launch_count() - n0
+    kms = (C.c_double * 8)()
+    kcount = (C.c_longlong * 8)()
+    lib.zg_kernel_times(mesh.ctx, kms, kcount)
+    lib.zg_set_timing(mesh.ctx, 0)
+    clocks = sampler.stop()
+    dt_last = solver.dt()
+
+    # ---- end-to-end through the public API with host buffers ---------------
+    pin = [torch.empty(cells, dtype=torch.float64, pin_memory=True) for _ in range(5)]
+    for t, a in zip(pin, mesh.get_state()):
+        t.numpy()[:] = a
+    outp = [torch.empty(cells, dtype=torch.float64, pin_memory=True) for _ in range(5)]
+    P = C.POINTER(C.c_double)
+    inp_ptrs = [C.cast(C.c_void_p(t.data_ptr()), P) for t in pin]
+    out_ptrs = [C.cast(C.c_void_p(t.data_ptr()), P) for t in outp]
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize(dev)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        Z._lib.check(mesh.ctx, lib.zg_state_upload(mesh.ctx, *inp_ptrs))
+        Z._lib.check(mesh.ctx, lib.zg_smf_update(mesh.ctx))
+        Z._lib.check(mesh.ctx, lib.zg_state_download(mesh.ctx, *out_ptrs))
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_ms = f0.elapsed_time(f1)
+
+    # ---- max over ranks -------------------------------------------------------
+    vals = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_ms = float(vals[0]), float(vals[1])
+
+    if rank != 0:
+        return
+    value = world * cells * args.steps / (ms / 1e3)
+    e2e_value = world * cells * e2e_steps / (e2e_ms / 1e3)
+
+    kernels = {}
+    for k, name in enumerate(KERNEL_KINDS):
+        if kcount[k]:
+            kernels[name] = {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k],
+                             "share": kms[k] / max(sum(kms), 1e-12)}
+    top = max(kernels, key=lambda n: kernels[n]["ms_total"])
+    peak, peak_kind = hbm_peak()
+    balg = B_ALG_KERNEL[top] * cells
+    achieved = balg / (kernels[top]["ms_avg"] / 1e3) / 1e9
+    tpc = traffic_per_cell(top)
+    roof = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": (tpc * cells) if tpc is not None else None,
+            "algorithmic_bytes_per_launch": balg,
+            "step_achieved": B_ALG_STEP[cfg["acc"]] * cells * args.steps / (ms / 1e3) / 1e9}
+    roof["step_frac"] = roof["step_achieved"] / peak
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(args, w, cfg, world),
+        "roofline": roof, "kernels": kernels, "gpu_launches": int(launches), "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
+                "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
+                "note": "per step: upload of the whole state from pinned host memory, zg_smf_update, "
+                        "download of the whole state"},
+        "dt_last": dt_last,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, cfg, args.scheme)
+    print(json.dumps(line), flush=True)
+    mesh.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import datetime
+
+    import torch
+    if world > 1:
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

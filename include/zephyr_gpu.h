@@ -1,0 +1,200 @@
+/* zephyr_gpu.h -- C ABI of the B200 finite-volume step.
+ *
+ * The library replaces, on one GPU, the hot path of zephyr's single-material
+ * solver: SmFluid::update (math/solver/sm_fluid.cpp:81-102) with its CFL time
+ * step, fluxes, gradients, predictor and corrector, plus SmFluid::set_flags
+ * (sm_fluid.cpp:517-559).  Paths in the comments are relative to the zephyr
+ * source tree.
+ *
+ * Conventions
+ *   - Every call returns 0 on success and a negative ZG_ERR_* code on failure;
+ *     zg_last_error() then gives a message.  No C++ exception crosses the ABI.
+ *   - A context owns one mesh, one solver configuration and all device memory
+ *     for them, on the device it was created on.  Calls on one context must
+ *     come from one host thread at a time (like SmFluid, the reference is not
+ *     re-entrant either).
+ *   - Host arrays are plain pointers; cell i of an array is element i, with
+ *     the reference's cell numbering of a Rectangle mesh, ic = i * ny + j
+ *     (mesh/euler/amr_cells_gen.cpp:145-151).
+ *   - Work is queued on the context's stream; calls that return host data
+ *     synchronise that stream.
+ */
+#ifndef ZEPHYR_GPU_H
+#define ZEPHYR_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define ZG_OK 0
+#define ZG_ERR_ARG (-1)     /* invalid argument or size */
+#define ZG_ERR_CUDA (-2)    /* a CUDA call failed */
+#define ZG_ERR_STATE (-3)   /* call out of order (no mesh, no configuration) */
+#define ZG_ERR_ALLOC (-4)   /* device memory allocation failed */
+#define ZG_ERR_NUMERIC (-5) /* a non-finite flux or state was produced */
+
+/* Boundary flags; values of zephyr's `enum class Boundary`
+ * (geom/boundary.h:9-16). */
+enum zg_boundary {
+    ZG_BC_INNER = 0,
+    ZG_BC_WALL = 1,
+    ZG_BC_ZOE = 2,
+    ZG_BC_PERIODIC = 3
+};
+
+/* Numerical fluxes; values of zephyr's `enum class Fluxes`
+ * (math/cfd/flux/num_flux.h:11-21).  HLL and HLLC are implemented. */
+enum zg_flux {
+    ZG_FLUX_GODUNOV = 0,
+    ZG_FLUX_RUSANOV = 1,
+    ZG_FLUX_HLL = 2,
+    ZG_FLUX_HLLC = 3
+};
+
+/* Slope limiters of math/cfd/limiter.cxx:15-153 (binary forms). */
+enum zg_limiter {
+    ZG_LIM_NONE = 0,
+    ZG_LIM_UNIT,
+    ZG_LIM_MINMOD,
+    ZG_LIM_MC,
+    ZG_LIM_VANLEER,
+    ZG_LIM_VANALBADA1,
+    ZG_LIM_VANALBADA2,
+    ZG_LIM_CHARM,
+    ZG_LIM_HCUS,
+    ZG_LIM_HQUICK,
+    ZG_LIM_KOREN,
+    ZG_LIM_SMART,
+    ZG_LIM_SUPERBEE
+};
+
+/* Equations of state (phys/matter/eos/ideal_gas.cpp, stiffened_gas.cpp). */
+enum zg_eos { ZG_EOS_IDEAL = 0, ZG_EOS_STIFFENED = 1 };
+
+/* Second-order time integration.  PREDICTOR_CORRECTOR is the reference
+ * scheme (sm_fluid.cpp:89-98); HEUN is an extension: Heun's two-stage
+ * Runge-Kutta on the corrector's spatial operator. */
+enum zg_scheme { ZG_SCHEME_PREDICTOR_CORRECTOR = 0, ZG_SCHEME_HEUN = 1 };
+
+/* Arithmetic of the face loop.  FP64 is the drop-in form. */
+enum zg_precision { ZG_FP64 = 0, ZG_MIXED = 1 };
+
+/* Kernel family.  PARITY evaluates every face flux from both sides in the
+ * reference's order of operations without fused multiply-adds (bit-exact with
+ * the reference); FAST computes each face once and lets the compiler fuse. */
+enum zg_kernels { ZG_KERNELS_PARITY = 0, ZG_KERNELS_FAST = 1 };
+
+/* Solver configuration: SmFluid(Eos::Ptr) plus its setters
+ * (math/solver/sm_fluid.h:41-71; defaults sm_fluid.cpp:16-23). */
+typedef struct zg_smf_params {
+    int eos_kind;    /* zg_eos */
+    double gamma;    /* adiabatic index */
+    double P0;       /* stiffened-gas pressure constant (0 for ideal gas) */
+    double e0;       /* stiffened-gas energy constant (0 for ideal gas) */
+    int flux;        /* zg_flux; SmFluid::set_method */
+    int limiter;     /* zg_limiter; SmFluid::set_limiter */
+    int accuracy;    /* 1 or 2, clamped like SmFluid::set_accuracy */
+    int scheme;      /* zg_scheme */
+    int precision;   /* zg_precision */
+    int kernels;     /* zg_kernels */
+    double CFL;      /* clamped to [0, 1] like SmFluid::set_CFL */
+    double max_dt;   /* SmFluid::set_max_dt */
+} zg_smf_params;
+
+typedef struct zg_ctx zg_ctx;
+
+/* Fill `p` with SmFluid's constructor defaults (sm_fluid.cpp:16-23):
+ * HLLC, MC limiter, CFL 0.5, first order, no dt cap; ideal gas gamma 1.4. */
+void zg_smf_default_params(zg_smf_params *p);
+
+/* Map a limiter name to zg_limiter with the rules of Limiter(name)
+ * (limiter.cxx:163-252); returns -1 for an unknown name. */
+int zg_limiter_from_name(const char *name);
+
+/* Create a context on CUDA device `device`. */
+int zg_create(zg_ctx **out, int device);
+int zg_destroy(zg_ctx *ctx);
+const char *zg_last_error(const zg_ctx *ctx);
+
+/* Use `stream` (a cudaStream_t) for all later work; NULL selects the
+ * context's own stream. */
+int zg_set_stream(zg_ctx *ctx, void *stream);
+
+/* Build the mesh of Rectangle(x_min, x_max, y_min, y_max) with nx by ny
+ * cells and boundary flags {left, right, bottom, top}; replaces
+ * EuMesh(const Rectangle&) (mesh/euler/eu_mesh.cpp:70-102 ->
+ * mesh/euler/amr_cells_gen.cpp:128-281).  PERIODIC on one side of an axis
+ * makes both sides periodic (geom/generator/rectangle.cpp:182-189).  Any
+ * previous state is discarded. */
+int zg_mesh_rectangle(zg_ctx *ctx, int nx, int ny, double x_min, double x_max, double y_min,
+                      double y_max, const int bounds[4]);
+int zg_mesh_n_cells(const zg_ctx *ctx, int *n);
+
+/* Configure the solver; replaces SmFluid(eos) and its setters.  The first
+ * call allocates the solver's fields (SmFluid::add_types, sm_fluid.cpp:25-35)
+ * with zero state and isolation counters; later calls only change the
+ * parameters and keep the data, as the reference's setters do. */
+int zg_smf_configure(zg_ctx *ctx, const zg_smf_params *p);
+int zg_smf_set_max_dt(zg_ctx *ctx, double max_dt);
+
+/* Copy the primitive state of every cell (the field `init`: density,
+ * velocity x, velocity y, pressure, specific internal energy) from / to host
+ * arrays of n_cells doubles each. */
+int zg_state_upload(zg_ctx *ctx, const double *rho, const double *vx, const double *vy, const double *p,
+                    const double *e);
+int zg_state_download(zg_ctx *ctx, double *rho, double *vx, double *vy, double *p, double *e);
+
+/* Isolation counters (the field `wait`, sm_fluid.cpp:354-364). */
+int zg_wait_upload(zg_ctx *ctx, const int *wait);
+int zg_wait_download(zg_ctx *ctx, int *wait);
+
+/* One time step; replaces SmFluid::update (sm_fluid.cpp:81-102).
+ * Asynchronous: the step's dt stays on the device until zg_smf_dt. */
+int zg_smf_update(zg_ctx *ctx);
+
+/* `n_steps` consecutive steps without host synchronisation (a driver's time
+ * loop with a fixed max_dt). */
+int zg_smf_update_n(zg_ctx *ctx, int n_steps);
+
+/* dt of the last step; replaces SmFluid::dt() (sm_fluid.h:68).
+ * Synchronises the stream. */
+int zg_smf_dt(zg_ctx *ctx, double *dt);
+
+/* Refinement flags of every cell into a host array of n_cells ints
+ * (-1 coarsen, 0 keep, 1 refine); replaces the flag loop of
+ * SmFluid::set_flags (sm_fluid.cpp:524-559). */
+int zg_smf_set_flags(zg_ctx *ctx, int *flags);
+
+/* Number of kernels this context has launched (for launch accounting). */
+int zg_launch_count(const zg_ctx *ctx, long long *count);
+
+/* Kernel kinds reported by zg_kernel_times. */
+enum zg_kernel_kind {
+    ZG_K_DT = 0,      /* CFL minimum (SmFluid::compute_dt) */
+    ZG_K_FLUX1,       /* first-order step (SmFluid::fluxes) */
+    ZG_K_GRAD,        /* limited gradients (SmFluid::compute_grad) */
+    ZG_K_STAGE1,      /* predictor (SmFluid::fluxes_stage1) */
+    ZG_K_STAGE2,      /* corrector (SmFluid::fluxes_stage2) */
+    ZG_K_HEUN_A,      /* Heun first stage */
+    ZG_K_HEUN_B,      /* Heun second stage */
+    ZG_K_FLAGS,       /* refinement flags */
+    ZG_K_COUNT
+};
+
+/* Per-kernel device timing.  While enabled, every kernel launch is bracketed
+ * by CUDA events on the context's stream.  zg_kernel_times synchronises the
+ * stream, adds the elapsed times of all launches since the previous call into
+ * ms[ZG_K_COUNT] and launches[ZG_K_COUNT] (either may be NULL), and resets. */
+int zg_set_timing(zg_ctx *ctx, int on);
+int zg_kernel_times(zg_ctx *ctx, double *ms, long long *launches);
+const char *zg_kernel_name(int kind);
+
+/* Wait for the context's stream. */
+int zg_synchronize(zg_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZEPHYR_GPU_H */

@@ -1,0 +1,100 @@
+"""ctypes binding of ``libzephyr_gpu.so`` (the C ABI in include/zephyr_gpu.h).
+
+The shared library is built in-tree by ``zephyr_b200.build``.  There is no
+fallback: if the library is missing or a call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libzephyr_gpu.so"
+
+ZG_OK = 0
+_ERR_NAMES = {-1: "ZG_ERR_ARG", -2: "ZG_ERR_CUDA", -3: "ZG_ERR_STATE", -4: "ZG_ERR_ALLOC", -5: "ZG_ERR_NUMERIC"}
+
+
+class ZgError(RuntimeError):
+    """A C-ABI call returned a negative status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{_ERR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class SmfParams(C.Structure):
+    _fields_ = [
+        ("eos_kind", C.c_int),
+        ("gamma", C.c_double),
+        ("P0", C.c_double),
+        ("e0", C.c_double),
+        ("flux", C.c_int),
+        ("limiter", C.c_int),
+        ("accuracy", C.c_int),
+        ("scheme", C.c_int),
+        ("precision", C.c_int),
+        ("kernels", C.c_int),
+        ("CFL", C.c_double),
+        ("max_dt", C.c_double),
+    ]
+
+
+_P = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_V = C.c_void_p
+
+# name -> (restype, argtypes); every symbol include/zephyr_gpu.h declares.
+SIGNATURES = {
+    "zg_smf_default_params": (None, [C.POINTER(SmfParams)]),
+    "zg_limiter_from_name": (C.c_int, [C.c_char_p]),
+    "zg_create": (C.c_int, [C.POINTER(_V), C.c_int]),
+    "zg_destroy": (C.c_int, [_V]),
+    "zg_last_error": (C.c_char_p, [_V]),
+    "zg_set_stream": (C.c_int, [_V, _V]),
+    "zg_mesh_rectangle": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I]),
+    "zg_mesh_n_cells": (C.c_int, [_V, _I]),
+    "zg_smf_configure": (C.c_int, [_V, C.POINTER(SmfParams)]),
+    "zg_smf_set_max_dt": (C.c_int, [_V, C.c_double]),
+    "zg_state_upload": (C.c_int, [_V, _P, _P, _P, _P, _P]),
+    "zg_state_download": (C.c_int, [_V, _P, _P, _P, _P, _P]),
+    "zg_wait_upload": (C.c_int, [_V, _I]),
+    "zg_wait_download": (C.c_int, [_V, _I]),
+    "zg_smf_update": (C.c_int, [_V]),
+    "zg_smf_update_n": (C.c_int, [_V, C.c_int]),
+    "zg_smf_dt": (C.c_int, [_V, _P]),
+    "zg_smf_set_flags": (C.c_int, [_V, _I]),
+    "zg_launch_count": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
+    "zg_synchronize": (C.c_int, [_V]),
+    "zg_set_timing": (C.c_int, [_V, C.c_int]),
+    "zg_kernel_times": (C.c_int, [_V, _P, C.POINTER(C.c_longlong)]),
+    "zg_kernel_name": (C.c_char_p, [C.c_int]),
+}
+
+# enum zg_kernel_kind
+KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags"]
+
+_lib = None
+
+
+def load():
+    """Load the library (once) and declare the signatures."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build the CUDA extension first "
+                "(python -m zephyr_b200.build); there is no CPU fallback")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(ctx, rc: int):
+    if rc != ZG_OK:
+        msg = load().zg_last_error(ctx) if ctx else b""
+        raise ZgError(rc, (msg or b"").decode(errors="replace"))
+    return rc

@@ -1,0 +1,71 @@
+"""Build the in-tree CUDA library ``zephyr_b200/libzephyr_gpu.so`` for sm_100a.
+
+Each translation unit is compiled with nvcc to an object, then linked into one
+shared library.  The parity kernels are compiled with ``-fmad=false`` so that
+no multiply is fused into an add (bit-exact with the reference's x86-64
+build); the other kernels keep nvcc's default contraction.
+
+Run ``python -m zephyr_b200.build`` (or ``__graft_entry__.build()``).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+OUT = PKG / "libzephyr_gpu.so"
+BUILD = PKG / "_build"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+          "--expt-relaxed-constexpr"]
+
+# translation unit -> extra flags
+UNITS = {
+    "zg_api.cu": [],
+    "smf_parity.cu": ["-fmad=false"],
+}
+
+
+def nvcc() -> str:
+    exe = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(exe).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build zephyr_b200")
+    return exe
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "zephyr_gpu.h"]
+    objs = []
+    for unit, extra in UNITS.items():
+        src = CSRC / unit
+        obj = BUILD / (unit + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src, *headers, Path(__file__)]):
+            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if force or _stale(OUT, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-cudart", "static"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(OUT)

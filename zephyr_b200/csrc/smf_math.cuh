@@ -1,0 +1,243 @@
+// smf_math.cuh -- pointwise FP64 numerics of zephyr's single-material step,
+// written for sm_100a.  The FP64 forms keep the reference's operation order
+// term by term; translation units that include this header for the parity
+// kernels are compiled with -fmad=false so that no product is fused into an
+// add, which makes the results bit-identical to the reference's x86-64 build
+// (apart from the signs of exact zeros).
+//
+// Reference lines (zephyr source tree):
+//   EoS            phys/matter/eos/ideal_gas.cpp:32-106, stiffened_gas.cpp:103-175
+//   PState/QState  math/cfd/models.cpp:27-32 (P from Q), 85-89 (Q from P), 131-137 (Flux)
+//   is_bad         math/cfd/models.cpp:58-63
+//   HLLC           math/cfd/flux/hllc.cpp:23-83
+//   HLL            math/cfd/flux/hll.cpp:23-57
+//   limiters       math/cfd/limiter.cxx:15-153 (binary forms)
+//   rotation       math/cfd/rotate.cpp:7-77 (2-D branch)
+#pragma once
+
+#include <cstdint>
+
+namespace zg {
+
+enum : int { EOS_IDEAL = 0, EOS_STIFFENED = 1 };
+enum : int { FLUX_GODUNOV = 0, FLUX_RUSANOV = 1, FLUX_HLL = 2, FLUX_HLLC = 3 };
+enum : int {
+    LIM_NONE = 0, LIM_UNIT, LIM_MINMOD, LIM_MC, LIM_VANLEER, LIM_VANALBADA1, LIM_VANALBADA2,
+    LIM_CHARM, LIM_HCUS, LIM_HQUICK, LIM_KOREN, LIM_SMART, LIM_SUPERBEE
+};
+enum : int { BC_UNDEFINED = -1, BC_INNER = 0, BC_WALL = 1, BC_ZOE = 2, BC_PERIODIC = 3, BC_FUNCTION = 4 };
+
+// amr_faces.h:157-161
+__host__ __device__ inline bool is_boundary(int flag) {
+    return flag != BC_INNER && flag != BC_PERIODIC && flag != BC_UNDEFINED;
+}
+
+// std::min / std::max as the reference uses them (NaN in the second slot
+// loses, ties return the first argument).
+__host__ __device__ inline double smin(double a, double b) { return (b < a) ? b : a; }
+__host__ __device__ inline double smax(double a, double b) { return (a < b) ? b : a; }
+
+// Correctly rounded x^3 (stands in for glibc pow(x, 3) in gradient.h:256):
+// Dekker/Knuth error-free products give x^3 = q + qe + pe*x exactly, and the
+// final sum rounds once.  Exact whenever x^3 is representable.
+__host__ __device__ inline double cube_rn(double x) {
+    double p = x * x;
+    double pe = fma(x, x, -p);
+    double q = p * x;
+    double qe = fma(p, x, -q);
+    return q + (qe + pe * x);
+}
+
+struct EosD {
+    int kind;
+    double gamma, gm1, P0, e0, pmin;
+
+    __device__ inline double pressure_re(double rho, double e) const {
+        if (kind == EOS_IDEAL) return gm1 * rho * e;
+        return gm1 * rho * (e - e0) - gamma * P0;
+    }
+    __device__ inline double energy_rP(double rho, double P) const {
+        if (kind == EOS_IDEAL) return P / (gm1 * rho);
+        return e0 + (P + gamma * P0) / (gm1 * rho);
+    }
+    __device__ inline double sound_speed_rP(double rho, double P) const {
+        if (kind == EOS_IDEAL) return sqrt(gamma * P / rho);
+        return sqrt(gamma * (P + P0) / rho);
+    }
+};
+
+// 2-D primitive state (the reference's PState with vz == 0).
+struct Prim {
+    double r, u, v, p, e;
+};
+// Conservative vector / flux (density, momentum x, momentum y, total energy).
+struct Cons {
+    double r, mu, mv, E;
+};
+
+__device__ inline double v2(const Prim &z) { return z.u * z.u + z.v * z.v; }
+
+// models.cpp:85-89
+__device__ inline Cons q_from_p(const Prim &z) {
+    Cons q;
+    q.r = z.r;
+    q.mu = z.r * z.u;
+    q.mv = z.r * z.v;
+    q.E = z.r * (z.e + 0.5 * v2(z));
+    return q;
+}
+// models.cpp:27-32
+__device__ inline Prim p_from_q(const Cons &q, const EosD &eos) {
+    Prim z;
+    z.r = q.r;
+    z.u = q.mu / z.r;
+    z.v = q.mv / z.r;
+    z.e = q.E / z.r - 0.5 * v2(z);
+    z.p = eos.pressure_re(z.r, z.e);
+    return z;
+}
+// models.cpp:131-137
+__device__ inline Cons flux_from_p(const Prim &z) {
+    Cons f;
+    double ru = z.r * z.u;
+    f.r = ru;
+    f.mu = ru * z.u + z.p;
+    f.mv = ru * z.v;
+    f.E = (z.r * (z.e + 0.5 * v2(z)) + z.p) * z.u;
+    return f;
+}
+// models.cpp:58-63
+__device__ inline bool is_bad(const Prim &z, const EosD &eos) {
+    if (!isfinite(z.r) || !isfinite(z.p) || !isfinite(z.e)) return true;
+    return z.r <= 0.0 || z.p < eos.pmin;
+}
+
+// rotate.cpp:7-41: velocity into the frame of the unit normal (c, s).
+__device__ inline void rot_local(double &u, double &v, double c, double s) {
+    double a = c * u + s * v;
+    double b = -s * u + c * v;
+    u = a;
+    v = b;
+}
+// rotate.cpp:43-77
+__device__ inline void rot_global(double &u, double &v, double c, double s) {
+    double a = c * u + -s * v;
+    double b = s * u + c * v;
+    u = a;
+    v = b;
+}
+
+// hllc.cpp:23-83
+__device__ inline Cons hllc(const Prim &zL, const Prim &zR, const EosD &eos) {
+    double c_L = eos.sound_speed_rP(zL.r, zL.p);
+    double c_R = eos.sound_speed_rP(zR.r, zR.p);
+    double S_L = smin(zL.u - c_L, zR.u - c_R);
+    double S_R = smax(zL.u + c_L, zR.u + c_R);
+    if (S_L >= 0.0) return flux_from_p(zL);
+    if (S_R <= 0.0) return flux_from_p(zR);
+
+    double a_L = zL.r * (S_L - zL.u);
+    double a_R = zR.r * (S_R - zR.u);
+    double S_C = (zL.p - zR.p + a_R * zR.u - a_L * zL.u) / (a_R - a_L);
+    double rho_sL = a_L / (S_L - S_C);
+    double rho_sR = a_R / (S_R - S_C);
+    double EL = zL.e + 0.5 * v2(zL);
+    double ER = zR.e + 0.5 * v2(zR);
+    double E_sL = EL + (S_C - zL.u) * (S_C + zL.p / a_L);
+    double E_sR = ER + (S_C - zR.u) * (S_C + zR.p / a_R);
+
+    Cons QsL{rho_sL, rho_sL * S_C, rho_sL * zL.v, rho_sL * E_sL};
+    Cons QsR{rho_sR, rho_sR * S_C, rho_sR * zR.v, rho_sR * E_sR};
+    Cons QL = q_from_p(zL), QR = q_from_p(zR);
+    Cons FL = flux_from_p(zL), FR = flux_from_p(zR);
+    double aSC = fabs(S_C);
+    Cons F;
+    F.r = 0.5 * (FL.r + FR.r + S_L * (QsL.r - QL.r) + aSC * (QsL.r - QsR.r) + S_R * (QsR.r - QR.r));
+    F.mu = 0.5 * (FL.mu + FR.mu + S_L * (QsL.mu - QL.mu) + aSC * (QsL.mu - QsR.mu) + S_R * (QsR.mu - QR.mu));
+    F.mv = 0.5 * (FL.mv + FR.mv + S_L * (QsL.mv - QL.mv) + aSC * (QsL.mv - QsR.mv) + S_R * (QsR.mv - QR.mv));
+    F.E = 0.5 * (FL.E + FR.E + S_L * (QsL.E - QL.E) + aSC * (QsL.E - QsR.E) + S_R * (QsR.E - QR.E));
+    return F;
+}
+
+// hll.cpp:23-57
+__device__ inline Cons hll(const Prim &zL, const Prim &zR, const EosD &eos) {
+    double c_L = eos.sound_speed_rP(zL.r, zL.p);
+    double c_R = eos.sound_speed_rP(zR.r, zR.p);
+    double S_L = smin(zL.u - c_L, smin(zR.u - c_R, 0.0));
+    double S_R = smax(zL.u + c_L, smax(zR.u + c_R, 0.0));
+    Cons QL = q_from_p(zL), QR = q_from_p(zR);
+    Cons FL = flux_from_p(zL), FR = flux_from_p(zR);
+    double SLR = S_L * S_R;
+    double den = S_R - S_L;
+    Cons F;
+    F.r = (S_R * FL.r - S_L * FR.r + SLR * (QR.r - QL.r)) / den;
+    F.mu = (S_R * FL.mu - S_L * FR.mu + SLR * (QR.mu - QL.mu)) / den;
+    F.mv = (S_R * FL.mv - S_L * FR.mv + SLR * (QR.mv - QL.mv)) / den;
+    F.E = (S_R * FL.E - S_L * FR.E + SLR * (QR.E - QL.E)) / den;
+    return F;
+}
+
+__device__ inline Cons num_flux(int kind, const Prim &zL, const Prim &zR, const EosD &eos) {
+    return kind == FLUX_HLL ? hll(zL, zR, eos) : hllc(zL, zR, eos);
+}
+
+// limiter.cxx binary forms phi(a, b)
+__device__ inline double lim_MC1(double r) {
+    if (isnan(r)) return 0.0;
+    return smax(0.0, smin(2 * r, smin(0.5 * (1.0 + r), 2.0)));
+}
+__device__ inline double limiter2(int kind, double a, double b) {
+    switch (kind) {
+        case LIM_NONE: return 0.0;
+        case LIM_UNIT: return 1.0;
+        case LIM_MINMOD:
+            if (a * b <= 0.0) return 0.0;
+            return smin(a / b, 1.0);
+        case LIM_MC: return lim_MC1(a / b);
+        case LIM_VANLEER:
+            if (a * b < 0.0) return 0.0;
+            if (a == 0.0) return 0.0;
+            return 2 * fabs(a) / (fabs(a) + fabs(b));
+        case LIM_VANALBADA1:
+            if (a * b <= 0.0) return 0.0;
+            if (b == 0.0) return 1.0;
+            return a * (a + b) / (a * a + b * b);
+        case LIM_VANALBADA2: {
+            if (a * b <= 0.0) return 0.0;
+            const double eps = 10e-6;
+            return (2.0 * a * b + eps) / (a * a + b * b + eps);
+        }
+        case LIM_CHARM: {
+            if (a * b <= 0.0) return 0.0;
+            double s = a + b;
+            return a * (3 * a + b) / (s * s);
+        }
+        case LIM_HCUS:
+            if (a * b <= 0.0) return 0.0;
+            return (3.0 * a) / (a + 2.0 * b);
+        case LIM_HQUICK:
+            if (a * b <= 0.0) return 0.0;
+            return (4.0 * a) / (a + 3.0 * b);
+        case LIM_KOREN: {
+            double r = a / b;
+            if (isnan(r)) return 0.0;
+            return smax(0.0, smin(2 * r, smin(2.0, (1 + 2 * r) / 3.0)));
+        }
+        case LIM_SMART: {
+            double r = a / b;
+            if (isnan(r)) return 0.0;
+            return smax(0.0, smin(2.0 * r, smin(0.25 + 0.75 * r, 4.0)));
+        }
+        case LIM_SUPERBEE: {
+            double r = a / b;
+            if (isnan(r)) return 0.0;
+            return smax(0.0, smin(smin(2 * r, 1.0), smin(r, 2.0)));
+        }
+        default: return 0.0;
+    }
+}
+
+// Ordered-integer image of a non-negative double, for atomicMin reductions.
+__device__ inline unsigned long long dbits(double x) { return (unsigned long long)__double_as_longlong(x); }
+
+}  // namespace zg

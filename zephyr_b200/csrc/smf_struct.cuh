@@ -1,0 +1,479 @@
+// smf_struct.cuh -- FP64 kernels of SmFluid::update on a structured
+// rectangle (zephyr's AmrCells(Rectangle) without refinement), in the
+// reference's per-cell gather form: every cell walks its face slots in the
+// order L, R, B, T and evaluates each face flux in its own frame, exactly as
+// math/solver/sm_fluid.cpp does.  Compiled with -fmad=false these kernels are
+// the parity path.
+//
+// Cell numbering follows amr_cells_gen.cpp:145-151: ic = i * ny + j.  Face
+// geometry is derived from per-axis tables that the host fills with the
+// reference's own formulas (amr_cells_gen.cpp:158-253, quad.cpp:429-436).
+#pragma once
+
+#include "smf_math.cuh"
+#include "smf_types.h"
+
+namespace zg {
+
+// ---------------------------------------------------------------------------
+// Face geometry of slot s (0 L, 1 R, 2 B, 3 T) of cell (i, j).
+struct FaceG {
+    int flag;     // boundary flag of the slot
+    int nb;       // neighbour cell (the cell itself on boundary slots)
+    double nx, ny;  // outward unit normal
+    double fcx, fcy;  // face centre
+    double area;
+};
+
+__device__ inline FaceG face_geo(const StructMesh &m, int i, int j, int ic, int s) {
+    FaceG g;
+    if (s == 0) {
+        g.flag = i > 0 ? BC_INNER : m.bc[0];
+        g.nb = i > 0 ? ic - m.ny : (m.xper ? ic + (m.nx - 1) * m.ny : ic);
+        g.nx = -1.0; g.ny = -0.0;
+        g.fcx = m.X[i]; g.fcy = m.fym[j];
+        g.area = m.hy;
+    } else if (s == 1) {
+        g.flag = i < m.nx - 1 ? BC_INNER : m.bc[1];
+        g.nb = i < m.nx - 1 ? ic + m.ny : (m.xper ? ic - (m.nx - 1) * m.ny : ic);
+        g.nx = 1.0; g.ny = 0.0;
+        g.fcx = m.X[i + 1]; g.fcy = m.fym[j];
+        g.area = m.hy;
+    } else if (s == 2) {
+        g.flag = j > 0 ? BC_INNER : m.bc[2];
+        g.nb = j > 0 ? ic - 1 : (m.yper ? ic + (m.ny - 1) : ic);
+        g.nx = -0.0; g.ny = -1.0;
+        g.fcx = m.fxm[i]; g.fcy = m.Y[j];
+        g.area = m.hx;
+    } else {
+        g.flag = j < m.ny - 1 ? BC_INNER : m.bc[3];
+        g.nb = j < m.ny - 1 ? ic + 1 : (m.yper ? ic - (m.ny - 1) : ic);
+        g.nx = 0.0; g.ny = 1.0;
+        g.fcx = m.fxm[i]; g.fcy = m.Y[j + 1];
+        g.area = m.hx;
+    }
+    return g;
+}
+
+// Centre of the neighbour across slot s, or the mirror of the cell centre in
+// the face (sm_fluid.cpp:211-212; amr_faces.h:197-199 symm_point).
+__device__ inline void neib_center(const StructMesh &m, const FaceG &g, int i, int j, int s, double pcx,
+                                   double pcy, double &ncx, double &ncy) {
+    if (g.flag == BC_INNER) {
+        int in = i, jn = j;
+        if (s == 0) in = i - 1;
+        else if (s == 1) in = i + 1;
+        else if (s == 2) jn = j - 1;
+        else jn = j + 1;
+        ncx = m.cx[in];
+        ncy = m.cy[jn];
+    } else {
+        double d = (g.fcx - pcx) * g.nx + (g.fcy - pcy) * g.ny;
+        double t = 2.0 * d;
+        ncx = pcx + t * g.nx;
+        ncy = pcy + t * g.ny;
+    }
+}
+
+__device__ inline Prim load_prim(const PrimPtr &z, int ic) {
+    Prim s;
+    s.r = z.r[ic];
+    s.u = z.u[ic];
+    s.v = z.v[ic];
+    s.p = z.p[ic];
+    s.e = z.e[ic];
+    return s;
+}
+__device__ inline void store_prim(const PrimPtr &z, int ic, const Prim &s) {
+    z.r[ic] = s.r;
+    z.u[ic] = s.u;
+    z.v[ic] = s.v;
+    z.p[ic] = s.p;
+    z.e[ic] = s.e;
+}
+
+// sm_fluid.cpp:69-79
+__device__ inline Prim boundary_value(const Prim &zc, double nx, double ny, int flag) {
+    if (flag != BC_WALL) return zc;
+    Prim zn = zc;
+    double d = zc.u * nx + zc.v * ny;
+    double vx = nx * d, vy = ny * d;
+    zn.u = zc.u - 2.0 * vx;
+    zn.v = zc.v - 2.0 * vy;
+    return zn;
+}
+
+// dt of the current step, written by the last block of k_dt.
+__device__ inline double finalize_dt(const SmfArgs &a) { return *a.dt_out; }
+
+// ---------------------------------------------------------------------------
+// K1: CFL minimum over cells (sm_fluid.cpp:104-114, amr_cells.cpp:107-116).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_dt(SmfArgs a) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
+    if (ic < m.n) {
+        int i = ic / m.ny, j = ic - i * m.ny;
+        double rho = a.z.r[ic], u = a.z.u[ic], v = a.z.v[ic], p = a.z.p[ic];
+        double c = a.eos.sound_speed_rP(rho, p);
+        double dinc = sqrt(smin(m.inc2x[i], m.inc2y[j]));
+        double lam = dinc / (sqrt(u * u + v * v) + c);
+        // std::min skips a NaN in its second slot; NaN bits sort above all
+        // finite positives, so the unsigned minimum skips it too.
+        unsigned long long b = dbits(lam);
+        if (!(lam >= 0.0)) b = 0x7FEFFFFFFFFFFFFFull;
+        best = b;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+        best = t < best ? t : best;
+    }
+    __shared__ unsigned long long sm[BLOCK / 32];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        best = threadIdx.x < BLOCK / 32 ? sm[threadIdx.x] : 0x7FEFFFFFFFFFFFFFull;
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+            best = t < best ? t : best;
+        }
+        if (threadIdx.x == 0) {
+            atomicMin(a.dmin_bits, best);
+            // The last block to finish turns the minimum into
+            // dt = min(CFL * min, max_dt) (sm_fluid.cpp:112) and resets the
+            // accumulator for the next step.  No block waits for another.
+            __threadfence();
+            unsigned int ticket = atomicAdd(a.dt_ticket, 1u);
+            if (ticket == gridDim.x - 1) {
+                unsigned long long bits = atomicMin(a.dmin_bits, 0x7FEFFFFFFFFFFFFFull);
+                double dmin = __longlong_as_double((long long)bits);
+                *a.dt_out = smin(a.CFL * dmin, a.max_dt);
+                *a.dmin_bits = 0x7FEFFFFFFFFFFFFFull;
+                *a.dt_ticket = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// K2: first-order step (sm_fluid.cpp:127-174).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_flux1(SmfArgs a) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= m.n) return;
+    double dt = finalize_dt(a);
+    int i = ic / m.ny, j = ic - i * m.ny;
+    Prim zc = load_prim(a.z, ic);
+    Cons q = q_from_p(zc);
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = face_geo(m, i, j, ic, s);
+        Prim zn = !is_boundary(g.flag) ? load_prim(a.z, g.nb) : boundary_value(zc, g.nx, g.ny, g.flag);
+        Prim zm = zc, zp = zn;
+        rot_local(zm.u, zm.v, g.nx, g.ny);
+        rot_local(zp.u, zp.v, g.nx, g.ny);
+        Cons lf = num_flux(a.flux, zm, zp, a.eos);
+        rot_global(lf.mu, lf.mv, g.nx, g.ny);
+        F.r += lf.r * g.area;
+        F.mu += lf.mu * g.area;
+        F.mv += lf.mv * g.area;
+        F.E += lf.E * g.area;
+    }
+    double coef = dt / m.vol;
+    q.r -= coef * F.r;
+    q.mu -= coef * F.mu;
+    q.mv -= coef * F.mv;
+    q.E -= coef * F.E;
+    store_prim(a.znext, ic, p_from_q(q, a.eos));
+}
+
+// ---------------------------------------------------------------------------
+// K3: least-squares gradient and its limited re-fit
+// (gradient.h:226-282 LSM, gradient.h:412-474 limiting), for the four
+// fields that the later stages read: density, vx, vy, pressure.  (The energy
+// gradient is computed by the reference but every use overwrites it with
+// energy_rP, sm_fluid.cpp:223 and 312/322.)
+//
+// 2-D reduction of the 3x3 system: A(i,2) and A(2,j) are exact zeros, A(2,2)
+// is set to 1 (gradient.h:268-273), and Eigen's cofactor inverse then gives
+//   det = A11*A00 + (-A01)*A10,  B = [A11 -A01; -A10 A00] * (1/det).
+__device__ inline void lsm_limited(const StructMesh &m, const PrimPtr &z, int lim, int ic, int i, int j,
+                                   const Prim &zc, double gx[4], double gy[4]) {
+    double pcx = m.cx[i], pcy = m.cy[j];
+    double wv[4], drx[4], dry[4], drnx[4], drny[4], dn[4][4];
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
+    double Fx[4] = {0.0, 0.0, 0.0, 0.0}, Fy[4] = {0.0, 0.0, 0.0, 0.0};
+    const double zcv[4] = {zc.r, zc.u, zc.v, zc.p};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = face_geo(m, i, j, ic, s);
+        Prim zn = !is_boundary(g.flag) ? load_prim(z, g.nb) : boundary_value(zc, g.nx, g.ny, g.flag);
+        double ncx, ncy;
+        neib_center(m, g, i, j, s, pcx, pcy, ncx, ncy);
+        double rx = ncx - pcx, ry = ncy - pcy;
+        double d = rx * g.nx + ry * g.ny;
+        double nxx = d * g.nx, nyy = d * g.ny;
+        double w = g.area / cube_rn(sqrt(nxx * nxx + nyy * nyy));
+        double wdx = w * nxx, wdy = w * nyy;
+        A00 += wdx * rx;
+        A01 += wdx * ry;
+        A10 += wdy * rx;
+        A11 += wdy * ry;
+        wv[s] = w; drx[s] = rx; dry[s] = ry; drnx[s] = nxx; drny[s] = nyy;
+        const double znv[4] = {zn.r, zn.u, zn.v, zn.p};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double dF = znv[k] - zcv[k];
+            dn[s][k] = dF;
+            Fx[k] += w * dF * nxx;
+            Fy[k] += w * dF * nyy;
+        }
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;  // 1-D case (gradient.h:270-272)
+    double det = A11 * A00 + (-A01) * A10;
+    double inv = 1.0 / det;
+    double B00 = A11 * inv, B01 = (-A01) * inv, B10 = (-A10) * inv, B11 = A00 * inv;
+    double g0x[4], g0y[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        g0x[k] = B00 * Fx[k] + B01 * Fy[k];
+        g0y[k] = B10 * Fx[k] + B11 * Fy[k];
+    }
+    double Lx[4] = {0.0, 0.0, 0.0, 0.0}, Ly[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double dF_p = dn[s][k];
+            double du_n = g0x[k] * drx[s] + g0y[k] * dry[s];
+            double dF_m = 2.0 * du_n - dF_p;
+            double dF_lim = limiter2(lim, dF_m, dF_p) * dF_p;
+            Lx[k] += wv[s] * dF_lim * drnx[s];
+            Ly[k] += wv[s] * dF_lim * drny[s];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        gx[k] = B00 * Lx[k] + B01 * Ly[k];
+        gy[k] = B10 * Lx[k] + B11 * Ly[k];
+    }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_grad(SmfArgs a, PrimPtr z) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= m.n) return;
+    int i = ic / m.ny, j = ic - i * m.ny;
+    Prim zc = load_prim(z, ic);
+    double gx[4], gy[4];
+    lsm_limited(m, z, a.limiter, ic, i, j, zc, gx, gy);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        a.gx[k][ic] = gx[k];
+        a.gy[k][ic] = gy[k];
+    }
+}
+
+// face_extra.h:135-163: value + grad . (x_face - x_cell); the energy entry
+// is recomputed from the EoS by every caller.
+__device__ inline Prim extrap(const Prim &u, const SmfArgs &a, int ic, double dx, double dy) {
+    Prim o;
+    o.r = u.r + (a.gx[0][ic] * dx + a.gy[0][ic] * dy);
+    o.u = u.u + (a.gx[1][ic] * dx + a.gy[1][ic] * dy);
+    o.v = u.v + (a.gx[2][ic] * dx + a.gy[2][ic] * dy);
+    o.p = u.p + (a.gx[3][ic] * dx + a.gy[3][ic] * dy);
+    o.e = 0.0;
+    return o;
+}
+
+// ---------------------------------------------------------------------------
+// K4: predictor, half step with the physical flux (sm_fluid.cpp:176-253).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_stage1(SmfArgs a) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= m.n) return;
+    double dt = finalize_dt(a);
+    Prim zc = load_prim(a.z, ic);
+    if (a.wait_in[ic] > 0) {
+        store_prim(a.zhalf, ic, zc);
+        return;
+    }
+    int i = ic / m.ny, j = ic - i * m.ny;
+    double pcx = m.cx[i], pcy = m.cy[j];
+    Cons q = q_from_p(zc);
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = face_geo(m, i, j, ic, s);
+        Prim zm = extrap(zc, a, ic, g.fcx - pcx, g.fcy - pcy);
+        zm.e = a.eos.energy_rP(zm.r, zm.p);
+        if (is_bad(zm, a.eos)) zm = zc;
+        rot_local(zm.u, zm.v, g.nx, g.ny);
+        Cons lf = flux_from_p(zm);
+        rot_global(lf.mu, lf.mv, g.nx, g.ny);
+        F.r += lf.r * g.area;
+        F.mu += lf.mu * g.area;
+        F.mv += lf.mv * g.area;
+        F.E += lf.E * g.area;
+    }
+    double coef = 0.5 * dt / m.vol;
+    q.r -= coef * F.r;
+    q.mu -= coef * F.mu;
+    q.mv -= coef * F.mv;
+    q.E -= coef * F.E;
+    Prim h = p_from_q(q, a.eos);
+    if (is_bad(h, a.eos)) h = zc;
+    store_prim(a.zhalf, ic, h);
+}
+
+// Face flux of the corrector (sm_fluid.cpp:271-341): reconstruct with the
+// gradients of z at the states zh and solve the Riemann problem.
+__device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &z, const PrimPtr &zh, const int *wt,
+                                      int ic, int i, int j, int s, const Prim &zc, const Prim &zch,
+                                      double pcx, double pcy, int wc) {
+    const StructMesh &m = a.mesh;
+    FaceG g = face_geo(m, i, j, ic, s);
+    bool bnd = is_boundary(g.flag);
+    Prim z_nh = !bnd ? load_prim(zh, g.nb) : boundary_value(zch, g.nx, g.ny, g.flag);
+    Prim zm, zp;
+    bool robust = wc > 0 || (wt != nullptr && wt[g.nb] > 0);
+    if (robust) {
+        zm = zch;
+        zp = z_nh;
+    } else {
+        double ncx, ncy;
+        neib_center(m, g, i, j, s, pcx, pcy, ncx, ncy);
+        zm = extrap(zch, a, ic, g.fcx - pcx, g.fcy - pcy);
+        zm.e = a.eos.energy_rP(zm.r, zm.p);
+        if (is_bad(zm, a.eos)) zm = zch;
+        if (!bnd) {
+            zp = extrap(z_nh, a, g.nb, g.fcx - ncx, g.fcy - ncy);
+            zp.e = a.eos.energy_rP(zp.r, zp.p);
+            if (is_bad(zp, a.eos)) zp = z_nh;
+        } else {
+            zp = boundary_value(zm, g.nx, g.ny, g.flag);
+        }
+    }
+    rot_local(zm.u, zm.v, g.nx, g.ny);
+    rot_local(zp.u, zp.v, g.nx, g.ny);
+    Cons lf = robust ? hll(zm, zp, a.eos) : num_flux(a.flux, zm, zp, a.eos);
+    rot_global(lf.mu, lf.mv, g.nx, g.ny);
+    lf.r *= g.area;
+    lf.mu *= g.area;
+    lf.mv *= g.area;
+    lf.E *= g.area;
+    return lf;
+}
+
+// K5: corrector with the isolation bit (sm_fluid.cpp:255-366).  `wait` is
+// read from the previous step's array and written to the other one.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_stage2(SmfArgs a) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= m.n) return;
+    double dt = finalize_dt(a);
+    int i = ic / m.ny, j = ic - i * m.ny;
+    double pcx = m.cx[i], pcy = m.cy[j];
+    Prim zc = load_prim(a.z, ic);
+    Prim zch = load_prim(a.zhalf, ic);
+    int wc = a.wait_in[ic];
+    Cons q = q_from_p(zc);
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        Cons lf = corrector_face(a, a.z, a.zhalf, a.wait_in, ic, i, j, s, zc, zch, pcx, pcy, wc);
+        F.r += lf.r;
+        F.mu += lf.mu;
+        F.mv += lf.mv;
+        F.E += lf.E;
+    }
+    double coef = dt / m.vol;
+    q.r -= coef * F.r;
+    q.mu -= coef * F.mu;
+    q.mv -= coef * F.mv;
+    q.E -= coef * F.E;
+    Prim n = p_from_q(q, a.eos);
+    int wn = wc;
+    if (is_bad(n, a.eos)) {
+        n = zc;
+        wn = 3;
+    } else if (wn > 0) {
+        --wn;
+    }
+    store_prim(a.znext, ic, n);
+    a.wait_out[ic] = wn;
+}
+
+// ---------------------------------------------------------------------------
+// Heun extension (no counterpart in the reference; same operator L as the
+// corrector with z_half = z, no isolation):
+//   stage A: z* = P(Q(z^n) - dt/V * sum F(z^n))
+//   stage B: z^{n+1} = P(0.5 * (Q(z^n) + Q(z*) - dt/V * sum F(z*)))
+template <int BLOCK, bool FINAL>
+__global__ void __launch_bounds__(BLOCK) k_heun(SmfArgs a, PrimPtr zin, PrimPtr zout) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= m.n) return;
+    double dt = finalize_dt(a);
+    int i = ic / m.ny, j = ic - i * m.ny;
+    double pcx = m.cx[i], pcy = m.cy[j];
+    Prim zc = load_prim(zin, ic);
+    Cons q = q_from_p(zc);
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        Cons lf = corrector_face(a, zin, zin, nullptr, ic, i, j, s, zc, zc, pcx, pcy, 0);
+        F.r += lf.r;
+        F.mu += lf.mu;
+        F.mv += lf.mv;
+        F.E += lf.E;
+    }
+    double coef = dt / m.vol;
+    q.r -= coef * F.r;
+    q.mu -= coef * F.mu;
+    q.mv -= coef * F.mv;
+    q.E -= coef * F.E;
+    if (FINAL) {
+        Cons q0 = q_from_p(load_prim(a.z, ic));
+        q.r = 0.5 * (q0.r + q.r);
+        q.mu = 0.5 * (q0.mu + q.mu);
+        q.mv = 0.5 * (q0.mv + q.mv);
+        q.E = 0.5 * (q0.E + q.E);
+    }
+    store_prim(zout, ic, p_from_q(q, a.eos));
+}
+
+// ---------------------------------------------------------------------------
+// AMR flags by neighbour jumps (sm_fluid.cpp:517-559).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_flags(SmfArgs a, int *flags) {
+    const StructMesh &m = a.mesh;
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= m.n) return;
+    int i = ic / m.ny, j = ic - i * m.ny;
+    const double xi_dens = 0.05, xi_pres = 0.05;
+    double dens = a.z.r[ic], pres = a.z.p[ic];
+    double dens_split = xi_dens * fabs(dens);
+    double pres_split = xi_pres * fabs(pres);
+    int fl = -1;
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = face_geo(m, i, j, ic, s);
+        if (is_boundary(g.flag)) continue;
+        double dn = a.z.r[g.nb], pn = a.z.p[g.nb];
+        if (fabs(dn - dens) > dens_split || fabs(pn - pres) > pres_split) {
+            fl = 1;
+            break;
+        }
+        if (fabs(dn - dens) > 0.4 * dens_split || fabs(pn - pres) > 0.4 * pres_split) fl = 0;
+    }
+    flags[ic] = fl;
+}
+
+}  // namespace zg

@@ -1,0 +1,560 @@
+// zg_api.cu -- the C ABI declared in include/zephyr_gpu.h: context, device
+// memory, mesh tables and the orchestration of SmFluid::update on one GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/zephyr_gpu.h"
+#include "smf_types.h"
+
+using namespace zg;
+
+struct zg_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long launches = 0;
+
+    // mesh (structured rectangle)
+    bool have_mesh = false;
+    int nx = 0, ny = 0, n = 0;
+    StructMesh mesh{};
+    double *d_geo = nullptr;  // all geometry tables
+
+    // solver
+    bool configured = false;
+    zg_smf_params par{};
+    EosD eos{};
+    double *d_state = nullptr;  // init/half/next (5 fields each) + 8 gradient fields
+    int *d_wait = nullptr;      // two isolation-counter buffers
+    unsigned long long *d_dmin = nullptr;
+    unsigned int *d_ticket = nullptr;
+    double *d_dt = nullptr;
+    int *d_flags = nullptr;
+    PrimPtr z{}, zhalf{}, znext{};
+    double *gx[4] = {}, *gy[4] = {};
+    int wait_cur = 0;  // index of the buffer holding the current counters
+    bool stepped = false;
+
+    // per-kernel timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, int>> ev_pending;  // (kind, index of the start event)
+    size_t ev_used = 0;
+};
+
+namespace {
+
+int fail(zg_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(zg_ctx *c, cudaError_t e, const char *what) {
+    return fail(c, e == cudaErrorMemoryAllocation ? ZG_ERR_ALLOC : ZG_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define ZG_CUDA(ctx, call)                                  \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void free_solver(zg_ctx *c) {
+    cudaFree(c->d_state);
+    cudaFree(c->d_wait);
+    cudaFree(c->d_dmin);
+    cudaFree(c->d_flags);
+    c->d_state = nullptr;
+    c->d_wait = nullptr;
+    c->d_dmin = nullptr;
+    c->d_ticket = nullptr;
+    c->d_dt = nullptr;
+    c->d_flags = nullptr;
+    c->configured = false;
+    c->stepped = false;
+}
+
+void free_mesh(zg_ctx *c) {
+    cudaFree(c->d_geo);
+    c->d_geo = nullptr;
+    c->have_mesh = false;
+}
+
+SmfArgs make_args(const zg_ctx *c) {
+    SmfArgs a{};
+    a.mesh = c->mesh;
+    a.eos = c->eos;
+    a.flux = c->par.flux;
+    a.limiter = c->par.limiter;
+    a.CFL = c->par.CFL;
+    a.max_dt = c->par.max_dt;
+    a.z = c->z;
+    a.zhalf = c->zhalf;
+    a.znext = c->znext;
+    for (int k = 0; k < 4; ++k) {
+        a.gx[k] = c->gx[k];
+        a.gy[k] = c->gy[k];
+    }
+    a.wait_in = c->d_wait + (size_t)c->wait_cur * c->n;
+    a.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->n;
+    a.dmin_bits = c->d_dmin;
+    a.dt_ticket = c->d_ticket;
+    a.dt_out = c->d_dt;
+    return a;
+}
+
+std::string lower_strip(const char *name) {
+    std::string s;
+    for (const char *p = name; *p; ++p) s.push_back((char)std::tolower((unsigned char)*p));
+    auto erase_all = [&s](const std::string &t) {
+        size_t pos;
+        while ((pos = s.find(t)) != std::string::npos) s.erase(pos, t.size());
+    };
+    erase_all(" ");
+    erase_all("-");
+    erase_all("_");
+    erase_all("lim");
+    erase_all("limiter");
+    return s;
+}
+
+// Bracket one launch with timing events when timing is on.
+template <class F>
+void timed(zg_ctx *c, int kind, F &&launch) {
+    c->launches += 1;
+    if (!c->timing) {
+        launch();
+        return;
+    }
+    if (c->ev_used + 2 > c->ev_pool.size()) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            c->ev_pool.push_back(e);
+        }
+    }
+    int i0 = (int)c->ev_used;
+    c->ev_used += 2;
+    cudaEventRecord(c->ev_pool[i0], c->stream);
+    launch();
+    cudaEventRecord(c->ev_pool[i0 + 1], c->stream);
+    c->ev_pending.emplace_back(kind, i0);
+}
+
+// One step of SmFluid::update (sm_fluid.cpp:81-102) as kernel launches.
+int enqueue_step(zg_ctx *c) {
+    SmfArgs a = make_args(c);
+    void *st = (void *)c->stream;
+    timed(c, ZG_K_DT, [&] { parity::launch_dt(a, c->z, st); });
+    if (c->par.accuracy == 1) {
+        timed(c, ZG_K_FLUX1, [&] { parity::launch_flux1(a, st); });
+    } else if (c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
+        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, st); });
+        timed(c, ZG_K_STAGE1, [&] { parity::launch_stage1(a, st); });
+        timed(c, ZG_K_STAGE2, [&] { parity::launch_stage2(a, st); });
+        c->wait_cur = 1 - c->wait_cur;
+    } else {
+        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, st); });
+        timed(c, ZG_K_HEUN_A, [&] { parity::launch_heun(a, c->z, c->zhalf, false, st); });
+        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->zhalf, st); });
+        timed(c, ZG_K_HEUN_B, [&] { parity::launch_heun(a, c->zhalf, c->znext, true, st); });
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    std::swap(c->z, c->znext);  // Storage::swap of init and next (sm_fluid.cpp:368-370)
+    c->stepped = true;
+    return ZG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void zg_smf_default_params(zg_smf_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->eos_kind = ZG_EOS_IDEAL;
+    p->gamma = 1.4;
+    p->P0 = 0.0;
+    p->e0 = 0.0;
+    p->flux = ZG_FLUX_HLLC;
+    p->limiter = ZG_LIM_MC;
+    p->accuracy = 1;
+    p->scheme = ZG_SCHEME_PREDICTOR_CORRECTOR;
+    p->precision = ZG_FP64;
+    p->kernels = ZG_KERNELS_PARITY;
+    p->CFL = 0.5;
+    p->max_dt = std::numeric_limits<double>::max();
+}
+
+int zg_limiter_from_name(const char *name) {
+    if (!name) return -1;
+    std::string s = lower_strip(name);
+    auto has = [&s](const char *t) { return s.find(t) != std::string::npos; };
+    if (s.empty() || has("off") || has("none") || has("zero") || has("empty")) return ZG_LIM_NONE;
+    if (has("one") || has("unit")) return ZG_LIM_UNIT;
+    if (has("minmod")) return ZG_LIM_MINMOD;
+    if (has("mc")) return ZG_LIM_MC;
+    if (has("leer")) return ZG_LIM_VANLEER;
+    if (has("albada")) return has("2") ? ZG_LIM_VANALBADA2 : ZG_LIM_VANALBADA1;
+    if (has("charm")) return ZG_LIM_CHARM;
+    if (has("hcus")) return ZG_LIM_HCUS;
+    if (has("hquick")) return ZG_LIM_HQUICK;
+    if (has("koren")) return ZG_LIM_KOREN;
+    if (has("smart")) return ZG_LIM_SMART;
+    if (has("superbee")) return ZG_LIM_SUPERBEE;
+    return -1;
+}
+
+int zg_create(zg_ctx **out, int device) {
+    if (!out) return ZG_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return ZG_ERR_CUDA;
+    auto *c = new zg_ctx();
+    c->device = device;
+    DeviceGuard g(device);
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return ZG_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return ZG_OK;
+}
+
+int zg_destroy(zg_ctx *c) {
+    if (!c) return ZG_ERR_ARG;
+    {
+        DeviceGuard g(c->device);
+        cudaStreamSynchronize(c->stream);
+        free_solver(c);
+        free_mesh(c);
+        for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+        if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    }
+    delete c;
+    return ZG_OK;
+}
+
+const char *zg_last_error(const zg_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+int zg_set_stream(zg_ctx *c, void *stream) {
+    if (!c) return ZG_ERR_ARG;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return ZG_OK;
+}
+
+int zg_mesh_rectangle(zg_ctx *c, int nx, int ny, double x_min, double x_max, double y_min, double y_max,
+                      const int bounds[4]) {
+    if (!c) return ZG_ERR_ARG;
+    if (nx < 1 || ny < 1 || !bounds) return fail(c, ZG_ERR_ARG, "zg_mesh_rectangle: nx, ny >= 1 and bounds required");
+    if ((long long)nx * ny > (long long)std::numeric_limits<int>::max() / 8)
+        return fail(c, ZG_ERR_ARG, "zg_mesh_rectangle: too many cells for 32-bit cell indices");
+    if (!(x_max > x_min) || !(y_max > y_min)) return fail(c, ZG_ERR_ARG, "zg_mesh_rectangle: empty box");
+    for (int k = 0; k < 4; ++k) {
+        if (bounds[k] < ZG_BC_INNER || bounds[k] > ZG_BC_PERIODIC || bounds[k] == ZG_BC_INNER)
+            return fail(c, ZG_ERR_ARG, "zg_mesh_rectangle: boundary flags must be WALL, ZOE or PERIODIC");
+    }
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_solver(c);
+    free_mesh(c);
+
+    int bc[4] = {bounds[0], bounds[1], bounds[2], bounds[3]};
+    bool xper = bc[0] == ZG_BC_PERIODIC || bc[1] == ZG_BC_PERIODIC;
+    bool yper = bc[2] == ZG_BC_PERIODIC || bc[3] == ZG_BC_PERIODIC;
+    if (xper) bc[0] = bc[1] = ZG_BC_PERIODIC;
+    if (yper) bc[2] = bc[3] = ZG_BC_PERIODIC;
+
+    // Geometry tables with the reference's formulas:
+    //   vertices  amr_cells_gen.cpp:155-161  x_min + ((x_max - x_min) * i) / nx
+    //   centre    quad.cpp:434               0.25 * (v00 + v01 + v10 + v11)
+    //   mid-edges quad.cpp:433-435           0.5 * (a + b)
+    //   incircle  amr_cells.cpp:107-116      |vs<+1,0> - vs<-1,0>|^2, |vs<0,+1> - vs<0,-1>|^2
+    std::vector<double> X(nx + 1), Y(ny + 1), cx(nx), cy(ny), fxm(nx), fym(ny), i2x(nx), i2y(ny);
+    for (int i = 0; i <= nx; ++i) X[i] = x_min + ((x_max - x_min) * i) / nx;
+    for (int j = 0; j <= ny; ++j) Y[j] = y_min + ((y_max - y_min) * j) / ny;
+    for (int i = 0; i < nx; ++i) {
+        cx[i] = 0.25 * (X[i] + X[i + 1] + X[i] + X[i + 1]);
+        fxm[i] = 0.5 * (X[i] + X[i + 1]);
+        double d = 0.5 * (X[i + 1] + X[i + 1]) - 0.5 * (X[i] + X[i]);
+        i2x[i] = d * d + 0.0 * 0.0 + 0.0 * 0.0;
+    }
+    for (int j = 0; j < ny; ++j) {
+        cy[j] = 0.25 * (Y[j] + Y[j] + Y[j + 1] + Y[j + 1]);
+        fym[j] = 0.5 * (Y[j] + Y[j + 1]);
+        double d = 0.5 * (Y[j + 1] + Y[j + 1]) - 0.5 * (Y[j] + Y[j]);
+        i2y[j] = 0.0 * 0.0 + d * d + 0.0 * 0.0;
+    }
+    size_t total = (size_t)(nx + 1) + (ny + 1) + 3 * (size_t)nx + 3 * (size_t)ny + 2 * (size_t)nx + 2 * (size_t)ny;
+    ZG_CUDA(c, cudaMalloc(&c->d_geo, total * sizeof(double)));
+    std::vector<double> host;
+    host.reserve(total);
+    auto put = [&host](const std::vector<double> &v) {
+        size_t off = host.size();
+        host.insert(host.end(), v.begin(), v.end());
+        return off;
+    };
+    size_t oX = put(X), oY = put(Y), ocx = put(cx), ocy = put(cy), ofx = put(fxm), ofy = put(fym),
+           oix = put(i2x), oiy = put(i2y);
+    ZG_CUDA(c, cudaMemcpy(c->d_geo, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+    StructMesh &m = c->mesh;
+    m.nx = nx;
+    m.ny = ny;
+    m.n = nx * ny;
+    for (int k = 0; k < 4; ++k) m.bc[k] = bc[k];
+    m.xper = xper;
+    m.yper = yper;
+    m.X = c->d_geo + oX;
+    m.Y = c->d_geo + oY;
+    m.cx = c->d_geo + ocx;
+    m.cy = c->d_geo + ocy;
+    m.fxm = c->d_geo + ofx;
+    m.fym = c->d_geo + ofy;
+    m.inc2x = c->d_geo + oix;
+    m.inc2y = c->d_geo + oiy;
+    m.hx = (x_max - x_min) / nx;
+    m.hy = (y_max - y_min) / ny;
+    m.vol = m.hx * m.hy;
+    c->nx = nx;
+    c->ny = ny;
+    c->n = m.n;
+    c->have_mesh = true;
+    return ZG_OK;
+}
+
+int zg_mesh_n_cells(const zg_ctx *c, int *n) {
+    if (!c || !n) return ZG_ERR_ARG;
+    *n = c->have_mesh ? c->n : 0;
+    return ZG_OK;
+}
+
+int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
+    if (!c || !p) return ZG_ERR_ARG;
+    if (!c->have_mesh) return fail(c, ZG_ERR_STATE, "zg_smf_configure: no mesh");
+    if (p->eos_kind != ZG_EOS_IDEAL && p->eos_kind != ZG_EOS_STIFFENED)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown EoS");
+    if (p->flux != ZG_FLUX_HLLC && p->flux != ZG_FLUX_HLL)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: only HLL and HLLC fluxes are implemented");
+    if (p->limiter < ZG_LIM_NONE || p->limiter > ZG_LIM_SUPERBEE)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown limiter");
+    if (p->scheme != ZG_SCHEME_PREDICTOR_CORRECTOR && p->scheme != ZG_SCHEME_HEUN)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown scheme");
+    if (p->precision != ZG_FP64) return fail(c, ZG_ERR_ARG, "zg_smf_configure: unsupported precision");
+    if (p->kernels != ZG_KERNELS_PARITY) return fail(c, ZG_ERR_ARG, "zg_smf_configure: unsupported kernels");
+    if (!(p->gamma > 1.0)) return fail(c, ZG_ERR_ARG, "zg_smf_configure: gamma must exceed 1");
+
+    DeviceGuard g(c->device);
+    c->par = *p;
+    c->par.accuracy = std::min(std::max(1, p->accuracy), 2);        // sm_fluid.cpp:41-43
+    c->par.CFL = std::max(0.0, std::min(p->CFL, 1.0));               // sm_fluid.cpp:37-39
+    c->eos.kind = p->eos_kind;
+    c->eos.gamma = p->gamma;
+    c->eos.gm1 = p->gamma - 1.0;
+    c->eos.P0 = p->eos_kind == ZG_EOS_IDEAL ? 0.0 : p->P0;
+    c->eos.e0 = p->eos_kind == ZG_EOS_IDEAL ? 0.0 : p->e0;
+    c->eos.pmin = p->eos_kind == ZG_EOS_IDEAL ? 0.0 : -p->P0;  // min_pressure()
+    if (c->configured) return ZG_OK;  // fields exist already: keep the state (setters do not reset data)
+
+    size_t n = (size_t)c->n;
+    size_t nfields = 3 * 5 + 8;
+    ZG_CUDA(c, cudaMalloc(&c->d_state, nfields * n * sizeof(double)));
+    ZG_CUDA(c, cudaMalloc(&c->d_wait, 2 * n * sizeof(int)));
+    ZG_CUDA(c, cudaMalloc(&c->d_flags, n * sizeof(int)));
+    ZG_CUDA(c, cudaMalloc(&c->d_dmin, 64));
+    c->d_ticket = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dmin) + 8);
+    c->d_dt = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_dmin) + 16);
+    double *b = c->d_state;
+    auto take = [&b, n]() {
+        double *p0 = b;
+        b += n;
+        return p0;
+    };
+    PrimPtr *sets[3] = {&c->z, &c->zhalf, &c->znext};
+    for (PrimPtr *s : sets) {
+        s->r = take();
+        s->u = take();
+        s->v = take();
+        s->p = take();
+        s->e = take();
+    }
+    for (int k = 0; k < 4; ++k) c->gx[k] = take();
+    for (int k = 0; k < 4; ++k) c->gy[k] = take();
+    ZG_CUDA(c, cudaMemsetAsync(c->d_state, 0, nfields * n * sizeof(double), c->stream));
+    ZG_CUDA(c, cudaMemsetAsync(c->d_wait, 0, 2 * n * sizeof(int), c->stream));
+    unsigned long long init[3] = {0x7FEFFFFFFFFFFFFFull, 0ull, 0ull};
+    double nan = std::numeric_limits<double>::quiet_NaN();
+    std::memcpy(&init[2], &nan, sizeof(double));
+    ZG_CUDA(c, cudaMemcpyAsync(c->d_dmin, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->wait_cur = 0;
+    c->configured = true;
+    return ZG_OK;
+}
+
+int zg_smf_set_max_dt(zg_ctx *c, double max_dt) {
+    if (!c) return ZG_ERR_ARG;
+    c->par.max_dt = max_dt;
+    return ZG_OK;
+}
+
+int zg_state_upload(zg_ctx *c, const double *rho, const double *vx, const double *vy, const double *p,
+                    const double *e) {
+    if (!c || !rho || !vx || !vy || !p || !e) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_state_upload: solver not configured");
+    DeviceGuard g(c->device);
+    size_t bytes = (size_t)c->n * sizeof(double);
+    const double *src[5] = {rho, vx, vy, p, e};
+    double *dst[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
+    for (int k = 0; k < 5; ++k)
+        ZG_CUDA(c, cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyHostToDevice, c->stream));
+    return ZG_OK;
+}
+
+int zg_state_download(zg_ctx *c, double *rho, double *vx, double *vy, double *p, double *e) {
+    if (!c || !rho || !vx || !vy || !p || !e) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_state_download: solver not configured");
+    DeviceGuard g(c->device);
+    size_t bytes = (size_t)c->n * sizeof(double);
+    double *dst[5] = {rho, vx, vy, p, e};
+    const double *src[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
+    for (int k = 0; k < 5; ++k)
+        ZG_CUDA(c, cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_wait_upload(zg_ctx *c, const int *wait) {
+    if (!c || !wait) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_wait_upload: solver not configured");
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(c->d_wait + (size_t)c->wait_cur * c->n, wait, (size_t)c->n * sizeof(int),
+                               cudaMemcpyHostToDevice, c->stream));
+    return ZG_OK;
+}
+
+int zg_wait_download(zg_ctx *c, int *wait) {
+    if (!c || !wait) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_wait_download: solver not configured");
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(wait, c->d_wait + (size_t)c->wait_cur * c->n, (size_t)c->n * sizeof(int),
+                               cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_smf_update(zg_ctx *c) {
+    if (!c) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_update: solver not configured");
+    DeviceGuard g(c->device);
+    return enqueue_step(c);
+}
+
+int zg_smf_update_n(zg_ctx *c, int n_steps) {
+    if (!c || n_steps < 0) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_update_n: solver not configured");
+    DeviceGuard g(c->device);
+    for (int k = 0; k < n_steps; ++k) {
+        int rc = enqueue_step(c);
+        if (rc != ZG_OK) return rc;
+    }
+    return ZG_OK;
+}
+
+int zg_smf_dt(zg_ctx *c, double *dt) {
+    if (!c || !dt) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_dt: solver not configured");
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(dt, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_smf_set_flags(zg_ctx *c, int *flags) {
+    if (!c || !flags) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_set_flags: solver not configured");
+    DeviceGuard g(c->device);
+    SmfArgs a = make_args(c);
+    timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, c->d_flags, (void *)c->stream); });
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "flags kernel launch");
+    ZG_CUDA(c, cudaMemcpyAsync(flags, c->d_flags, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost,
+                               c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_launch_count(const zg_ctx *c, long long *count) {
+    if (!c || !count) return ZG_ERR_ARG;
+    *count = c->launches;
+    return ZG_OK;
+}
+
+int zg_synchronize(zg_ctx *c) {
+    if (!c) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_set_timing(zg_ctx *c, int on) {
+    if (!c) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->timing = on != 0;
+    c->ev_pending.clear();
+    c->ev_used = 0;
+    return ZG_OK;
+}
+
+int zg_kernel_times(zg_ctx *c, double *ms, long long *launches) {
+    if (!c) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (ms)
+        for (int k = 0; k < ZG_K_COUNT; ++k) ms[k] = 0.0;
+    if (launches)
+        for (int k = 0; k < ZG_K_COUNT; ++k) launches[k] = 0;
+    for (auto &pe : c->ev_pending) {
+        float t = 0.0f;
+        ZG_CUDA(c, cudaEventElapsedTime(&t, c->ev_pool[pe.second], c->ev_pool[pe.second + 1]));
+        if (ms) ms[pe.first] += t;
+        if (launches) launches[pe.first] += 1;
+    }
+    c->ev_pending.clear();
+    c->ev_used = 0;
+    return ZG_OK;
+}
+
+const char *zg_kernel_name(int kind) {
+    static const char *names[ZG_K_COUNT] = {"dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b",
+                                            "flags"};
+    return (kind >= 0 && kind < ZG_K_COUNT) ? names[kind] : "unknown";
+}
+
+}  // extern "C"

@@ -1,0 +1,339 @@
+"""Host-side mirror of zephyr's single-material solver API on the B200 library.
+
+The classes keep the reference's names and argument meaning so that a driver
+such as problems/single-fluid/smf_test_2D.cpp:34-160 reads the same:
+
+    gen = Rectangle(0.0, 1.0, 0.0, 1.0)          # geom/generator/rectangle.h
+    gen.set_boundaries(Boundaries(ZOE, ZOE, ZOE, ZOE))
+    gen.set_nx(256)                              # rectangle.cpp:105-118
+    mesh = EuMesh(gen)                           # mesh/euler/eu_mesh.h
+    solver = SmFluid(IdealGas(1.4))              # math/solver/sm_fluid.h:41
+    solver.set_accuracy(2); solver.set_CFL(0.4)
+    solver.set_limiter("van Albada"); solver.set_method(Fluxes.HLLC)
+    part = solver.add_types(mesh)                # sm_fluid.cpp:25-35
+    mesh.set_state(rho, vx, vy, p, e)            # the driver's init loop
+    solver.update(mesh)                          # sm_fluid.cpp:81-102
+    solver.dt()
+
+Cell data cross the boundary as host arrays in the reference's numbering
+(ic = i * ny + j).  Errors raise ZgError (the reference throws
+std::runtime_error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import SmfParams, ZgError, check, load
+
+
+class Boundary(enum.IntEnum):
+    """geom/boundary.h:9-16"""
+    UNDEFINED = -1
+    INNER = 0
+    WALL = 1
+    ZOE = 2
+    PERIODIC = 3
+    FUNCTION = 4
+
+
+class Fluxes(enum.IntEnum):
+    """math/cfd/flux/num_flux.h:11-21"""
+    GODUNOV = 0
+    RUSANOV = 1
+    HLL = 2
+    HLLC = 3
+    HLLC_M = 4
+    HLLC_LM = 5
+    CIR1 = 6
+    CIR2 = 7
+    CRP = 8
+
+
+class Scheme(enum.IntEnum):
+    PREDICTOR_CORRECTOR = 0  # the reference scheme (sm_fluid.cpp:89-98)
+    HEUN = 1                 # extension: Heun RK2 on the corrector's operator
+
+
+class Precision(enum.IntEnum):
+    FP64 = 0
+    MIXED = 1
+
+
+class Kernels(enum.IntEnum):
+    PARITY = 0
+    FAST = 1
+
+
+@dataclass(frozen=True)
+class IdealGas:
+    """phys/matter/eos/ideal_gas.cpp: P = (gamma - 1) rho e."""
+    gamma: float = 1.4
+    kind = 0
+    P0 = 0.0
+    e0 = 0.0
+
+    def energy_rP(self, rho, P):  # ideal_gas.cpp:50-57
+        return P / ((self.gamma - 1.0) * rho)
+
+    def pressure_re(self, rho, e):  # ideal_gas.cpp:32-39
+        return (self.gamma - 1.0) * rho * e
+
+
+@dataclass(frozen=True)
+class StiffenedGas:
+    """phys/matter/eos/stiffened_gas.cpp: P = (gamma - 1) rho (e - e0) - gamma P0."""
+    gamma: float
+    P0: float = 0.0
+    e0: float = 0.0
+    kind = 1
+
+    def energy_rP(self, rho, P):  # stiffened_gas.cpp:121-128
+        return self.e0 + (P + self.gamma * self.P0) / ((self.gamma - 1.0) * rho)
+
+    def pressure_re(self, rho, e):  # stiffened_gas.cpp:103-110
+        return (self.gamma - 1.0) * rho * (e - self.e0) - self.gamma * self.P0
+
+
+@dataclass
+class Boundaries:
+    """geom/generator/rectangle.h Boundaries {left, right, bottom, top}."""
+    left: int = Boundary.ZOE
+    right: int = Boundary.ZOE
+    bottom: int = Boundary.ZOE
+    top: int = Boundary.ZOE
+
+
+class Rectangle:
+    """geom/generator/rectangle.{h,cpp} (the non-Voronoi generator)."""
+
+    def __init__(self, x_min, x_max, y_min, y_max):
+        self.x_min, self.x_max, self.y_min, self.y_max = map(float, (x_min, x_max, y_min, y_max))
+        self.bounds = Boundaries()
+        self.m_nx = self.m_ny = 1
+
+    def set_boundaries(self, bounds: Boundaries):  # rectangle.cpp:182-189
+        b = Boundaries(bounds.left, bounds.right, bounds.bottom, bounds.top)
+        if Boundary.PERIODIC in (b.left, b.right):
+            b.left = b.right = Boundary.PERIODIC
+        if Boundary.PERIODIC in (b.bottom, b.top):
+            b.bottom = b.top = Boundary.PERIODIC
+        self.bounds = b
+
+    def set_nx(self, nx: int):  # rectangle.cpp:105-118
+        if nx < 1:
+            raise ValueError("Rectangle: Nx < 1")
+        self.m_nx = nx
+        self.m_ny = max(int(_round_half_away(nx * (self.y_max - self.y_min) / (self.x_max - self.x_min))), 1)
+
+    def set_ny(self, ny: int):  # rectangle.cpp:120-133
+        if ny < 1:
+            raise ValueError("Rectangle: Ny < 1")
+        self.m_ny = ny
+        self.m_nx = max(int(_round_half_away(ny * (self.x_max - self.x_min) / (self.y_max - self.y_min))), 1)
+
+    def set_sizes(self, nx: int, ny: int):  # rectangle.cpp:135-162
+        if nx < 1 or ny < 1:
+            raise ValueError("Rectangle: Nx < 1 or Ny < 1")
+        self.m_nx, self.m_ny = nx, ny
+
+    def nx(self):
+        return self.m_nx
+
+    def ny(self):
+        return self.m_ny
+
+
+def _round_half_away(x):
+    """std::round: halves away from zero."""
+    return math.floor(x + 0.5) if x >= 0 else -math.floor(-x + 0.5)
+
+
+class EuMesh:
+    """mesh/euler/eu_mesh.h over one GPU context.  Owns the device data."""
+
+    def __init__(self, gen: Rectangle, device: int = 0, stream=None):
+        self._lib = load()
+        self.ctx = C.c_void_p()
+        check(None, self._lib.zg_create(C.byref(self.ctx), device))
+        self.device = device
+        if stream is not None:
+            self.set_stream(stream)
+        b = (C.c_int * 4)(int(gen.bounds.left), int(gen.bounds.right), int(gen.bounds.bottom),
+                          int(gen.bounds.top))
+        check(self.ctx, self._lib.zg_mesh_rectangle(self.ctx, gen.nx(), gen.ny(), gen.x_min, gen.x_max,
+                                                    gen.y_min, gen.y_max, b))
+        self.nx, self.ny = gen.nx(), gen.ny()
+        self.gen = gen
+        self.solver = None
+
+    def set_stream(self, stream):
+        """Queue all work on `stream` (a cudaStream_t handle as int, or None)."""
+        handle = int(stream) if stream is not None else None
+        check(self.ctx, self._lib.zg_set_stream(self.ctx, C.c_void_p(handle) if handle else None))
+
+    def n_cells(self) -> int:
+        n = C.c_int()
+        check(self.ctx, self._lib.zg_mesh_n_cells(self.ctx, C.byref(n)))
+        return n.value
+
+    def centers(self):
+        """Cell centres (x, y) in cell order, with the reference's formulas."""
+        g = self.gen
+        X = g.x_min + ((g.x_max - g.x_min) * np.arange(g.nx() + 1)) / g.nx()
+        Y = g.y_min + ((g.y_max - g.y_min) * np.arange(g.ny() + 1)) / g.ny()
+        cx = 0.25 * (((X[:-1] + X[1:]) + X[:-1]) + X[1:])
+        cy = 0.25 * (((Y[:-1] + Y[:-1]) + Y[1:]) + Y[1:])
+        return np.repeat(cx, g.ny()), np.tile(cy, g.nx())
+
+    def _require_solver(self):
+        if self.solver is None:
+            raise ZgError(-3, "no solver fields on this mesh: call SmFluid.add_types(mesh) first")
+
+    def set_state(self, rho, vx, vy, p, e):
+        """Write the primitive state (field `init`) of every cell."""
+        self._require_solver()
+        n = self.n_cells()
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, vx, vy, p, e)]
+        for a in arrs:
+            if a.shape != (n,):
+                raise ZgError(-1, f"state arrays must have shape ({n},)")
+        ptrs = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in arrs]
+        check(self.ctx, self._lib.zg_state_upload(self.ctx, *ptrs))
+        check(self.ctx, self._lib.zg_synchronize(self.ctx))
+
+    def get_state(self):
+        """(density, vx, vy, pressure, energy) host arrays of the field `init`."""
+        self._require_solver()
+        n = self.n_cells()
+        out = [np.empty(n) for _ in range(5)]
+        check(self.ctx, self._lib.zg_state_download(self.ctx, *[a.ctypes.data_as(C.POINTER(C.c_double))
+                                                                 for a in out]))
+        return out
+
+    def set_wait(self, wait):
+        self._require_solver()
+        w = np.ascontiguousarray(wait, dtype=np.int32)
+        check(self.ctx, self._lib.zg_wait_upload(self.ctx, w.ctypes.data_as(C.POINTER(C.c_int))))
+        check(self.ctx, self._lib.zg_synchronize(self.ctx))
+
+    def get_wait(self):
+        self._require_solver()
+        w = np.empty(self.n_cells(), np.int32)
+        check(self.ctx, self._lib.zg_wait_download(self.ctx, w.ctypes.data_as(C.POINTER(C.c_int))))
+        return w
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        check(self.ctx, self._lib.zg_launch_count(self.ctx, C.byref(n)))
+        return n.value
+
+    def synchronize(self):
+        check(self.ctx, self._lib.zg_synchronize(self.ctx))
+
+    def close(self):
+        if getattr(self, "ctx", None) and self.ctx.value:
+            self._lib.zg_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Parts:
+    """SmFluid::Parts (sm_fluid.h:26-36): names of the solver's fields."""
+    init: str = "init"
+    half: str = "half"
+    next: str = "next"
+    d_dx: str = "d_dx"
+    d_dy: str = "d_dy"
+    d_dz: str = "d_dz"
+    wait: str = "wait"
+
+
+class SmFluid:
+    """math/solver/sm_fluid.{h,cpp} on the GPU."""
+
+    def __init__(self, eos, precision: Precision = Precision.FP64, kernels: Kernels = Kernels.PARITY):
+        self._lib = load()
+        p = SmfParams()
+        self._lib.zg_smf_default_params(C.byref(p))  # sm_fluid.cpp:16-23
+        p.eos_kind, p.gamma, p.P0, p.e0 = eos.kind, eos.gamma, eos.P0, eos.e0
+        p.precision, p.kernels = int(precision), int(kernels)
+        self.params = p
+        self.eos = eos
+        self.mesh = None
+        self.part = Parts()
+
+    def _push(self):
+        if self.mesh is not None:
+            check(self.mesh.ctx, self._lib.zg_smf_configure(self.mesh.ctx, C.byref(self.params)))
+
+    def add_types(self, mesh: EuMesh) -> Parts:  # sm_fluid.cpp:25-35
+        self.mesh = mesh
+        mesh.solver = self
+        self._push()
+        return self.part
+
+    def set_CFL(self, CFL: float):  # sm_fluid.cpp:37-39
+        self.params.CFL = max(0.0, min(float(CFL), 1.0))
+        self._push()
+
+    def set_accuracy(self, acc: int):  # sm_fluid.cpp:41-43
+        self.params.accuracy = min(max(1, int(acc)), 2)
+        self._push()
+
+    def set_method(self, method: Fluxes):  # sm_fluid.cpp:49-51
+        if int(method) not in (Fluxes.HLL, Fluxes.HLLC):
+            raise ZgError(-1, f"numerical flux {Fluxes(method).name} is not implemented on the GPU")
+        self.params.flux = int(method)
+        self._push()
+
+    def set_limiter(self, name: str):  # sm_fluid.cpp:53-55 -> limiter.cxx:163-252
+        k = self._lib.zg_limiter_from_name(name.encode())
+        if k < 0:
+            raise ZgError(-1, f"Unknown limiter '{name}'")
+        self.params.limiter = k
+        self._push()
+
+    def set_scheme(self, scheme: Scheme):
+        self.params.scheme = int(scheme)
+        self._push()
+
+    def set_max_dt(self, dt: float):  # sm_fluid.cpp:65-67
+        self.params.max_dt = float(dt)
+        if self.mesh is not None:
+            check(self.mesh.ctx, self._lib.zg_smf_set_max_dt(self.mesh.ctx, float(dt)))
+
+    def CFL(self) -> float:
+        return self.params.CFL
+
+    def update(self, mesh: EuMesh, steps: int = 1):  # sm_fluid.cpp:81-102
+        if mesh is not self.mesh:
+            self.add_types(mesh)
+        if steps == 1:
+            check(mesh.ctx, self._lib.zg_smf_update(mesh.ctx))
+        else:
+            check(mesh.ctx, self._lib.zg_smf_update_n(mesh.ctx, int(steps)))
+
+    def dt(self) -> float:  # sm_fluid.h:68
+        if self.mesh is None:
+            return float("nan")
+        d = C.c_double()
+        check(self.mesh.ctx, self._lib.zg_smf_dt(self.mesh.ctx, C.byref(d)))
+        return d.value
+
+    def set_flags(self, mesh: EuMesh):  # sm_fluid.cpp:517-559 (flag values)
+        if mesh is not self.mesh:
+            self.add_types(mesh)
+        f = np.empty(mesh.n_cells(), np.int32)
+        check(mesh.ctx, self._lib.zg_smf_set_flags(mesh.ctx, f.ctypes.data_as(C.POINTER(C.c_int))))
+        return f
