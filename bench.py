@@ -52,16 +52,17 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["fourier2048", "riemann256"], default="fourier2048")
+    ap.add_argument("--size", type=int, default=0, help="override the mesh size (n x n) for small profiling runs")
     ap.add_argument("--scheme", choices=["pc", "heun"], default="pc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
-def workload(name):
+def workload(name, size=0):
     from zephyr_b200.workloads import fourier_smooth, riemann2d_case3
     if name == "fourier2048":
-        return fourier_smooth(2048), dict(acc=2, lim="van Albada", CFL=0.4, lim_id=5, bounds=(3, 3, 3, 3))
-    return riemann2d_case3(256), dict(acc=1, lim="MC", CFL=0.4, lim_id=3, bounds=(2, 2, 2, 2))
+        return fourier_smooth(size or 2048), dict(acc=2, lim="van Albada", CFL=0.4, lim_id=5, bounds=(3, 3, 3, 3))
+    return riemann2d_case3(size or 256), dict(acc=1, lim="MC", CFL=0.4, lim_id=3, bounds=(2, 2, 2, 2))
 
 
 def config_of(args, w, cfg, n_gpus):
@@ -81,57 +82,59 @@ def config_of(args, w, cfg, n_gpus):
 
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML in a
+    background thread while the timed region runs (read-only queries)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.stop_flag = threading.Event()
+        self.thread = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = None
+            try:  # the CUDA device's own GPU, whatever CUDA_VISIBLE_DEVICES maps it to
+                import torch
+                uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+                self.h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_sm = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+            return
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((sm, rs))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def stop(self):
-        if self.proc is None:
+        if self.thread is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        self.stop_flag.set()
+        self.thread.join(timeout=2)
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [s for s, _ in self.samples]
+        reasons = sorted({name for _, r in self.samples for name, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_sm, "reasons": reasons,
+                "samples": len(sm), "source": "NVML during the timed region"}
 
 
 # ---------------------------------------------------------------------------
@@ -155,64 +158,76 @@ def traffic_per_cell(kernel):
     return None
 
 
-def cpu_baseline(w, cfg, scheme, budget_s=12.0):
-    """The oracle (CPU restatement of the reference step) on this host's cores."""
-    from oracle import oracle as O
-    threads = os.cpu_count() or 1
+def cpu_solver(w, cfg, scheme, threads):
+    """The reference's own SmFluid compiled from its sources (oracle/_ref,
+    kind "reference") when that build exists and the scheme is the
+    reference's; otherwise the oracle restatement (kind "port")."""
     gen = w.gen
+    if scheme == "pc":
+        from oracle import ref as R
+        if R.available():
+            r = R.RefSolver(gen.nx(), gen.ny(), box=(gen.x_min, gen.x_max, gen.y_min, gen.y_max),
+                            bounds=cfg["bounds"], accuracy=cfg["acc"], limiter=cfg["lim"], CFL=cfg["CFL"])
+            r.set_threads(threads)
+            r.set_state(*w.state)
+            return r, "reference", "zephyr's SmFluid::update compiled from its sources (oracle/_ref)"
+    from oracle import oracle as O
     om = O.Mesh(gen.nx(), gen.ny(), gen.x_min, gen.x_max, gen.y_min, gen.y_max, cfg["bounds"])
     osv = O.Solver(om, gamma=1.4, flux=O.FLUX_HLLC, limiter=cfg["lim_id"], accuracy=cfg["acc"],
                    scheme=0 if scheme == "pc" else 1, CFL=cfg["CFL"], threads=threads)
     osv.set_state(*w.state)
+    osv._keep = om
+    return osv, "port", "oracle restatement of the reference step"
+
+
+def cpu_baseline(w, cfg, scheme, budget_s=12.0):
+    """The reference's CPU path on this host's cores, on a bounded sample."""
+    threads = os.cpu_count() or 1
+    solver, kind, what = cpu_solver(w, cfg, scheme, threads)
     t0 = time.perf_counter()
-    osv.step()
+    solver.step()
     t1 = time.perf_counter()
     steps = 1
     per = t1 - t0
     extra = max(0, min(20, int(budget_s / max(per, 1e-3)) - 1))
     if extra:
         t0 = time.perf_counter()
-        osv.steps(extra)
+        solver.steps(extra)
         t1 = time.perf_counter()
         steps = extra
         per = (t1 - t0) / extra
-    cells = gen.nx() * gen.ny()
-    return {"value": cells / per, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"{steps} step(s) of the full {gen.nx()}x{gen.ny()} workload after 1 untimed step, "
-                      f"oracle restatement, {threads} std::threads"}
+    cells = w.gen.nx() * w.gen.ny()
+    return {"value": cells / per, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": f"{steps} step(s) of the full {w.gen.nx()}x{w.gen.ny()} workload after 1 untimed step; "
+                      f"{what}; {threads} std::threads"}
 
 
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    w, cfg = workload(args.workload)
-    from oracle import oracle as O
+    w, cfg = workload(args.workload, args.size)
     threads = os.cpu_count() or 1
-    gen = w.gen
-    om = O.Mesh(gen.nx(), gen.ny(), gen.x_min, gen.x_max, gen.y_min, gen.y_max, cfg["bounds"])
-    osv = O.Solver(om, gamma=1.4, flux=O.FLUX_HLLC, limiter=cfg["lim_id"], accuracy=cfg["acc"],
-                   scheme=0 if args.scheme == "pc" else 1, CFL=cfg["CFL"], threads=threads)
-    osv.set_state(*w.state)
+    solver, kind, what = cpu_solver(w, cfg, args.scheme, threads)
     for _ in range(args.warmup):
-        osv.step()
+        solver.step()
     t0 = time.perf_counter()
-    osv.steps(args.steps)
+    solver.steps(args.steps)
     t1 = time.perf_counter()
-    cells = gen.nx() * gen.ny()
+    cells = w.gen.nx() * w.gen.ny()
     sec = t1 - t0
     value = cells * args.steps / sec
+    sample = f"{args.steps} full steps of the {w.gen.nx()}x{w.gen.ny()} workload; {what}; {threads} std::threads"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_of(args, w, cfg, 1),
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full steps of the {gen.nx()}x{gen.ny()} workload on the "
-                                   f"oracle restatement (std::threads={threads})"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference cannot be built here (Eigen3/Boost absent); its algorithm is timed through the "
-                "oracle restatement on the host cores",
+        "note": "the reference is a CMake C++ project with no Python packaging (pip cannot install it); its "
+                "own step code is compiled from its sources against stand-ins for Eigen/Boost and run on the "
+                "host cores",
     }
     print(json.dumps(line), flush=True)
 
@@ -224,10 +239,13 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    stream = torch.cuda.current_stream(dev)
+    # A dedicated (non-default) stream: the library queues its kernels on it
+    # and the timing events are recorded on it.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     lib = Z.load()
 
-    w, cfg = workload(args.workload)
+    w, cfg = workload(args.workload, args.size)
     cells = w.gen.nx() * w.gen.ny()
     mesh = Z.EuMesh(w.gen, device=local_rank, stream=stream.cuda_stream)
     solver = Z.SmFluid(w.eos)
@@ -250,7 +268,6 @@ def run_ours(args, rank, world, local_rank):
     # ---- device-resident timed region -----------------------------------
     sampler = ClockSampler(local_rank)
     sampler.start()
-    time.sleep(0.3)
     lib.zg_set_timing(mesh.ctx, 1)
     n0 = mesh.launch_count()
     barrier()

@@ -1,0 +1,98 @@
+"""Pin the oracle to the reference: the oracle (CPU restatement) against the
+golden fixtures that tests/golden/make_golden.py produced from the
+reference's own SmFluid, fluxes and limiters compiled from its sources.
+Bit-exact equality is required."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+LIM_ID = {"none": 0, "unit": 1, "minmod": 2, "MC": 3, "van Leer": 4, "van Albada 1": 5, "van Albada": 5,
+          "van Albada 2": 6, "CHARM": 7, "HCUS": 8, "HQUICK": 9, "Koren": 10, "smart": 11, "superbee": 12}
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem not in ("pointwise", "isolation_20_mc"))
+
+
+def load(name):
+    return np.load(GOLDEN / f"{name}.npz", allow_pickle=False)
+
+
+def oracle_for(g):
+    nx, ny = int(g["nx"]), int(g["ny"])
+    box = tuple(float(x) for x in g["box"])
+    ek, gamma, P0 = g["eos"]
+    m = O.Mesh(nx, ny, *box, bounds=tuple(int(b) for b in g["bounds"]))
+    s = O.Solver(m, eos_kind=int(ek), gamma=float(gamma), P0=float(P0), flux=int(g["flux"]),
+                 limiter=LIM_ID[str(g["limiter"])], accuracy=int(g["accuracy"]), CFL=float(g["CFL"]))
+    return m, s
+
+
+def test_fixtures_present():
+    assert len(CASES) >= 7
+    assert (GOLDEN / "pointwise.npz").exists()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference_step(name):
+    g = load(name)
+    m, s = oracle_for(g)
+    s.set_state(*g["init"])
+    dts = np.array([s.step() for _ in range(int(g["steps"]))])
+    assert np.array_equal(dts, g["dts"]), "dt sequence differs from the reference"
+    final = np.array(s.state())
+    assert np.array_equal(final, g["final"]), f"{np.count_nonzero(final != g['final'])} values differ"
+    assert np.array_equal(s.wait(), g["wait"])
+    assert np.array_equal(s.set_flags(), g["flags"]), "refinement flags differ"
+
+
+def test_oracle_matches_reference_isolation():
+    g = load("isolation_20_mc")
+    m = O.Mesh(20, 20, bounds=(2, 2, 2, 2))
+    s = O.Solver(m, limiter=3, accuracy=2, CFL=0.4)
+    s.set_state(*g["init"])
+    s.set_wait(g["wait0"])
+    assert s.step() == g["dts"][0]
+    assert np.array_equal(np.array(s.state()), g["final"])
+    assert np.array_equal(s.wait(), g["wait"])
+
+
+def test_oracle_fluxes_match_reference():
+    g = load("pointwise")
+    for kind, tag in ((O.FLUX_HLLC, "hllc"), (O.FLUX_HLL, "hll")):
+        got = np.array([O.flux(kind, a, b) for a, b in zip(g["zL"], g["zR"])])
+        assert np.array_equal(got, g[tag]), tag
+
+
+def test_oracle_limiters_match_reference():
+    g = load("pointwise")
+    vals = g["limiter_values"]
+    for name, table in zip(g["limiter_names"], g["limiter_table"]):
+        got = np.array([[O.limiter(LIM_ID[str(name)], a, b) for b in vals] for a in vals])
+        assert np.array_equal(got, table, equal_nan=True), str(name)
+
+
+def test_oracle_matches_reference_build_directly():
+    """When the reference-source build is present, compare on fresh inputs."""
+    from oracle import ref as R
+    if not R.available():
+        pytest.skip("oracle/_ref/libzref.so not built (no reference tree on this machine)")
+    rng = np.random.default_rng(99)
+    for bounds, acc, lim in (((3, 3, 2, 2), 2, "van Albada"), ((1, 2, 1, 2), 2, "MC"), ((2, 2, 3, 3), 1, "MC")):
+        n = 18
+        N = n * n
+        rho = 1.0 + rng.random(N)
+        u = 0.5 * rng.standard_normal(N)
+        v = 0.5 * rng.standard_normal(N)
+        p = 0.5 + rng.random(N)
+        st = (rho, u, v, p, p / (0.4 * rho))
+        r = R.RefSolver(n, n, bounds=bounds, accuracy=acc, limiter=lim, CFL=0.45)
+        s = O.Solver(O.Mesh(n, n, bounds=bounds), limiter=LIM_ID[lim], accuracy=acc, CFL=0.45)
+        r.set_state(*st)
+        s.set_state(*st)
+        for _ in range(12):
+            assert r.step() == s.step()
+        assert np.array_equal(np.array(r.state()), np.array(s.state()))
+        gr, go = r.grad(), s.grad()
+        assert np.array_equal(gr[0], go[0]) and np.array_equal(gr[1], go[1])
