@@ -42,6 +42,8 @@ FALLBACK_HBM_GBS = 6650.0
 # state = 4 doubles).  Kernels that the model folds into others carry 0.
 B_ALG_KERNEL = {"dt": 0, "flux1": 64, "grad": 0, "stage1": 64, "stage2": 96, "heun_a": 64, "heun_b": 96,
                 "flags": 0}
+# (the FAST predictor pass "stage1" is fused with the gradients; the
+# corrector "stage2" carries the next step's CFL minimum)
 B_ALG_STEP = {1: 64, 2: 160}
 
 
@@ -232,23 +234,9 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local_rank):
-    import torch
-    import zephyr_b200 as Z
-    from zephyr_b200._lib import KERNEL_KINDS
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    # A dedicated (non-default) stream: the library queues its kernels on it
-    # and the timing events are recorded on it.
-    stream = torch.cuda.Stream(dev)
-    torch.cuda.set_stream(stream)
-    lib = Z.load()
-
-    w, cfg = workload(args.workload, args.size)
-    cells = w.gen.nx() * w.gen.ny()
+def _solver(Z, w, cfg, args, local_rank, stream, precision, kernels):
     mesh = Z.EuMesh(w.gen, device=local_rank, stream=stream.cuda_stream)
-    solver = Z.SmFluid(w.eos)
+    solver = Z.SmFluid(w.eos, precision=precision, kernels=kernels)
     solver.set_accuracy(cfg["acc"])
     solver.set_CFL(cfg["CFL"])
     solver.set_limiter(cfg["lim"])
@@ -256,25 +244,23 @@ def run_ours(args, rank, world, local_rank):
     solver.set_scheme(Z.Scheme.HEUN if args.scheme == "heun" else Z.Scheme.PREDICTOR_CORRECTOR)
     solver.add_types(mesh)
     mesh.set_state(*w.state)
+    return mesh, solver
 
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
 
-    # warm-up
-    solver.update(mesh, steps=max(args.warmup, 3))
-    mesh.synchronize()
-
-    # ---- device-resident timed region -----------------------------------
-    sampler = ClockSampler(local_rank)
-    sampler.start()
+def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=False):
+    """K steps between a barrier + synchronise and CUDA events on the
+    library's stream; returns (ms, per-kernel dict, launches, clocks)."""
+    from zephyr_b200._lib import KERNEL_KINDS
+    sampler = ClockSampler(torch.cuda.current_device()) if clocks else None
+    if sampler:
+        sampler.start()
     lib.zg_set_timing(mesh.ctx, 1)
     n0 = mesh.launch_count()
     barrier()
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    solver.update(mesh, steps=args.steps)
+    solver.update(mesh, steps=steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -284,10 +270,50 @@ def run_ours(args, rank, world, local_rank):
     kcount = (C.c_longlong * 8)()
     lib.zg_kernel_times(mesh.ctx, kms, kcount)
     lib.zg_set_timing(mesh.ctx, 0)
-    clocks = sampler.stop()
+    kernels = {}
+    tot = max(sum(kms), 1e-12)
+    for k, name in enumerate(KERNEL_KINDS):
+        if kcount[k]:
+            kernels[name] = {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k],
+                             "share": kms[k] / tot}
+    return ms, kernels, launches, (sampler.stop() if sampler else None)
+
+
+def _max_over_ranks(torch, vals, dev, world):
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import zephyr_b200 as Z
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    # A dedicated (non-default) stream: the library queues its kernels on it
+    # and the timing events are recorded on it.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    lib = Z.load()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    w, cfg = workload(args.workload, args.size)
+    cells = w.gen.nx() * w.gen.ny()
+    K, W = args.steps, max(args.warmup, 3)
+
+    # ---- headline: the FP64 step (FAST kernels), inputs resident in HBM ----
+    mesh, solver = _solver(Z, w, cfg, args, local_rank, stream, Z.Precision.FP64, Z.Kernels.FAST)
+    solver.update(mesh, steps=W)
+    mesh.synchronize()
+    ms, kernels, launches, clocks = _timed_steps(torch, lib, mesh, solver, K, dev, stream, barrier, clocks=True)
     dt_last = solver.dt()
 
-    # ---- end-to-end through the public API with host buffers ---------------
+    # ---- end to end through the public API with host buffers ---------------
     pin = [torch.empty(cells, dtype=torch.float64, pin_memory=True) for _ in range(5)]
     for t, a in zip(pin, mesh.get_state()):
         t.numpy()[:] = a
@@ -295,7 +321,7 @@ def run_ours(args, rank, world, local_rank):
     P = C.POINTER(C.c_double)
     inp_ptrs = [C.cast(C.c_void_p(t.data_ptr()), P) for t in pin]
     out_ptrs = [C.cast(C.c_void_p(t.data_ptr()), P) for t in outp]
-    e2e_steps = max(3, min(args.steps, 10))
+    e2e_steps = max(3, min(K, 10))
     barrier()
     torch.cuda.synchronize(dev)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -308,23 +334,37 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     barrier()
     e2e_ms = f0.elapsed_time(f1)
+    mesh.close()
 
-    # ---- max over ranks -------------------------------------------------------
-    vals = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(vals, op=torch.distributed.ReduceOp.MAX)
-    ms, e2e_ms = float(vals[0]), float(vals[1])
+    # ---- the other forms on the same workload ------------------------------
+    variants = {}
+    for name, prec, kern in (("fp64_parity", Z.Precision.FP64, Z.Kernels.PARITY),
+                             ("mixed", Z.Precision.MIXED, Z.Kernels.FAST)):
+        m2, s2 = _solver(Z, w, cfg, args, local_rank, stream, prec, kern)
+        s2.update(m2, steps=W)
+        m2.synchronize()
+        v_ms, v_kernels, v_launch, _ = _timed_steps(torch, lib, m2, s2, K, dev, stream, barrier)
+        variants[name] = {"ms": v_ms, "kernels": v_kernels, "launches": v_launch, "mesh": m2, "solver": s2}
 
+    # accuracy of the mixed form: density after W + K steps against the FP64
+    # step run for the same steps from the same initial state
+    m_ref, s_ref = _solver(Z, w, cfg, args, local_rank, stream, Z.Precision.FP64, Z.Kernels.FAST)
+    s_ref.update(m_ref, steps=W + K)
+    rho64 = m_ref.get_state()[0]
+    rho_mx = variants["mixed"]["mesh"].get_state()[0]
+    l1 = float(np.sum(np.abs(rho_mx - rho64)) / np.sum(np.abs(rho64)))
+    linf = float(np.max(np.abs(rho_mx - rho64)) / np.max(np.abs(rho64)))
+    m_ref.close()
+
+    vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix = vals
+    for v in variants.values():
+        v["mesh"].close()
     if rank != 0:
         return
-    value = world * cells * args.steps / (ms / 1e3)
-    e2e_value = world * cells * e2e_steps / (e2e_ms / 1e3)
 
-    kernels = {}
-    for k, name in enumerate(KERNEL_KINDS):
-        if kcount[k]:
-            kernels[name] = {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k],
-                             "share": kms[k] / max(sum(kms), 1e-12)}
+    value = world * cells * K / (ms / 1e3)
+    e2e_value = world * cells * e2e_steps / (e2e_ms / 1e3)
     top = max(kernels, key=lambda n: kernels[n]["ms_total"])
     peak, peak_kind = hbm_peak()
     balg = B_ALG_KERNEL[top] * cells
@@ -334,24 +374,36 @@ def run_ours(args, rank, world, local_rank):
             "frac": achieved / peak, "peak_source": peak_kind,
             "traffic": (tpc * cells) if tpc is not None else None,
             "algorithmic_bytes_per_launch": balg,
-            "step_achieved": B_ALG_STEP[cfg["acc"]] * cells * args.steps / (ms / 1e3) / 1e9}
+            "step_achieved": B_ALG_STEP[cfg["acc"]] * cells * K / (ms / 1e3) / 1e9}
     roof["step_frac"] = roof["step_achieved"] / peak
-
+    mixed_balg = {1: 64, 2: 144}[cfg["acc"]]
     line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(args, w, cfg, world),
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
         "roofline": roof, "kernels": kernels, "gpu_launches": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
                 "note": "per step: upload of the whole state from pinned host memory, zg_smf_update, "
                         "download of the whole state"},
+        "variants": {
+            "fp64_parity": {"value": world * cells * K / (ms_par / 1e3), "ms_per_step": ms_par / K,
+                            "note": "bit-exact with the reference (gather form, no FMA)",
+                            "kernels": variants["fp64_parity"]["kernels"]},
+            "mixed": {"value": world * cells * K / (ms_mix / 1e3), "ms_per_step": ms_mix / K,
+                      "speedup_vs_fp64": ms / ms_mix,
+                      "l1_rel_density_err_vs_fp64": l1, "linf_rel_density_err_vs_fp64": linf,
+                      "err_after_steps": W + K,
+                      "step_achieved_GBs": mixed_balg * cells * K / (ms_mix / 1e3) / 1e9,
+                      "step_frac": mixed_balg * cells * K / (ms_mix / 1e3) / 1e9 / peak,
+                      "kernels": variants["mixed"]["kernels"]},
+        },
         "dt_last": dt_last,
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, cfg, args.scheme)
     print(json.dumps(line), flush=True)
-    mesh.close()
 
 
 def main():

@@ -28,6 +28,10 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "zg_api.cu": [],
     "smf_parity.cu": ["-fmad=false"],
+    "smf_fast.cu": [],
+    # FP32 face arithmetic: approximate single-precision division and square
+    # root; FP64 operations are unaffected by these flags.
+    "smf_mixed.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
 }
 
 

@@ -1,0 +1,51 @@
+// smf_fast.cu -- the tiled FP64 kernels (FAST); multiply-adds may be fused.
+#include "smf_tiled.cuh"
+#include "smf_tiled_launch.h"
+
+namespace zg {
+namespace fast {
+
+using tiled::Fields;
+constexpr int BLOCK = 128, TX = 32, TY = 8;  // faces: 32 x 8 threads, 31 x 7 interior cells
+constexpr int GX = 32, GY = 4;               // gradients + predictor: 32 x 4 cells
+
+static inline unsigned blocks(int n) { return (unsigned)((n + BLOCK - 1) / BLOCK); }
+
+void launch_cfl(const SmfArgs &a, const Fields<double> &f, void *stream) {
+    tiled::k_cfl<double, BLOCK><<<blocks(a.mesh.n), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+}
+
+template <int LIM>
+static void grad_predict(const SmfArgs &a, const Fields<double> &f, bool predict, cudaStream_t s) {
+    dim3 block(GX, GY);
+    dim3 grid((a.mesh.ny + GX - 1) / GX, (a.mesh.nx + GY - 1) / GY);
+    if (predict)
+        tiled::k_grad_predict<double, false, true, LIM, GX, GY><<<grid, block, 0, s>>>(a, f);
+    else
+        tiled::k_grad_predict<double, false, false, LIM, GX, GY><<<grid, block, 0, s>>>(a, f);
+}
+
+void launch_grad_predict(const SmfArgs &a, const Fields<double> &f, bool predict, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (a.limiter) {  // the common limiters are compiled in; others are selected at run time
+        case LIM_VANALBADA1: grad_predict<LIM_VANALBADA1>(a, f, predict, s); break;
+        case LIM_MC: grad_predict<LIM_MC>(a, f, predict, s); break;
+        case LIM_MINMOD: grad_predict<LIM_MINMOD>(a, f, predict, s); break;
+        default: grad_predict<-1>(a, f, predict, s); break;
+    }
+}
+
+void launch_faces(const SmfArgs &a, const Fields<double> &f, int mode, void *stream) {
+    dim3 block(TX, TY);
+    dim3 grid((a.mesh.ny + TX - 2) / (TX - 1), (a.mesh.nx + TY - 2) / (TY - 1));
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (mode) {
+        case 0: tiled::k_faces<double, false, 0, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        case 1: tiled::k_faces<double, false, 1, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        case 2: tiled::k_faces<double, false, 2, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        default: tiled::k_faces<double, false, 3, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+    }
+}
+
+}  // namespace fast
+}  // namespace zg

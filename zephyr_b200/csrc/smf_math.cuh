@@ -36,6 +36,10 @@ __host__ __device__ inline bool is_boundary(int flag) {
 // loses, ties return the first argument).
 __host__ __device__ inline double smin(double a, double b) { return (b < a) ? b : a; }
 __host__ __device__ inline double smax(double a, double b) { return (a < b) ? b : a; }
+template <typename T>
+__host__ __device__ inline T smin_t(T a, T b) { return (b < a) ? b : a; }
+template <typename T>
+__host__ __device__ inline T smax_t(T a, T b) { return (a < b) ? b : a; }
 
 // Correctly rounded x^3 (stands in for glibc pow(x, 3) in gradient.h:256):
 // Dekker/Knuth error-free products give x^3 = q + qe + pe*x exactly, and the

@@ -1,0 +1,61 @@
+// smf_mixed.cu -- the tiled MIXED kernels: FP32 reconstruction and Riemann
+// fluxes (approximate single-precision division and square root allowed),
+// FP64 conserved state, accumulation, update and dt.
+#include "smf_tiled.cuh"
+#include "smf_tiled_launch.h"
+
+namespace zg {
+namespace mixed {
+
+using tiled::Fields;
+constexpr int BLOCK = 128, TX = 32, TY = 8;  // faces: 32 x 8 threads, 31 x 7 interior cells
+constexpr int GX = 32, GY = 4;               // gradients + predictor: 32 x 4 cells
+
+static inline unsigned blocks(int n) { return (unsigned)((n + BLOCK - 1) / BLOCK); }
+
+void launch_cfl(const SmfArgs &a, const Fields<float> &f, void *stream) {
+    tiled::k_cfl<float, BLOCK><<<blocks(a.mesh.n), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+}
+
+template <int LIM>
+static void grad_predict(const SmfArgs &a, const Fields<float> &f, bool predict, cudaStream_t s) {
+    dim3 block(GX, GY);
+    dim3 grid((a.mesh.ny + GX - 1) / GX, (a.mesh.nx + GY - 1) / GY);
+    if (predict)
+        tiled::k_grad_predict<float, true, true, LIM, GX, GY><<<grid, block, 0, s>>>(a, f);
+    else
+        tiled::k_grad_predict<float, true, false, LIM, GX, GY><<<grid, block, 0, s>>>(a, f);
+}
+
+void launch_grad_predict(const SmfArgs &a, const Fields<float> &f, bool predict, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (a.limiter) {  // the common limiters are compiled in; others are selected at run time
+        case LIM_VANALBADA1: grad_predict<LIM_VANALBADA1>(a, f, predict, s); break;
+        case LIM_MC: grad_predict<LIM_MC>(a, f, predict, s); break;
+        case LIM_MINMOD: grad_predict<LIM_MINMOD>(a, f, predict, s); break;
+        default: grad_predict<-1>(a, f, predict, s); break;
+    }
+}
+
+void launch_faces(const SmfArgs &a, const Fields<float> &f, int mode, void *stream) {
+    dim3 block(TX, TY);
+    dim3 grid((a.mesh.ny + TX - 2) / (TX - 1), (a.mesh.nx + TY - 2) / (TY - 1));
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (mode) {
+        case 0: tiled::k_faces<float, true, 0, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        case 1: tiled::k_faces<float, true, 1, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        case 2: tiled::k_faces<float, true, 2, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        default: tiled::k_faces<float, true, 3, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+    }
+}
+
+void launch_to_mixed(int n, PrimPtr z, const Fields<float> &f, void *stream) {
+    tiled::k_to_mixed<BLOCK><<<blocks(n), BLOCK, 0, (cudaStream_t)stream>>>(n, z, f);
+}
+
+void launch_to_prim(int n, const Fields<float> &f, EosD eos, PrimPtr z, void *stream) {
+    tiled::k_to_prim<BLOCK><<<blocks(n), BLOCK, 0, (cudaStream_t)stream>>>(n, f, eos, z);
+}
+
+}  // namespace mixed
+}  // namespace zg

@@ -1,0 +1,26 @@
+// smf_tiled_launch.h -- launchers of the tiled kernels (FAST: FP64,
+// MIXED: FP32 face arithmetic with FP64 conserved state).
+#pragma once
+
+#include "smf_types.h"
+
+namespace zg {
+namespace tiled {
+template <typename R>
+struct Fields;
+}
+
+namespace fast {
+void launch_cfl(const SmfArgs &a, const tiled::Fields<double> &f, void *stream);
+void launch_grad_predict(const SmfArgs &a, const tiled::Fields<double> &f, bool predict, void *stream);
+void launch_faces(const SmfArgs &a, const tiled::Fields<double> &f, int mode, void *stream);
+}  // namespace fast
+
+namespace mixed {
+void launch_cfl(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
+void launch_grad_predict(const SmfArgs &a, const tiled::Fields<float> &f, bool predict, void *stream);
+void launch_faces(const SmfArgs &a, const tiled::Fields<float> &f, int mode, void *stream);
+void launch_to_mixed(int n, PrimPtr z, const tiled::Fields<float> &f, void *stream);
+void launch_to_prim(int n, const tiled::Fields<float> &f, EosD eos, PrimPtr z, void *stream);
+}  // namespace mixed
+}  // namespace zg

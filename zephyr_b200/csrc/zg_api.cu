@@ -12,6 +12,8 @@
 #include <vector>
 
 #include "../../include/zephyr_gpu.h"
+#include "smf_tiled.cuh"
+#include "smf_tiled_launch.h"
 #include "smf_types.h"
 
 using namespace zg;
@@ -28,6 +30,9 @@ struct zg_ctx {
     int nx = 0, ny = 0, n = 0;
     StructMesh mesh{};
     double *d_geo = nullptr;  // all geometry tables
+    double *d_tgeo = nullptr;  // per-axis tables of the tiled kernels, FP64 then FP32
+    tiled::AxisGeo<double> ax64{}, ay64{};
+    tiled::AxisGeo<float> ax32{}, ay32{};
 
     // solver
     bool configured = false;
@@ -43,6 +48,17 @@ struct zg_ctx {
     double *gx[4] = {}, *gy[4] = {};
     int wait_cur = 0;  // index of the buffer holding the current counters
     bool stepped = false;
+
+    // tiled kernels (FAST / MIXED)
+    unsigned long long *d_slots = nullptr;  // three rotating CFL accumulators
+    int slot_k = 0;
+    bool cfl_valid = false;
+    int state_mode = ZG_FP64;  // representation of the current state
+    double *d_mq = nullptr;    // MIXED conserved state, two sets of 4 fields
+    float *d_mf = nullptr;     // MIXED FP32 fields: two state mirrors (5), stage (5), gradients (8)
+    double *mq[2][4] = {};
+    float *mw[2][5] = {}, *mh[5] = {}, *mg[8] = {};
+    int mcur = 0;
 
     // per-kernel timing
     bool timing = false;
@@ -83,6 +99,10 @@ struct DeviceGuard {
 };
 
 void free_solver(zg_ctx *c) {
+    cudaFree(c->d_mq);
+    cudaFree(c->d_mf);
+    c->d_mq = nullptr;
+    c->d_mf = nullptr;
     cudaFree(c->d_state);
     cudaFree(c->d_wait);
     cudaFree(c->d_dmin);
@@ -99,7 +119,9 @@ void free_solver(zg_ctx *c) {
 
 void free_mesh(zg_ctx *c) {
     cudaFree(c->d_geo);
+    cudaFree(c->d_tgeo);
     c->d_geo = nullptr;
+    c->d_tgeo = nullptr;
     c->have_mesh = false;
 }
 
@@ -124,6 +146,129 @@ SmfArgs make_args(const zg_ctx *c) {
     a.dt_ticket = c->d_ticket;
     a.dt_out = c->d_dt;
     return a;
+}
+
+const unsigned long long *slot_ptr(const zg_ctx *c, int k) { return c->d_slots + ((c->slot_k + k) % 3); }
+
+tiled::Fields<double> fast_fields(const zg_ctx *c) {
+    tiled::Fields<double> f{};
+    f.gxa = c->ax64;
+    f.gya = c->ay64;
+    const double *w[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
+    double *h[5] = {c->zhalf.r, c->zhalf.u, c->zhalf.v, c->zhalf.p, c->zhalf.e};
+    double *wn[5] = {c->znext.r, c->znext.u, c->znext.v, c->znext.p, c->znext.e};
+    for (int k = 0; k < 5; ++k) {
+        f.w[k] = w[k];
+        f.h[k] = h[k];
+        f.wn[k] = wn[k];
+    }
+    for (int k = 0; k < 4; ++k) {
+        f.gx[k] = c->gx[k];
+        f.gy[k] = c->gy[k];
+    }
+    f.wait_in = c->d_wait + (size_t)c->wait_cur * c->n;
+    f.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->n;
+    f.slot_cur = const_cast<unsigned long long *>(slot_ptr(c, 0));
+    f.slot_nxt = const_cast<unsigned long long *>(slot_ptr(c, 1));
+    f.slot_clr = const_cast<unsigned long long *>(slot_ptr(c, 2));
+    f.dt_out = c->d_dt;
+    return f;
+}
+
+tiled::Fields<float> mixed_fields(const zg_ctx *c) {
+    tiled::Fields<float> f{};
+    f.gxa = c->ax32;
+    f.gya = c->ay32;
+    int a = c->mcur, b = 1 - c->mcur;
+    for (int k = 0; k < 4; ++k) {
+        f.q[k] = c->mq[a][k];
+        f.qn[k] = c->mq[b][k];
+        f.gx[k] = c->mg[k];
+        f.gy[k] = c->mg[4 + k];
+    }
+    for (int k = 0; k < 5; ++k) {
+        f.w[k] = c->mw[a][k];
+        f.wn[k] = c->mw[b][k];
+        f.h[k] = c->mh[k];
+    }
+    f.wait_in = c->d_wait + (size_t)c->wait_cur * c->n;
+    f.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->n;
+    f.slot_cur = const_cast<unsigned long long *>(slot_ptr(c, 0));
+    f.slot_nxt = const_cast<unsigned long long *>(slot_ptr(c, 1));
+    f.slot_clr = const_cast<unsigned long long *>(slot_ptr(c, 2));
+    f.dt_out = c->d_dt;
+    return f;
+}
+
+// Move the current state into the representation `mode` (FP64 primitive or
+// MIXED) on the device.
+int convert_state(zg_ctx *c, int mode) {
+    if (mode == c->state_mode) return ZG_OK;
+    if (mode == ZG_MIXED) {
+        tiled::Fields<float> f = mixed_fields(c);
+        for (int k = 0; k < 4; ++k) f.qn[k] = c->mq[c->mcur][k];
+        for (int k = 0; k < 5; ++k) f.wn[k] = c->mw[c->mcur][k];
+        mixed::launch_to_mixed(c->n, c->z, f, (void *)c->stream);
+    } else {
+        mixed::launch_to_prim(c->n, mixed_fields(c), c->eos, c->z, (void *)c->stream);
+    }
+    c->launches += 1;
+    c->state_mode = mode;
+    c->cfl_valid = false;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "state conversion");
+}
+
+// Write the FP64 primitive form of the current state into c->z without
+// changing the representation the steps use (MIXED keeps its FP64 conserved
+// variables, so no conversion round trip enters the solution).
+int materialize_prim(zg_ctx *c) {
+    if (c->state_mode != ZG_MIXED) return ZG_OK;
+    mixed::launch_to_prim(c->n, mixed_fields(c), c->eos, c->z, (void *)c->stream);
+    c->launches += 1;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "state conversion");
+}
+
+// Per-axis least-squares geometry of a uniform axis (gradient.h:251-275 for
+// axis-aligned faces): V = vertices, C = cell centres, M = mid-edges of the
+// other axis' faces, h = face area of this axis' faces, bc_lo / bc_hi the
+// boundary flags of the two ends.  Eight tables of n values: wl, wh, rl, rh,
+// binv, ol, oh, om.
+std::vector<double> axis_tables(const std::vector<double> &V, const std::vector<double> &C,
+                                const std::vector<double> &M, double h, int bc_lo, int bc_hi) {
+    const int n = (int)C.size();
+    std::vector<double> t(8 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        double r[2], w[2];
+        for (int side = 0; side < 2; ++side) {
+            const bool inner = side == 0 ? i > 0 : i < n - 1;
+            const double fc = side == 0 ? V[i] : V[i + 1];
+            const double nrm = side == 0 ? -1.0 : 1.0;
+            double dr;
+            if (inner) {
+                dr = (side == 0 ? C[i - 1] : C[i + 1]) - C[i];
+            } else {  // mirror of the centre in the face (amr_faces.h:197-199)
+                double d = (fc - C[i]) * nrm;
+                dr = (C[i] + (2.0 * d) * nrm) - C[i];
+            }
+            (void)bc_lo;
+            (void)bc_hi;
+            const double drn = (dr * nrm) * nrm;
+            const double ad = std::fabs(drn);
+            w[side] = h / (ad * ad * ad);
+            r[side] = dr;
+            t[(size_t)(0 + side) * n + i] = w[side] * drn;
+            t[(size_t)(2 + side) * n + i] = dr;
+        }
+        double A = t[(size_t)0 * n + i] * r[0] + t[(size_t)1 * n + i] * r[1];
+        if (std::fabs(A) < 1e-8) A = 1.0;  // gradient.h:268-273
+        t[(size_t)4 * n + i] = 1.0 / A;
+        t[(size_t)5 * n + i] = V[i] - C[i];
+        t[(size_t)6 * n + i] = V[i + 1] - C[i];
+        t[(size_t)7 * n + i] = M[i] - C[i];
+    }
+    return t;
 }
 
 std::string lower_strip(const char *name) {
@@ -165,7 +310,7 @@ void timed(zg_ctx *c, int kind, F &&launch) {
 }
 
 // One step of SmFluid::update (sm_fluid.cpp:81-102) as kernel launches.
-int enqueue_step(zg_ctx *c) {
+int enqueue_parity_step(zg_ctx *c) {
     SmfArgs a = make_args(c);
     void *st = (void *)c->stream;
     timed(c, ZG_K_DT, [&] { parity::launch_dt(a, c->z, st); });
@@ -185,8 +330,75 @@ int enqueue_step(zg_ctx *c) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     std::swap(c->z, c->znext);  // Storage::swap of init and next (sm_fluid.cpp:368-370)
+    c->cfl_valid = false;
     c->stepped = true;
     return ZG_OK;
+}
+
+// The same step with the tiled kernels: pass A (gradients + predictor),
+// pass B (face-once corrector with the next step's CFL minimum).
+template <typename R, bool MIXED>
+int enqueue_tiled_step(zg_ctx *c) {
+    SmfArgs a = make_args(c);
+    void *st = (void *)c->stream;
+    auto fields = [c]() {
+        if constexpr (MIXED) return mixed_fields(c);
+        else return fast_fields(c);
+    };
+    auto L_cfl = [&](const tiled::Fields<R> &f) {
+        if constexpr (MIXED) mixed::launch_cfl(a, f, st);
+        else fast::launch_cfl(a, f, st);
+    };
+    auto L_grad = [&](const tiled::Fields<R> &f, bool predict) {
+        if constexpr (MIXED) mixed::launch_grad_predict(a, f, predict, st);
+        else fast::launch_grad_predict(a, f, predict, st);
+    };
+    auto L_faces = [&](const tiled::Fields<R> &f, int mode) {
+        if constexpr (MIXED) mixed::launch_faces(a, f, mode, st);
+        else fast::launch_faces(a, f, mode, st);
+    };
+    tiled::Fields<R> f = fields();
+    if (!c->cfl_valid) {
+        // Fresh accumulators for this step's minimum and the next one's
+        // (0x7F bytes: a finite double far above any CFL term).
+        cudaMemsetAsync(f.slot_cur, 0x7F, sizeof(unsigned long long), c->stream);
+        cudaMemsetAsync(f.slot_nxt, 0x7F, sizeof(unsigned long long), c->stream);
+        timed(c, ZG_K_DT, [&] { L_cfl(f); });
+    }
+    if (c->par.accuracy == 1) {
+        timed(c, ZG_K_FLUX1, [&] { L_faces(f, 0); });
+    } else if (c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
+        timed(c, ZG_K_STAGE1, [&] { L_grad(f, true); });
+        timed(c, ZG_K_STAGE2, [&] { L_faces(f, 1); });
+        c->wait_cur = 1 - c->wait_cur;
+    } else {
+        timed(c, ZG_K_GRAD, [&] { L_grad(f, false); });
+        timed(c, ZG_K_HEUN_A, [&] { L_faces(f, 2); });
+        tiled::Fields<R> fs = f;  // gradients of the stage value z*
+        for (int k = 0; k < 5; ++k) fs.w[k] = f.h[k];
+        timed(c, ZG_K_GRAD, [&] { L_grad(fs, false); });
+        timed(c, ZG_K_HEUN_B, [&] { L_faces(f, 3); });
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    if constexpr (MIXED) c->mcur = 1 - c->mcur;
+    else std::swap(c->z, c->znext);
+    c->slot_k = (c->slot_k + 1) % 3;
+    c->cfl_valid = true;
+    c->stepped = true;
+    return ZG_OK;
+}
+
+int enqueue_step(zg_ctx *c) {
+    if (c->par.precision == ZG_MIXED) {
+        int rc = convert_state(c, ZG_MIXED);
+        if (rc != ZG_OK) return rc;
+        return enqueue_tiled_step<float, true>(c);
+    }
+    int rc = convert_state(c, ZG_FP64);
+    if (rc != ZG_OK) return rc;
+    if (c->par.kernels == ZG_KERNELS_FAST) return enqueue_tiled_step<double, false>(c);
+    return enqueue_parity_step(c);
 }
 
 }  // namespace
@@ -323,6 +535,34 @@ int zg_mesh_rectangle(zg_ctx *c, int nx, int ny, double x_min, double x_max, dou
            oix = put(i2x), oiy = put(i2y);
     ZG_CUDA(c, cudaMemcpy(c->d_geo, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice));
 
+    // per-axis tables of the tiled kernels (FP64 and FP32 copies)
+    {
+        std::vector<double> tx = axis_tables(X, cx, fxm, (y_max - y_min) / ny, bc[0], bc[1]);
+        std::vector<double> ty = axis_tables(Y, cy, fym, (x_max - x_min) / nx, bc[2], bc[3]);
+        size_t nd = tx.size() + ty.size();
+        ZG_CUDA(c, cudaMalloc(&c->d_tgeo, nd * (sizeof(double) + sizeof(float))));
+        std::vector<double> all(tx);
+        all.insert(all.end(), ty.begin(), ty.end());
+        std::vector<float> allf(all.begin(), all.end());
+        ZG_CUDA(c, cudaMemcpy(c->d_tgeo, all.data(), nd * sizeof(double), cudaMemcpyHostToDevice));
+        float *f32 = reinterpret_cast<float *>(c->d_tgeo + nd);
+        ZG_CUDA(c, cudaMemcpy(f32, allf.data(), nd * sizeof(float), cudaMemcpyHostToDevice));
+        auto fill = [](auto &g, auto *base, int n) {
+            g.wl = base;
+            g.wh = base + n;
+            g.rl = base + 2 * (size_t)n;
+            g.rh = base + 3 * (size_t)n;
+            g.binv = base + 4 * (size_t)n;
+            g.ol = base + 5 * (size_t)n;
+            g.oh = base + 6 * (size_t)n;
+            g.om = base + 7 * (size_t)n;
+        };
+        fill(c->ax64, c->d_tgeo, nx);
+        fill(c->ay64, c->d_tgeo + tx.size(), ny);
+        fill(c->ax32, f32, nx);
+        fill(c->ay32, f32 + tx.size(), ny);
+    }
+
     StructMesh &m = c->mesh;
     m.nx = nx;
     m.ny = ny;
@@ -365,8 +605,12 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown limiter");
     if (p->scheme != ZG_SCHEME_PREDICTOR_CORRECTOR && p->scheme != ZG_SCHEME_HEUN)
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown scheme");
-    if (p->precision != ZG_FP64) return fail(c, ZG_ERR_ARG, "zg_smf_configure: unsupported precision");
-    if (p->kernels != ZG_KERNELS_PARITY) return fail(c, ZG_ERR_ARG, "zg_smf_configure: unsupported kernels");
+    if (p->precision != ZG_FP64 && p->precision != ZG_MIXED)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown precision");
+    if (p->kernels != ZG_KERNELS_PARITY && p->kernels != ZG_KERNELS_FAST)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown kernel family");
+    if (p->precision == ZG_MIXED && p->kernels != ZG_KERNELS_FAST)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: the mixed form uses the FAST kernels");
     if (!(p->gamma > 1.0)) return fail(c, ZG_ERR_ARG, "zg_smf_configure: gamma must exceed 1");
 
     DeviceGuard g(c->device);
@@ -389,6 +633,24 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     ZG_CUDA(c, cudaMalloc(&c->d_dmin, 64));
     c->d_ticket = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dmin) + 8);
     c->d_dt = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_dmin) + 16);
+    c->d_slots = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(c->d_dmin) + 24);
+    ZG_CUDA(c, cudaMalloc(&c->d_mq, 8 * n * sizeof(double)));
+    ZG_CUDA(c, cudaMalloc(&c->d_mf, 23 * n * sizeof(float)));
+    for (int s2 = 0; s2 < 2; ++s2)
+        for (int k = 0; k < 4; ++k) c->mq[s2][k] = c->d_mq + (size_t)(4 * s2 + k) * n;
+    {
+        float *fb = c->d_mf;
+        for (int s2 = 0; s2 < 2; ++s2)
+            for (int k = 0; k < 5; ++k) c->mw[s2][k] = fb + (size_t)(5 * s2 + k) * n;
+        for (int k = 0; k < 5; ++k) c->mh[k] = fb + (size_t)(10 + k) * n;
+        for (int k = 0; k < 8; ++k) c->mg[k] = fb + (size_t)(15 + k) * n;
+    }
+    ZG_CUDA(c, cudaMemsetAsync(c->d_mq, 0, 8 * n * sizeof(double), c->stream));
+    ZG_CUDA(c, cudaMemsetAsync(c->d_mf, 0, 23 * n * sizeof(float), c->stream));
+    c->state_mode = ZG_FP64;
+    c->mcur = 0;
+    c->slot_k = 0;
+    c->cfl_valid = false;
     double *b = c->d_state;
     auto take = [&b, n]() {
         double *p0 = b;
@@ -433,6 +695,9 @@ int zg_state_upload(zg_ctx *c, const double *rho, const double *vx, const double
     double *dst[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
     for (int k = 0; k < 5; ++k)
         ZG_CUDA(c, cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyHostToDevice, c->stream));
+    // the uploaded state is FP64 primitive; MIXED steps convert it on use
+    c->state_mode = ZG_FP64;
+    c->cfl_valid = false;
     return ZG_OK;
 }
 
@@ -440,6 +705,8 @@ int zg_state_download(zg_ctx *c, double *rho, double *vx, double *vy, double *p,
     if (!c || !rho || !vx || !vy || !p || !e) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_state_download: solver not configured");
     DeviceGuard g(c->device);
+    int rc = materialize_prim(c);
+    if (rc != ZG_OK) return rc;
     size_t bytes = (size_t)c->n * sizeof(double);
     double *dst[5] = {rho, vx, vy, p, e};
     const double *src[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
@@ -499,6 +766,8 @@ int zg_smf_set_flags(zg_ctx *c, int *flags) {
     if (!c || !flags) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_set_flags: solver not configured");
     DeviceGuard g(c->device);
+    int rc = materialize_prim(c);
+    if (rc != ZG_OK) return rc;
     SmfArgs a = make_args(c);
     timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, c->d_flags, (void *)c->stream); });
     cudaError_t e = cudaGetLastError();
