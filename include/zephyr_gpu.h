@@ -131,6 +131,30 @@ int zg_mesh_rectangle(zg_ctx *ctx, int nx, int ny, double x_min, double x_max, d
                       double y_max, const int bounds[4]);
 int zg_mesh_n_cells(const zg_ctx *ctx, int *n);
 
+/* A mesh given cell by cell in the layout of zephyr's AmrCells / AmrFaces
+ * (mesh/euler/amr_cells.h:49-104, amr_faces.h:83-154): every cell has 8 face
+ * slots (slot k of cell i is entry 8*i + k); a slot holds a face or is
+ * UNDEFINED (boundary flag -1) and is then skipped; a side shared with two
+ * finer neighbours uses slots side and side + 4.  Cells are in the mesh's
+ * storage order.  All arrays are host arrays. */
+typedef struct zg_mesh_view {
+    int n_cells;
+    const double *center_x, *center_y; /* cell barycentres, n_cells each */
+    const double *volume;              /* cell areas */
+    const double *incircle;            /* incircle diameters (AmrCells::incircle_diameter) */
+    const int *face_boundary;          /* 8 * n_cells: zephyr Boundary code, -1 = UNDEFINED */
+    const int *face_neib;              /* 8 * n_cells: neighbour cell (the cell itself on boundaries) */
+    const double *face_nx, *face_ny;   /* 8 * n_cells: outward normals */
+    const double *face_cx, *face_cy;   /* 8 * n_cells: face centres */
+    const double *face_area;           /* 8 * n_cells: face lengths */
+} zg_mesh_view;
+
+/* Load a mesh given cell by cell (for example a refined EuMesh); replaces
+ * the EuMesh's AmrCells for the step.  Any previous state is discarded.  The
+ * PARITY kernels run on such meshes; the FAST / MIXED kernels need a mesh from
+ * zg_mesh_rectangle. */
+int zg_mesh_upload(zg_ctx *ctx, const zg_mesh_view *mesh);
+
 /* Configure the solver; replaces SmFluid(eos) and its setters.  The first
  * call allocates the solver's fields (SmFluid::add_types, sm_fluid.cpp:25-35)
  * with zero state and isolation counters; later calls only change the

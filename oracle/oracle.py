@@ -31,6 +31,8 @@ def lib():
         L.zo_mesh_rect.restype = C.c_void_p
         L.zo_mesh_rect.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I]
         L.zo_mesh_free.argtypes = [C.c_void_p]
+        L.zo_mesh_arrays.restype = C.c_void_p
+        L.zo_mesh_arrays.argtypes = [C.c_int, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P]
         L.zo_mesh_ncells.argtypes = [C.c_void_p]
         L.zo_mesh_ncells.restype = C.c_int
         L.zo_mesh_geometry.argtypes = [C.c_void_p, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P]
@@ -75,6 +77,21 @@ class Mesh:
         b = np.ascontiguousarray(bounds, dtype=np.int32)
         self.h = lib().zo_mesh_rect(nx, ny, x_min, x_max, y_min, y_max, _ip(b))
         self.nx, self.ny, self.n = nx, ny, nx * ny
+
+    @classmethod
+    def from_arrays(cls, g):
+        """Mesh given cell by cell: dict with cx, cy, vol, inc (n) and
+        boundary, neib, nx, ny, fx, fy, area (8 n)."""
+        self = cls.__new__(cls)
+        keep = {k: np.ascontiguousarray(g[k], dtype=np.int32 if k in ("boundary", "neib") else np.float64)
+                for k in ("cx", "cy", "vol", "inc", "boundary", "neib", "nx", "ny", "fx", "fy", "area")}
+        self._keep = keep
+        n = keep["cx"].size
+        self.h = lib().zo_mesh_arrays(n, _dp(keep["cx"]), _dp(keep["cy"]), _dp(keep["vol"]), _dp(keep["inc"]),
+                                      _ip(keep["boundary"]), _ip(keep["neib"]), _dp(keep["nx"]), _dp(keep["ny"]),
+                                      _dp(keep["fx"]), _dp(keep["fy"]), _dp(keep["area"]))
+        self.nx, self.ny, self.n = 0, 0, n
+        return self
 
     def geometry(self):
         n = self.n

@@ -21,12 +21,13 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REF = Path(os.environ.get("ZEPHYR_REFERENCE", "/root/reference"))
-SHIM = HERE / "ref_shim"
+SHIM_COMMON = HERE / "ref_shim" / "common"          # Eigen subset, boost bits, configuration.h
+SHIM_MESH = HERE / "ref_shim" / "mesh_standin"      # plain-array EuMesh for the uniform checker
 OUT_DIR = HERE / "_ref"
-OBJ_DIR = OUT_DIR / "obj"
 LIB = OUT_DIR / "libzref.so"
+LIB_MESH = OUT_DIR / "libzref_mesh.so"
 
-# The reference translation units the checker needs (paths in the zephyr tree).
+# The reference translation units of the step (uniform checker, stand-in mesh).
 UNITS = [
     "zephyr/math/solver/sm_fluid.cpp",
     "zephyr/math/solver/riemann.cpp",
@@ -54,40 +55,86 @@ UNITS = [
     "zephyr/geom/primitives/line.cpp",
 ]
 
+# Directories whose every translation unit joins the real-mesh checker, and
+# the units left out: solvers off this path.
+MESH_DIRS = ["zephyr/mesh", "zephyr/geom", "zephyr/math/cfd", "zephyr/math/solver", "zephyr/phys"]
+MESH_FILES = ["zephyr/utils/mpi.cpp", "zephyr/utils/threads.cpp", "zephyr/utils/json.cpp",
+              "zephyr/utils/stopwatch.cpp", "zephyr/utils/numpy.cpp", "zephyr/math/funcs.cpp",
+              "zephyr/math/random.cpp", "zephyr/math/sle/tridiagonal.cpp", "zephyr/math/calc/integrals.cpp"]
+MESH_SKIP = {
+             "zephyr/math/solver/convection.cpp", "zephyr/math/solver/transfer.cpp",
+             "zephyr/math/solver/mm_fluid.cpp"}
+
 FLAGS = ["-std=c++20", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-w"]
+# The reference relies on <cstring> and <functional> arriving through Eigen
+# and Boost headers; the stand-ins do not include them.
+FORCE = ["-include", "cstring", "-include", "functional"]
 
 
 def reference_present() -> bool:
     return (REF / "zephyr" / "math" / "solver" / "sm_fluid.cpp").exists()
 
 
+def _compile(cxx, src, obj, inc, force, verbose, newest_shim):
+    if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_shim):
+        cmd = [cxx, *FLAGS, *FORCE, "-x", "c++", *inc, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+
+def _link(cxx, lib, objs, force, verbose):
+    if force or not lib.exists() or lib.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [cxx, "-shared", "-o", str(lib), *map(str, objs), "-pthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+
+def mesh_units():
+    units = []
+    for d in MESH_DIRS:
+        for ext in ("*.cpp", "*.cxx"):
+            for p in sorted((REF / d).rglob(ext)):
+                rel = str(p.relative_to(REF))
+                if rel not in MESH_SKIP:
+                    units.append(rel)
+    return units + MESH_FILES
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Build both checkers; returns the uniform one's path."""
     if not reference_present():
         if LIB.exists():
             return LIB
         raise FileNotFoundError(f"reference sources not found under {REF}")
     cxx = shutil.which("g++") or "g++"
-    OBJ_DIR.mkdir(parents=True, exist_ok=True)
-    inc = ["-I", str(SHIM), "-I", str(REF)]
-    shims = list(SHIM.rglob("*"))
-    newest_shim = max(p.stat().st_mtime for p in shims if p.is_file())
-    objs = []
-    for unit in UNITS + ["DRIVER"]:
-        src = HERE / "ref_driver.cpp" if unit == "DRIVER" else REF / unit
-        obj = OBJ_DIR / (src.name + ".o")
-        objs.append(obj)
-        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_shim):
-            cmd = [cxx, *FLAGS, "-x", "c++", *inc, "-c", str(src), "-o", str(obj)]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
-    if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [cxx, "-shared", "-o", str(LIB), *map(str, objs), "-pthread"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+    newest_shim = max(p.stat().st_mtime for p in (HERE / "ref_shim").rglob("*") if p.is_file())
+    jobs = os.cpu_count() or 4
+    from concurrent.futures import ThreadPoolExecutor
+
+    # uniform checker: stand-in mesh
+    obj_dir = OUT_DIR / "obj"
+    obj_dir.mkdir(parents=True, exist_ok=True)
+    inc = ["-I", str(SHIM_COMMON), "-I", str(SHIM_MESH), "-I", str(REF)]
+    srcs = [REF / u for u in UNITS] + [HERE / "ref_driver.cpp"]
+    objs = [obj_dir / (s.name + ".o") for s in srcs]
+    with ThreadPoolExecutor(jobs) as ex:
+        list(ex.map(lambda so: _compile(cxx, so[0], so[1], inc, force, verbose, newest_shim), zip(srcs, objs)))
+    _link(cxx, LIB, objs, force, verbose)
+
+    # real-mesh checker: the reference's EuMesh and AMR
+    obj_dir = OUT_DIR / "obj_mesh"
+    obj_dir.mkdir(parents=True, exist_ok=True)
+    inc = ["-I", str(SHIM_COMMON), "-I", str(REF)]
+    units = mesh_units()
+    srcs = [REF / u for u in units] + [HERE / "ref_mesh_driver.cpp"]
+    objs = [obj_dir / (u.replace("/", "_") + ".o") for u in units] + [obj_dir / "ref_mesh_driver.cpp.o"]
+    with ThreadPoolExecutor(jobs) as ex:
+        list(ex.map(lambda so: _compile(cxx, so[0], so[1], inc, force, verbose, newest_shim), zip(srcs, objs)))
+    _link(cxx, LIB_MESH, objs, force, verbose)
     return LIB
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=False))

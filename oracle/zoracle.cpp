@@ -318,6 +318,7 @@ struct Mesh {
     std::vector<int> adj;  // neighbour cell index (self index on boundary slots)
     std::vector<V3> fnormal, fcenter;
     std::vector<double> farea;
+    std::vector<double> incircle;  // given diameters (meshes built from arrays)
 };
 
 // zephyr/mesh/euler/amr_cells_gen.cpp:128-281  AmrCells(const Rectangle&),
@@ -410,6 +411,7 @@ static inline V3 symm_point(const Mesh &m, size_t f, V3 p) {
 }
 // amr_cells.cpp:107-116  incircle_diameter (adaptive, 2-D)
 static inline double incircle_diameter(const Mesh &m, int ic) {
+    if (!m.incircle.empty()) return m.incircle[ic];
     const V3 *q = &m.verts[9 * (size_t)ic];
     return std::sqrt(std::min(sqnorm(sub(q[5], q[3])), sqnorm(sub(q[7], q[1]))));
 }
@@ -863,6 +865,35 @@ void *zo_mesh_rect(int nx, int ny, double x_min, double x_max, double y_min, dou
     zo::make_rectangle(*m, nx, ny, x_min, x_max, y_min, y_max, bounds);
     return m;
 }
+// A mesh given cell by cell (8 slots per cell), e.g. a refined zephyr mesh.
+// The incircle diameters are given; verts then hold them on the vs<+1,0> /
+// vs<-1,0> axis so that incircle_diameter() returns them unchanged.
+void *zo_mesh_arrays(int n, const double *cx, const double *cy, const double *vol, const double *inc,
+                     const int *boundary, const int *adj, const double *nx, const double *ny, const double *fx,
+                     const double *fy, const double *area) {
+    auto *m = new zo::Mesh();
+    m->n_cells = n;
+    m->center.resize(n);
+    m->volume.assign(vol, vol + n);
+    m->verts.assign(9 * (size_t)n, zo::V3{0, 0, 0});
+    m->level.assign(n, 0);
+    m->flag.assign(n, 0);
+    m->b_idx.assign(n, 0);
+    m->z_idx.assign(n, 0);
+    m->boundary.assign(boundary, boundary + 8 * (size_t)n);
+    m->adj.assign(adj, adj + 8 * (size_t)n);
+    m->fnormal.resize(8 * (size_t)n);
+    m->fcenter.resize(8 * (size_t)n);
+    m->farea.assign(area, area + 8 * (size_t)n);
+    m->incircle.assign(inc, inc + n);
+    for (int i = 0; i < n; ++i) m->center[i] = zo::V3{cx[i], cy[i], 0.0};
+    for (size_t f = 0; f < 8 * (size_t)n; ++f) {
+        m->fnormal[f] = zo::V3{nx[f], ny[f], 0.0};
+        m->fcenter[f] = zo::V3{fx[f], fy[f], 0.0};
+    }
+    return m;
+}
+
 void zo_mesh_free(void *m) { delete static_cast<zo::Mesh *>(m); }
 int zo_mesh_ncells(void *m) { return static_cast<zo::Mesh *>(m)->n_cells; }
 

@@ -117,6 +117,37 @@ def make_pointwise():
                         limiter_table=lim, **out)
 
 
+def blast(cx, cy, p_in=10.0):
+    r = np.hypot(cx - 0.5, cy - 0.5)
+    rho = np.ones_like(cx)
+    p = np.where(r < 0.1, p_in, 0.1)
+    return rho, np.zeros_like(cx), np.zeros_like(cx), p, p / (0.4 * rho)
+
+
+def make_amr(name, n, acc, limiter, bounds, max_level, steps, adapt_rounds):
+    """A mesh refined by the reference's EuMesh::refine (flags from
+    SmFluid::set_flags on blast data, as in smf_test_2D.cpp:112-117), then
+    `steps` steps of the reference's SmFluid::update on it."""
+    from oracle import ref_mesh as RM
+    R = RM.RefEuMesh(n, n, bounds=bounds, accuracy=acc, limiter=limiter, CFL=0.4, max_level=max_level)
+    for _ in range(adapt_rounds):
+        c = R.cells()
+        R.set_state(*blast(c["cx"], c["cy"]))
+        R.solver_flags()
+        R.refine()
+    c = R.cells()
+    R.set_state(*blast(c["cx"], c["cy"]))
+    g = R.mesh_arrays()
+    init = np.array(R.state())
+    dts = np.array([R.step() for _ in range(steps)])
+    final = np.array(R.state())
+    flags = R.solver_flags()
+    np.savez_compressed(OUT / f"{name}.npz", steps=steps, accuracy=acc, limiter=limiter, CFL=0.4,
+                        init=init, dts=dts, final=final, flags=flags, wait=R.wait(),
+                        **{k: g[k] for k in ("cx", "cy", "vol", "inc", "level", "z_idx", "b_idx", "boundary",
+                                             "neib", "nx", "ny", "fx", "fy", "area")})
+
+
 def main():
     for name, spec in CASES.items():
         make_case(name, spec)
@@ -124,6 +155,10 @@ def main():
     make_isolation()
     make_pointwise()
     print("wrote isolation, pointwise")
+    make_amr("amr_blast_16_first_order", 16, 1, "MC", (2, 2, 1, 1), 2, 20, 4)
+    make_amr("amr_blast_16_vanalbada", 16, 2, "van Albada", (2, 2, 2, 2), 2, 20, 4)
+    make_amr("amr_blast_12_mc_3levels", 12, 2, "MC", (1, 1, 1, 1), 3, 10, 5)
+    print("wrote amr cases")
 
 
 if __name__ == "__main__":

@@ -10,7 +10,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem not in ("pointwise", "isolation_20_mc"))
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz")
+               if p.stem not in ("pointwise", "isolation_20_mc") and not p.stem.startswith("amr_"))
+AMR_CASES = sorted(p.stem for p in GOLDEN.glob("amr_*.npz"))
 
 
 def _gpu_for(Z, g):
@@ -46,6 +48,40 @@ def test_gpu_matches_reference_fixture(gpu_lib, name):
     assert np.array_equal(final, g["final"]), f"{np.count_nonzero(final != g['final'])} values differ"
     assert np.array_equal(mesh.get_wait(), g["wait"])
     assert np.array_equal(solver.set_flags(mesh), g["flags"])
+
+
+@pytest.mark.parametrize("name", AMR_CASES)
+def test_gpu_matches_reference_on_refined_mesh(gpu_lib, name):
+    """The parity kernels on meshes refined by the reference's refine()
+    (hanging faces, up to three levels), against the reference's steps."""
+    Z = gpu_lib
+    g = np.load(GOLDEN / f"{name}.npz", allow_pickle=False)
+    mesh = Z.EuMesh.from_arrays(g)
+    solver = Z.SmFluid(Z.IdealGas(1.4))
+    solver.set_accuracy(int(g["accuracy"]))
+    solver.set_CFL(float(g["CFL"]))
+    solver.set_limiter(str(g["limiter"]))
+    solver.add_types(mesh)
+    mesh.set_state(*g["init"])
+    dts = []
+    for _ in range(int(g["steps"])):
+        solver.update(mesh)
+        dts.append(solver.dt())
+    assert np.array_equal(np.array(dts), g["dts"])
+    final = np.array(mesh.get_state())
+    assert np.array_equal(final, g["final"]), f"{np.count_nonzero(final != g['final'])} values differ"
+    assert np.array_equal(solver.set_flags(mesh), g["flags"])
+
+
+def test_gpu_refuses_tiled_kernels_on_slot_mesh(gpu_lib):
+    Z = gpu_lib
+    g = np.load(GOLDEN / f"{AMR_CASES[0]}.npz", allow_pickle=False)
+    mesh = Z.EuMesh.from_arrays(g)
+    solver = Z.SmFluid(Z.IdealGas(1.4), kernels=Z.Kernels.FAST)
+    solver.add_types(mesh)
+    mesh.set_state(*g["init"])
+    with pytest.raises(Z.ZgError):
+        solver.update(mesh)
 
 
 def test_gpu_matches_reference_isolation(gpu_lib):

@@ -39,6 +39,17 @@ class SmfParams(C.Structure):
     ]
 
 
+class MeshView(C.Structure):
+    _fields_ = [(n, t) for n, t in (
+        ("n_cells", C.c_int),
+        ("center_x", C.POINTER(C.c_double)), ("center_y", C.POINTER(C.c_double)),
+        ("volume", C.POINTER(C.c_double)), ("incircle", C.POINTER(C.c_double)),
+        ("face_boundary", C.POINTER(C.c_int)), ("face_neib", C.POINTER(C.c_int)),
+        ("face_nx", C.POINTER(C.c_double)), ("face_ny", C.POINTER(C.c_double)),
+        ("face_cx", C.POINTER(C.c_double)), ("face_cy", C.POINTER(C.c_double)),
+        ("face_area", C.POINTER(C.c_double)))]
+
+
 _P = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
 _V = C.c_void_p
@@ -53,6 +64,7 @@ SIGNATURES = {
     "zg_set_stream": (C.c_int, [_V, _V]),
     "zg_mesh_rectangle": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I]),
     "zg_mesh_n_cells": (C.c_int, [_V, _I]),
+    "zg_mesh_upload": (C.c_int, [_V, C.POINTER(MeshView)]),
     "zg_smf_configure": (C.c_int, [_V, C.POINTER(SmfParams)]),
     "zg_smf_set_max_dt": (C.c_int, [_V, C.c_double]),
     "zg_state_upload": (C.c_int, [_V, _P, _P, _P, _P, _P]),

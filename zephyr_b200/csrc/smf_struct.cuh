@@ -1,13 +1,16 @@
-// smf_struct.cuh -- FP64 kernels of SmFluid::update on a structured
-// rectangle (zephyr's AmrCells(Rectangle) without refinement), in the
-// reference's per-cell gather form: every cell walks its face slots in the
-// order L, R, B, T and evaluates each face flux in its own frame, exactly as
-// math/solver/sm_fluid.cpp does.  Compiled with -fmad=false these kernels are
-// the parity path.
+// smf_struct.cuh -- FP64 kernels of SmFluid::update in the reference's
+// per-cell gather form: every cell walks its face slots in slot order (L, R,
+// B, T, then the second halves of split sides) and evaluates each face flux in
+// its own frame, exactly as math/solver/sm_fluid.cpp does.  Compiled with
+// -fmad=false these kernels are the parity path.
 //
-// Cell numbering follows amr_cells_gen.cpp:145-151: ic = i * ny + j.  Face
-// geometry is derived from per-axis tables that the host fills with the
-// reference's own formulas (amr_cells_gen.cpp:158-253, quad.cpp:429-436).
+// The kernels are templated on a mesh accessor:
+//  * StructAcc: a uniform rectangle (zephyr's AmrCells(Rectangle) before any
+//    refinement), cell numbering ic = i * ny + j (amr_cells_gen.cpp:145-151),
+//    geometry from per-axis tables filled with the reference's formulas
+//    (amr_cells_gen.cpp:158-253, quad.cpp:429-436);
+//  * SlotAcc: any mesh given cell by cell with 8 face slots (AMR meshes with
+//    hanging faces).
 #pragma once
 
 #include "smf_math.cuh"
@@ -25,41 +28,54 @@ struct FaceG {
     double area;
 };
 
-__device__ inline FaceG face_geo(const StructMesh &m, int i, int j, int ic, int s) {
-    FaceG g;
-    if (s == 0) {
-        g.flag = i > 0 ? BC_INNER : m.bc[0];
-        g.nb = i > 0 ? ic - m.ny : (m.xper ? ic + (m.nx - 1) * m.ny : ic);
-        g.nx = -1.0; g.ny = -0.0;
-        g.fcx = m.X[i]; g.fcy = m.fym[j];
-        g.area = m.hy;
-    } else if (s == 1) {
-        g.flag = i < m.nx - 1 ? BC_INNER : m.bc[1];
-        g.nb = i < m.nx - 1 ? ic + m.ny : (m.xper ? ic - (m.nx - 1) * m.ny : ic);
-        g.nx = 1.0; g.ny = 0.0;
-        g.fcx = m.X[i + 1]; g.fcy = m.fym[j];
-        g.area = m.hy;
-    } else if (s == 2) {
-        g.flag = j > 0 ? BC_INNER : m.bc[2];
-        g.nb = j > 0 ? ic - 1 : (m.yper ? ic + (m.ny - 1) : ic);
-        g.nx = -0.0; g.ny = -1.0;
-        g.fcx = m.fxm[i]; g.fcy = m.Y[j];
-        g.area = m.hx;
-    } else {
-        g.flag = j < m.ny - 1 ? BC_INNER : m.bc[3];
-        g.nb = j < m.ny - 1 ? ic + 1 : (m.yper ? ic - (m.ny - 1) : ic);
-        g.nx = 0.0; g.ny = 1.0;
-        g.fcx = m.fxm[i]; g.fcy = m.Y[j + 1];
-        g.area = m.hx;
+// Uniform rectangle.
+struct StructAcc {
+    static constexpr int NSLOT = 4;
+    const StructMesh &m;
+    int ic, i, j;
+    __device__ StructAcc(const SmfArgs &a, int ic_) : m(a.mesh), ic(ic_) {
+        i = ic / m.ny;
+        j = ic - i * m.ny;
     }
-    return g;
-}
+    __device__ static int n(const SmfArgs &a) { return a.mesh.n; }
+    __device__ double cx() const { return m.cx[i]; }
+    __device__ double cy() const { return m.cy[j]; }
+    __device__ double vol() const { return m.vol; }
+    // incircle diameter (amr_cells.cpp:107-116)
+    __device__ double dinc() const { return sqrt(smin(m.inc2x[i], m.inc2y[j])); }
 
-// Centre of the neighbour across slot s, or the mirror of the cell centre in
-// the face (sm_fluid.cpp:211-212; amr_faces.h:197-199 symm_point).
-__device__ inline void neib_center(const StructMesh &m, const FaceG &g, int i, int j, int s, double pcx,
-                                   double pcy, double &ncx, double &ncy) {
-    if (g.flag == BC_INNER) {
+    // Face geometry of slot s (0 L, 1 R, 2 B, 3 T).
+    __device__ FaceG face(int s) const {
+        FaceG g;
+        if (s == 0) {
+            g.flag = i > 0 ? BC_INNER : m.bc[0];
+            g.nb = i > 0 ? ic - m.ny : (m.xper ? ic + (m.nx - 1) * m.ny : ic);
+            g.nx = -1.0; g.ny = -0.0;
+            g.fcx = m.X[i]; g.fcy = m.fym[j];
+            g.area = m.hy;
+        } else if (s == 1) {
+            g.flag = i < m.nx - 1 ? BC_INNER : m.bc[1];
+            g.nb = i < m.nx - 1 ? ic + m.ny : (m.xper ? ic - (m.nx - 1) * m.ny : ic);
+            g.nx = 1.0; g.ny = 0.0;
+            g.fcx = m.X[i + 1]; g.fcy = m.fym[j];
+            g.area = m.hy;
+        } else if (s == 2) {
+            g.flag = j > 0 ? BC_INNER : m.bc[2];
+            g.nb = j > 0 ? ic - 1 : (m.yper ? ic + (m.ny - 1) : ic);
+            g.nx = -0.0; g.ny = -1.0;
+            g.fcx = m.fxm[i]; g.fcy = m.Y[j];
+            g.area = m.hx;
+        } else {
+            g.flag = j < m.ny - 1 ? BC_INNER : m.bc[3];
+            g.nb = j < m.ny - 1 ? ic + 1 : (m.yper ? ic - (m.ny - 1) : ic);
+            g.nx = 0.0; g.ny = 1.0;
+            g.fcx = m.fxm[i]; g.fcy = m.Y[j + 1];
+            g.area = m.hx;
+        }
+        return g;
+    }
+    // Centre of the neighbour across slot s (INNER faces only).
+    __device__ void nb_center(const FaceG &g, int s, double &ncx, double &ncy) const {
         int in = i, jn = j;
         if (s == 0) in = i - 1;
         else if (s == 1) in = i + 1;
@@ -67,6 +83,45 @@ __device__ inline void neib_center(const StructMesh &m, const FaceG &g, int i, i
         else jn = j + 1;
         ncx = m.cx[in];
         ncy = m.cy[jn];
+    }
+};
+
+// Mesh given slot by slot (AMR).
+struct SlotAcc {
+    static constexpr int NSLOT = 8;
+    const SlotMesh &m;
+    int ic;
+    __device__ SlotAcc(const SmfArgs &a, int ic_) : m(a.smesh), ic(ic_) {}
+    __device__ static int n(const SmfArgs &a) { return a.smesh.n; }
+    __device__ double cx() const { return m.cx[ic]; }
+    __device__ double cy() const { return m.cy[ic]; }
+    __device__ double vol() const { return m.vol[ic]; }
+    __device__ double dinc() const { return m.inc[ic]; }
+    __device__ FaceG face(int s) const {
+        const int f = 8 * ic + s;
+        FaceG g;
+        g.flag = m.fb[f];
+        g.nb = m.fn[f];
+        g.nx = m.fnx[f];
+        g.ny = m.fny[f];
+        g.fcx = m.fcx[f];
+        g.fcy = m.fcy[f];
+        g.area = m.fa[f];
+        return g;
+    }
+    __device__ void nb_center(const FaceG &g, int, double &ncx, double &ncy) const {
+        ncx = m.cx[g.nb];
+        ncy = m.cy[g.nb];
+    }
+};
+
+// Centre of the neighbour across slot s, or the mirror of the cell centre in
+// the face (sm_fluid.cpp:211-212; amr_faces.h:197-199 symm_point).
+template <class Acc>
+__device__ inline void neib_center(const Acc &c, const FaceG &g, int s, double pcx, double pcy, double &ncx,
+                                   double &ncy) {
+    if (g.flag == BC_INNER) {
+        c.nb_center(g, s, ncx, ncy);
     } else {
         double d = (g.fcx - pcx) * g.nx + (g.fcy - pcy) * g.ny;
         double t = 2.0 * d;
@@ -106,19 +161,34 @@ __device__ inline Prim boundary_value(const Prim &zc, double nx, double ny, int 
 // dt of the current step, written by the last block of k_dt.
 __device__ inline double finalize_dt(const SmfArgs &a) { return *a.dt_out; }
 
+// Rotation of a velocity into / out of the face frame (rotate.cpp:7-77): the
+// normal is normalised first.  Axis normals of a rectangle are unit vectors
+// already, so the structured accessor skips the normalisation.
+template <class Acc>
+__device__ inline void frame(const FaceG &g, double &c, double &s) {
+    c = g.nx;
+    s = g.ny;
+    if (Acc::NSLOT == 8) {
+        double sn = g.nx * g.nx + g.ny * g.ny;
+        if (sn > 0.0) {
+            double r = sqrt(sn);
+            c = g.nx / r;
+            s = g.ny / r;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // K1: CFL minimum over cells (sm_fluid.cpp:104-114, amr_cells.cpp:107-116).
-template <int BLOCK>
+template <class Acc, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_dt(SmfArgs a) {
-    const StructMesh &m = a.mesh;
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
-    if (ic < m.n) {
-        int i = ic / m.ny, j = ic - i * m.ny;
+    if (ic < Acc::n(a)) {
+        Acc c(a, ic);
         double rho = a.z.r[ic], u = a.z.u[ic], v = a.z.v[ic], p = a.z.p[ic];
-        double c = a.eos.sound_speed_rP(rho, p);
-        double dinc = sqrt(smin(m.inc2x[i], m.inc2y[j]));
-        double lam = dinc / (sqrt(u * u + v * v) + c);
+        double cs = a.eos.sound_speed_rP(rho, p);
+        double lam = c.dinc() / (sqrt(u * u + v * v) + cs);
         // std::min skips a NaN in its second slot; NaN bits sort above all
         // finite positives, so the unsigned minimum skips it too.
         unsigned long long b = dbits(lam);
@@ -157,37 +227,46 @@ __global__ void __launch_bounds__(BLOCK) k_dt(SmfArgs a) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// K2: first-order step (sm_fluid.cpp:127-174).
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_flux1(SmfArgs a) {
-    const StructMesh &m = a.mesh;
-    int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= m.n) return;
-    double dt = finalize_dt(a);
-    int i = ic / m.ny, j = ic - i * m.ny;
-    Prim zc = load_prim(a.z, ic);
-    Cons q = q_from_p(zc);
-    Cons F{0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        FaceG g = face_geo(m, i, j, ic, s);
-        Prim zn = !is_boundary(g.flag) ? load_prim(a.z, g.nb) : boundary_value(zc, g.nx, g.ny, g.flag);
-        Prim zm = zc, zp = zn;
-        rot_local(zm.u, zm.v, g.nx, g.ny);
-        rot_local(zp.u, zp.v, g.nx, g.ny);
-        Cons lf = num_flux(a.flux, zm, zp, a.eos);
-        rot_global(lf.mu, lf.mv, g.nx, g.ny);
-        F.r += lf.r * g.area;
-        F.mu += lf.mu * g.area;
-        F.mv += lf.mv * g.area;
-        F.E += lf.E * g.area;
-    }
-    double coef = dt / m.vol;
+__device__ inline void add_area(Cons &F, const Cons &lf, double area) {
+    F.r += lf.r * area;
+    F.mu += lf.mu * area;
+    F.mv += lf.mv * area;
+    F.E += lf.E * area;
+}
+
+__device__ inline void update(Cons &q, double coef, const Cons &F) {
     q.r -= coef * F.r;
     q.mu -= coef * F.mu;
     q.mv -= coef * F.mv;
     q.E -= coef * F.E;
+}
+
+// ---------------------------------------------------------------------------
+// K2: first-order step (sm_fluid.cpp:127-174).
+template <class Acc, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_flux1(SmfArgs a) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= Acc::n(a)) return;
+    Acc c(a, ic);
+    double dt = finalize_dt(a);
+    Prim zc = load_prim(a.z, ic);
+    Cons q = q_from_p(zc);
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < Acc::NSLOT; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        Prim zn = !is_boundary(g.flag) ? load_prim(a.z, g.nb) : boundary_value(zc, g.nx, g.ny, g.flag);
+        double cs, sn;
+        frame<Acc>(g, cs, sn);
+        Prim zm = zc, zp = zn;
+        rot_local(zm.u, zm.v, cs, sn);
+        rot_local(zp.u, zp.v, cs, sn);
+        Cons lf = num_flux(a.flux, zm, zp, a.eos);
+        rot_global(lf.mu, lf.mv, cs, sn);
+        add_area(F, lf, g.area);
+    }
+    update(q, dt / c.vol(), F);
     store_prim(a.znext, ic, p_from_q(q, a.eos));
 }
 
@@ -201,19 +280,24 @@ __global__ void __launch_bounds__(BLOCK) k_flux1(SmfArgs a) {
 // 2-D reduction of the 3x3 system: A(i,2) and A(2,j) are exact zeros, A(2,2)
 // is set to 1 (gradient.h:268-273), and Eigen's cofactor inverse then gives
 //   det = A11*A00 + (-A01)*A10,  B = [A11 -A01; -A10 A00] * (1/det).
-__device__ inline void lsm_limited(const StructMesh &m, const PrimPtr &z, int lim, int ic, int i, int j,
-                                   const Prim &zc, double gx[4], double gy[4]) {
-    double pcx = m.cx[i], pcy = m.cy[j];
-    double wv[4], drx[4], dry[4], drnx[4], drny[4], dn[4][4];
+template <class Acc>
+__device__ inline void lsm_limited(const Acc &c, const PrimPtr &z, int lim, const Prim &zc, double gx[4],
+                                   double gy[4]) {
+    constexpr int NS = Acc::NSLOT;
+    const double pcx = c.cx(), pcy = c.cy();
+    double wv[NS], drx[NS], dry[NS], drnx[NS], drny[NS], dn[NS][4];
+    bool on[NS];
     double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
     double Fx[4] = {0.0, 0.0, 0.0, 0.0}, Fy[4] = {0.0, 0.0, 0.0, 0.0};
     const double zcv[4] = {zc.r, zc.u, zc.v, zc.p};
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        FaceG g = face_geo(m, i, j, ic, s);
+    for (int s = 0; s < NS; ++s) {
+        FaceG g = c.face(s);
+        on[s] = g.flag != BC_UNDEFINED;
+        if (!on[s]) continue;
         Prim zn = !is_boundary(g.flag) ? load_prim(z, g.nb) : boundary_value(zc, g.nx, g.ny, g.flag);
         double ncx, ncy;
-        neib_center(m, g, i, j, s, pcx, pcy, ncx, ncy);
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
         double rx = ncx - pcx, ry = ncy - pcy;
         double d = rx * g.nx + ry * g.ny;
         double nxx = d * g.nx, nyy = d * g.ny;
@@ -245,7 +329,8 @@ __device__ inline void lsm_limited(const StructMesh &m, const PrimPtr &z, int li
     }
     double Lx[4] = {0.0, 0.0, 0.0, 0.0}, Ly[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < NS; ++s) {
+        if (!on[s]) continue;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             double dF_p = dn[s][k];
@@ -263,15 +348,14 @@ __device__ inline void lsm_limited(const StructMesh &m, const PrimPtr &z, int li
     }
 }
 
-template <int BLOCK>
+template <class Acc, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_grad(SmfArgs a, PrimPtr z) {
-    const StructMesh &m = a.mesh;
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= m.n) return;
-    int i = ic / m.ny, j = ic - i * m.ny;
+    if (ic >= Acc::n(a)) return;
+    Acc c(a, ic);
     Prim zc = load_prim(z, ic);
     double gx[4], gy[4];
-    lsm_limited(m, z, a.limiter, ic, i, j, zc, gx, gy);
+    lsm_limited(c, z, a.limiter, zc, gx, gy);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         a.gx[k][ic] = gx[k];
@@ -293,52 +377,47 @@ __device__ inline Prim extrap(const Prim &u, const SmfArgs &a, int ic, double dx
 
 // ---------------------------------------------------------------------------
 // K4: predictor, half step with the physical flux (sm_fluid.cpp:176-253).
-template <int BLOCK>
+template <class Acc, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_stage1(SmfArgs a) {
-    const StructMesh &m = a.mesh;
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= m.n) return;
+    if (ic >= Acc::n(a)) return;
+    Acc c(a, ic);
     double dt = finalize_dt(a);
     Prim zc = load_prim(a.z, ic);
     if (a.wait_in[ic] > 0) {
         store_prim(a.zhalf, ic, zc);
         return;
     }
-    int i = ic / m.ny, j = ic - i * m.ny;
-    double pcx = m.cx[i], pcy = m.cy[j];
+    double pcx = c.cx(), pcy = c.cy();
     Cons q = q_from_p(zc);
     Cons F{0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        FaceG g = face_geo(m, i, j, ic, s);
+    for (int s = 0; s < Acc::NSLOT; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
         Prim zm = extrap(zc, a, ic, g.fcx - pcx, g.fcy - pcy);
         zm.e = a.eos.energy_rP(zm.r, zm.p);
         if (is_bad(zm, a.eos)) zm = zc;
-        rot_local(zm.u, zm.v, g.nx, g.ny);
+        double cs, sn;
+        frame<Acc>(g, cs, sn);
+        rot_local(zm.u, zm.v, cs, sn);
         Cons lf = flux_from_p(zm);
-        rot_global(lf.mu, lf.mv, g.nx, g.ny);
-        F.r += lf.r * g.area;
-        F.mu += lf.mu * g.area;
-        F.mv += lf.mv * g.area;
-        F.E += lf.E * g.area;
+        rot_global(lf.mu, lf.mv, cs, sn);
+        add_area(F, lf, g.area);
     }
-    double coef = 0.5 * dt / m.vol;
-    q.r -= coef * F.r;
-    q.mu -= coef * F.mu;
-    q.mv -= coef * F.mv;
-    q.E -= coef * F.E;
+    update(q, 0.5 * dt / c.vol(), F);
     Prim h = p_from_q(q, a.eos);
     if (is_bad(h, a.eos)) h = zc;
     store_prim(a.zhalf, ic, h);
 }
 
 // Face flux of the corrector (sm_fluid.cpp:271-341): reconstruct with the
-// gradients of z at the states zh and solve the Riemann problem.
-__device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &z, const PrimPtr &zh, const int *wt,
-                                      int ic, int i, int j, int s, const Prim &zc, const Prim &zch,
-                                      double pcx, double pcy, int wc) {
-    const StructMesh &m = a.mesh;
-    FaceG g = face_geo(m, i, j, ic, s);
+// gradients of z at the states zh and solve the Riemann problem; returned
+// multiplied by the face area.
+template <class Acc>
+__device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &zh, const int *wt, const Acc &c, int s,
+                                      const FaceG &g, const Prim &zch, double pcx, double pcy, int wc) {
+    const int ic = c.ic;
     bool bnd = is_boundary(g.flag);
     Prim z_nh = !bnd ? load_prim(zh, g.nb) : boundary_value(zch, g.nx, g.ny, g.flag);
     Prim zm, zp;
@@ -348,7 +427,7 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &z, const 
         zp = z_nh;
     } else {
         double ncx, ncy;
-        neib_center(m, g, i, j, s, pcx, pcy, ncx, ncy);
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
         zm = extrap(zch, a, ic, g.fcx - pcx, g.fcy - pcy);
         zm.e = a.eos.energy_rP(zm.r, zm.p);
         if (is_bad(zm, a.eos)) zm = zch;
@@ -360,10 +439,12 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &z, const 
             zp = boundary_value(zm, g.nx, g.ny, g.flag);
         }
     }
-    rot_local(zm.u, zm.v, g.nx, g.ny);
-    rot_local(zp.u, zp.v, g.nx, g.ny);
+    double cs, sn;
+    frame<Acc>(g, cs, sn);
+    rot_local(zm.u, zm.v, cs, sn);
+    rot_local(zp.u, zp.v, cs, sn);
     Cons lf = robust ? hll(zm, zp, a.eos) : num_flux(a.flux, zm, zp, a.eos);
-    rot_global(lf.mu, lf.mv, g.nx, g.ny);
+    rot_global(lf.mu, lf.mv, cs, sn);
     lf.r *= g.area;
     lf.mu *= g.area;
     lf.mv *= g.area;
@@ -373,32 +454,29 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &z, const 
 
 // K5: corrector with the isolation bit (sm_fluid.cpp:255-366).  `wait` is
 // read from the previous step's array and written to the other one.
-template <int BLOCK>
+template <class Acc, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_stage2(SmfArgs a) {
-    const StructMesh &m = a.mesh;
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= m.n) return;
+    if (ic >= Acc::n(a)) return;
+    Acc c(a, ic);
     double dt = finalize_dt(a);
-    int i = ic / m.ny, j = ic - i * m.ny;
-    double pcx = m.cx[i], pcy = m.cy[j];
+    double pcx = c.cx(), pcy = c.cy();
     Prim zc = load_prim(a.z, ic);
     Prim zch = load_prim(a.zhalf, ic);
     int wc = a.wait_in[ic];
     Cons q = q_from_p(zc);
     Cons F{0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        Cons lf = corrector_face(a, a.z, a.zhalf, a.wait_in, ic, i, j, s, zc, zch, pcx, pcy, wc);
+    for (int s = 0; s < Acc::NSLOT; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        Cons lf = corrector_face(a, a.zhalf, a.wait_in, c, s, g, zch, pcx, pcy, wc);
         F.r += lf.r;
         F.mu += lf.mu;
         F.mv += lf.mv;
         F.E += lf.E;
     }
-    double coef = dt / m.vol;
-    q.r -= coef * F.r;
-    q.mu -= coef * F.mu;
-    q.mv -= coef * F.mv;
-    q.E -= coef * F.E;
+    update(q, dt / c.vol(), F);
     Prim n = p_from_q(q, a.eos);
     int wn = wc;
     if (is_bad(n, a.eos)) {
@@ -416,30 +494,27 @@ __global__ void __launch_bounds__(BLOCK) k_stage2(SmfArgs a) {
 // corrector with z_half = z, no isolation):
 //   stage A: z* = P(Q(z^n) - dt/V * sum F(z^n))
 //   stage B: z^{n+1} = P(0.5 * (Q(z^n) + Q(z*) - dt/V * sum F(z*)))
-template <int BLOCK, bool FINAL>
+template <class Acc, int BLOCK, bool FINAL>
 __global__ void __launch_bounds__(BLOCK) k_heun(SmfArgs a, PrimPtr zin, PrimPtr zout) {
-    const StructMesh &m = a.mesh;
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= m.n) return;
+    if (ic >= Acc::n(a)) return;
+    Acc c(a, ic);
     double dt = finalize_dt(a);
-    int i = ic / m.ny, j = ic - i * m.ny;
-    double pcx = m.cx[i], pcy = m.cy[j];
+    double pcx = c.cx(), pcy = c.cy();
     Prim zc = load_prim(zin, ic);
     Cons q = q_from_p(zc);
     Cons F{0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        Cons lf = corrector_face(a, zin, zin, nullptr, ic, i, j, s, zc, zc, pcx, pcy, 0);
+    for (int s = 0; s < Acc::NSLOT; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        Cons lf = corrector_face(a, zin, nullptr, c, s, g, zc, pcx, pcy, 0);
         F.r += lf.r;
         F.mu += lf.mu;
         F.mv += lf.mv;
         F.E += lf.E;
     }
-    double coef = dt / m.vol;
-    q.r -= coef * F.r;
-    q.mu -= coef * F.mu;
-    q.mv -= coef * F.mv;
-    q.E -= coef * F.E;
+    update(q, dt / c.vol(), F);
     if (FINAL) {
         Cons q0 = q_from_p(load_prim(a.z, ic));
         q.r = 0.5 * (q0.r + q.r);
@@ -452,20 +527,19 @@ __global__ void __launch_bounds__(BLOCK) k_heun(SmfArgs a, PrimPtr zin, PrimPtr 
 
 // ---------------------------------------------------------------------------
 // AMR flags by neighbour jumps (sm_fluid.cpp:517-559).
-template <int BLOCK>
+template <class Acc, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_flags(SmfArgs a, int *flags) {
-    const StructMesh &m = a.mesh;
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= m.n) return;
-    int i = ic / m.ny, j = ic - i * m.ny;
+    if (ic >= Acc::n(a)) return;
+    Acc c(a, ic);
     const double xi_dens = 0.05, xi_pres = 0.05;
     double dens = a.z.r[ic], pres = a.z.p[ic];
     double dens_split = xi_dens * fabs(dens);
     double pres_split = xi_pres * fabs(pres);
     int fl = -1;
-    for (int s = 0; s < 4; ++s) {
-        FaceG g = face_geo(m, i, j, ic, s);
-        if (is_boundary(g.flag)) continue;
+    for (int s = 0; s < Acc::NSLOT; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED || is_boundary(g.flag)) continue;
         double dn = a.z.r[g.nb], pn = a.z.p[g.nb];
         if (fabs(dn - dens) > dens_split || fabs(pn - pres) > pres_split) {
             fl = 1;

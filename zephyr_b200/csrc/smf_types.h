@@ -21,12 +21,24 @@ struct StructMesh {
     double hx, hy, vol;
 };
 
+// Mesh given cell by cell in the layout of zephyr's AmrCells / AmrFaces
+// (amr_cells.h:49-104, amr_faces.h:83-154): 8 face slots per cell
+// (face_begin = 8 * ic), UNDEFINED slots skipped in slot order; hanging faces
+// of a refined neighbour occupy slots side and side + 4.  Used for AMR meshes.
+struct SlotMesh {
+    int n;
+    const double *cx, *cy, *vol, *inc;  // centre, volume, incircle diameter
+    const int *fb, *fn;                 // per slot: boundary flag, neighbour cell
+    const double *fnx, *fny, *fcx, *fcy, *fa;  // per slot: normal, centre, area
+};
+
 struct PrimPtr {
     double *r, *u, *v, *p, *e;
 };
 
 struct SmfArgs {
     StructMesh mesh;
+    SlotMesh smesh;  // used instead of `mesh` by the slot-mesh kernels
     EosD eos;
     int flux, limiter;
     double CFL, max_dt;
@@ -40,14 +52,15 @@ struct SmfArgs {
 };
 
 // Launchers (one set per numerics flavour).
+// Parity kernels; `slots` selects the slot-mesh (AMR) geometry.
 namespace parity {
-void launch_dt(const SmfArgs &a, PrimPtr z, void *stream);
-void launch_flux1(const SmfArgs &a, void *stream);
-void launch_grad(const SmfArgs &a, PrimPtr z, void *stream);
-void launch_stage1(const SmfArgs &a, void *stream);
-void launch_stage2(const SmfArgs &a, void *stream);
-void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream);
-void launch_flags(const SmfArgs &a, int *flags, void *stream);
+void launch_dt(const SmfArgs &a, PrimPtr z, bool slots, void *stream);
+void launch_flux1(const SmfArgs &a, bool slots, void *stream);
+void launch_grad(const SmfArgs &a, PrimPtr z, bool slots, void *stream);
+void launch_stage1(const SmfArgs &a, bool slots, void *stream);
+void launch_stage2(const SmfArgs &a, bool slots, void *stream);
+void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, bool slots, void *stream);
+void launch_flags(const SmfArgs &a, int *flags, bool slots, void *stream);
 }  // namespace parity
 
 }  // namespace zg

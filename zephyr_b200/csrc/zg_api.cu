@@ -29,6 +29,9 @@ struct zg_ctx {
     bool have_mesh = false;
     int nx = 0, ny = 0, n = 0;
     StructMesh mesh{};
+    bool slots = false;        // mesh given cell by cell (zg_mesh_upload)
+    SlotMesh smesh{};
+    void *d_slot = nullptr;    // slot-mesh arrays
     double *d_geo = nullptr;  // all geometry tables
     double *d_tgeo = nullptr;  // per-axis tables of the tiled kernels, FP64 then FP32
     tiled::AxisGeo<double> ax64{}, ay64{};
@@ -120,14 +123,18 @@ void free_solver(zg_ctx *c) {
 void free_mesh(zg_ctx *c) {
     cudaFree(c->d_geo);
     cudaFree(c->d_tgeo);
+    cudaFree(c->d_slot);
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
+    c->d_slot = nullptr;
+    c->slots = false;
     c->have_mesh = false;
 }
 
 SmfArgs make_args(const zg_ctx *c) {
     SmfArgs a{};
     a.mesh = c->mesh;
+    a.smesh = c->smesh;
     a.eos = c->eos;
     a.flux = c->par.flux;
     a.limiter = c->par.limiter;
@@ -313,19 +320,19 @@ void timed(zg_ctx *c, int kind, F &&launch) {
 int enqueue_parity_step(zg_ctx *c) {
     SmfArgs a = make_args(c);
     void *st = (void *)c->stream;
-    timed(c, ZG_K_DT, [&] { parity::launch_dt(a, c->z, st); });
+    timed(c, ZG_K_DT, [&] { parity::launch_dt(a, c->z, c->slots, st); });
     if (c->par.accuracy == 1) {
-        timed(c, ZG_K_FLUX1, [&] { parity::launch_flux1(a, st); });
+        timed(c, ZG_K_FLUX1, [&] { parity::launch_flux1(a, c->slots, st); });
     } else if (c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
-        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, st); });
-        timed(c, ZG_K_STAGE1, [&] { parity::launch_stage1(a, st); });
-        timed(c, ZG_K_STAGE2, [&] { parity::launch_stage2(a, st); });
+        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, c->slots, st); });
+        timed(c, ZG_K_STAGE1, [&] { parity::launch_stage1(a, c->slots, st); });
+        timed(c, ZG_K_STAGE2, [&] { parity::launch_stage2(a, c->slots, st); });
         c->wait_cur = 1 - c->wait_cur;
     } else {
-        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, st); });
-        timed(c, ZG_K_HEUN_A, [&] { parity::launch_heun(a, c->z, c->zhalf, false, st); });
-        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->zhalf, st); });
-        timed(c, ZG_K_HEUN_B, [&] { parity::launch_heun(a, c->zhalf, c->znext, true, st); });
+        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, c->slots, st); });
+        timed(c, ZG_K_HEUN_A, [&] { parity::launch_heun(a, c->z, c->zhalf, false, c->slots, st); });
+        timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->zhalf, c->slots, st); });
+        timed(c, ZG_K_HEUN_B, [&] { parity::launch_heun(a, c->zhalf, c->znext, true, c->slots, st); });
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
@@ -390,6 +397,8 @@ int enqueue_tiled_step(zg_ctx *c) {
 }
 
 int enqueue_step(zg_ctx *c) {
+    if (c->slots && (c->par.precision == ZG_MIXED || c->par.kernels == ZG_KERNELS_FAST))
+        return fail(c, ZG_ERR_STATE, "the FAST and MIXED kernels need a rectangle mesh (zg_mesh_rectangle)");
     if (c->par.precision == ZG_MIXED) {
         int rc = convert_state(c, ZG_MIXED);
         if (rc != ZG_OK) return rc;
@@ -594,6 +603,65 @@ int zg_mesh_n_cells(const zg_ctx *c, int *n) {
     return ZG_OK;
 }
 
+int zg_mesh_upload(zg_ctx *c, const zg_mesh_view *v) {
+    if (!c || !v) return ZG_ERR_ARG;
+    if (v->n_cells < 1) return fail(c, ZG_ERR_ARG, "zg_mesh_upload: n_cells must be positive");
+    if ((long long)v->n_cells > (long long)std::numeric_limits<int>::max() / 8)
+        return fail(c, ZG_ERR_ARG, "zg_mesh_upload: too many cells for 32-bit indices");
+    const void *need[] = {v->center_x, v->center_y, v->volume, v->incircle, v->face_boundary, v->face_neib,
+                          v->face_nx, v->face_ny, v->face_cx, v->face_cy, v->face_area};
+    for (const void *q : need)
+        if (!q) return fail(c, ZG_ERR_ARG, "zg_mesh_upload: null array");
+    const int n = v->n_cells;
+    for (long long f = 0; f < 8LL * n; ++f) {  // neighbour indices must stay inside the mesh
+        int b = v->face_boundary[f], nb = v->face_neib[f];
+        if (b != -1 && (nb < 0 || nb >= n))
+            return fail(c, ZG_ERR_ARG, "zg_mesh_upload: neighbour index out of range");
+        if (b < -1 || b > ZG_BC_PERIODIC) return fail(c, ZG_ERR_ARG, "zg_mesh_upload: unknown boundary flag");
+    }
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_solver(c);
+    free_mesh(c);
+    size_t nd = 4 * (size_t)n + 5 * 8 * (size_t)n, ni = 2 * 8 * (size_t)n;
+    ZG_CUDA(c, cudaMalloc(&c->d_slot, nd * sizeof(double) + ni * sizeof(int)));
+    double *d = static_cast<double *>(c->d_slot);
+    int *ip = reinterpret_cast<int *>(d + nd);
+    const double *srcd[9] = {v->center_x, v->center_y, v->volume, v->incircle, v->face_nx, v->face_ny,
+                             v->face_cx, v->face_cy, v->face_area};
+    size_t lens[9] = {(size_t)n, (size_t)n, (size_t)n, (size_t)n, 8 * (size_t)n, 8 * (size_t)n, 8 * (size_t)n,
+                      8 * (size_t)n, 8 * (size_t)n};
+    const double *dst[9];
+    size_t off = 0;
+    for (int k = 0; k < 9; ++k) {
+        ZG_CUDA(c, cudaMemcpy(d + off, srcd[k], lens[k] * sizeof(double), cudaMemcpyHostToDevice));
+        dst[k] = d + off;
+        off += lens[k];
+    }
+    ZG_CUDA(c, cudaMemcpy(ip, v->face_boundary, 8 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice));
+    ZG_CUDA(c, cudaMemcpy(ip + 8 * (size_t)n, v->face_neib, 8 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice));
+    SlotMesh &m = c->smesh;
+    m.n = n;
+    m.cx = dst[0];
+    m.cy = dst[1];
+    m.vol = dst[2];
+    m.inc = dst[3];
+    m.fnx = dst[4];
+    m.fny = dst[5];
+    m.fcx = dst[6];
+    m.fcy = dst[7];
+    m.fa = dst[8];
+    m.fb = ip;
+    m.fn = ip + 8 * (size_t)n;
+    c->mesh = StructMesh{};
+    c->mesh.n = n;
+    c->n = n;
+    c->nx = c->ny = 0;
+    c->slots = true;
+    c->have_mesh = true;
+    return ZG_OK;
+}
+
 int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     if (!c || !p) return ZG_ERR_ARG;
     if (!c->have_mesh) return fail(c, ZG_ERR_STATE, "zg_smf_configure: no mesh");
@@ -769,7 +837,7 @@ int zg_smf_set_flags(zg_ctx *c, int *flags) {
     int rc = materialize_prim(c);
     if (rc != ZG_OK) return rc;
     SmfArgs a = make_args(c);
-    timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, c->d_flags, (void *)c->stream); });
+    timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, c->d_flags, c->slots, (void *)c->stream); });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "flags kernel launch");
     ZG_CUDA(c, cudaMemcpyAsync(flags, c->d_flags, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost,

@@ -171,6 +171,36 @@ class EuMesh:
         self.gen = gen
         self.solver = None
 
+    @classmethod
+    def from_arrays(cls, g: dict, device: int = 0, stream=None):
+        """A mesh given cell by cell (for example a refined zephyr mesh):
+        dict with cx, cy, vol, inc (n cells) and boundary, neib, nx, ny, fx,
+        fy, area (8 slots per cell), in zephyr's AmrCells order."""
+        from ._lib import MeshView
+        self = cls.__new__(cls)
+        self._lib = load()
+        self.ctx = C.c_void_p()
+        check(None, self._lib.zg_create(C.byref(self.ctx), device))
+        self.device = device
+        if stream is not None:
+            self.set_stream(stream)
+        keep = {k: np.ascontiguousarray(g[k], dtype=np.int32 if k in ("boundary", "neib") else np.float64)
+                for k in ("cx", "cy", "vol", "inc", "boundary", "neib", "nx", "ny", "fx", "fy", "area")}
+        n = keep["cx"].size
+        for k in ("boundary", "neib", "nx", "ny", "fx", "fy", "area"):
+            if keep[k].size != 8 * n:
+                raise ZgError(-1, f"{k} must have 8 entries per cell")
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        view = MeshView(n, dp(keep["cx"]), dp(keep["cy"]), dp(keep["vol"]), dp(keep["inc"]),
+                        ip(keep["boundary"]), ip(keep["neib"]), dp(keep["nx"]), dp(keep["ny"]),
+                        dp(keep["fx"]), dp(keep["fy"]), dp(keep["area"]))
+        check(self.ctx, self._lib.zg_mesh_upload(self.ctx, C.byref(view)))
+        self.nx = self.ny = 0
+        self.gen = None
+        self.solver = None
+        return self
+
     def set_stream(self, stream):
         """Queue all work on `stream` (a cudaStream_t handle as int, or None)."""
         handle = int(stream) if stream is not None else None
