@@ -33,6 +33,7 @@ extern "C" {
 #define ZG_ERR_STATE (-3)   /* call out of order (no mesh, no configuration) */
 #define ZG_ERR_ALLOC (-4)   /* device memory allocation failed */
 #define ZG_ERR_NUMERIC (-5) /* a non-finite flux or state was produced */
+#define ZG_ERR_TOO_LARGE (-6) /* mesh larger than zg_rect_step_noalloc accepts */
 
 /* Boundary flags; values of zephyr's `enum class Boundary`
  * (geom/boundary.h:9-16). */
@@ -216,6 +217,38 @@ const char *zg_kernel_name(int kind);
 
 /* Wait for the context's stream. */
 int zg_synchronize(zg_ctx *ctx);
+
+/* Largest nx and ny that zg_rect_step_noalloc accepts. */
+#define ZG_NOALLOC_MAX_AXIS 8192
+
+/* One first-order step (accuracy 1, FP64, PARITY kernels) on the rectangle
+ * of zg_mesh_rectangle, without a context and without allocating any memory.
+ * It has no counterpart in the reference: it is for callers that cannot let
+ * a library allocate device memory -- a program that hands out every byte of
+ * each GPU from its own pool, or one that must not have an allocation
+ * synchronise the device between its own stream operations.
+ *
+ * in[5] and out[5] are device arrays of nx * ny doubles each (density,
+ * velocity x, velocity y, pressure, specific internal energy, cells in
+ * row-major order, x fastest); out must not overlap in.  The result equals
+ * one zg_smf_update step of a context configured with the same parameters.
+ * `dt` (device or pinned host memory, may be NULL) receives the step's dt.
+ * The work is enqueued on `stream` (a cudaStream_t; NULL = default stream)
+ * on CUDA device `device` and is asynchronous.
+ *
+ * Scratch: the CFL minimum, the dt and the coordinate tables live in one
+ * fixed array of device memory inside the library (512 KiB on every
+ * GPU that loads the library, held until the process exits).  nx and ny up
+ * to ZG_NOALLOC_MAX_AXIS are accepted; larger meshes return
+ * ZG_ERR_TOO_LARGE.  Every call resets the scratch it needs on `stream`
+ * before use.  The first call on a device looks up that array's address (and
+ * may load the library's device code there); make it before any stream
+ * capture on that device.  Calls that overlap on one device -- on different
+ * streams, or from different host threads -- share the one array and race:
+ * serialise them. */
+int zg_rect_step_noalloc(int device, int nx, int ny, double x_min, double x_max, double y_min,
+                         double y_max, const int bounds[4], const zg_smf_params *p, const double *const in[5],
+                         double *const out[5], double *dt, void *stream);
 
 #ifdef __cplusplus
 }

@@ -11,7 +11,8 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libzephyr_gpu.so"
 
 ZG_OK = 0
-_ERR_NAMES = {-1: "ZG_ERR_ARG", -2: "ZG_ERR_CUDA", -3: "ZG_ERR_STATE", -4: "ZG_ERR_ALLOC", -5: "ZG_ERR_NUMERIC"}
+_ERR_NAMES = {-1: "ZG_ERR_ARG", -2: "ZG_ERR_CUDA", -3: "ZG_ERR_STATE", -4: "ZG_ERR_ALLOC", -5: "ZG_ERR_NUMERIC",
+              -6: "ZG_ERR_TOO_LARGE"}
 
 
 class ZgError(RuntimeError):
@@ -80,6 +81,9 @@ SIGNATURES = {
     "zg_set_timing": (C.c_int, [_V, C.c_int]),
     "zg_kernel_times": (C.c_int, [_V, _P, C.POINTER(C.c_longlong)]),
     "zg_kernel_name": (C.c_char_p, [C.c_int]),
+    "zg_rect_step_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, _I, C.POINTER(SmfParams), C.POINTER(_V), C.POINTER(_V), _V,
+                                       _V]),
 }
 
 # enum zg_kernel_kind
