@@ -229,8 +229,9 @@ int zg_synchronize(zg_ctx *ctx);
  * synchronise the device between its own stream operations.
  *
  * in[5] and out[5] are device arrays of nx * ny doubles each (density,
- * velocity x, velocity y, pressure, specific internal energy, cells in
- * row-major order, x fastest); out must not overlap in.  The result equals
+ * velocity x, velocity y, pressure, specific internal energy; cell (i, j)
+ * at index i * ny + j, the order of the reference's base mesh,
+ * amr_cells_gen.cpp:128-281); out must not overlap in.  The result equals
  * one zg_smf_update step of a context configured with the same parameters.
  * `dt` (device or pinned host memory, may be NULL) receives the step's dt.
  * The work is enqueued on `stream` (a cudaStream_t; NULL = default stream)
