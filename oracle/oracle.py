@@ -58,6 +58,38 @@ def lib():
         L.zo_limiter.argtypes = [C.c_int, C.c_double, C.c_double]
         L.zo_limiter.restype = C.c_double
         L.zo_eos.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _P]
+        L.zo_mm_material.argtypes = [C.c_char_p, C.c_char_p, _P]
+        L.zo_mm_material.restype = C.c_int
+        L.zo_mm_create.restype = C.c_void_p
+        L.zo_mm_create.argtypes = [C.c_void_p, C.c_int, _P, C.c_double, C.c_int, C.c_int]
+        for name in ("zo_mm_free",):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.zo_mm_set_max_dt.argtypes = [C.c_void_p, C.c_double]
+        L.zo_mm_set_threads.argtypes = [C.c_void_p, C.c_int]
+        L.zo_mm_make_states.argtypes = [C.c_void_p, _P, _P, _P, _P, _P]
+        L.zo_mm_set_states.argtypes = [C.c_void_p, _P]
+        L.zo_mm_get_states.argtypes = [C.c_void_p, _P]
+        L.zo_mm_step.argtypes = [C.c_void_p]
+        L.zo_mm_step.restype = C.c_double
+        L.zo_mm_steps.argtypes = [C.c_void_p, C.c_int, _P]
+        L.zo_mm_steps.restype = C.c_double
+        L.zo_mm_compute_dt.argtypes = [C.c_void_p]
+        L.zo_mm_compute_dt.restype = C.c_double
+        L.zo_mm_bad.argtypes = [C.c_void_p]
+        L.zo_mm_bad.restype = C.c_int
+        L.zo_mm_interface.argtypes = [C.c_void_p, _P, _P]
+        L.zo_mm_flags.argtypes = [C.c_void_p, _I]
+        L.zo_mm_state_from_q.argtypes = [C.c_void_p, _P, _P, _P]
+        L.zo_mm_sound_speed.argtypes = [C.c_void_p, _P]
+        L.zo_mm_sound_speed.restype = C.c_double
+        L.zo_mm_hllc.argtypes = [C.c_void_p, _P, _P, _P]
+        L.zo_mm_hllc.restype = C.c_int
+        L.zo_mm_crp_flux.argtypes = [C.c_void_p, _P, _P, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, _P]
+        L.zo_mm_crp_flux.restype = C.c_int
+        for name, nargs in (("zo_mm_face_fraction", 2), ("zo_mm_quad_find_section", 5),
+                            ("zo_mm_quad_volume_fraction", 5), ("zo_mm_average_flux", 3)):
+            getattr(L, name).argtypes = [C.c_double] * nargs
+            getattr(L, name).restype = C.c_double
         _lib = L
     return _lib
 
@@ -185,3 +217,117 @@ def eos(eos_kind, gamma, P0, e0, rho, x):
     out = np.empty(3)
     lib().zo_eos(eos_kind, gamma, P0, e0, rho, x, _dp(out))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Multi-material step (zoracle_mm.inc): restated MmFluid, first order.
+CRP_NONE, CRP_V3, CRP_V5, CRP_VS, CRP_PLIC = 0, 1, 2, 3, 4
+MM_NSTATE = 14  # density, vx, vy, P, e, T, beta[4], rhos[4]
+
+
+def mm_material(kind, name):
+    """(stiffened, gamma, P0, e0, Cv, T0, rho_ref) of IdealGas(name) /
+    StiffenedGas(name)."""
+    out = np.empty(7)
+    if lib().zo_mm_material(kind.encode(), name.encode(), _dp(out)) != 0:
+        raise ValueError(f"unknown material {kind}:{name}")
+    return out
+
+
+class MmSolver:
+    """Restated MmFluid (mm_fluid.cpp) on an oracle Mesh."""
+
+    def __init__(self, mesh, materials=(("stiffened", "Water"), ("ideal", "Air")), CFL=0.4, crp_mode=CRP_PLIC,
+                 threads=1):
+        self.mesh = mesh
+        self.nmat = len(materials)
+        mats = np.concatenate([mm_material(k, n) for k, n in materials])
+        self._mats = mats
+        self.h = lib().zo_mm_create(mesh.h, self.nmat, _dp(mats), CFL, crp_mode, threads)
+
+    def make_states(self, rho, vx, vy, p, beta):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, vx, vy, p)]
+        b = np.zeros((self.mesh.n, 4))
+        b[:, :np.asarray(beta).shape[1]] = beta
+        lib().zo_mm_make_states(self.h, *map(_dp, arrs), _dp(np.ascontiguousarray(b)))
+
+    def set_states(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float64).reshape(self.mesh.n, MM_NSTATE)
+        lib().zo_mm_set_states(self.h, _dp(s))
+
+    def states(self):
+        s = np.empty((self.mesh.n, MM_NSTATE))
+        lib().zo_mm_get_states(self.h, _dp(s))
+        return s
+
+    def set_max_dt(self, dt):
+        lib().zo_mm_set_max_dt(self.h, dt)
+
+    def set_threads(self, n):
+        lib().zo_mm_set_threads(self.h, n)
+
+    def step(self):
+        return lib().zo_mm_step(self.h)
+
+    def steps(self, n):
+        dts = np.empty(max(n, 1))
+        lib().zo_mm_steps(self.h, n, _dp(dts))
+        return dts[:n]
+
+    def compute_dt(self):
+        return lib().zo_mm_compute_dt(self.h)
+
+    def bad(self):
+        return bool(lib().zo_mm_bad(self.h))
+
+    def interface(self):
+        nrm = np.empty((self.mesh.n, self.nmat, 2))
+        off = np.empty((self.mesh.n, self.nmat))
+        lib().zo_mm_interface(self.h, _dp(nrm), _dp(off))
+        return nrm, off
+
+    def flags(self):
+        f = np.empty(self.mesh.n, np.int32)
+        lib().zo_mm_flags(self.h, _ip(f))
+        return f
+
+    def state_from_q(self, q, guess):
+        out = np.empty(MM_NSTATE)
+        lib().zo_mm_state_from_q(self.h, _dp(np.ascontiguousarray(q, float)),
+                                 _dp(np.ascontiguousarray(guess, float)), _dp(out))
+        return out
+
+    def sound_speed(self, s):
+        return lib().zo_mm_sound_speed(self.h, _dp(np.ascontiguousarray(s, float)))
+
+    def hllc(self, sl, sr):
+        out = np.empty(8)
+        lib().zo_mm_hllc(self.h, _dp(np.ascontiguousarray(sl, float)), _dp(np.ascontiguousarray(sr, float)), _dp(out))
+        return out
+
+    def crp_flux(self, sl, sr, hL, hR, iA, a_sig, dt):
+        out = np.empty(8)
+        lib().zo_mm_crp_flux(self.h, _dp(np.ascontiguousarray(sl, float)), _dp(np.ascontiguousarray(sr, float)),
+                             hL, hR, iA, a_sig, dt, _dp(out))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.zo_mm_free(self.h)
+            self.h = None
+
+
+def mm_face_fraction(a1, a2):
+    return lib().zo_mm_face_fraction(a1, a2)
+
+
+def mm_quad_find_section(alpha, nx, ny, A, B):
+    return lib().zo_mm_quad_find_section(alpha, nx, ny, A, B)
+
+
+def mm_quad_volume_fraction(p, nx, ny, A, B):
+    return lib().zo_mm_quad_volume_fraction(p, nx, ny, A, B)
+
+
+def mm_average_flux(alpha, cos, CFL):
+    return lib().zo_mm_average_flux(alpha, cos, CFL)

@@ -61,14 +61,17 @@ MESH_DIRS = ["zephyr/mesh", "zephyr/geom", "zephyr/math/cfd", "zephyr/math/solve
 MESH_FILES = ["zephyr/utils/mpi.cpp", "zephyr/utils/threads.cpp", "zephyr/utils/json.cpp",
               "zephyr/utils/stopwatch.cpp", "zephyr/utils/numpy.cpp", "zephyr/math/funcs.cpp",
               "zephyr/math/random.cpp", "zephyr/math/sle/tridiagonal.cpp", "zephyr/math/calc/integrals.cpp"]
-MESH_SKIP = {
-             "zephyr/math/solver/convection.cpp", "zephyr/math/solver/transfer.cpp",
-             "zephyr/math/solver/mm_fluid.cpp"}
+MESH_SKIP = {"zephyr/math/solver/convection.cpp", "zephyr/math/solver/transfer.cpp"}
 
 FLAGS = ["-std=c++20", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-w"]
 # The reference relies on <cstring> and <functional> arriving through Eigen
 # and Boost headers; the stand-ins do not include them.
 FORCE = ["-include", "cstring", "-include", "functional"]
+# sections.cpp calls unqualified abs() on doubles (quad_volume_fraction,
+# quad_find_section).  With the reference's real Eigen/Boost headers the C++
+# <math.h> overloads are in scope; with the stand-ins only the C int abs(int)
+# would be, truncating every normal component to 0.  Force the C++ <math.h>.
+UNIT_FORCE = {"sections.cpp": ["-include", "math.h"]}
 
 
 def reference_present() -> bool:
@@ -77,7 +80,8 @@ def reference_present() -> bool:
 
 def _compile(cxx, src, obj, inc, force, verbose, newest_shim):
     if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_shim):
-        cmd = [cxx, *FLAGS, *FORCE, "-x", "c++", *inc, "-c", str(src), "-o", str(obj)]
+        cmd = [cxx, *FLAGS, *FORCE, *UNIT_FORCE.get(src.name, []), "-x", "c++", *inc, "-c", str(src), "-o",
+               str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
@@ -128,8 +132,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     obj_dir.mkdir(parents=True, exist_ok=True)
     inc = ["-I", str(SHIM_COMMON), "-I", str(REF)]
     units = mesh_units()
-    srcs = [REF / u for u in units] + [HERE / "ref_mesh_driver.cpp"]
-    objs = [obj_dir / (u.replace("/", "_") + ".o") for u in units] + [obj_dir / "ref_mesh_driver.cpp.o"]
+    drivers = ["ref_mesh_driver.cpp", "ref_mm_driver.cpp"]
+    srcs = [REF / u for u in units] + [HERE / d for d in drivers]
+    objs = [obj_dir / (u.replace("/", "_") + ".o") for u in units] + [obj_dir / (d + ".o") for d in drivers]
     with ThreadPoolExecutor(jobs) as ex:
         list(ex.map(lambda so: _compile(cxx, so[0], so[1], inc, force, verbose, newest_shim), zip(srcs, objs)))
     _link(cxx, LIB_MESH, objs, force, verbose)

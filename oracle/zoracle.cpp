@@ -28,6 +28,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -852,6 +853,9 @@ struct Solver {
     }
 };
 
+// Multi-material step (MmFluid): namespace zo::mm.
+#include "zoracle_mm.inc"
+
 }  // namespace zo
 
 // ---------------------------------------------------------------------------
@@ -1018,5 +1022,113 @@ void zo_eos(int eos_kind, double gamma, double P0, double e0, double rho, double
     out[1] = eos.energy_rP(rho, x);
     out[2] = eos.sound_speed_rP(rho, x);
 }
+
+// ---- multi-material step (zo::mm) ----
+// Material presets: out = stiffened flag, gamma, P0, e0, Cv, T0, rho_ref.
+int zo_mm_material(const char *kind, const char *name, double *out) {
+    zo::mm::Mat m;
+    if (!zo::mm::named_material(kind, name, m)) return -1;
+    double v[7] = {double(m.stiffened), m.gamma, m.P0, m.e0, m.Cv, m.T0, m.rho_ref};
+    std::memcpy(out, v, sizeof(v));
+    return 0;
+}
+// nm materials, 7 parameters each as from zo_mm_material.
+void *zo_mm_create(void *mesh, int nm, const double *mats, double CFL, int crp_mode, int threads) {
+    auto *s = new zo::mm::MmSolver(*static_cast<zo::Mesh *>(mesh));
+    s->mx.nm = nm;
+    for (int i = 0; i < nm; ++i) {
+        const double *p = mats + 7 * i;
+        s->mx.mat[i] = {int(p[0]), p[1], p[2], p[3], p[4], p[5], p[6]};
+    }
+    s->CFL = std::max(0.0, std::min(CFL, 1.0));
+    s->crp = crp_mode;
+    s->threads = threads;
+    return s;
+}
+void zo_mm_free(void *p) { delete static_cast<zo::mm::MmSolver *>(p); }
+void zo_mm_set_max_dt(void *p, double dt) { static_cast<zo::mm::MmSolver *>(p)->max_dt = dt; }
+void zo_mm_set_threads(void *p, int n) { static_cast<zo::mm::MmSolver *>(p)->threads = n; }
+// States from (density, velocity, pressure, mass fractions) through the
+// mixture closure, as PState(density, velocity, pressure, Fractions(array),
+// mixture); beta holds 4 fractions per cell and is normalised first.
+void zo_mm_make_states(void *p, const double *rho, const double *vx, const double *vy, const double *P,
+                       const double *beta) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    for (int i = 0; i < s->m.n_cells; ++i) {
+        zo::mm::Frac b;
+        for (int k = 0; k < 4; ++k) b.f[k] = beta[4 * (size_t)i + k];
+        zo::mm::normalize(b);
+        s->z[i] = zo::mm::state_of_rvp(s->mx, rho[i], {vx[i], vy[i], 0.0}, P[i], b);
+    }
+}
+void zo_mm_set_states(void *p, const double *st) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    for (int i = 0; i < s->m.n_cells; ++i) s->z[i] = zo::mm::unpack(st + 14 * (size_t)i);
+}
+void zo_mm_get_states(void *p, double *st) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    for (int i = 0; i < s->m.n_cells; ++i) zo::mm::pack(s->z[i], st + 14 * (size_t)i);
+}
+double zo_mm_step(void *p) { return static_cast<zo::mm::MmSolver *>(p)->step(); }
+double zo_mm_steps(void *p, int n, double *dts) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    for (int k = 0; k < n; ++k) {
+        double d = s->step();
+        if (dts) dts[k] = d;
+    }
+    return s->dt;
+}
+double zo_mm_compute_dt(void *p) { return static_cast<zo::mm::MmSolver *>(p)->compute_dt(); }
+int zo_mm_bad(void *p) { return static_cast<zo::mm::MmSolver *>(p)->bad ? 1 : 0; }
+void zo_mm_interface(void *p, double *nrm, double *off) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    int nm = s->mx.nm;
+    s->nrm.assign((size_t)s->m.n_cells * nm, zo::V3{0.0, 0.0, 0.0});
+    s->off.assign((size_t)s->m.n_cells * nm, 0.0);
+    for (int ic = 0; ic < s->m.n_cells; ++ic) s->recover(ic);
+    for (size_t k = 0; k < s->nrm.size(); ++k) {
+        nrm[2 * k] = s->nrm[k].x;
+        nrm[2 * k + 1] = s->nrm[k].y;
+        off[k] = s->off[k];
+    }
+}
+void zo_mm_flags(void *p, int *flags) { static_cast<zo::mm::MmSolver *>(p)->set_flags(flags); }
+void zo_mm_state_from_q(void *p, const double *q, const double *guess, double *out) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    zo::mm::QV Q;
+    for (int k = 0; k < zo::mm::NQ; ++k) Q.a[k] = q[k];
+    zo::mm::pack(zo::mm::state_of_q(s->mx, Q, guess[0], guess[1], guess + 2), out);
+}
+double zo_mm_sound_speed(void *p, const double *st) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    zo::mm::MState z = zo::mm::unpack(st);
+    zo::mm::Opts o;
+    o.T0 = z.T;
+    o.rhos = z.rhos;
+    return zo::mm::sound_speed_rP(s->mx, z.rho, z.P, z.beta, o);
+}
+int zo_mm_hllc(void *p, const double *sl, const double *sr, double *out) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    bool bad = false;
+    zo::mm::QV f = zo::mm::hllc(s->mx, zo::mm::unpack(sl), zo::mm::unpack(sr), bad);
+    std::memcpy(out, f.a, sizeof(f.a));
+    return bad ? 1 : 0;
+}
+int zo_mm_crp_flux(void *p, const double *sl, const double *sr, double hL, double hR, int iA, double a_sig,
+                   double dt, double *out) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    bool bad = false;
+    zo::mm::QV f = zo::mm::crp_flux(s->mx, zo::mm::unpack(sl), zo::mm::unpack(sr), hL, hR, iA, a_sig, dt, bad);
+    std::memcpy(out, f.a, sizeof(f.a));
+    return bad ? 1 : 0;
+}
+double zo_mm_face_fraction(double a1, double a2) { return zo::mm::face_fraction(a1, a2); }
+double zo_mm_quad_find_section(double alpha, double nx, double ny, double A, double B) {
+    return zo::mm::quad_find_section(alpha, {nx, ny, 0.0}, A, B);
+}
+double zo_mm_quad_volume_fraction(double p, double nx, double ny, double A, double B) {
+    return zo::mm::quad_volume_fraction(p, {nx, ny, 0.0}, A, B);
+}
+double zo_mm_average_flux(double alpha, double cos, double CFL) { return zo::mm::average_flux(alpha, cos, CFL); }
 
 }  // extern "C"

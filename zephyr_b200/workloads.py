@@ -81,3 +81,60 @@ def fourier_smooth(n: int = 2048) -> Workload:
     p = 1.0 + 0.1 * _fourier(4, cx, cy)
     e = p / ((eos.gamma - 1.0) * rho)
     return Workload("fourier_smooth", gen, eos, (rho, u, v, p, e))
+
+
+@dataclass
+class MmWorkload:
+    name: str
+    nx: int
+    ny: int
+    box: tuple        # x_min, x_max, y_min, y_max
+    bounds: tuple     # left, right, bottom, top (zephyr Boundary codes)
+    materials: tuple  # (kind, name) per material, e.g. ("stiffened", "Water")
+    rho: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    p: np.ndarray
+    beta: np.ndarray  # mass fractions, (n_cells, 4)
+
+
+def shock_water_column(n: int = 1024, sub: int = 8) -> MmWorkload:
+    """Two-material shock / water-column interaction on [0, 0.1]^2 m.
+
+    Material 0 is water (StiffenedGas "Water": gamma 4.4, P0 6e8 Pa), material
+    1 air (IdealGas "Air": gamma 1.4).  A water column of radius 0.01 m sits at
+    the centre at rest in air (rho 1.2 kg/m^3, p 1e5 Pa); a planar shock in the
+    air with post-shock pressure 1e6 Pa (Rankine-Hugoniot state) starts at
+    x = 0.005 m and moves in +x.  Left/right boundaries ZOE, bottom/top WALL.
+    Cells cut by the column get the water volume fraction alpha from sub x sub
+    sample points, density alpha rho_w + (1 - alpha) rho_a and the matching
+    mass fractions; energy, temperature and true densities then come from the
+    mixture closure when the states are loaded."""
+    box = (0.0, 0.1, 0.0, 0.1)
+    h = (box[1] - box[0]) / n
+    xc = box[0] + (np.arange(n) + 0.5) * h
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")  # cell ic = i * n + j
+    x, y = xc[i].ravel(), xc[j].ravel()
+    # water volume fraction by sub-sampling
+    s = (np.arange(sub) + 0.5) / sub - 0.5
+    inside = np.zeros(n * n)
+    for a in s:
+        for b in s:
+            inside += ((x + a * h - 0.05) ** 2 + (y + b * h - 0.05) ** 2) < 0.01 ** 2
+    alpha = inside / (sub * sub)
+    g, p1, rho1, p2 = 1.4, 1.0e5, 1.2, 1.0e6
+    rho2 = rho1 * ((g + 1) * p2 + (g - 1) * p1) / ((g - 1) * p2 + (g + 1) * p1)
+    u2 = (p2 - p1) / np.sqrt((p2 - p1) / (1 / rho1 - 1 / rho2))
+    shocked = x < 0.005
+    rho_a = np.where(shocked, rho2, rho1)
+    rho_w = 1000.0
+    rho = alpha * rho_w + (1 - alpha) * rho_a
+    beta = np.zeros((n * n, 4))
+    beta[:, 0] = alpha * rho_w / rho
+    beta[:, 1] = 1.0 - beta[:, 0]
+    beta[alpha >= 1.0, :2] = (1.0, 0.0)
+    beta[alpha <= 0.0, :2] = (0.0, 1.0)
+    vx = np.where(shocked & (alpha <= 0.0), u2, 0.0)
+    p = np.where(shocked & (alpha <= 0.0), p2, p1)
+    return MmWorkload("shock_water_column", n, n, box, (2, 2, 1, 1), (("stiffened", "Water"), ("ideal", "Air")),
+                      rho, vx, np.zeros(n * n), p, beta)
