@@ -148,6 +148,89 @@ def make_amr(name, n, acc, limiter, bounds, max_level, steps, adapt_rounds):
                                              "neib", "nx", "ny", "fx", "fy", "area")})
 
 
+MM_MATERIALS = "stiffened:Water,ideal:Air"
+
+
+def make_mm(name, n, crp_mode, steps):
+    """The reference's MmFluid (first order, CFL 0.4) on the shock / water
+    column problem at n x n: initial states through the reference's mixture
+    closure, the interface reconstruction of the first step, `steps` steps,
+    and the refinement flags at the end."""
+    from oracle import ref_mm as RM
+    from zephyr_b200.workloads import shock_water_column
+    w = shock_water_column(n)
+    r = RM.RefMmFluid(n, n, box=w.box, bounds=w.bounds, materials=MM_MATERIALS, CFL=0.4, accuracy=1,
+                      crp_mode=crp_mode)
+    r.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
+    init = r.states()
+    nrm, off = r.interface()
+    dts = np.array([r.step() for _ in range(steps)])
+    np.savez_compressed(OUT / f"{name}.npz", n=n, box=np.array(w.box), bounds=np.array(w.bounds), crp_mode=crp_mode,
+                        CFL=0.4, steps=steps, inputs=np.stack([w.rho, w.vx, w.vy, w.p]), beta=w.beta, init=init,
+                        normals=nrm, offsets=off, dts=dts, final=r.states(), flags=r.flags())
+
+
+def make_mm_pointwise():
+    """Mixture closure, sound speed, mixture HLLC and CRP fluxes of the
+    reference on states taken from a running shock / water-column problem,
+    and the PLIC helpers on a grid of arguments."""
+    from oracle import ref_mm as RM
+    from zephyr_b200.workloads import shock_water_column
+    n = 48
+    w = shock_water_column(n)
+    r = RM.RefMmFluid(n, n, box=w.box, bounds=w.bounds, materials=MM_MATERIALS, CFL=0.4, accuracy=1, crp_mode=4)
+    r.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
+    for _ in range(70):
+        dt = r.step()
+    s = r.states()
+    beta = s[:, 6:10]
+    mixed = np.where(((beta > 0).sum(axis=1) > 1))[0]
+    # pairs (cell, right neighbour) touching a mixed cell: the +x face, local frame = global
+    pairs = [(i, i + n) for i in range(n * (n - 1)) if i in set(mixed) or (i + n) in set(mixed)]
+    pairs = pairs[:96]
+    h = 0.1 / n
+    sl = np.array([s[a] for a, _ in pairs])
+    sr = np.array([s[b] for _, b in pairs])
+    hllc = np.array([r.hllc(a, b) for a, b in zip(sl, sr)])
+    crp, crp_args = [], []
+    for a, b in zip(sl, sr):
+        # master material: the larger volume fraction on the upwind side (mm_fluid.cpp:201-226)
+        up = a if 0.5 * (a[1] + b[1]) > 0.0 else b
+        al = [min(max(up[6 + k] * up[0] / up[10 + k], 0.0), 1.0) if up[6 + k] > 0 and not np.isnan(up[10 + k]) else 0.0
+              for k in range(2)]
+        iA = int(np.argmax(al))
+        aL = min(max(a[6 + iA] * a[0] / a[10 + iA], 0.0), 1.0) if not np.isnan(a[10 + iA]) else 0.0
+        aR = min(max(b[6 + iA] * b[0] / b[10 + iA], 0.0), 1.0) if not np.isnan(b[10 + iA]) else 0.0
+        a_sig = 0.5 * (aL + aR)
+        crp_args.append((h, h, iA, a_sig, dt))
+        crp.append(r.crp_flux(a, b, h, h, iA, a_sig, dt))
+    sound = np.array([r.sound_speed(x) for x in s[mixed]])
+    # closure from conservative states (models.cpp:190-204): q of each mixed cell, guesses from its state
+    q = np.zeros((len(mixed), 8))
+    z = s[mixed]
+    q[:, 0] = z[:, 0]
+    q[:, 1] = z[:, 0] * z[:, 1]
+    q[:, 2] = z[:, 0] * z[:, 2]
+    q[:, 3] = z[:, 0] * (z[:, 4] + 0.5 * (z[:, 1] ** 2 + z[:, 2] ** 2))
+    q[:, 4:8] = z[:, 0:1] * z[:, 6:10]
+    q *= 1.0 + 1.0e-3 * np.sin(np.arange(q.size).reshape(q.shape))  # perturbed, as after an update
+    guess = np.concatenate([z[:, 3:4], z[:, 5:6], z[:, 10:14]], axis=1)
+    closure = np.array([r.state_from_q(a, g) for a, g in zip(q, guess)])
+    al = np.array([0.0, 1e-9, 0.03, 0.2, 0.5, 0.7, 0.97, 1.0 - 1e-9, 1.0])
+    ff = np.array([[RM.face_fraction(a, b) for b in al] for a in al])
+    cosv = np.array([-1.0, -0.8, -0.3, 0.0, 0.25, 0.6, 0.99, 1.0])
+    cflv = np.array([0.0, 0.05, 0.3, 0.9])
+    avg = np.array([[[RM.average_flux(a, c, k) for k in cflv] for c in cosv] for a in al])
+    nv = np.array([[0.6, 0.8], [1.0, 0.0], [-0.28, 0.96], [0.0, -1.0], [0.70710678, -0.70710678]])
+    qfs = np.array([[RM.quad_find_section(a, x, y, 1.0, 0.5) for a in al] for x, y in nv])
+    pv = np.linspace(-0.8, 0.8, 17)
+    qvf = np.array([[RM.quad_volume_fraction(p, x, y, 1.0, 0.5) for p in pv] for x, y in nv])
+    np.savez_compressed(OUT / "mm_pointwise.npz", sl=sl, sr=sr, hllc=hllc, crp=np.array(crp),
+                        crp_args=np.array(crp_args), sound_states=s[mixed], sound=sound, q=q, guess=guess,
+                        closure=closure, alphas=al, face_fraction=ff, cos=cosv, cfl=cflv, average_flux=avg,
+                        normals=nv, quad_find_section=qfs, p=pv, quad_volume_fraction=qvf)
+
+
 def main():
     for name, spec in CASES.items():
         make_case(name, spec)
@@ -159,7 +242,18 @@ def main():
     make_amr("amr_blast_16_vanalbada", 16, 2, "van Albada", (2, 2, 2, 2), 2, 20, 4)
     make_amr("amr_blast_12_mc_3levels", 12, 2, "MC", (1, 1, 1, 1), 3, 10, 5)
     print("wrote amr cases")
+    make_mm("mm_shock_column_32_plic", 32, 4, 200)
+    make_mm("mm_shock_column_24_hllc", 24, 0, 120)
+    make_mm("mm_shock_column_24_vs", 24, 3, 120)
+    make_mm_pointwise()
+    print("wrote multi-material cases")
 
 
 if __name__ == "__main__":
-    main()
+    if "--mm" in sys.argv:
+        make_mm("mm_shock_column_32_plic", 32, 4, 200)
+        make_mm("mm_shock_column_24_hllc", 24, 0, 120)
+        make_mm("mm_shock_column_24_vs", 24, 3, 120)
+        make_mm_pointwise()
+    else:
+        main()
