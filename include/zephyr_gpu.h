@@ -204,6 +204,9 @@ enum zg_kernel_kind {
     ZG_K_HEUN_A,      /* Heun first stage */
     ZG_K_HEUN_B,      /* Heun second stage */
     ZG_K_FLAGS,       /* refinement flags */
+    ZG_K_MM_DT,       /* multi-material CFL minimum (MmFluid::compute_dt) */
+    ZG_K_MM_RECOVER,  /* PLIC reconstruction (MmFluid::interface_recovery) */
+    ZG_K_MM_FLUX,     /* multi-material first-order step (MmFluid::fluxes) */
     ZG_K_COUNT
 };
 
@@ -217,6 +220,86 @@ const char *zg_kernel_name(int kind);
 
 /* Wait for the context's stream. */
 int zg_synchronize(zg_ctx *ctx);
+
+/* ------------------------------------------------------------------------
+ * Multi-material step: MmFluid (math/solver/mm_fluid.h:45-163), materials
+ * in pressure and temperature equilibrium (MixturePT,
+ * phys/matter/mixture_pt.h), first order, on a mesh from zg_mesh_rectangle.
+ * The kernels are compiled for mixtures of two materials.
+ * ------------------------------------------------------------------------ */
+
+/* A material: IdealGas (kind ZG_EOS_IDEAL; P0, e0, T0 unused) or
+ * StiffenedGas (ZG_EOS_STIFFENED), phys/matter/eos/ideal_gas.h,
+ * stiffened_gas.h.  rho_ref is the reference density the mixture closure
+ * starts from when no guess is given (Eos::density()). */
+typedef struct zg_material {
+    int kind;
+    double gamma, P0, e0, Cv, T0, rho_ref;
+} zg_material;
+
+/* The named materials of IdealGas(name) (ideal_gas.cpp:14-24: "Air", "SF6")
+ * and StiffenedGas(name) (stiffened_gas.cpp:13-86: "Air", "SF6", "Water",
+ * "Water2", "Copper"/"Cu", "Lead"/"Pb", "Gas", "HeavyGas", "Liquid",
+ * "Solid"), with the unit literals of phys/literals.h evaluated as the
+ * reference evaluates them.  Returns ZG_ERR_ARG for an unknown name. */
+int zg_material_named(int kind, const char *name, zg_material *out);
+
+/* CRP mode: values of the reference's CrpMode (mm_fluid.h:31-37).  NONE
+ * uses the plain mixture HLLC flux on every face; V3, V5, VS choose the
+ * interface fraction by the heuristics of sections.cpp:50-84; PLIC
+ * reconstructs the interface (the default). */
+enum zg_crp_mode { ZG_CRP_NONE = 0, ZG_CRP_V3 = 1, ZG_CRP_V5 = 2, ZG_CRP_VS = 3, ZG_CRP_PLIC = 4 };
+
+/* MmFluid(MixturePT) and its setters (mm_fluid.h:58-100). */
+typedef struct zg_mmf_params {
+    int n_materials;          /* 2 */
+    zg_material materials[4]; /* MixturePT{...}, in order */
+    int crp_mode;             /* zg_crp_mode; set_crp_mode / set_method(CRP) */
+    int accuracy;             /* 1 (set_accuracy) */
+    double CFL;               /* clamped to [0, 1] (set_CFL) */
+    double max_dt;            /* set_max_dt */
+} zg_mmf_params;
+
+/* MmFluid's constructor defaults (mm_fluid.cpp:16-26): CRP with PLIC,
+ * CFL 0.7, first order, no dt cap; no materials. */
+void zg_mmf_default_params(zg_mmf_params *p);
+
+/* Configure the multi-material solver on the context's rectangle mesh;
+ * replaces MmFluid(mixture), its setters and add_types (mm_fluid.cpp:28-40).
+ * The first call allocates the fields; later calls keep the data. */
+int zg_mmf_configure(zg_ctx *ctx, const zg_mmf_params *p);
+
+/* Cell states as 14 doubles per cell: density, velocity x, velocity y,
+ * pressure, specific internal energy, temperature, mass fractions [4], true
+ * densities [4] (the fields of mmf::PState, math/cfd/models.h:167-180;
+ * slots past n_materials hold fraction 0).  Host arrays. */
+int zg_mmf_state_upload(zg_ctx *ctx, const double *cells);
+int zg_mmf_state_download(zg_ctx *ctx, double *cells);
+
+/* Initial states from density, velocity, pressure and mass fractions (4 per
+ * cell), through the mixture closure as PState(density, velocity, pressure,
+ * Fractions, mixture) does (models.cpp:180-188).  Host arrays. */
+int zg_mmf_make_states(zg_ctx *ctx, const double *rho, const double *vx, const double *vy, const double *p,
+                       const double *beta);
+
+/* One time step; replaces MmFluid::update (mm_fluid.cpp:112-137).
+ * Asynchronous; a state the reference would reject (negative density, a NaN
+ * flux, the composite Riemann case it throws on) is reported as
+ * ZG_ERR_NUMERIC by the next zg_mmf_dt or zg_mmf_state_download. */
+int zg_mmf_update(zg_ctx *ctx);
+int zg_mmf_update_n(zg_ctx *ctx, int n_steps);
+
+/* dt of the last step (MmFluid::dt()); synchronises the stream. */
+int zg_mmf_dt(zg_ctx *ctx, double *dt);
+
+/* Refinement flags of MmFluid::set_flags (mm_fluid.cpp:836-885). */
+int zg_mmf_set_flags(zg_ctx *ctx, int *flags);
+
+/* The PLIC reconstruction of the current state (interface_recovery,
+ * mm_fluid.cpp:484-519): per cell and material the unit normal (x, y) and
+ * the plane offset.  normals: 2 * n_materials doubles per cell; offsets:
+ * n_materials per cell. */
+int zg_mmf_interface(zg_ctx *ctx, double *normals, double *offsets);
 
 /* Largest nx and ny that zg_rect_step_noalloc accepts. */
 #define ZG_NOALLOC_MAX_AXIS 8192

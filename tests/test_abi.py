@@ -53,7 +53,7 @@ def test_limiter_names_follow_reference_parsing(name, kind):
 
 def test_kernel_names():
     lib = Z.load()
-    assert [lib.zg_kernel_name(k).decode() for k in range(8)] == _lib.KERNEL_KINDS
+    assert [lib.zg_kernel_name(k).decode() for k in range(len(_lib.KERNEL_KINDS))] == _lib.KERNEL_KINDS
 
 
 def test_null_arguments_are_rejected():
@@ -90,3 +90,16 @@ def test_unimplemented_flux_is_refused():
         s.set_method(Z.Fluxes.GODUNOV)
     with pytest.raises(Z.ZgError):
         s.set_limiter("no-such-limiter")
+
+
+@pytest.mark.parametrize("kind,name", [(1, "Water"), (0, "Air"), (1, "Air")])
+def test_named_materials_match_the_oracle(kind, name):
+    """zg_material_named (host only) against the oracle's restatement of
+    IdealGas(name) / StiffenedGas(name) with the reference's literals."""
+    from oracle import oracle as O
+    m = _lib.Material()
+    assert Z.load().zg_material_named(kind, name.encode(), C.byref(m)) == 0
+    want = O.mm_material("stiffened" if kind == 1 else "ideal", name)
+    got = [float(kind), m.gamma, m.P0, m.e0, m.Cv, m.T0, m.rho_ref]
+    assert got == list(want)
+    assert Z.load().zg_material_named(kind, b"Unobtainium", C.byref(m)) != 0

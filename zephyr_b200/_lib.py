@@ -56,6 +56,18 @@ _I = C.POINTER(C.c_int)
 _V = C.c_void_p
 
 # name -> (restype, argtypes); every symbol include/zephyr_gpu.h declares.
+class Material(C.Structure):
+    """zg_material"""
+    _fields_ = [("kind", C.c_int), ("gamma", C.c_double), ("P0", C.c_double), ("e0", C.c_double),
+                ("Cv", C.c_double), ("T0", C.c_double), ("rho_ref", C.c_double)]
+
+
+class MmfParams(C.Structure):
+    """zg_mmf_params"""
+    _fields_ = [("n_materials", C.c_int), ("materials", Material * 4), ("crp_mode", C.c_int),
+                ("accuracy", C.c_int), ("CFL", C.c_double), ("max_dt", C.c_double)]
+
+
 SIGNATURES = {
     "zg_smf_default_params": (None, [C.POINTER(SmfParams)]),
     "zg_limiter_from_name": (C.c_int, [C.c_char_p]),
@@ -81,13 +93,25 @@ SIGNATURES = {
     "zg_set_timing": (C.c_int, [_V, C.c_int]),
     "zg_kernel_times": (C.c_int, [_V, _P, C.POINTER(C.c_longlong)]),
     "zg_kernel_name": (C.c_char_p, [C.c_int]),
+    "zg_material_named": (C.c_int, [C.c_int, C.c_char_p, C.POINTER(Material)]),
+    "zg_mmf_default_params": (None, [C.POINTER(MmfParams)]),
+    "zg_mmf_configure": (C.c_int, [_V, C.POINTER(MmfParams)]),
+    "zg_mmf_state_upload": (C.c_int, [_V, _P]),
+    "zg_mmf_state_download": (C.c_int, [_V, _P]),
+    "zg_mmf_make_states": (C.c_int, [_V, _P, _P, _P, _P, _P]),
+    "zg_mmf_update": (C.c_int, [_V]),
+    "zg_mmf_update_n": (C.c_int, [_V, C.c_int]),
+    "zg_mmf_dt": (C.c_int, [_V, _P]),
+    "zg_mmf_set_flags": (C.c_int, [_V, _I]),
+    "zg_mmf_interface": (C.c_int, [_V, _P, _P]),
     "zg_rect_step_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                        C.c_double, _I, C.POINTER(SmfParams), C.POINTER(_V), C.POINTER(_V), _V,
                                        _V]),
 }
 
 # enum zg_kernel_kind
-KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags"]
+KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags", "mm_dt", "mm_recover",
+                "mm_flux"]
 
 _lib = None
 

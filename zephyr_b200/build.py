@@ -28,6 +28,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "zg_api.cu": [],
     "smf_parity.cu": ["-fmad=false"],
+    "mmf_parity.cu": ["-fmad=false"],
     # allocation-free first-order step; its device-built coordinate tables
     # must match the host-built ones, hence no fused multiply-adds
     "zg_noalloc.cu": ["-fmad=false"],

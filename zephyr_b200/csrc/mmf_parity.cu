@@ -1,0 +1,332 @@
+// mmf_parity.cu -- kernels of zephyr's multi-material first-order step
+// MmFluid::update (math/solver/mm_fluid.cpp:112-171, DirSplit::NONE,
+// accuracy 1) on a rectangle: CFL time step, PLIC interface reconstruction,
+// and the face loop with mixture HLLC / composite Riemann fluxes and the
+// PT-equilibrium closure of every updated cell.  One thread per cell; each
+// cell evaluates its own faces in the reference's order (gather form).
+// Compiled with -fmad=false: results agree bit for bit with the reference.
+#include <cuda_runtime.h>
+
+#include "mmf_types.h"
+#include "smf_struct.cuh"
+
+namespace zg {
+namespace mmf {
+
+constexpr int BLOCK = 128;
+constexpr int NM = NMAT;
+
+__device__ __forceinline__ MSt<NM> load(const MmField &f, int ic) {
+    MSt<NM> z;
+    z.rho = f.rho[ic];
+    z.vx = f.vx[ic];
+    z.vy = f.vy[ic];
+    z.P = f.P[ic];
+    z.e = f.e[ic];
+    z.T = f.T[ic];
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        z.b.f[i] = f.b[i][ic];
+        z.r[i] = f.r[i][ic];
+    }
+    return z;
+}
+__device__ __forceinline__ void store(const MmField &f, int ic, const MSt<NM> &z) {
+    f.rho[ic] = z.rho;
+    f.vx[ic] = z.vx;
+    f.vy[ic] = z.vy;
+    f.P[ic] = z.P;
+    f.e[ic] = z.e;
+    f.T[ic] = z.T;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        f.b[i][ic] = z.b.f[i];
+        f.r[i][ic] = z.r[i];
+    }
+}
+
+// alpha of material i (models.cpp:234-237) for a runtime index
+__device__ __forceinline__ double alpha_rt(const MSt<NM> &z, int idx) {
+    double r = z.r[0], b = z.b.f[0];
+#pragma unroll
+    for (int i = 1; i < NM; ++i)
+        if (i == idx) {
+            r = z.r[i];
+            b = z.b.f[i];
+        }
+    return isnan(r) ? 0.0 : fmax_std(0.0, fmin_std(b * z.rho / r, 1.0));
+}
+
+// ---------------------------------------------------------------------------
+// CFL time step (mm_fluid.cpp:173-196): per cell min over faces of
+// V / (S (|v.n| + c)), c the mixture sound speed; the last block to finish
+// writes dt = min(CFL * min, max_dt) and resets the accumulator.
+__global__ void __launch_bounds__(BLOCK) k_dt(MmArgs a) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;
+    if (ic < a.mesh.n) {
+        StructAcc c(a.mesh, ic);
+        MSt<NM> z = load(a.z, ic);
+        double cs = sound_speed_rP(a.mix, z.rho, z.P, z.b, z.T, z.r);
+        double d = 1.7976931348623157e308;  // std::numeric_limits<double>::max()
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            FaceG g = c.face(s);
+            double vn = z.vx * g.nx + z.vy * g.ny + 0.0 * 0.0;
+            double lambda = fabs(vn) + cs;
+            d = fmin_std(d, c.vol() / (g.area * lambda));
+        }
+        best = dbits(d);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+        best = t < best ? t : best;
+    }
+    __shared__ unsigned long long sm[BLOCK / 32];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        best = threadIdx.x < BLOCK / 32 ? sm[threadIdx.x] : 0x7FEFFFFFFFFFFFFFull;
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+            best = t < best ? t : best;
+        }
+        if (threadIdx.x == 0) {
+            atomicMin(a.dmin_bits, best);
+            __threadfence();
+            unsigned int ticket = atomicAdd(a.dt_ticket, 1u);
+            if (ticket == gridDim.x - 1) {
+                unsigned long long bits = atomicMin(a.dmin_bits, 0x7FEFFFFFFFFFFFFFull);
+                double dmin = __longlong_as_double((long long)bits);
+                *a.dt_out = fmin_std(a.CFL * dmin, a.max_dt);
+                *a.dmin_bits = 0x7FEFFFFFFFFFFFFFull;
+                *a.dt_ticket = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PLIC reconstruction (interface_recovery, mm_fluid.cpp:484-519): for every
+// material present in a mixed cell, the normal -sum face_fraction(a_c, a_n) S
+// over the faces, normalised, and the plane offset quad_find_section.
+__global__ void __launch_bounds__(BLOCK) k_recover(MmArgs a) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    StructAcc c(a.mesh, ic);
+    MSt<NM> z = load(a.z, ic);
+    double nx[NM], ny[NM], ac[NM];
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        nx[i] = 0.0;
+        ny[i] = 0.0;
+        ac[i] = z.b.f[i] > 0.0 ? z.b.f[i] * z.rho / z.r[i] : 0.0;  // volume_fractions()
+    }
+    bool pure = frac_index(z.b) >= 0;
+    if (!pure) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            FaceG g = c.face(s);
+            double Sx = g.area * g.nx, Sy = g.area * g.ny;
+            MSt<NM> zn = load(a.z, g.nb);
+#pragma unroll
+            for (int i = 0; i < NM; ++i) {
+                if (ac[i] > 0.0) {
+                    double a_n = isnan(zn.r[i]) ? 0.0 : fmax_std(0.0, fmin_std(zn.b.f[i] * zn.rho / zn.r[i], 1.0));
+                    double ff = face_fraction(ac[i], a_n);
+                    nx[i] = nx[i] - ff * Sx;
+                    ny[i] = ny[i] - ff * Sy;
+                }
+            }
+        }
+    }
+    double hx = sqrt(a.mesh.inc2x[c.i]), hy = sqrt(a.mesh.inc2y[c.j]);  // AmrCells::hx / hy
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        double off = 0.0;
+        if (!pure && ac[i] > 0.0) {
+            double sn = nx[i] * nx[i] + ny[i] * ny[i] + 0.0 * 0.0;
+            if (sn > 0.0) {
+                double r = sqrt(sn);
+                nx[i] = nx[i] / r;
+                ny[i] = ny[i] / r;
+            }
+            off = quad_find_section(ac[i], nx[i], ny[i], hx, hy);
+        }
+        a.nrm_x[i][ic] = pure ? 0.0 : nx[i];
+        a.nrm_y[i][ic] = pure ? 0.0 : ny[i];
+        a.off[i][ic] = off;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// master_component (mm_fluid.cpp:201-226)
+__device__ __forceinline__ int master_component(const MSt<NM> &zm, const MSt<NM> &zp) {
+    double vi = 0.5 * (zm.vx + zp.vx);
+    const MSt<NM> &w = vi > 0.0 ? zm : zp;
+    int master = 0;
+    double alpha_max = 0.0;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        if (w.b.f[i] > 0.0) {
+            double al = isnan(w.r[i]) ? 0.0 : fmax_std(0.0, fmin_std(w.b.f[i] * w.rho / w.r[i], 1.0));
+            if (al > alpha_max) {
+                alpha_max = al;
+                master = i;
+            }
+        }
+    }
+    return master;
+}
+
+__device__ __forceinline__ double normal_of(double *const arr[NM], int idx, int ic) {
+    double v = arr[0][ic];
+#pragma unroll
+    for (int i = 1; i < NM; ++i)
+        if (i == idx) v = arr[i][ic];
+    return v;
+}
+
+// The face flux of calc_flux (mm_fluid.cpp:347-371) with alpha_sigma
+// (229-261); states in the face frame.
+__device__ QVd<NM> calc_flux(const MmArgs &a, double dt, int ic, const FaceG &g, const MSt<NM> &zm,
+                             const MSt<NM> &zp, double hL, double hR, bool &bad) {
+    if (a.crp == CRP_NONE) return hllc(a.mix, zm, zp, bad);
+    int iL = frac_index(zm.b), iR = frac_index(zp.b);
+    if (iL >= 0 && iR >= 0) return hllc(a.mix, zm, zp, bad);
+    int iA = master_component(zm, zp);
+    double a_L = alpha_rt(zm, iA), a_R = alpha_rt(zp, iA);
+    double a_sig;
+    if (a.crp == CRP_V3) {
+        a_sig = face_fraction_v3(a_L, a_R);
+    } else if (a.crp == CRP_V5) {
+        a_sig = face_fraction_v5(a_L, a_R);
+    } else if (a.crp == CRP_VS) {
+        a_sig = face_fraction_s(a_L, a_R);
+    } else {
+        double vi = 0.5 * (zm.vx + zp.vx);
+        bool upwind = vi > 0.0;
+        double cfl = dt * fabs(vi) / (upwind ? hL : hR);
+        int owner = upwind ? ic : g.nb;
+        double nx = normal_of(a.nrm_x, iA, owner), ny = normal_of(a.nrm_y, iA, owner);
+        if (!upwind) {
+            nx = -nx;
+            ny = -ny;
+        }
+        double cs = g.nx * nx + g.ny * ny + 0.0 * 0.0;
+        a_sig = between(average_flux(upwind ? a_L : a_R, cs, cfl), a_L, a_R);
+    }
+    return crp_flux(a.mix, zm, zp, hL, hR, iA, a_sig, dt, bad);
+}
+
+// First-order face loop and update (fluxes, mm_fluid.cpp:373-437).
+__global__ void __launch_bounds__(BLOCK) k_flux1(MmArgs a) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    const double dt = *a.dt_out;
+    StructAcc c(a.mesh, ic);
+    const double V_c = c.vol();
+    MSt<NM> zc = load(a.z, ic);
+    QVd<NM> flux = qv_zero<NM>();
+    bool bad = false;
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = c.face(s);
+        MSt<NM> zn;
+        double V_n;
+        if (!is_boundary(g.flag)) {
+            zn = load(a.z, g.nb);
+            V_n = V_c;
+        } else {
+            zn = zc;
+            if (g.flag == BC_WALL) {  // boundary_value (mm_fluid.cpp:88-97)
+                double d = zc.vx * g.nx + zc.vy * g.ny + 0.0 * 0.0;
+                zn.vx = zc.vx - 2.0 * (d * g.nx);
+                zn.vy = zc.vy - 2.0 * (d * g.ny);
+            }
+            V_n = V_c;
+        }
+        // Rotate::to_local (rotate.cpp:7-41); axis normals are unit vectors
+        const double cs = g.nx, sn = g.ny;
+        MSt<NM> zm = zc, zp = zn;
+        zm.vx = cs * zc.vx + sn * zc.vy + 0.0 * 0.0;
+        zm.vy = -sn * zc.vx + cs * zc.vy + 0.0 * 0.0;
+        zp.vx = cs * zn.vx + sn * zn.vy + 0.0 * 0.0;
+        zp.vy = -sn * zn.vx + cs * zn.vy + 0.0 * 0.0;
+        const double S = g.area;
+        QVd<NM> lf = calc_flux(a, dt, ic, g, zm, zp, V_c / S, V_n / S, bad);
+        // Rotate::to_global of the momentum (rotate.cpp:43-77)
+        double mx = cs * lf.a[1] + -sn * lf.a[2] + 0.0 * 0.0;
+        double my = sn * lf.a[1] + cs * lf.a[2] + 0.0 * 0.0;
+        lf.a[1] = mx;
+        lf.a[2] = my;
+#pragma unroll
+        for (int k = 0; k < 4 + NM; ++k) flux.a[k] += lf.a[k] * S;
+    }
+    QVd<NM> q = q_of(zc);
+    double coef = dt / V_c;
+#pragma unroll
+    for (int k = 0; k < 4 + NM; ++k) q.a[k] -= coef * flux.a[k];
+    if (q.a[0] < 0.0) bad = true;  // the reference throws (mm_fluid.cpp:431-433)
+    MSt<NM> zn = state_of_q(a.mix, q, zc.P, zc.T, zc.r);
+    store(a.znext, ic, zn);
+    if (bad) atomicOr(a.err, 1);
+}
+
+// Refinement flags (MmFluid::set_flags, mm_fluid.cpp:836-885).
+__global__ void __launch_bounds__(BLOCK) k_flags(MmArgs a, int *flags) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    StructAcc c(a.mesh, ic);
+    Frac<NM> b;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) b.f[i] = a.z.b[i][ic];
+    int idx = frac_index(b);
+    if (idx < 0) {
+        flags[ic] = 1;
+        return;
+    }
+    bool need = false;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = c.face(s);
+        if (is_boundary(g.flag)) continue;
+        Frac<NM> bn;
+#pragma unroll
+        for (int i = 0; i < NM; ++i) bn.f[i] = a.z.b[i][g.nb];
+        if (frac_index(bn) != idx) need = true;
+    }
+    flags[ic] = need ? 1 : -1;
+}
+
+// Initial states from (density, velocity, pressure, mass fractions): the
+// PState(density, velocity, pressure, Fractions, mixture) constructor
+// (models.cpp:180-188); the fractions are normalised first, as the
+// Fractions constructor does.  beta holds 4 fractions per cell.
+__global__ void __launch_bounds__(BLOCK) k_make_states(MmArgs a, const double *rho, const double *vx,
+                                                       const double *vy, const double *P, const double *beta) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    Frac<NM> b;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) b.f[i] = beta[4 * (size_t)ic + i];
+    normalize(b);
+    store(a.z, ic, state_of_rvp(a.mix, rho[ic], vx[ic], vy[ic], P[ic], b));
+}
+
+static inline unsigned blocks(const MmArgs &a) { return (unsigned)((a.mesh.n + BLOCK - 1) / BLOCK); }
+
+void launch_dt(const MmArgs &a, void *stream) { k_dt<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_recover(const MmArgs &a, void *stream) { k_recover<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_flux1(const MmArgs &a, void *stream) { k_flux1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_flags(const MmArgs &a, int *flags, void *stream) {
+    k_flags<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, flags);
+}
+void launch_make_states(const MmArgs &a, const double *rho, const double *vx, const double *vy, const double *P,
+                        const double *beta, void *stream) {
+    k_make_states<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, rho, vx, vy, P, beta);
+}
+
+}  // namespace mmf
+}  // namespace zg

@@ -1,0 +1,44 @@
+// mmf_types.h -- arguments and launchers of the multi-material step
+// (MmFluid, first order) on a rectangle mesh.
+#pragma once
+
+#include "mmf_math.cuh"
+#include "smf_types.h"
+
+namespace zg {
+namespace mmf {
+
+constexpr int NMAT = 2;  // materials per mixture in the compiled kernels
+
+// Primitive mixture state of every cell, one array per field (structure of
+// arrays): density, velocity, pressure, specific internal energy,
+// temperature, mass fractions and true densities (the fields of
+// mmf::PState, math/cfd/models.h:167-180).
+struct MmField {
+    double *rho, *vx, *vy, *P, *e, *T;
+    double *b[NMAT];
+    double *r[NMAT];
+};
+
+struct MmArgs {
+    StructMesh mesh;
+    MixD<NMAT> mix;
+    int crp;
+    double CFL, max_dt;
+    MmField z, znext;
+    double *nrm_x[NMAT], *nrm_y[NMAT], *off[NMAT];  // interface reconstruction per material
+    unsigned long long *dmin_bits;
+    unsigned int *dt_ticket;
+    double *dt_out;
+    int *err;  // set to 1 where the reference would throw
+};
+
+void launch_dt(const MmArgs &a, void *stream);
+void launch_recover(const MmArgs &a, void *stream);
+void launch_flux1(const MmArgs &a, void *stream);
+void launch_flags(const MmArgs &a, int *flags, void *stream);
+void launch_make_states(const MmArgs &a, const double *rho, const double *vx, const double *vy, const double *P,
+                        const double *beta, void *stream);
+
+}  // namespace mmf
+}  // namespace zg

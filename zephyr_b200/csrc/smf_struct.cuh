@@ -37,6 +37,10 @@ struct StructAcc {
         i = ic / m.ny;
         j = ic - i * m.ny;
     }
+    __device__ StructAcc(const StructMesh &mesh, int ic_) : m(mesh), ic(ic_) {
+        i = ic / m.ny;
+        j = ic - i * m.ny;
+    }
     __device__ static int n(const SmfArgs &a) { return a.mesh.n; }
     __device__ double cx() const { return m.cx[i]; }
     __device__ double cy() const { return m.cy[j]; }

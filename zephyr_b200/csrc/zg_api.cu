@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/zephyr_gpu.h"
+#include "mmf_types.h"
 #include "smf_tiled.cuh"
 #include "smf_tiled_launch.h"
 #include "smf_types.h"
@@ -63,6 +64,15 @@ struct zg_ctx {
     float *mw[2][5] = {}, *mh[5] = {}, *mg[8] = {};
     int mcur = 0;
 
+    // multi-material solver (MmFluid)
+    bool mm_configured = false;
+    zg_mmf_params mpar{};
+    double *d_mm = nullptr;        // two states of 6 + 2 NMAT fields, then 3 NMAT interface fields
+    unsigned long long *d_mm_scalars = nullptr;  // CFL minimum @0, ticket @8, dt @16, error flag @24
+    int *d_mm_flags = nullptr;
+    mmf::MmField mz{}, mznext{};
+    double *mnx[mmf::NMAT] = {}, *mny[mmf::NMAT] = {}, *moff[mmf::NMAT] = {};
+
     // per-kernel timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -101,7 +111,18 @@ struct DeviceGuard {
     }
 };
 
+void free_mm(zg_ctx *c) {
+    cudaFree(c->d_mm);
+    cudaFree(c->d_mm_scalars);
+    cudaFree(c->d_mm_flags);
+    c->d_mm = nullptr;
+    c->d_mm_scalars = nullptr;
+    c->d_mm_flags = nullptr;
+    c->mm_configured = false;
+}
+
 void free_solver(zg_ctx *c) {
+    free_mm(c);
     cudaFree(c->d_mq);
     cudaFree(c->d_mf);
     c->d_mq = nullptr;
@@ -890,8 +911,373 @@ int zg_kernel_times(zg_ctx *c, double *ms, long long *launches) {
 
 const char *zg_kernel_name(int kind) {
     static const char *names[ZG_K_COUNT] = {"dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b",
-                                            "flags"};
+                                            "flags", "mm_dt", "mm_recover", "mm_flux"};
     return (kind >= 0 && kind < ZG_K_COUNT) ? names[kind] : "unknown";
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Multi-material step (MmFluid)
+
+namespace {
+
+// Unit literals of phys/literals.h: the value is double(x * factor) computed
+// in long double, x the literal as a long double.
+double lit(long double x, double factor) { return double(x * factor); }
+double lit_C(long double x) { return double(x + 273.15); }
+
+double ideal_ref_density(double gamma, double Cv, double P, double T) {
+    return 1.0 / (((gamma - 1.0) * Cv * T) / P);  // 1 / IdealGas::volume_PT(P, T)
+}
+
+mmf::MmArgs make_mm_args(const zg_ctx *c) {
+    mmf::MmArgs a{};
+    a.mesh = c->mesh;
+    for (int i = 0; i < mmf::NMAT; ++i) {
+        const zg_material &m = c->mpar.materials[i];
+        a.mix.mat[i] = {m.kind == ZG_EOS_STIFFENED ? 1 : 0, m.gamma, m.P0, m.e0, m.Cv, m.T0, m.rho_ref};
+        a.nrm_x[i] = c->mnx[i];
+        a.nrm_y[i] = c->mny[i];
+        a.off[i] = c->moff[i];
+    }
+    a.crp = c->mpar.crp_mode;
+    a.CFL = c->mpar.CFL;
+    a.max_dt = c->mpar.max_dt;
+    a.z = c->mz;
+    a.znext = c->mznext;
+    a.dmin_bits = c->d_mm_scalars;
+    a.dt_ticket = reinterpret_cast<unsigned int *>(c->d_mm_scalars + 1);
+    a.dt_out = reinterpret_cast<double *>(c->d_mm_scalars + 2);
+    a.err = reinterpret_cast<int *>(c->d_mm_scalars + 3);
+    return a;
+}
+
+int mm_ready(zg_ctx *c, const char *who) {
+    if (!c) return ZG_ERR_ARG;
+    if (!c->mm_configured) return fail(c, ZG_ERR_STATE, std::string(who) + ": zg_mmf_configure first");
+    return ZG_OK;
+}
+
+int mm_check_error(zg_ctx *c) {
+    int err = 0;
+    ZG_CUDA(c, cudaMemcpyAsync(&err, c->d_mm_scalars + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err) return fail(c, ZG_ERR_NUMERIC, "MmFluid: negative density, NaN flux or an unsupported composite "
+                                            "Riemann configuration (the reference throws here)");
+    return ZG_OK;
+}
+
+int enqueue_mm_step(zg_ctx *c) {
+    mmf::MmArgs a = make_mm_args(c);
+    void *st = (void *)c->stream;
+    timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(a, st); });
+    if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
+    timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux1(a, st); });
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    std::swap(c->mz, c->mznext);  // MmFluid::swap (mm_fluid.cpp:682-684)
+    return ZG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zg_material_named(int kind, const char *name, zg_material *out) {
+    if (!name || !out) return ZG_ERR_ARG;
+    std::string n(name);
+    zg_material m{};
+    if (kind == ZG_EOS_IDEAL) {  // ideal_gas.cpp:14-24
+        m.kind = ZG_EOS_IDEAL;
+        if (n == "Air") {
+            m.gamma = 1.4;
+            m.Cv = lit(718.0L, 1.0);
+        } else if (n == "SF6") {
+            m.gamma = 1.1074;
+            m.Cv = lit(567.0L, 1.0);
+        } else {
+            return ZG_ERR_ARG;
+        }
+        m.rho_ref = ideal_ref_density(m.gamma, m.Cv, lit(1.0L, 1.0e5), lit_C(0.0L));
+        *out = m;
+        return ZG_OK;
+    }
+    if (kind != ZG_EOS_STIFFENED) return ZG_ERR_ARG;
+    // stiffened_gas.cpp:13-86: defaults, then the named set
+    m.kind = ZG_EOS_STIFFENED;
+    m.P0 = 0.0;
+    m.e0 = 0.0;
+    m.Cv = 1.0;
+    m.T0 = 0.0;
+    double rho_0 = 1.0;
+    if (n == "Air") {
+        m.gamma = 1.4;
+        m.Cv = lit(718.0L, 1.0);
+        rho_0 = lit(1.25L, 1.0);
+    } else if (n == "SF6") {
+        m.gamma = 1.1074;
+        m.Cv = lit(567.0L, 1.0);
+        rho_0 = lit(6.17L, 1.0);
+    } else if (n == "Water") {
+        m.gamma = 4.4;
+        m.Cv = lit(4160.0L, 1.0);
+        m.P0 = lit(600.0L, 1.0e6);
+        m.e0 = 0.0;
+        m.T0 = 230.7;
+        rho_0 = lit(1.0L, 1.0e3);
+    } else if (n == "Water2") {
+        m.gamma = 3.0;
+        m.Cv = lit(4160.0L, 1.0);
+        m.P0 = lit(853.3L, 1.0e6);
+        m.e0 = -lit(1.148L, 1.0e6);
+        rho_0 = lit(1.0L, 1.0e3);
+    } else if (n == "Copper" || n == "Cu") {
+        m.gamma = 4.0;
+        m.Cv = lit(384.0L, 1.0);
+        m.P0 = 341.0;
+        m.e0 = 0.0;
+        rho_0 = lit(8.96L, 1.0e3);
+    } else if (n == "Lead" || n == "Pb") {
+        m.gamma = 3.77;
+        m.Cv = lit(121.0L, 1.0);
+        m.P0 = lit(11.8L, 1.0e9);
+        m.e0 = -lit(1.42L, 1.0e6);
+        m.T0 = -2832.57;
+        rho_0 = lit(11.35L, 1.0e3);
+    } else if (n == "Gas") {
+        m.gamma = 1.4;
+        m.Cv = 2.5;
+        rho_0 = 1.0;
+    } else if (n == "HeavyGas") {
+        m.gamma = 1.1;
+        m.Cv = 2.5;
+        rho_0 = 4.0;
+    } else if (n == "Liquid") {
+        m.gamma = 4.4;
+        m.Cv = 20.0;
+        m.P0 = 6.8e4;
+        rho_0 = 1000.0;
+    } else if (n == "Solid") {
+        m.gamma = 3.8;
+        m.Cv = 0.5;
+        m.P0 = 1.4e5;
+        m.e0 = -15.0;
+        m.T0 = -7.0;
+        rho_0 = 12500;
+    } else {
+        return ZG_ERR_ARG;
+    }
+    m.rho_ref = rho_0;
+    *out = m;
+    return ZG_OK;
+}
+
+void zg_mmf_default_params(zg_mmf_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->n_materials = 0;
+    p->crp_mode = ZG_CRP_PLIC;
+    p->accuracy = 1;
+    p->CFL = 0.7;
+    p->max_dt = 1.0e+300;
+}
+
+int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
+    if (!c || !p) return ZG_ERR_ARG;
+    if (!c->have_mesh || c->slots) return fail(c, ZG_ERR_STATE, "zg_mmf_configure: needs a zg_mesh_rectangle mesh");
+    if (p->n_materials != mmf::NMAT)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: the kernels are compiled for mixtures of two materials");
+    for (int i = 0; i < p->n_materials; ++i) {
+        const zg_material &m = p->materials[i];
+        if ((m.kind != ZG_EOS_IDEAL && m.kind != ZG_EOS_STIFFENED) || !(m.gamma > 1.0) || !(m.Cv > 0.0))
+            return fail(c, ZG_ERR_ARG, "zg_mmf_configure: invalid material");
+    }
+    if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_PLIC)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown CRP mode");
+    if (std::min(std::max(1, p->accuracy), 2) != 1)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: only the first-order MmFluid step is implemented");
+    DeviceGuard g(c->device);
+    c->mpar = *p;
+    c->mpar.accuracy = 1;
+    c->mpar.CFL = std::max(0.0, std::min(p->CFL, 1.0));  // mm_fluid.cpp:43-45
+    if (c->mm_configured) return ZG_OK;
+    size_t n = (size_t)c->n;
+    constexpr int NF = 6 + 2 * mmf::NMAT;
+    ZG_CUDA(c, cudaMalloc(&c->d_mm, (2 * NF + 3 * mmf::NMAT) * n * sizeof(double)));
+    ZG_CUDA(c, cudaMalloc(&c->d_mm_scalars, 64));
+    ZG_CUDA(c, cudaMalloc(&c->d_mm_flags, n * sizeof(int)));
+    double *b = c->d_mm;
+    auto take = [&b, n]() {
+        double *p0 = b;
+        b += n;
+        return p0;
+    };
+    for (mmf::MmField *f : {&c->mz, &c->mznext}) {
+        f->rho = take();
+        f->vx = take();
+        f->vy = take();
+        f->P = take();
+        f->e = take();
+        f->T = take();
+        for (int i = 0; i < mmf::NMAT; ++i) f->b[i] = take();
+        for (int i = 0; i < mmf::NMAT; ++i) f->r[i] = take();
+    }
+    for (int i = 0; i < mmf::NMAT; ++i) {
+        c->mnx[i] = take();
+        c->mny[i] = take();
+        c->moff[i] = take();
+    }
+    ZG_CUDA(c, cudaMemsetAsync(c->d_mm, 0, (2 * NF + 3 * mmf::NMAT) * n * sizeof(double), c->stream));
+    unsigned long long init[4] = {0x7FEFFFFFFFFFFFFFull, 0ull, 0ull, 0ull};
+    ZG_CUDA(c, cudaMemcpyAsync(c->d_mm_scalars, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->mm_configured = true;
+    return ZG_OK;
+}
+
+int zg_mmf_state_upload(zg_ctx *c, const double *cells) {
+    int rc = mm_ready(c, "zg_mmf_state_upload");
+    if (rc != ZG_OK) return rc;
+    if (!cells) return fail(c, ZG_ERR_ARG, "zg_mmf_state_upload: null array");
+    size_t n = (size_t)c->n;
+    constexpr int NF = 6 + 2 * mmf::NMAT;
+    std::vector<double> soa(NF * n);
+    for (size_t i = 0; i < n; ++i) {
+        const double *s = cells + 14 * i;
+        for (int k = mmf::NMAT; k < 4; ++k)
+            if (s[6 + k] != 0.0) return fail(c, ZG_ERR_ARG, "zg_mmf_state_upload: fraction of an absent material");
+        for (int k = 0; k < 6; ++k) soa[k * n + i] = s[k];
+        for (int k = 0; k < mmf::NMAT; ++k) {
+            soa[(6 + k) * n + i] = s[6 + k];
+            soa[(6 + mmf::NMAT + k) * n + i] = s[10 + k];
+        }
+    }
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(c->mz.rho, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_mmf_state_download(zg_ctx *c, double *cells) {
+    int rc = mm_ready(c, "zg_mmf_state_download");
+    if (rc != ZG_OK) return rc;
+    if (!cells) return fail(c, ZG_ERR_ARG, "zg_mmf_state_download: null array");
+    DeviceGuard g(c->device);
+    size_t n = (size_t)c->n;
+    std::vector<double *> fields = {c->mz.rho, c->mz.vx, c->mz.vy, c->mz.P, c->mz.e, c->mz.T};
+    for (int k = 0; k < mmf::NMAT; ++k) fields.push_back(c->mz.b[k]);
+    for (int k = 0; k < mmf::NMAT; ++k) fields.push_back(c->mz.r[k]);
+    std::vector<double> soa(fields.size() * n);
+    for (size_t k = 0; k < fields.size(); ++k)
+        ZG_CUDA(c, cudaMemcpyAsync(soa.data() + k * n, fields[k], n * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    rc = mm_check_error(c);
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    for (size_t i = 0; i < n; ++i) {
+        double *s = cells + 14 * i;
+        for (int k = 0; k < 6; ++k) s[k] = soa[k * n + i];
+        for (int k = 0; k < 4; ++k) {
+            s[6 + k] = k < mmf::NMAT ? soa[(6 + k) * n + i] : 0.0;
+            s[10 + k] = k < mmf::NMAT ? soa[(6 + mmf::NMAT + k) * n + i] : nan;
+        }
+    }
+    return rc;
+}
+
+int zg_mmf_make_states(zg_ctx *c, const double *rho, const double *vx, const double *vy, const double *p,
+                       const double *beta) {
+    int rc = mm_ready(c, "zg_mmf_make_states");
+    if (rc != ZG_OK) return rc;
+    if (!rho || !vx || !vy || !p || !beta) return fail(c, ZG_ERR_ARG, "zg_mmf_make_states: null array");
+    DeviceGuard g(c->device);
+    size_t n = (size_t)c->n;
+    for (size_t i = 0; i < n; ++i)
+        for (int k = mmf::NMAT; k < 4; ++k)
+            if (beta[4 * i + k] != 0.0) return fail(c, ZG_ERR_ARG, "zg_mmf_make_states: fraction of an absent material");
+    // staging: rho, vx, vy, p (n each) and beta (4 n) in the next-state buffer's fields
+    double *tmp = nullptr;
+    ZG_CUDA(c, cudaMalloc(&tmp, 8 * n * sizeof(double)));
+    const double *src[4] = {rho, vx, vy, p};
+    for (int k = 0; k < 4; ++k)
+        ZG_CUDA(c, cudaMemcpyAsync(tmp + k * n, src[k], n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ZG_CUDA(c, cudaMemcpyAsync(tmp + 4 * n, beta, 4 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    mmf::MmArgs a = make_mm_args(c);
+    mmf::launch_make_states(a, tmp, tmp + n, tmp + 2 * n, tmp + 3 * n, tmp + 4 * n, (void *)c->stream);
+    ++c->launches;
+    cudaError_t e = cudaGetLastError();
+    cudaError_t s = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(c, e, "zg_mmf_make_states launch");
+    if (s != cudaSuccess) return cuda_fail(c, s, "zg_mmf_make_states");
+    return ZG_OK;
+}
+
+int zg_mmf_update(zg_ctx *c) { return zg_mmf_update_n(c, 1); }
+
+int zg_mmf_update_n(zg_ctx *c, int n_steps) {
+    int rc = mm_ready(c, "zg_mmf_update");
+    if (rc != ZG_OK) return rc;
+    if (n_steps < 0) return fail(c, ZG_ERR_ARG, "zg_mmf_update_n: negative step count");
+    DeviceGuard g(c->device);
+    for (int k = 0; k < n_steps; ++k) {
+        rc = enqueue_mm_step(c);
+        if (rc != ZG_OK) return rc;
+    }
+    return ZG_OK;
+}
+
+int zg_mmf_dt(zg_ctx *c, double *dt) {
+    int rc = mm_ready(c, "zg_mmf_dt");
+    if (rc != ZG_OK) return rc;
+    if (!dt) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(dt, c->d_mm_scalars + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return mm_check_error(c);
+}
+
+int zg_mmf_set_flags(zg_ctx *c, int *flags) {
+    int rc = mm_ready(c, "zg_mmf_set_flags");
+    if (rc != ZG_OK) return rc;
+    if (!flags) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    mmf::MmArgs a = make_mm_args(c);
+    mmf::launch_flags(a, c->d_mm_flags, (void *)c->stream);
+    ++c->launches;
+    ZG_CUDA(c, cudaGetLastError());
+    ZG_CUDA(c, cudaMemcpyAsync(flags, c->d_mm_flags, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_mmf_interface(zg_ctx *c, double *normals, double *offsets) {
+    int rc = mm_ready(c, "zg_mmf_interface");
+    if (rc != ZG_OK) return rc;
+    if (!normals || !offsets) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    mmf::MmArgs a = make_mm_args(c);
+    mmf::launch_recover(a, (void *)c->stream);
+    ++c->launches;
+    ZG_CUDA(c, cudaGetLastError());
+    size_t n = (size_t)c->n;
+    std::vector<double> buf(3 * mmf::NMAT * n);
+    for (int i = 0; i < mmf::NMAT; ++i) {
+        ZG_CUDA(c, cudaMemcpyAsync(buf.data() + (3 * i) * n, c->mnx[i], n * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream));
+        ZG_CUDA(c, cudaMemcpyAsync(buf.data() + (3 * i + 1) * n, c->mny[i], n * sizeof(double),
+                                   cudaMemcpyDeviceToHost, c->stream));
+        ZG_CUDA(c, cudaMemcpyAsync(buf.data() + (3 * i + 2) * n, c->moff[i], n * sizeof(double),
+                                   cudaMemcpyDeviceToHost, c->stream));
+    }
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t ic = 0; ic < n; ++ic)
+        for (int i = 0; i < mmf::NMAT; ++i) {
+            normals[(ic * mmf::NMAT + i) * 2] = buf[(3 * i) * n + ic];
+            normals[(ic * mmf::NMAT + i) * 2 + 1] = buf[(3 * i + 1) * n + ic];
+            offsets[ic * mmf::NMAT + i] = buf[(3 * i + 2) * n + ic];
+        }
+    return ZG_OK;
 }
 
 }  // extern "C"
