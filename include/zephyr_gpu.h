@@ -206,7 +206,9 @@ enum zg_kernel_kind {
     ZG_K_FLAGS,       /* refinement flags */
     ZG_K_MM_DT,       /* multi-material CFL minimum (MmFluid::compute_dt) */
     ZG_K_MM_RECOVER,  /* PLIC reconstruction (MmFluid::interface_recovery) */
-    ZG_K_MM_FLUX,     /* multi-material first-order step (MmFluid::fluxes) */
+    ZG_K_MM_FLUX,     /* multi-material face loop, cells whose stencil is all pure (MmFluid::fluxes) */
+    ZG_K_MM_CRP,      /* multi-material face loop, cells next to a mixed cell (composite Riemann fluxes) */
+    ZG_K_MM_CLOSURE,  /* PT-equilibrium closure of updates that came out mixed (MixturePT::get_rPT) */
     ZG_K_COUNT
 };
 

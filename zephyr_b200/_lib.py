@@ -111,7 +111,7 @@ SIGNATURES = {
 
 # enum zg_kernel_kind
 KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags", "mm_dt", "mm_recover",
-                "mm_flux"]
+                "mm_flux", "mm_crp", "mm_closure"]
 
 _lib = None
 

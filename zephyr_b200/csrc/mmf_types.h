@@ -31,11 +31,21 @@ struct MmArgs {
     unsigned int *dt_ticket;
     double *dt_out;
     int *err;  // set to 1 where the reference would throw
+    // Work lists of the face loop: cells whose stencil holds a mixed state
+    // (composite Riemann fluxes) and cells whose update came out mixed
+    // (Newton closure), with their conservative states.
+    int *counts;     // [0] cells in list_crp, [1] cells in list_closure
+    int *list_crp, *list_closure;
+    double *qbuf;    // (4 + NMAT) doubles per closure-list entry
+    double *fbuf;    // (4 + NMAT) doubles per face of every list_crp cell (4 per cell)
 };
 
 void launch_dt(const MmArgs &a, void *stream);
 void launch_recover(const MmArgs &a, void *stream);
-void launch_flux1(const MmArgs &a, void *stream);
+// the face loop: pure stencils, then the two work lists
+void launch_flux_pure(const MmArgs &a, void *stream);
+void launch_flux_crp(const MmArgs &a, void *stream);  // face fluxes, then the cell updates
+void launch_closure(const MmArgs &a, void *stream);
 void launch_flags(const MmArgs &a, int *flags, void *stream);
 void launch_make_states(const MmArgs &a, const double *rho, const double *vx, const double *vy, const double *P,
                         const double *beta, void *stream);

@@ -70,6 +70,8 @@ struct zg_ctx {
     double *d_mm = nullptr;        // two states of 6 + 2 NMAT fields, then 3 NMAT interface fields
     unsigned long long *d_mm_scalars = nullptr;  // CFL minimum @0, ticket @8, dt @16, error flag @24
     int *d_mm_flags = nullptr;
+    int *d_mm_lists = nullptr;     // 8 counters, then the two work lists of the face loop (n each)
+    double *d_mm_qbuf = nullptr;   // conservative states of the closure list
     mmf::MmField mz{}, mznext{};
     double *mnx[mmf::NMAT] = {}, *mny[mmf::NMAT] = {}, *moff[mmf::NMAT] = {};
 
@@ -115,6 +117,10 @@ void free_mm(zg_ctx *c) {
     cudaFree(c->d_mm);
     cudaFree(c->d_mm_scalars);
     cudaFree(c->d_mm_flags);
+    cudaFree(c->d_mm_lists);
+    cudaFree(c->d_mm_qbuf);
+    c->d_mm_lists = nullptr;
+    c->d_mm_qbuf = nullptr;
     c->d_mm = nullptr;
     c->d_mm_scalars = nullptr;
     c->d_mm_flags = nullptr;
@@ -911,7 +917,8 @@ int zg_kernel_times(zg_ctx *c, double *ms, long long *launches) {
 
 const char *zg_kernel_name(int kind) {
     static const char *names[ZG_K_COUNT] = {"dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b",
-                                            "flags", "mm_dt", "mm_recover", "mm_flux"};
+                                            "flags", "mm_dt", "mm_recover", "mm_flux", "mm_crp",
+                                            "mm_closure"};
     return (kind >= 0 && kind < ZG_K_COUNT) ? names[kind] : "unknown";
 }
 
@@ -950,6 +957,11 @@ mmf::MmArgs make_mm_args(const zg_ctx *c) {
     a.dt_ticket = reinterpret_cast<unsigned int *>(c->d_mm_scalars + 1);
     a.dt_out = reinterpret_cast<double *>(c->d_mm_scalars + 2);
     a.err = reinterpret_cast<int *>(c->d_mm_scalars + 3);
+    a.counts = c->d_mm_lists;
+    a.list_crp = c->d_mm_lists + 8;
+    a.list_closure = c->d_mm_lists + 8 + c->n;
+    a.qbuf = c->d_mm_qbuf;
+    a.fbuf = c->d_mm_qbuf + (4 + mmf::NMAT) * (size_t)c->n;
     return a;
 }
 
@@ -973,7 +985,9 @@ int enqueue_mm_step(zg_ctx *c) {
     void *st = (void *)c->stream;
     timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(a, st); });
     if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
-    timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux1(a, st); });
+    timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux_pure(a, st); });
+    timed(c, ZG_K_MM_CRP, [&] { mmf::launch_flux_crp(a, st); });
+    timed(c, ZG_K_MM_CLOSURE, [&] { mmf::launch_closure(a, st); });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     std::swap(c->mz, c->mznext);  // MmFluid::swap (mm_fluid.cpp:682-684)
@@ -1107,6 +1121,9 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
     ZG_CUDA(c, cudaMalloc(&c->d_mm, (2 * NF + 3 * mmf::NMAT) * n * sizeof(double)));
     ZG_CUDA(c, cudaMalloc(&c->d_mm_scalars, 64));
     ZG_CUDA(c, cudaMalloc(&c->d_mm_flags, n * sizeof(int)));
+    ZG_CUDA(c, cudaMalloc(&c->d_mm_lists, (2 * n + 8) * sizeof(int)));
+    ZG_CUDA(c, cudaMalloc(&c->d_mm_qbuf, 5 * (4 + mmf::NMAT) * n * sizeof(double)));  // closure q, face terms
+    ZG_CUDA(c, cudaMemsetAsync(c->d_mm_lists, 0, (2 * n + 8) * sizeof(int), c->stream));
     double *b = c->d_mm;
     auto take = [&b, n]() {
         double *p0 = b;
