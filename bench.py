@@ -266,8 +266,8 @@ def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=F
     barrier()
     ms = e0.elapsed_time(e1)
     launches = mesh.launch_count() - n0
-    kms = (C.c_double * 8)()
-    kcount = (C.c_longlong * 8)()
+    kms = (C.c_double * len(KERNEL_KINDS))()
+    kcount = (C.c_longlong * len(KERNEL_KINDS))()
     lib.zg_kernel_times(mesh.ctx, kms, kcount)
     lib.zg_set_timing(mesh.ctx, 0)
     kernels = {}
@@ -277,6 +277,64 @@ def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=F
             kernels[name] = {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k],
                              "share": kms[k] / tot}
     return ms, kernels, launches, (sampler.stop() if sampler else None)
+
+
+MM_SIZE = 1024     # shock / water-column problem, cells per side
+MM_B_ALG = 160     # bytes per cell and step: 10 FP64 state fields read once and written once
+
+
+def mm_cpu_reference(w, steps_budget_s=10.0):
+    """The reference's own MmFluid (oracle/_ref) on this host's cores, a few
+    steps of the full problem; None when that build is absent."""
+    from oracle import ref_mm as RM
+    if not RM.available():
+        return None
+    threads = os.cpu_count() or 1
+    r = RM.RefMmFluid(w.nx, w.ny, box=w.box, bounds=w.bounds, materials="stiffened:Water,ideal:Air", CFL=0.4,
+                      accuracy=1, crp_mode=4)
+    r.set_threads(threads)
+    r.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
+    t0 = time.perf_counter()
+    r.step()
+    per = time.perf_counter() - t0
+    steps = max(1, min(10, int(steps_budget_s / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.step()
+    per = (time.perf_counter() - t0) / steps
+    return {"value": w.nx * w.ny / per, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": f"{steps} step(s) of the {w.nx}x{w.ny} problem after 1 untimed step; zephyr's "
+                      f"MmFluid::update compiled from its sources (oracle/_ref); {threads} threads"}
+
+
+def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu):
+    """The multi-material step (MmFluid, first order, CRP + PLIC) on the
+    two-material shock / water-column problem, 1024 x 1024."""
+    import zephyr_b200 as Z
+    from zephyr_b200.mmf import Material, MixturePT, MmFluid
+    from zephyr_b200.workloads import shock_water_column
+    w = shock_water_column(MM_SIZE)
+    gen = Z.Rectangle(*w.box)
+    gen.set_boundaries(Z.Boundaries(*w.bounds))
+    gen.set_sizes(w.nx, w.ny)
+    mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
+    solver = MmFluid(MixturePT([Material.stiffened("Water"), Material.ideal("Air")]))
+    solver.set_CFL(0.4)
+    solver.add_types(mesh)
+    solver.make_states(mesh, w.rho, w.vx, w.vy, w.p, w.beta)
+    solver.update(mesh, W)
+    mesh.synchronize()
+    ms, kernels, launches, _ = _timed_steps(torch, lib, mesh, solver, K, dev, stream, barrier)
+    solver.dt()  # raises if a step produced a state the reference rejects
+    cells = w.nx * w.ny
+    out = {"workload": f"shock_water_column {w.nx}x{w.ny} (water column in air, planar shock, "
+                       "StiffenedGas Water + IdealGas Air)",
+           "form": "FP64, bit-exact with the reference (MmFluid first order, CRP + PLIC, CFL 0.4)",
+           "ms": ms, "kernels": kernels, "launches": launches, "cells": cells}
+    mesh.close()
+    if want_cpu:
+        out["cpu_baseline"] = mm_cpu_reference(w)
+    return out
 
 
 def _max_over_ranks(torch, vals, dev, world):
@@ -356,8 +414,12 @@ def run_ours(args, rank, world, local_rank):
     linf = float(np.max(np.abs(rho_mx - rho64)) / np.max(np.abs(rho64)))
     m_ref.close()
 
-    vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix = vals
+    mm = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
+                    want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
+
+    vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"]],
+                           dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm = vals
     for v in variants.values():
         v["mesh"].close()
     if rank != 0:
@@ -382,7 +444,10 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
-        "roofline": roof, "kernels": kernels, "gpu_launches": int(launches), "clocks": clocks,
+        "roofline": roof, "kernels": kernels,
+        "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
+                            mm["launches"]),
+        "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
                 "note": "per step: upload of the whole state from pinned host memory, zg_smf_update, "
@@ -398,6 +463,13 @@ def run_ours(args, rank, world, local_rank):
                       "step_achieved_GBs": mixed_balg * cells * K / (ms_mix / 1e3) / 1e9,
                       "step_frac": mixed_balg * cells * K / (ms_mix / 1e3) / 1e9 / peak,
                       "kernels": variants["mixed"]["kernels"]},
+            "multimaterial": {
+                "value": world * mm["cells"] * K / (ms_mm / 1e3), "unit": METRIC, "ms_per_step": ms_mm / K,
+                "workload": mm["workload"], "form": mm["form"], "steps": K, "warmup": W,
+                "step_achieved_GBs": MM_B_ALG * mm["cells"] * K / (ms_mm / 1e3) / 1e9,
+                "step_frac": MM_B_ALG * mm["cells"] * K / (ms_mm / 1e3) / 1e9 / peak,
+                "algorithmic_bytes_per_cell": MM_B_ALG, "gpu_launches": int(mm["launches"]),
+                "kernels": mm["kernels"], "cpu_baseline": mm.get("cpu_baseline")},
         },
         "dt_last": dt_last,
     }

@@ -29,6 +29,7 @@ def lib():
         L.zmm_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I, C.c_char_p,
                                  C.c_double, C.c_int, C.c_int]
         L.zmm_free.argtypes = [C.c_void_p]
+        L.zm_threads.argtypes = [C.c_int]
         L.zmm_n_cells.argtypes = [C.c_void_p]
         L.zmm_n_cells.restype = C.c_int
         L.zmm_make_states.argtypes = [C.c_void_p, _P, _P, _P, _P, _P]
@@ -69,6 +70,10 @@ class RefMmFluid:
         self.h = lib().zmm_create(nx, ny, *box, b.ctypes.data_as(_I), materials.encode(), CFL, accuracy, crp_mode)
         self.n = lib().zmm_n_cells(self.h)
         self.nmat = materials.count(",") + 1
+
+    def set_threads(self, n):
+        """Worker threads of the reference's threads::for_each (0 or 1: off)."""
+        lib().zm_threads(n)
 
     def make_states(self, rho, vx, vy, P, beta):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, vx, vy, P)]
