@@ -303,6 +303,49 @@ int zg_mmf_set_flags(zg_ctx *ctx, int *flags);
  * n_materials per cell. */
 int zg_mmf_interface(zg_ctx *ctx, double *normals, double *offsets);
 
+/* ------------------------------------------------------------------------
+ * Adjoint mode (no counterpart in the reference): the gradient of
+ *   J = mean pressure over the cells whose centre lies in a probe box
+ * after `steps` Heun steps at a fixed dt, with respect to the initial density
+ * field and the adiabatic index, by a discrete adjoint (reverse sweep) with
+ * checkpoints every `checkpoint_every` steps.  The differentiated step: Heun's
+ * method on the finite-volume operator of the second-order step (limited
+ * least-squares slopes with a smooth van Albada limiter
+ * phi(a, b) = (a (a + b) + eps) / (a^2 + b^2 + eps), HLLC with Davis wave
+ * speeds, ideal gas), on a uniform rectangle periodic on both axes.  HLLC
+ * branches are differentiated on the side the forward takes.
+ * ------------------------------------------------------------------------ */
+typedef struct zg_adj zg_adj;
+typedef struct zg_adj_params {
+    double gamma;          /* adiabatic index */
+    double dt;             /* fixed time step (zg_adj_cfl_dt gives the CFL one) */
+    int steps;             /* Heun steps */
+    int checkpoint_every;  /* steps between stored states */
+    double limiter_eps;    /* eps of the smooth limiter (default 1e-8) */
+    double probe[4];       /* x_min, x_max, y_min, y_max of the probe box */
+} zg_adj_params;
+
+/* gamma 1.4, 100 steps, checkpoints every 10, eps 1e-8, probe [0.6,0.7]^2. */
+void zg_adj_default_params(zg_adj_params *p);
+int zg_adj_create(zg_adj **out, int device, int nx, int ny, double x_min, double x_max, double y_min,
+                  double y_max);
+int zg_adj_destroy(zg_adj *a);
+const char *zg_adj_last_error(const zg_adj *a);
+int zg_adj_set_stream(zg_adj *a, void *stream);
+int zg_adj_launch_count(const zg_adj *a, long long *count);
+/* dt = CFL min(hx, hy) / (|v| + c) over the cells (SmFluid::compute_dt on a
+ * rectangle) for the given initial state (device arrays). */
+int zg_adj_cfl_dt(zg_adj *a, double gamma, double CFL, const double *rho, const double *u, const double *v,
+                  const double *p, double *dt);
+/* J of the run from the initial state (rho, u, v, p: device arrays of
+ * nx * ny doubles, cell (i, j) at i * ny + j); J on the host. */
+int zg_adj_forward(zg_adj *a, const zg_adj_params *prm, const double *rho, const double *u, const double *v,
+                   const double *p, double *J);
+/* J, dJ/drho_0 (device array of nx * ny doubles, or NULL) and dJ/dgamma
+ * (host, or NULL). */
+int zg_adj_gradient(zg_adj *a, const zg_adj_params *prm, const double *rho, const double *u, const double *v,
+                    const double *p, double *J, double *dJ_drho, double *dJ_dgamma);
+
 /* Largest nx and ny that zg_rect_step_noalloc accepts. */
 #define ZG_NOALLOC_MAX_AXIS 8192
 

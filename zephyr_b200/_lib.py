@@ -68,6 +68,12 @@ class MmfParams(C.Structure):
                 ("accuracy", C.c_int), ("CFL", C.c_double), ("max_dt", C.c_double)]
 
 
+class AdjParams(C.Structure):
+    """zg_adj_params"""
+    _fields_ = [("gamma", C.c_double), ("dt", C.c_double), ("steps", C.c_int), ("checkpoint_every", C.c_int),
+                ("limiter_eps", C.c_double), ("probe", C.c_double * 4)]
+
+
 SIGNATURES = {
     "zg_smf_default_params": (None, [C.POINTER(SmfParams)]),
     "zg_limiter_from_name": (C.c_int, [C.c_char_p]),
@@ -104,6 +110,16 @@ SIGNATURES = {
     "zg_mmf_dt": (C.c_int, [_V, _P]),
     "zg_mmf_set_flags": (C.c_int, [_V, _I]),
     "zg_mmf_interface": (C.c_int, [_V, _P, _P]),
+    "zg_adj_default_params": (None, [C.POINTER(AdjParams)]),
+    "zg_adj_create": (C.c_int, [C.POINTER(_V), C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                C.c_double]),
+    "zg_adj_destroy": (C.c_int, [_V]),
+    "zg_adj_last_error": (C.c_char_p, [_V]),
+    "zg_adj_set_stream": (C.c_int, [_V, _V]),
+    "zg_adj_launch_count": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
+    "zg_adj_cfl_dt": (C.c_int, [_V, C.c_double, C.c_double, _V, _V, _V, _V, _P]),
+    "zg_adj_forward": (C.c_int, [_V, C.POINTER(AdjParams), _V, _V, _V, _V, _P]),
+    "zg_adj_gradient": (C.c_int, [_V, C.POINTER(AdjParams), _V, _V, _V, _V, _P, _V, _P]),
     "zg_rect_step_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                        C.c_double, _I, C.POINTER(SmfParams), C.POINTER(_V), C.POINTER(_V), _V,
                                        _V]),

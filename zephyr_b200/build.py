@@ -33,6 +33,7 @@ UNITS = {
     # must match the host-built ones, hence no fused multiply-adds
     "zg_noalloc.cu": ["-fmad=false"],
     "smf_fast.cu": [],
+    "adj.cu": [],
     # FP32 face arithmetic: approximate single-precision division and square
     # root; FP64 operations are unaffected by these flags.
     "smf_mixed.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],

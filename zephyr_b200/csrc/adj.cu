@@ -1,0 +1,710 @@
+// adj.cu -- discrete adjoint of the Heun step (the adjoint mode, no
+// counterpart in the reference), the C ABI zg_adj_*.
+//
+// Forward: Heun's method at a fixed dt on a uniform periodic rectangle
+// (adj_math.cuh has the step's definition), state U = (rho, rho u, rho v,
+// rho E) as four arrays of n doubles, cell ic = i * ny + j.
+// Objective: J = mean pressure over the cells whose centre lies in the probe
+// box.  Gradient: dJ / d rho_0 (the initial density field, the initial
+// velocity and pressure held fixed) and dJ / d gamma.
+//
+// Reverse sweep.  With lambda^n = dJ/dU^n and mu = a cotangent of L(X):
+//   U* = U + dt L(U),  U^{n+1} = 1/2 U + 1/2 U* + 1/2 dt L(U*)
+//   lambda*   = 1/2 lambda^{n+1} + L'(U*)^T (1/2 dt lambda^{n+1})
+//   lambda^n  = 1/2 lambda^{n+1} + lambda* + L'(U)^T (dt lambda*)
+// and the gamma derivative collects <mu, dL/dgamma> of both stages.  The
+// vector-Jacobian product L'(X)^T mu is two passes: per cell, the four face
+// fluxes' partials with respect to their two face states and gamma (dual
+// numbers through the HLLC formulas) give the cotangents of the cell's face
+// states, hence of its primitive state and its two slopes; per cell again,
+// the slopes' partials carry those back to the three cells each slope reads,
+// and the primitive map's partials to U and gamma.  HLLC branches and the
+// limiter are differentiated on the side the forward took.
+//
+// Checkpoints: U is kept every `checkpoint_every` steps during the forward;
+// the reverse sweep recomputes each segment's U^n and U* from its checkpoint
+// and walks it backwards, so memory grows with steps / checkpoint_every plus
+// one segment, not with the number of steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/zephyr_gpu.h"
+#include "adj_math.cuh"
+
+namespace zg {
+namespace adj {
+
+constexpr int BLOCK = 128;
+
+struct Grid {
+    int nx, ny, n;
+    double hx, hy, vol;
+    double x0, y0;
+};
+struct F4 {  // four field arrays
+    double *f[4];
+};
+struct CF4 {
+    const double *f[4];
+};
+
+__device__ __forceinline__ int xm(const Grid &g, int ic) {
+    int i = ic / g.ny;
+    return i > 0 ? ic - g.ny : ic + (g.nx - 1) * g.ny;
+}
+__device__ __forceinline__ int xp(const Grid &g, int ic) {
+    int i = ic / g.ny;
+    return i < g.nx - 1 ? ic + g.ny : ic - (g.nx - 1) * g.ny;
+}
+__device__ __forceinline__ int ym(const Grid &g, int ic) {
+    int j = ic % g.ny;
+    return j > 0 ? ic - 1 : ic + (g.ny - 1);
+}
+__device__ __forceinline__ int yp(const Grid &g, int ic) {
+    int j = ic % g.ny;
+    return j < g.ny - 1 ? ic + 1 : ic - (g.ny - 1);
+}
+
+__device__ __forceinline__ void load4(const CF4 &a, int ic, double o[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = a.f[k][ic];
+}
+__device__ __forceinline__ void prim_at(const CF4 &U, int ic, double gamma, double W[4]) {
+    double u[4];
+    load4(U, ic, u);
+    prim<double>(u, gamma, W);
+}
+
+// U from (rho, u, v, p)
+__global__ void k_init(Grid g, CF4 W0, double gamma, F4 U) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= g.n) return;
+    double r = W0.f[0][ic], u = W0.f[1][ic], v = W0.f[2][ic], p = W0.f[3][ic];
+    U.f[0][ic] = r;
+    U.f[1][ic] = r * u;
+    U.f[2][ic] = r * v;
+    U.f[3][ic] = p / (gamma - 1.0) + 0.5 * (r * (u * u + v * v));
+}
+
+// primitive state and limited slopes of every cell
+__global__ void __launch_bounds__(BLOCK) k_prim_grad(Grid g, CF4 U, double gamma, double eps, F4 W, F4 gx, F4 gy) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= g.n) return;
+    double wc[4], wl[4], wr[4], wb[4], wt[4];
+    prim_at(U, ic, gamma, wc);
+    prim_at(U, xm(g, ic), gamma, wl);
+    prim_at(U, xp(g, ic), gamma, wr);
+    prim_at(U, ym(g, ic), gamma, wb);
+    prim_at(U, yp(g, ic), gamma, wt);
+    const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        W.f[k][ic] = wc[k];
+        gx.f[k][ic] = slope<double>(wl[k], wc[k], wr[k], i2x, eps);
+        gy.f[k][ic] = slope<double>(wb[k], wc[k], wt[k], i2y, eps);
+    }
+}
+
+// Face states of the face between `lo` and `hi` along an axis, in the face
+// frame (x faces: (rho, u, v, p); y faces: (rho, v, -u, p)).
+__device__ __forceinline__ void face_states(const CF4 &W, const CF4 &G, int lo, int hi, double half_h, bool yface,
+                                            double L[4], double R[4]) {
+    double a[4], b[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        a[k] = W.f[k][lo] + G.f[k][lo] * half_h;
+        b[k] = W.f[k][hi] - G.f[k][hi] * half_h;
+    }
+    if (!yface) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            L[k] = a[k];
+            R[k] = b[k];
+        }
+    } else {
+        L[0] = a[0]; L[1] = a[2]; L[2] = -a[1]; L[3] = a[3];
+        R[0] = b[0]; R[1] = b[2]; R[2] = -b[1]; R[3] = b[3];
+    }
+}
+// face-frame flux back to the global frame
+__device__ __forceinline__ void flux_global(const double Fl[4], bool yface, double F[4]) {
+    if (!yface) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) F[k] = Fl[k];
+    } else {
+        F[0] = Fl[0];
+        F[1] = -Fl[2];
+        F[2] = Fl[1];
+        F[3] = Fl[3];
+    }
+}
+
+// out = alpha * base + beta * (X + dt L(X)), L from the face fluxes of W, G
+__global__ void __launch_bounds__(BLOCK) k_flux_update(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 X,
+                                                       CF4 base, double alpha, double beta, double dt, F4 out) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= g.n) return;
+    const int nb[4] = {xm(g, ic), xp(g, ic), ym(g, ic), yp(g, ic)};
+    double sum[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const bool yface = s >= 2, high = (s & 1) == 1;
+        const int lo = high ? ic : nb[s], hi = high ? nb[s] : ic;
+        const double half_h = 0.5 * (yface ? g.hy : g.hx), S = yface ? g.hx : g.hy;
+        double L[4], R[4], Fl[4], F[4];
+        face_states(W, yface ? gy : gx, lo, hi, half_h, yface, L, R);
+        hllc<double>(L, R, gamma, Fl);
+        flux_global(Fl, yface, F);
+        const double sgn = high ? S : -S;  // outward flux of this cell
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sum[k] += sgn * F[k];
+    }
+    const double c = dt / g.vol;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double v = beta * (X.f[k][ic] - c * sum[k]);
+        if (alpha != 0.0) v += alpha * base.f[k][ic];
+        out.f[k][ic] = v;
+    }
+}
+
+__device__ __forceinline__ bool in_probe(const Grid &g, int ic, const double probe[4]) {
+    int i = ic / g.ny, j = ic - (ic / g.ny) * g.ny;
+    double cx = g.x0 + (i + 0.5) * g.hx, cy = g.y0 + (j + 0.5) * g.hy;
+    return cx >= probe[0] && cx <= probe[1] && cy >= probe[2] && cy <= probe[3];
+}
+
+// Deterministic block sums: thread 0 of block b adds the block's sum to acc[b]
+// (each kernel of the sweep launches the same number of blocks).
+__device__ __forceinline__ void block_add(double x, double *acc) {
+    __shared__ double sm[BLOCK / 32];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < BLOCK / 32; ++w) s += sm[w];
+        acc[blockIdx.x] += s;
+    }
+    __syncthreads();  // sm is reused by the next call
+}
+
+// J partial sums (sum of p over the probe) and, with lam != null, dJ/dU at the
+// final state (scale = 1 / probe cells) with the gamma part into gacc.
+__global__ void __launch_bounds__(BLOCK) k_probe(Grid g, CF4 U, double gamma, double p0, double p1, double p2,
+                                                 double p3, double scale, double *jacc, F4 lam, double *gacc) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    const double probe[4] = {p0, p1, p2, p3};
+    double pj = 0.0, gj = 0.0;
+    if (ic < g.n) {
+        double u[4];
+        load4(U, ic, u);
+        bool in = in_probe(g, ic, probe);
+        double ke = 0.5 * ((u[1] * u[1] + u[2] * u[2]) / u[0]);
+        if (in) {
+            pj = (gamma - 1.0) * (u[3] - ke);
+            gj = scale * (u[3] - ke);
+        }
+        if (lam.f[0]) {
+            double vx = u[1] / u[0], vy = u[2] / u[0];
+            double s = in ? scale * (gamma - 1.0) : 0.0;
+            lam.f[0][ic] = s * 0.5 * (vx * vx + vy * vy);
+            lam.f[1][ic] = -s * vx;
+            lam.f[2][ic] = -s * vy;
+            lam.f[3][ic] = s;
+        }
+    }
+    block_add(pj, jacc);
+    if (lam.f[0]) block_add(gj, gacc);
+}
+
+// --- vector-Jacobian product of L, pass 1: per cell, its four faces ----------
+// mu_eff = coef * mu.  Writes the cotangents of the cell's primitive state
+// (Wb) and slopes (gbx, gby); the gamma part of the faces the cell owns (its
+// high faces) goes to gacc.
+__global__ void __launch_bounds__(BLOCK) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
+                                                     double coef, F4 Wb, F4 gbx, F4 gby, double *gacc) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    double gpart = 0.0;
+    if (ic < g.n) {
+        const int nb[4] = {xm(g, ic), xp(g, ic), ym(g, ic), yp(g, ic)};
+        double wb[4] = {0.0, 0.0, 0.0, 0.0}, bx[4] = {0.0, 0.0, 0.0, 0.0}, by[4] = {0.0, 0.0, 0.0, 0.0};
+        const double cv = coef / g.vol;
+#pragma unroll 1
+        for (int s = 0; s < 4; ++s) {
+            const bool yface = s >= 2, high = (s & 1) == 1;
+            const int lo = high ? ic : nb[s], hi = high ? nb[s] : ic;
+            const double half_h = 0.5 * (yface ? g.hy : g.hx), S = yface ? g.hx : g.hy;
+            // cotangent of the global face flux: L_lo gets -S/V F, L_hi +S/V F
+            double mF[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) mF[k] = cv * S * (mu.f[k][hi] - mu.f[k][lo]);
+            double ml[4];  // in the face frame (transpose of flux_global)
+            if (!yface) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) ml[k] = mF[k];
+            } else {
+                ml[0] = mF[0];
+                ml[1] = mF[2];
+                ml[2] = -mF[1];
+                ml[3] = mF[3];
+            }
+            double L[4], R[4];
+            face_states(W, yface ? gy : gx, lo, hi, half_h, yface, L, R);
+            Dual<9> dL[4], dR[4], Fl[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                dL[k] = dvar<9>(L[k], k);
+                dR[k] = dvar<9>(R[k], 4 + k);
+            }
+            Dual<9> dg = dvar<9>(gamma, 8);
+            hllc<Dual<9>>(dL, dR, dg, Fl);
+            double bar[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                double a = 0.0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) a += ml[k] * Fl[k].d[q];
+                bar[q] = a;
+            }
+            if (high) gpart += bar[8];
+            // this cell's side of the face, face frame -> global primitive
+            const double *side = high ? bar : bar + 4;
+            double wl[4];
+            if (!yface) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) wl[k] = side[k];
+            } else {
+                wl[0] = side[0];
+                wl[1] = -side[2];
+                wl[2] = side[1];
+                wl[3] = side[3];
+            }
+            // face state = W_c +- slope_c h/2 (+ on the cell's high face)
+            const double sh = high ? half_h : -half_h;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                wb[k] += wl[k];
+                if (yface) by[k] += sh * wl[k];
+                else bx[k] += sh * wl[k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            Wb.f[k][ic] = wb[k];
+            gbx.f[k][ic] = bx[k];
+            gby.f[k][ic] = by[k];
+        }
+    }
+    block_add(gpart, gacc);
+}
+
+// d slope(wm, w0, wp) / d(wm, w0, wp)
+__device__ __forceinline__ void slope_partials(double wm, double w0, double wp, double inv2h, double eps,
+                                               double d[3]) {
+    Dual<3> a = dvar<3>(wm, 0), b = dvar<3>(w0, 1), c = dvar<3>(wp, 2);
+    Dual<3> s = slope<Dual<3>>(a, b, c, inv2h, eps);
+    d[0] = s.d[0];
+    d[1] = s.d[1];
+    d[2] = s.d[2];
+}
+
+// --- vector-Jacobian product of L, pass 2: per cell ----------------------------
+// The slopes of this cell and of its two neighbours on each axis read this
+// cell's primitive state; their cotangents come back here, then through the
+// primitive map to U and gamma.  out = base_coef * base + add + Ubar.
+__global__ void __launch_bounds__(BLOCK) k_vjp_cells(Grid g, CF4 X, CF4 W, double gamma, double eps, CF4 Wb,
+                                                     CF4 gbx, CF4 gby, CF4 base, double base_coef, CF4 add,
+                                                     F4 out, double *gacc) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    double gpart = 0.0;
+    if (ic < g.n) {
+        const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy;
+        const int l = xm(g, ic), r = xp(g, ic), b = ym(g, ic), t = yp(g, ic);
+        const int ll = xm(g, l), rr = xp(g, r), bb = ym(g, b), tt = yp(g, t);
+        double wt[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double w_ll = W.f[k][ll], w_l = W.f[k][l], w_c = W.f[k][ic], w_r = W.f[k][r], w_rr = W.f[k][rr];
+            double w_bb = W.f[k][bb], w_b = W.f[k][b], w_t = W.f[k][t], w_tt = W.f[k][tt];
+            double d[3], acc = Wb.f[k][ic];
+            slope_partials(w_ll, w_l, w_c, i2x, eps, d);  // slope of the left cell: this cell is its wp
+            acc += d[2] * gbx.f[k][l];
+            slope_partials(w_l, w_c, w_r, i2x, eps, d);   // own slope
+            acc += d[1] * gbx.f[k][ic];
+            slope_partials(w_c, w_r, w_rr, i2x, eps, d);  // right cell: this cell is its wm
+            acc += d[0] * gbx.f[k][r];
+            slope_partials(w_bb, w_b, w_c, i2y, eps, d);
+            acc += d[2] * gby.f[k][b];
+            slope_partials(w_b, w_c, w_t, i2y, eps, d);
+            acc += d[1] * gby.f[k][ic];
+            slope_partials(w_c, w_t, w_tt, i2y, eps, d);
+            acc += d[0] * gby.f[k][t];
+            wt[k] = acc;
+        }
+        // primitive map (rho, u, v, p)(U, gamma)
+        Dual<5> du[4], dgm = dvar<5>(gamma, 4), dw[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) du[k] = dvar<5>(X.f[k][ic], k);
+        prim<Dual<5>>(du, dgm, dw);
+        double ub[5];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double a = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a += wt[k] * dw[k].d[q];
+            ub[q] = a;
+        }
+        gpart = ub[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double v = ub[k];
+            if (base.f[0]) v += base_coef * base.f[k][ic];
+            if (add.f[0]) v += add.f[k][ic];
+            out.f[k][ic] = v;
+        }
+    }
+    block_add(gpart, gacc);
+}
+
+// dJ/d rho_0 from lambda^0 (U_0 = (rho, rho u, rho v, p/(gamma-1) + rho |v|^2 / 2)),
+// and the gamma part of U_0's energy.
+__global__ void __launch_bounds__(BLOCK) k_seed(Grid g, CF4 W0, double gamma, CF4 lam, double *grad,
+                                                double *gacc) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    double gpart = 0.0;
+    if (ic < g.n) {
+        double u = W0.f[1][ic], v = W0.f[2][ic], p = W0.f[3][ic];
+        double l0 = lam.f[0][ic], l1 = lam.f[1][ic], l2 = lam.f[2][ic], l3 = lam.f[3][ic];
+        if (grad) grad[ic] = l0 + l1 * u + l2 * v + l3 * (0.5 * (u * u + v * v));
+        double gm1 = gamma - 1.0;
+        gpart = l3 * (-p / (gm1 * gm1));
+    }
+    block_add(gpart, gacc);
+}
+
+}  // namespace adj
+}  // namespace zg
+
+using namespace zg::adj;
+
+struct zg_adj {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    Grid g{};
+    // storage
+    double *d_all = nullptr;
+    size_t cap_ckpt = 0, cap_seg = 0;  // checkpoints and segment states held
+    double *d_acc = nullptr;           // per-block accumulators: J, gamma
+    F4 U0{}, Ua{}, Ub{}, Ustar{}, W{}, gx{}, gy{}, Wb{}, gbx{}, gby{}, lamA{}, lamB{}, lamS{};
+    std::vector<F4> ckpt, seg, segstar;
+    long long launches = 0;
+};
+
+namespace {
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int afail(zg_adj *a, int code, const std::string &m) {
+    if (a) a->err = m;
+    return code;
+}
+
+CF4 cf(const F4 &x) { return CF4{{x.f[0], x.f[1], x.f[2], x.f[3]}}; }
+const CF4 kNull{{nullptr, nullptr, nullptr, nullptr}};
+const F4 kNullW{{nullptr, nullptr, nullptr, nullptr}};
+
+unsigned nblocks(const zg_adj *a) { return (unsigned)((a->g.n + BLOCK - 1) / BLOCK); }
+
+// (re)allocate for `ckpts` checkpoints and segments of `seglen` steps
+int reserve(zg_adj *a, size_t ckpts, size_t seglen) {
+    if (a->d_all && ckpts <= a->cap_ckpt && seglen <= a->cap_seg) return ZG_OK;
+    cudaFree(a->d_all);
+    a->d_all = nullptr;
+    size_t n = (size_t)a->g.n;
+    size_t fields = 13 * 4 + 4 * ckpts + 4 * (seglen + 1) + 4 * seglen;
+    cudaError_t e = cudaMalloc(&a->d_all, fields * n * sizeof(double));
+    if (e != cudaSuccess) return afail(a, ZG_ERR_ALLOC, std::string("adjoint storage: ") + cudaGetErrorString(e));
+    double *p = a->d_all;
+    auto take = [&p, n]() {
+        F4 x;
+        for (int k = 0; k < 4; ++k) {
+            x.f[k] = p;
+            p += n;
+        }
+        return x;
+    };
+    for (F4 *x : {&a->U0, &a->Ua, &a->Ub, &a->Ustar, &a->W, &a->gx, &a->gy, &a->Wb, &a->gbx, &a->gby, &a->lamA,
+                  &a->lamB, &a->lamS})
+        *x = take();
+    a->ckpt.assign(ckpts, F4{});
+    for (auto &c : a->ckpt) c = take();
+    a->seg.assign(seglen + 1, F4{});
+    for (auto &c : a->seg) c = take();
+    a->segstar.assign(seglen, F4{});
+    for (auto &c : a->segstar) c = take();
+    a->cap_ckpt = ckpts;
+    a->cap_seg = seglen;
+    return ZG_OK;
+}
+
+void copy4(zg_adj *a, const F4 &dst, const F4 &src) {
+    for (int k = 0; k < 4; ++k)
+        cudaMemcpyAsync(dst.f[k], src.f[k], (size_t)a->g.n * sizeof(double), cudaMemcpyDeviceToDevice, a->stream);
+}
+
+// one Heun step: X -> out (stage value into `star`)
+void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out) {
+    unsigned nb = nblocks(a);
+    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, a->W, a->gx, a->gy);
+    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(a->W), cf(a->gx), cf(a->gy), p.gamma, cf(X), kNull, 0.0,
+                                               1.0, p.dt, star);
+    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, a->W, a->gx, a->gy);
+    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(a->W), cf(a->gx), cf(a->gy), p.gamma, cf(star), cf(X), 0.5,
+                                               0.5, p.dt, out);
+    a->launches += 4;
+}
+
+// out = base_coef * base + add + L'(X)^T (coef * mu)
+void vjp(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &mu, double coef, const F4 &base,
+         double base_coef, const CF4 &add, const F4 &out, double *gacc) {
+    unsigned nb = nblocks(a);
+    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, a->W, a->gx, a->gy);
+    k_vjp_faces<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(a->W), cf(a->gx), cf(a->gy), p.gamma, cf(mu), coef, a->Wb,
+                                             a->gbx, a->gby, gacc);
+    k_vjp_cells<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), cf(a->W), p.gamma, p.limiter_eps, cf(a->Wb), cf(a->gbx),
+                                             cf(a->gby), cf(base), base_coef, add, out, gacc);
+    a->launches += 3;
+}
+
+int check_params(zg_adj *a, const zg_adj_params *p) {
+    if (!p) return afail(a, ZG_ERR_ARG, "null parameters");
+    if (!(p->gamma > 1.0)) return afail(a, ZG_ERR_ARG, "gamma must exceed 1");
+    if (!(p->dt > 0.0)) return afail(a, ZG_ERR_ARG, "dt must be positive (see zg_adj_cfl_dt)");
+    if (p->steps < 1 || p->checkpoint_every < 1) return afail(a, ZG_ERR_ARG, "steps and checkpoint_every >= 1");
+    if (!(p->limiter_eps > 0.0)) return afail(a, ZG_ERR_ARG, "limiter_eps must be positive");
+    return ZG_OK;
+}
+
+int finish_sum(zg_adj *a, double *out2) {
+    unsigned nb = nblocks(a);
+    std::vector<double> h(2 * (size_t)nb);
+    cudaError_t e = cudaMemcpyAsync(h.data(), a->d_acc, h.size() * sizeof(double), cudaMemcpyDeviceToHost, a->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
+    if (e != cudaSuccess) return afail(a, ZG_ERR_CUDA, cudaGetErrorString(e));
+    out2[0] = out2[1] = 0.0;
+    for (unsigned b = 0; b < nb; ++b) out2[0] += h[b];
+    for (unsigned b = 0; b < nb; ++b) out2[1] += h[nb + b];
+    return ZG_OK;
+}
+
+int probe_count(const zg_adj *a, const zg_adj_params &p) {
+    int c = 0;
+    for (int i = 0; i < a->g.nx; ++i)
+        for (int j = 0; j < a->g.ny; ++j) {
+            double cx = a->g.x0 + (i + 0.5) * a->g.hx, cy = a->g.y0 + (j + 0.5) * a->g.hy;
+            if (cx >= p.probe[0] && cx <= p.probe[1] && cy >= p.probe[2] && cy <= p.probe[3]) ++c;
+        }
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+void zg_adj_default_params(zg_adj_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->gamma = 1.4;
+    p->dt = 0.0;
+    p->steps = 100;
+    p->checkpoint_every = 10;
+    p->limiter_eps = 1.0e-8;
+    p->probe[0] = 0.6;
+    p->probe[1] = 0.7;
+    p->probe[2] = 0.6;
+    p->probe[3] = 0.7;
+}
+
+int zg_adj_create(zg_adj **out, int device, int nx, int ny, double x_min, double x_max, double y_min, double y_max) {
+    if (!out) return ZG_ERR_ARG;
+    *out = nullptr;
+    if (nx < 3 || ny < 3 || !(x_max > x_min) || !(y_max > y_min)) return ZG_ERR_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return ZG_ERR_CUDA;
+    auto *a = new zg_adj();
+    a->device = device;
+    a->g.nx = nx;
+    a->g.ny = ny;
+    a->g.n = nx * ny;
+    a->g.hx = (x_max - x_min) / nx;
+    a->g.hy = (y_max - y_min) / ny;
+    a->g.vol = a->g.hx * a->g.hy;
+    a->g.x0 = x_min;
+    a->g.y0 = y_min;
+    DevGuard gd(device);
+    if (cudaMalloc(&a->d_acc, 2 * nblocks(a) * sizeof(double)) != cudaSuccess) {
+        delete a;
+        return ZG_ERR_ALLOC;
+    }
+    *out = a;
+    return ZG_OK;
+}
+
+int zg_adj_destroy(zg_adj *a) {
+    if (!a) return ZG_ERR_ARG;
+    {
+        DevGuard gd(a->device);
+        if (a->stream) cudaStreamSynchronize(a->stream);
+        else cudaDeviceSynchronize();
+        cudaFree(a->d_all);
+        cudaFree(a->d_acc);
+    }
+    delete a;
+    return ZG_OK;
+}
+
+const char *zg_adj_last_error(const zg_adj *a) { return a ? a->err.c_str() : "null handle"; }
+
+int zg_adj_set_stream(zg_adj *a, void *stream) {
+    if (!a) return ZG_ERR_ARG;
+    a->stream = (cudaStream_t)stream;
+    return ZG_OK;
+}
+
+int zg_adj_launch_count(const zg_adj *a, long long *count) {
+    if (!a || !count) return ZG_ERR_ARG;
+    *count = a->launches;
+    return ZG_OK;
+}
+
+int zg_adj_forward(zg_adj *a, const zg_adj_params *p, const double *rho, const double *u, const double *v,
+                   const double *pr, double *J) {
+    if (!a) return ZG_ERR_ARG;
+    int rc = check_params(a, p);
+    if (rc != ZG_OK) return rc;
+    if (!rho || !u || !v || !pr || !J) return afail(a, ZG_ERR_ARG, "null array");
+    DevGuard gd(a->device);
+    rc = reserve(a, std::max<size_t>(a->cap_ckpt, 1), std::max<size_t>(a->cap_seg, 1));
+    if (rc != ZG_OK) return rc;
+    unsigned nb = nblocks(a);
+    CF4 w0{{rho, u, v, pr}};
+    k_init<<<nb, BLOCK, 0, a->stream>>>(a->g, w0, p->gamma, a->Ua);
+    ++a->launches;
+    F4 cur = a->Ua, nxt = a->Ub;
+    for (int s = 0; s < p->steps; ++s) {
+        heun_step(a, *p, cur, a->Ustar, nxt);
+        std::swap(cur, nxt);
+    }
+    cudaMemsetAsync(a->d_acc, 0, 2 * nb * sizeof(double), a->stream);
+    int np = probe_count(a, *p);
+    if (np == 0) return afail(a, ZG_ERR_ARG, "no cell centre inside the probe box");
+    k_probe<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(cur), p->gamma, p->probe[0], p->probe[1], p->probe[2], p->probe[3],
+                                         1.0 / np, a->d_acc, kNullW, a->d_acc + nb);
+    ++a->launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return afail(a, ZG_ERR_CUDA, cudaGetErrorString(e));
+    double s2[2];
+    rc = finish_sum(a, s2);
+    if (rc != ZG_OK) return rc;
+    *J = s2[0] / np;
+    return ZG_OK;
+}
+
+int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const double *u, const double *v,
+                    const double *pr, double *J, double *dJ_drho, double *dJ_dgamma) {
+    if (!a) return ZG_ERR_ARG;
+    int rc = check_params(a, p);
+    if (rc != ZG_OK) return rc;
+    if (!rho || !u || !v || !pr || !J) return afail(a, ZG_ERR_ARG, "null array");
+    DevGuard gd(a->device);
+    const int N = p->steps, K = p->checkpoint_every;
+    const int nseg = (N + K - 1) / K;
+    rc = reserve(a, (size_t)nseg, (size_t)std::min(K, N));
+    if (rc != ZG_OK) return rc;
+    const unsigned nb = nblocks(a);
+    const int np = probe_count(a, *p);
+    if (np == 0) return afail(a, ZG_ERR_ARG, "no cell centre inside the probe box");
+    CF4 w0{{rho, u, v, pr}};
+
+    // forward with checkpoints at steps 0, K, 2K, ...
+    k_init<<<nb, BLOCK, 0, a->stream>>>(a->g, w0, p->gamma, a->ckpt[0]);
+    ++a->launches;
+    F4 cur = a->ckpt[0];
+    for (int s = 0; s < N; ++s) {
+        bool keep = (s + 1) % K == 0 && (s + 1) / K < nseg;
+        F4 nxt = keep ? a->ckpt[(s + 1) / K] : (cur.f[0] == a->Ua.f[0] ? a->Ub : a->Ua);
+        heun_step(a, *p, cur, a->Ustar, nxt);
+        cur = nxt;
+    }
+    // J and lambda^N
+    cudaMemsetAsync(a->d_acc, 0, 2 * nb * sizeof(double), a->stream);
+    F4 lam = a->lamA, lam_prev = a->lamB;
+    k_probe<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(cur), p->gamma, p->probe[0], p->probe[1], p->probe[2], p->probe[3],
+                                         1.0 / np, a->d_acc, lam, a->d_acc + nb);
+    ++a->launches;
+    double *gacc = a->d_acc + nb;
+
+    // reverse sweep, segment by segment
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int s0 = sg * K, len = std::min(K, N - s0);
+        copy4(a, a->seg[0], a->ckpt[sg]);
+        for (int t = 0; t < len; ++t) heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1]);
+        for (int t = len - 1; t >= 0; --t) {
+            // stage B: lambda* = 1/2 lambda^{n+1} + L'(U*)^T (dt/2 lambda^{n+1})
+            vjp(a, *p, a->segstar[t], lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
+            // stage A: lambda^n = 1/2 lambda^{n+1} + lambda* + L'(U^n)^T (dt lambda*)
+            vjp(a, *p, a->seg[t], a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
+            std::swap(lam, lam_prev);
+        }
+    }
+    k_seed<<<nb, BLOCK, 0, a->stream>>>(a->g, w0, p->gamma, cf(lam), dJ_drho, gacc);
+    ++a->launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return afail(a, ZG_ERR_CUDA, cudaGetErrorString(e));
+    double s2[2];
+    rc = finish_sum(a, s2);
+    if (rc != ZG_OK) return rc;
+    *J = s2[0] / np;
+    if (dJ_dgamma) *dJ_dgamma = s2[1];
+    return ZG_OK;
+}
+
+int zg_adj_cfl_dt(zg_adj *a, double gamma, double CFL, const double *rho, const double *u, const double *v,
+                  const double *pr, double *dt) {
+    if (!a || !rho || !u || !v || !pr || !dt) return ZG_ERR_ARG;
+    DevGuard gd(a->device);
+    size_t n = (size_t)a->g.n;
+    std::vector<double> r(n), uu(n), vv(n), pp(n);
+    const double *src[4] = {rho, u, v, pr};
+    double *dst[4] = {r.data(), uu.data(), vv.data(), pp.data()};
+    for (int k = 0; k < 4; ++k)
+        if (cudaMemcpyAsync(dst[k], src[k], n * sizeof(double), cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+            return afail(a, ZG_ERR_CUDA, "zg_adj_cfl_dt copy");
+    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return afail(a, ZG_ERR_CUDA, "zg_adj_cfl_dt sync");
+    // SmFluid::compute_dt (sm_fluid.cpp:104-114) with the incircle of a
+    // rectangle cell: min(hx, hy) / (|v| + c)
+    double h = std::min(a->g.hx, a->g.hy), best = 1.0e300;
+    for (size_t i = 0; i < n; ++i) {
+        double c = std::sqrt(gamma * pp[i] / r[i]);
+        best = std::min(best, h / (std::sqrt(uu[i] * uu[i] + vv[i] * vv[i]) + c));
+    }
+    *dt = CFL * best;
+    return ZG_OK;
+}
+
+}  // extern "C"
