@@ -14,8 +14,8 @@
 //   lambda^n  = 1/2 lambda^{n+1} + lambda* + L'(U)^T (dt lambda*)
 // and the gamma derivative collects <mu, dL/dgamma> of both stages.  The
 // vector-Jacobian product L'(X)^T mu is two passes: per cell, the four face
-// fluxes' partials with respect to their two face states and gamma (dual
-// numbers through the HLLC formulas) give the cotangents of the cell's face
+// fluxes' partials with respect to their two face states and gamma (the
+// hand-written reverse of the HLLC formulas) give the cotangents of the cell's face
 // states, hence of its primitive state and its two slopes; per cell again,
 // the slopes' partials carry those back to the three cells each slope reads,
 // and the primitive map's partials to U and gamma.  HLLC branches and the
@@ -222,22 +222,21 @@ __global__ void __launch_bounds__(BLOCK) k_probe(Grid g, CF4 U, double gamma, do
     if (lam.f[0]) block_add(gj, gacc);
 }
 
-// --- vector-Jacobian product of L, pass 1: per cell, its four faces ----------
-// mu_eff = coef * mu.  Writes the cotangents of the cell's primitive state
-// (Wb) and slopes (gbx, gby); the gamma part of the faces the cell owns (its
-// high faces) goes to gacc.
+// --- vector-Jacobian product of L, pass 1: per face --------------------------
+// mu_eff = coef * mu.  Each cell takes its two high faces (x and y): the
+// cotangents of the face's low-side and high-side states, in the global
+// primitive frame, go to fb[face][0..3] and fb[face][4..7]; the faces' gamma
+// parts to gacc.
 __global__ void __launch_bounds__(BLOCK) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
-                                                     double coef, F4 Wb, F4 gbx, F4 gby, double *gacc) {
+                                                     double coef, double *fbx, double *fby, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     double gpart = 0.0;
     if (ic < g.n) {
-        const int nb[4] = {xm(g, ic), xp(g, ic), ym(g, ic), yp(g, ic)};
-        double wb[4] = {0.0, 0.0, 0.0, 0.0}, bx[4] = {0.0, 0.0, 0.0, 0.0}, by[4] = {0.0, 0.0, 0.0, 0.0};
         const double cv = coef / g.vol;
 #pragma unroll 1
-        for (int s = 0; s < 4; ++s) {
-            const bool yface = s >= 2, high = (s & 1) == 1;
-            const int lo = high ? ic : nb[s], hi = high ? nb[s] : ic;
+        for (int axis = 0; axis < 2; ++axis) {
+            const bool yface = axis == 1;
+            const int lo = ic, hi = yface ? yp(g, ic) : xp(g, ic);
             const double half_h = 0.5 * (yface ? g.hy : g.hx), S = yface ? g.hx : g.hy;
             // cotangent of the global face flux: L_lo gets -S/V F, L_hi +S/V F
             double mF[4];
@@ -253,51 +252,28 @@ __global__ void __launch_bounds__(BLOCK) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 
                 ml[2] = -mF[1];
                 ml[3] = mF[3];
             }
-            double L[4], R[4];
+            double L[4], R[4], Lb[4], Rb[4];
             face_states(W, yface ? gy : gx, lo, hi, half_h, yface, L, R);
-            Dual<9> dL[4], dR[4], Fl[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                dL[k] = dvar<9>(L[k], k);
-                dR[k] = dvar<9>(R[k], 4 + k);
-            }
-            Dual<9> dg = dvar<9>(gamma, 8);
-            hllc<Dual<9>>(dL, dR, dg, Fl);
-            double bar[9];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) {
-                double a = 0.0;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) a += ml[k] * Fl[k].d[q];
-                bar[q] = a;
-            }
-            if (high) gpart += bar[8];
-            // this cell's side of the face, face frame -> global primitive
-            const double *side = high ? bar : bar + 4;
-            double wl[4];
+            hllc_vjp(L, R, gamma, ml, Lb, Rb, gpart);
+            double *fb = yface ? fby : fbx;
+            const size_t n = (size_t)g.n;
+            // face frame -> global primitive (transpose of face_states' permutation)
             if (!yface) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) wl[k] = side[k];
+                for (int k = 0; k < 4; ++k) {
+                    fb[k * n + ic] = Lb[k];
+                    fb[(4 + k) * n + ic] = Rb[k];
+                }
             } else {
-                wl[0] = side[0];
-                wl[1] = -side[2];
-                wl[2] = side[1];
-                wl[3] = side[3];
+                fb[0 * n + ic] = Lb[0];
+                fb[1 * n + ic] = -Lb[2];
+                fb[2 * n + ic] = Lb[1];
+                fb[3 * n + ic] = Lb[3];
+                fb[4 * n + ic] = Rb[0];
+                fb[5 * n + ic] = -Rb[2];
+                fb[6 * n + ic] = Rb[1];
+                fb[7 * n + ic] = Rb[3];
             }
-            // face state = W_c +- slope_c h/2 (+ on the cell's high face)
-            const double sh = high ? half_h : -half_h;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                wb[k] += wl[k];
-                if (yface) by[k] += sh * wl[k];
-                else bx[k] += sh * wl[k];
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            Wb.f[k][ic] = wb[k];
-            gbx.f[k][ic] = bx[k];
-            gby.f[k][ic] = by[k];
         }
     }
     block_add(gpart, gacc);
@@ -314,36 +290,50 @@ __device__ __forceinline__ void slope_partials(double wm, double w0, double wp, 
 }
 
 // --- vector-Jacobian product of L, pass 2: per cell ----------------------------
-// The slopes of this cell and of its two neighbours on each axis read this
-// cell's primitive state; their cotangents come back here, then through the
-// primitive map to U and gamma.  out = base_coef * base + add + Ubar.
-__global__ void __launch_bounds__(BLOCK) k_vjp_cells(Grid g, CF4 X, CF4 W, double gamma, double eps, CF4 Wb,
-                                                     CF4 gbx, CF4 gby, CF4 base, double base_coef, CF4 add,
-                                                     F4 out, double *gacc) {
+// A cell's state enters the face states of its four faces (as W_c +- slope
+// h/2) and the slopes of itself and of its two neighbours on each axis; the
+// cotangents come back here, then through the primitive map to U and gamma.
+// out = base_coef * base + add + Ubar.
+__global__ void __launch_bounds__(BLOCK) k_vjp_cells(Grid g, CF4 X, CF4 W, double gamma, double eps,
+                                                     const double *fbx, const double *fby, CF4 base,
+                                                     double base_coef, CF4 add, F4 out, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     double gpart = 0.0;
     if (ic < g.n) {
-        const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy;
+        const size_t n = (size_t)g.n;
+        const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy, hx2 = 0.5 * g.hx, hy2 = 0.5 * g.hy;
         const int l = xm(g, ic), r = xp(g, ic), b = ym(g, ic), t = yp(g, ic);
         const int ll = xm(g, l), rr = xp(g, r), bb = ym(g, b), tt = yp(g, t);
         double wt[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
+            // face-state cotangents: low side of the face a cell owns (index
+            // of the low cell), high side of the face below it
+            const double xl_l = fbx[k * n + l], xh_ll = fbx[(4 + k) * n + ll];
+            const double xl_c = fbx[k * n + ic], xh_l = fbx[(4 + k) * n + l];
+            const double xl_r = fbx[k * n + r], xh_c = fbx[(4 + k) * n + ic];
+            const double yl_b = fby[k * n + b], yh_bb = fby[(4 + k) * n + bb];
+            const double yl_c = fby[k * n + ic], yh_b = fby[(4 + k) * n + b];
+            const double yl_t = fby[k * n + t], yh_c = fby[(4 + k) * n + ic];
+            // slope cotangents of l, c, r (x) and b, c, t (y)
+            const double gbl = hx2 * (xl_l - xh_ll), gbc = hx2 * (xl_c - xh_l), gbr = hx2 * (xl_r - xh_c);
+            const double gbb = hy2 * (yl_b - yh_bb), gbcy = hy2 * (yl_c - yh_b), gbt = hy2 * (yl_t - yh_c);
+            double acc = xl_c + xh_l + yl_c + yh_b;
             double w_ll = W.f[k][ll], w_l = W.f[k][l], w_c = W.f[k][ic], w_r = W.f[k][r], w_rr = W.f[k][rr];
             double w_bb = W.f[k][bb], w_b = W.f[k][b], w_t = W.f[k][t], w_tt = W.f[k][tt];
-            double d[3], acc = Wb.f[k][ic];
+            double d[3];
             slope_partials(w_ll, w_l, w_c, i2x, eps, d);  // slope of the left cell: this cell is its wp
-            acc += d[2] * gbx.f[k][l];
+            acc += d[2] * gbl;
             slope_partials(w_l, w_c, w_r, i2x, eps, d);   // own slope
-            acc += d[1] * gbx.f[k][ic];
+            acc += d[1] * gbc;
             slope_partials(w_c, w_r, w_rr, i2x, eps, d);  // right cell: this cell is its wm
-            acc += d[0] * gbx.f[k][r];
+            acc += d[0] * gbr;
             slope_partials(w_bb, w_b, w_c, i2y, eps, d);
-            acc += d[2] * gby.f[k][b];
+            acc += d[2] * gbb;
             slope_partials(w_b, w_c, w_t, i2y, eps, d);
-            acc += d[1] * gby.f[k][ic];
+            acc += d[1] * gbcy;
             slope_partials(w_c, w_t, w_tt, i2y, eps, d);
-            acc += d[0] * gby.f[k][t];
+            acc += d[0] * gbt;
             wt[k] = acc;
         }
         // primitive map (rho, u, v, p)(U, gamma)
@@ -401,8 +391,12 @@ struct zg_adj {
     double *d_all = nullptr;
     size_t cap_ckpt = 0, cap_seg = 0;  // checkpoints and segment states held
     double *d_acc = nullptr;           // per-block accumulators: J, gamma
-    F4 U0{}, Ua{}, Ub{}, Ustar{}, W{}, gx{}, gy{}, Wb{}, gbx{}, gby{}, lamA{}, lamB{}, lamS{};
+    F4 U0{}, Ua{}, Ub{}, Ustar{}, W{}, gx{}, gy{}, lamA{}, lamB{}, lamS{};
+    double *fbx = nullptr, *fby = nullptr;  // face-state cotangents, 8 n each
     std::vector<F4> ckpt, seg, segstar;
+    // primitive states and slopes of both stages of every step of a segment,
+    // kept from the segment's recomputation for the reverse sweep
+    std::vector<F4> segW, segGx, segGy;
     long long launches = 0;
 };
 
@@ -436,7 +430,7 @@ int reserve(zg_adj *a, size_t ckpts, size_t seglen) {
     cudaFree(a->d_all);
     a->d_all = nullptr;
     size_t n = (size_t)a->g.n;
-    size_t fields = 13 * 4 + 4 * ckpts + 4 * (seglen + 1) + 4 * seglen;
+    size_t fields = 10 * 4 + 16 + 4 * ckpts + 4 * (seglen + 1) + 4 * seglen + 3 * 4 * (2 * seglen);
     cudaError_t e = cudaMalloc(&a->d_all, fields * n * sizeof(double));
     if (e != cudaSuccess) return afail(a, ZG_ERR_ALLOC, std::string("adjoint storage: ") + cudaGetErrorString(e));
     double *p = a->d_all;
@@ -448,15 +442,22 @@ int reserve(zg_adj *a, size_t ckpts, size_t seglen) {
         }
         return x;
     };
-    for (F4 *x : {&a->U0, &a->Ua, &a->Ub, &a->Ustar, &a->W, &a->gx, &a->gy, &a->Wb, &a->gbx, &a->gby, &a->lamA,
-                  &a->lamB, &a->lamS})
+    for (F4 *x : {&a->U0, &a->Ua, &a->Ub, &a->Ustar, &a->W, &a->gx, &a->gy, &a->lamA, &a->lamB, &a->lamS})
         *x = take();
+    a->fbx = take().f[0];  // two consecutive groups of 4 n: 8 n
+    take();
+    a->fby = take().f[0];
+    take();
     a->ckpt.assign(ckpts, F4{});
     for (auto &c : a->ckpt) c = take();
     a->seg.assign(seglen + 1, F4{});
     for (auto &c : a->seg) c = take();
     a->segstar.assign(seglen, F4{});
     for (auto &c : a->segstar) c = take();
+    for (auto *v : {&a->segW, &a->segGx, &a->segGy}) {
+        v->assign(2 * seglen, F4{});
+        for (auto &c : *v) c = take();
+    }
     a->cap_ckpt = ckpts;
     a->cap_seg = seglen;
     return ZG_OK;
@@ -467,28 +468,38 @@ void copy4(zg_adj *a, const F4 &dst, const F4 &src) {
         cudaMemcpyAsync(dst.f[k], src.f[k], (size_t)a->g.n * sizeof(double), cudaMemcpyDeviceToDevice, a->stream);
 }
 
-// one Heun step: X -> out (stage value into `star`)
-void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out) {
+struct WG {  // primitive states and slopes of one stage
+    F4 W, gx, gy;
+};
+
+// one Heun step: X -> out (stage value into `star`); the stages' primitive
+// states and slopes go to sa and sb
+void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
+               const WG &sb) {
     unsigned nb = nblocks(a);
-    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, a->W, a->gx, a->gy);
-    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(a->W), cf(a->gx), cf(a->gy), p.gamma, cf(X), kNull, 0.0,
+    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, sa.W, sa.gx, sa.gy);
+    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(sa.W), cf(sa.gx), cf(sa.gy), p.gamma, cf(X), kNull, 0.0,
                                                1.0, p.dt, star);
-    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, a->W, a->gx, a->gy);
-    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(a->W), cf(a->gx), cf(a->gy), p.gamma, cf(star), cf(X), 0.5,
+    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, sb.W, sb.gx, sb.gy);
+    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(sb.W), cf(sb.gx), cf(sb.gy), p.gamma, cf(star), cf(X), 0.5,
                                                0.5, p.dt, out);
     a->launches += 4;
 }
+WG scratch(const zg_adj *a) { return WG{a->W, a->gx, a->gy}; }
+WG seg_stage(const zg_adj *a, int t, int stage) {
+    return WG{a->segW[2 * t + stage], a->segGx[2 * t + stage], a->segGy[2 * t + stage]};
+}
 
-// out = base_coef * base + add + L'(X)^T (coef * mu)
-void vjp(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &mu, double coef, const F4 &base,
+// out = base_coef * base + add + L'(X)^T (coef * mu), with X's primitive
+// states and slopes in wg
+void vjp(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F4 &mu, double coef, const F4 &base,
          double base_coef, const CF4 &add, const F4 &out, double *gacc) {
     unsigned nb = nblocks(a);
-    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, a->W, a->gx, a->gy);
-    k_vjp_faces<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(a->W), cf(a->gx), cf(a->gy), p.gamma, cf(mu), coef, a->Wb,
-                                             a->gbx, a->gby, gacc);
-    k_vjp_cells<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), cf(a->W), p.gamma, p.limiter_eps, cf(a->Wb), cf(a->gbx),
-                                             cf(a->gby), cf(base), base_coef, add, out, gacc);
-    a->launches += 3;
+    k_vjp_faces<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(wg.W), cf(wg.gx), cf(wg.gy), p.gamma, cf(mu), coef, a->fbx,
+                                             a->fby, gacc);
+    k_vjp_cells<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), cf(wg.W), p.gamma, p.limiter_eps, a->fbx, a->fby, cf(base),
+                                             base_coef, add, out, gacc);
+    a->launches += 2;
 }
 
 int check_params(zg_adj *a, const zg_adj_params *p) {
@@ -607,7 +618,7 @@ int zg_adj_forward(zg_adj *a, const zg_adj_params *p, const double *rho, const d
     ++a->launches;
     F4 cur = a->Ua, nxt = a->Ub;
     for (int s = 0; s < p->steps; ++s) {
-        heun_step(a, *p, cur, a->Ustar, nxt);
+        heun_step(a, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
         std::swap(cur, nxt);
     }
     cudaMemsetAsync(a->d_acc, 0, 2 * nb * sizeof(double), a->stream);
@@ -648,7 +659,7 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
     for (int s = 0; s < N; ++s) {
         bool keep = (s + 1) % K == 0 && (s + 1) / K < nseg;
         F4 nxt = keep ? a->ckpt[(s + 1) / K] : (cur.f[0] == a->Ua.f[0] ? a->Ub : a->Ua);
-        heun_step(a, *p, cur, a->Ustar, nxt);
+        heun_step(a, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
         cur = nxt;
     }
     // J and lambda^N
@@ -663,12 +674,13 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * K, len = std::min(K, N - s0);
         copy4(a, a->seg[0], a->ckpt[sg]);
-        for (int t = 0; t < len; ++t) heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1]);
+        for (int t = 0; t < len; ++t)
+            heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1], seg_stage(a, t, 0), seg_stage(a, t, 1));
         for (int t = len - 1; t >= 0; --t) {
             // stage B: lambda* = 1/2 lambda^{n+1} + L'(U*)^T (dt/2 lambda^{n+1})
-            vjp(a, *p, a->segstar[t], lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
+            vjp(a, *p, a->segstar[t], seg_stage(a, t, 1), lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
             // stage A: lambda^n = 1/2 lambda^{n+1} + lambda* + L'(U^n)^T (dt lambda*)
-            vjp(a, *p, a->seg[t], a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
+            vjp(a, *p, a->seg[t], seg_stage(a, t, 0), a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
             std::swap(lam, lam_prev);
         }
     }

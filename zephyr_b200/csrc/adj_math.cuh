@@ -206,5 +206,170 @@ __device__ void hllc(const T L[4], const T R[4], const T &gamma, T F[4]) {
         F[k] = 0.5 * (FL[k] + FR[k] + SL * (QsL[k] - QL[k]) + aSC * (QsL[k] - QsR[k]) + SR * (QsR[k] - QR[k]));
 }
 
+// Reverse of hllc<double>: given the cotangent Fb of the flux, the
+// cotangents of the two face states (Lb, Rb, overwritten) and of gamma
+// (added to gb).  The forward is re-evaluated first; every min / max / abs /
+// branch takes the side the forward took.
+__device__ inline void hllc_vjp(const double L[4], const double R[4], double gamma, const double Fb[4],
+                                double Lb[4], double Rb[4], double &gb) {
+    const double rL = L[0], uL = L[1], vL = L[2], pL = L[3];
+    const double rR = R[0], uR = R[1], vR = R[2], pR = R[3];
+    const double gm1 = gamma - 1.0, igm1 = 1.0 / gm1;
+    const double irL = 1.0 / rL, irR = 1.0 / rR;
+    const double kL = uL * uL + vL * vL, kR = uR * uR + vR * vR;
+    const double rEL = pL * igm1 + 0.5 * (rL * kL), rER = pR * igm1 + 0.5 * (rR * kR);
+    const double xL = gamma * pL * irL, xR = gamma * pR * irR;
+    const double cL = ::sqrt(xL), cR = ::sqrt(xR);
+    const double A = uL - cL, B = uR - cR, C = uL + cL, D = uR + cR;
+    const bool selB = B < A, selD = C < D;  // tmin / tmax choices
+    const double SL = selB ? B : A, SR = selD ? D : C;
+    double rLb = 0.0, uLb = 0.0, vLb = 0.0, pLb = 0.0, rELb = 0.0;
+    double rRb = 0.0, uRb = 0.0, vRb = 0.0, pRb = 0.0, rERb = 0.0;
+    double SLb = 0.0, SRb = 0.0;
+    // reverse of phys_flux(r, u, v, p, rE) scaled by w: F = w * Fb
+    auto phys_rev = [](double r, double u, double v, double p, double rE, const double *Fw, double &rb, double &ub,
+                       double &vb, double &pb, double &rEb) {
+        rb += Fw[0] * u + Fw[1] * (u * u) + Fw[2] * (u * v);
+        ub += Fw[0] * r + Fw[1] * (2.0 * r * u) + Fw[2] * (r * v) + Fw[3] * (rE + p);
+        vb += Fw[2] * (r * u);
+        pb += Fw[1] + Fw[3] * u;
+        rEb += Fw[3] * u;
+    };
+    if (SL >= 0.0) {
+        phys_rev(rL, uL, vL, pL, rEL, Fb, rLb, uLb, vLb, pLb, rELb);
+    } else if (SR <= 0.0) {
+        phys_rev(rR, uR, vR, pR, rER, Fb, rRb, uRb, vRb, pRb, rERb);
+    } else {
+        const double aL = rL * (SL - uL), aR = rR * (SR - uR);
+        const double num = pL - pR + aR * uR - aL * uL, den = aR - aL, iden = 1.0 / den;
+        const double SC = num * iden;
+        const double dLs = SL - SC, dRs = SR - SC, idL = 1.0 / dLs, idR = 1.0 / dRs;
+        const double rsL = aL * idL, rsR = aR * idR;
+        const double EL = rEL * irL, ER = rER * irR;
+        const double iaL = 1.0 / aL, iaR = 1.0 / aR;
+        const double tL = SC - uL, wL = SC + pL * iaL, tR = SC - uR, wR = SC + pR * iaR;
+        const double EsL = EL + tL * wL, EsR = ER + tR * wR;
+        const double QL[4] = {rL, rL * uL, rL * vL, rEL}, QR[4] = {rR, rR * uR, rR * vR, rER};
+        const double QsL[4] = {rsL, rsL * SC, rsL * vL, rsL * EsL}, QsR[4] = {rsR, rsR * SC, rsR * vR, rsR * EsR};
+        const double sgn = SC < 0.0 ? -1.0 : 1.0, aSC = sgn * SC;
+        double half[4], QsLb[4], QsRb[4], QLb[4], QRb[4], aSCb = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            half[k] = 0.5 * Fb[k];
+            SLb += half[k] * (QsL[k] - QL[k]);
+            SRb += half[k] * (QsR[k] - QR[k]);
+            aSCb += half[k] * (QsL[k] - QsR[k]);
+            QsLb[k] = half[k] * (SL + aSC);
+            QsRb[k] = half[k] * (SR - aSC);
+            QLb[k] = -half[k] * SL;
+            QRb[k] = -half[k] * SR;
+        }
+        phys_rev(rL, uL, vL, pL, rEL, half, rLb, uLb, vLb, pLb, rELb);
+        phys_rev(rR, uR, vR, pR, rER, half, rRb, uRb, vRb, pRb, rERb);
+        double SCb = aSCb * sgn;
+        // Qs = (rs, rs SC, rs v, rs Es)
+        double rsLb = QsLb[0] + QsLb[1] * SC + QsLb[2] * vL + QsLb[3] * EsL;
+        double rsRb = QsRb[0] + QsRb[1] * SC + QsRb[2] * vR + QsRb[3] * EsR;
+        SCb += QsLb[1] * rsL + QsRb[1] * rsR;
+        vLb += QsLb[2] * rsL;
+        vRb += QsRb[2] * rsR;
+        const double EsLb = QsLb[3] * rsL, EsRb = QsRb[3] * rsR;
+        // Q = (r, r u, r v, rE)
+        rLb += QLb[0] + QLb[1] * uL + QLb[2] * vL;
+        uLb += QLb[1] * rL;
+        vLb += QLb[2] * rL;
+        rELb += QLb[3];
+        rRb += QRb[0] + QRb[1] * uR + QRb[2] * vR;
+        uRb += QRb[1] * rR;
+        vRb += QRb[2] * rR;
+        rERb += QRb[3];
+        // Es = E + t w,  t = SC - u,  w = SC + p / a,  E = rE / r
+        double aLb = 0.0, aRb = 0.0;
+        {
+            double ELb = EsLb, tLb = EsLb * wL, wLb = EsLb * tL;
+            SCb += tLb + wLb;
+            uLb -= tLb;
+            pLb += wLb * iaL;
+            aLb -= wLb * pL * (iaL * iaL);
+            rELb += ELb * irL;
+            rLb -= ELb * EL * irL;
+            double ERb = EsRb, tRb = EsRb * wR, wRb = EsRb * tR;
+            SCb += tRb + wRb;
+            uRb -= tRb;
+            pRb += wRb * iaR;
+            aRb -= wRb * pR * (iaR * iaR);
+            rERb += ERb * irR;
+            rRb -= ERb * ER * irR;
+        }
+        // rs = a / (S - SC)
+        aLb += rsLb * idL;
+        double dLsb = -rsLb * rsL * idL;
+        SLb += dLsb;
+        SCb -= dLsb;
+        aRb += rsRb * idR;
+        double dRsb = -rsRb * rsR * idR;
+        SRb += dRsb;
+        SCb -= dRsb;
+        // SC = num / den
+        const double numb = SCb * iden, denb = -SCb * SC * iden;
+        aRb += denb;
+        aLb -= denb;
+        pLb += numb;
+        pRb -= numb;
+        aRb += numb * uR;
+        uRb += numb * aR;
+        aLb -= numb * uL;
+        uLb -= numb * aL;
+        // a = r (S - u)
+        rLb += aLb * (SL - uL);
+        SLb += aLb * rL;
+        uLb -= aLb * rL;
+        rRb += aRb * (SR - uR);
+        SRb += aRb * rR;
+        uRb -= aRb * rR;
+    }
+    // SL = min(uL - cL, uR - cR), SR = max(uL + cL, uR + cR)
+    double cLb = 0.0, cRb = 0.0;
+    if (selB) {
+        uRb += SLb;
+        cRb -= SLb;
+    } else {
+        uLb += SLb;
+        cLb -= SLb;
+    }
+    if (selD) {
+        uRb += SRb;
+        cRb += SRb;
+    } else {
+        uLb += SRb;
+        cLb += SRb;
+    }
+    // c = sqrt(gamma p / r)
+    const double xLb = cLb * 0.5 / cL, xRb = cRb * 0.5 / cR;
+    gb += xLb * (pL * irL) + xRb * (pR * irR);
+    pLb += xLb * gamma * irL;
+    rLb -= xLb * xL * irL;
+    pRb += xRb * gamma * irR;
+    rRb -= xRb * xR * irR;
+    // rE = p / (gamma - 1) + r k / 2,  k = u^2 + v^2
+    pLb += rELb * igm1;
+    pRb += rERb * igm1;
+    gb -= (rELb * pL + rERb * pR) * (igm1 * igm1);
+    rLb += rELb * 0.5 * kL;
+    rRb += rERb * 0.5 * kR;
+    uLb += rELb * rL * uL;
+    vLb += rELb * rL * vL;
+    uRb += rERb * rR * uR;
+    vRb += rERb * rR * vR;
+    Lb[0] = rLb;
+    Lb[1] = uLb;
+    Lb[2] = vLb;
+    Lb[3] = pLb;
+    Rb[0] = rRb;
+    Rb[1] = uRb;
+    Rb[2] = vRb;
+    Rb[3] = pRb;
+}
+
 }  // namespace adj
 }  // namespace zg
