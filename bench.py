@@ -337,6 +337,60 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu):
     return out
 
 
+ADJ_SIZE = 1024  # the smooth periodic problem at 1024^2, 100 Heun steps, checkpoints every 10
+
+
+def adjoint_variant(torch, dev, stream, local_rank):
+    """The adjoint mode on the smooth periodic problem: time of one forward
+    run (J) and of one gradient run (J, dJ/drho_0, dJ/dgamma with the
+    checkpointed reverse sweep), and the gradient against central finite
+    differences of the FP64 forward along 16 Gaussian directions (seed 5,
+    eps 1e-6)."""
+    from zephyr_b200.adjoint import Adjoint
+    from zephyr_b200.workloads import fourier_smooth
+    w = fourier_smooth(ADJ_SIZE)
+    r, u, v, p = [torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev) for a in w.state[:4]]
+    adj = Adjoint(ADJ_SIZE, ADJ_SIZE, device=local_rank, stream=stream.cuda_stream)
+    dt = adj.cfl_dt(1.4, 0.4, r, u, v, p)
+    prm = Adjoint.params(steps=100, checkpoint_every=10, dt=dt)
+    grad = torch.empty_like(r)
+    adj.forward(prm, r, u, v, p)
+    adj.gradient(prm, r, u, v, p, grad)
+    torch.cuda.synchronize(dev)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1), out
+
+    n0 = adj.launch_count()
+    ms_f, J = timed(lambda: adj.forward(prm, r, u, v, p))
+    ms_g, (J2, dg) = timed(lambda: adj.gradient(prm, r, u, v, p, grad))
+    launches = adj.launch_count() - n0
+    rng = np.random.default_rng(5)
+    eps = 1e-6
+    errs = []
+    for _ in range(16):
+        d = torch.tensor(rng.standard_normal(ADJ_SIZE * ADJ_SIZE), dtype=torch.float64, device=dev)
+        fd = (adj.forward(prm, r + eps * d, u, v, p) - adj.forward(prm, r - eps * d, u, v, p)) / (2 * eps)
+        ad = float(torch.dot(grad, d))
+        errs.append(abs(fd - ad) / abs(ad))
+    fd_g = (adj.forward(Adjoint.params(steps=100, checkpoint_every=10, dt=dt, gamma=1.4 + eps), r, u, v, p) -
+            adj.forward(Adjoint.params(steps=100, checkpoint_every=10, dt=dt, gamma=1.4 - eps), r, u, v, p)) / (2 * eps)
+    adj.close()
+    return {"workload": f"smooth periodic problem {ADJ_SIZE}x{ADJ_SIZE}, J = mean p over [0.6,0.7]^2 after 100 "
+                        "Heun steps at the CFL 0.4 dt of the initial state, smooth van Albada (eps 1e-8), HLLC",
+            "forward_ms": ms_f, "gradient_ms": ms_g, "adjoint_over_forward": ms_g / ms_f,
+            "checkpoint_every": 10, "J": J, "dJ_dgamma": dg,
+            "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)), "fd_directions": 16,
+            "fd_rel_err_gamma": abs(fd_g - dg) / abs(dg), "gpu_launches": int(launches),
+            "note": "gradient time includes the checkpointed forward, the segment recomputation and the reverse "
+                    "sweep; FD: central differences of the FP64 forward, eps 1e-6, Gaussian directions seed 5"}
+
+
 def _max_over_ranks(torch, vals, dev, world):
     t = torch.tensor(vals, dtype=torch.float64, device=dev)
     if world > 1:
@@ -416,6 +470,7 @@ def run_ours(args, rank, world, local_rank):
 
     mm = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
                     want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
+    adjv = adjoint_variant(torch, dev, stream, local_rank)
 
     vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"]],
                            dev, world)
@@ -446,7 +501,7 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
-                            mm["launches"]),
+                            mm["launches"] + adjv["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
@@ -470,6 +525,7 @@ def run_ours(args, rank, world, local_rank):
                 "step_frac": MM_B_ALG * mm["cells"] * K / (ms_mm / 1e3) / 1e9 / peak,
                 "algorithmic_bytes_per_cell": MM_B_ALG, "gpu_launches": int(mm["launches"]),
                 "kernels": mm["kernels"], "cpu_baseline": mm.get("cpu_baseline")},
+            "adjoint": adjv,
         },
         "dt_last": dt_last,
     }

@@ -14,11 +14,10 @@ def prim(U, gamma):
 
 
 def slope(wm, w0, wp, inv2h, eps):
-    dL, dR = wm - w0, wp - w0
-    a1, a2 = -dL, -dR
-    phiR = (a1 * (a1 + dR) + eps) / (a1 * a1 + dR * dR + eps)
-    phiL = (a2 * (a2 + dL) + eps) / (a2 * a2 + dL * dL + eps)
-    return inv2h * (phiR * dR - phiL * dL)
+    # (phi(-dL, dR) dR - phi(-dR, dL) dL) / (2h) with phi(a, b) = (a (a + b) + eps) / (a^2 + b^2 + eps):
+    # both limiter values share the denominator dL^2 + dR^2 + eps
+    a, b = wm - w0, wp - w0
+    return inv2h * ((a - b) * (2.0 * a * b - eps)) / (a * a + b * b + eps)
 
 
 def phys(r, u, v, p, rE):

@@ -104,8 +104,8 @@ __global__ void __launch_bounds__(BLOCK) k_prim_grad(Grid g, CF4 U, double gamma
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         W.f[k][ic] = wc[k];
-        gx.f[k][ic] = slope<double>(wl[k], wc[k], wr[k], i2x, eps);
-        gy.f[k][ic] = slope<double>(wb[k], wc[k], wt[k], i2y, eps);
+        gx.f[k][ic] = slope(wl[k], wc[k], wr[k], i2x, eps);
+        gy.f[k][ic] = slope(wb[k], wc[k], wt[k], i2y, eps);
     }
 }
 
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(BLOCK) k_probe(Grid g, CF4 U, double gamma, do
 // cotangents of the face's low-side and high-side states, in the global
 // primitive frame, go to fb[face][0..3] and fb[face][4..7]; the faces' gamma
 // parts to gacc.
-__global__ void __launch_bounds__(BLOCK) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
+__global__ void __launch_bounds__(BLOCK, 4) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
                                                      double coef, double *fbx, double *fby, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     double gpart = 0.0;
@@ -279,22 +279,12 @@ __global__ void __launch_bounds__(BLOCK) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 
     block_add(gpart, gacc);
 }
 
-// d slope(wm, w0, wp) / d(wm, w0, wp)
-__device__ __forceinline__ void slope_partials(double wm, double w0, double wp, double inv2h, double eps,
-                                               double d[3]) {
-    Dual<3> a = dvar<3>(wm, 0), b = dvar<3>(w0, 1), c = dvar<3>(wp, 2);
-    Dual<3> s = slope<Dual<3>>(a, b, c, inv2h, eps);
-    d[0] = s.d[0];
-    d[1] = s.d[1];
-    d[2] = s.d[2];
-}
-
 // --- vector-Jacobian product of L, pass 2: per cell ----------------------------
 // A cell's state enters the face states of its four faces (as W_c +- slope
 // h/2) and the slopes of itself and of its two neighbours on each axis; the
 // cotangents come back here, then through the primitive map to U and gamma.
 // out = base_coef * base + add + Ubar.
-__global__ void __launch_bounds__(BLOCK) k_vjp_cells(Grid g, CF4 X, CF4 W, double gamma, double eps,
+__global__ void __launch_bounds__(BLOCK, 5) k_vjp_cells(Grid g, CF4 X, CF4 W, double gamma, double eps,
                                                      const double *fbx, const double *fby, CF4 base,
                                                      double base_coef, CF4 add, F4 out, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
@@ -336,20 +326,16 @@ __global__ void __launch_bounds__(BLOCK) k_vjp_cells(Grid g, CF4 X, CF4 W, doubl
             acc += d[0] * gbt;
             wt[k] = acc;
         }
-        // primitive map (rho, u, v, p)(U, gamma)
-        Dual<5> du[4], dgm = dvar<5>(gamma, 4), dw[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) du[k] = dvar<5>(X.f[k][ic], k);
-        prim<Dual<5>>(du, dgm, dw);
-        double ub[5];
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            double a = 0.0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a += wt[k] * dw[k].d[q];
-            ub[q] = a;
-        }
-        gpart = ub[4];
+        // primitive map rho, u = m_x / rho, v = m_y / rho,
+        // p = (gamma - 1) (E - (m_x^2 + m_y^2) / (2 rho))
+        const double rho = X.f[0][ic], mx = X.f[1][ic], my = X.f[2][ic], E = X.f[3][ic];
+        const double ir = 1.0 / rho, u = mx * ir, v = my * ir, gm1 = gamma - 1.0;
+        double ub[4];
+        ub[0] = wt[0] - wt[1] * u * ir - wt[2] * v * ir + wt[3] * gm1 * 0.5 * (u * u + v * v);
+        ub[1] = wt[1] * ir - wt[3] * gm1 * u;
+        ub[2] = wt[2] * ir - wt[3] * gm1 * v;
+        ub[3] = wt[3] * gm1;
+        gpart = wt[3] * (E - 0.5 * ((mx * mx + my * my) * ir));
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             double v = ub[k];
@@ -474,16 +460,19 @@ struct WG {  // primitive states and slopes of one stage
 
 // one Heun step: X -> out (stage value into `star`); the stages' primitive
 // states and slopes go to sa and sb
+// (need_out = false: the step's result is not wanted, only its stages)
 void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
-               const WG &sb) {
+               const WG &sb, bool need_out = true) {
     unsigned nb = nblocks(a);
     k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, sa.W, sa.gx, sa.gy);
     k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(sa.W), cf(sa.gx), cf(sa.gy), p.gamma, cf(X), kNull, 0.0,
                                                1.0, p.dt, star);
     k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, sb.W, sb.gx, sb.gy);
+    a->launches += 3;
+    if (!need_out) return;
     k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(sb.W), cf(sb.gx), cf(sb.gy), p.gamma, cf(star), cf(X), 0.5,
                                                0.5, p.dt, out);
-    a->launches += 4;
+    ++a->launches;
 }
 WG scratch(const zg_adj *a) { return WG{a->W, a->gx, a->gy}; }
 WG seg_stage(const zg_adj *a, int t, int stage) {
@@ -652,11 +641,20 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
     if (np == 0) return afail(a, ZG_ERR_ARG, "no cell centre inside the probe box");
     CF4 w0{{rho, u, v, pr}};
 
-    // forward with checkpoints at steps 0, K, 2K, ...
+    // forward with checkpoints at steps 0, K, 2K, ...; the last segment keeps
+    // its states and stages for the reverse sweep
+    const int last0 = (nseg - 1) * K;
     k_init<<<nb, BLOCK, 0, a->stream>>>(a->g, w0, p->gamma, a->ckpt[0]);
     ++a->launches;
     F4 cur = a->ckpt[0];
     for (int s = 0; s < N; ++s) {
+        if (s >= last0) {
+            const int t = s - last0;
+            if (t == 0) copy4(a, a->seg[0], cur);
+            heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1], seg_stage(a, t, 0), seg_stage(a, t, 1));
+            cur = a->seg[t + 1];
+            continue;
+        }
         bool keep = (s + 1) % K == 0 && (s + 1) / K < nseg;
         F4 nxt = keep ? a->ckpt[(s + 1) / K] : (cur.f[0] == a->Ua.f[0] ? a->Ub : a->Ua);
         heun_step(a, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
@@ -673,9 +671,12 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
     // reverse sweep, segment by segment
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * K, len = std::min(K, N - s0);
-        copy4(a, a->seg[0], a->ckpt[sg]);
-        for (int t = 0; t < len; ++t)
-            heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1], seg_stage(a, t, 0), seg_stage(a, t, 1));
+        if (sg != nseg - 1) {  // recompute the segment from its checkpoint
+            copy4(a, a->seg[0], a->ckpt[sg]);
+            for (int t = 0; t < len; ++t)
+                heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1], seg_stage(a, t, 0), seg_stage(a, t, 1),
+                          t + 1 < len);
+        }
         for (int t = len - 1; t >= 0; --t) {
             // stage B: lambda* = 1/2 lambda^{n+1} + L'(U*)^T (dt/2 lambda^{n+1})
             vjp(a, *p, a->segstar[t], seg_stage(a, t, 1), lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);

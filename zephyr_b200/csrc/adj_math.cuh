@@ -149,14 +149,26 @@ __device__ __forceinline__ void prim(const T U[4], const T &gamma, T W[4]) {
     W[3] = (gamma - 1.0) * (U[3] - 0.5 * ((U[1] * U[1] + U[2] * U[2]) / U[0]));
 }
 
-// limited slope of one field along one axis from its three values
-template <class T>
-__device__ __forceinline__ T slope(const T &wm, const T &w0, const T &wp, double inv2h, double eps) {
-    T dL = wm - w0, dR = wp - w0;
-    T a1 = -dL, a2 = -dR;
-    T phiR = (a1 * (a1 + dR) + eps) / (a1 * a1 + dR * dR + eps);  // phi(-dL, dR)
-    T phiL = (a2 * (a2 + dL) + eps) / (a2 * a2 + dL * dL + eps);  // phi(-dR, dL)
-    return inv2h * (phiR * dR - phiL * dL);
+// limited slope of one field along one axis from its three values:
+//   (phi(-dL, dR) dR - phi(-dR, dL) dL) / (2h)
+// where both limiter values share the denominator dL^2 + dR^2 + eps, so that
+//   = (dL - dR) (2 dL dR - eps) / (dL^2 + dR^2 + eps) / (2h).
+__device__ __forceinline__ double slope(double wm, double w0, double wp, double inv2h, double eps) {
+    double a = wm - w0, b = wp - w0;
+    return inv2h * ((a - b) * (2.0 * a * b - eps)) / (a * a + b * b + eps);
+}
+// its partial derivatives with respect to (wm, w0, wp)
+__device__ __forceinline__ void slope_partials(double wm, double w0, double wp, double inv2h, double eps,
+                                               double d[3]) {
+    double a = wm - w0, b = wp - w0;
+    double q = 2.0 * a * b - eps, P = (a - b) * q;
+    double iD = 1.0 / (a * a + b * b + eps);
+    double Pa = q + (a - b) * (2.0 * b), Pb = -q + (a - b) * (2.0 * a);
+    double ga = inv2h * (Pa - P * (2.0 * a) * iD) * iD;
+    double gb = inv2h * (Pb - P * (2.0 * b) * iD) * iD;
+    d[0] = ga;
+    d[1] = -(ga + gb);
+    d[2] = gb;
 }
 
 // physical flux of a face-frame primitive state (models.cpp:131-137)
