@@ -337,6 +337,157 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu):
     return out
 
 
+AMR_BASE = 512         # quadtree AMR blast: base mesh cells per side
+AMR_LEVELS = 3         # refinement levels above the base
+AMR_CAPACITY = 8 << 20  # device room for cells (live + those held during a refine)
+AMR_WARM_STEPS = 100   # untimed steps (adapting every AMR_EVERY) before the timed window
+AMR_TIMED_STEPS = 400  # steps 100 to 500
+AMR_EVERY = 10         # set_flags + refine every AMR_EVERY steps
+AMR_B_ALG = 160 + 36   # bytes per cell-update: the FP64 two-stage step plus the slot-mesh neighbour indices
+AMR_CELL_BYTES = 600   # bytes of one cell's AmrCells arrays (63 doubles, 22 ints, 16 bytes)
+
+
+def _amr_setup(Z, init_state, mesh, solver):
+    """smf_test_2D.cpp:112-117: max_level + 3 rounds of (initial data by cell
+    means, set_flags, refine), then the initial data once more."""
+    for _ in range(AMR_LEVELS + 3):
+        g = init_state()
+        mesh.set_state(*g)
+        solver.set_flags(mesh, download=False)
+        mesh.refine()
+    mesh.set_state(*init_state())
+
+
+def amr_cpu_reference(budget_s=12.0):
+    """The reference's own EuMesh / SmFluid (oracle/_ref) on this host's
+    cores: the same setup, then steps with an adaptation every AMR_EVERY
+    steps; None when that build is absent."""
+    from oracle import ref_mesh as RM
+    from zephyr_b200.workloads import blast_cell_means
+    if not RM.available():
+        return None
+    threads = os.cpu_count() or 1
+    RM.lib().zm_threads(threads)
+    r = RM.RefEuMesh(AMR_BASE, AMR_BASE, bounds=(2, 2, 2, 2), accuracy=2, limiter="van Albada 1", CFL=0.4,
+                     max_level=AMR_LEVELS, distributor="slope")
+
+    def init():
+        vx, vy = r.verts()
+        return blast_cell_means(vx, vy)
+
+    for _ in range(AMR_LEVELS + 3):
+        r.set_state(*init())
+        r.solver_flags()
+        r.refine()
+    r.set_state(*init())
+    t0 = time.perf_counter()
+    updates, steps = 0, 0
+    while steps < AMR_EVERY or (time.perf_counter() - t0 < budget_s and steps < 4 * AMR_EVERY):
+        updates += r.n
+        r.step()
+        steps += 1
+        if steps % AMR_EVERY == 0:
+            r.solver_flags()
+            r.refine()
+    sec = time.perf_counter() - t0
+    RM.lib().zm_threads(0)
+    return {"value": updates / sec, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": f"steps 0-{steps} after the initial adaptation ({r.n} live cells at the end), "
+                      f"set_flags + refine every {AMR_EVERY} steps; zephyr's EuMesh / SmFluid compiled from its "
+                      f"sources (oracle/_ref); {threads} std::threads"}
+
+
+def amr_variant(torch, lib, dev, stream, local_rank, want_cpu):
+    """The quadtree AMR blast: base 512^2, 3 levels, the reference's
+    SmFluid::set_flags criterion and slope distributor, adaptation every 10
+    steps, the PARITY FP64 step on the slot mesh (bit-exact with the
+    reference).  Times steps 100-500 including every set_flags + refine."""
+    import zephyr_b200 as Z
+    from zephyr_b200._lib import KERNEL_KINDS
+    from zephyr_b200.workloads import blast_cell_means
+    gen = Z.Rectangle(0.0, 1.0, 0.0, 1.0)
+    gen.set_boundaries(Z.Boundaries(Z.Boundary.ZOE, Z.Boundary.ZOE, Z.Boundary.ZOE, Z.Boundary.ZOE))
+    gen.set_sizes(AMR_BASE, AMR_BASE)
+    mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
+    mesh.set_max_level(AMR_LEVELS, AMR_CAPACITY)
+    solver = Z.SmFluid(Z.IdealGas(1.4))
+    solver.add_types(mesh)
+    solver.set_accuracy(2)
+    solver.set_CFL(0.4)
+    solver.set_limiter("van Albada 1")
+    solver.set_method(Z.Fluxes.HLLC)
+    mesh.set_distributor(solver.distributor("slope"))
+
+    def init():
+        g = mesh.amr_arrays()
+        return blast_cell_means(g["vx"], g["vy"])
+
+    _amr_setup(Z, init, mesh, solver)
+    for s in range(AMR_WARM_STEPS):
+        solver.update(mesh)
+        if (s + 1) % AMR_EVERY == 0:
+            solver.set_flags(mesh, download=False)
+            mesh.refine()
+    torch.cuda.synchronize(dev)
+    lib.zg_set_timing(mesh.ctx, 1)
+    n0 = mesh.launch_count()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    e0, e1 = ev(), ev()
+    adapt_ev = []
+    live, held = [], []
+    e0.record(stream)
+    for s in range(AMR_TIMED_STEPS):
+        live.append(mesh.n_cells())
+        solver.update(mesh)
+        if (s + 1) % AMR_EVERY == 0:
+            a0, a1 = ev(), ev()
+            a0.record(stream)
+            solver.set_flags(mesh, download=False)
+            mesh.refine()
+            a1.record(stream)
+            adapt_ev.append((a0, a1))
+            st = mesh.amr_info()
+            held.append((st.n_before, st.n_large))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    adapt_ms = [a.elapsed_time(b) for a, b in adapt_ev]
+    launches = mesh.launch_count() - n0
+    kms = (C.c_double * len(KERNEL_KINDS))()
+    kcount = (C.c_longlong * len(KERNEL_KINDS))()
+    lib.zg_kernel_times(mesh.ctx, kms, kcount)
+    lib.zg_set_timing(mesh.ctx, 0)
+    kernels = {name: {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k]}
+               for k, name in enumerate(KERNEL_KINDS) if kcount[k]}
+    solver.dt()
+    mesh.close()
+    updates = int(sum(live))
+    step_ms = ms - sum(adapt_ms)
+    refine_bytes = sum(AMR_CELL_BYTES * (a + b) for a, b in held)
+    out = {
+        "workload": f"AMR blast, base {AMR_BASE}x{AMR_BASE}, max_level {AMR_LEVELS}, ZOE; rho = 1, u = v = 0, "
+                    f"p = 1e-5 except p = 1e3 for r < 0.01 at (0.5, 0.5), 20x20 sub-sampled cell means",
+        "form": "FP64 PARITY kernels on the slot mesh, bit-exact with the reference (SmFluid second order, "
+                "predictor-corrector, HLLC, van Albada 1, CFL 0.4; set_flags criterion; slope distributor)",
+        "value": updates / (ms / 1e3), "unit": METRIC, "timed_steps": AMR_TIMED_STEPS,
+        "window": f"steps {AMR_WARM_STEPS}-{AMR_WARM_STEPS + AMR_TIMED_STEPS}", "adapt_every": AMR_EVERY,
+        "ms_total": ms, "ms_per_step_incl_adapt": ms / AMR_TIMED_STEPS,
+        "step_only_value": updates / (step_ms / 1e3),
+        "adapt_ms_avg": sum(adapt_ms) / max(len(adapt_ms), 1), "adaptations": len(adapt_ms),
+        "live_cells": {"min": min(live), "max": max(live), "mean": updates / len(live)},
+        "cells_held_max": max(b for _, b in held) if held else None,
+        "refine_GBs": refine_bytes / (sum(adapt_ms) / 1e3) / 1e9 if adapt_ms else None,
+        "refine_bytes_rule": f"{AMR_CELL_BYTES} B per cell over the cells before plus the cells held "
+                             "(all cell and face arrays read once, new arrays written once)",
+        "algorithmic_bytes_per_cell_update": AMR_B_ALG,
+        "step_achieved_GBs": AMR_B_ALG * updates / (step_ms / 1e3) / 1e9,
+        "gpu_launches": int(launches), "kernels": kernels,
+    }
+    if want_cpu:
+        out["cpu_baseline"] = amr_cpu_reference()
+    return out
+
+
 ADJ_SIZE = 1024  # the smooth periodic problem at 1024^2, 100 Heun steps, checkpoints every 10
 
 
@@ -471,10 +622,13 @@ def run_ours(args, rank, world, local_rank):
     mm = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
                     want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     adjv = adjoint_variant(torch, dev, stream, local_rank)
+    amr = amr_variant(torch, lib, dev, stream, local_rank,
+                      want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
 
-    vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"]],
-                           dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm = vals
+    vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
+                                   amr["ms_total"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr = vals
+    amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
     for v in variants.values():
         v["mesh"].close()
     if rank != 0:
@@ -501,7 +655,7 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
-                            mm["launches"] + adjv["gpu_launches"]),
+                            mm["launches"] + adjv["gpu_launches"] + amr["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
@@ -526,6 +680,7 @@ def run_ours(args, rank, world, local_rank):
                 "algorithmic_bytes_per_cell": MM_B_ALG, "gpu_launches": int(mm["launches"]),
                 "kernels": mm["kernels"], "cpu_baseline": mm.get("cpu_baseline")},
             "adjoint": adjv,
+            "amr": amr,
         },
         "dt_last": dt_last,
     }

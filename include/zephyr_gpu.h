@@ -156,6 +156,66 @@ typedef struct zg_mesh_view {
  * zg_mesh_rectangle. */
 int zg_mesh_upload(zg_ctx *ctx, const zg_mesh_view *mesh);
 
+/* ---- Adaptive mesh on the device ------------------------------------------
+ * A rectangle mesh made adaptive keeps zephyr's AmrCells layout on the GPU
+ * (9 map points, level, z-index and 8 face slots per cell) with room for
+ * `capacity` cells.  The step then runs the PARITY kernels over the face
+ * slots, and zg_amr_refine adapts the mesh to the cells' flags on the GPU.
+ * Cell order, geometry, connectivity and distributed states match the
+ * reference's EuMesh::refine on one rank bit for bit. */
+
+/* State distributors of SmFluid::distributor(type) (sm_fluid.cpp:372-470). */
+enum zg_distributor { ZG_DISTR_CONST = 0, ZG_DISTR_SLOPE = 1 };
+
+/* Make the mesh of zg_mesh_rectangle adaptive with levels up to max_level
+ * (clamped to [0, 15] like EuMesh::set_max_level, eu_mesh.cpp:178-184) and
+ * device room for `capacity` cells; builds the base cells of
+ * AmrCells(const Rectangle&) (amr_cells_gen.cpp:128-281).  Call before
+ * zg_smf_configure.  Periodic boundaries are rejected: the reference's
+ * EuMesh::init_amr fails on them ("Invalid rotation", mesh/amr/rotations.h).
+ * The distributor starts as SLOPE, SmFluid::distributor's default type. */
+int zg_amr_enable(zg_ctx *ctx, int max_level, int capacity);
+
+/* EuMesh::set_distributor(solver.distributor(type)) (eu_mesh.cpp:194-196). */
+int zg_amr_set_distributor(zg_ctx *ctx, int kind);
+
+/* Set the adaptation flag of every cell from a host array of n_cells ints
+ * (EuCell::set_flag).  zg_smf_set_flags writes the same flags on the device
+ * (and may then be given a NULL host array); on an adaptive mesh it also
+ * computes the limited gradients the SLOPE distributor uses, as
+ * SmFluid::set_flags does (sm_fluid.cpp:517-522). */
+int zg_amr_put_flags(zg_ctx *ctx, const int *flags);
+
+/* Adapt the mesh to the flags; replaces EuMesh::refine (eu_mesh.cpp:290-359):
+ * flag balancing, split and merge of cells with their hanging faces, the
+ * distributor's states for new cells, compaction.  zg_mesh_n_cells gives the
+ * new number of cells.  ZG_ERR_TOO_LARGE when the adaptation needs more than
+ * `capacity` cells while it runs (the mesh is then unchanged; the flags are
+ * balanced). Synchronises the stream. */
+int zg_amr_refine(zg_ctx *ctx);
+
+/* Counts of the last zg_amr_refine. */
+typedef struct zg_amr_stats {
+    int max_level, capacity;
+    int n_before, n_after;   /* cells before / after */
+    int n_coarse, n_refine;  /* cells merged into parents / split into children */
+    int n_large;             /* cells held while the adaptation ran */
+} zg_amr_stats;
+int zg_amr_info(const zg_ctx *ctx, zg_amr_stats *out);
+
+/* Host copies of the adaptive mesh's arrays; NULL members are skipped.
+ * map_x, map_y: the 9 points of each cell's SqQuad map, point k of cell i at
+ * 9 i + k with k = 3 (y + 1) + (x + 1) for the map coordinates x, y in
+ * {-1, 0, 1}.  Face slots as in zg_mesh_view. */
+typedef struct zg_amr_cells {
+    double *center_x, *center_y, *volume, *incircle; /* n_cells each */
+    double *map_x, *map_y;                           /* 9 * n_cells */
+    int *level, *flag, *b_idx, *z_idx;               /* n_cells */
+    int *face_boundary, *face_neib;                  /* 8 * n_cells */
+    double *face_nx, *face_ny, *face_cx, *face_cy, *face_area; /* 8 * n_cells */
+} zg_amr_cells;
+int zg_amr_download(zg_ctx *ctx, const zg_amr_cells *out);
+
 /* Configure the solver; replaces SmFluid(eos) and its setters.  The first
  * call allocates the solver's fields (SmFluid::add_types, sm_fluid.cpp:25-35)
  * with zero state and isolation counters; later calls only change the

@@ -43,10 +43,13 @@ def lib():
         L.zm_step.restype = C.c_double
         L.zm_solver_flags.argtypes = [C.c_void_p, _I]
         L.zm_put_flags.argtypes = [C.c_void_p, _I]
+        L.zm_grad.argtypes = [C.c_void_p, _P, _P]
         L.zm_refine.argtypes = [C.c_void_p]
         L.zm_refine.restype = C.c_int
         L.zm_check.argtypes = [C.c_void_p]
         L.zm_check.restype = C.c_int
+        L.zm_check_refined.argtypes = [C.c_void_p]
+        L.zm_check_refined.restype = C.c_int
         L.zm_threads(0)
         _lib = L
     return _lib
@@ -90,6 +93,13 @@ class RefEuMesh:
             raise RuntimeError("cells without 8 face slots")
         return dict(boundary=boundary, neib=neib, area=area, nx=nx, ny=ny, fx=fx, fy=fy)
 
+    def verts(self):
+        """The 9 map points of every cell (x, y), 9 n each."""
+        n = self.n
+        vx, vy = np.empty(9 * n), np.empty(9 * n)
+        lib().zm_verts(self.h, _dp(vx), _dp(vy))
+        return vx, vy
+
     def mesh_arrays(self):
         g = self.cells()
         g.update(self.faces())
@@ -131,7 +141,18 @@ class RefEuMesh:
     def check(self):
         return lib().zm_check(self.h)
 
+    def check_refined(self):
+        return lib().zm_check_refined(self.h)
+
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.zm_free(self.h)
             self.h = None
+
+
+def grad_of(mesh: "RefEuMesh"):
+    """d_dx, d_dy (density, vx, vy, pressure) as (4, n) arrays."""
+    n = mesh.n
+    gx, gy = np.empty(4 * n), np.empty(4 * n)
+    lib().zm_grad(mesh.h, _dp(gx), _dp(gy))
+    return gx.reshape(4, n), gy.reshape(4, n)

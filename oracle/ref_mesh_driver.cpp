@@ -178,6 +178,23 @@ void zm_solver_flags(void *p, int *flags) {
     for (int i = 0; i < (int)c.size(); ++i) flags[i] = c.flag[i];
 }
 
+// The limited gradients SmFluid::compute_grad left in d_dx, d_dy: density,
+// velocity x, velocity y, pressure (4 n each, field-major).
+void zm_grad(void *p, double *gx, double *gy) {
+    auto *r = static_cast<RefMesh *>(p);
+    int n = (int)r->mesh->n_cells();
+    for (int ic = 0; ic < n; ++ic) {
+        EuCell cell = (*r->mesh)[ic];
+        const PState &dx = cell[r->part.d_dx], &dy = cell[r->part.d_dy];
+        const double vx[4] = {dx.density, dx.velocity.x(), dx.velocity.y(), dx.pressure};
+        const double vy[4] = {dy.density, dy.velocity.x(), dy.velocity.y(), dy.pressure};
+        for (int k = 0; k < 4; ++k) {
+            gx[(size_t)k * n + ic] = vx[k];
+            gy[(size_t)k * n + ic] = vy[k];
+        }
+    }
+}
+
 // Flags chosen by the caller (tests of refine on arbitrary flags).
 void zm_put_flags(void *p, const int *flags) {
     auto &c = static_cast<RefMesh *>(p)->mesh->locals();
@@ -193,5 +210,9 @@ int zm_refine(void *p) {
 
 // EuMesh::check_base (eu_mesh.cpp:585-679): 0 when the mesh is consistent.
 int zm_check(void *p) { return static_cast<RefMesh *>(p)->mesh->check_base() < 0 ? -1 : 0; }
+
+// EuMesh::check_refined (eu_mesh.cpp:681-): 0 when an adapted mesh is
+// consistent (hanging faces allowed).
+int zm_check_refined(void *p) { return static_cast<RefMesh *>(p)->mesh->check_refined() < 0 ? -1 : 0; }
 
 }  // extern "C"

@@ -148,6 +148,26 @@ def make_amr(name, n, acc, limiter, bounds, max_level, steps, adapt_rounds):
                                              "neib", "nx", "ny", "fx", "fy", "area")})
 
 
+def make_amr_cycle(name, n, bounds, max_level, distributor, acc, limiter, cycles, steps_per_cycle, random_rounds):
+    """The reference's EuMesh / SmFluid through one adaptation schedule
+    (tests/amr_cycle.py): set_flags, refine and steps with the solver's
+    distributor, then refines with random flags.  Stores the digests of the
+    mesh, state and flags after every call."""
+    import json
+    from oracle import ref_mesh as RM
+    sys.path.insert(0, str(ROOT / "tests"))
+    import amr_cycle as AC
+    R = RM.RefEuMesh(n, n, bounds=bounds, accuracy=acc, limiter=limiter, CFL=0.4, max_level=max_level,
+                     distributor=distributor)
+    ad = AC.RefAdapter(R)
+    ops = AC.schedule(cycles, steps_per_cycle, random_rounds)
+    log = AC.run(ad, ops)
+    np.savez_compressed(OUT / f"{name}.npz", n=n, bounds=np.array(bounds), max_level=max_level,
+                        distributor=distributor, accuracy=acc, limiter=limiter, CFL=0.4, cycles=cycles,
+                        steps_per_cycle=steps_per_cycle, random_rounds=random_rounds, log=json.dumps(log))
+    return log
+
+
 MM_MATERIALS = "stiffened:Water,ideal:Air"
 
 
@@ -247,10 +267,25 @@ def main():
     make_mm("mm_shock_column_24_vs", 24, 3, 120)
     make_mm_pointwise()
     print("wrote multi-material cases")
+    make_amr_cycles()
+
+
+AMR_CYCLES = {
+    "adapt_cycle_16_slope_mc": (16, (2, 1, 1, 2), 3, "slope", 2, "MC", 8, 2, 6),
+    "adapt_cycle_14_const_first_order": (14, (1, 2, 2, 1), 2, "const", 1, "MC", 6, 3, 5),
+}
+
+
+def make_amr_cycles():
+    for name, spec in AMR_CYCLES.items():
+        log = make_amr_cycle(name, *spec)
+        print("wrote", name, "cells", [e[1] for e in log if "refine" in e[0] or "random" in e[0]])
 
 
 if __name__ == "__main__":
-    if "--mm" in sys.argv:
+    if "--amr-cycle" in sys.argv:
+        make_amr_cycles()
+    elif "--mm" in sys.argv:
         make_mm("mm_shock_column_32_plic", 32, 4, 200)
         make_mm("mm_shock_column_24_hllc", 24, 0, 120)
         make_mm("mm_shock_column_24_vs", 24, 3, 120)

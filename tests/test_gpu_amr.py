@@ -1,0 +1,169 @@
+"""Adaptation on the GPU (zg_amr_*): the base mesh of an adaptive rectangle,
+and schedules of SmFluid::set_flags / EuMesh::refine / SmFluid::update with
+random flag rounds, bit-exact with the reference's EuMesh::refine on one rank
+(cell order, levels, z-indices, map points, geometry, face slots and
+neighbours, distributed states, isolation counters, flags and dt).
+
+Pinned by the digests of tests/golden/adapt_cycle_*.npz (made by the
+reference, tests/golden/make_golden.py); where the reference's build
+oracle/_ref/libzref_mesh.so is present, the same schedules (and a larger
+one) also run side by side with it, array by array."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import amr_cycle as AC
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CYCLE_CASES = sorted(p.stem for p in GOLDEN.glob("adapt_cycle_*.npz"))
+
+
+def ref_available():
+    from oracle import ref_mesh as RM
+    return RM.available()
+
+
+def gpu_mesh(n, bounds, max_level, distributor, acc, limiter, CFL, capacity=None, ny=None):
+    import zephyr_b200 as Z
+    gen = Z.Rectangle(0.0, 1.0, 0.0, 1.0)
+    gen.set_boundaries(Z.Boundaries(*bounds))
+    gen.set_sizes(n, ny or n)
+    mesh = Z.EuMesh(gen)
+    mesh.set_max_level(max_level, capacity)
+    solver = Z.SmFluid(Z.IdealGas(1.4))
+    solver.add_types(mesh)
+    solver.set_accuracy(acc)
+    solver.set_limiter(limiter)
+    solver.set_CFL(CFL)
+    mesh.set_distributor(solver.distributor(distributor))
+    return mesh, solver
+
+
+def compare_live(label, ref_ad, gpu_ad, g_gpu):
+    g_ref = ref_ad.mesh()
+    assert ref_ad.n() == gpu_ad.n(), (label, ref_ad.n(), gpu_ad.n())
+    a, b = AC.canonical(g_ref), AC.canonical(g_gpu)
+    for k in AC.MESH_KEYS:
+        if not np.array_equal(a[k], b[k]):
+            i = int(np.argmax(a[k] != b[k]))
+            raise AssertionError(f"{label}: {k} differs first at {i}: ref {a[k][i]!r} gpu {b[k][i]!r}")
+    sr, sg = ref_ad.state(), gpu_ad.state()
+    for k in AC.STATE_KEYS:
+        if not np.array_equal(sr[k], sg[k]):
+            i = int(np.argmax(sr[k] != sg[k]))
+            raise AssertionError(f"{label}: state {k} differs first at {i}: ref {sr[k][i]!r} gpu {sg[k][i]!r}")
+
+
+@pytest.mark.parametrize("case", CYCLE_CASES)
+def test_adaptation_schedule_matches_reference_digests(gpu_lib, case):
+    z = np.load(GOLDEN / f"{case}.npz")
+    want = json.loads(str(z["log"]))
+    mesh, solver = gpu_mesh(int(z["n"]), tuple(int(b) for b in z["bounds"]), int(z["max_level"]),
+                            str(z["distributor"]), int(z["accuracy"]), str(z["limiter"]), float(z["CFL"]))
+    ops = AC.schedule(int(z["cycles"]), int(z["steps_per_cycle"]), int(z["random_rounds"]))
+    got = AC.run(AC.GpuAdapter(mesh, solver), ops)
+    assert len(got) == len(want)
+    for g, w in zip(got, want):
+        label = w[0]
+        assert g[0] == label
+        assert g[1] == w[1], (label, "cells", g[1], w[1])
+        bad = [k for k in w[2] if g[2][k] != w[2][k]]
+        assert not bad, (label, "mesh arrays differ", bad)
+        bad = [k for k in w[3] if g[3][k] != w[3][k]]
+        assert not bad, (label, "state arrays differ", bad)
+        assert g[4] == w[4], (label, g[4], w[4])
+    mesh.close()
+
+
+@pytest.mark.parametrize("n,ny,bounds,max_level,distributor,acc,limiter,cycles,steps,rand", [
+    (16, None, (2, 1, 1, 2), 3, "slope", 2, "MC", 8, 2, 6),
+    (40, 28, (2, 2, 1, 1), 3, "slope", 2, "van Albada", 10, 2, 4),
+    (24, None, (1, 1, 1, 1), 4, "const", 1, "MC", 6, 3, 6),
+])
+def test_adaptation_side_by_side_with_reference(gpu_lib, n, ny, bounds, max_level, distributor, acc, limiter,
+                                                cycles, steps, rand):
+    if not ref_available():
+        pytest.skip("the reference's build (oracle/_ref/libzref_mesh.so) is not present; the digest test pins it")
+    from oracle import ref_mesh as RM
+    ref = RM.RefEuMesh(n, ny or n, bounds=bounds, accuracy=acc, limiter=limiter, CFL=0.4, max_level=max_level,
+                       distributor=distributor)
+    ref_ad = AC.RefAdapter(ref)
+    mesh, solver = gpu_mesh(n, bounds, max_level, distributor, acc, limiter, 0.4, ny=ny)
+    gpu_ad = AC.GpuAdapter(mesh, solver)
+    g0 = gpu_ad.mesh()
+    s0 = AC.init_state(g0["cx"], g0["cy"])
+    ref_ad.set_state(*s0)
+    gpu_ad.set_state(*s0)
+    compare_live("base", ref_ad, gpu_ad, g0)
+    for k, op in enumerate(AC.schedule(cycles, steps, rand, seed=7)):
+        if op == "set_flags":
+            fr, fg = ref_ad.set_flags(), gpu_ad.set_flags()
+            assert np.array_equal(fr, fg), (k, "flags")
+        elif op == "refine":
+            ref_ad.refine()
+            gpu_ad.refine()
+        elif op == "step":
+            assert ref_ad.step() == gpu_ad.step(), (k, "dt")
+        else:
+            f = AC.random_flags(ref_ad.n(), int(op.split(":")[1]))
+            ref_ad.put_flags(f)
+            gpu_ad.put_flags(f)
+            ref_ad.refine()
+            gpu_ad.refine()
+        compare_live(f"{k}:{op}", ref_ad, gpu_ad, gpu_ad.mesh())
+    mesh.close()
+
+
+def test_capacity_overflow_leaves_the_mesh_unchanged(gpu_lib):
+    import zephyr_b200 as Z
+    n = 12
+    mesh, solver = gpu_mesh(n, (2, 2, 2, 2), 2, "slope", 2, "MC", 0.4, capacity=n * n + 30)
+    g = mesh.amr_arrays()
+    mesh.set_state(*AC.init_state(g["cx"], g["cy"]))
+    before = AC.digest(AC.canonical(mesh.amr_arrays()))
+    state = mesh.get_state()
+    mesh.put_flags(np.ones(n * n, np.int32))  # 4 children per cell: far above the capacity
+    with pytest.raises(Z.ZgError) as e:
+        mesh.refine()
+    assert e.value.code == -6
+    assert mesh.n_cells() == n * n
+    after = AC.canonical(mesh.amr_arrays())
+    after.pop("flag")
+    before.pop("flag")
+    assert AC.digest(after) == before
+    assert all(np.array_equal(a, b) for a, b in zip(state, mesh.get_state()))
+    # a refine that fits still works afterwards
+    f = np.zeros(n * n, np.int32)
+    f[5] = 1
+    mesh.put_flags(f)
+    mesh.refine()
+    assert mesh.n_cells() == n * n + 3
+    st = mesh.amr_info()
+    assert (st.n_before, st.n_after, st.n_refine, st.n_coarse) == (n * n, n * n + 3, 1, 0)
+    mesh.close()
+
+
+def test_adaptive_mesh_rejects_periodic_and_late_enable(gpu_lib):
+    import zephyr_b200 as Z
+    gen = Z.Rectangle(0.0, 1.0, 0.0, 1.0)
+    gen.set_boundaries(Z.Boundaries(Z.Boundary.PERIODIC, Z.Boundary.PERIODIC, Z.Boundary.WALL, Z.Boundary.WALL))
+    gen.set_sizes(8, 8)
+    mesh = Z.EuMesh(gen)
+    with pytest.raises(Z.ZgError) as e:
+        mesh.set_max_level(2)
+    assert e.value.code == -1
+    mesh.close()
+    gen.set_boundaries(Z.Boundaries())
+    mesh = Z.EuMesh(gen)
+    solver = Z.SmFluid(Z.IdealGas(1.4))
+    solver.add_types(mesh)
+    with pytest.raises(Z.ZgError) as e:
+        mesh.set_max_level(2)
+    assert e.value.code == -3
+    with pytest.raises(Z.ZgError):
+        mesh.refine()
+    mesh.close()

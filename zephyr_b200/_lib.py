@@ -55,6 +55,20 @@ _P = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
 _V = C.c_void_p
 
+
+class AmrStats(C.Structure):
+    """zg_amr_stats"""
+    _fields_ = [(n, C.c_int) for n in ("max_level", "capacity", "n_before", "n_after", "n_coarse", "n_refine",
+                                        "n_large")]
+
+
+class AmrCells(C.Structure):
+    """zg_amr_cells (host arrays; NULL members are skipped)"""
+    _fields_ = [(n, t) for n, t in (
+        ("center_x", _P), ("center_y", _P), ("volume", _P), ("incircle", _P), ("map_x", _P), ("map_y", _P),
+        ("level", _I), ("flag", _I), ("b_idx", _I), ("z_idx", _I), ("face_boundary", _I), ("face_neib", _I),
+        ("face_nx", _P), ("face_ny", _P), ("face_cx", _P), ("face_cy", _P), ("face_area", _P))]
+
 # name -> (restype, argtypes); every symbol include/zephyr_gpu.h declares.
 class Material(C.Structure):
     """zg_material"""
@@ -84,6 +98,12 @@ SIGNATURES = {
     "zg_mesh_rectangle": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I]),
     "zg_mesh_n_cells": (C.c_int, [_V, _I]),
     "zg_mesh_upload": (C.c_int, [_V, C.POINTER(MeshView)]),
+    "zg_amr_enable": (C.c_int, [_V, C.c_int, C.c_int]),
+    "zg_amr_set_distributor": (C.c_int, [_V, C.c_int]),
+    "zg_amr_put_flags": (C.c_int, [_V, _I]),
+    "zg_amr_refine": (C.c_int, [_V]),
+    "zg_amr_info": (C.c_int, [_V, C.POINTER(AmrStats)]),
+    "zg_amr_download": (C.c_int, [_V, C.POINTER(AmrCells)]),
     "zg_smf_configure": (C.c_int, [_V, C.POINTER(SmfParams)]),
     "zg_smf_set_max_dt": (C.c_int, [_V, C.c_double]),
     "zg_state_upload": (C.c_int, [_V, _P, _P, _P, _P, _P]),

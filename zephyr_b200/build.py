@@ -32,6 +32,8 @@ UNITS = {
     # allocation-free first-order step; its device-built coordinate tables
     # must match the host-built ones, hence no fused multiply-adds
     "zg_noalloc.cu": ["-fmad=false"],
+    # AMR refine: geometry and distributed states bit-exact with the reference
+    "amr_refine.cu": ["-fmad=false"],
     "smf_fast.cu": [],
     "adj.cu": [],
     # FP32 face arithmetic: approximate single-precision division and square

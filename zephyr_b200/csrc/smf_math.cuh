@@ -56,15 +56,15 @@ struct EosD {
     int kind;
     double gamma, gm1, P0, e0, pmin;
 
-    __device__ inline double pressure_re(double rho, double e) const {
+    __host__ __device__ inline double pressure_re(double rho, double e) const {
         if (kind == EOS_IDEAL) return gm1 * rho * e;
         return gm1 * rho * (e - e0) - gamma * P0;
     }
-    __device__ inline double energy_rP(double rho, double P) const {
+    __host__ __device__ inline double energy_rP(double rho, double P) const {
         if (kind == EOS_IDEAL) return P / (gm1 * rho);
         return e0 + (P + gamma * P0) / (gm1 * rho);
     }
-    __device__ inline double sound_speed_rP(double rho, double P) const {
+    __host__ __device__ inline double sound_speed_rP(double rho, double P) const {
         if (kind == EOS_IDEAL) return sqrt(gamma * P / rho);
         return sqrt(gamma * (P + P0) / rho);
     }
@@ -79,10 +79,10 @@ struct Cons {
     double r, mu, mv, E;
 };
 
-__device__ inline double v2(const Prim &z) { return z.u * z.u + z.v * z.v; }
+__host__ __device__ inline double v2(const Prim &z) { return z.u * z.u + z.v * z.v; }
 
 // models.cpp:85-89
-__device__ inline Cons q_from_p(const Prim &z) {
+__host__ __device__ inline Cons q_from_p(const Prim &z) {
     Cons q;
     q.r = z.r;
     q.mu = z.r * z.u;
@@ -91,7 +91,7 @@ __device__ inline Cons q_from_p(const Prim &z) {
     return q;
 }
 // models.cpp:27-32
-__device__ inline Prim p_from_q(const Cons &q, const EosD &eos) {
+__host__ __device__ inline Prim p_from_q(const Cons &q, const EosD &eos) {
     Prim z;
     z.r = q.r;
     z.u = q.mu / z.r;
@@ -111,7 +111,7 @@ __device__ inline Cons flux_from_p(const Prim &z) {
     return f;
 }
 // models.cpp:58-63
-__device__ inline bool is_bad(const Prim &z, const EosD &eos) {
+__host__ __device__ inline bool is_bad(const Prim &z, const EosD &eos) {
     if (!isfinite(z.r) || !isfinite(z.p) || !isfinite(z.e)) return true;
     return z.r <= 0.0 || z.p < eos.pmin;
 }

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/zephyr_gpu.h"
+#include "amr_refine.h"
 #include "mmf_types.h"
 #include "smf_tiled.cuh"
 #include "smf_tiled_launch.h"
@@ -29,6 +30,7 @@ struct zg_ctx {
     // mesh (structured rectangle)
     bool have_mesh = false;
     int nx = 0, ny = 0, n = 0;
+    double box[4] = {};        // x_min, x_max, y_min, y_max of a rectangle mesh
     StructMesh mesh{};
     bool slots = false;        // mesh given cell by cell (zg_mesh_upload)
     SlotMesh smesh{};
@@ -37,6 +39,17 @@ struct zg_ctx {
     double *d_tgeo = nullptr;  // per-axis tables of the tiled kernels, FP64 then FP32
     tiled::AxisGeo<double> ax64{}, ay64{};
     tiled::AxisGeo<float> ax32{}, ay32{};
+    int cap = 0;  // cells every per-cell field holds (n, or the adaptive mesh's capacity)
+
+    // adaptive mesh (AmrCells layout on the device)
+    bool amr = false;
+    int amr_max_level = 0;
+    int amr_distr = ZG_DISTR_SLOPE;
+    void *d_amr = nullptr;          // cell and face arrays, `cap` cells
+    void *d_amr_scratch = nullptr;  // work space of the refine
+    size_t amr_scratch_size = 0;
+    amr::View av{};                 // mesh arrays; state pointers set per refine
+    zg_amr_stats amr_last{};
 
     // solver
     bool configured = false;
@@ -151,11 +164,20 @@ void free_mesh(zg_ctx *c) {
     cudaFree(c->d_geo);
     cudaFree(c->d_tgeo);
     cudaFree(c->d_slot);
+    cudaFree(c->d_amr);
+    cudaFree(c->d_amr_scratch);
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
     c->d_slot = nullptr;
+    c->d_amr = nullptr;
+    c->d_amr_scratch = nullptr;
+    c->amr_scratch_size = 0;
+    c->amr = false;
+    c->av = amr::View{};
+    c->amr_last = zg_amr_stats{};
     c->slots = false;
     c->have_mesh = false;
+    c->cap = 0;
 }
 
 SmfArgs make_args(const zg_ctx *c) {
@@ -174,8 +196,8 @@ SmfArgs make_args(const zg_ctx *c) {
         a.gx[k] = c->gx[k];
         a.gy[k] = c->gy[k];
     }
-    a.wait_in = c->d_wait + (size_t)c->wait_cur * c->n;
-    a.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->n;
+    a.wait_in = c->d_wait + (size_t)c->wait_cur * c->cap;
+    a.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->cap;
     a.dmin_bits = c->d_dmin;
     a.dt_ticket = c->d_ticket;
     a.dt_out = c->d_dt;
@@ -200,8 +222,8 @@ tiled::Fields<double> fast_fields(const zg_ctx *c) {
         f.gx[k] = c->gx[k];
         f.gy[k] = c->gy[k];
     }
-    f.wait_in = c->d_wait + (size_t)c->wait_cur * c->n;
-    f.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->n;
+    f.wait_in = c->d_wait + (size_t)c->wait_cur * c->cap;
+    f.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->cap;
     f.slot_cur = const_cast<unsigned long long *>(slot_ptr(c, 0));
     f.slot_nxt = const_cast<unsigned long long *>(slot_ptr(c, 1));
     f.slot_clr = const_cast<unsigned long long *>(slot_ptr(c, 2));
@@ -225,8 +247,8 @@ tiled::Fields<float> mixed_fields(const zg_ctx *c) {
         f.wn[k] = c->mw[b][k];
         f.h[k] = c->mh[k];
     }
-    f.wait_in = c->d_wait + (size_t)c->wait_cur * c->n;
-    f.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->n;
+    f.wait_in = c->d_wait + (size_t)c->wait_cur * c->cap;
+    f.wait_out = c->d_wait + (size_t)(1 - c->wait_cur) * c->cap;
     f.slot_cur = const_cast<unsigned long long *>(slot_ptr(c, 0));
     f.slot_nxt = const_cast<unsigned long long *>(slot_ptr(c, 1));
     f.slot_clr = const_cast<unsigned long long *>(slot_ptr(c, 2));
@@ -614,12 +636,17 @@ int zg_mesh_rectangle(zg_ctx *c, int nx, int ny, double x_min, double x_max, dou
     m.fym = c->d_geo + ofy;
     m.inc2x = c->d_geo + oix;
     m.inc2y = c->d_geo + oiy;
+    c->box[0] = x_min;
+    c->box[1] = x_max;
+    c->box[2] = y_min;
+    c->box[3] = y_max;
     m.hx = (x_max - x_min) / nx;
     m.hy = (y_max - y_min) / ny;
     m.vol = m.hx * m.hy;
     c->nx = nx;
     c->ny = ny;
     c->n = m.n;
+    c->cap = m.n;
     c->have_mesh = true;
     return ZG_OK;
 }
@@ -683,6 +710,7 @@ int zg_mesh_upload(zg_ctx *c, const zg_mesh_view *v) {
     c->mesh = StructMesh{};
     c->mesh.n = n;
     c->n = n;
+    c->cap = n;
     c->nx = c->ny = 0;
     c->slots = true;
     c->have_mesh = true;
@@ -720,7 +748,7 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     c->eos.pmin = p->eos_kind == ZG_EOS_IDEAL ? 0.0 : -p->P0;  // min_pressure()
     if (c->configured) return ZG_OK;  // fields exist already: keep the state (setters do not reset data)
 
-    size_t n = (size_t)c->n;
+    size_t n = (size_t)c->cap;
     size_t nfields = 3 * 5 + 8;
     ZG_CUDA(c, cudaMalloc(&c->d_state, nfields * n * sizeof(double)));
     ZG_CUDA(c, cudaMalloc(&c->d_wait, 2 * n * sizeof(int)));
@@ -815,7 +843,7 @@ int zg_wait_upload(zg_ctx *c, const int *wait) {
     if (!c || !wait) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_wait_upload: solver not configured");
     DeviceGuard g(c->device);
-    ZG_CUDA(c, cudaMemcpyAsync(c->d_wait + (size_t)c->wait_cur * c->n, wait, (size_t)c->n * sizeof(int),
+    ZG_CUDA(c, cudaMemcpyAsync(c->d_wait + (size_t)c->wait_cur * c->cap, wait, (size_t)c->n * sizeof(int),
                                cudaMemcpyHostToDevice, c->stream));
     return ZG_OK;
 }
@@ -824,7 +852,7 @@ int zg_wait_download(zg_ctx *c, int *wait) {
     if (!c || !wait) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_wait_download: solver not configured");
     DeviceGuard g(c->device);
-    ZG_CUDA(c, cudaMemcpyAsync(wait, c->d_wait + (size_t)c->wait_cur * c->n, (size_t)c->n * sizeof(int),
+    ZG_CUDA(c, cudaMemcpyAsync(wait, c->d_wait + (size_t)c->wait_cur * c->cap, (size_t)c->n * sizeof(int),
                                cudaMemcpyDeviceToHost, c->stream));
     ZG_CUDA(c, cudaStreamSynchronize(c->stream));
     return ZG_OK;
@@ -858,17 +886,24 @@ int zg_smf_dt(zg_ctx *c, double *dt) {
 }
 
 int zg_smf_set_flags(zg_ctx *c, int *flags) {
-    if (!c || !flags) return ZG_ERR_ARG;
+    if (!c || (!flags && !c->amr)) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_set_flags: solver not configured");
     DeviceGuard g(c->device);
     int rc = materialize_prim(c);
     if (rc != ZG_OK) return rc;
     SmfArgs a = make_args(c);
-    timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, c->d_flags, c->slots, (void *)c->stream); });
+    // on an adaptive mesh the flags go to the mesh's own flag array, where
+    // zg_amr_refine reads them (EuCell::set_flag)
+    int *dflags = c->amr ? c->av.flag : c->d_flags;
+    // an adaptive mesh also keeps the limited gradients of the state, which
+    // the slope distributor of the next refine uses (compute_grad,
+    // sm_fluid.cpp:521-522)
+    if (c->amr) timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, true, (void *)c->stream); });
+    timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, dflags, c->slots, (void *)c->stream); });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "flags kernel launch");
-    ZG_CUDA(c, cudaMemcpyAsync(flags, c->d_flags, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost,
-                               c->stream));
+    if (!flags) return ZG_OK;
+    ZG_CUDA(c, cudaMemcpyAsync(flags, dflags, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     ZG_CUDA(c, cudaStreamSynchronize(c->stream));
     return ZG_OK;
 }
@@ -1294,6 +1329,225 @@ int zg_mmf_interface(zg_ctx *c, double *normals, double *offsets) {
             normals[(ic * mmf::NMAT + i) * 2 + 1] = buf[(3 * i + 1) * n + ic];
             offsets[ic * mmf::NMAT + i] = buf[(3 * i + 2) * n + ic];
         }
+    return ZG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adaptive mesh: EuMesh::set_max_level / set_distributor / refine on the GPU
+
+namespace {
+
+// AmrCells arrays of `cap` cells in one allocation: 63 doubles, 22 ints and
+// 16 bytes per cell.
+size_t amr_bytes(size_t cap) { return cap * (63 * sizeof(double) + 22 * sizeof(int) + 16); }
+
+void amr_carve(zg_ctx *c, size_t cap) {
+    double *d = static_cast<double *>(c->d_amr);
+    amr::View &v = c->av;
+    auto td = [&d](size_t k) {
+        double *p = d;
+        d += k;
+        return p;
+    };
+    v.vx = td(9 * cap);
+    v.vy = td(9 * cap);
+    v.cx = td(cap);
+    v.cy = td(cap);
+    v.vol = td(cap);
+    double *inc = td(cap);
+    v.fnx = td(8 * cap);
+    v.fny = td(8 * cap);
+    v.fcx = td(8 * cap);
+    v.fcy = td(8 * cap);
+    v.fa = td(8 * cap);
+    int *ip = reinterpret_cast<int *>(d);
+    auto ti = [&ip](size_t k) {
+        int *p = ip;
+        ip += k;
+        return p;
+    };
+    v.level = ti(cap);
+    v.flag = ti(cap);
+    v.b_idx = ti(cap);
+    v.z_idx = ti(cap);
+    v.next = ti(cap);
+    v.index = ti(cap);
+    v.fb = ti(8 * cap);
+    v.fadj = ti(8 * cap);
+    v.fv = reinterpret_cast<signed char *>(ip);
+    SlotMesh &m = c->smesh;
+    m.cx = v.cx;
+    m.cy = v.cy;
+    m.vol = v.vol;
+    m.inc = inc;
+    m.fb = v.fb;
+    m.fn = v.fadj;
+    m.fnx = v.fnx;
+    m.fny = v.fny;
+    m.fcx = v.fcx;
+    m.fcy = v.fcy;
+    m.fa = v.fa;
+}
+
+void amr_set_n(zg_ctx *c, int n) {
+    c->n = n;
+    c->smesh.n = n;
+    c->mesh = StructMesh{};
+    c->mesh.n = n;
+}
+
+// The mesh view with the current state, isolation counters and gradients.
+amr::View amr_view(const zg_ctx *c) {
+    amr::View v = c->av;
+    v.n = c->n;
+    v.zr = c->z.r;
+    v.zu = c->z.u;
+    v.zv = c->z.v;
+    v.zp = c->z.p;
+    v.ze = c->z.e;
+    v.wait = c->d_wait + (size_t)c->wait_cur * c->cap;
+    for (int k = 0; k < 4; ++k) {
+        v.gx[k] = c->gx[k];
+        v.gy[k] = c->gy[k];
+    }
+    v.slope = c->amr_distr == ZG_DISTR_SLOPE ? 1 : 0;
+    v.eos = c->eos;
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zg_amr_enable(zg_ctx *c, int max_level, int capacity) {
+    if (!c) return ZG_ERR_ARG;
+    if (!c->have_mesh || c->slots || c->nx < 1)
+        return fail(c, ZG_ERR_STATE, "zg_amr_enable: needs a mesh from zg_mesh_rectangle");
+    if (c->configured || c->mm_configured)
+        return fail(c, ZG_ERR_STATE, "zg_amr_enable: call before zg_smf_configure");
+    if (c->mesh.xper || c->mesh.yper)
+        return fail(c, ZG_ERR_ARG,
+                    "zg_amr_enable: periodic boundaries cannot be adaptive (faces across the period have no "
+                    "matching vertices; EuMesh::init_amr -> find_rotations fails with 'Invalid rotation')");
+    if (capacity < c->n) return fail(c, ZG_ERR_ARG, "zg_amr_enable: capacity below the number of cells");
+    if ((long long)capacity > (long long)std::numeric_limits<int>::max() / 16)
+        return fail(c, ZG_ERR_ARG, "zg_amr_enable: capacity too large for 32-bit face indices");
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->stream);
+    const size_t cap = (size_t)capacity;
+    size_t scratch = 0;
+    if (amr::scratch_bytes(capacity, &scratch) != 0) return fail(c, ZG_ERR_CUDA, "zg_amr_enable: scan size query");
+    ZG_CUDA(c, cudaMalloc(&c->d_amr, amr_bytes(cap)));
+    ZG_CUDA(c, cudaMalloc(&c->d_amr_scratch, scratch));
+    c->amr_scratch_size = scratch;
+    amr_carve(c, cap);
+    amr::RectSpec r{};
+    r.nx = c->nx;
+    r.ny = c->ny;
+    r.x_min = c->box[0];
+    r.x_max = c->box[1];
+    r.y_min = c->box[2];
+    r.y_max = c->box[3];
+    for (int k = 0; k < 4; ++k) r.bc[k] = c->mesh.bc[k];
+    r.xper = c->mesh.xper;
+    r.yper = c->mesh.yper;
+    amr::View v = c->av;
+    v.n = c->n;
+    if (amr::init_rect(v, r, const_cast<double *>(c->smesh.inc), c->stream) != 0)
+        return cuda_fail(c, cudaGetLastError(), "zg_amr_enable: base mesh kernels");
+    c->launches += 2;
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the rectangle's axis tables are not used on a slot mesh
+    cudaFree(c->d_geo);
+    cudaFree(c->d_tgeo);
+    c->d_geo = nullptr;
+    c->d_tgeo = nullptr;
+    c->cap = capacity;
+    c->amr = true;
+    c->slots = true;
+    c->amr_max_level = std::max(0, std::min(max_level, 15));  // EuMesh::set_max_level
+    amr_set_n(c, c->n);
+    c->nx = c->ny = 0;
+    return ZG_OK;
+}
+
+int zg_amr_set_distributor(zg_ctx *c, int kind) {
+    if (!c) return ZG_ERR_ARG;
+    if (kind != ZG_DISTR_CONST && kind != ZG_DISTR_SLOPE)
+        return fail(c, ZG_ERR_ARG, "zg_amr_set_distributor: unknown distributor");  // sm_fluid.cpp:373-375
+    c->amr_distr = kind;
+    return ZG_OK;
+}
+
+int zg_amr_put_flags(zg_ctx *c, const int *flags) {
+    if (!c || !flags) return ZG_ERR_ARG;
+    if (!c->amr) return fail(c, ZG_ERR_STATE, "zg_amr_put_flags: mesh is not adaptive");
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(c->av.flag, flags, (size_t)c->n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    return ZG_OK;
+}
+
+int zg_amr_refine(zg_ctx *c) {
+    if (!c) return ZG_ERR_ARG;
+    if (!c->amr) return fail(c, ZG_ERR_STATE, "zg_amr_refine: mesh is not adaptive (zg_amr_enable)");
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_amr_refine: solver not configured");
+    if (c->amr_max_level < 1) return ZG_OK;  // EuMesh::refine returns on a non-adaptive mesh
+    DeviceGuard g(c->device);
+    const int n0 = c->n;
+    amr::RefineResult res = amr::refine(amr_view(c), c->n, c->cap, c->amr_max_level, c->d_amr_scratch,
+                                        c->amr_scratch_size, const_cast<double *>(c->smesh.inc), c->stream);
+    c->launches += res.launches;
+    if (res.err == -6)
+        return fail(c, ZG_ERR_TOO_LARGE,
+                    "zg_amr_refine: the adaptation needs " + std::to_string(res.n_large) + " cells, capacity is " +
+                        std::to_string(c->cap));
+    if (res.err != 0) return cuda_fail(c, cudaGetLastError(), "zg_amr_refine");
+    amr_set_n(c, res.n);
+    c->cfl_valid = false;
+    c->amr_last.n_before = n0;
+    c->amr_last.n_after = res.n;
+    c->amr_last.n_coarse = res.n_coarse;
+    c->amr_last.n_refine = res.n_refine;
+    c->amr_last.n_large = res.n_large;
+    return ZG_OK;
+}
+
+int zg_amr_info(const zg_ctx *c, zg_amr_stats *out) {
+    if (!c || !out) return ZG_ERR_ARG;
+    *out = c->amr_last;
+    out->max_level = c->amr ? c->amr_max_level : 0;
+    out->capacity = c->amr ? c->cap : 0;
+    return ZG_OK;
+}
+
+int zg_amr_download(zg_ctx *c, const zg_amr_cells *out) {
+    if (!c || !out) return ZG_ERR_ARG;
+    if (!c->amr) return fail(c, ZG_ERR_STATE, "zg_amr_download: mesh is not adaptive");
+    DeviceGuard g(c->device);
+    const size_t n = (size_t)c->n;
+    const amr::View &v = c->av;
+    auto cp = [c](void *dst, const void *src, size_t bytes) {
+        if (!dst) return cudaSuccess;
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    };
+    const size_t D = sizeof(double), I = sizeof(int);
+    struct Item {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    } items[] = {{out->center_x, v.cx, n * D},       {out->center_y, v.cy, n * D},
+                 {out->volume, v.vol, n * D},        {out->incircle, c->smesh.inc, n * D},
+                 {out->map_x, v.vx, 9 * n * D},      {out->map_y, v.vy, 9 * n * D},
+                 {out->level, v.level, n * I},       {out->flag, v.flag, n * I},
+                 {out->b_idx, v.b_idx, n * I},       {out->z_idx, v.z_idx, n * I},
+                 {out->face_boundary, v.fb, 8 * n * I}, {out->face_neib, v.fadj, 8 * n * I},
+                 {out->face_nx, v.fnx, 8 * n * D},   {out->face_ny, v.fny, 8 * n * D},
+                 {out->face_cx, v.fcx, 8 * n * D},   {out->face_cy, v.fcy, 8 * n * D},
+                 {out->face_area, v.fa, 8 * n * D}};
+    for (const Item &it : items) ZG_CUDA(c, cp(it.dst, it.src, it.bytes));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
     return ZG_OK;
 }
 

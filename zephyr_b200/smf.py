@@ -170,6 +170,7 @@ class EuMesh:
         self.nx, self.ny = gen.nx(), gen.ny()
         self.gen = gen
         self.solver = None
+        self._amr = False
 
     @classmethod
     def from_arrays(cls, g: dict, device: int = 0, stream=None):
@@ -199,6 +200,7 @@ class EuMesh:
         self.nx = self.ny = 0
         self.gen = None
         self.solver = None
+        self._amr = False
         return self
 
     def set_stream(self, stream):
@@ -213,6 +215,13 @@ class EuMesh:
 
     def centers(self):
         """Cell centres (x, y) in cell order, with the reference's formulas."""
+        if self._amr:
+            from ._lib import AmrCells
+            n = self.n_cells()
+            cx, cy = np.empty(n), np.empty(n)
+            view = AmrCells(cx.ctypes.data_as(C.POINTER(C.c_double)), cy.ctypes.data_as(C.POINTER(C.c_double)))
+            check(self.ctx, self._lib.zg_amr_download(self.ctx, C.byref(view)))
+            return cx, cy
         g = self.gen
         X = g.x_min + ((g.x_max - g.x_min) * np.arange(g.nx() + 1)) / g.nx()
         Y = g.y_min + ((g.y_max - g.y_min) * np.arange(g.ny() + 1)) / g.ny()
@@ -257,6 +266,66 @@ class EuMesh:
         check(self.ctx, self._lib.zg_wait_download(self.ctx, w.ctypes.data_as(C.POINTER(C.c_int))))
         return w
 
+    # ---- adaptation (eu_mesh.h: set_max_level, set_distributor, refine) ----
+    def set_max_level(self, max_level: int, capacity: int | None = None):
+        """EuMesh::set_max_level on a rectangle mesh: the cells get the AMR
+        layout on the device with room for `capacity` cells (default
+        max(16 n, 2^20)).  Call before SmFluid.add_types."""
+        n = self.n_cells()
+        if capacity is None:
+            capacity = min(max(16 * n, 1 << 20), (2 ** 31 - 1) // 16)
+        check(self.ctx, self._lib.zg_amr_enable(self.ctx, int(max_level), int(capacity)))
+        self._amr = True
+
+    def max_level(self) -> int:
+        return self.amr_info().max_level
+
+    def adaptive(self) -> bool:  # eu_mesh.cpp:170-172
+        return self.max_level() > 0
+
+    def set_distributor(self, kind):
+        """EuMesh::set_distributor(solver.distributor(type)); `kind` is the
+        value of SmFluid.distributor or the type name ("const", "slope")."""
+        if isinstance(kind, str):
+            kind = SmFluid.DISTRIBUTORS.get(kind, -1)
+        check(self.ctx, self._lib.zg_amr_set_distributor(self.ctx, int(kind)))
+
+    def put_flags(self, flags):
+        """EuCell::set_flag for every cell."""
+        f = np.ascontiguousarray(flags, dtype=np.int32)
+        if f.shape != (self.n_cells(),):
+            raise ZgError(-1, f"flags must have shape ({self.n_cells()},)")
+        check(self.ctx, self._lib.zg_amr_put_flags(self.ctx, f.ctypes.data_as(C.POINTER(C.c_int))))
+        check(self.ctx, self._lib.zg_synchronize(self.ctx))
+
+    def refine(self):  # eu_mesh.cpp:290-359
+        check(self.ctx, self._lib.zg_amr_refine(self.ctx))
+
+    def amr_info(self):
+        from ._lib import AmrStats
+        st = AmrStats()
+        check(self.ctx, self._lib.zg_amr_info(self.ctx, C.byref(st)))
+        return st
+
+    def amr_arrays(self) -> dict:
+        """Host copies of the adaptive mesh: cells (cx, cy, vol, inc, level,
+        flag, b_idx, z_idx), map points (vx, vy: 9 per cell) and face slots
+        (boundary, neib, nx, ny, fx, fy, area: 8 per cell)."""
+        from ._lib import AmrCells
+        n = self.n_cells()
+        g = {k: np.empty(n) for k in ("cx", "cy", "vol", "inc")}
+        g.update({k: np.empty(9 * n) for k in ("vx", "vy")})
+        g.update({k: np.empty(n, np.int32) for k in ("level", "flag", "b_idx", "z_idx")})
+        g.update({k: np.empty(8 * n, np.int32) for k in ("boundary", "neib")})
+        g.update({k: np.empty(8 * n) for k in ("nx", "ny", "fx", "fy", "area")})
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        view = AmrCells(dp(g["cx"]), dp(g["cy"]), dp(g["vol"]), dp(g["inc"]), dp(g["vx"]), dp(g["vy"]),
+                        ip(g["level"]), ip(g["flag"]), ip(g["b_idx"]), ip(g["z_idx"]), ip(g["boundary"]),
+                        ip(g["neib"]), dp(g["nx"]), dp(g["ny"]), dp(g["fx"]), dp(g["fy"]), dp(g["area"]))
+        check(self.ctx, self._lib.zg_amr_download(self.ctx, C.byref(view)))
+        return g
+
     def launch_count(self) -> int:
         n = C.c_longlong()
         check(self.ctx, self._lib.zg_launch_count(self.ctx, C.byref(n)))
@@ -291,6 +360,8 @@ class Parts:
 
 class SmFluid:
     """math/solver/sm_fluid.{h,cpp} on the GPU."""
+
+    DISTRIBUTORS = {"const": 0, "slope": 1}  # enum zg_distributor
 
     def __init__(self, eos, precision: Precision = Precision.FP64, kernels: Kernels = Kernels.PARITY):
         self._lib = load()
@@ -361,9 +432,19 @@ class SmFluid:
         check(self.mesh.ctx, self._lib.zg_smf_dt(self.mesh.ctx, C.byref(d)))
         return d.value
 
-    def set_flags(self, mesh: EuMesh):  # sm_fluid.cpp:517-559 (flag values)
+    def set_flags(self, mesh: EuMesh, download: bool = True):  # sm_fluid.cpp:517-559 (flag values)
+        """Flags of every cell; on an adaptive mesh they stay on the device for
+        EuMesh.refine, and `download=False` skips the host copy."""
         if mesh is not self.mesh:
             self.add_types(mesh)
+        if not download:
+            check(mesh.ctx, self._lib.zg_smf_set_flags(mesh.ctx, None))
+            return None
         f = np.empty(mesh.n_cells(), np.int32)
         check(mesh.ctx, self._lib.zg_smf_set_flags(mesh.ctx, f.ctypes.data_as(C.POINTER(C.c_int))))
         return f
+
+    def distributor(self, type: str = "slope") -> int:  # sm_fluid.cpp:372-375
+        if type not in self.DISTRIBUTORS:
+            raise ZgError(-1, f"SmFluid error: unknown m_distributor type '{type}'")
+        return self.DISTRIBUTORS[type]

@@ -9,6 +9,11 @@ fourier_smooth    smooth periodic data: rho = 1 + 0.2 f, u = 0.3 f, v = 0.3 f,
                   sin(2 pi m y + psi_m), a_m ~ U(0,1)/8, phi, psi ~ U(0, 2 pi),
                   drawn (a_m, phi_m, psi_m) for m = 1..8 from numpy's PCG64
                   with seeds 1, 2, 3, 4 for rho, u, v, p.
+blast_cell_means  the AMR blast: rho = 1, u = v = 0, p = 1e-5 except p = 1e3
+                  for r < 0.01 around (0.5, 0.5); cell means of the
+                  conservative state by n x n midpoint sub-sampling of each
+                  cell (the sub-sampled initialisation of smf_test_2D.cpp:77-87,
+                  IVP::*_mean), for the cells of an adaptive mesh.
 """
 from __future__ import annotations
 
@@ -138,3 +143,35 @@ def shock_water_column(n: int = 1024, sub: int = 8) -> MmWorkload:
     p = np.where(shocked & (alpha <= 0.0), p2, p1)
     return MmWorkload("shock_water_column", n, n, box, (2, 2, 1, 1), (("stiffened", "Water"), ("ideal", "Air")),
                       rho, vx, np.zeros(n * n), p, beta)
+
+
+BLAST_R0 = 0.01
+BLAST_P_IN, BLAST_P_OUT = 1.0e3, 1.0e-5
+
+
+def blast_cell_means(map_x, map_y, n_sub: int = 20, gamma: float = 1.4):
+    """(rho, vx, vy, p, e) of the blast for cells given by their 9 map points
+    (axis-aligned rectangles: corners at map points 0 and 8).  The mean total
+    energy of a cell is the sub-sample mean of p / (gamma - 1); cells the
+    circle does not cross take the centre value."""
+    x0, x1 = map_x[0::9], map_x[8::9]
+    y0, y1 = map_y[0::9], map_y[8::9]
+    n = x0.size
+    # distance range of each rectangle from the centre
+    dx_near = np.maximum(np.maximum(0.5 - x1, x0 - 0.5), 0.0)
+    dy_near = np.maximum(np.maximum(0.5 - y1, y0 - 0.5), 0.0)
+    dx_far = np.maximum(np.abs(x0 - 0.5), np.abs(x1 - 0.5))
+    dy_far = np.maximum(np.abs(y0 - 0.5), np.abs(y1 - 0.5))
+    r_near, r_far = np.hypot(dx_near, dy_near), np.hypot(dx_far, dy_far)
+    frac = (r_far < BLAST_R0).astype(np.float64)
+    cut = np.where((r_near < BLAST_R0) & (r_far >= BLAST_R0))[0]
+    if cut.size:
+        t = (np.arange(n_sub) + 0.5) / n_sub
+        sx = x0[cut, None] + (x1 - x0)[cut, None] * t[None, :]
+        sy = y0[cut, None] + (y1 - y0)[cut, None] * t[None, :]
+        inside = np.hypot(sx[:, :, None] - 0.5, sy[:, None, :] - 0.5) < BLAST_R0
+        frac[cut] = inside.mean(axis=(1, 2))
+    E = (frac * BLAST_P_IN + (1.0 - frac) * BLAST_P_OUT) / (gamma - 1.0)
+    rho = np.ones(n)
+    p = (gamma - 1.0) * E
+    return rho, np.zeros(n), np.zeros(n), p, p / ((gamma - 1.0) * rho)
