@@ -39,6 +39,19 @@ namespace zg {
 namespace adj {
 
 constexpr int BLOCK = 128;
+// Minimum resident blocks per SM of the heavy kernels.  They are latency-
+// bound; these caps on their registers (a few spilled bytes in some) were
+// chosen by timing the 1024^2, 100-step forward and gradient runs over a
+// sweep of the values on a B200 (-D overrides).
+#ifndef ZG_ADJ_PG_MINB
+#define ZG_ADJ_PG_MINB 8
+#endif
+#ifndef ZG_ADJ_FU_MINB
+#define ZG_ADJ_FU_MINB 6
+#endif
+#ifndef ZG_ADJ_VF_MINB
+#define ZG_ADJ_VF_MINB 6
+#endif
 
 struct Grid {
     int nx, ny, n;
@@ -52,21 +65,26 @@ struct CF4 {
     const double *f[4];
 };
 
-__device__ __forceinline__ int xm(const Grid &g, int ic) {
+// A cell with its (i, j): the periodic neighbours follow without integer
+// division (one division per thread, in cell_of).
+struct Cell {
+    int ic, i, j;
+};
+__device__ __forceinline__ Cell cell_of(const Grid &g, int ic) {
     int i = ic / g.ny;
-    return i > 0 ? ic - g.ny : ic + (g.nx - 1) * g.ny;
+    return Cell{ic, i, ic - i * g.ny};
 }
-__device__ __forceinline__ int xp(const Grid &g, int ic) {
-    int i = ic / g.ny;
-    return i < g.nx - 1 ? ic + g.ny : ic - (g.nx - 1) * g.ny;
+__device__ __forceinline__ Cell xm(const Grid &g, Cell c) {
+    return c.i > 0 ? Cell{c.ic - g.ny, c.i - 1, c.j} : Cell{c.ic + (g.nx - 1) * g.ny, g.nx - 1, c.j};
 }
-__device__ __forceinline__ int ym(const Grid &g, int ic) {
-    int j = ic % g.ny;
-    return j > 0 ? ic - 1 : ic + (g.ny - 1);
+__device__ __forceinline__ Cell xp(const Grid &g, Cell c) {
+    return c.i < g.nx - 1 ? Cell{c.ic + g.ny, c.i + 1, c.j} : Cell{c.ic - (g.nx - 1) * g.ny, 0, c.j};
 }
-__device__ __forceinline__ int yp(const Grid &g, int ic) {
-    int j = ic % g.ny;
-    return j < g.ny - 1 ? ic + 1 : ic - (g.ny - 1);
+__device__ __forceinline__ Cell ym(const Grid &g, Cell c) {
+    return c.j > 0 ? Cell{c.ic - 1, c.i, c.j - 1} : Cell{c.ic + (g.ny - 1), c.i, g.ny - 1};
+}
+__device__ __forceinline__ Cell yp(const Grid &g, Cell c) {
+    return c.j < g.ny - 1 ? Cell{c.ic + 1, c.i, c.j + 1} : Cell{c.ic - (g.ny - 1), c.i, 0};
 }
 
 __device__ __forceinline__ void load4(const CF4 &a, int ic, double o[4]) {
@@ -91,15 +109,16 @@ __global__ void k_init(Grid g, CF4 W0, double gamma, F4 U) {
 }
 
 // primitive state and limited slopes of every cell
-__global__ void __launch_bounds__(BLOCK) k_prim_grad(Grid g, CF4 U, double gamma, double eps, F4 W, F4 gx, F4 gy) {
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_PG_MINB) k_prim_grad(Grid g, CF4 U, double gamma, double eps, F4 W, F4 gx, F4 gy) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= g.n) return;
     double wc[4], wl[4], wr[4], wb[4], wt[4];
     prim_at(U, ic, gamma, wc);
-    prim_at(U, xm(g, ic), gamma, wl);
-    prim_at(U, xp(g, ic), gamma, wr);
-    prim_at(U, ym(g, ic), gamma, wb);
-    prim_at(U, yp(g, ic), gamma, wt);
+    const Cell c = cell_of(g, ic);
+    prim_at(U, xm(g, c).ic, gamma, wl);
+    prim_at(U, xp(g, c).ic, gamma, wr);
+    prim_at(U, ym(g, c).ic, gamma, wb);
+    prim_at(U, yp(g, c).ic, gamma, wt);
     const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -144,11 +163,12 @@ __device__ __forceinline__ void flux_global(const double Fl[4], bool yface, doub
 }
 
 // out = alpha * base + beta * (X + dt L(X)), L from the face fluxes of W, G
-__global__ void __launch_bounds__(BLOCK) k_flux_update(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 X,
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 X,
                                                        CF4 base, double alpha, double beta, double dt, F4 out) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= g.n) return;
-    const int nb[4] = {xm(g, ic), xp(g, ic), ym(g, ic), yp(g, ic)};
+    const Cell cc = cell_of(g, ic);
+    const int nb[4] = {xm(g, cc).ic, xp(g, cc).ic, ym(g, cc).ic, yp(g, cc).ic};
     double sum[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
@@ -227,7 +247,7 @@ __global__ void __launch_bounds__(BLOCK) k_probe(Grid g, CF4 U, double gamma, do
 // cotangents of the face's low-side and high-side states, in the global
 // primitive frame, go to fb[face][0..3] and fb[face][4..7]; the faces' gamma
 // parts to gacc.
-__global__ void __launch_bounds__(BLOCK, 4) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_VF_MINB) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
                                                      double coef, double *fbx, double *fby, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     double gpart = 0.0;
@@ -236,7 +256,8 @@ __global__ void __launch_bounds__(BLOCK, 4) k_vjp_faces(Grid g, CF4 W, CF4 gx, C
 #pragma unroll 1
         for (int axis = 0; axis < 2; ++axis) {
             const bool yface = axis == 1;
-            const int lo = ic, hi = yface ? yp(g, ic) : xp(g, ic);
+            const Cell c = cell_of(g, ic);
+            const int lo = ic, hi = yface ? yp(g, c).ic : xp(g, c).ic;
             const double half_h = 0.5 * (yface ? g.hy : g.hx), S = yface ? g.hx : g.hy;
             // cotangent of the global face flux: L_lo gets -S/V F, L_hi +S/V F
             double mF[4];
@@ -284,50 +305,117 @@ __global__ void __launch_bounds__(BLOCK, 4) k_vjp_faces(Grid g, CF4 W, CF4 gx, C
 // h/2) and the slopes of itself and of its two neighbours on each axis; the
 // cotangents come back here, then through the primitive map to U and gamma.
 // out = base_coef * base + add + Ubar.
-__global__ void __launch_bounds__(BLOCK, 5) k_vjp_cells(Grid g, CF4 X, CF4 W, double gamma, double eps,
-                                                     const double *fbx, const double *fby, CF4 base,
-                                                     double base_coef, CF4 add, F4 out, double *gacc) {
-    int ic = blockIdx.x * BLOCK + threadIdx.x;
-    double gpart = 0.0;
-    if (ic < g.n) {
-        const size_t n = (size_t)g.n;
-        const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy, hx2 = 0.5 * g.hx, hy2 = 0.5 * g.hy;
-        const int l = xm(g, ic), r = xp(g, ic), b = ym(g, ic), t = yp(g, ic);
-        const int ll = xm(g, l), rr = xp(g, r), bb = ym(g, b), tt = yp(g, t);
-        double wt[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            // face-state cotangents: low side of the face a cell owns (index
-            // of the low cell), high side of the face below it
-            const double xl_l = fbx[k * n + l], xh_ll = fbx[(4 + k) * n + ll];
-            const double xl_c = fbx[k * n + ic], xh_l = fbx[(4 + k) * n + l];
-            const double xl_r = fbx[k * n + r], xh_c = fbx[(4 + k) * n + ic];
-            const double yl_b = fby[k * n + b], yh_bb = fby[(4 + k) * n + bb];
-            const double yl_c = fby[k * n + ic], yh_b = fby[(4 + k) * n + b];
-            const double yl_t = fby[k * n + t], yh_c = fby[(4 + k) * n + ic];
-            // slope cotangents of l, c, r (x) and b, c, t (y)
-            const double gbl = hx2 * (xl_l - xh_ll), gbc = hx2 * (xl_c - xh_l), gbr = hx2 * (xl_r - xh_c);
-            const double gbb = hy2 * (yl_b - yh_bb), gbcy = hy2 * (yl_c - yh_b), gbt = hy2 * (yl_t - yh_c);
-            double acc = xl_c + xh_l + yl_c + yh_b;
-            double w_ll = W.f[k][ll], w_l = W.f[k][l], w_c = W.f[k][ic], w_r = W.f[k][r], w_rr = W.f[k][rr];
-            double w_bb = W.f[k][bb], w_b = W.f[k][b], w_t = W.f[k][t], w_tt = W.f[k][tt];
-            double d[3];
-            slope_partials(w_ll, w_l, w_c, i2x, eps, d);  // slope of the left cell: this cell is its wp
-            acc += d[2] * gbl;
-            slope_partials(w_l, w_c, w_r, i2x, eps, d);   // own slope
-            acc += d[1] * gbc;
-            slope_partials(w_c, w_r, w_rr, i2x, eps, d);  // right cell: this cell is its wm
-            acc += d[0] * gbr;
-            slope_partials(w_bb, w_b, w_c, i2y, eps, d);
-            acc += d[2] * gbb;
-            slope_partials(w_b, w_c, w_t, i2y, eps, d);
-            acc += d[1] * gbcy;
-            slope_partials(w_c, w_t, w_tt, i2y, eps, d);
-            acc += d[0] * gbt;
-            wt[k] = acc;
+// Tiles of VJ x VI cells (j x i): every cell's slope partials are computed
+// once and shared through shared memory with its two neighbours on each axis.
+// Tile positions map to periodically wrapped cells, so a position outside the
+// mesh (last tiles) holds a copy of the wrapped cell and every neighbour read
+// from shared memory is the true periodic neighbour.
+constexpr int VJ = 32, VI = 8;
+#ifndef ZG_ADJ_VT_MINB
+#define ZG_ADJ_VT_MINB 4
+#endif
+
+__device__ __forceinline__ int wrapc(int x, int n) {
+    if (x < 0) x += n;
+    if (x >= n) {
+        x -= n;
+        if (x >= n) x %= n;
+    }
+    return x;
+}
+
+// d0 * gb and d2 * gb of a cell's slope along one axis (its contributions to
+// its low and high neighbour), and d1 * gb (its own), for field k
+__device__ __forceinline__ void slope_terms(double wm, double w0, double wp, double i2h, double eps, double gb,
+                                            double &to_lo, double &own, double &to_hi) {
+    double d[3];
+    slope_partials(wm, w0, wp, i2h, eps, d);
+    to_lo = d[0] * gb;
+    own = d[1] * gb;
+    to_hi = d[2] * gb;
+}
+
+__global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
+    Grid g, CF4 X, CF4 W, double gamma, double eps, const double *fbx, const double *fby, CF4 base, double base_coef,
+    CF4 add, F4 out, double *gacc) {
+    // contributions of tile positions to their neighbours: x (i) rows -1..VI,
+    // y (j) columns -1..VJ
+    __shared__ double sx_lo[VI + 2][VJ], sx_hi[VI + 2][VJ];
+    __shared__ double sy_lo[VI][VJ + 2], sy_hi[VI][VJ + 2];
+    __shared__ double red[VJ * VI / 32];
+    const int tj = threadIdx.x, ti = threadIdx.y, tid = ti * VJ + tj;
+    const int i0 = blockIdx.y * VI, j0 = blockIdx.x * VJ;
+    const size_t n = (size_t)g.n;
+    const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy, hx2 = 0.5 * g.hx, hy2 = 0.5 * g.hy;
+    const Cell c{wrapc(i0 + ti, g.nx) * g.ny + wrapc(j0 + tj, g.ny), wrapc(i0 + ti, g.nx), wrapc(j0 + tj, g.ny)};
+    const Cell cl = xm(g, c), cr = xp(g, c), cb = ym(g, c), ct = yp(g, c);
+    const bool live = i0 + ti < g.nx && j0 + tj < g.ny;
+    // halo work: positions of row -1 / VI (x terms only) and columns -1 / VJ
+    // (y terms only), one per thread for the first 2 (VJ + VI) threads
+    int h_axis = -1, h_side = 0, h_pos = 0;
+    if (tid < 2 * VJ) {
+        h_axis = 0;
+        h_side = tid < VJ ? 0 : 1;
+        h_pos = tid % VJ;
+    } else if (tid < 2 * VJ + 2 * VI) {
+        h_axis = 1;
+        h_side = tid - 2 * VJ < VI ? 0 : 1;
+        h_pos = (tid - 2 * VJ) % VI;
+    }
+    Cell hc{}, hm{}, hp{};
+    if (h_axis == 0) {
+        int hi_ = wrapc(h_side == 0 ? i0 - 1 : i0 + VI, g.nx), hj = wrapc(j0 + h_pos, g.ny);
+        hc = Cell{hi_ * g.ny + hj, hi_, hj};
+        hm = xm(g, hc);
+        hp = xp(g, hc);
+    } else if (h_axis == 1) {
+        int hi_ = wrapc(i0 + h_pos, g.nx), hj = wrapc(h_side == 0 ? j0 - 1 : j0 + VJ, g.ny);
+        hc = Cell{hi_ * g.ny + hj, hi_, hj};
+        hm = ym(g, hc);
+        hp = yp(g, hc);
+    }
+    double wt[4];
+#pragma unroll 1
+    for (int k = 0; k < 4; ++k) {
+        const double *fl = fbx + k * n, *fh = fbx + (4 + k) * n, *gl = fby + k * n, *gh = fby + (4 + k) * n;
+        const double *w = W.f[k];
+        // own position: slope cotangents and partials on both axes
+        const double xl_c = fl[c.ic], xh_l = fh[cl.ic], yl_c = gl[c.ic], yh_b = gh[cb.ic];
+        const double w_c = w[c.ic];
+        double ox, oy, lo, hi;
+        slope_terms(w[cl.ic], w_c, w[cr.ic], i2x, eps, hx2 * (xl_c - xh_l), lo, ox, hi);
+        sx_lo[ti + 1][tj] = lo;
+        sx_hi[ti + 1][tj] = hi;
+        slope_terms(w[cb.ic], w_c, w[ct.ic], i2y, eps, hy2 * (yl_c - yh_b), lo, oy, hi);
+        sy_lo[ti][tj + 1] = lo;
+        sy_hi[ti][tj + 1] = hi;
+        if (h_axis == 0) {
+            const double gb = hx2 * (fl[hc.ic] - fh[hm.ic]);
+            double o;
+            slope_terms(w[hm.ic], w[hc.ic], w[hp.ic], i2x, eps, gb, lo, o, hi);
+            if (h_side == 0) sx_hi[0][h_pos] = hi;
+            else sx_lo[VI + 1][h_pos] = lo;
+        } else if (h_axis == 1) {
+            const double gb = hy2 * (gl[hc.ic] - gh[hm.ic]);
+            double o;
+            slope_terms(w[hm.ic], w[hc.ic], w[hp.ic], i2y, eps, gb, lo, o, hi);
+            if (h_side == 0) sy_hi[h_pos][0] = hi;
+            else sy_lo[h_pos][VJ + 1] = lo;
         }
-        // primitive map rho, u = m_x / rho, v = m_y / rho,
-        // p = (gamma - 1) (E - (m_x^2 + m_y^2) / (2 rho))
+        __syncthreads();
+        double acc = xl_c + xh_l + yl_c + yh_b;
+        acc += sx_hi[ti][tj];      // the left cell's slope (this cell is its high neighbour)
+        acc += ox;                 // own slope
+        acc += sx_lo[ti + 2][tj];  // the right cell's slope
+        acc += sy_hi[ti][tj];
+        acc += oy;
+        acc += sy_lo[ti][tj + 2];
+        wt[k] = acc;
+        __syncthreads();
+    }
+    double gpart = 0.0;
+    if (live) {
+        const int ic = c.ic;
         const double rho = X.f[0][ic], mx = X.f[1][ic], my = X.f[2][ic], E = X.f[3][ic];
         const double ir = 1.0 / rho, u = mx * ir, v = my * ir, gm1 = gamma - 1.0;
         double ub[4];
@@ -338,13 +426,20 @@ __global__ void __launch_bounds__(BLOCK, 5) k_vjp_cells(Grid g, CF4 X, CF4 W, do
         gpart = wt[3] * (E - 0.5 * ((mx * mx + my * my) * ir));
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            double v = ub[k];
-            if (base.f[0]) v += base_coef * base.f[k][ic];
-            if (add.f[0]) v += add.f[k][ic];
-            out.f[k][ic] = v;
+            double vv = ub[k];
+            if (base.f[0]) vv += base_coef * base.f[k][ic];
+            if (add.f[0]) vv += add.f[k][ic];
+            out.f[k][ic] = vv;
         }
     }
-    block_add(gpart, gacc);
+    for (int o = 16; o > 0; o >>= 1) gpart += __shfl_xor_sync(0xffffffffu, gpart, o);
+    if ((tid & 31) == 0) red[tid >> 5] = gpart;
+    __syncthreads();
+    if (tid == 0) {
+        double s2 = 0.0;
+        for (int w2 = 0; w2 < VJ * VI / 32; ++w2) s2 += red[w2];
+        gacc[blockIdx.y * gridDim.x + blockIdx.x] += s2;
+    }
 }
 
 // dJ/d rho_0 from lambda^0 (U_0 = (rho, rho u, rho v, p/(gamma-1) + rho |v|^2 / 2)),
@@ -409,6 +504,12 @@ const CF4 kNull{{nullptr, nullptr, nullptr, nullptr}};
 const F4 kNullW{{nullptr, nullptr, nullptr, nullptr}};
 
 unsigned nblocks(const zg_adj *a) { return (unsigned)((a->g.n + BLOCK - 1) / BLOCK); }
+dim3 vtiles(const zg_adj *a) { return dim3((unsigned)((a->g.ny + VJ - 1) / VJ), (unsigned)((a->g.nx + VI - 1) / VI)); }
+// per-block accumulator slots: enough for the 1-D kernels and the tiles
+unsigned nacc(const zg_adj *a) {
+    dim3 t = vtiles(a);
+    return std::max(nblocks(a), t.x * t.y);
+}
 
 // (re)allocate for `ckpts` checkpoints and segments of `seglen` steps
 int reserve(zg_adj *a, size_t ckpts, size_t seglen) {
@@ -486,8 +587,9 @@ void vjp(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F4 
     unsigned nb = nblocks(a);
     k_vjp_faces<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(wg.W), cf(wg.gx), cf(wg.gy), p.gamma, cf(mu), coef, a->fbx,
                                              a->fby, gacc);
-    k_vjp_cells<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), cf(wg.W), p.gamma, p.limiter_eps, a->fbx, a->fby, cf(base),
-                                             base_coef, add, out, gacc);
+    k_vjp_cells_tiled<<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(X), cf(wg.W), p.gamma, p.limiter_eps,
+                                                                  a->fbx, a->fby, cf(base), base_coef, add, out,
+                                                                  gacc);
     a->launches += 2;
 }
 
@@ -501,7 +603,7 @@ int check_params(zg_adj *a, const zg_adj_params *p) {
 }
 
 int finish_sum(zg_adj *a, double *out2) {
-    unsigned nb = nblocks(a);
+    unsigned nb = nacc(a);
     std::vector<double> h(2 * (size_t)nb);
     cudaError_t e = cudaMemcpyAsync(h.data(), a->d_acc, h.size() * sizeof(double), cudaMemcpyDeviceToHost, a->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(a->stream);
@@ -557,7 +659,7 @@ int zg_adj_create(zg_adj **out, int device, int nx, int ny, double x_min, double
     a->g.x0 = x_min;
     a->g.y0 = y_min;
     DevGuard gd(device);
-    if (cudaMalloc(&a->d_acc, 2 * nblocks(a) * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&a->d_acc, 2 * nacc(a) * sizeof(double)) != cudaSuccess) {
         delete a;
         return ZG_ERR_ALLOC;
     }
@@ -610,11 +712,11 @@ int zg_adj_forward(zg_adj *a, const zg_adj_params *p, const double *rho, const d
         heun_step(a, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
         std::swap(cur, nxt);
     }
-    cudaMemsetAsync(a->d_acc, 0, 2 * nb * sizeof(double), a->stream);
+    cudaMemsetAsync(a->d_acc, 0, 2 * nacc(a) * sizeof(double), a->stream);
     int np = probe_count(a, *p);
     if (np == 0) return afail(a, ZG_ERR_ARG, "no cell centre inside the probe box");
     k_probe<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(cur), p->gamma, p->probe[0], p->probe[1], p->probe[2], p->probe[3],
-                                         1.0 / np, a->d_acc, kNullW, a->d_acc + nb);
+                                         1.0 / np, a->d_acc, kNullW, a->d_acc + nacc(a));
     ++a->launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return afail(a, ZG_ERR_CUDA, cudaGetErrorString(e));
@@ -661,12 +763,12 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
         cur = nxt;
     }
     // J and lambda^N
-    cudaMemsetAsync(a->d_acc, 0, 2 * nb * sizeof(double), a->stream);
+    cudaMemsetAsync(a->d_acc, 0, 2 * nacc(a) * sizeof(double), a->stream);
     F4 lam = a->lamA, lam_prev = a->lamB;
     k_probe<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(cur), p->gamma, p->probe[0], p->probe[1], p->probe[2], p->probe[3],
-                                         1.0 / np, a->d_acc, lam, a->d_acc + nb);
+                                         1.0 / np, a->d_acc, lam, a->d_acc + nacc(a));
     ++a->launches;
-    double *gacc = a->d_acc + nb;
+    double *gacc = a->d_acc + nacc(a);
 
     // reverse sweep, segment by segment
     for (int sg = nseg - 1; sg >= 0; --sg) {

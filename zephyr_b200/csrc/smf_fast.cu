@@ -6,8 +6,25 @@ namespace zg {
 namespace fast {
 
 using tiled::Fields;
-constexpr int BLOCK = 128, TX = 32, TY = 8;  // faces: 32 x 8 threads, 31 x 7 interior cells
-constexpr int GX = 32, GY = 4;               // gradients + predictor: 32 x 4 cells
+// Tile shapes and minimum resident blocks per SM.  The kernels are latency-
+// bound, so residency decides their speed: the minimum-block counts cap the
+// registers per thread (spilling a few bytes in the gradient pass) and were
+// chosen by timing the 2048^2 step over a sweep of these values on a B200.
+#ifndef ZG_FAST_TY
+#define ZG_FAST_TY 8
+#endif
+#ifndef ZG_FAST_GY
+#define ZG_FAST_GY 4
+#endif
+#ifndef ZG_FAST_FACES_MINB
+#define ZG_FAST_FACES_MINB 4
+#endif
+#ifndef ZG_FAST_GP_MINB
+#define ZG_FAST_GP_MINB 7
+#endif
+constexpr int BLOCK = 128, TX = 32, TY = ZG_FAST_TY;  // faces: 32 x TY threads, 31 x (TY - 1) interior cells
+constexpr int GX = 32, GY = ZG_FAST_GY;               // gradients + predictor: 32 x GY cells
+constexpr int FMINB = ZG_FAST_FACES_MINB, GMINB = ZG_FAST_GP_MINB;
 
 static inline unsigned blocks(int n) { return (unsigned)((n + BLOCK - 1) / BLOCK); }
 
@@ -20,9 +37,9 @@ static void grad_predict(const SmfArgs &a, const Fields<double> &f, bool predict
     dim3 block(GX, GY);
     dim3 grid((a.mesh.ny + GX - 1) / GX, (a.mesh.nx + GY - 1) / GY);
     if (predict)
-        tiled::k_grad_predict<double, false, true, LIM, GX, GY><<<grid, block, 0, s>>>(a, f);
+        tiled::k_grad_predict<double, false, true, LIM, GX, GY, GMINB><<<grid, block, 0, s>>>(a, f);
     else
-        tiled::k_grad_predict<double, false, false, LIM, GX, GY><<<grid, block, 0, s>>>(a, f);
+        tiled::k_grad_predict<double, false, false, LIM, GX, GY, GMINB><<<grid, block, 0, s>>>(a, f);
 }
 
 void launch_grad_predict(const SmfArgs &a, const Fields<double> &f, bool predict, void *stream) {
@@ -40,10 +57,10 @@ void launch_faces(const SmfArgs &a, const Fields<double> &f, int mode, void *str
     dim3 grid((a.mesh.ny + TX - 2) / (TX - 1), (a.mesh.nx + TY - 2) / (TY - 1));
     cudaStream_t s = (cudaStream_t)stream;
     switch (mode) {
-        case 0: tiled::k_faces<double, false, 0, TX, TY><<<grid, block, 0, s>>>(a, f); break;
-        case 1: tiled::k_faces<double, false, 1, TX, TY><<<grid, block, 0, s>>>(a, f); break;
-        case 2: tiled::k_faces<double, false, 2, TX, TY><<<grid, block, 0, s>>>(a, f); break;
-        default: tiled::k_faces<double, false, 3, TX, TY><<<grid, block, 0, s>>>(a, f); break;
+        case 0: tiled::k_faces<double, false, 0, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
+        case 1: tiled::k_faces<double, false, 1, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
+        case 2: tiled::k_faces<double, false, 2, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
+        default: tiled::k_faces<double, false, 3, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
     }
 }
 

@@ -346,6 +346,17 @@ struct CellTile {
     unsigned char in[ROWS][COLS];
 };
 
+// x wrapped into [0, n) for x >= -n: a compare and an add in the common case
+// instead of an integer division.
+__device__ __forceinline__ int wrap_idx(int x, int n) {
+    if (x < 0) x += n;
+    if (x >= n) {
+        x -= n;
+        if (x >= n) x %= n;
+    }
+    return x;
+}
+
 // Global cell of tile entry (a, b) for a tile whose entry (H, H) is (i0, j0):
 // returns false outside a non-periodic side.
 __device__ inline bool tile_cell(const StructMesh &m, int i0, int j0, int a, int b, int H, int &gi, int &gj) {
@@ -353,11 +364,11 @@ __device__ inline bool tile_cell(const StructMesh &m, int i0, int j0, int a, int
     gj = j0 + b - H;
     if (gi < 0 || gi >= m.nx) {
         if (!m.xper) return false;
-        gi = (gi + m.nx) % m.nx;
+        gi = wrap_idx(gi, m.nx);
     }
     if (gj < 0 || gj >= m.ny) {
         if (!m.yper) return false;
-        gj = (gj + m.ny) % m.ny;
+        gj = wrap_idx(gj, m.ny);
     }
     return true;
 }
@@ -366,8 +377,8 @@ __device__ inline bool tile_cell(const StructMesh &m, int i0, int j0, int a, int
 // Pass A: limited gradients of w (stored) and, for the predictor-corrector,
 // the half step (sm_fluid.cpp:176-253) of every cell.  Block TX x TY cells
 // (x = j, contiguous in memory), stencil staged with a one-cell halo.
-template <typename R, bool MIXED, bool PREDICT, int LIM, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY, (sizeof(R) == 8 ? 4 : 6)) k_grad_predict(SmfArgs a, Fields<R> f) {
+template <typename R, bool MIXED, bool PREDICT, int LIM, int TX, int TY, int MINB = (sizeof(R) == 8 ? 4 : 6)>
+__global__ void __launch_bounds__(TX *TY, MINB) k_grad_predict(SmfArgs a, Fields<R> f) {
     constexpr int ROWS = TY + 2, COLS = TX + 2;
     __shared__ CellTile<R, 5, ROWS, COLS> t;
     const StructMesh &m = a.mesh;
@@ -500,13 +511,13 @@ struct FaceSmem {
     R g[8][TY + 1][TX + 1];   // gradients (x: 0-3, y: 4-7)
     int w[TY + 1][TX + 1];    // isolation counters
     unsigned char in[TY + 1][TX + 1];
-    double fx[TY][TX][4];
-    double fy[TY][TX][4];
+    R fx[TY][TX][4];  // face fluxes as computed (in R; widened exactly for the FP64 sums)
+    R fy[TY][TX][4];
     unsigned long long red[TX * TY / 32];
 };
 
-template <typename R, bool MIXED, int MODE, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY) k_faces(SmfArgs a, Fields<R> f) {
+template <typename R, bool MIXED, int MODE, int TX, int TY, int MINB = 1>
+__global__ void __launch_bounds__(TX *TY, MINB) k_faces(SmfArgs a, Fields<R> f) {
     __shared__ FaceSmem<R, TX, TY> sm;
     const StructMesh &m = a.mesh;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -565,7 +576,7 @@ __global__ void __launch_bounds__(TX *TY) k_faces(SmfArgs a, Fields<R> f) {
     // ---- the right (+x) and top (+y) face of the owner cell (ty, tx) ----
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
-        double out[4] = {0.0, 0.0, 0.0, 0.0};
+        R out[4] = {R(0), R(0), R(0), R(0)};
         const bool needed = dir == 0 ? tx >= 1 : ty >= 1;
         const int raB = dir == 0 ? ty + 1 : ty, cbB = dir == 0 ? tx : tx + 1;
         const bool inA = sm.in[ty][tx], inB = sm.in[raB][cbB];
@@ -574,18 +585,18 @@ __global__ void __launch_bounds__(TX *TY) k_faces(SmfArgs a, Fields<R> f) {
             int giA = i0 + ty - 1, gjA = j0 + tx - 1;
             int giB = giA + (dir == 0), gjB = gjA + (dir == 1);
             if (m.xper) {
-                giA = (giA + m.nx) % m.nx;
-                giB = (giB + m.nx) % m.nx;
+                giA = wrap_idx(giA, m.nx);
+                giB = wrap_idx(giB, m.nx);
             }
             if (m.yper) {
-                gjA = (gjA + m.ny) % m.ny;
-                gjB = (gjB + m.ny) % m.ny;
+                gjA = wrap_idx(gjA, m.ny);
+                gjB = wrap_idx(gjB, m.ny);
             }
             const int sA = dir == 0 ? 1 : 3, sB = dir == 0 ? 0 : 2;
             P5<R> zm, zp;
             bool robust;
             int s_own;
-            double sgn = 1.0;
+            R sgn = R(1);
             if (inA && inB) {
                 s_own = sA;
                 P5<R> zA = cell(ty, tx), zB = cell(raB, cbB);
@@ -602,7 +613,7 @@ __global__ void __launch_bounds__(TX *TY) k_faces(SmfArgs a, Fields<R> f) {
                 const bool own_a = inA;
                 const int ra = own_a ? ty : raB, cb = own_a ? tx : cbB;
                 s_own = own_a ? sA : sB;
-                sgn = own_a ? 1.0 : -1.0;
+                sgn = own_a ? R(1) : R(-1);
                 const int flag = m.bc[s_own];
                 P5<R> zo = cell(ra, cb);
                 robust = robust_on && sm.w[ra][cb] > 0;
@@ -613,12 +624,12 @@ __global__ void __launch_bounds__(TX *TY) k_faces(SmfArgs a, Fields<R> f) {
             to_local(s_own, zp.u, zp.v);
             C4<R> lf = (robust || a.flux == FLUX_HLL) ? hll(zm, zp, eos) : hllc(zm, zp, eos);
             to_global(s_own, lf.mu, lf.mv);
-            out[0] = sgn * (double)lf.r;
-            out[1] = sgn * (double)lf.mu;
-            out[2] = sgn * (double)lf.mv;
-            out[3] = sgn * (double)lf.E;
+            out[0] = sgn * lf.r;
+            out[1] = sgn * lf.mu;
+            out[2] = sgn * lf.mv;
+            out[3] = sgn * lf.E;
         }
-        double(*dst)[TX][4] = dir == 0 ? sm.fx : sm.fy;
+        R(*dst)[TX][4] = dir == 0 ? sm.fx : sm.fy;
 #pragma unroll
         for (int k = 0; k < 4; ++k) dst[ty][tx][k] = out[k];
     }
@@ -634,8 +645,9 @@ __global__ void __launch_bounds__(TX *TY) k_faces(SmfArgs a, Fields<R> f) {
         double F[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            F[k] = ((-sm.fx[ty - 1][tx][k] * hy + sm.fx[ty][tx][k] * hy) - sm.fy[ty][tx - 1][k] * hx) +
-                   sm.fy[ty][tx][k] * hx;
+            F[k] = ((-(double)sm.fx[ty - 1][tx][k] * hy + (double)sm.fx[ty][tx][k] * hy) -
+                    (double)sm.fy[ty][tx - 1][k] * hx) +
+                   (double)sm.fy[ty][tx][k] * hx;
         const double coef = dt / m.vol;
         C4<double> q;
         if (MODE == 3) {
