@@ -345,6 +345,7 @@ AMR_TIMED_STEPS = 400  # steps 100 to 500
 AMR_EVERY = 10         # set_flags + refine every AMR_EVERY steps
 AMR_B_ALG = 160 + 36   # bytes per cell-update: the FP64 two-stage step plus the slot-mesh neighbour indices
 AMR_CELL_BYTES = 600   # bytes of one cell's AmrCells arrays (63 doubles, 22 ints, 16 bytes)
+AMR_KERNELS = "fast"   # kernel family of the AMR step: "fast" (slot FAST) or "parity" (bit-exact)
 
 
 def _amr_setup(Z, init_state, mesh, solver):
@@ -397,11 +398,12 @@ def amr_cpu_reference(budget_s=12.0):
                       f"sources (oracle/_ref); {threads} std::threads"}
 
 
-def amr_variant(torch, lib, dev, stream, local_rank, want_cpu):
+def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None):
     """The quadtree AMR blast: base 512^2, 3 levels, the reference's
     SmFluid::set_flags criterion and slope distributor, adaptation every 10
-    steps, the PARITY FP64 step on the slot mesh (bit-exact with the
-    reference).  Times steps 100-500 including every set_flags + refine."""
+    steps; the FP64 step on the slot mesh with the FAST kernels (derived face
+    geometry) or the PARITY kernels (bit-exact with the reference).  Times
+    steps 100-500 including every set_flags + refine."""
     import zephyr_b200 as Z
     from zephyr_b200._lib import KERNEL_KINDS
     from zephyr_b200.workloads import blast_cell_means
@@ -410,7 +412,9 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu):
     gen.set_sizes(AMR_BASE, AMR_BASE)
     mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
     mesh.set_max_level(AMR_LEVELS, AMR_CAPACITY)
-    solver = Z.SmFluid(Z.IdealGas(1.4))
+    kernels_name = kernels_name or AMR_KERNELS
+    kernels = Z.Kernels.FAST if kernels_name == "fast" else Z.Kernels.PARITY
+    solver = Z.SmFluid(Z.IdealGas(1.4), kernels=kernels)
     solver.add_types(mesh)
     solver.set_accuracy(2)
     solver.set_CFL(0.4)
@@ -467,8 +471,11 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu):
     out = {
         "workload": f"AMR blast, base {AMR_BASE}x{AMR_BASE}, max_level {AMR_LEVELS}, ZOE; rho = 1, u = v = 0, "
                     f"p = 1e-5 except p = 1e3 for r < 0.01 at (0.5, 0.5), 20x20 sub-sampled cell means",
-        "form": "FP64 PARITY kernels on the slot mesh, bit-exact with the reference (SmFluid second order, "
-                "predictor-corrector, HLLC, van Albada 1, CFL 0.4; set_flags criterion; slope distributor)",
+        "form": ("FP64 FAST kernels on the slot mesh (face geometry from centre and level, fused multiply-adds; "
+                 "within 1e-12 of the parity form per step)" if kernels_name == "fast" else
+                 "FP64 PARITY kernels on the slot mesh, bit-exact with the reference") +
+                " -- SmFluid second order, predictor-corrector, HLLC, van Albada 1, CFL 0.4; set_flags criterion; "
+                "slope distributor",
         "value": updates / (ms / 1e3), "unit": METRIC, "timed_steps": AMR_TIMED_STEPS,
         "window": f"steps {AMR_WARM_STEPS}-{AMR_WARM_STEPS + AMR_TIMED_STEPS}", "adapt_every": AMR_EVERY,
         "ms_total": ms, "ms_per_step_incl_adapt": ms / AMR_TIMED_STEPS,
@@ -623,12 +630,14 @@ def run_ours(args, rank, world, local_rank):
                     want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     adjv = adjoint_variant(torch, dev, stream, local_rank)
     amr = amr_variant(torch, lib, dev, stream, local_rank,
-                      want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
+                      want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), kernels_name="fast")
+    amr_par = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="parity")
 
     vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
-                                   amr["ms_total"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr = vals
+                                   amr["ms_total"], amr_par["ms_total"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par = vals
     amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
+    amr_par["value"] = world * amr_par["value"] * amr_par["ms_total"] / ms_amr_par
     for v in variants.values():
         v["mesh"].close()
     if rank != 0:
@@ -655,7 +664,8 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
-                            mm["launches"] + adjv["gpu_launches"] + amr["gpu_launches"]),
+                            mm["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
+                            amr_par["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
@@ -681,6 +691,9 @@ def run_ours(args, rank, world, local_rank):
                 "kernels": mm["kernels"], "cpu_baseline": mm.get("cpu_baseline")},
             "adjoint": adjv,
             "amr": amr,
+            "amr_parity": {k: amr_par[k] for k in ("form", "value", "unit", "ms_per_step_incl_adapt",
+                                                     "step_only_value", "adapt_ms_avg", "live_cells",
+                                                     "gpu_launches", "kernels")},
         },
         "dt_last": dt_last,
     }

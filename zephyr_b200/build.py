@@ -35,6 +35,7 @@ UNITS = {
     # AMR refine: geometry and distributed states bit-exact with the reference
     "amr_refine.cu": ["-fmad=false"],
     "smf_fast.cu": [],
+    "smf_slot_fast.cu": [],
     "adj.cu": [],
     # FP32 face arithmetic: approximate single-precision division and square
     # root; FP64 operations are unaffected by these flags.

@@ -31,6 +31,8 @@ struct FaceG {
 // Uniform rectangle.
 struct StructAcc {
     static constexpr int NSLOT = 4;
+    static constexpr bool UNIT_NORMALS = true;  // axis normals: no normalisation
+    static constexpr bool LSM_TWO_PASS = false;
     const StructMesh &m;
     int ic, i, j;
     __device__ StructAcc(const SmfArgs &a, int ic_) : m(a.mesh), ic(ic_) {
@@ -93,6 +95,8 @@ struct StructAcc {
 // Mesh given slot by slot (AMR).
 struct SlotAcc {
     static constexpr int NSLOT = 8;
+    static constexpr bool UNIT_NORMALS = false;
+    static constexpr bool LSM_TWO_PASS = false;
     const SlotMesh &m;
     int ic;
     __device__ SlotAcc(const SmfArgs &a, int ic_) : m(a.smesh), ic(ic_) {}
@@ -111,6 +115,64 @@ struct SlotAcc {
         g.fcx = m.fcx[f];
         g.fcy = m.fcy[f];
         g.area = m.fa[f];
+        return g;
+    }
+    __device__ void nb_center(const FaceG &g, int, double &ncx, double &ncy) const {
+        ncx = m.cx[g.nb];
+        ncy = m.cy[g.nb];
+    }
+};
+
+// Slot accessor of an adaptive rectangle (a quadtree of axis-aligned cells):
+// the face geometry follows from the cell's centre, its level and the slot,
+// so per slot only the boundary flag and the neighbour are read.  Slot side
+// (0 L, 1 R, 2 B, 3 T) holds the whole side, or, when slot side + 4 is
+// defined, its first half (lower / left along the side) and side + 4 the
+// second half (subface_nodes2d).  Used by the FAST slot kernels; on dyadic
+// meshes it reproduces the stored geometry exactly.
+struct SlotFastAcc {
+    static constexpr int NSLOT = 8;
+    static constexpr bool UNIT_NORMALS = true;
+    static constexpr bool LSM_TWO_PASS = true;
+    const SlotMesh &m;
+    int ic;
+    double hx, hy, pcx, pcy;
+    __device__ SlotFastAcc(const SmfArgs &a, int ic_) : m(a.smesh), ic(ic_) {
+        const int L = m.level[ic];
+        hx = ldexp(m.hx0, -L);
+        hy = ldexp(m.hy0, -L);
+        pcx = m.cx[ic];
+        pcy = m.cy[ic];
+    }
+    __device__ static int n(const SmfArgs &a) { return a.smesh.n; }
+    __device__ double cx() const { return pcx; }
+    __device__ double cy() const { return pcy; }
+    __device__ double vol() const { return m.vol[ic]; }
+    __device__ double dinc() const { return m.inc[ic]; }
+    __device__ FaceG face(int s) const {
+        const int f = 8 * ic + s;
+        FaceG g;
+        g.flag = m.fb[f];
+        if (g.flag == BC_UNDEFINED) return g;
+        g.nb = m.fn[f];
+        const int side = s & 3;
+        const bool split = s >= 4 || m.fb[f + 4] != BC_UNDEFINED;
+        const double q = s >= 4 ? 0.25 : -0.25;  // offset of a half face along the side
+        if (side < 2) {
+            const bool hi = side == 1;
+            g.nx = hi ? 1.0 : -1.0;
+            g.ny = hi ? 0.0 : -0.0;
+            g.fcx = pcx + (hi ? 0.5 : -0.5) * hx;
+            g.fcy = split ? pcy + q * hy : pcy;
+            g.area = split ? 0.5 * hy : hy;
+        } else {
+            const bool hi = side == 3;
+            g.nx = hi ? 0.0 : -0.0;
+            g.ny = hi ? 1.0 : -1.0;
+            g.fcx = split ? pcx + q * hx : pcx;
+            g.fcy = pcy + (hi ? 0.5 : -0.5) * hy;
+            g.area = split ? 0.5 * hx : hx;
+        }
         return g;
     }
     __device__ void nb_center(const FaceG &g, int, double &ncx, double &ncy) const {
@@ -172,7 +234,7 @@ template <class Acc>
 __device__ inline void frame(const FaceG &g, double &c, double &s) {
     c = g.nx;
     s = g.ny;
-    if (Acc::NSLOT == 8) {
+    if (!Acc::UNIT_NORMALS) {
         double sn = g.nx * g.nx + g.ny * g.ny;
         if (sn > 0.0) {
             double r = sqrt(sn);
@@ -184,8 +246,8 @@ __device__ inline void frame(const FaceG &g, double &c, double &s) {
 
 // ---------------------------------------------------------------------------
 // K1: CFL minimum over cells (sm_fluid.cpp:104-114, amr_cells.cpp:107-116).
-template <class Acc, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_dt(SmfArgs a) {
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_dt(SmfArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
     if (ic < Acc::n(a)) {
@@ -247,8 +309,8 @@ __device__ inline void update(Cons &q, double coef, const Cons &F) {
 
 // ---------------------------------------------------------------------------
 // K2: first-order step (sm_fluid.cpp:127-174).
-template <class Acc, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_flux1(SmfArgs a) {
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_flux1(SmfArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
     Acc c(a, ic);
@@ -352,14 +414,95 @@ __device__ inline void lsm_limited(const Acc &c, const PrimPtr &z, int lim, cons
     }
 }
 
-template <class Acc, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_grad(SmfArgs a, PrimPtr z) {
+// The same computation in two passes over the slots that both evaluate the
+// slot's geometry and neighbour difference (the second pass re-reads them),
+// instead of holding eight slots' worth of them in registers: same
+// operations, same results, a fraction of the registers.
+template <class Acc>
+__device__ inline void lsm_limited_2pass(const Acc &c, const PrimPtr &z, int lim, const Prim &zc, double gx[4],
+                                         double gy[4]) {
+    constexpr int NS = Acc::NSLOT;
+    const double pcx = c.cx(), pcy = c.cy();
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
+    double Fx[4] = {0.0, 0.0, 0.0, 0.0}, Fy[4] = {0.0, 0.0, 0.0, 0.0};
+    const double zcv[4] = {zc.r, zc.u, zc.v, zc.p};
+    struct SlotTerms {
+        double w, rx, ry, nxx, nyy, dF[4];
+    };
+    auto terms = [&](const FaceG &g, int s, SlotTerms &t) {
+        Prim zn = !is_boundary(g.flag) ? load_prim(z, g.nb) : boundary_value(zc, g.nx, g.ny, g.flag);
+        double ncx, ncy;
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
+        t.rx = ncx - pcx;
+        t.ry = ncy - pcy;
+        double d = t.rx * g.nx + t.ry * g.ny;
+        t.nxx = d * g.nx;
+        t.nyy = d * g.ny;
+        t.w = g.area / cube_rn(sqrt(t.nxx * t.nxx + t.nyy * t.nyy));
+        const double znv[4] = {zn.r, zn.u, zn.v, zn.p};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) t.dF[k] = znv[k] - zcv[k];
+    };
+#pragma unroll 1
+    for (int s = 0; s < NS; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        SlotTerms t;
+        terms(g, s, t);
+        double wdx = t.w * t.nxx, wdy = t.w * t.nyy;
+        A00 += wdx * t.rx;
+        A01 += wdx * t.ry;
+        A10 += wdy * t.rx;
+        A11 += wdy * t.ry;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            Fx[k] += t.w * t.dF[k] * t.nxx;
+            Fy[k] += t.w * t.dF[k] * t.nyy;
+        }
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;  // 1-D case (gradient.h:270-272)
+    double det = A11 * A00 + (-A01) * A10;
+    double inv = 1.0 / det;
+    double B00 = A11 * inv, B01 = (-A01) * inv, B10 = (-A10) * inv, B11 = A00 * inv;
+    double g0x[4], g0y[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        g0x[k] = B00 * Fx[k] + B01 * Fy[k];
+        g0y[k] = B10 * Fx[k] + B11 * Fy[k];
+    }
+    double Lx[4] = {0.0, 0.0, 0.0, 0.0}, Ly[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int s = 0; s < NS; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        SlotTerms t;
+        terms(g, s, t);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            double dF_p = t.dF[k];
+            double du_n = g0x[k] * t.rx + g0y[k] * t.ry;
+            double dF_m = 2.0 * du_n - dF_p;
+            double dF_lim = limiter2(lim, dF_m, dF_p) * dF_p;
+            Lx[k] += t.w * dF_lim * t.nxx;
+            Ly[k] += t.w * dF_lim * t.nyy;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        gx[k] = B00 * Lx[k] + B01 * Ly[k];
+        gy[k] = B10 * Lx[k] + B11 * Ly[k];
+    }
+}
+
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_grad(SmfArgs a, PrimPtr z) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
     Acc c(a, ic);
     Prim zc = load_prim(z, ic);
     double gx[4], gy[4];
-    lsm_limited(c, z, a.limiter, zc, gx, gy);
+    if constexpr (Acc::LSM_TWO_PASS) lsm_limited_2pass(c, z, a.limiter, zc, gx, gy);
+    else lsm_limited(c, z, a.limiter, zc, gx, gy);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         a.gx[k][ic] = gx[k];
@@ -381,8 +524,8 @@ __device__ inline Prim extrap(const Prim &u, const SmfArgs &a, int ic, double dx
 
 // ---------------------------------------------------------------------------
 // K4: predictor, half step with the physical flux (sm_fluid.cpp:176-253).
-template <class Acc, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_stage1(SmfArgs a) {
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_stage1(SmfArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
     Acc c(a, ic);
@@ -458,8 +601,8 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &zh, const
 
 // K5: corrector with the isolation bit (sm_fluid.cpp:255-366).  `wait` is
 // read from the previous step's array and written to the other one.
-template <class Acc, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_stage2(SmfArgs a) {
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_stage2(SmfArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
     Acc c(a, ic);
@@ -498,8 +641,8 @@ __global__ void __launch_bounds__(BLOCK) k_stage2(SmfArgs a) {
 // corrector with z_half = z, no isolation):
 //   stage A: z* = P(Q(z^n) - dt/V * sum F(z^n))
 //   stage B: z^{n+1} = P(0.5 * (Q(z^n) + Q(z*) - dt/V * sum F(z*)))
-template <class Acc, int BLOCK, bool FINAL>
-__global__ void __launch_bounds__(BLOCK) k_heun(SmfArgs a, PrimPtr zin, PrimPtr zout) {
+template <class Acc, int BLOCK, bool FINAL, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_heun(SmfArgs a, PrimPtr zin, PrimPtr zout) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
     Acc c(a, ic);
@@ -531,8 +674,8 @@ __global__ void __launch_bounds__(BLOCK) k_heun(SmfArgs a, PrimPtr zin, PrimPtr 
 
 // ---------------------------------------------------------------------------
 // AMR flags by neighbour jumps (sm_fluid.cpp:517-559).
-template <class Acc, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_flags(SmfArgs a, int *flags) {
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_flags(SmfArgs a, int *flags) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
     Acc c(a, ic);

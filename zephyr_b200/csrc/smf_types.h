@@ -30,6 +30,10 @@ struct SlotMesh {
     const double *cx, *cy, *vol, *inc;  // centre, volume, incircle diameter
     const int *fb, *fn;                 // per slot: boundary flag, neighbour cell
     const double *fnx, *fny, *fcx, *fcy, *fa;  // per slot: normal, centre, area
+    // adaptive rectangle only: cell levels and the base cell size (a cell of
+    // level L is hx0 / 2^L by hy0 / 2^L, axis-aligned); null level otherwise
+    const int *level;
+    double hx0, hy0;
 };
 
 struct PrimPtr {
@@ -62,5 +66,15 @@ void launch_stage2(const SmfArgs &a, bool slots, void *stream);
 void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, bool slots, void *stream);
 void launch_flags(const SmfArgs &a, int *flags, bool slots, void *stream);
 }  // namespace parity
+
+// FAST kernels on an adaptive rectangle (SlotFastAcc; smf_slot_fast.cu).
+namespace slotfast {
+void launch_dt(const SmfArgs &a, PrimPtr z, void *stream);
+void launch_flux1(const SmfArgs &a, void *stream);
+void launch_grad(const SmfArgs &a, PrimPtr z, void *stream);
+void launch_stage1(const SmfArgs &a, void *stream);
+void launch_stage2(const SmfArgs &a, void *stream);
+void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream);
+}  // namespace slotfast
 
 }  // namespace zg

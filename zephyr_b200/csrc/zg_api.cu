@@ -175,6 +175,7 @@ void free_mesh(zg_ctx *c) {
     c->amr = false;
     c->av = amr::View{};
     c->amr_last = zg_amr_stats{};
+    c->smesh = SlotMesh{};
     c->slots = false;
     c->have_mesh = false;
     c->cap = 0;
@@ -445,9 +446,38 @@ int enqueue_tiled_step(zg_ctx *c) {
     return ZG_OK;
 }
 
+// The FAST step on an adaptive rectangle: the gather-form kernels of the
+// parity step over derived face geometry, with fused multiply-adds.
+int enqueue_slot_fast_step(zg_ctx *c) {
+    SmfArgs a = make_args(c);
+    void *st = (void *)c->stream;
+    timed(c, ZG_K_DT, [&] { slotfast::launch_dt(a, c->z, st); });
+    if (c->par.accuracy == 1) {
+        timed(c, ZG_K_FLUX1, [&] { slotfast::launch_flux1(a, st); });
+    } else if (c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->z, st); });
+        timed(c, ZG_K_STAGE1, [&] { slotfast::launch_stage1(a, st); });
+        timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2(a, st); });
+        c->wait_cur = 1 - c->wait_cur;
+    } else {
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->z, st); });
+        timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun(a, c->z, c->zhalf, false, st); });
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->zhalf, st); });
+        timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun(a, c->zhalf, c->znext, true, st); });
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    std::swap(c->z, c->znext);
+    c->cfl_valid = false;
+    c->stepped = true;
+    return ZG_OK;
+}
+
 int enqueue_step(zg_ctx *c) {
+    if (c->amr && c->par.precision == ZG_FP64 && c->par.kernels == ZG_KERNELS_FAST) return enqueue_slot_fast_step(c);
     if (c->slots && (c->par.precision == ZG_MIXED || c->par.kernels == ZG_KERNELS_FAST))
-        return fail(c, ZG_ERR_STATE, "the FAST and MIXED kernels need a rectangle mesh (zg_mesh_rectangle)");
+        return fail(c, ZG_ERR_STATE,
+                    "the MIXED kernels need a rectangle mesh; the FAST kernels a rectangle or an adaptive rectangle");
     if (c->par.precision == ZG_MIXED) {
         int rc = convert_state(c, ZG_MIXED);
         if (rc != ZG_OK) return rc;
@@ -1382,6 +1412,7 @@ void amr_carve(zg_ctx *c, size_t cap) {
     m.cy = v.cy;
     m.vol = v.vol;
     m.inc = inc;
+    m.level = v.level;
     m.fb = v.fb;
     m.fn = v.fadj;
     m.fnx = v.fnx;
@@ -1453,6 +1484,8 @@ int zg_amr_enable(zg_ctx *c, int max_level, int capacity) {
     for (int k = 0; k < 4; ++k) r.bc[k] = c->mesh.bc[k];
     r.xper = c->mesh.xper;
     r.yper = c->mesh.yper;
+    c->smesh.hx0 = (r.x_max - r.x_min) / r.nx;  // amr_cells_gen.cpp:138-139
+    c->smesh.hy0 = (r.y_max - r.y_min) / r.ny;
     amr::View v = c->av;
     v.n = c->n;
     if (amr::init_rect(v, r, const_cast<double *>(c->smesh.inc), c->stream) != 0)
