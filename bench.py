@@ -307,9 +307,10 @@ def mm_cpu_reference(w, steps_budget_s=10.0):
                       f"MmFluid::update compiled from its sources (oracle/_ref); {threads} threads"}
 
 
-def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu):
+def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, precision=None):
     """The multi-material step (MmFluid, first order, CRP + PLIC) on the
-    two-material shock / water-column problem, 1024 x 1024."""
+    two-material shock / water-column problem, 1024 x 1024; FP64 (bit-exact)
+    or the mixed form."""
     import zephyr_b200 as Z
     from zephyr_b200.mmf import Material, MixturePT, MmFluid
     from zephyr_b200.workloads import shock_water_column
@@ -321,6 +322,8 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu):
     solver = MmFluid(MixturePT([Material.stiffened("Water"), Material.ideal("Air")]))
     solver.set_CFL(0.4)
     solver.add_types(mesh)
+    if precision is not None:
+        solver.set_precision(precision)
     solver.make_states(mesh, w.rho, w.vx, w.vy, w.p, w.beta)
     solver.update(mesh, W)
     mesh.synchronize()
@@ -330,7 +333,8 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu):
     out = {"workload": f"shock_water_column {w.nx}x{w.ny} (water column in air, planar shock, "
                        "StiffenedGas Water + IdealGas Air)",
            "form": "FP64, bit-exact with the reference (MmFluid first order, CRP + PLIC, CFL 0.4)",
-           "ms": ms, "kernels": kernels, "launches": launches, "cells": cells}
+           "ms": ms, "kernels": kernels, "launches": launches, "cells": cells,
+           "final": solver.states(mesh) if precision is not None else None}
     mesh.close()
     if want_cpu:
         out["cpu_baseline"] = mm_cpu_reference(w)
@@ -627,15 +631,20 @@ def run_ours(args, rank, world, local_rank):
     m_ref.close()
 
     mm = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
-                    want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
+                    want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), precision=Z.Precision.FP64)
+    mm_mx = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
+                       precision=Z.Precision.MIXED)
+    z64, zmx = mm.pop("final"), mm_mx.pop("final")
+    mm_err = {f"l1_rel_{name}_err_vs_fp64": float(np.sum(np.abs(zmx[:, k] - z64[:, k])) / np.sum(np.abs(z64[:, k])))
+              for name, k in (("density", 0), ("pressure", 3))}
     adjv = adjoint_variant(torch, dev, stream, local_rank)
     amr = amr_variant(torch, lib, dev, stream, local_rank,
                       want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), kernels_name="fast")
     amr_par = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="parity")
 
     vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
-                                   amr["ms_total"], amr_par["ms_total"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par = vals
+                                   amr["ms_total"], amr_par["ms_total"], mm_mx["ms"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx = vals
     amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
     amr_par["value"] = world * amr_par["value"] * amr_par["ms_total"] / ms_amr_par
     for v in variants.values():
@@ -664,7 +673,7 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
-                            mm["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
+                            mm["launches"] + mm_mx["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
                             amr_par["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
@@ -689,6 +698,14 @@ def run_ours(args, rank, world, local_rank):
                 "step_frac": MM_B_ALG * mm["cells"] * K / (ms_mm / 1e3) / 1e9 / peak,
                 "algorithmic_bytes_per_cell": MM_B_ALG, "gpu_launches": int(mm["launches"]),
                 "kernels": mm["kernels"], "cpu_baseline": mm.get("cpu_baseline")},
+            "multimaterial_mixed": {
+                "value": world * mm_mx["cells"] * K / (ms_mm_mx / 1e3), "unit": METRIC,
+                "ms_per_step": ms_mm_mx / K, "speedup_vs_fp64": ms_mm / ms_mm_mx,
+                "form": "FP32 face states, wave speeds and HLLC fluxes of the pure-stencil faces (IEEE, no FMA); "
+                        "FP64 accumulation, update, EoS pressure recovery, composite Riemann fluxes, "
+                        "PT closure, PLIC and dt",
+                **mm_err, "err_after_steps": W + K, "kernels": mm_mx["kernels"],
+                "gpu_launches": int(mm_mx["launches"])},
             "adjoint": adjv,
             "amr": amr,
             "amr_parity": {k: amr_par[k] for k in ("form", "value", "unit", "ms_per_step_incl_adapt",

@@ -159,8 +159,10 @@ int zg_mesh_upload(zg_ctx *ctx, const zg_mesh_view *mesh);
 /* ---- Adaptive mesh on the device ------------------------------------------
  * A rectangle mesh made adaptive keeps zephyr's AmrCells layout on the GPU
  * (9 map points, level, z-index and 8 face slots per cell) with room for
- * `capacity` cells.  The step then runs the PARITY kernels over the face
- * slots, and zg_amr_refine adapts the mesh to the cells' flags on the GPU.
+ * `capacity` cells.  The step then runs over the face slots with the PARITY
+ * kernels (bit-exact) or the FAST kernels (FP64, face geometry derived from
+ * each cell's centre and level), and zg_amr_refine adapts the mesh to the
+ * cells' flags on the GPU.
  * Cell order, geometry, connectivity and distributed states match the
  * reference's EuMesh::refine on one rank bit for bit. */
 
@@ -320,6 +322,10 @@ typedef struct zg_mmf_params {
     int accuracy;             /* 1 (set_accuracy) */
     double CFL;               /* clamped to [0, 1] (set_CFL) */
     double max_dt;            /* set_max_dt */
+    int precision;            /* zg_precision: FP64 (the reference's arithmetic) or MIXED (FP32 face
+                                 states, wave speeds and HLLC fluxes of the pure-stencil faces; FP64
+                                 accumulation, update, EoS pressure recovery, composite Riemann
+                                 fluxes, PLIC and dt) */
 } zg_mmf_params;
 
 /* MmFluid's constructor defaults (mm_fluid.cpp:16-26): CRP with PLIC,

@@ -29,6 +29,12 @@ UNITS = {
     "zg_api.cu": [],
     "smf_parity.cu": ["-fmad=false"],
     "mmf_parity.cu": ["-fmad=false"],
+    # the multi-material mixed form: FP32 face arithmetic with IEEE division
+    # and square root and no fused multiply-adds.  With either, the HLLC
+    # terms of two equal states no longer cancel exactly: spurious mass
+    # fluxes of a few ulps in quiescent water (1e-6 in density after 500
+    # steps) and a slower step.
+    "mmf_mixed.cu": ["-fmad=false"],
     # allocation-free first-order step; its device-built coordinate tables
     # must match the host-built ones, hence no fused multiply-adds
     "zg_noalloc.cu": ["-fmad=false"],

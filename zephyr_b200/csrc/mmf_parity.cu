@@ -9,14 +9,10 @@
 
 #include <algorithm>
 
-#include "mmf_types.h"
-#include "smf_struct.cuh"
+#include "mmf_pure.cuh"
 
 namespace zg {
 namespace mmf {
-
-constexpr int BLOCK = 128;
-constexpr int NM = NMAT;
 
 __device__ __forceinline__ MSt<NM> load(const MmField &f, int ic) {
     MSt<NM> z;
@@ -33,20 +29,6 @@ __device__ __forceinline__ MSt<NM> load(const MmField &f, int ic) {
     }
     return z;
 }
-__device__ __forceinline__ void store(const MmField &f, int ic, const MSt<NM> &z) {
-    f.rho[ic] = z.rho;
-    f.vx[ic] = z.vx;
-    f.vy[ic] = z.vy;
-    f.P[ic] = z.P;
-    f.e[ic] = z.e;
-    f.T[ic] = z.T;
-#pragma unroll
-    for (int i = 0; i < NM; ++i) {
-        f.b[i][ic] = z.b.f[i];
-        f.r[i][ic] = z.r[i];
-    }
-}
-
 // alpha of material i (models.cpp:234-237) for a runtime index
 __device__ __forceinline__ double alpha_rt(const MSt<NM> &z, int idx) {
     double r = z.r[0], b = z.b.f[0];
@@ -232,13 +214,6 @@ __device__ __forceinline__ void to_local(double cs, double sn, double vx, double
     ox = cs * vx + sn * vy + 0.0 * 0.0;
     oy = -sn * vx + cs * vy + 0.0 * 0.0;
 }
-// boundary_value (mm_fluid.cpp:88-97): the wall mirrors the normal velocity
-__device__ __forceinline__ void wall_velocity(const FaceG &g, double vx, double vy, double &ox, double &oy) {
-    double d = vx * g.nx + vy * g.ny + 0.0 * 0.0;
-    ox = vx - 2.0 * (d * g.nx);
-    oy = vy - 2.0 * (d * g.ny);
-}
-
 // One face of the first-order face loop (fluxes, mm_fluid.cpp:385-420):
 // the flux through face s of cell ic, turned back to the global frame and
 // multiplied by the face area.
@@ -268,208 +243,6 @@ __device__ void face_term(const MmArgs &a, int ic, int s, double dt, double *out
     lf.a[2] = my;
 #pragma unroll
     for (int k = 0; k < 4 + NM; ++k) out[k] = lf.a[k] * S;
-}
-
-// --- pure stencils ---------------------------------------------------------
-// A cell whose own state and whose neighbours' states each hold one material
-// only: every face takes calc_flux's plain-HLLC branch (mm_fluid.cpp:358-361)
-// with the materials' own sound speeds (mixture_pt.cpp:101-106), and an
-// update that stays pure takes get_rPT's one-material branch
-// (mixture_pt.cpp:199-208).  The same arithmetic as the general path, in a
-// kernel small enough to keep many warps resident; everything else is
-// handed to the work lists.
-struct PureSt {
-    double rho, vx, vy, P, e;
-    double b[NM];
-    int idx;
-};
-__device__ __forceinline__ void pure_flux_of(const PureSt &z, const MixD<NM> &mx, double *F, double &c) {
-    double E = z.e + 0.5 * (z.vx * z.vx + z.vy * z.vy + 0.0 * 0.0);
-    F[0] = z.rho * z.vx;
-    F[1] = z.rho * z.vx * z.vx + z.P;
-    F[2] = z.rho * z.vx * z.vy;
-    F[3] = (z.rho * E + z.P) * z.vx;
-#pragma unroll
-    for (int i = 0; i < NM; ++i) F[4 + i] = z.rho * z.vx * z.b[i];
-    MatD m = mx.mat[0];
-#pragma unroll
-    for (int i = 1; i < NM; ++i)
-        if (i == z.idx) m = mx.mat[i];
-    c = m_sound_speed_rP(m, z.rho, z.P);
-}
-// hllc (hllc.cpp:344-421) for two one-material states
-__device__ void hllc_pure(const MixD<NM> &mx, const PureSt &zL, const PureSt &zR, double *F, bool &bad) {
-    double FL[4 + NM], FR[4 + NM], c_L, c_R;
-    pure_flux_of(zL, mx, FL, c_L);
-    pure_flux_of(zR, mx, FR, c_R);
-    double S_L = fmin_std(zL.vx - c_L, zR.vx - c_L);
-    double S_R = fmax_std(zL.vx + c_R, zR.vx + c_R);
-    if (S_L >= S_R || zL.idx == zR.idx) {
-        S_L = fmin_std(zL.vx - c_L, zR.vx - c_R);
-        S_R = fmax_std(zL.vx + c_L, zR.vx + c_R);
-    }
-    if (S_L >= 0.0) {
-#pragma unroll
-        for (int k = 0; k < 4 + NM; ++k) F[k] = FL[k];
-        return;
-    }
-    if (S_R <= 0.0) {
-#pragma unroll
-        for (int k = 0; k < 4 + NM; ++k) F[k] = FR[k];
-        return;
-    }
-    double a_L = zL.rho * (S_L - zL.vx);
-    double a_R = zR.rho * (S_R - zR.vx);
-    double S_C = (zL.P - zR.P + a_R * zR.vx - a_L * zL.vx) / (a_R - a_L);
-    if (S_C < S_L) S_C = S_L + 1.0e-9 * fmax_std(c_L, c_R);
-    if (S_C > S_R) S_C = S_R - 1.0e-9 * fmax_std(c_L, c_R);
-    double rho_sL = a_L / (S_L - S_C);
-    double rho_sR = a_R / (S_R - S_C);
-    double E_L = zL.e + 0.5 * (zL.vx * zL.vx + zL.vy * zL.vy + 0.0 * 0.0);
-    double E_R = zR.e + 0.5 * (zR.vx * zR.vx + zR.vy * zR.vy + 0.0 * 0.0);
-    double E_sL = E_L + (S_C - zL.vx) * (S_C + zL.P / a_L);
-    double E_sR = E_R + (S_C - zR.vx) * (S_C + zR.P / a_R);
-    double QsL[4 + NM], QsR[4 + NM], QL[4 + NM], QR[4 + NM];
-    QsL[0] = rho_sL;
-    QsR[0] = rho_sR;
-    QsL[1] = rho_sL * S_C;
-    QsL[2] = rho_sL * zL.vy;
-    QsR[1] = rho_sR * S_C;
-    QsR[2] = rho_sR * zR.vy;
-    QsL[3] = rho_sL * E_sL;
-    QsR[3] = rho_sR * E_sR;
-    QL[0] = zL.rho;
-    QL[1] = zL.rho * zL.vx;
-    QL[2] = zL.rho * zL.vy;
-    QL[3] = zL.rho * E_L;
-    QR[0] = zR.rho;
-    QR[1] = zR.rho * zR.vx;
-    QR[2] = zR.rho * zR.vy;
-    QR[3] = zR.rho * E_R;
-#pragma unroll
-    for (int i = 0; i < NM; ++i) {
-        QsL[4 + i] = rho_sL * zL.b[i];
-        QsR[4 + i] = rho_sR * zR.b[i];
-        QL[4 + i] = zL.rho * zL.b[i];
-        QR[4 + i] = zR.rho * zR.b[i];
-    }
-    double aSC = fabs(S_C);
-#pragma unroll
-    for (int k = 0; k < 4 + NM; ++k) {
-        F[k] = 0.5 * (FL[k] + FR[k] + S_L * (QsL[k] - QL[k]) + aSC * (QsL[k] - QsR[k]) + S_R * (QsR[k] - QR[k]));
-        if (isnan(F[k])) bad = true;
-    }
-}
-__device__ __forceinline__ int pure_index(const MmField &f, int ic) {
-    Frac<NM> b;
-#pragma unroll
-    for (int i = 0; i < NM; ++i) b.f[i] = f.b[i][ic];
-    return frac_index(b);
-}
-__device__ __forceinline__ PureSt load_pure(const MmField &f, int ic, int idx) {
-    PureSt z;
-    z.rho = f.rho[ic];
-    z.vx = f.vx[ic];
-    z.vy = f.vy[ic];
-    z.P = f.P[ic];
-    z.e = f.e[ic];
-#pragma unroll
-    for (int i = 0; i < NM; ++i) z.b[i] = f.b[i][ic];
-    z.idx = idx;
-    return z;
-}
-
-__global__ void __launch_bounds__(BLOCK, 6) k_flux_pure(MmArgs a) {
-    int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= a.mesh.n) return;
-    StructAcc c(a.mesh, ic);
-    int idx_c = pure_index(a.z, ic);
-    bool pure = idx_c >= 0;
-    int idx_n[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        FaceG g = c.face(s);
-        idx_n[s] = is_boundary(g.flag) ? idx_c : pure_index(a.z, g.nb);
-        pure = pure && idx_n[s] >= 0;
-    }
-    if (!pure) {  // a mixed state in the stencil: the general path
-        int k = atomicAdd(&a.counts[0], 1);
-        a.list_crp[k] = ic;
-        return;
-    }
-    const double dt = *a.dt_out;
-    const double V_c = c.vol();
-    PureSt zc = load_pure(a.z, ic, idx_c);
-    double flux[4 + NM];
-#pragma unroll
-    for (int k = 0; k < 4 + NM; ++k) flux[k] = 0.0;
-    bool bad = false;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        FaceG g = c.face(s);
-        PureSt zn;
-        if (!is_boundary(g.flag)) {
-            zn = load_pure(a.z, g.nb, idx_n[s]);
-        } else {
-            zn = zc;
-            if (g.flag == BC_WALL) wall_velocity(g, zc.vx, zc.vy, zn.vx, zn.vy);
-        }
-        const double cs = g.nx, sn = g.ny;
-        PureSt zm = zc, zp = zn;
-        to_local(cs, sn, zc.vx, zc.vy, zm.vx, zm.vy);
-        to_local(cs, sn, zn.vx, zn.vy, zp.vx, zp.vy);
-        double lf[4 + NM];
-        hllc_pure(a.mix, zm, zp, lf, bad);
-        double mx = cs * lf[1] + -sn * lf[2] + 0.0 * 0.0;
-        double my = sn * lf[1] + cs * lf[2] + 0.0 * 0.0;
-        lf[1] = mx;
-        lf[2] = my;
-        const double S = g.area;
-#pragma unroll
-        for (int k = 0; k < 4 + NM; ++k) flux[k] += lf[k] * S;
-    }
-    // QState(z_c) (models.cpp:421-428) and the update
-    double E = zc.e + 0.5 * (zc.vx * zc.vx + zc.vy * zc.vy + 0.0 * 0.0);
-    QVd<NM> q;
-    q.a[0] = zc.rho;
-    q.a[1] = zc.rho * zc.vx;
-    q.a[2] = zc.rho * zc.vy;
-    q.a[3] = zc.rho * E;
-#pragma unroll
-    for (int i = 0; i < NM; ++i) q.a[4 + i] = zc.rho * zc.b[i];
-    double coef = dt / V_c;
-#pragma unroll
-    for (int k = 0; k < 4 + NM; ++k) q.a[k] -= coef * flux[k];
-    if (q.a[0] < 0.0) bad = true;
-    // PState(QState, ...) (models.cpp:190-204): the one-material closure here,
-    // mixed results go to the closure list
-    MSt<NM> z;
-    z.rho = q.a[0];
-    z.vx = q.a[1] / z.rho;
-    z.vy = q.a[2] / z.rho;
-    z.e = q.a[3] / z.rho - 0.5 * (z.vx * z.vx + z.vy * z.vy + 0.0 * 0.0);
-#pragma unroll
-    for (int i = 0; i < NM; ++i) z.b.f[i] = q.a[4 + i] / z.rho;
-    cutoff(z.b, 1.0e-12);
-    normalize(z.b);
-    int idx = frac_index(z.b);
-    if (idx >= 0) {
-        MatD m = a.mix.mat[0];
-#pragma unroll
-        for (int i = 1; i < NM; ++i)
-            if (i == idx) m = a.mix.mat[i];
-#pragma unroll
-        for (int i = 0; i < NM; ++i) z.r[i] = i == idx ? z.rho : MM_NAN;
-        z.P = m_pressure_re(m, z.rho, z.e);
-        z.T = m_temperature_rP(m, z.rho, z.P);
-        store(a.znext, ic, z);
-    } else {
-        int k = atomicAdd(&a.counts[1], 1);
-        a.list_closure[k] = ic;
-#pragma unroll
-        for (int j = 0; j < 4 + NM; ++j) a.qbuf[(size_t)k * (4 + NM) + j] = q.a[j];
-    }
-    if (bad) atomicOr(a.err, 1);
 }
 
 // --- work lists ------------------------------------------------------------
@@ -572,7 +345,8 @@ static inline unsigned blocks(const MmArgs &a) { return (unsigned)((a.mesh.n + B
 void launch_dt(const MmArgs &a, void *stream) { k_dt<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
 void launch_recover(const MmArgs &a, void *stream) { k_recover<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
 void launch_flux_pure(const MmArgs &a, void *stream) {
-    k_flux_pure<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
+    if (a.fp32_flux) launch_flux_pure_fp32(a, stream);
+    else k_flux_pure<double><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
 void launch_flux_crp(const MmArgs &a, void *stream) {
     k_crp_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);

@@ -24,6 +24,7 @@ struct MmArgs {
     StructMesh mesh;
     MixD<NMAT> mix;
     int crp;
+    int fp32_flux;  // mixed form: FP32 face arithmetic in the pure-stencil kernel
     double CFL, max_dt;
     MmField z, znext;
     double *nrm_x[NMAT], *nrm_y[NMAT], *off[NMAT];  // interface reconstruction per material
@@ -44,6 +45,7 @@ void launch_dt(const MmArgs &a, void *stream);
 void launch_recover(const MmArgs &a, void *stream);
 // the face loop: pure stencils, then the two work lists
 void launch_flux_pure(const MmArgs &a, void *stream);
+void launch_flux_pure_fp32(const MmArgs &a, void *stream);  // mmf_mixed.cu
 void launch_flux_crp(const MmArgs &a, void *stream);  // face fluxes, then the cell updates
 void launch_closure(const MmArgs &a, void *stream);
 void launch_flags(const MmArgs &a, int *flags, void *stream);

@@ -1014,6 +1014,7 @@ mmf::MmArgs make_mm_args(const zg_ctx *c) {
         a.off[i] = c->moff[i];
     }
     a.crp = c->mpar.crp_mode;
+    a.fp32_flux = c->mpar.precision == ZG_MIXED ? 1 : 0;
     a.CFL = c->mpar.CFL;
     a.max_dt = c->mpar.max_dt;
     a.z = c->mz;
@@ -1172,6 +1173,8 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
         if ((m.kind != ZG_EOS_IDEAL && m.kind != ZG_EOS_STIFFENED) || !(m.gamma > 1.0) || !(m.Cv > 0.0))
             return fail(c, ZG_ERR_ARG, "zg_mmf_configure: invalid material");
     }
+    if (p->precision != ZG_FP64 && p->precision != ZG_MIXED)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown precision");
     if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_PLIC)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown CRP mode");
     if (std::min(std::max(1, p->accuracy), 2) != 1)

@@ -107,6 +107,12 @@ class MmFluid:
         self._push()
         return self
 
+    def set_precision(self, precision: int):
+        """Precision.FP64 (the reference's arithmetic) or Precision.MIXED (FP32
+        face arithmetic of the pure-stencil faces, FP64 elsewhere)."""
+        self.p.precision = int(precision)
+        self._push()
+
     def set_CFL(self, CFL: float):  # mm_fluid.cpp:42-44
         self.p.CFL = max(0.0, min(CFL, 1.0))
         self._push()
