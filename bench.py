@@ -417,8 +417,9 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
     mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
     mesh.set_max_level(AMR_LEVELS, AMR_CAPACITY)
     kernels_name = kernels_name or AMR_KERNELS
-    kernels = Z.Kernels.FAST if kernels_name == "fast" else Z.Kernels.PARITY
-    solver = Z.SmFluid(Z.IdealGas(1.4), kernels=kernels)
+    kernels = Z.Kernels.PARITY if kernels_name == "parity" else Z.Kernels.FAST
+    precision = Z.Precision.MIXED if kernels_name == "mixed" else Z.Precision.FP64
+    solver = Z.SmFluid(Z.IdealGas(1.4), precision=precision, kernels=kernels)
     solver.add_types(mesh)
     solver.set_accuracy(2)
     solver.set_CFL(0.4)
@@ -468,6 +469,7 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
     kernels = {name: {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k]}
                for k, name in enumerate(KERNEL_KINDS) if kcount[k]}
     solver.dt()
+    final = (mesh.get_state()[0], mesh.amr_arrays()["level"])
     mesh.close()
     updates = int(sum(live))
     step_ms = ms - sum(adapt_ms)
@@ -475,9 +477,11 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
     out = {
         "workload": f"AMR blast, base {AMR_BASE}x{AMR_BASE}, max_level {AMR_LEVELS}, ZOE; rho = 1, u = v = 0, "
                     f"p = 1e-5 except p = 1e3 for r < 0.01 at (0.5, 0.5), 20x20 sub-sampled cell means",
-        "form": ("FP64 FAST kernels on the slot mesh (face geometry from centre and level, fused multiply-adds; "
-                 "within 1e-12 of the parity form per step)" if kernels_name == "fast" else
-                 "FP64 PARITY kernels on the slot mesh, bit-exact with the reference") +
+        "form": {"fast": "FP64 FAST kernels on the slot mesh (face geometry from centre and level, fused "
+                         "multiply-adds; within 1e-12 of the parity form per step)",
+                 "mixed": "MIXED kernels on the slot mesh (FP32 states, gradients and fluxes; FP64 conserved "
+                          "sums, update, pressure recovery and dt)",
+                 "parity": "FP64 PARITY kernels on the slot mesh, bit-exact with the reference"}[kernels_name] +
                 " -- SmFluid second order, predictor-corrector, HLLC, van Albada 1, CFL 0.4; set_flags criterion; "
                 "slope distributor",
         "value": updates / (ms / 1e3), "unit": METRIC, "timed_steps": AMR_TIMED_STEPS,
@@ -492,7 +496,7 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
                              "(all cell and face arrays read once, new arrays written once)",
         "algorithmic_bytes_per_cell_update": AMR_B_ALG,
         "step_achieved_GBs": AMR_B_ALG * updates / (step_ms / 1e3) / 1e9,
-        "gpu_launches": int(launches), "kernels": kernels,
+        "gpu_launches": int(launches), "kernels": kernels, "final": final,
     }
     if want_cpu:
         out["cpu_baseline"] = amr_cpu_reference()
@@ -641,10 +645,19 @@ def run_ours(args, rank, world, local_rank):
     amr = amr_variant(torch, lib, dev, stream, local_rank,
                       want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), kernels_name="fast")
     amr_par = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="parity")
+    amr_mx = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="mixed")
+    (r64, lv64), (rmx, lvmx) = amr.pop("final"), amr_mx.pop("final")
+    amr_par.pop("final")
+    same_mesh = r64.shape == rmx.shape and bool(np.array_equal(lv64, lvmx))
+    amr_mx["l1_rel_density_err_vs_fp64"] = (float(np.sum(np.abs(rmx - r64)) / np.sum(np.abs(r64)))
+                                            if same_mesh else None)
+    amr_mx["same_mesh_as_fp64"] = same_mesh
 
     vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
-                                   amr["ms_total"], amr_par["ms_total"], mm_mx["ms"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx = vals
+                                   amr["ms_total"], amr_par["ms_total"], mm_mx["ms"], amr_mx["ms_total"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx = vals
+    amr_mx["value"] = world * amr_mx["value"] * amr_mx["ms_total"] / ms_amr_mx
+    amr_mx["speedup_vs_fp64"] = ms_amr / ms_amr_mx
     amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
     amr_par["value"] = world * amr_par["value"] * amr_par["ms_total"] / ms_amr_par
     for v in variants.values():
@@ -674,7 +687,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
                             mm["launches"] + mm_mx["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
-                            amr_par["gpu_launches"]),
+                            amr_par["gpu_launches"] + amr_mx["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
@@ -711,6 +724,10 @@ def run_ours(args, rank, world, local_rank):
             "amr_parity": {k: amr_par[k] for k in ("form", "value", "unit", "ms_per_step_incl_adapt",
                                                      "step_only_value", "adapt_ms_avg", "live_cells",
                                                      "gpu_launches", "kernels")},
+            "amr_mixed": {k: amr_mx[k] for k in ("form", "value", "unit", "ms_per_step_incl_adapt", "speedup_vs_fp64",
+                                                  "l1_rel_density_err_vs_fp64", "same_mesh_as_fp64",
+                                                  "step_only_value", "adapt_ms_avg", "live_cells", "gpu_launches",
+                                                  "kernels")},
         },
         "dt_last": dt_last,
     }

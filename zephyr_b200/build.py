@@ -42,6 +42,7 @@ UNITS = {
     "amr_refine.cu": ["-fmad=false"],
     "smf_fast.cu": [],
     "smf_slot_fast.cu": [],
+    "smf_slot_mixed.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "adj.cu": [],
     # FP32 face arithmetic: approximate single-precision division and square
     # root; FP64 operations are unaffected by these flags.

@@ -1,0 +1,343 @@
+// smf_slot_mixed.cu -- the MIXED form of the step on an adaptive rectangle:
+// FP32 primitive states, limited least-squares gradients, reconstruction and
+// Riemann fluxes over the face slots (geometry from SlotFastAcc, offsets
+// formed in FP64 and rounded once); FP64 conserved variables, flux sums,
+// update, pressure recovery and the dt reduction.  Approximate FP32 division
+// and square root (the flags of the rectangle's MIXED kernels).
+#include <cuda_runtime.h>
+
+#include "smf_struct.cuh"
+#include "smf_tiled.cuh"
+#include "smf_tiled_launch.h"
+
+namespace zg {
+namespace slotmixed {
+
+using tiled::C4;
+using tiled::EosR;
+using tiled::Fields;
+using tiled::P5;
+using R = float;
+
+constexpr int BLOCK = 128;
+// Minimum resident blocks per SM (register caps; -D overrides for sweeps)
+#ifndef ZG_SLOTMX_GRAD_MINB
+#define ZG_SLOTMX_GRAD_MINB 8
+#endif
+#ifndef ZG_SLOTMX_S1_MINB
+#define ZG_SLOTMX_S1_MINB 8
+#endif
+#ifndef ZG_SLOTMX_S2_MINB
+#define ZG_SLOTMX_S2_MINB 6
+#endif
+
+static inline unsigned blocks(const SmfArgs &a) { return (unsigned)((a.smesh.n + BLOCK - 1) / BLOCK); }
+
+__device__ __forceinline__ P5<R> ldw(const R *const p[5], int ic) {
+    return P5<R>{p[0][ic], p[1][ic], p[2][ic], p[3][ic], p[4][ic]};
+}
+__device__ __forceinline__ void stw(R *const p[5], int ic, const P5<R> &z) {
+    p[0][ic] = z.r;
+    p[1][ic] = z.u;
+    p[2][ic] = z.v;
+    p[3][ic] = z.p;
+    p[4][ic] = z.e;
+}
+// wall reflection (sm_fluid.cpp:69-79) for the unit normal (nx, ny)
+__device__ __forceinline__ P5<R> wall_of(const P5<R> &z, R nx, R ny, int flag) {
+    if (flag != BC_WALL) return z;
+    P5<R> o = z;
+    R d = z.u * nx + z.v * ny;
+    o.u = z.u - R(2) * (nx * d);
+    o.v = z.v - R(2) * (ny * d);
+    return o;
+}
+// rotation into the face frame and back (rotate.cpp) for a unit normal
+__device__ __forceinline__ void rot_in(R nx, R ny, R &u, R &v) {
+    R a = u, b = v;
+    u = nx * a + ny * b;
+    v = -ny * a + nx * b;
+}
+__device__ __forceinline__ void rot_out(R nx, R ny, R &mu, R &mv) {
+    R a = mu, b = mv;
+    mu = nx * a - ny * b;
+    mv = ny * a + nx * b;
+}
+__device__ __forceinline__ P5<R> recon(const P5<R> &z, const R gx[4], const R gy[4], R dx, R dy,
+                                       const EosR<R> &eos) {
+    P5<R> o;
+    o.r = z.r + (gx[0] * dx + gy[0] * dy);
+    o.u = z.u + (gx[1] * dx + gy[1] * dy);
+    o.v = z.v + (gx[2] * dx + gy[2] * dy);
+    o.p = z.p + (gx[3] * dx + gy[3] * dy);
+    o.e = eos.energy_rP(o.r, o.p);
+    return tiled::bad(o, eos) ? z : o;
+}
+__device__ __forceinline__ void ldg(const Fields<R> &f, int ic, R gx[4], R gy[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        gx[k] = f.gx[k][ic];
+        gy[k] = f.gy[k][ic];
+    }
+}
+__device__ __forceinline__ C4<double> ldq(const Fields<R> &f, int ic) {
+    return C4<double>{f.q[0][ic], f.q[1][ic], f.q[2][ic], f.q[3][ic]};
+}
+
+// CFL time step from the FP64 conserved state (sm_fluid.cpp:104-114): the
+// last block turns the minimum into dt and resets the accumulator.
+__global__ void __launch_bounds__(BLOCK) k_dt(SmfArgs a, Fields<R> f) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;
+    if (ic < a.smesh.n) {
+        SlotFastAcc c(a, ic);
+        P5<double> z = tiled::prim_of(ldq(f, ic), a.eos);
+        double cs = a.eos.sound_speed_rP(z.r, z.p);
+        double lam = c.dinc() / (sqrt(z.u * z.u + z.v * z.v) + cs);
+        if (lam >= 0.0) best = dbits(lam);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+        best = t < best ? t : best;
+    }
+    __shared__ unsigned long long sm[BLOCK / 32];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        best = threadIdx.x < BLOCK / 32 ? sm[threadIdx.x] : 0x7FEFFFFFFFFFFFFFull;
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
+            best = t < best ? t : best;
+        }
+        if (threadIdx.x == 0) {
+            atomicMin(a.dmin_bits, best);
+            __threadfence();
+            unsigned int ticket = atomicAdd(a.dt_ticket, 1u);
+            if (ticket == gridDim.x - 1) {
+                unsigned long long bits = atomicMin(a.dmin_bits, 0x7FEFFFFFFFFFFFFFull);
+                double dmin = __longlong_as_double((long long)bits);
+                *a.dt_out = smin(a.CFL * dmin, a.max_dt);
+                *a.dmin_bits = 0x7FEFFFFFFFFFFFFFull;
+                *a.dt_ticket = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
+// One slot's least-squares terms: neighbour difference, centre offset, the
+// normal part of the offset and the weight (gradient.h:226-282), offsets in
+// FP64 rounded once to FP32.
+struct Terms {
+    R w, rx, ry, nxx, nyy, dF[4];
+};
+__device__ __forceinline__ void slot_terms(const SlotFastAcc &c, const Fields<R> &f, const FaceG &g, int s,
+                                           const P5<R> &zc, Terms &t) {
+    const R nx = (R)g.nx, ny = (R)g.ny;
+    P5<R> zn = !is_boundary(g.flag) ? ldw(f.w, g.nb) : wall_of(zc, nx, ny, g.flag);
+    double ncx, ncy;
+    neib_center(c, g, s, c.cx(), c.cy(), ncx, ncy);
+    const double rx = ncx - c.cx(), ry = ncy - c.cy();
+    const double d = rx * g.nx + ry * g.ny;
+    const double nxx = d * g.nx, nyy = d * g.ny;
+    const double an = sqrt(nxx * nxx + nyy * nyy);
+    t.w = (R)(g.area / (an * an * an));
+    t.rx = (R)rx;
+    t.ry = (R)ry;
+    t.nxx = (R)nxx;
+    t.nyy = (R)nyy;
+    t.dF[0] = zn.r - zc.r;
+    t.dF[1] = zn.u - zc.u;
+    t.dF[2] = zn.v - zc.v;
+    t.dF[3] = zn.p - zc.p;
+}
+
+// Limited least-squares gradients of the FP32 state (two passes over the
+// slots; gradient.h:226-282 and 412-474).
+template <int LIM>
+__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad(SmfArgs a, Fields<R> f) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    SlotFastAcc c(a, ic);
+    const P5<R> zc = ldw(f.w, ic);
+    R A00 = 0, A01 = 0, A10 = 0, A11 = 0, Fx[4] = {0, 0, 0, 0}, Fy[4] = {0, 0, 0, 0};
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        Terms t;
+        slot_terms(c, f, g, s, zc, t);
+        R wdx = t.w * t.nxx, wdy = t.w * t.nyy;
+        A00 += wdx * t.rx;
+        A01 += wdx * t.ry;
+        A10 += wdy * t.rx;
+        A11 += wdy * t.ry;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            Fx[k] += t.w * t.dF[k] * t.nxx;
+            Fy[k] += t.w * t.dF[k] * t.nyy;
+        }
+    }
+    if (fabsf(A11) < R(1e-8)) A11 = R(1);  // 1-D case (gradient.h:270-272)
+    const R inv = R(1) / (A11 * A00 - A01 * A10);
+    const R B00 = A11 * inv, B01 = -A01 * inv, B10 = -A10 * inv, B11 = A00 * inv;
+    R g0x[4], g0y[4], Lx[4] = {0, 0, 0, 0}, Ly[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        g0x[k] = B00 * Fx[k] + B01 * Fy[k];
+        g0y[k] = B10 * Fx[k] + B11 * Fy[k];
+    }
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        Terms t;
+        slot_terms(c, f, g, s, zc, t);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            R dF_p = t.dF[k];
+            R dF_m = R(2) * (g0x[k] * t.rx + g0y[k] * t.ry) - dF_p;
+            R dl = tiled::limit<LIM, R>(a.limiter, dF_m, dF_p) * dF_p;
+            Lx[k] += t.w * dl * t.nxx;
+            Ly[k] += t.w * dl * t.nyy;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        f.gx[k][ic] = B00 * Lx[k] + B01 * Ly[k];
+        f.gy[k][ic] = B10 * Lx[k] + B11 * Ly[k];
+    }
+}
+
+// Predictor (sm_fluid.cpp:176-253): half step with the physical flux of the
+// reconstructed face states; FP64 sums, update and pressure recovery.
+__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S1_MINB) k_stage1(SmfArgs a, Fields<R> f) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    SlotFastAcc c(a, ic);
+    const P5<R> zc = ldw(f.w, ic);
+    if (f.wait_in[ic] > 0) {
+        stw(f.h, ic, zc);
+        return;
+    }
+    const EosR<R> eos = tiled::eos_as<R>(a.eos);
+    R gx[4], gy[4];
+    ldg(f, ic, gx, gy);
+    double F[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        const R nx = (R)g.nx, ny = (R)g.ny;
+        P5<R> zm = recon(zc, gx, gy, (R)(g.fcx - c.cx()), (R)(g.fcy - c.cy()), eos);
+        rot_in(nx, ny, zm.u, zm.v);
+        C4<R> lf = tiled::phys_flux(zm);
+        rot_out(nx, ny, lf.mu, lf.mv);
+        F[0] += (double)lf.r * g.area;
+        F[1] += (double)lf.mu * g.area;
+        F[2] += (double)lf.mv * g.area;
+        F[3] += (double)lf.E * g.area;
+    }
+    const double coef = 0.5 * (*a.dt_out) / c.vol();
+    C4<double> q = ldq(f, ic);
+    q.r -= coef * F[0];
+    q.mu -= coef * F[1];
+    q.mv -= coef * F[2];
+    q.E -= coef * F[3];
+    P5<double> hz = tiled::prim_of(q, a.eos);
+    stw(f.h, ic, tiled::bad64(hz, a.eos) ? zc : tiled::down<R>(hz));
+}
+
+// Face loop and update.  MODE 0: first order (faces from the state,
+// sm_fluid.cpp:127-174); MODE 1: corrector of the predictor-corrector scheme
+// with the isolation counters (sm_fluid.cpp:255-366).
+template <int MODE>
+__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S2_MINB) k_faces(SmfArgs a, Fields<R> f) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    SlotFastAcc c(a, ic);
+    const EosR<R> eos = tiled::eos_as<R>(a.eos);
+    const R *const *src = MODE == 1 ? const_cast<const R *const *>(f.h) : f.w;
+    const P5<R> zch = ldw(src, ic);
+    const int wc = MODE == 1 ? f.wait_in[ic] : 0;
+    R gx[4], gy[4];
+    if (MODE == 1) ldg(f, ic, gx, gy);
+    double F[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        const bool bnd = is_boundary(g.flag);
+        const R nx = (R)g.nx, ny = (R)g.ny;
+        const P5<R> z_nh = bnd ? wall_of(zch, nx, ny, g.flag) : ldw(src, g.nb);
+        const bool robust = MODE == 1 && (wc > 0 || f.wait_in[g.nb] > 0);
+        P5<R> zm = zch, zp = z_nh;
+        if (MODE == 1 && !robust) {
+            double ncx, ncy;
+            neib_center(c, g, s, c.cx(), c.cy(), ncx, ncy);
+            zm = recon(zch, gx, gy, (R)(g.fcx - c.cx()), (R)(g.fcy - c.cy()), eos);
+            if (!bnd) {
+                R hx[4], hy[4];
+                ldg(f, g.nb, hx, hy);
+                zp = recon(z_nh, hx, hy, (R)(g.fcx - ncx), (R)(g.fcy - ncy), eos);
+            } else {
+                zp = wall_of(zm, nx, ny, g.flag);
+            }
+        }
+        rot_in(nx, ny, zm.u, zm.v);
+        rot_in(nx, ny, zp.u, zp.v);
+        C4<R> lf = (robust || a.flux == FLUX_HLL) ? tiled::hll(zm, zp, eos) : tiled::hllc(zm, zp, eos);
+        rot_out(nx, ny, lf.mu, lf.mv);
+        F[0] += (double)lf.r * g.area;
+        F[1] += (double)lf.mu * g.area;
+        F[2] += (double)lf.mv * g.area;
+        F[3] += (double)lf.E * g.area;
+    }
+    const double coef = (*a.dt_out) / c.vol();
+    const C4<double> q0 = ldq(f, ic);
+    C4<double> q = q0;
+    q.r -= coef * F[0];
+    q.mu -= coef * F[1];
+    q.mv -= coef * F[2];
+    q.E -= coef * F[3];
+    P5<double> zn = tiled::prim_of(q, a.eos);
+    if (MODE == 1) {
+        int wn = wc;
+        if (tiled::bad64(zn, a.eos)) {  // isolation: keep the old state
+            q = q0;
+            zn = tiled::prim_of(q0, a.eos);
+            wn = 3;
+        } else if (wn > 0) {
+            --wn;
+        }
+        f.wait_out[ic] = wn;
+    }
+    f.qn[0][ic] = q.r;
+    f.qn[1][ic] = q.mu;
+    f.qn[2][ic] = q.mv;
+    f.qn[3][ic] = q.E;
+    stw(f.wn, ic, tiled::down<R>(zn));
+}
+
+void launch_dt(const SmfArgs &a, const Fields<R> &f, void *stream) {
+    k_dt<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+}
+void launch_grad(const SmfArgs &a, const Fields<R> &f, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (a.limiter) {  // the common limiters compiled in, the others at run time
+        case LIM_VANALBADA1: k_grad<LIM_VANALBADA1><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        case LIM_MC: k_grad<LIM_MC><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        case LIM_MINMOD: k_grad<LIM_MINMOD><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        default: k_grad<-1><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+    }
+}
+void launch_stage1(const SmfArgs &a, const Fields<R> &f, void *stream) {
+    k_stage1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+}
+void launch_faces(const SmfArgs &a, const Fields<R> &f, int mode, void *stream) {
+    if (mode == 0) k_faces<0><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+    else k_faces<1><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+}
+
+}  // namespace slotmixed
+}  // namespace zg

@@ -23,4 +23,14 @@ void launch_faces(const SmfArgs &a, const tiled::Fields<float> &f, int mode, voi
 void launch_to_mixed(int n, PrimPtr z, const tiled::Fields<float> &f, void *stream);
 void launch_to_prim(int n, const tiled::Fields<float> &f, EosD eos, PrimPtr z, void *stream);
 }  // namespace mixed
+
+// MIXED kernels on an adaptive rectangle (smf_slot_mixed.cu): dt from the FP64
+// conserved state, FP32 gradients, predictor, and the face loop (mode 0 first
+// order, 1 corrector).
+namespace slotmixed {
+void launch_dt(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
+void launch_grad(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
+void launch_stage1(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
+void launch_faces(const SmfArgs &a, const tiled::Fields<float> &f, int mode, void *stream);
+}  // namespace slotmixed
 }  // namespace zg

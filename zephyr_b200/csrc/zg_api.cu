@@ -473,8 +473,37 @@ int enqueue_slot_fast_step(zg_ctx *c) {
     return ZG_OK;
 }
 
+// The MIXED step on an adaptive rectangle (FP64 conserved state with an FP32
+// primitive mirror, as on a rectangle).
+int enqueue_slot_mixed_step(zg_ctx *c) {
+    if (c->par.accuracy == 2 && c->par.scheme != ZG_SCHEME_PREDICTOR_CORRECTOR)
+        return fail(c, ZG_ERR_STATE,
+                    "the MIXED form on an adaptive mesh runs first order or the predictor-corrector scheme");
+    int rc = convert_state(c, ZG_MIXED);
+    if (rc != ZG_OK) return rc;
+    SmfArgs a = make_args(c);
+    tiled::Fields<float> f = mixed_fields(c);
+    void *st = (void *)c->stream;
+    timed(c, ZG_K_DT, [&] { slotmixed::launch_dt(a, f, st); });
+    if (c->par.accuracy == 1) {
+        timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_faces(a, f, 0, st); });
+    } else {
+        timed(c, ZG_K_GRAD, [&] { slotmixed::launch_grad(a, f, st); });
+        timed(c, ZG_K_STAGE1, [&] { slotmixed::launch_stage1(a, f, st); });
+        timed(c, ZG_K_STAGE2, [&] { slotmixed::launch_faces(a, f, 1, st); });
+        c->wait_cur = 1 - c->wait_cur;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
+    c->mcur = 1 - c->mcur;
+    c->cfl_valid = false;
+    c->stepped = true;
+    return ZG_OK;
+}
+
 int enqueue_step(zg_ctx *c) {
     if (c->amr && c->par.precision == ZG_FP64 && c->par.kernels == ZG_KERNELS_FAST) return enqueue_slot_fast_step(c);
+    if (c->amr && c->par.precision == ZG_MIXED) return enqueue_slot_mixed_step(c);
     if (c->slots && (c->par.precision == ZG_MIXED || c->par.kernels == ZG_KERNELS_FAST))
         return fail(c, ZG_ERR_STATE,
                     "the MIXED kernels need a rectangle mesh; the FAST kernels a rectangle or an adaptive rectangle");
@@ -1500,6 +1529,8 @@ int zg_amr_enable(zg_ctx *c, int max_level, int capacity) {
     cudaFree(c->d_tgeo);
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
+    c->ax64 = c->ay64 = tiled::AxisGeo<double>{};
+    c->ax32 = c->ay32 = tiled::AxisGeo<float>{};
     c->cap = capacity;
     c->amr = true;
     c->slots = true;
@@ -1531,6 +1562,9 @@ int zg_amr_refine(zg_ctx *c) {
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_amr_refine: solver not configured");
     if (c->amr_max_level < 1) return ZG_OK;  // EuMesh::refine returns on a non-adaptive mesh
     DeviceGuard g(c->device);
+    // the refine moves and splits the FP64 primitive state
+    int rc0 = convert_state(c, ZG_FP64);
+    if (rc0 != ZG_OK) return rc0;
     const int n0 = c->n;
     amr::RefineResult res = amr::refine(amr_view(c), c->n, c->cap, c->amr_max_level, c->d_amr_scratch,
                                         c->amr_scratch_size, const_cast<double *>(c->smesh.inc), c->stream);
