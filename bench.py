@@ -57,6 +57,11 @@ def parse():
     ap.add_argument("--size", type=int, default=0, help="override the mesh size (n x n) for small profiling runs")
     ap.add_argument("--scheme", choices=["pc", "heun"], default="pc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # profiling aids: one section alone on a smaller case (not the bench line)
+    ap.add_argument("--only", choices=["amr", "mm", "adjoint"], default=None,
+                    help="run one section alone and print its JSON (for ncu captures)")
+    ap.add_argument("--amr-base", type=int, default=0, help="AMR base cells per side (default 512)")
+    ap.add_argument("--amr-kernels", choices=["fast", "mixed", "parity"], default="fast")
     return ap.parse_args()
 
 
@@ -580,9 +585,27 @@ def run_ours(args, rank, world, local_rank):
         if world > 1:
             torch.distributed.barrier()
 
+    K, W = args.steps, max(args.warmup, 3)
+    if args.only:
+        global AMR_BASE, AMR_CAPACITY
+        if args.amr_base:
+            AMR_BASE = args.amr_base
+            AMR_CAPACITY = max(1 << 20, 32 * AMR_BASE * AMR_BASE)
+        if args.only == "amr":
+            out = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name=args.amr_kernels)
+            out.pop("final")
+        elif args.only == "mm":
+            out = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
+                             precision=Z.Precision.MIXED if args.amr_kernels == "mixed" else Z.Precision.FP64)
+            out.pop("final")
+        else:
+            out = adjoint_variant(torch, dev, stream, local_rank)
+        if rank == 0:
+            print(json.dumps({"only": args.only, **out}, default=str), flush=True)
+        return
+
     w, cfg = workload(args.workload, args.size)
     cells = w.gen.nx() * w.gen.ny()
-    K, W = args.steps, max(args.warmup, 3)
 
     # ---- headline: the FP64 step (FAST kernels), inputs resident in HBM ----
     mesh, solver = _solver(Z, w, cfg, args, local_rank, stream, Z.Precision.FP64, Z.Kernels.FAST)
