@@ -540,15 +540,23 @@ def adjoint_variant(torch, dev, stream, local_rank):
     n0 = adj.launch_count()
     ms_f, J = timed(lambda: adj.forward(prm, r, u, v, p))
     ms_g, (J2, dg) = timed(lambda: adj.gradient(prm, r, u, v, p, grad))
+    # the mixed form: FP32 primitive states, slopes, HLLC and its reverse
+    pmx = Adjoint.params(steps=100, checkpoint_every=10, dt=dt, precision=1)
+    gmx = torch.empty_like(r)
+    adj.forward(pmx, r, u, v, p)
+    adj.gradient(pmx, r, u, v, p, gmx)
+    ms_fm, Jm = timed(lambda: adj.forward(pmx, r, u, v, p))
+    ms_gm, (_, dgm) = timed(lambda: adj.gradient(pmx, r, u, v, p, gmx))
     launches = adj.launch_count() - n0
     rng = np.random.default_rng(5)
     eps = 1e-6
-    errs = []
+    errs, errs_m = [], []
     for _ in range(16):
         d = torch.tensor(rng.standard_normal(ADJ_SIZE * ADJ_SIZE), dtype=torch.float64, device=dev)
         fd = (adj.forward(prm, r + eps * d, u, v, p) - adj.forward(prm, r - eps * d, u, v, p)) / (2 * eps)
         ad = float(torch.dot(grad, d))
         errs.append(abs(fd - ad) / abs(ad))
+        errs_m.append(abs(fd - float(torch.dot(gmx, d))) / abs(ad))
     fd_g = (adj.forward(Adjoint.params(steps=100, checkpoint_every=10, dt=dt, gamma=1.4 + eps), r, u, v, p) -
             adj.forward(Adjoint.params(steps=100, checkpoint_every=10, dt=dt, gamma=1.4 - eps), r, u, v, p)) / (2 * eps)
     adj.close()
@@ -558,6 +566,13 @@ def adjoint_variant(torch, dev, stream, local_rank):
             "checkpoint_every": 10, "J": J, "dJ_dgamma": dg,
             "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)), "fd_directions": 16,
             "fd_rel_err_gamma": abs(fd_g - dg) / abs(dg), "gpu_launches": int(launches),
+            "mixed": {"form": "FP32 primitive states, slopes, face states, HLLC and its reverse; FP64 conserved "
+                              "and adjoint states, flux and cotangent sums, primitive map and gamma",
+                      "forward_ms": ms_fm, "gradient_ms": ms_gm, "adjoint_over_forward": ms_gm / ms_fm,
+                      "gradient_speedup_vs_fp64": ms_g / ms_gm, "J_rel_err_vs_fp64": abs(Jm - J) / abs(J),
+                      "grad_l2_rel_err_vs_fp64": float(torch.linalg.norm(gmx - grad) / torch.linalg.norm(grad)),
+                      "dJ_dgamma_rel_err_vs_fp64": abs(dgm - dg) / abs(dg),
+                      "fd_rel_err_max": max(errs_m), "fd_rel_err_median": float(np.median(errs_m))},
             "note": "gradient time includes the checkpointed forward, the segment recomputation and the reverse "
                     "sweep; FD: central differences of the FP64 forward, eps 1e-6, Gaussian directions seed 5"}
 

@@ -143,3 +143,34 @@ def test_adjoint_through_torch_autograd(gpu_lib):
     assert float(J) == J2
     assert torch.equal(rho0.grad, 2.0 * g) and float(gamma.grad) == 2.0 * dg
     adj.close()
+
+
+def test_mixed_adjoint_tracks_the_fp64_adjoint(gpu_lib):
+    """The mixed adjoint (FP32 primitive states, slopes, HLLC and its reverse;
+    FP64 conserved and adjoint states and sums): J to 1e-8, the gradient to
+    1e-4 in the L2 norm against the FP64 adjoint, and directional derivatives
+    within 1e-3 of central differences of the FP64 forward."""
+    import torch
+    from zephyr_b200.adjoint import Adjoint
+    n, steps = 64, 20
+    st = smooth_state(n, n, seed=3)
+    adj = Adjoint(n, n)
+    r, u, v, p = cuda(*st)
+    dt = adj.cfl_dt(1.4, 0.4, r, u, v, p)
+    p64 = Adjoint.params(steps=steps, checkpoint_every=5, dt=dt)
+    pmx = Adjoint.params(steps=steps, checkpoint_every=5, dt=dt, precision=1)
+    g64, gmx = torch.empty_like(r), torch.empty_like(r)
+    J64, dg64 = adj.gradient(p64, r, u, v, p, g64)
+    Jmx, dgmx = adj.gradient(pmx, r, u, v, p, gmx)
+    assert Jmx == adj.forward(pmx, r, u, v, p)
+    assert abs(Jmx - J64) <= 1e-8 * abs(J64)
+    assert float(torch.linalg.norm(gmx - g64) / torch.linalg.norm(g64)) <= 1e-4
+    assert abs(dgmx - dg64) <= 1e-4 * abs(dg64)
+    rng = np.random.default_rng(5)
+    eps = 1e-6
+    for _ in range(3):
+        d = torch.tensor(rng.standard_normal(n * n), dtype=torch.float64, device="cuda")
+        fd = (adj.forward(p64, r + eps * d, u, v, p) - adj.forward(p64, r - eps * d, u, v, p)) / (2 * eps)
+        ad = float(torch.dot(gmx, d))
+        assert abs(fd - ad) <= 1e-3 * abs(ad), (fd, ad)
+    adj.close()

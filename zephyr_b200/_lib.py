@@ -85,7 +85,7 @@ class MmfParams(C.Structure):
 class AdjParams(C.Structure):
     """zg_adj_params"""
     _fields_ = [("gamma", C.c_double), ("dt", C.c_double), ("steps", C.c_int), ("checkpoint_every", C.c_int),
-                ("limiter_eps", C.c_double), ("probe", C.c_double * 4)]
+                ("limiter_eps", C.c_double), ("probe", C.c_double * 4), ("precision", C.c_int)]
 
 
 SIGNATURES = {

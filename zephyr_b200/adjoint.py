@@ -25,10 +25,13 @@ class Adjoint:
             self._lib.zg_adj_set_stream(self.h, C.c_void_p(stream))
 
     @staticmethod
-    def params(steps=100, checkpoint_every=10, gamma=1.4, dt=0.0, limiter_eps=1e-8, probe=(0.6, 0.7, 0.6, 0.7)):
+    def params(steps=100, checkpoint_every=10, gamma=1.4, dt=0.0, limiter_eps=1e-8, probe=(0.6, 0.7, 0.6, 0.7),
+               precision=0):
+        """zg_adj_params; precision 0 = FP64, 1 = MIXED (zg_precision)."""
         p = AdjParams()
         load().zg_adj_default_params(C.byref(p))
         p.steps, p.checkpoint_every, p.gamma, p.dt, p.limiter_eps = steps, checkpoint_every, gamma, dt, limiter_eps
+        p.precision = int(precision)
         for k in range(4):
             p.probe[k] = probe[k]
         return p

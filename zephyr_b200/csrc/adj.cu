@@ -58,12 +58,19 @@ struct Grid {
     double hx, hy, vol;
     double x0, y0;
 };
-struct F4 {  // four field arrays
-    double *f[4];
+// four field arrays of element type S (FP64 state and adjoint fields are
+// double; the primitive states, slopes and face cotangents are S = double in
+// the FP64 form and S = float in the mixed form)
+template <class S>
+struct F4T {
+    S *f[4];
 };
-struct CF4 {
-    const double *f[4];
+template <class S>
+struct CF4T {
+    const S *f[4];
 };
+using F4 = F4T<double>;
+using CF4 = CF4T<double>;
 
 // A cell with its (i, j): the periodic neighbours follow without integer
 // division (one division per thread, in cell_of).
@@ -108,8 +115,11 @@ __global__ void k_init(Grid g, CF4 W0, double gamma, F4 U) {
     U.f[3][ic] = p / (gamma - 1.0) + 0.5 * (r * (u * u + v * v));
 }
 
-// primitive state and limited slopes of every cell
-__global__ void __launch_bounds__(BLOCK, ZG_ADJ_PG_MINB) k_prim_grad(Grid g, CF4 U, double gamma, double eps, F4 W, F4 gx, F4 gy) {
+// primitive state and limited slopes of every cell: the primitive map in
+// FP64, rounded to S; the slopes from the rounded values in S
+template <class S>
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_PG_MINB) k_prim_grad(Grid g, CF4 U, double gamma, double eps,
+                                                                     F4T<S> W, F4T<S> gx, F4T<S> gy) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= g.n) return;
     double wc[4], wl[4], wr[4], wb[4], wt[4];
@@ -119,20 +129,21 @@ __global__ void __launch_bounds__(BLOCK, ZG_ADJ_PG_MINB) k_prim_grad(Grid g, CF4
     prim_at(U, xp(g, c).ic, gamma, wr);
     prim_at(U, ym(g, c).ic, gamma, wb);
     prim_at(U, yp(g, c).ic, gamma, wt);
-    const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy;
+    const S i2x = S(0.5 / g.hx), i2y = S(0.5 / g.hy), e = S(eps);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        W.f[k][ic] = wc[k];
-        gx.f[k][ic] = slope(wl[k], wc[k], wr[k], i2x, eps);
-        gy.f[k][ic] = slope(wb[k], wc[k], wt[k], i2y, eps);
+        W.f[k][ic] = S(wc[k]);
+        gx.f[k][ic] = slope<S>(S(wl[k]), S(wc[k]), S(wr[k]), i2x, e);
+        gy.f[k][ic] = slope<S>(S(wb[k]), S(wc[k]), S(wt[k]), i2y, e);
     }
 }
 
 // Face states of the face between `lo` and `hi` along an axis, in the face
 // frame (x faces: (rho, u, v, p); y faces: (rho, v, -u, p)).
-__device__ __forceinline__ void face_states(const CF4 &W, const CF4 &G, int lo, int hi, double half_h, bool yface,
-                                            double L[4], double R[4]) {
-    double a[4], b[4];
+template <class S>
+__device__ __forceinline__ void face_states(const CF4T<S> &W, const CF4T<S> &G, int lo, int hi, S half_h, bool yface,
+                                            S L[4], S R[4]) {
+    S a[4], b[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         a[k] = W.f[k][lo] + G.f[k][lo] * half_h;
@@ -150,7 +161,8 @@ __device__ __forceinline__ void face_states(const CF4 &W, const CF4 &G, int lo, 
     }
 }
 // face-frame flux back to the global frame
-__device__ __forceinline__ void flux_global(const double Fl[4], bool yface, double F[4]) {
+template <class S>
+__device__ __forceinline__ void flux_global(const S Fl[4], bool yface, S F[4]) {
     if (!yface) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) F[k] = Fl[k];
@@ -163,8 +175,10 @@ __device__ __forceinline__ void flux_global(const double Fl[4], bool yface, doub
 }
 
 // out = alpha * base + beta * (X + dt L(X)), L from the face fluxes of W, G
-__global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 X,
-                                                       CF4 base, double alpha, double beta, double dt, F4 out) {
+template <class S>
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, CF4T<S> W, CF4T<S> gx, CF4T<S> gy,
+                                                                       double gamma, CF4 X, CF4 base, double alpha,
+                                                                       double beta, double dt, F4 out) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= g.n) return;
     const Cell cc = cell_of(g, ic);
@@ -174,14 +188,14 @@ __global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, C
     for (int s = 0; s < 4; ++s) {
         const bool yface = s >= 2, high = (s & 1) == 1;
         const int lo = high ? ic : nb[s], hi = high ? nb[s] : ic;
-        const double half_h = 0.5 * (yface ? g.hy : g.hx), S = yface ? g.hx : g.hy;
-        double L[4], R[4], Fl[4], F[4];
-        face_states(W, yface ? gy : gx, lo, hi, half_h, yface, L, R);
-        hllc<double>(L, R, gamma, Fl);
-        flux_global(Fl, yface, F);
-        const double sgn = high ? S : -S;  // outward flux of this cell
+        const double half_h = 0.5 * (yface ? g.hy : g.hx), A = yface ? g.hx : g.hy;
+        S L[4], R[4], Fl[4], F[4];
+        face_states<S>(W, yface ? gy : gx, lo, hi, S(half_h), yface, L, R);
+        hllc<S>(L, R, S(gamma), Fl);
+        flux_global<S>(Fl, yface, F);
+        const double sgn = high ? A : -A;  // outward flux of this cell
 #pragma unroll
-        for (int k = 0; k < 4; ++k) sum[k] += sgn * F[k];
+        for (int k = 0; k < 4; ++k) sum[k] += sgn * (double)F[k];
     }
     const double c = dt / g.vol;
 #pragma unroll
@@ -247,8 +261,10 @@ __global__ void __launch_bounds__(BLOCK) k_probe(Grid g, CF4 U, double gamma, do
 // cotangents of the face's low-side and high-side states, in the global
 // primitive frame, go to fb[face][0..3] and fb[face][4..7]; the faces' gamma
 // parts to gacc.
-__global__ void __launch_bounds__(BLOCK, ZG_ADJ_VF_MINB) k_vjp_faces(Grid g, CF4 W, CF4 gx, CF4 gy, double gamma, CF4 mu,
-                                                     double coef, double *fbx, double *fby, double *gacc) {
+template <class S>
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_VF_MINB) k_vjp_faces(Grid g, CF4T<S> W, CF4T<S> gx, CF4T<S> gy,
+                                                                     double gamma, CF4 mu, double coef, S *fbx,
+                                                                     S *fby, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     double gpart = 0.0;
     if (ic < g.n) {
@@ -258,25 +274,31 @@ __global__ void __launch_bounds__(BLOCK, ZG_ADJ_VF_MINB) k_vjp_faces(Grid g, CF4
             const bool yface = axis == 1;
             const Cell c = cell_of(g, ic);
             const int lo = ic, hi = yface ? yp(g, c).ic : xp(g, c).ic;
-            const double half_h = 0.5 * (yface ? g.hy : g.hx), S = yface ? g.hx : g.hy;
-            // cotangent of the global face flux: L_lo gets -S/V F, L_hi +S/V F
+            const double half_h = 0.5 * (yface ? g.hy : g.hx), A = yface ? g.hx : g.hy;
+            // cotangent of the global face flux: L_lo gets -A/V F, L_hi +A/V F
             double mF[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) mF[k] = cv * S * (mu.f[k][hi] - mu.f[k][lo]);
-            double ml[4];  // in the face frame (transpose of flux_global)
+            for (int k = 0; k < 4; ++k) mF[k] = cv * A * (mu.f[k][hi] - mu.f[k][lo]);
+            S ml[4];  // in the face frame (transpose of flux_global)
             if (!yface) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) ml[k] = mF[k];
+                for (int k = 0; k < 4; ++k) ml[k] = S(mF[k]);
             } else {
-                ml[0] = mF[0];
-                ml[1] = mF[2];
-                ml[2] = -mF[1];
-                ml[3] = mF[3];
+                ml[0] = S(mF[0]);
+                ml[1] = S(mF[2]);
+                ml[2] = S(-mF[1]);
+                ml[3] = S(mF[3]);
             }
-            double L[4], R[4], Lb[4], Rb[4];
-            face_states(W, yface ? gy : gx, lo, hi, half_h, yface, L, R);
-            hllc_vjp(L, R, gamma, ml, Lb, Rb, gpart);
-            double *fb = yface ? fby : fbx;
+            S L[4], R[4], Lb[4], Rb[4];
+            face_states<S>(W, yface ? gy : gx, lo, hi, S(half_h), yface, L, R);
+            if constexpr (sizeof(S) == sizeof(double)) {
+                hllc_vjp<double>(L, R, gamma, ml, Lb, Rb, gpart);
+            } else {
+                S gb = S(0);
+                hllc_vjp<S>(L, R, S(gamma), ml, Lb, Rb, gb);
+                gpart += (double)gb;
+            }
+            S *fb = yface ? fby : fbx;
             const size_t n = (size_t)g.n;
             // face frame -> global primitive (transpose of face_states' permutation)
             if (!yface) {
@@ -325,18 +347,20 @@ __device__ __forceinline__ int wrapc(int x, int n) {
 }
 
 // d0 * gb and d2 * gb of a cell's slope along one axis (its contributions to
-// its low and high neighbour), and d1 * gb (its own), for field k
-__device__ __forceinline__ void slope_terms(double wm, double w0, double wp, double i2h, double eps, double gb,
-                                            double &to_lo, double &own, double &to_hi) {
-    double d[3];
-    slope_partials(wm, w0, wp, i2h, eps, d);
-    to_lo = d[0] * gb;
-    own = d[1] * gb;
-    to_hi = d[2] * gb;
+// its low and high neighbour), and d1 * gb (its own), for field k, in S
+template <class S>
+__device__ __forceinline__ void slope_terms(S wm, S w0, S wp, S i2h, S eps, S gb, double &to_lo, double &own,
+                                            double &to_hi) {
+    S d[3];
+    slope_partials<S>(wm, w0, wp, i2h, eps, d);
+    to_lo = (double)(d[0] * gb);
+    own = (double)(d[1] * gb);
+    to_hi = (double)(d[2] * gb);
 }
 
+template <class S>
 __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
-    Grid g, CF4 X, CF4 W, double gamma, double eps, const double *fbx, const double *fby, CF4 base, double base_coef,
+    Grid g, CF4 X, CF4T<S> W, double gamma, double eps, const S *fbx, const S *fby, CF4 base, double base_coef,
     CF4 add, F4 out, double *gacc) {
     // contributions of tile positions to their neighbours: x (i) rows -1..VI,
     // y (j) columns -1..VJ
@@ -346,7 +370,7 @@ __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
     const int tj = threadIdx.x, ti = threadIdx.y, tid = ti * VJ + tj;
     const int i0 = blockIdx.y * VI, j0 = blockIdx.x * VJ;
     const size_t n = (size_t)g.n;
-    const double i2x = 0.5 / g.hx, i2y = 0.5 / g.hy, hx2 = 0.5 * g.hx, hy2 = 0.5 * g.hy;
+    const S i2x = S(0.5 / g.hx), i2y = S(0.5 / g.hy), hx2 = S(0.5 * g.hx), hy2 = S(0.5 * g.hy), se = S(eps);
     const Cell c{wrapc(i0 + ti, g.nx) * g.ny + wrapc(j0 + tj, g.ny), wrapc(i0 + ti, g.nx), wrapc(j0 + tj, g.ny)};
     const Cell cl = xm(g, c), cr = xp(g, c), cb = ym(g, c), ct = yp(g, c);
     const bool live = i0 + ti < g.nx && j0 + tj < g.ny;
@@ -377,33 +401,33 @@ __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
     double wt[4];
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
-        const double *fl = fbx + k * n, *fh = fbx + (4 + k) * n, *gl = fby + k * n, *gh = fby + (4 + k) * n;
-        const double *w = W.f[k];
+        const S *fl = fbx + k * n, *fh = fbx + (4 + k) * n, *gl = fby + k * n, *gh = fby + (4 + k) * n;
+        const S *w = W.f[k];
         // own position: slope cotangents and partials on both axes
-        const double xl_c = fl[c.ic], xh_l = fh[cl.ic], yl_c = gl[c.ic], yh_b = gh[cb.ic];
-        const double w_c = w[c.ic];
+        const S xl_c = fl[c.ic], xh_l = fh[cl.ic], yl_c = gl[c.ic], yh_b = gh[cb.ic];
+        const S w_c = w[c.ic];
         double ox, oy, lo, hi;
-        slope_terms(w[cl.ic], w_c, w[cr.ic], i2x, eps, hx2 * (xl_c - xh_l), lo, ox, hi);
+        slope_terms<S>(w[cl.ic], w_c, w[cr.ic], i2x, se, hx2 * (xl_c - xh_l), lo, ox, hi);
         sx_lo[ti + 1][tj] = lo;
         sx_hi[ti + 1][tj] = hi;
-        slope_terms(w[cb.ic], w_c, w[ct.ic], i2y, eps, hy2 * (yl_c - yh_b), lo, oy, hi);
+        slope_terms<S>(w[cb.ic], w_c, w[ct.ic], i2y, se, hy2 * (yl_c - yh_b), lo, oy, hi);
         sy_lo[ti][tj + 1] = lo;
         sy_hi[ti][tj + 1] = hi;
         if (h_axis == 0) {
-            const double gb = hx2 * (fl[hc.ic] - fh[hm.ic]);
+            const S gb = hx2 * (fl[hc.ic] - fh[hm.ic]);
             double o;
-            slope_terms(w[hm.ic], w[hc.ic], w[hp.ic], i2x, eps, gb, lo, o, hi);
+            slope_terms<S>(w[hm.ic], w[hc.ic], w[hp.ic], i2x, se, gb, lo, o, hi);
             if (h_side == 0) sx_hi[0][h_pos] = hi;
             else sx_lo[VI + 1][h_pos] = lo;
         } else if (h_axis == 1) {
-            const double gb = hy2 * (gl[hc.ic] - gh[hm.ic]);
+            const S gb = hy2 * (gl[hc.ic] - gh[hm.ic]);
             double o;
-            slope_terms(w[hm.ic], w[hc.ic], w[hp.ic], i2y, eps, gb, lo, o, hi);
+            slope_terms<S>(w[hm.ic], w[hc.ic], w[hp.ic], i2y, se, gb, lo, o, hi);
             if (h_side == 0) sy_hi[h_pos][0] = hi;
             else sy_lo[h_pos][VJ + 1] = lo;
         }
         __syncthreads();
-        double acc = xl_c + xh_l + yl_c + yh_b;
+        double acc = (double)xl_c + (double)xh_l + (double)yl_c + (double)yh_b;
         acc += sx_hi[ti][tj];      // the left cell's slope (this cell is its high neighbour)
         acc += ox;                 // own slope
         acc += sx_lo[ti + 2][tj];  // the right cell's slope
@@ -562,18 +586,40 @@ struct WG {  // primitive states and slopes of one stage
 // one Heun step: X -> out (stage value into `star`); the stages' primitive
 // states and slopes go to sa and sb
 // (need_out = false: the step's result is not wanted, only its stages)
-void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
-               const WG &sb, bool need_out = true) {
+// the same arrays viewed as element type S (the mixed form keeps its FP32
+// primitive states, slopes and face cotangents in the first half of the
+// FP64-sized buffers)
+template <class S>
+F4T<S> as(const F4 &x) {
+    return F4T<S>{{reinterpret_cast<S *>(x.f[0]), reinterpret_cast<S *>(x.f[1]), reinterpret_cast<S *>(x.f[2]),
+                   reinterpret_cast<S *>(x.f[3])}};
+}
+template <class S>
+CF4T<S> cas(const F4 &x) {
+    F4T<S> y = as<S>(x);
+    return CF4T<S>{{y.f[0], y.f[1], y.f[2], y.f[3]}};
+}
+
+template <class S>
+void heun_step_t(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
+                 const WG &sb, bool need_out) {
     unsigned nb = nblocks(a);
-    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, sa.W, sa.gx, sa.gy);
-    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(sa.W), cf(sa.gx), cf(sa.gy), p.gamma, cf(X), kNull, 0.0,
-                                               1.0, p.dt, star);
-    k_prim_grad<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, sb.W, sb.gx, sb.gy);
+    k_prim_grad<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, as<S>(sa.W), as<S>(sa.gx),
+                                                as<S>(sa.gy));
+    k_flux_update<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cas<S>(sa.W), cas<S>(sa.gx), cas<S>(sa.gy), p.gamma, cf(X),
+                                                  kNull, 0.0, 1.0, p.dt, star);
+    k_prim_grad<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, as<S>(sb.W), as<S>(sb.gx),
+                                                as<S>(sb.gy));
     a->launches += 3;
     if (!need_out) return;
-    k_flux_update<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(sb.W), cf(sb.gx), cf(sb.gy), p.gamma, cf(star), cf(X), 0.5,
-                                               0.5, p.dt, out);
+    k_flux_update<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cas<S>(sb.W), cas<S>(sb.gx), cas<S>(sb.gy), p.gamma,
+                                                  cf(star), cf(X), 0.5, 0.5, p.dt, out);
     ++a->launches;
+}
+void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
+               const WG &sb, bool need_out = true) {
+    if (p.precision == ZG_MIXED) heun_step_t<float>(a, p, X, star, out, sa, sb, need_out);
+    else heun_step_t<double>(a, p, X, star, out, sa, sb, need_out);
 }
 WG scratch(const zg_adj *a) { return WG{a->W, a->gx, a->gy}; }
 WG seg_stage(const zg_adj *a, int t, int stage) {
@@ -582,15 +628,22 @@ WG seg_stage(const zg_adj *a, int t, int stage) {
 
 // out = base_coef * base + add + L'(X)^T (coef * mu), with X's primitive
 // states and slopes in wg
+template <class S>
+void vjp_t(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F4 &mu, double coef, const F4 &base,
+           double base_coef, const CF4 &add, const F4 &out, double *gacc) {
+    unsigned nb = nblocks(a);
+    S *fbx = reinterpret_cast<S *>(a->fbx), *fby = reinterpret_cast<S *>(a->fby);
+    k_vjp_faces<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cas<S>(wg.W), cas<S>(wg.gx), cas<S>(wg.gy), p.gamma, cf(mu),
+                                                coef, fbx, fby, gacc);
+    k_vjp_cells_tiled<S><<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(X), cas<S>(wg.W), p.gamma,
+                                                                     p.limiter_eps, fbx, fby, cf(base), base_coef,
+                                                                     add, out, gacc);
+    a->launches += 2;
+}
 void vjp(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F4 &mu, double coef, const F4 &base,
          double base_coef, const CF4 &add, const F4 &out, double *gacc) {
-    unsigned nb = nblocks(a);
-    k_vjp_faces<<<nb, BLOCK, 0, a->stream>>>(a->g, cf(wg.W), cf(wg.gx), cf(wg.gy), p.gamma, cf(mu), coef, a->fbx,
-                                             a->fby, gacc);
-    k_vjp_cells_tiled<<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(X), cf(wg.W), p.gamma, p.limiter_eps,
-                                                                  a->fbx, a->fby, cf(base), base_coef, add, out,
-                                                                  gacc);
-    a->launches += 2;
+    if (p.precision == ZG_MIXED) vjp_t<float>(a, p, X, wg, mu, coef, base, base_coef, add, out, gacc);
+    else vjp_t<double>(a, p, X, wg, mu, coef, base, base_coef, add, out, gacc);
 }
 
 int check_params(zg_adj *a, const zg_adj_params *p) {
@@ -599,6 +652,7 @@ int check_params(zg_adj *a, const zg_adj_params *p) {
     if (!(p->dt > 0.0)) return afail(a, ZG_ERR_ARG, "dt must be positive (see zg_adj_cfl_dt)");
     if (p->steps < 1 || p->checkpoint_every < 1) return afail(a, ZG_ERR_ARG, "steps and checkpoint_every >= 1");
     if (!(p->limiter_eps > 0.0)) return afail(a, ZG_ERR_ARG, "limiter_eps must be positive");
+    if (p->precision != ZG_FP64 && p->precision != ZG_MIXED) return afail(a, ZG_ERR_ARG, "unknown precision");
     return ZG_OK;
 }
 

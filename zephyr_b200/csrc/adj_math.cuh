@@ -1,5 +1,7 @@
-// adj_math.cuh -- the differentiable forward of the adjoint mode, written
-// once for plain doubles and for dual numbers.
+// adj_math.cuh -- the differentiable forward of the adjoint mode and its
+// hand-written reverse, templated on the face arithmetic: double (the FP64
+// form) or float (the mixed form).  Constants are written T(x), so that the
+// double instantiation performs exactly the FP64 operations.
 //
 // The step differentiated is Heun's method on the finite-volume operator
 //   L(U)_c = -(1/V) sum_faces S F(face states),
@@ -27,116 +29,20 @@
 namespace zg {
 namespace adj {
 
-// ---- dual numbers: value and N partial derivatives ------------------------
-template <int N>
-struct Dual {
-    double v;
-    double d[N];
-};
-template <int N>
-__device__ __forceinline__ Dual<N> dconst(double x) {
-    Dual<N> r;
-    r.v = x;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = 0.0;
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> dvar(double x, int k) {
-    Dual<N> r = dconst<N>(x);
-    r.d[k] = 1.0;
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator+(const Dual<N> &a, const Dual<N> &b) {
-    Dual<N> r;
-    r.v = a.v + b.v;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] + b.d[k];
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(const Dual<N> &a, const Dual<N> &b) {
-    Dual<N> r;
-    r.v = a.v - b.v;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] - b.d[k];
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(const Dual<N> &a) {
-    Dual<N> r;
-    r.v = -a.v;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = -a.d[k];
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator*(const Dual<N> &a, const Dual<N> &b) {
-    Dual<N> r;
-    r.v = a.v * b.v;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator/(const Dual<N> &a, const Dual<N> &b) {
-    Dual<N> r;
-    double inv = 1.0 / b.v;
-    r.v = a.v * inv;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * inv;
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator*(double s, const Dual<N> &a) {
-    Dual<N> r;
-    r.v = s * a.v;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = s * a.d[k];
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator+(const Dual<N> &a, double s) {
-    Dual<N> r = a;
-    r.v += s;
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> operator-(const Dual<N> &a, double s) {
-    Dual<N> r = a;
-    r.v -= s;
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> tsqrt(const Dual<N> &a) {
-    Dual<N> r;
-    r.v = ::sqrt(a.v);
-    double h = 0.5 / r.v;
-#pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = h * a.d[k];
-    return r;
-}
-template <int N>
-__device__ __forceinline__ Dual<N> tabs(const Dual<N> &a) {
-    return a.v < 0.0 ? -a : a;
-}
+// ---- scalar helpers for T = double (FP64 form) and T = float (mixed form) ----
 __device__ __forceinline__ double tsqrt(double x) { return ::sqrt(x); }
+__device__ __forceinline__ float tsqrt(float x) { return ::sqrtf(x); }
 __device__ __forceinline__ double tabs(double x) { return ::fabs(x); }
-__device__ __forceinline__ double val(double x) { return x; }
-template <int N>
-__device__ __forceinline__ double val(const Dual<N> &x) {
-    return x.v;
-}
+__device__ __forceinline__ float tabs(float x) { return ::fabsf(x); }
 // min / max: the argument the forward picks (first unless the second is
-// strictly better), differentiated on that side
+// strictly better); the reverse differentiates that side
 template <class T>
 __device__ __forceinline__ T tmin(const T &a, const T &b) {
-    return val(b) < val(a) ? b : a;
+    return b < a ? b : a;
 }
 template <class T>
 __device__ __forceinline__ T tmax(const T &a, const T &b) {
-    return val(a) < val(b) ? b : a;
+    return a < b ? b : a;
 }
 
 // ---- the step's pieces, generic in T ----------------------------------------
@@ -146,26 +52,27 @@ __device__ __forceinline__ void prim(const T U[4], const T &gamma, T W[4]) {
     W[0] = U[0];
     W[1] = U[1] / U[0];
     W[2] = U[2] / U[0];
-    W[3] = (gamma - 1.0) * (U[3] - 0.5 * ((U[1] * U[1] + U[2] * U[2]) / U[0]));
+    W[3] = (gamma - T(1)) * (U[3] - T(0.5) * ((U[1] * U[1] + U[2] * U[2]) / U[0]));
 }
 
 // limited slope of one field along one axis from its three values:
 //   (phi(-dL, dR) dR - phi(-dR, dL) dL) / (2h)
 // where both limiter values share the denominator dL^2 + dR^2 + eps, so that
 //   = (dL - dR) (2 dL dR - eps) / (dL^2 + dR^2 + eps) / (2h).
-__device__ __forceinline__ double slope(double wm, double w0, double wp, double inv2h, double eps) {
-    double a = wm - w0, b = wp - w0;
-    return inv2h * ((a - b) * (2.0 * a * b - eps)) / (a * a + b * b + eps);
+template <class T>
+__device__ __forceinline__ T slope(T wm, T w0, T wp, T inv2h, T eps) {
+    T a = wm - w0, b = wp - w0;
+    return inv2h * ((a - b) * (T(2) * a * b - eps)) / (a * a + b * b + eps);
 }
 // its partial derivatives with respect to (wm, w0, wp)
-__device__ __forceinline__ void slope_partials(double wm, double w0, double wp, double inv2h, double eps,
-                                               double d[3]) {
-    double a = wm - w0, b = wp - w0;
-    double q = 2.0 * a * b - eps, P = (a - b) * q;
-    double iD = 1.0 / (a * a + b * b + eps);
-    double Pa = q + (a - b) * (2.0 * b), Pb = -q + (a - b) * (2.0 * a);
-    double ga = inv2h * (Pa - P * (2.0 * a) * iD) * iD;
-    double gb = inv2h * (Pb - P * (2.0 * b) * iD) * iD;
+template <class T>
+__device__ __forceinline__ void slope_partials(T wm, T w0, T wp, T inv2h, T eps, T d[3]) {
+    T a = wm - w0, b = wp - w0;
+    T q = T(2) * a * b - eps, P = (a - b) * q;
+    T iD = T(1) / (a * a + b * b + eps);
+    T Pa = q + (a - b) * (T(2) * b), Pb = -q + (a - b) * (T(2) * a);
+    T ga = inv2h * (Pa - P * (T(2) * a) * iD) * iD;
+    T gb = inv2h * (Pb - P * (T(2) * b) * iD) * iD;
     d[0] = ga;
     d[1] = -(ga + gb);
     d[2] = gb;
@@ -185,17 +92,17 @@ template <class T>
 __device__ void hllc(const T L[4], const T R[4], const T &gamma, T F[4]) {
     const T &rL = L[0], &uL = L[1], &vL = L[2], &pL = L[3];
     const T &rR = R[0], &uR = R[1], &vR = R[2], &pR = R[3];
-    T gm1 = gamma - 1.0;
-    T rEL = pL / gm1 + 0.5 * (rL * (uL * uL + vL * vL));
-    T rER = pR / gm1 + 0.5 * (rR * (uR * uR + vR * vR));
+    T gm1 = gamma - T(1);
+    T rEL = pL / gm1 + T(0.5) * (rL * (uL * uL + vL * vL));
+    T rER = pR / gm1 + T(0.5) * (rR * (uR * uR + vR * vR));
     T cL = tsqrt(gamma * pL / rL), cR = tsqrt(gamma * pR / rR);
     T SL = tmin(uL - cL, uR - cR);
     T SR = tmax(uL + cL, uR + cR);
-    if (val(SL) >= 0.0) {
+    if (SL >= T(0)) {
         phys_flux(rL, uL, vL, pL, rEL, F);
         return;
     }
-    if (val(SR) <= 0.0) {
+    if (SR <= T(0)) {
         phys_flux(rR, uR, vR, pR, rER, F);
         return;
     }
@@ -215,59 +122,59 @@ __device__ void hllc(const T L[4], const T R[4], const T &gamma, T F[4]) {
     T aSC = tabs(SC);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-        F[k] = 0.5 * (FL[k] + FR[k] + SL * (QsL[k] - QL[k]) + aSC * (QsL[k] - QsR[k]) + SR * (QsR[k] - QR[k]));
+        F[k] = T(0.5) * (FL[k] + FR[k] + SL * (QsL[k] - QL[k]) + aSC * (QsL[k] - QsR[k]) + SR * (QsR[k] - QR[k]));
 }
 
-// Reverse of hllc<double>: given the cotangent Fb of the flux, the
+// Reverse of hllc<T>: given the cotangent Fb of the flux, the
 // cotangents of the two face states (Lb, Rb, overwritten) and of gamma
 // (added to gb).  The forward is re-evaluated first; every min / max / abs /
 // branch takes the side the forward took.
-__device__ inline void hllc_vjp(const double L[4], const double R[4], double gamma, const double Fb[4],
-                                double Lb[4], double Rb[4], double &gb) {
-    const double rL = L[0], uL = L[1], vL = L[2], pL = L[3];
-    const double rR = R[0], uR = R[1], vR = R[2], pR = R[3];
-    const double gm1 = gamma - 1.0, igm1 = 1.0 / gm1;
-    const double irL = 1.0 / rL, irR = 1.0 / rR;
-    const double kL = uL * uL + vL * vL, kR = uR * uR + vR * vR;
-    const double rEL = pL * igm1 + 0.5 * (rL * kL), rER = pR * igm1 + 0.5 * (rR * kR);
-    const double xL = gamma * pL * irL, xR = gamma * pR * irR;
-    const double cL = ::sqrt(xL), cR = ::sqrt(xR);
-    const double A = uL - cL, B = uR - cR, C = uL + cL, D = uR + cR;
+template <class T>
+__device__ inline void hllc_vjp(const T L[4], const T R[4], T gamma, const T Fb[4], T Lb[4], T Rb[4], T &gb) {
+    const T rL = L[0], uL = L[1], vL = L[2], pL = L[3];
+    const T rR = R[0], uR = R[1], vR = R[2], pR = R[3];
+    const T gm1 = gamma - T(1.0), igm1 = T(1.0) / gm1;
+    const T irL = T(1.0) / rL, irR = T(1.0) / rR;
+    const T kL = uL * uL + vL * vL, kR = uR * uR + vR * vR;
+    const T rEL = pL * igm1 + T(0.5) * (rL * kL), rER = pR * igm1 + T(0.5) * (rR * kR);
+    const T xL = gamma * pL * irL, xR = gamma * pR * irR;
+    const T cL = tsqrt(xL), cR = tsqrt(xR);
+    const T A = uL - cL, B = uR - cR, C = uL + cL, D = uR + cR;
     const bool selB = B < A, selD = C < D;  // tmin / tmax choices
-    const double SL = selB ? B : A, SR = selD ? D : C;
-    double rLb = 0.0, uLb = 0.0, vLb = 0.0, pLb = 0.0, rELb = 0.0;
-    double rRb = 0.0, uRb = 0.0, vRb = 0.0, pRb = 0.0, rERb = 0.0;
-    double SLb = 0.0, SRb = 0.0;
+    const T SL = selB ? B : A, SR = selD ? D : C;
+    T rLb = T(0.0), uLb = T(0.0), vLb = T(0.0), pLb = T(0.0), rELb = T(0.0);
+    T rRb = T(0.0), uRb = T(0.0), vRb = T(0.0), pRb = T(0.0), rERb = T(0.0);
+    T SLb = T(0.0), SRb = T(0.0);
     // reverse of phys_flux(r, u, v, p, rE) scaled by w: F = w * Fb
-    auto phys_rev = [](double r, double u, double v, double p, double rE, const double *Fw, double &rb, double &ub,
-                       double &vb, double &pb, double &rEb) {
+    auto phys_rev = [](T r, T u, T v, T p, T rE, const T *Fw, T &rb, T &ub,
+                       T &vb, T &pb, T &rEb) {
         rb += Fw[0] * u + Fw[1] * (u * u) + Fw[2] * (u * v);
-        ub += Fw[0] * r + Fw[1] * (2.0 * r * u) + Fw[2] * (r * v) + Fw[3] * (rE + p);
+        ub += Fw[0] * r + Fw[1] * (T(2.0) * r * u) + Fw[2] * (r * v) + Fw[3] * (rE + p);
         vb += Fw[2] * (r * u);
         pb += Fw[1] + Fw[3] * u;
         rEb += Fw[3] * u;
     };
-    if (SL >= 0.0) {
+    if (SL >= T(0.0)) {
         phys_rev(rL, uL, vL, pL, rEL, Fb, rLb, uLb, vLb, pLb, rELb);
-    } else if (SR <= 0.0) {
+    } else if (SR <= T(0.0)) {
         phys_rev(rR, uR, vR, pR, rER, Fb, rRb, uRb, vRb, pRb, rERb);
     } else {
-        const double aL = rL * (SL - uL), aR = rR * (SR - uR);
-        const double num = pL - pR + aR * uR - aL * uL, den = aR - aL, iden = 1.0 / den;
-        const double SC = num * iden;
-        const double dLs = SL - SC, dRs = SR - SC, idL = 1.0 / dLs, idR = 1.0 / dRs;
-        const double rsL = aL * idL, rsR = aR * idR;
-        const double EL = rEL * irL, ER = rER * irR;
-        const double iaL = 1.0 / aL, iaR = 1.0 / aR;
-        const double tL = SC - uL, wL = SC + pL * iaL, tR = SC - uR, wR = SC + pR * iaR;
-        const double EsL = EL + tL * wL, EsR = ER + tR * wR;
-        const double QL[4] = {rL, rL * uL, rL * vL, rEL}, QR[4] = {rR, rR * uR, rR * vR, rER};
-        const double QsL[4] = {rsL, rsL * SC, rsL * vL, rsL * EsL}, QsR[4] = {rsR, rsR * SC, rsR * vR, rsR * EsR};
-        const double sgn = SC < 0.0 ? -1.0 : 1.0, aSC = sgn * SC;
-        double half[4], QsLb[4], QsRb[4], QLb[4], QRb[4], aSCb = 0.0;
+        const T aL = rL * (SL - uL), aR = rR * (SR - uR);
+        const T num = pL - pR + aR * uR - aL * uL, den = aR - aL, iden = T(1.0) / den;
+        const T SC = num * iden;
+        const T dLs = SL - SC, dRs = SR - SC, idL = T(1.0) / dLs, idR = T(1.0) / dRs;
+        const T rsL = aL * idL, rsR = aR * idR;
+        const T EL = rEL * irL, ER = rER * irR;
+        const T iaL = T(1.0) / aL, iaR = T(1.0) / aR;
+        const T tL = SC - uL, wL = SC + pL * iaL, tR = SC - uR, wR = SC + pR * iaR;
+        const T EsL = EL + tL * wL, EsR = ER + tR * wR;
+        const T QL[4] = {rL, rL * uL, rL * vL, rEL}, QR[4] = {rR, rR * uR, rR * vR, rER};
+        const T QsL[4] = {rsL, rsL * SC, rsL * vL, rsL * EsL}, QsR[4] = {rsR, rsR * SC, rsR * vR, rsR * EsR};
+        const T sgn = SC < T(0.0) ? -T(1.0) : T(1.0), aSC = sgn * SC;
+        T half[4], QsLb[4], QsRb[4], QLb[4], QRb[4], aSCb = T(0.0);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            half[k] = 0.5 * Fb[k];
+            half[k] = T(0.5) * Fb[k];
             SLb += half[k] * (QsL[k] - QL[k]);
             SRb += half[k] * (QsR[k] - QR[k]);
             aSCb += half[k] * (QsL[k] - QsR[k]);
@@ -278,14 +185,14 @@ __device__ inline void hllc_vjp(const double L[4], const double R[4], double gam
         }
         phys_rev(rL, uL, vL, pL, rEL, half, rLb, uLb, vLb, pLb, rELb);
         phys_rev(rR, uR, vR, pR, rER, half, rRb, uRb, vRb, pRb, rERb);
-        double SCb = aSCb * sgn;
+        T SCb = aSCb * sgn;
         // Qs = (rs, rs SC, rs v, rs Es)
-        double rsLb = QsLb[0] + QsLb[1] * SC + QsLb[2] * vL + QsLb[3] * EsL;
-        double rsRb = QsRb[0] + QsRb[1] * SC + QsRb[2] * vR + QsRb[3] * EsR;
+        T rsLb = QsLb[0] + QsLb[1] * SC + QsLb[2] * vL + QsLb[3] * EsL;
+        T rsRb = QsRb[0] + QsRb[1] * SC + QsRb[2] * vR + QsRb[3] * EsR;
         SCb += QsLb[1] * rsL + QsRb[1] * rsR;
         vLb += QsLb[2] * rsL;
         vRb += QsRb[2] * rsR;
-        const double EsLb = QsLb[3] * rsL, EsRb = QsRb[3] * rsR;
+        const T EsLb = QsLb[3] * rsL, EsRb = QsRb[3] * rsR;
         // Q = (r, r u, r v, rE)
         rLb += QLb[0] + QLb[1] * uL + QLb[2] * vL;
         uLb += QLb[1] * rL;
@@ -296,16 +203,16 @@ __device__ inline void hllc_vjp(const double L[4], const double R[4], double gam
         vRb += QRb[2] * rR;
         rERb += QRb[3];
         // Es = E + t w,  t = SC - u,  w = SC + p / a,  E = rE / r
-        double aLb = 0.0, aRb = 0.0;
+        T aLb = T(0.0), aRb = T(0.0);
         {
-            double ELb = EsLb, tLb = EsLb * wL, wLb = EsLb * tL;
+            T ELb = EsLb, tLb = EsLb * wL, wLb = EsLb * tL;
             SCb += tLb + wLb;
             uLb -= tLb;
             pLb += wLb * iaL;
             aLb -= wLb * pL * (iaL * iaL);
             rELb += ELb * irL;
             rLb -= ELb * EL * irL;
-            double ERb = EsRb, tRb = EsRb * wR, wRb = EsRb * tR;
+            T ERb = EsRb, tRb = EsRb * wR, wRb = EsRb * tR;
             SCb += tRb + wRb;
             uRb -= tRb;
             pRb += wRb * iaR;
@@ -315,15 +222,15 @@ __device__ inline void hllc_vjp(const double L[4], const double R[4], double gam
         }
         // rs = a / (S - SC)
         aLb += rsLb * idL;
-        double dLsb = -rsLb * rsL * idL;
+        T dLsb = -rsLb * rsL * idL;
         SLb += dLsb;
         SCb -= dLsb;
         aRb += rsRb * idR;
-        double dRsb = -rsRb * rsR * idR;
+        T dRsb = -rsRb * rsR * idR;
         SRb += dRsb;
         SCb -= dRsb;
         // SC = num / den
-        const double numb = SCb * iden, denb = -SCb * SC * iden;
+        const T numb = SCb * iden, denb = -SCb * SC * iden;
         aRb += denb;
         aLb -= denb;
         pLb += numb;
@@ -341,7 +248,7 @@ __device__ inline void hllc_vjp(const double L[4], const double R[4], double gam
         uRb -= aRb * rR;
     }
     // SL = min(uL - cL, uR - cR), SR = max(uL + cL, uR + cR)
-    double cLb = 0.0, cRb = 0.0;
+    T cLb = T(0.0), cRb = T(0.0);
     if (selB) {
         uRb += SLb;
         cRb -= SLb;
@@ -357,7 +264,7 @@ __device__ inline void hllc_vjp(const double L[4], const double R[4], double gam
         cLb += SRb;
     }
     // c = sqrt(gamma p / r)
-    const double xLb = cLb * 0.5 / cL, xRb = cRb * 0.5 / cR;
+    const T xLb = cLb * T(0.5) / cL, xRb = cRb * T(0.5) / cR;
     gb += xLb * (pL * irL) + xRb * (pR * irR);
     pLb += xLb * gamma * irL;
     rLb -= xLb * xL * irL;
@@ -367,8 +274,8 @@ __device__ inline void hllc_vjp(const double L[4], const double R[4], double gam
     pLb += rELb * igm1;
     pRb += rERb * igm1;
     gb -= (rELb * pL + rERb * pR) * (igm1 * igm1);
-    rLb += rELb * 0.5 * kL;
-    rRb += rERb * 0.5 * kR;
+    rLb += rELb * T(0.5) * kL;
+    rRb += rERb * T(0.5) * kR;
     uLb += rELb * rL * uL;
     vLb += rELb * rL * vL;
     uRb += rERb * rR * uR;
