@@ -62,6 +62,7 @@ def parse():
                     help="run one section alone and print its JSON (for ncu captures)")
     ap.add_argument("--amr-base", type=int, default=0, help="AMR base cells per side (default 512)")
     ap.add_argument("--amr-kernels", choices=["fast", "mixed", "parity"], default="fast")
+    ap.add_argument("--amr-criterion", choices=["gradient", "reference"], default="gradient")
     return ap.parse_args()
 
 
@@ -357,13 +358,20 @@ AMR_CELL_BYTES = 600   # bytes of one cell's AmrCells arrays (63 doubles, 22 int
 AMR_KERNELS = "fast"   # kernel family of the AMR step: "fast" (slot FAST) or "parity" (bit-exact)
 
 
-def _amr_setup(Z, init_state, mesh, solver):
+def _amr_flags(solver, mesh, criterion):
+    if criterion == "gradient":  # |grad rho| h / rho: refine above 0.05, coarsen below 0.01
+        solver.set_flags_gradient(mesh, 0.05, 0.01, download=False)
+    else:  # SmFluid::set_flags (neighbour jumps)
+        solver.set_flags(mesh, download=False)
+
+
+def _amr_setup(Z, init_state, mesh, solver, criterion="reference"):
     """smf_test_2D.cpp:112-117: max_level + 3 rounds of (initial data by cell
     means, set_flags, refine), then the initial data once more."""
     for _ in range(AMR_LEVELS + 3):
         g = init_state()
         mesh.set_state(*g)
-        solver.set_flags(mesh, download=False)
+        _amr_flags(solver, mesh, criterion)
         mesh.refine()
     mesh.set_state(*init_state())
 
@@ -403,11 +411,12 @@ def amr_cpu_reference(budget_s=12.0):
     RM.lib().zm_threads(0)
     return {"value": updates / sec, "unit": METRIC, "cores": threads, "kind": "reference",
             "sample": f"steps 0-{steps} after the initial adaptation ({r.n} live cells at the end), "
-                      f"set_flags + refine every {AMR_EVERY} steps; zephyr's EuMesh / SmFluid compiled from its "
+                      f"set_flags + refine every {AMR_EVERY} steps (the reference has the neighbour-jump "
+                      f"criterion only); zephyr's EuMesh / SmFluid compiled from its "
                       f"sources (oracle/_ref); {threads} std::threads"}
 
 
-def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None):
+def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None, criterion="reference"):
     """The quadtree AMR blast: base 512^2, 3 levels, the reference's
     SmFluid::set_flags criterion and slope distributor, adaptation every 10
     steps; the FP64 step on the slot mesh with the FAST kernels (derived face
@@ -436,11 +445,11 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
         g = mesh.amr_arrays()
         return blast_cell_means(g["vx"], g["vy"])
 
-    _amr_setup(Z, init, mesh, solver)
+    _amr_setup(Z, init, mesh, solver, criterion)
     for s in range(AMR_WARM_STEPS):
         solver.update(mesh)
         if (s + 1) % AMR_EVERY == 0:
-            solver.set_flags(mesh, download=False)
+            _amr_flags(solver, mesh, criterion)
             mesh.refine()
     torch.cuda.synchronize(dev)
     lib.zg_set_timing(mesh.ctx, 1)
@@ -456,7 +465,7 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
         if (s + 1) % AMR_EVERY == 0:
             a0, a1 = ev(), ev()
             a0.record(stream)
-            solver.set_flags(mesh, download=False)
+            _amr_flags(solver, mesh, criterion)
             mesh.refine()
             a1.record(stream)
             adapt_ev.append((a0, a1))
@@ -489,6 +498,8 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
                  "parity": "FP64 PARITY kernels on the slot mesh, bit-exact with the reference"}[kernels_name] +
                 " -- SmFluid second order, predictor-corrector, HLLC, van Albada 1, CFL 0.4; set_flags criterion; "
                 "slope distributor",
+        "criterion": ("|grad rho| h / rho: refine above 0.05, coarsen below 0.01" if criterion == "gradient" else
+                      "SmFluid::set_flags (neighbour jumps 0.05 / 0.4x, sm_fluid.cpp:517-559)"),
         "value": updates / (ms / 1e3), "unit": METRIC, "timed_steps": AMR_TIMED_STEPS,
         "window": f"steps {AMR_WARM_STEPS}-{AMR_WARM_STEPS + AMR_TIMED_STEPS}", "adapt_every": AMR_EVERY,
         "ms_total": ms, "ms_per_step_incl_adapt": ms / AMR_TIMED_STEPS,
@@ -607,7 +618,8 @@ def run_ours(args, rank, world, local_rank):
             AMR_BASE = args.amr_base
             AMR_CAPACITY = max(1 << 20, 32 * AMR_BASE * AMR_BASE)
         if args.only == "amr":
-            out = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name=args.amr_kernels)
+            out = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name=args.amr_kernels,
+                              criterion=args.amr_criterion)
             out.pop("final")
         elif args.only == "mm":
             out = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
@@ -680,10 +692,15 @@ def run_ours(args, rank, world, local_rank):
     mm_err = {f"l1_rel_{name}_err_vs_fp64": float(np.sum(np.abs(zmx[:, k] - z64[:, k])) / np.sum(np.abs(z64[:, k])))
               for name, k in (("density", 0), ("pressure", 3))}
     adjv = adjoint_variant(torch, dev, stream, local_rank)
+    # the benchmark's criterion (|grad rho| h / rho) for the FP64 FAST and
+    # MIXED forms; the reference's own set_flags for the bit-exact form
     amr = amr_variant(torch, lib, dev, stream, local_rank,
-                      want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), kernels_name="fast")
-    amr_par = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="parity")
-    amr_mx = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="mixed")
+                      want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), kernels_name="fast",
+                      criterion="gradient")
+    amr_par = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="parity",
+                          criterion="reference")
+    amr_mx = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name="mixed",
+                         criterion="gradient")
     (r64, lv64), (rmx, lvmx) = amr.pop("final"), amr_mx.pop("final")
     amr_par.pop("final")
     same_mesh = r64.shape == rmx.shape and bool(np.array_equal(lv64, lvmx))
@@ -759,10 +776,11 @@ def run_ours(args, rank, world, local_rank):
                 "gpu_launches": int(mm_mx["launches"])},
             "adjoint": adjv,
             "amr": amr,
-            "amr_parity": {k: amr_par[k] for k in ("form", "value", "unit", "ms_per_step_incl_adapt",
+            "amr_parity": {k: amr_par[k] for k in ("form", "criterion", "value", "unit", "ms_per_step_incl_adapt",
                                                      "step_only_value", "adapt_ms_avg", "live_cells",
                                                      "gpu_launches", "kernels")},
-            "amr_mixed": {k: amr_mx[k] for k in ("form", "value", "unit", "ms_per_step_incl_adapt", "speedup_vs_fp64",
+            "amr_mixed": {k: amr_mx[k] for k in ("form", "criterion", "value", "unit", "ms_per_step_incl_adapt",
+                                                  "speedup_vs_fp64",
                                                   "l1_rel_density_err_vs_fp64", "same_mesh_as_fp64",
                                                   "step_only_value", "adapt_ms_avg", "live_cells", "gpu_launches",
                                                   "kernels")},

@@ -188,6 +188,15 @@ int zg_amr_set_distributor(zg_ctx *ctx, int kind);
  * SmFluid::set_flags does (sm_fluid.cpp:517-522). */
 int zg_amr_put_flags(zg_ctx *ctx, const int *flags);
 
+/* Flags by the density-gradient criterion |grad rho| h / rho, h the square
+ * root of the cell's volume: 1 above refine_above, -1 below coarsen_below, 0
+ * between (no reference counterpart: the benchmark's AMR criterion, refine
+ * above 0.05 and coarsen below 0.01), with the unlimited least-squares
+ * density gradient.  The limited gradients of the current state are computed
+ * too and kept for the SLOPE distributor, as zg_smf_set_flags keeps its own.
+ * `flags` may be NULL (flags stay on the device). */
+int zg_amr_set_flags_gradient(zg_ctx *ctx, double refine_above, double coarsen_below, int *flags);
+
 /* Adapt the mesh to the flags; replaces EuMesh::refine (eu_mesh.cpp:290-359):
  * flag balancing, split and merge of cells with their hanging faces, the
  * distributor's states for new cells, compaction.  zg_mesh_n_cells gives the

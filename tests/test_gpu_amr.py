@@ -275,3 +275,24 @@ def test_mixed_form_adapts_and_conserves_mass(gpu_lib):
         assert abs(mass() - m0) <= 1e-9 * m0
     assert len(set(counts)) > 1  # the mesh did change
     mesh.close()
+
+
+def test_gradient_criterion_flags(gpu_lib):
+    """|grad rho| h / rho flags (the unlimited least-squares density
+    gradient): uniform density coarsens everywhere; a density step refines
+    the two columns next to it and coarsens the rest; a refine follows them."""
+    mesh, solver = gpu_mesh(32, (2, 2, 2, 2), 2, "slope", 2, "MC", 0.4)
+    g = mesh.amr_arrays()
+    n = mesh.n_cells()
+    ones = np.ones(n)
+    mesh.set_state(ones, 0 * ones, 0 * ones, ones, ones / 0.4)
+    assert (solver.set_flags_gradient(mesh) == -1).all()
+    rho = np.where(g["cx"] < 0.5, 1.0, 1.5)
+    mesh.set_state(rho, 0 * ones, 0 * ones, ones, ones / (0.4 * rho))
+    f = solver.set_flags_gradient(mesh, 0.05, 0.01)
+    near = np.abs(g["cx"] - 0.5) < 1.0 / 32
+    far = np.abs(g["cx"] - 0.5) > 3.0 / 32
+    assert (f[near] == 1).all() and (f[far] == -1).all()
+    mesh.refine()
+    assert mesh.n_cells() == n + 3 * int(near.sum())
+    mesh.close()

@@ -101,6 +101,7 @@ SIGNATURES = {
     "zg_amr_enable": (C.c_int, [_V, C.c_int, C.c_int]),
     "zg_amr_set_distributor": (C.c_int, [_V, C.c_int]),
     "zg_amr_put_flags": (C.c_int, [_V, _I]),
+    "zg_amr_set_flags_gradient": (C.c_int, [_V, C.c_double, C.c_double, _I]),
     "zg_amr_refine": (C.c_int, [_V]),
     "zg_amr_info": (C.c_int, [_V, C.POINTER(AmrStats)]),
     "zg_amr_download": (C.c_int, [_V, C.POINTER(AmrCells)]),

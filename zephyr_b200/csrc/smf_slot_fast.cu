@@ -49,5 +49,43 @@ void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *
     else k_heun<SlotFastAcc, BLOCK, false, S2M><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
 }
 
+// Refinement flags by the density-gradient criterion |grad rho| h / rho (h =
+// sqrt(volume)): 1 above `refine`, -1 below `coarsen`, 0 between.  The
+// gradient is the unlimited least-squares one (gradient.h:226-282 for the
+// density alone): a limited slope vanishes next to an isolated jump, which is
+// where refinement is wanted.
+__global__ void __launch_bounds__(BLOCK) k_grad_flags(SmfArgs a, int *flags, double refine, double coarsen) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    SlotFastAcc c(a, ic);
+    const double rc = a.z.r[ic];
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0, Fx = 0.0, Fy = 0.0;
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        const double rn = is_boundary(g.flag) ? rc : a.z.r[g.nb];
+        double ncx, ncy;
+        neib_center(c, g, s, c.cx(), c.cy(), ncx, ncy);
+        const double rx = ncx - c.cx(), ry = ncy - c.cy();
+        const double d = rx * g.nx + ry * g.ny, nxx = d * g.nx, nyy = d * g.ny;
+        const double an = sqrt(nxx * nxx + nyy * nyy), w = g.area / (an * an * an);
+        A00 += w * nxx * rx;
+        A01 += w * nxx * ry;
+        A10 += w * nyy * rx;
+        A11 += w * nyy * ry;
+        Fx += w * (rn - rc) * nxx;
+        Fy += w * (rn - rc) * nyy;
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;
+    const double inv = 1.0 / (A11 * A00 - A01 * A10);
+    const double gx = (A11 * Fx - A01 * Fy) * inv, gy = (-A10 * Fx + A00 * Fy) * inv;
+    const double crit = sqrt(gx * gx + gy * gy) * sqrt(c.vol()) / rc;
+    flags[ic] = crit > refine ? 1 : (crit < coarsen ? -1 : 0);
+}
+void launch_grad_flags(const SmfArgs &a, int *flags, double refine, double coarsen, void *stream) {
+    k_grad_flags<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, flags, refine, coarsen);
+}
+
 }  // namespace slotfast
 }  // namespace zg

@@ -75,6 +75,7 @@ void launch_grad(const SmfArgs &a, PrimPtr z, void *stream);
 void launch_stage1(const SmfArgs &a, void *stream);
 void launch_stage2(const SmfArgs &a, void *stream);
 void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream);
+void launch_grad_flags(const SmfArgs &a, int *flags, double refine, double coarsen, void *stream);
 }  // namespace slotfast
 
 }  // namespace zg

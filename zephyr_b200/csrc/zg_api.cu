@@ -1548,6 +1548,25 @@ int zg_amr_set_distributor(zg_ctx *c, int kind) {
     return ZG_OK;
 }
 
+int zg_amr_set_flags_gradient(zg_ctx *c, double refine_above, double coarsen_below, int *flags) {
+    if (!c || !(refine_above > coarsen_below)) return ZG_ERR_ARG;
+    if (!c->amr) return fail(c, ZG_ERR_STATE, "zg_amr_set_flags_gradient: mesh is not adaptive");
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_amr_set_flags_gradient: solver not configured");
+    DeviceGuard g(c->device);
+    int rc = materialize_prim(c);
+    if (rc != ZG_OK) return rc;
+    SmfArgs a = make_args(c);
+    void *st = (void *)c->stream;
+    timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->z, st); });
+    timed(c, ZG_K_FLAGS, [&] { slotfast::launch_grad_flags(a, c->av.flag, refine_above, coarsen_below, st); });
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "flags kernel launch");
+    if (!flags) return ZG_OK;
+    ZG_CUDA(c, cudaMemcpyAsync(flags, c->av.flag, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
 int zg_amr_put_flags(zg_ctx *c, const int *flags) {
     if (!c || !flags) return ZG_ERR_ARG;
     if (!c->amr) return fail(c, ZG_ERR_STATE, "zg_amr_put_flags: mesh is not adaptive");

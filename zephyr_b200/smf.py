@@ -444,6 +444,19 @@ class SmFluid:
         check(mesh.ctx, self._lib.zg_smf_set_flags(mesh.ctx, f.ctypes.data_as(C.POINTER(C.c_int))))
         return f
 
+    def set_flags_gradient(self, mesh: EuMesh, refine: float = 0.05, coarsen: float = 0.01, download: bool = True):
+        """Flags by |grad rho| h / rho (refine above `refine`, coarsen below
+        `coarsen`) on an adaptive mesh; no reference counterpart."""
+        if mesh is not self.mesh:
+            self.add_types(mesh)
+        if not download:
+            check(mesh.ctx, self._lib.zg_amr_set_flags_gradient(mesh.ctx, refine, coarsen, None))
+            return None
+        f = np.empty(mesh.n_cells(), np.int32)
+        check(mesh.ctx, self._lib.zg_amr_set_flags_gradient(mesh.ctx, refine, coarsen,
+                                                             f.ctypes.data_as(C.POINTER(C.c_int))))
+        return f
+
     def distributor(self, type: str = "slope") -> int:  # sm_fluid.cpp:372-375
         if type not in self.DISTRIBUTORS:
             raise ZgError(-1, f"SmFluid error: unknown m_distributor type '{type}'")
