@@ -324,6 +324,12 @@ int zg_material_named(int kind, const char *name, zg_material *out);
 enum zg_crp_mode { ZG_CRP_NONE = 0, ZG_CRP_V3 = 1, ZG_CRP_V5 = 2, ZG_CRP_VS = 3, ZG_CRP_PLIC = 4 };
 
 /* MmFluid(MixturePT) and its setters (mm_fluid.h:58-100). */
+/* Direction splitting of the multi-material step, values of DirSplit
+ * (mm_fluid.h:28-32): NONE, one face loop over all faces; SIMPLE, the x faces
+ * then the y faces, each with dt; STRANG, x faces with dt/2, y faces with dt,
+ * x faces with dt/2 (mm_fluid.cpp:112-137). */
+enum zg_dir_split { ZG_SPLIT_NONE = 0, ZG_SPLIT_SIMPLE = 1, ZG_SPLIT_STRANG = 2 };
+
 typedef struct zg_mmf_params {
     int n_materials;          /* 2 */
     zg_material materials[4]; /* MixturePT{...}, in order */
@@ -331,6 +337,7 @@ typedef struct zg_mmf_params {
     int accuracy;             /* 1 (set_accuracy) */
     double CFL;               /* clamped to [0, 1] (set_CFL) */
     double max_dt;            /* set_max_dt */
+    int split;                /* zg_dir_split (set_splitting) */
     int precision;            /* zg_precision: FP64 (the reference's arithmetic) or MIXED (FP32 face
                                  states, wave speeds and HLLC fluxes of the pure-stencil faces; FP64
                                  accumulation, update, EoS pressure recovery, composite Riemann

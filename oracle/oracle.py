@@ -66,6 +66,7 @@ def lib():
             getattr(L, name).argtypes = [C.c_void_p]
         L.zo_mm_set_max_dt.argtypes = [C.c_void_p, C.c_double]
         L.zo_mm_set_threads.argtypes = [C.c_void_p, C.c_int]
+        L.zo_mm_set_split.argtypes = [C.c_void_p, C.c_int]
         L.zo_mm_make_states.argtypes = [C.c_void_p, _P, _P, _P, _P, _P]
         L.zo_mm_set_states.argtypes = [C.c_void_p, _P]
         L.zo_mm_get_states.argtypes = [C.c_void_p, _P]
@@ -265,6 +266,10 @@ class MmSolver:
 
     def set_threads(self, n):
         lib().zo_mm_set_threads(self.h, n)
+
+    def set_splitting(self, split):
+        """DirSplit: 0 NONE, 1 SIMPLE, 2 STRANG (mm_fluid.cpp:112-137)."""
+        lib().zo_mm_set_split(self.h, int(split))
 
     def step(self):
         return lib().zo_mm_step(self.h)

@@ -29,6 +29,7 @@ def lib():
         L.zmm_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I, C.c_char_p,
                                  C.c_double, C.c_int, C.c_int]
         L.zmm_free.argtypes = [C.c_void_p]
+        L.zmm_set_split.argtypes = [C.c_void_p, C.c_int]
         L.zm_threads.argtypes = [C.c_int]
         L.zmm_n_cells.argtypes = [C.c_void_p]
         L.zmm_n_cells.restype = C.c_int
@@ -70,6 +71,10 @@ class RefMmFluid:
         self.h = lib().zmm_create(nx, ny, *box, b.ctypes.data_as(_I), materials.encode(), CFL, accuracy, crp_mode)
         self.n = lib().zmm_n_cells(self.h)
         self.nmat = materials.count(",") + 1
+
+    def set_splitting(self, split):
+        """MmFluid::set_splitting: 0 NONE, 1 SIMPLE, 2 STRANG."""
+        lib().zmm_set_split(self.h, int(split))
 
     def set_threads(self, n):
         """Worker threads of the reference's threads::for_each (0 or 1: off)."""

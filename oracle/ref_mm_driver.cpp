@@ -109,6 +109,11 @@ void *zmm_create(int nx, int ny, double x_min, double x_max, double y_min, doubl
 
 void zmm_free(void *p) { delete static_cast<RefMm *>(p); }
 
+// MmFluid::set_splitting (mm_fluid.cpp:75-77): 0 NONE, 1 SIMPLE, 2 STRANG
+void zmm_set_split(void *p, int split) {
+    static_cast<RefMm *>(p)->solver->set_splitting(math::DirSplit(split));
+}
+
 int zmm_n_cells(void *p) { return (int)static_cast<RefMm *>(p)->mesh->n_cells(); }
 
 // Initial states through the reference's PState(density, velocity, pressure,

@@ -1048,6 +1048,8 @@ void *zo_mm_create(void *mesh, int nm, const double *mats, double CFL, int crp_m
 void zo_mm_free(void *p) { delete static_cast<zo::mm::MmSolver *>(p); }
 void zo_mm_set_max_dt(void *p, double dt) { static_cast<zo::mm::MmSolver *>(p)->max_dt = dt; }
 void zo_mm_set_threads(void *p, int n) { static_cast<zo::mm::MmSolver *>(p)->threads = n; }
+// MmFluid::set_splitting (mm_fluid.cpp:75-77): 0 NONE, 1 SIMPLE, 2 STRANG
+void zo_mm_set_split(void *p, int split) { static_cast<zo::mm::MmSolver *>(p)->split = split; }
 // States from (density, velocity, pressure, mass fractions) through the
 // mixture closure, as PState(density, velocity, pressure, Fractions(array),
 // mixture); beta holds 4 fractions per cell and is normalised first.

@@ -171,22 +171,24 @@ def make_amr_cycle(name, n, bounds, max_level, distributor, acc, limiter, cycles
 MM_MATERIALS = "stiffened:Water,ideal:Air"
 
 
-def make_mm(name, n, crp_mode, steps):
-    """The reference's MmFluid (first order, CFL 0.4) on the shock / water
-    column problem at n x n: initial states through the reference's mixture
-    closure, the interface reconstruction of the first step, `steps` steps,
-    and the refinement flags at the end."""
+def make_mm(name, n, crp_mode, steps, split=0):
+    """The reference's MmFluid (first order, CFL 0.4, direction splitting
+    `split`: 0 NONE, 1 SIMPLE, 2 STRANG) on the shock / water column problem
+    at n x n: initial states through the reference's mixture closure, the
+    interface reconstruction of the first step, `steps` steps, and the
+    refinement flags at the end."""
     from oracle import ref_mm as RM
     from zephyr_b200.workloads import shock_water_column
     w = shock_water_column(n)
     r = RM.RefMmFluid(n, n, box=w.box, bounds=w.bounds, materials=MM_MATERIALS, CFL=0.4, accuracy=1,
                       crp_mode=crp_mode)
+    r.set_splitting(split)
     r.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
     init = r.states()
     nrm, off = r.interface()
     dts = np.array([r.step() for _ in range(steps)])
     np.savez_compressed(OUT / f"{name}.npz", n=n, box=np.array(w.box), bounds=np.array(w.bounds), crp_mode=crp_mode,
-                        CFL=0.4, steps=steps, inputs=np.stack([w.rho, w.vx, w.vy, w.p]), beta=w.beta, init=init,
+                        split=split, CFL=0.4, steps=steps, inputs=np.stack([w.rho, w.vx, w.vy, w.p]), beta=w.beta, init=init,
                         normals=nrm, offsets=off, dts=dts, final=r.states(), flags=r.flags())
 
 
@@ -265,6 +267,8 @@ def main():
     make_mm("mm_shock_column_32_plic", 32, 4, 200)
     make_mm("mm_shock_column_24_hllc", 24, 0, 120)
     make_mm("mm_shock_column_24_vs", 24, 3, 120)
+    make_mm("mm_shock_column_24_strang_plic", 24, 4, 80, split=2)
+    make_mm("mm_shock_column_24_simple_vs", 24, 3, 80, split=1)
     make_mm_pointwise()
     print("wrote multi-material cases")
     make_amr_cycles()
@@ -285,6 +289,9 @@ def make_amr_cycles():
 if __name__ == "__main__":
     if "--amr-cycle" in sys.argv:
         make_amr_cycles()
+    elif "--mm-split" in sys.argv:
+        make_mm("mm_shock_column_24_strang_plic", 24, 4, 80, split=2)
+        make_mm("mm_shock_column_24_simple_vs", 24, 3, 80, split=1)
     elif "--mm" in sys.argv:
         make_mm("mm_shock_column_32_plic", 32, 4, 200)
         make_mm("mm_shock_column_24_hllc", 24, 0, 120)

@@ -22,7 +22,9 @@ def same(a, b):
 def solver_for(g):
     n = int(g["n"])
     m = O.Mesh(n, n, *(float(x) for x in g["box"]), bounds=tuple(int(b) for b in g["bounds"]))
-    return m, O.MmSolver(m, CFL=float(g["CFL"]), crp_mode=int(g["crp_mode"]))
+    s = O.MmSolver(m, CFL=float(g["CFL"]), crp_mode=int(g["crp_mode"]))
+    s.set_splitting(int(g["split"]) if "split" in g.files else 0)
+    return m, s
 
 
 def test_mm_fixtures_present():

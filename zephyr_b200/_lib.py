@@ -79,7 +79,8 @@ class Material(C.Structure):
 class MmfParams(C.Structure):
     """zg_mmf_params"""
     _fields_ = [("n_materials", C.c_int), ("materials", Material * 4), ("crp_mode", C.c_int),
-                ("accuracy", C.c_int), ("CFL", C.c_double), ("max_dt", C.c_double), ("precision", C.c_int)]
+                ("accuracy", C.c_int), ("CFL", C.c_double), ("max_dt", C.c_double), ("split", C.c_int),
+                ("precision", C.c_int)]
 
 
 class AdjParams(C.Structure):

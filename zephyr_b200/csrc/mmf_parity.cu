@@ -252,9 +252,10 @@ constexpr int LIST_BLOCKS = 148 * 4;
 // independent), then one per cell summing its four face terms in slot order
 // as the reference's loop does, updating and closing the state.
 __global__ void __launch_bounds__(BLOCK) k_crp_faces(MmArgs a) {
-    const double dt = *a.dt_out;
+    const double dt = a.dt_scale * *a.dt_out;
     const int count = 4 * a.counts[0];
     for (int t = blockIdx.x * BLOCK + threadIdx.x; t < count; t += gridDim.x * BLOCK) {
+        if (skip_face(a.dir, t & 3)) continue;
         bool bad = false;
         double term[4 + NM];
         face_term(a, a.list_crp[t >> 2], t & 3, dt, term, bad);
@@ -264,16 +265,18 @@ __global__ void __launch_bounds__(BLOCK) k_crp_faces(MmArgs a) {
     }
 }
 __global__ void __launch_bounds__(BLOCK) k_crp_update(MmArgs a) {
-    const double dt = *a.dt_out;
+    const double dt = a.dt_scale * *a.dt_out;
     const int count = a.counts[0];
     for (int k = blockIdx.x * BLOCK + threadIdx.x; k < count; k += gridDim.x * BLOCK) {
         int ic = a.list_crp[k];
         MSt<NM> zc = load(a.z, ic);
         QVd<NM> flux = qv_zero<NM>();
 #pragma unroll
-        for (int s = 0; s < 4; ++s)
+        for (int s = 0; s < 4; ++s) {
+            if (skip_face(a.dir, s)) continue;
 #pragma unroll
             for (int j = 0; j < 4 + NM; ++j) flux.a[j] += a.fbuf[(size_t)(4 * k + s) * (4 + NM) + j];
+        }
         QVd<NM> q = q_of(zc);
         double coef = dt / a.mesh.vol;
 #pragma unroll

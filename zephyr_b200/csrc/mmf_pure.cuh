@@ -15,6 +15,10 @@ namespace mmf {
 constexpr int BLOCK = 128;
 constexpr int NM = NMAT;
 
+// a face the sub-step of direction `dir` leaves out (slots 0, 1 are the x
+// faces, 2, 3 the y faces of a rectangle cell)
+__device__ __forceinline__ bool skip_face(int dir, int s) { return (dir == 1 && s >= 2) || (dir == 2 && s < 2); }
+
 __device__ __forceinline__ void store(const MmField &f, int ic, const MSt<NM> &z) {
     f.rho[ic] = z.rho;
     f.vx[ic] = z.vx;
@@ -186,7 +190,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_flux_pure(MmArgs a) {
         a.list_crp[k] = ic;
         return;
     }
-    const double dt = *a.dt_out;
+    const double dt = a.dt_scale * *a.dt_out;
     const double V_c = c.vol();
     const PureSt<double> zc = load_pure<double>(a.z, ic, idx_c);
     const PureSt<R> zcR = load_pure<R>(a.z, ic, idx_c);
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_flux_pure(MmArgs a) {
     bool bad = false;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
+        if (skip_face(a.dir, s)) continue;
         FaceG g = c.face(s);
         PureSt<R> zn;
         if (!is_boundary(g.flag)) {

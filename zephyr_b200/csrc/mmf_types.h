@@ -25,6 +25,10 @@ struct MmArgs {
     MixD<NMAT> mix;
     int crp;
     int fp32_flux;  // mixed form: FP32 face arithmetic in the pure-stencil kernel
+    // direction splitting: the faces of this sub-step (0 all, 1 x faces, 2 y
+    // faces; AmrFaces::to_skip, amr_faces.cpp:186-197) and its share of dt
+    int dir;
+    double dt_scale;
     double CFL, max_dt;
     MmField z, znext;
     double *nrm_x[NMAT], *nrm_y[NMAT], *off[NMAT];  // interface reconstruction per material

@@ -1044,6 +1044,8 @@ mmf::MmArgs make_mm_args(const zg_ctx *c) {
     }
     a.crp = c->mpar.crp_mode;
     a.fp32_flux = c->mpar.precision == ZG_MIXED ? 1 : 0;
+    a.dir = 0;
+    a.dt_scale = 1.0;
     a.CFL = c->mpar.CFL;
     a.max_dt = c->mpar.max_dt;
     a.z = c->mz;
@@ -1075,17 +1077,39 @@ int mm_check_error(zg_ctx *c) {
     return ZG_OK;
 }
 
+// MmFluid::update (mm_fluid.cpp:112-137): dt once (the dt kernel also
+// empties the work lists), then integrate (139-170) over all faces, or over
+// the x and y faces in turn with direction splitting.
 int enqueue_mm_step(zg_ctx *c) {
-    mmf::MmArgs a = make_mm_args(c);
     void *st = (void *)c->stream;
-    timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(a, st); });
-    if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
-    timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux_pure(a, st); });
-    timed(c, ZG_K_MM_CRP, [&] { mmf::launch_flux_crp(a, st); });
-    timed(c, ZG_K_MM_CLOSURE, [&] { mmf::launch_closure(a, st); });
+    {
+        mmf::MmArgs a = make_mm_args(c);
+        timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(a, st); });
+    }
+    int sub = 0;
+    auto integrate = [&](int dir, double scale) {
+        mmf::MmArgs a = make_mm_args(c);
+        a.dir = dir;
+        a.dt_scale = scale;
+        if (sub++ > 0) cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), c->stream);  // empty work lists
+        if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
+        timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux_pure(a, st); });
+        timed(c, ZG_K_MM_CRP, [&] { mmf::launch_flux_crp(a, st); });
+        timed(c, ZG_K_MM_CLOSURE, [&] { mmf::launch_closure(a, st); });
+        std::swap(c->mz, c->mznext);  // MmFluid::swap (mm_fluid.cpp:682-684)
+    };
+    if (c->mpar.split == ZG_SPLIT_SIMPLE) {
+        integrate(1, 1.0);
+        integrate(2, 1.0);
+    } else if (c->mpar.split == ZG_SPLIT_STRANG) {
+        integrate(1, 0.5);
+        integrate(2, 1.0);
+        integrate(1, 0.5);
+    } else {
+        integrate(0, 1.0);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
-    std::swap(c->mz, c->mznext);  // MmFluid::swap (mm_fluid.cpp:682-684)
     return ZG_OK;
 }
 
@@ -1204,6 +1228,8 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
     }
     if (p->precision != ZG_FP64 && p->precision != ZG_MIXED)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown precision");
+    if (p->split < ZG_SPLIT_NONE || p->split > ZG_SPLIT_STRANG)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown direction splitting");
     if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_PLIC)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown CRP mode");
     if (std::min(std::max(1, p->accuracy), 2) != 1)

@@ -141,8 +141,8 @@ class MmFluid:
             self._push()
 
     def set_splitting(self, split: DirSplit):  # mm_fluid.cpp:75-77
-        if split != DirSplit.NONE:
-            raise ZgError(-1, "direction splitting is not implemented (DirSplit::NONE only)")
+        self.p.split = int(split)
+        self._push()
 
     def set_max_dt(self, dt: float):  # mm_fluid.cpp:91-93
         self.p.max_dt = dt
