@@ -58,9 +58,10 @@ def parse():
     ap.add_argument("--scheme", choices=["pc", "heun"], default="pc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids: one section alone on a smaller case (not the bench line)
-    ap.add_argument("--only", choices=["amr", "mm", "adjoint"], default=None,
+    ap.add_argument("--only", choices=["amr", "mm", "adjoint", "transfer"], default=None,
                     help="run one section alone and print its JSON (for ncu captures)")
     ap.add_argument("--amr-base", type=int, default=0, help="AMR base cells per side (default 512)")
+    ap.add_argument("--tr-nx", type=int, default=0, help="transport mesh cells along x (default 4096)")
     ap.add_argument("--amr-kernels", choices=["fast", "mixed", "parity"], default="fast")
     ap.add_argument("--amr-criterion", choices=["gradient", "reference"], default="gradient")
     return ap.parse_args()
@@ -595,6 +596,102 @@ def _max_over_ranks(torch, vals, dev, world):
     return [float(x) for x in t]
 
 
+TR_NX = 4096             # VOF transport: cells along x of [0, 1] x [0, 0.7]
+TR_DISKS = 64            # seeded disks of the transport workload
+# bytes per cell and split step (two sub-steps), each sub-step: face fluxes
+# read u1, n, p (40) and write two fluxes per face (16); the update reads the
+# two fluxes and u1 and writes u1 (32); the normals read u1 and write n, p
+# (40); three smoothing passes read u1, n, p and write n, p (3 x 72)
+TR_B_ALG = 2 * (56 + 32 + 40 + 216)
+
+
+def tr_cpu_reference(box, budget_s=10.0):
+    """The reference's own Transfer (oracle/_ref; its loops are serial) on a
+    512 x 358 sample of the workload; None when that build is absent."""
+    from oracle import ref_tr as RT
+    from zephyr_b200.workloads import transfer_disk_field
+    if not RT.available():
+        return None
+    nx, ny = 512, 358
+    r = RT.RefTransfer(nx, ny, box=box, method="VOF", CFL=0.5, vel=("translation", 0.7, -0.35))
+    r.set_u(transfer_disk_field(nx, ny, box, count=TR_DISKS, seed=7))
+    r.update_interface(3)
+
+    def step():
+        r.set_dt(r.compute_dt())
+        r.update(1)
+        r.update(2)
+
+    t0 = time.perf_counter()
+    step()
+    per = time.perf_counter() - t0
+    steps = max(1, min(20, int(budget_s / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    per = (time.perf_counter() - t0) / steps
+    return {"value": nx * ny / per, "unit": METRIC, "cores": 1, "kind": "reference",
+            "sample": f"{steps} split step(s) of a {nx}x{ny} mesh of the same disk field after 1 untimed step; "
+                      "zephyr's Transfer (VOF) compiled from its sources (oracle/_ref); serial loops"}
+
+
+def transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, nx=0):
+    """The scalar VOF transport (Transfer, method VOF with direction
+    splitting, the transfer problem's translation velocity) on a field of
+    disks, bit-exact with the reference; the transfer problem's time loop runs
+    on the device (zg_tr_advance)."""
+    import zephyr_b200 as Z
+    from zephyr_b200._lib import KERNEL_KINDS
+    from zephyr_b200.transfer import Method, Transfer
+    from zephyr_b200.workloads import transfer_disk_field
+    box = (0.0, 1.0, 0.0, 0.7)
+    nx = nx or TR_NX
+    ny = int(round(nx * 0.7))
+    u0 = transfer_disk_field(nx, ny, box, count=TR_DISKS, seed=7)
+    gen = Z.Rectangle(*box)
+    gen.set_boundaries(Z.Boundaries(Z.Boundary.ZOE, Z.Boundary.ZOE, Z.Boundary.ZOE, Z.Boundary.ZOE))
+    gen.set_sizes(nx, ny)
+    mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
+    s = Transfer()
+    s.set_method(Method.VOF)
+    s.set_CFL(0.5)
+    s.set_velocity_translation(0.7, -0.35)
+    s.add_types(mesh)
+    s.set_u1(mesh, u0)
+    s.update_interface(mesh)
+    t = s.advance(mesh, W, 0.0, 1.0e9, splitting=True)
+    lib.zg_set_timing(mesh.ctx, 1)
+    n0 = mesh.launch_count()
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.advance(mesh, K, t, 1.0e9, splitting=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = mesh.launch_count() - n0
+    kms = (C.c_double * len(KERNEL_KINDS))()
+    kcount = (C.c_longlong * len(KERNEL_KINDS))()
+    lib.zg_kernel_times(mesh.ctx, kms, kcount)
+    lib.zg_set_timing(mesh.ctx, 0)
+    tot = max(sum(kms), 1e-12)
+    kernels = {name: {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k],
+                      "share": kms[k] / tot} for k, name in enumerate(KERNEL_KINDS) if kcount[k]}
+    u = s.u1(mesh)  # raises if a polygon overflowed the kernels' capacity
+    cells = nx * ny
+    out = {"workload": f"transfer_disks {nx}x{ny} ([0,1]x[0,0.7], {TR_DISKS} seeded disks, ZOE walls)",
+           "form": "FP64, bit-exact with the reference (Transfer VOF, CFL 0.5, translation (0.7, -0.35), "
+                   "split X then Y, 3 smoothing passes)",
+           "ms": ms, "kernels": kernels, "launches": launches, "cells": cells,
+           "mixed_cells": int(((u > 0.0) & (u < 1.0)).sum())}
+    mesh.close()
+    if want_cpu:
+        out["cpu_baseline"] = tr_cpu_reference(box)
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import zephyr_b200 as Z
@@ -621,6 +718,8 @@ def run_ours(args, rank, world, local_rank):
             out = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name=args.amr_kernels,
                               criterion=args.amr_criterion)
             out.pop("final")
+        elif args.only == "transfer":
+            out = transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False, nx=args.tr_nx)
         elif args.only == "mm":
             out = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
                              precision=Z.Precision.MIXED if args.amr_kernels == "mixed" else Z.Precision.FP64)
@@ -692,6 +791,8 @@ def run_ours(args, rank, world, local_rank):
     mm_err = {f"l1_rel_{name}_err_vs_fp64": float(np.sum(np.abs(zmx[:, k] - z64[:, k])) / np.sum(np.abs(z64[:, k])))
               for name, k in (("density", 0), ("pressure", 3))}
     adjv = adjoint_variant(torch, dev, stream, local_rank)
+    trv = transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
+                           want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     # the benchmark's criterion (|grad rho| h / rho) for the FP64 FAST and
     # MIXED forms; the reference's own set_flags for the bit-exact form
     amr = amr_variant(torch, lib, dev, stream, local_rank,
@@ -709,8 +810,9 @@ def run_ours(args, rank, world, local_rank):
     amr_mx["same_mesh_as_fp64"] = same_mesh
 
     vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
-                                   amr["ms_total"], amr_par["ms_total"], mm_mx["ms"], amr_mx["ms_total"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx = vals
+                                   amr["ms_total"], amr_par["ms_total"], mm_mx["ms"], amr_mx["ms_total"],
+                                   trv["ms"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr = vals
     amr_mx["value"] = world * amr_mx["value"] * amr_mx["ms_total"] / ms_amr_mx
     amr_mx["speedup_vs_fp64"] = ms_amr / ms_amr_mx
     amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
@@ -742,7 +844,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
                             mm["launches"] + mm_mx["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
-                            amr_par["gpu_launches"] + amr_mx["gpu_launches"]),
+                            amr_par["gpu_launches"] + amr_mx["gpu_launches"] + trv["launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
@@ -775,6 +877,14 @@ def run_ours(args, rank, world, local_rank):
                 **mm_err, "err_after_steps": W + K, "kernels": mm_mx["kernels"],
                 "gpu_launches": int(mm_mx["launches"])},
             "adjoint": adjv,
+            "transfer": {
+                "value": world * trv["cells"] * K / (ms_tr / 1e3), "unit": METRIC, "ms_per_step": ms_tr / K,
+                "workload": trv["workload"], "form": trv["form"], "steps": K, "warmup": W,
+                "mixed_cells_at_end": trv["mixed_cells"],
+                "step_achieved_GBs": TR_B_ALG * trv["cells"] * K / (ms_tr / 1e3) / 1e9,
+                "step_frac": TR_B_ALG * trv["cells"] * K / (ms_tr / 1e3) / 1e9 / peak,
+                "algorithmic_bytes_per_cell": TR_B_ALG, "gpu_launches": int(trv["launches"]),
+                "kernels": trv["kernels"], "cpu_baseline": trv.get("cpu_baseline")},
             "amr": amr,
             "amr_parity": {k: amr_par[k] for k in ("form", "criterion", "value", "unit", "ms_per_step_incl_adapt",
                                                      "step_only_value", "adapt_ms_avg", "live_cells",

@@ -280,6 +280,11 @@ enum zg_kernel_kind {
     ZG_K_MM_FLUX,     /* multi-material face loop, cells whose stencil is all pure (MmFluid::fluxes) */
     ZG_K_MM_CRP,      /* multi-material face loop, cells next to a mixed cell (composite Riemann fluxes) */
     ZG_K_MM_CLOSURE,  /* PT-equilibrium closure of updates that came out mixed (MixturePT::get_rPT) */
+    ZG_K_TR_DT,       /* transport CFL minimum (Transfer::compute_dt) */
+    ZG_K_TR_FLUX,     /* transport face fluxes, swept polygons or CRP (Transfer::fluxes_VOF / fluxes_CRP) */
+    ZG_K_TR_UPDATE,   /* transport update of u1 */
+    ZG_K_TR_NORMALS,  /* interface normals and sections (InterfaceRecovery compute_normals + find_sections) */
+    ZG_K_TR_ADJUST,   /* one smoothing pass (InterfaceRecovery adjust_normals + find_sections) */
     ZG_K_COUNT
 };
 
@@ -384,6 +389,72 @@ int zg_mmf_set_flags(zg_ctx *ctx, int *flags);
  * the plane offset.  normals: 2 * n_materials doubles per cell; offsets:
  * n_materials per cell. */
 int zg_mmf_interface(zg_ctx *ctx, double *normals, double *offsets);
+
+/* ------------------------------------------------------------------------
+ * Scalar VOF transport: zephyr's Transfer (math/solver/transfer.h:21-150)
+ * advecting a volume fraction u1 with a prescribed velocity field, on the
+ * context's rectangle mesh (non-periodic).  The velocity is the transfer
+ * problem's field (problems/transfer.cpp:367-380), set in the parameters
+ * instead of by overriding Transfer::velocity.
+ * ------------------------------------------------------------------------ */
+
+/* Transfer::Method values (transfer.h:25-51) with kernels: the CRP family and
+ * VOF / VOF_CRP (swept-polygon fluxes with the PLIC reconstruction). */
+enum zg_tr_method {
+    ZG_TR_CRP_V3 = 0, ZG_TR_CRP_V5 = 1, ZG_TR_CRP_SE = 2, ZG_TR_CRP_N1 = 3, ZG_TR_CRP_N2 = 4,
+    ZG_TR_VOF = 5, ZG_TR_VOF_CRP = 6
+};
+enum zg_tr_velocity { ZG_TR_TRANSLATION = 0, ZG_TR_ROTATION = 1 };
+/* Face directions of one update (mesh::Direction, amr_faces.h:75-80). */
+enum zg_direction { ZG_DIR_ANY = 0, ZG_DIR_X = 1, ZG_DIR_Y = 2 };
+
+typedef struct zg_tr_params {
+    int method;      /* zg_tr_method (set_method) */
+    double CFL;      /* clamped to [0, 1] (set_CFL) */
+    int velocity;    /* zg_tr_velocity */
+    double vel[3];   /* TRANSLATION: vx, vy; ROTATION: centre x, y and the angular velocity about z */
+} zg_tr_params;
+
+/* Transfer()'s defaults (transfer.cpp:44-49): VOF, CFL 0.5, and the base
+ * class's velocity, the unit x translation (transfer.cpp:84-86). */
+void zg_tr_default_params(zg_tr_params *p);
+
+/* Configure on the context's rectangle (add_types, set_method, set_CFL);
+ * the first call allocates the fields (u1 = 0), later calls keep them. */
+int zg_tr_configure(zg_ctx *ctx, const zg_tr_params *p);
+
+/* u1 per cell from a host array (u2 = 0); the interface is not rebuilt:
+ * call zg_tr_update_interface as the reference's drivers do. */
+int zg_tr_upload(zg_ctx *ctx, const double *u1);
+
+/* u1 per cell; the interface normal n and base point p, (x, y) per cell;
+ * any pointer may be NULL.  Host arrays; synchronises. */
+int zg_tr_download(zg_ctx *ctx, double *u1, double *n, double *p);
+
+/* Transfer::update_interface(mesh, smoothing) (transfer.cpp:656-658). */
+int zg_tr_update_interface(zg_ctx *ctx, int smoothing);
+
+/* Transfer::compute_dt (transfer.cpp:98-105): returns the CFL step (and
+ * makes it the current dt, as the drivers then call set_dt with it). */
+int zg_tr_compute_dt(zg_ctx *ctx, double *dt);
+int zg_tr_set_dt(zg_ctx *ctx, double dt);
+int zg_tr_get_dt(zg_ctx *ctx, double *dt);
+
+/* Transfer::update(mesh, dir) (transfer.cpp:471-485): fluxes through the
+ * faces of direction dir, the update of u1 and the reconstruction (three
+ * smoothing passes for VOF, none for CRP). */
+int zg_tr_update(zg_ctx *ctx, int dir);
+
+/* `steps` iterations of the transfer problem's time loop
+ * (problems/transfer.cpp:213-236) without leaving the device: dt from
+ * compute_dt, clipped so that the time *time ends at t_end at most, then
+ * update(X) and update(Y) when `split`, else update(ANY); *time is read
+ * before and written after.  Asynchronous apart from the time copies. */
+int zg_tr_advance(zg_ctx *ctx, int steps, int split, double t_end, double *time);
+
+/* Transfer::set_flags (transfer.cpp:660-680): 1 where a neighbour's u1
+ * differs, else -1.  Host array. */
+int zg_tr_set_flags(zg_ctx *ctx, int *flags);
 
 /* ------------------------------------------------------------------------
  * Adjoint mode (no counterpart in the reference): the gradient of

@@ -15,11 +15,11 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "liboracle.so"
 SRC = HERE / "zoracle.cpp"
-INC = HERE / "zoracle_mm.inc"  # multi-material step, included by zoracle.cpp
+INCS = [HERE / "zoracle_mm.inc", HERE / "zoracle_tr.inc"]  # multi-material step, transport; included
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    if force or not OUT.exists() or OUT.stat().st_mtime < max(SRC.stat().st_mtime, INC.stat().st_mtime):
+    if force or not OUT.exists() or OUT.stat().st_mtime < max(p.stat().st_mtime for p in [SRC, *INCS]):
         cxx = shutil.which("g++") or "g++"
         cmd = [cxx, "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
                "-pthread", "-o", str(OUT), str(SRC)]

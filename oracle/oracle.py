@@ -91,6 +91,17 @@ def lib():
                             ("zo_mm_quad_volume_fraction", 5), ("zo_mm_average_flux", 3)):
             getattr(L, name).argtypes = [C.c_double] * nargs
             getattr(L, name).restype = C.c_double
+        L.zo_tr_create.restype = C.c_void_p
+        L.zo_tr_create.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, _P]
+        L.zo_tr_free.argtypes = [C.c_void_p]
+        L.zo_tr_set_u.argtypes = [C.c_void_p, _P]
+        L.zo_tr_update_interface.argtypes = [C.c_void_p, C.c_int]
+        L.zo_tr_compute_dt.argtypes = [C.c_void_p]
+        L.zo_tr_compute_dt.restype = C.c_double
+        L.zo_tr_set_dt.argtypes = [C.c_void_p, C.c_double]
+        L.zo_tr_update.argtypes = [C.c_void_p, C.c_int]
+        L.zo_tr_get.argtypes = [C.c_void_p, _P, _P, _P]
+        L.zo_tr_flags.argtypes = [C.c_void_p, _I]
         _lib = L
     return _lib
 
@@ -336,3 +347,48 @@ def mm_quad_volume_fraction(p, nx, ny, A, B):
 
 def mm_average_flux(alpha, cos, CFL):
     return lib().zo_mm_average_flux(alpha, cos, CFL)
+
+
+# Transfer::Method values (transfer.h:25-51) that the restatement covers
+TR_METHODS = {"CRP_V3": 0, "CRP_V5": 1, "CRP_SE": 2, "CRP_N1": 3, "CRP_N2": 4, "VOF": 5, "VOF_CRP": 6}
+
+
+class TrSolver:
+    """Restated Transfer (transfer.cpp) on an oracle Mesh; ``vel`` is
+    ``("translation", vx, vy)`` or ``("rotation", cx, cy, omega)``."""
+
+    def __init__(self, mesh, method="VOF", CFL=0.5, vel=("translation", 0.7, -0.35)):
+        self.mesh = mesh
+        kind = 0 if vel[0] == "translation" else 1
+        v = np.ascontiguousarray(list(vel[1:]) + [0.0] * (3 - len(vel[1:])), dtype=np.float64)
+        self.h = lib().zo_tr_create(mesh.h, TR_METHODS[method], CFL, kind, _dp(v))
+
+    def set_u(self, u):
+        lib().zo_tr_set_u(self.h, _dp(np.ascontiguousarray(u, dtype=np.float64)))
+
+    def update_interface(self, smoothing=3):
+        lib().zo_tr_update_interface(self.h, smoothing)
+
+    def compute_dt(self):
+        return lib().zo_tr_compute_dt(self.h)
+
+    def set_dt(self, dt):
+        lib().zo_tr_set_dt(self.h, dt)
+
+    def update(self, direction=0):
+        lib().zo_tr_update(self.h, direction)
+
+    def get(self):
+        n = self.mesh.n
+        u, nrm, pt = np.empty(n), np.empty((n, 2)), np.empty((n, 2))
+        lib().zo_tr_get(self.h, _dp(u), _dp(nrm), _dp(pt))
+        return u, nrm, pt
+
+    def flags(self):
+        f = np.empty(self.mesh.n, np.int32)
+        lib().zo_tr_flags(self.h, _ip(f))
+        return f
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.zo_tr_free(self.h)

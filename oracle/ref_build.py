@@ -61,7 +61,7 @@ MESH_DIRS = ["zephyr/mesh", "zephyr/geom", "zephyr/math/cfd", "zephyr/math/solve
 MESH_FILES = ["zephyr/utils/mpi.cpp", "zephyr/utils/threads.cpp", "zephyr/utils/json.cpp",
               "zephyr/utils/stopwatch.cpp", "zephyr/utils/numpy.cpp", "zephyr/math/funcs.cpp",
               "zephyr/math/random.cpp", "zephyr/math/sle/tridiagonal.cpp", "zephyr/math/calc/integrals.cpp"]
-MESH_SKIP = {"zephyr/math/solver/convection.cpp", "zephyr/math/solver/transfer.cpp"}
+MESH_SKIP = {"zephyr/math/solver/convection.cpp"}
 
 FLAGS = ["-std=c++20", "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-w"]
 # The reference relies on <cstring> and <functional> arriving through Eigen
@@ -132,7 +132,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     obj_dir.mkdir(parents=True, exist_ok=True)
     inc = ["-I", str(SHIM_COMMON), "-I", str(REF)]
     units = mesh_units()
-    drivers = ["ref_mesh_driver.cpp", "ref_mm_driver.cpp"]
+    drivers = ["ref_mesh_driver.cpp", "ref_mm_driver.cpp", "ref_tr_driver.cpp"]
     srcs = [REF / u for u in units] + [HERE / d for d in drivers]
     objs = [obj_dir / (u.replace("/", "_") + ".o") for u in units] + [obj_dir / (d + ".o") for d in drivers]
     with ThreadPoolExecutor(jobs) as ex:

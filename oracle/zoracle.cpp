@@ -856,6 +856,9 @@ struct Solver {
 // Multi-material step (MmFluid): namespace zo::mm.
 #include "zoracle_mm.inc"
 
+// Scalar VOF transport (Transfer): namespace zo::tr.
+#include "zoracle_tr.inc"
+
 }  // namespace zo
 
 // ---------------------------------------------------------------------------
@@ -1132,5 +1135,45 @@ double zo_mm_quad_volume_fraction(double p, double nx, double ny, double A, doub
     return zo::mm::quad_volume_fraction(p, {nx, ny, 0.0}, A, B);
 }
 double zo_mm_average_flux(double alpha, double cos, double CFL) { return zo::mm::average_flux(alpha, cos, CFL); }
+
+// ---- Transfer (zo::tr) ----
+// method: Transfer::Method value (VOF and CRP families); vel_kind 0: vel =
+// {vx, vy}; 1: vel = {cx, cy, omega}.
+void *zo_tr_create(void *mesh, int method, double CFL, int vel_kind, const double *vel) {
+    auto *s = new zo::tr::TrSolver(*static_cast<zo::Mesh *>(mesh));
+    s->method = method;
+    s->CFL = std::max(0.0, std::min(CFL, 1.0));  // Transfer::set_CFL (transfer.cpp:65-67)
+    s->vel_kind = vel_kind;
+    if (vel_kind == 0) {
+        s->V0 = {vel[0], vel[1], 0.0};
+    } else {
+        s->center = {vel[0], vel[1], 0.0};
+        s->omega = {0.0, 0.0, vel[2]};
+    }
+    return s;
+}
+void zo_tr_free(void *p) { delete static_cast<zo::tr::TrSolver *>(p); }
+void zo_tr_set_u(void *p, const double *u1) {
+    auto *s = static_cast<zo::tr::TrSolver *>(p);
+    for (int i = 0; i < s->m.n_cells; ++i) {
+        s->u1[i] = u1[i];
+        s->u2[i] = 0.0;
+    }
+}
+void zo_tr_update_interface(void *p, int smoothing) { static_cast<zo::tr::TrSolver *>(p)->update_interface(smoothing); }
+double zo_tr_compute_dt(void *p) { return static_cast<zo::tr::TrSolver *>(p)->compute_dt(); }
+void zo_tr_set_dt(void *p, double dt) { static_cast<zo::tr::TrSolver *>(p)->dt = dt; }
+void zo_tr_update(void *p, int dir) { static_cast<zo::tr::TrSolver *>(p)->update(dir); }
+void zo_tr_get(void *p, double *u1, double *nrm, double *pt) {
+    auto *s = static_cast<zo::tr::TrSolver *>(p);
+    for (int i = 0; i < s->m.n_cells; ++i) {
+        u1[i] = s->u1[i];
+        nrm[2 * i] = s->n[i].x;
+        nrm[2 * i + 1] = s->n[i].y;
+        pt[2 * i] = s->p[i].x;
+        pt[2 * i + 1] = s->p[i].y;
+    }
+}
+void zo_tr_flags(void *p, int *flags) { static_cast<zo::tr::TrSolver *>(p)->set_flags(flags); }
 
 }  // extern "C"

@@ -192,6 +192,54 @@ def make_mm(name, n, crp_mode, steps, split=0):
                         normals=nrm, offsets=off, dts=dts, final=r.states(), flags=r.flags())
 
 
+# Transfer fixtures: name -> (nx, ny, method, velocity, split, steps).  The
+# transfer problem (problems/transfer.cpp): a disk of radius 0.1 at
+# (0.15, 0.5) in [0, 1] x [0, 0.7] with ZOE walls, CFL 0.5.
+TR_TRANSLATION = ("translation", 0.7, -0.35)
+TR_ROTATION = ("rotation", 0.5, 0.5, float(np.pi))
+TR_CASES = {
+    "tr_disk_40x28_vof_translation_split": (40, 28, "VOF", TR_TRANSLATION, True, 30),
+    "tr_disk_40x28_vof_rotation_any": (40, 28, "VOF", TR_ROTATION, False, 30),
+    "tr_disk_36x25_vofcrp_rotation_split": (36, 25, "VOF_CRP", TR_ROTATION, True, 25),
+    "tr_disk_32x22_crpn1_translation_split": (32, 22, "CRP_N1", TR_TRANSLATION, True, 25),
+    "tr_disk_32x22_crpn2_rotation_any": (32, 22, "CRP_N2", TR_ROTATION, False, 25),
+    "tr_disk_30x21_crpse_translation_any": (30, 21, "CRP_SE", TR_TRANSLATION, False, 20),
+    "tr_disk_30x21_crpv3_rotation_split": (30, 21, "CRP_V3", TR_ROTATION, True, 20),
+    "tr_disk_30x21_crpv5_translation_split": (30, 21, "CRP_V5", TR_TRANSLATION, True, 20),
+}
+
+
+def make_tr(name, nx, ny, method, vel, split, steps):
+    """The reference's Transfer on the transfer problem: the disk's exact
+    cell fractions (BodyDisk::initial), the interface of update_interface,
+    `steps` iterations of the problem's time loop (compute_dt, set_dt,
+    update X then Y, or ANY), and the refinement flags at the end."""
+    from oracle import ref_tr as RT
+    box = (0.0, 1.0, 0.0, 0.7)
+    r = RT.RefTransfer(nx, ny, box=box, bounds=(2, 2, 2, 2), method=method, CFL=0.5, vel=vel)
+    u0 = r.disk(0.15, 0.5, 0.1)
+    r.set_u(u0)
+    r.update_interface(3 if method.startswith("VOF") else 0)
+    _, n0, p0 = r.get()
+    dts = []
+    for _ in range(steps):
+        dt = r.compute_dt()
+        r.set_dt(dt)
+        for d in ((1, 2) if split else (0,)):
+            r.update(d)
+        dts.append(dt)
+    u, n, p = r.get()
+    np.savez_compressed(OUT / f"{name}.npz", nx=nx, ny=ny, box=np.array(box), bounds=np.array((2, 2, 2, 2)),
+                        method=method, vel_kind=vel[0], vel=np.array(vel[1:], float), split=split, steps=steps,
+                        CFL=0.5, u0=u0, n0=n0, p0=p0, dts=np.array(dts), u=u, n=n, p=p, flags=r.flags())
+
+
+def make_trs():
+    for name, spec in TR_CASES.items():
+        make_tr(name, *spec)
+    print("wrote transfer cases")
+
+
 def make_mm_pointwise():
     """Mixture closure, sound speed, mixture HLLC and CRP fluxes of the
     reference on states taken from a running shock / water-column problem,
@@ -272,6 +320,7 @@ def main():
     make_mm_pointwise()
     print("wrote multi-material cases")
     make_amr_cycles()
+    make_trs()
 
 
 AMR_CYCLES = {
@@ -287,7 +336,9 @@ def make_amr_cycles():
 
 
 if __name__ == "__main__":
-    if "--amr-cycle" in sys.argv:
+    if "--transfer" in sys.argv:
+        make_trs()
+    elif "--amr-cycle" in sys.argv:
         make_amr_cycles()
     elif "--mm-split" in sys.argv:
         make_mm("mm_shock_column_24_strang_plic", 24, 4, 80, split=2)

@@ -83,6 +83,11 @@ class MmfParams(C.Structure):
                 ("precision", C.c_int)]
 
 
+class TrParams(C.Structure):
+    """zg_tr_params"""
+    _fields_ = [("method", C.c_int), ("CFL", C.c_double), ("velocity", C.c_int), ("vel", C.c_double * 3)]
+
+
 class AdjParams(C.Structure):
     """zg_adj_params"""
     _fields_ = [("gamma", C.c_double), ("dt", C.c_double), ("steps", C.c_int), ("checkpoint_every", C.c_int),
@@ -132,6 +137,17 @@ SIGNATURES = {
     "zg_mmf_dt": (C.c_int, [_V, _P]),
     "zg_mmf_set_flags": (C.c_int, [_V, _I]),
     "zg_mmf_interface": (C.c_int, [_V, _P, _P]),
+    "zg_tr_default_params": (None, [C.POINTER(TrParams)]),
+    "zg_tr_configure": (C.c_int, [_V, C.POINTER(TrParams)]),
+    "zg_tr_upload": (C.c_int, [_V, _P]),
+    "zg_tr_download": (C.c_int, [_V, _P, _P, _P]),
+    "zg_tr_update_interface": (C.c_int, [_V, C.c_int]),
+    "zg_tr_compute_dt": (C.c_int, [_V, _P]),
+    "zg_tr_set_dt": (C.c_int, [_V, C.c_double]),
+    "zg_tr_get_dt": (C.c_int, [_V, _P]),
+    "zg_tr_update": (C.c_int, [_V, C.c_int]),
+    "zg_tr_advance": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, _P]),
+    "zg_tr_set_flags": (C.c_int, [_V, _I]),
     "zg_adj_default_params": (None, [C.POINTER(AdjParams)]),
     "zg_adj_create": (C.c_int, [C.POINTER(_V), C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                 C.c_double]),
@@ -149,7 +165,7 @@ SIGNATURES = {
 
 # enum zg_kernel_kind
 KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags", "mm_dt", "mm_recover",
-                "mm_flux", "mm_crp", "mm_closure"]
+                "mm_flux", "mm_crp", "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals", "tr_adjust"]
 
 _lib = None
 

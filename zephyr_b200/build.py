@@ -40,6 +40,8 @@ UNITS = {
     "zg_noalloc.cu": ["-fmad=false"],
     # AMR refine: geometry and distributed states bit-exact with the reference
     "amr_refine.cu": ["-fmad=false"],
+    # scalar VOF transport: polygon clipping and sections bit-exact with the reference
+    "tr_vof.cu": ["-fmad=false"],
     "smf_fast.cu": [],
     "smf_slot_fast.cu": [],
     "smf_slot_mixed.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],

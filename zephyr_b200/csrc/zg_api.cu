@@ -17,6 +17,7 @@
 #include "smf_tiled.cuh"
 #include "smf_tiled_launch.h"
 #include "smf_types.h"
+#include "tr_types.h"
 
 using namespace zg;
 
@@ -88,6 +89,12 @@ struct zg_ctx {
     mmf::MmField mz{}, mznext{};
     double *mnx[mmf::NMAT] = {}, *mny[mmf::NMAT] = {}, *moff[mmf::NMAT] = {};
 
+    // scalar VOF transport (Transfer)
+    bool tr_configured = false;
+    zg_tr_params tpar{};
+    double *d_tr = nullptr;  // u1, n and p (two buffers), face fluxes, then 8 scalar slots
+    tr::TrArgs targs{};
+
     // per-kernel timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -140,8 +147,16 @@ void free_mm(zg_ctx *c) {
     c->mm_configured = false;
 }
 
+void free_tr(zg_ctx *c) {
+    cudaFree(c->d_tr);
+    c->d_tr = nullptr;
+    c->targs = tr::TrArgs{};
+    c->tr_configured = false;
+}
+
 void free_solver(zg_ctx *c) {
     free_mm(c);
+    free_tr(c);
     cudaFree(c->d_mq);
     cudaFree(c->d_mf);
     c->d_mq = nullptr;
@@ -1012,7 +1027,8 @@ int zg_kernel_times(zg_ctx *c, double *ms, long long *launches) {
 const char *zg_kernel_name(int kind) {
     static const char *names[ZG_K_COUNT] = {"dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b",
                                             "flags", "mm_dt", "mm_recover", "mm_flux", "mm_crp",
-                                            "mm_closure"};
+                                            "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals",
+                                            "tr_adjust"};
     return (kind >= 0 && kind < ZG_K_COUNT) ? names[kind] : "unknown";
 }
 
@@ -1417,6 +1433,258 @@ int zg_mmf_interface(zg_ctx *c, double *normals, double *offsets) {
             normals[(ic * mmf::NMAT + i) * 2 + 1] = buf[(3 * i + 1) * n + ic];
             offsets[ic * mmf::NMAT + i] = buf[(3 * i + 2) * n + ic];
         }
+    return ZG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Scalar VOF transport (Transfer, math/solver/transfer.cpp)
+
+void zg_tr_default_params(zg_tr_params *p) {
+    if (!p) return;
+    *p = zg_tr_params{};
+    p->method = ZG_TR_VOF;  // transfer.cpp:44-49
+    p->CFL = 0.5;
+    p->velocity = ZG_TR_TRANSLATION;  // Transfer::velocity: Vector3d::UnitX() (transfer.cpp:84-86)
+    p->vel[0] = 1.0;
+}
+
+}  // extern "C"
+
+namespace {
+
+int tr_ready(zg_ctx *c, const char *who) {
+    if (!c) return ZG_ERR_ARG;
+    if (!c->tr_configured) return fail(c, ZG_ERR_STATE, std::string(who) + ": zg_tr_configure first");
+    return ZG_OK;
+}
+
+// scalar slots after the fields: dt, time, CFL minimum bits, ticket, error
+// counter, the two work-list lengths
+enum { TR_DT = 0, TR_TIME = 1, TR_DMIN = 2, TR_TICKET = 3, TR_ERR = 4, TR_COUNT = 5, TR_NSCALAR = 8 };
+
+int tr_check_error(zg_ctx *c) {
+    int err = 0;
+    ZG_CUDA(c, cudaMemcpyAsync(&err, c->targs.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err) return fail(c, ZG_ERR_NUMERIC, "Transfer: a clipped polygon exceeded the kernels' vertex capacity");
+    return ZG_OK;
+}
+
+// InterfaceRecovery::update (interface_recovery.cpp:106-113)
+void tr_interface(zg_ctx *c, int smoothing) {
+    tr::TrArgs &a = c->targs;
+    timed(c, ZG_K_TR_NORMALS, [&] { tr::launch_normals(a, c->stream); });
+    for (int k = 0; k < smoothing; ++k) {
+        timed(c, ZG_K_TR_ADJUST, [&] { tr::launch_adjust(a, c->stream); });
+        a.cur = 1 - a.cur;
+    }
+}
+
+// Transfer::update (transfer.cpp:471-537): fluxes, update, reconstruction
+// (three smoothing passes for the VOF methods, none for CRP).
+void tr_update(zg_ctx *c, int dir) {
+    const tr::TrArgs &a = c->targs;
+    timed(c, ZG_K_TR_FLUX, [&] { tr::launch_flux(a, dir, c->stream); });
+    timed(c, ZG_K_TR_UPDATE, [&] { tr::launch_apply(a, dir, c->stream); });
+    tr_interface(c, tr::vof_type(c->tpar.method) ? 3 : 0);
+}
+
+void tr_dt(zg_ctx *c, bool advance, double t_end) {
+    timed(c, ZG_K_TR_DT, [&] { tr::launch_compute_dt(c->targs, advance, t_end, c->stream); });
+}
+
+}  // namespace
+
+extern "C" {
+
+int zg_tr_configure(zg_ctx *c, const zg_tr_params *p) {
+    if (!c || !p) return ZG_ERR_ARG;
+    if (!c->have_mesh || c->slots || c->amr)
+        return fail(c, ZG_ERR_STATE, "zg_tr_configure: needs a zg_mesh_rectangle mesh (not adaptive)");
+    if (c->mesh.xper || c->mesh.yper)
+        return fail(c, ZG_ERR_ARG, "zg_tr_configure: periodic boundaries are not supported (the reference clips "
+                                   "the upwind cell's polygon across the domain there)");
+    if (p->method < ZG_TR_CRP_V3 || p->method > ZG_TR_VOF_CRP)
+        return fail(c, ZG_ERR_ARG, "zg_tr_configure: method without GPU kernels (MUSCL and WENO families)");
+    if (p->velocity != ZG_TR_TRANSLATION && p->velocity != ZG_TR_ROTATION)
+        return fail(c, ZG_ERR_ARG, "zg_tr_configure: unknown velocity field");
+    DeviceGuard g(c->device);
+    c->tpar = *p;
+    c->tpar.CFL = std::max(0.0, std::min(p->CFL, 1.0));  // Transfer::set_CFL (transfer.cpp:65-67)
+    tr::TrArgs &a = c->targs;
+    a.m = tr::TrMesh{c->mesh.nx, c->mesh.ny, c->mesh.X,  c->mesh.Y,  c->mesh.cx, c->mesh.cy,
+                     c->mesh.fxm, c->mesh.fym, c->mesh.hx, c->mesh.hy, c->mesh.vol};
+    a.vel = tr::TrVel{p->velocity, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (p->velocity == ZG_TR_TRANSLATION) {
+        a.vel.vx = p->vel[0];
+        a.vel.vy = p->vel[1];
+    } else {
+        a.vel.cx = p->vel[0];
+        a.vel.cy = p->vel[1];
+        a.vel.w = p->vel[2];
+    }
+    a.method = p->method;
+    a.CFL = c->tpar.CFL;
+    if (c->tr_configured) return ZG_OK;
+
+    const size_t n = (size_t)c->n, nx = (size_t)c->mesh.nx, ny = (size_t)c->mesh.ny;
+    const size_t nfx = (nx + 1) * ny, nfy = nx * (ny + 1);
+    // fields, then the scalars, then the work lists (ints): faces, cells
+    const size_t total = 9 * n + 2 * nfx + 2 * nfy + TR_NSCALAR + (nfx + nfy + n + 1) / 2 + 1;
+    ZG_CUDA(c, cudaMalloc(&c->d_tr, total * sizeof(double)));
+    ZG_CUDA(c, cudaMemsetAsync(c->d_tr, 0, total * sizeof(double), c->stream));
+    double *b = c->d_tr;
+    a.u = b;
+    b += n;
+    for (int k = 0; k < 2; ++k) {
+        a.nx[k] = b;
+        a.ny[k] = b + n;
+        a.px[k] = b + 2 * n;
+        a.py[k] = b + 3 * n;
+        b += 4 * n;
+    }
+    a.cur = 0;
+    a.fxa = b;
+    a.fxb = b + nfx;
+    b += 2 * nfx;
+    a.fya = b;
+    a.fyb = b + nfy;
+    b += 2 * nfy;
+    a.dt = b + TR_DT;
+    a.time = b + TR_TIME;
+    a.dmin = reinterpret_cast<unsigned long long *>(b + TR_DMIN);
+    a.ticket = reinterpret_cast<unsigned int *>(b + TR_TICKET);
+    a.err = reinterpret_cast<int *>(b + TR_ERR);
+    a.count = reinterpret_cast<int *>(b + TR_COUNT);
+    a.flist = reinterpret_cast<int *>(b + TR_NSCALAR);
+    a.clist = a.flist + nfx + nfy;
+    double init[TR_NSCALAR] = {1.0e+300, 0.0, std::numeric_limits<double>::max(), 0.0, 0.0, 0.0, 0.0, 0.0};
+    ZG_CUDA(c, cudaMemcpyAsync(b, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));  // dt 1e300 (transfer.cpp:45)
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->tr_configured = true;
+    return ZG_OK;
+}
+
+int zg_tr_upload(zg_ctx *c, const double *u1) {
+    int rc = tr_ready(c, "zg_tr_upload");
+    if (rc != ZG_OK) return rc;
+    if (!u1) return fail(c, ZG_ERR_ARG, "zg_tr_upload: null array");
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(c->targs.u, u1, (size_t)c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_tr_download(zg_ctx *c, double *u1, double *nrm, double *pt) {
+    int rc = tr_ready(c, "zg_tr_download");
+    if (rc != ZG_OK) return rc;
+    DeviceGuard g(c->device);
+    const size_t n = (size_t)c->n;
+    const tr::TrArgs &a = c->targs;
+    std::vector<double> buf(4 * n);
+    if (u1) ZG_CUDA(c, cudaMemcpyAsync(u1, a.u, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    // the current buffers' nx, ny, px, py are contiguous
+    if (nrm || pt)
+        ZG_CUDA(c, cudaMemcpyAsync(buf.data(), a.nx[a.cur], 4 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < n && (nrm || pt); ++i) {
+        if (nrm) {
+            nrm[2 * i] = buf[i];
+            nrm[2 * i + 1] = buf[n + i];
+        }
+        if (pt) {
+            pt[2 * i] = buf[2 * n + i];
+            pt[2 * i + 1] = buf[3 * n + i];
+        }
+    }
+    return tr_check_error(c);
+}
+
+int zg_tr_update_interface(zg_ctx *c, int smoothing) {
+    int rc = tr_ready(c, "zg_tr_update_interface");
+    if (rc != ZG_OK) return rc;
+    if (smoothing < 0) return fail(c, ZG_ERR_ARG, "zg_tr_update_interface: negative smoothing");
+    DeviceGuard g(c->device);
+    tr_interface(c, smoothing);
+    ZG_CUDA(c, cudaGetLastError());
+    return ZG_OK;
+}
+
+int zg_tr_compute_dt(zg_ctx *c, double *dt) {
+    int rc = tr_ready(c, "zg_tr_compute_dt");
+    if (rc != ZG_OK) return rc;
+    DeviceGuard g(c->device);
+    tr_dt(c, false, 0.0);
+    ZG_CUDA(c, cudaGetLastError());
+    if (dt) {
+        ZG_CUDA(c, cudaMemcpyAsync(dt, c->targs.dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return ZG_OK;
+}
+
+int zg_tr_set_dt(zg_ctx *c, double dt) {
+    int rc = tr_ready(c, "zg_tr_set_dt");
+    if (rc != ZG_OK) return rc;
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(c->targs.dt, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_tr_get_dt(zg_ctx *c, double *dt) {
+    int rc = tr_ready(c, "zg_tr_get_dt");
+    if (rc != ZG_OK) return rc;
+    if (!dt) return ZG_ERR_ARG;
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(dt, c->targs.dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_tr_update(zg_ctx *c, int dir) {
+    int rc = tr_ready(c, "zg_tr_update");
+    if (rc != ZG_OK) return rc;
+    if (dir < ZG_DIR_ANY || dir > ZG_DIR_Y) return fail(c, ZG_ERR_ARG, "zg_tr_update: unknown direction");
+    DeviceGuard g(c->device);
+    tr_update(c, dir);
+    ZG_CUDA(c, cudaGetLastError());
+    return ZG_OK;
+}
+
+int zg_tr_advance(zg_ctx *c, int steps, int split, double t_end, double *time) {
+    int rc = tr_ready(c, "zg_tr_advance");
+    if (rc != ZG_OK) return rc;
+    if (steps < 0 || !time) return fail(c, ZG_ERR_ARG, "zg_tr_advance: steps >= 0 and a time required");
+    DeviceGuard g(c->device);
+    ZG_CUDA(c, cudaMemcpyAsync(c->targs.time, time, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    for (int k = 0; k < steps; ++k) {
+        tr_dt(c, true, t_end);
+        if (split) {
+            tr_update(c, ZG_DIR_X);
+            tr_update(c, ZG_DIR_Y);
+        } else {
+            tr_update(c, ZG_DIR_ANY);
+        }
+    }
+    ZG_CUDA(c, cudaGetLastError());
+    ZG_CUDA(c, cudaMemcpyAsync(time, c->targs.time, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+int zg_tr_set_flags(zg_ctx *c, int *flags) {
+    int rc = tr_ready(c, "zg_tr_set_flags");
+    if (rc != ZG_OK) return rc;
+    if (!flags) return fail(c, ZG_ERR_ARG, "zg_tr_set_flags: null array");
+    DeviceGuard g(c->device);
+    int *d = nullptr;
+    ZG_CUDA(c, cudaMallocAsync(&d, (size_t)c->n * sizeof(int), c->stream));
+    timed(c, ZG_K_FLAGS, [&] { tr::launch_flags(c->targs, d, c->stream); });
+    cudaError_t e = cudaMemcpyAsync(flags, d, (size_t)c->n * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    if (e != cudaSuccess) return fail(c, ZG_ERR_CUDA, cudaGetErrorString(e));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
     return ZG_OK;
 }
 

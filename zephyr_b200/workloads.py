@@ -9,6 +9,11 @@ fourier_smooth    smooth periodic data: rho = 1 + 0.2 f, u = 0.3 f, v = 0.3 f,
                   sin(2 pi m y + psi_m), a_m ~ U(0,1)/8, phi, psi ~ U(0, 2 pi),
                   drawn (a_m, phi_m, psi_m) for m = 1..8 from numpy's PCG64
                   with seeds 1, 2, 3, 4 for rho, u, v, p.
+transfer_disks    volume fractions of disks for the VOF transport (Transfer):
+                  the transfer problem's disk (problems/transfer.cpp:334-354,
+                  radius 0.1 at (0.15, 0.5) in [0, 1] x [0, 0.7]) or a seeded
+                  field of disks; cell fractions by sub x sub midpoint
+                  sampling of the cells that the circles cross.
 blast_cell_means  the AMR blast: rho = 1, u = v = 0, p = 1e-5 except p = 1e3
                   for r < 0.01 around (0.5, 0.5); cell means of the
                   conservative state by n x n midpoint sub-sampling of each
@@ -175,3 +180,50 @@ def blast_cell_means(map_x, map_y, n_sub: int = 20, gamma: float = 1.4):
     rho = np.ones(n)
     p = (gamma - 1.0) * E
     return rho, np.zeros(n), np.zeros(n), p, p / ((gamma - 1.0) * rho)
+
+
+def transfer_disks(nx: int, ny: int, box=(0.0, 1.0, 0.0, 0.7), disks=((0.15, 0.5, 0.1),), sub: int = 8) -> np.ndarray:
+    """Volume fraction of the union of `disks` (cx, cy, R) in every cell of the
+    nx by ny rectangle `box` (cell order ic = i * ny + j); cells a circle
+    crosses are sampled at sub x sub midpoints."""
+    x0, x1, y0, y1 = box
+    X = x0 + ((x1 - x0) * np.arange(nx + 1)) / nx
+    Y = y0 + ((y1 - y0) * np.arange(ny + 1)) / ny
+    u = np.zeros((nx, ny))
+    t = (np.arange(sub) + 0.5) / sub
+    for cx, cy, R in disks:
+        i0 = max(int(np.searchsorted(X, cx - R)) - 1, 0)
+        i1 = min(int(np.searchsorted(X, cx + R)) + 1, nx)
+        j0 = max(int(np.searchsorted(Y, cy - R)) - 1, 0)
+        j1 = min(int(np.searchsorted(Y, cy + R)) + 1, ny)
+        if i0 >= i1 or j0 >= j1:
+            continue
+        xa, xb = X[i0:i1][:, None], X[i0 + 1:i1 + 1][:, None]
+        ya, yb = Y[j0:j1][None, :], Y[j0 + 1:j1 + 1][None, :]
+        # nearest and farthest point of each cell from the centre
+        dnx = np.maximum(np.maximum(xa - cx, cx - xb), 0.0)
+        dny = np.maximum(np.maximum(ya - cy, cy - yb), 0.0)
+        dfx = np.maximum(np.abs(xa - cx), np.abs(xb - cx))
+        dfy = np.maximum(np.abs(ya - cy), np.abs(yb - cy))
+        near = dnx ** 2 + dny ** 2
+        far = dfx ** 2 + dfy ** 2
+        blk = u[i0:i1, j0:j1]
+        blk[far <= R * R] = 1.0
+        cut = np.argwhere((near < R * R) & (far > R * R))
+        for a, b in cut:
+            sx = X[i0 + a] + (X[i0 + a + 1] - X[i0 + a]) * t
+            sy = Y[j0 + b] + (Y[j0 + b + 1] - Y[j0 + b]) * t
+            inside = (sx[:, None] - cx) ** 2 + (sy[None, :] - cy) ** 2 < R * R
+            blk[a, b] = max(blk[a, b], inside.mean())
+    return np.ascontiguousarray(u.ravel())
+
+
+def transfer_disk_field(nx: int, ny: int, box=(0.0, 1.0, 0.0, 1.0), count: int = 64, seed: int = 7,
+                        sub: int = 8) -> np.ndarray:
+    """A seeded field of `count` disks (radii 0.01-0.04) for the transport
+    benchmark: more interface than the single disk at the same size."""
+    rng = np.random.default_rng(seed)
+    x0, x1, y0, y1 = box
+    disks = [(x0 + (x1 - x0) * (0.1 + 0.8 * rng.random()), y0 + (y1 - y0) * (0.1 + 0.8 * rng.random()),
+              0.01 + 0.03 * rng.random()) for _ in range(count)]
+    return transfer_disks(nx, ny, box, disks, sub)
