@@ -660,18 +660,21 @@ def transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cp
     s.set_u1(mesh, u0)
     s.update_interface(mesh)
     t = s.advance(mesh, W, 0.0, 1.0e9, splitting=True)
-    lib.zg_set_timing(mesh.ctx, 1)
     n0 = mesh.launch_count()
     barrier()
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    s.advance(mesh, K, t, 1.0e9, splitting=True)
+    t = s.advance(mesh, K, t, 1.0e9, splitting=True)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
     ms = e0.elapsed_time(e1)
     launches = mesh.launch_count() - n0
+    u = s.u1(mesh)  # raises if a polygon overflowed the kernels' capacity
+    # per-kernel times over K more steps (events around every launch)
+    lib.zg_set_timing(mesh.ctx, 1)
+    s.advance(mesh, K, t, 1.0e9, splitting=True)
     kms = (C.c_double * len(KERNEL_KINDS))()
     kcount = (C.c_longlong * len(KERNEL_KINDS))()
     lib.zg_kernel_times(mesh.ctx, kms, kcount)
@@ -679,7 +682,6 @@ def transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cp
     tot = max(sum(kms), 1e-12)
     kernels = {name: {"launches": int(kcount[k]), "ms_total": kms[k], "ms_avg": kms[k] / kcount[k],
                       "share": kms[k] / tot} for k, name in enumerate(KERNEL_KINDS) if kcount[k]}
-    u = s.u1(mesh)  # raises if a polygon overflowed the kernels' capacity
     cells = nx * ny
     out = {"workload": f"transfer_disks {nx}x{ny} ([0,1]x[0,0.7], {TR_DISKS} seeded disks, ZOE walls)",
            "form": "FP64, bit-exact with the reference (Transfer VOF, CFL 0.5, translation (0.7, -0.35), "

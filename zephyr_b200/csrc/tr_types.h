@@ -36,6 +36,7 @@ struct TrArgs {
     int method;
     double CFL;
     double *u;                               // volume fraction u1 per cell
+    double *u_next;                          // u1 after the update (the host swaps u and u_next)
     double *nx[2], *ny[2], *px[2], *py[2];   // interface normal and base point, two buffers
     int cur;                                 // buffer holding the current n and p
     double *fxa, *fxb;  // x faces ((nx + 1) * ny, face i * ny + j): flux summed by the left / right cell
@@ -48,6 +49,7 @@ struct TrArgs {
     int *count;                // work-list lengths: [0] faces, [1] cells
     int *flist;                // faces whose VOF flux clips polygons (index over the update's faces)
     int *clist;                // cells with a non-zero interface normal
+    unsigned char *zero_np;    // 1: both n / p buffers of the cell hold n = (+0, +0) and p = its centre
 };
 
 // Transfer::compute_dt (transfer.cpp:88-105) into *a.dt.  With `advance`
@@ -59,7 +61,8 @@ void launch_compute_dt(const TrArgs &a, bool advance, double t_end, cudaStream_t
 // swept polygons (VOF, VOF_CRP) or the CRP formulas.
 void launch_flux(const TrArgs &a, int dir, cudaStream_t st);
 
-// u1 <- between(u1 - sum of face fluxes / volume, 0, 1).
+// u_next <- between(u1 - sum of face fluxes / volume, 0, 1); the caller
+// swaps u and u_next.
 void launch_apply(const TrArgs &a, int dir, cudaStream_t st);
 
 // compute_normals + find_sections into the buffers a.cur.

@@ -51,7 +51,6 @@ using mmf::sgn;
 using mmf::sorted2;
 
 constexpr int BLOCK = 128;
-constexpr unsigned LIST_GRID = 148u * 4u;  // blocks of the work-list kernels
 constexpr int MAXV = 12;  // polygon capacity (a convex quadrilateral clipped three times has at most 7)
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
@@ -102,21 +101,6 @@ __device__ __forceinline__ void set_center(Poly &P) {
     }
     P.cx = sx;
     P.cy = sy;
-}
-
-// AmrCells::polygon of a linear cell: vs<-1,-1>, vs<+1,-1>, vs<+1,+1>, vs<-1,+1>
-__device__ __forceinline__ void cell_poly(const TrMesh &m, int i, int j, Poly &P) {
-    double x0 = m.X[i], x1 = m.X[i + 1], y0 = m.Y[j], y1 = m.Y[j + 1];
-    P.n = 4;
-    P.x[0] = x0;
-    P.y[0] = y0;
-    P.x[1] = x1;
-    P.y[1] = y0;
-    P.x[2] = x1;
-    P.y[2] = y1;
-    P.x[3] = x0;
-    P.y[3] = y1;
-    set_center(P);
 }
 
 // Polygon::area (polygon.cpp:191-209)
@@ -258,34 +242,125 @@ __device__ AnS clip_area_and_slice(const Poly &P, P2 p, P2 n, bool slice) {
     return r;
 }
 
-// Polygon::find_section (polygon.cpp:555-574) with find_section_newton
-// (polygon.cpp:487-553): the middle of the section by the line of normal n
-// that cuts off the fraction alpha.
-__device__ P2 find_section(const Poly &P, P2 n_in, double alpha) {
-    const P2 n = normalized(n_in);
-    if (bad_normal(n)) return alpha < 0.5 ? mk(CUDART_NAN, CUDART_NAN) : mk(P.cx, P.cy);
-    // minmax (polygon.cpp:406-429)
-    int imin = 0, imax = 0;
-    double min_dot = P.x[0] * n.x + P.y[0] * n.y, max_dot = min_dot;
-    for (int i = 1; i < P.n; ++i) {
-        double d = P.x[i] * n.x + P.y[i] * n.y;
-        if (d < min_dot) {
-            imin = i;
-            min_dot = d;
-        } else if (d > max_dot) {
-            imax = i;
-            max_dot = d;
+// ---------------------------------------------------------------------------
+// Polygon operations on the cell's own rectangle (x0, x1) x (y0, y1),
+// vertices v0 = (x0, y0), v1 = (x1, y0), v2 = (x1, y1), v3 = (x0, y1) in
+// AmrCells::polygon order (vs<-1,-1>, vs<+1,-1>, vs<+1,+1>, vs<-1,+1>,
+// amr_cells.cpp:157-180): every vertex index is static or selected, so the
+// polygon stays in registers.  The operations and their order are those of
+// clip_area_and_slice above and of Polygon::find_section (polygon.cpp:555-574)
+// with find_section_newton (polygon.cpp:487-553).
+struct Rect {
+    double x0, x1, y0, y1, cx, cy;
+    __device__ __forceinline__ double vx(int k) const { return (k == 1 || k == 2) ? x1 : x0; }
+    __device__ __forceinline__ double vy(int k) const { return k >= 2 ? y1 : y0; }
+};
+
+__device__ __forceinline__ Rect make_rect(const TrMesh &m, int i, int j) {
+    Rect r;
+    r.x0 = m.X[i];
+    r.x1 = m.X[i + 1];
+    r.y0 = m.Y[j];
+    r.y1 = m.Y[j + 1];
+    // m_center: ((0 + v0) + v1 + v2 + v3) / 4
+    r.cx = (((0.0 + r.x0) + r.x1) + r.x1 + r.x0) / 4.0;
+    r.cy = (((0.0 + r.y0) + r.y0) + r.y1 + r.y1) / 4.0;
+    return r;
+}
+
+__device__ __forceinline__ double rect_area(const Rect &r) {
+    double S = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) S += cross_c(r.cx, r.cy, r.vx(k), r.vy(k), r.vx((k + 1) & 3), r.vy((k + 1) & 3));
+    return 0.5 * S;
+}
+
+__device__ AnS rect_clip_area_and_slice(const Rect &r, P2 p, P2 n) {
+    AnS res;
+    res.area = 0.0;
+    res.tri_in = res.tri_out = false;
+    res.p1 = res.p2 = mk(0.0, 0.0);
+    if (bad_normal(n)) {
+        // Polygon::inside on the rectangle (unreached from find_section, whose
+        // normal is unit)
+        const P2 tau = mk(0.123, 0.346433);
+        int counter = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (exist_ray(p, tau, r.vx(k), r.vy(k), r.vx((k + 1) & 3), r.vy((k + 1) & 3))) ++counter;
+        res.p1 = res.p2 = mk(CUDART_NAN, CUDART_NAN);
+        res.area = counter % 2 > 0 ? rect_area(r) : 0.0;
+        return res;
+    }
+    double d[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) d[k] = (r.vx(k) - p.x) * n.x + (r.vy(k) - p.y) * n.y;
+    int idx_out_in = -1, idx_in_out = -1;
+    P2 sec_out_in = mk(0.0, 0.0), sec_in_out = mk(0.0, 0.0);
+#pragma unroll
+    for (int i2 = 0; i2 < 4; ++i2) {
+        const int i1 = (i2 + 3) & 3;
+        const double dot1 = d[i1], dot2 = d[i2];
+        if (dot1 * dot2 < 0.0) {
+            const double x1 = r.vx(i1), y1 = r.vy(i1), x2 = r.vx(i2), y2 = r.vy(i2);
+            const double Det = (x2 - x1) * n.x + (y2 - y1) * n.y;
+            const P2 sec = mk((dot2 * x1 - dot1 * x2) / Det, (dot2 * y1 - dot1 * y2) / Det);
+            if (dot1 <= 0.0) {
+                idx_in_out = i1;
+                sec_in_out = sec;
+            } else {
+                idx_out_in = i1;
+                sec_out_in = sec;
+            }
         }
     }
-    const P2 vmin = mk(P.x[imin], P.y[imin]), vmax = mk(P.x[imax], P.y[imax]);
+    if (idx_in_out < 0 || idx_out_in < 0) {
+        res.area = d[3] < 0.0 ? rect_area(r) : 0.0;
+        return res;
+    }
+    res.p1 = sec_in_out;
+    res.p2 = sec_out_in;
+    res.tri_in = ((idx_in_out - idx_out_in + 4) & 3) == 1;
+    res.tri_out = ((idx_out_in - idx_in_out + 4) & 3) == 1;
+    const int k1 = (idx_out_in + 1) & 3;
+    double a = 0.0;
+    a += cross_c(r.cx, r.cy, sec_out_in.x, sec_out_in.y, r.vx(k1), r.vy(k1));
+    a += cross_c(r.cx, r.cy, r.vx(idx_in_out), r.vy(idx_in_out), sec_in_out.x, sec_in_out.y);
+    a += cross_c(r.cx, r.cy, sec_in_out.x, sec_in_out.y, sec_out_in.x, sec_out_in.y);
+    const int end = idx_in_out < idx_out_in ? idx_in_out + 4 : idx_in_out;
+#pragma unroll
+    for (int q = 1; q < 4; ++q) {
+        const int i = idx_out_in + q;
+        if (i < end) a += cross_c(r.cx, r.cy, r.vx(i & 3), r.vy(i & 3), r.vx((i + 1) & 3), r.vy((i + 1) & 3));
+    }
+    res.area = a * 0.5;
+    return res;
+}
+
+__device__ P2 rect_find_section(const Rect &r, P2 n_in, double alpha) {
+    const P2 n = normalized(n_in);
+    if (bad_normal(n)) return alpha < 0.5 ? mk(CUDART_NAN, CUDART_NAN) : mk(r.cx, r.cy);
+    int imin = 0, imax = 0;
+    double min_dot = r.vx(0) * n.x + r.vy(0) * n.y, max_dot = min_dot;
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+        const double dk = r.vx(k) * n.x + r.vy(k) * n.y;
+        if (dk < min_dot) {
+            imin = k;
+            min_dot = dk;
+        } else if (dk > max_dot) {
+            imax = k;
+            max_dot = dk;
+        }
+    }
+    const P2 vmin = mk(r.vx(imin), r.vy(imin)), vmax = mk(r.vx(imax), r.vy(imax));
     if (alpha < 1.0e-14) return mk(vmin.x - 0.1 * n.x, vmin.y - 0.1 * n.y);
     if (alpha > 1.0 - 1.0e-14) return mk(vmax.x + 0.1 * n.x, vmax.y + 0.1 * n.y);
-
     const double DV = (vmax.x - vmin.x) * n.x + (vmax.y - vmin.y) * n.y;
     const P2 dv = mk(DV * n.x, DV * n.y);
-    const double S = area(P);
+    const double S = rect_area(r);
     double x = alpha;
-    AnS f = clip_area_and_slice(P, mk(vmin.x + x * dv.x, vmin.y + x * dv.y), n, true);
+    AnS f = rect_clip_area_and_slice(r, mk(vmin.x + x * dv.x, vmin.y + x * dv.y), n);
     double err = fabs(f.area / S - alpha);
     int it = 0;
     while (err > 1.0e-12 && it < 30) {
@@ -295,7 +370,7 @@ __device__ P2 find_section(const Poly &P, P2 n_in, double alpha) {
         else if (f.tri_out) x = 1.0 - sqrt(2.0 * (1.0 - alpha) * (1.0 - x) * S / (DV * slice));
         else x -= (f.area - alpha * S) / (DV * slice);
         x = dmax(0.0, dmin(x, 1.0));
-        f = clip_area_and_slice(P, mk(vmin.x + x * dv.x, vmin.y + x * dv.y), n, true);
+        f = rect_clip_area_and_slice(r, mk(vmin.x + x * dv.x, vmin.y + x * dv.y), n);
         err = fabs(f.area / S - alpha);
         ++it;
     }
@@ -349,7 +424,19 @@ __device__ double flux_vof(const TrArgs &a, int i, int j, P2 v1, P2 v2, P2 fc, P
     const P2 n2 = perpendicular(mk(l2b.x - v2.x, l2b.y - v2.y), mk(v2.x - fc.x, v2.y - fc.y));
 
     Poly A, B;
-    cell_poly(a.m, i, j, A);
+    {
+        // AmrCells::polygon of the linear cell (amr_cells.cpp:157-180)
+        const double x0 = a.m.X[i], x1 = a.m.X[i + 1], y0 = a.m.Y[j], y1 = a.m.Y[j + 1];
+        A.n = 4;
+        A.x[0] = x0;
+        A.y[0] = y0;
+        A.x[1] = x1;
+        A.y[1] = y0;
+        A.x[2] = x1;
+        A.y[2] = y1;
+        A.x[3] = x0;
+        A.y[3] = y1;
+    }
     clip(A, mk(fc.x - xi * fn.x, fc.y - xi * fn.y), mk(-fn.x, -fn.y), B, a.err);
     clip(B, c1, n1, A, a.err);
     clip(A, c2, n2, B, a.err);
@@ -603,7 +690,9 @@ __global__ void __launch_bounds__(BLOCK) k_flux_classify(TrArgs a, int dir) {
     if (live) {
         f = face_at(a.m, dir, t, is_x, slot);
         defer = vof_type(a.method) && face_needs_polygon(a, f, dir);
-        if (!defer) {
+        // plain VOF: a face that clips no polygon carries +-0, which the
+        // update skips (k_update); nothing to store
+        if (!defer && a.method != VOF) {
             double fa, fb;
             face_fluxes<false>(a, f, dir, fa, fb);
             store_face(a, is_x, slot, fa, fb);
@@ -613,7 +702,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux_classify(TrArgs a, int dir) {
 }
 
 // The deferred VOF faces.
-__global__ void __launch_bounds__(BLOCK) k_flux_list(TrArgs a, int dir) {
+__global__ void __launch_bounds__(BLOCK, 4) k_flux_list(TrArgs a, int dir) {
     const int cnt = a.count[0];
     for (int k = blockIdx.x * BLOCK + threadIdx.x; k < cnt; k += gridDim.x * BLOCK) {
         bool is_x;
@@ -627,6 +716,15 @@ __global__ void __launch_bounds__(BLOCK) k_flux_list(TrArgs a, int dir) {
 
 // u1 <- between(u1 - sum of fluxes / volume, 0, 1), faces in slot order
 // L, R, B, T (update_VOF / update_CRP, transfer.cpp:487-511)
+// For plain VOF a face that clips no polygon carries +-0: adding it changes
+// no sum except the sign of an exact zero, which u1 - 0 / V does not show,
+// so such faces are skipped (and k_flux_classify stores nothing for them).
+// The new u1 goes to the other buffer: the predicate reads the neighbours'
+// old u1.
+__device__ __forceinline__ bool carries_flux(const TrArgs &a, const Face &f, int dir) {
+    return a.method != VOF || face_needs_polygon(a, f, dir);
+}
+
 __global__ void __launch_bounds__(BLOCK) k_update(TrArgs a, int dir) {
     const int nx = a.m.nx, ny = a.m.ny;
     const int ic = blockIdx.x * BLOCK + threadIdx.x;
@@ -634,15 +732,15 @@ __global__ void __launch_bounds__(BLOCK) k_update(TrArgs a, int dir) {
     const int i = ic / ny, j = ic - i * ny;
     double fl = 0.0;
     if (dir != 2) {
-        if (i > 0) fl += a.fxb[(size_t)i * ny + j];
-        if (i < nx - 1) fl += a.fxa[(size_t)(i + 1) * ny + j];
+        if (i > 0 && carries_flux(a, x_face(a.m, i, j), dir)) fl += a.fxb[(size_t)i * ny + j];
+        if (i < nx - 1 && carries_flux(a, x_face(a.m, i + 1, j), dir)) fl += a.fxa[(size_t)(i + 1) * ny + j];
     }
     if (dir != 1) {
-        if (j > 0) fl += a.fyb[(size_t)i * (ny + 1) + j];
-        if (j < ny - 1) fl += a.fya[(size_t)i * (ny + 1) + j + 1];
+        if (j > 0 && carries_flux(a, y_face(a.m, i, j), dir)) fl += a.fyb[(size_t)i * (ny + 1) + j];
+        if (j < ny - 1 && carries_flux(a, y_face(a.m, i, j + 1), dir)) fl += a.fya[(size_t)i * (ny + 1) + j + 1];
     }
     const double u2 = a.u[ic] - fl / a.m.vol;
-    a.u[ic] = dmax(0.0, dmin(u2, 1.0));
+    a.u_next[ic] = dmax(0.0, dmin(u2, 1.0));
 }
 
 // compute_normal (interface_recovery.cpp:18-38) for every cell.  Cells
@@ -683,17 +781,22 @@ __global__ void __launch_bounds__(BLOCK) k_normals(TrArgs a) {
             n = normalized(mk(ax, ay));
         }
         const int c = a.cur;
-        a.nx[c][ic] = n.x;
-        a.ny[c][ic] = n.y;
         if (is_zero(n.x, n.y)) {
-            const double px = a.m.cx[i], py = a.m.cy[j];
-            a.px[c][ic] = px;
-            a.py[c][ic] = py;
-            a.nx[1 - c][ic] = n.x;
-            a.ny[1 - c][ic] = n.y;
-            a.px[1 - c][ic] = px;
-            a.py[1 - c][ic] = py;
+            // zero_np[ic] = 1: both buffers already hold this normal and the centre
+            if (!(a.zero_np[ic] && n.x == 0.0 && n.y == 0.0 && !signbit(n.x) && !signbit(n.y))) {
+                const double px = a.m.cx[i], py = a.m.cy[j];
+                for (int b = 0; b < 2; ++b) {
+                    a.nx[b][ic] = n.x;
+                    a.ny[b][ic] = n.y;
+                    a.px[b][ic] = px;
+                    a.py[b][ic] = py;
+                }
+                a.zero_np[ic] = (n.x == 0.0 && n.y == 0.0 && !signbit(n.x) && !signbit(n.y)) ? 1 : 0;
+            }
         } else {
+            a.nx[c][ic] = n.x;
+            a.ny[c][ic] = n.y;
+            if (a.zero_np[ic]) a.zero_np[ic] = 0;
             listed = true;
         }
     }
@@ -706,9 +809,7 @@ __global__ void __launch_bounds__(BLOCK) k_sections(TrArgs a) {
     for (int k = blockIdx.x * BLOCK + threadIdx.x; k < cnt; k += gridDim.x * BLOCK) {
         const int ic = a.clist[k];
         const int i = ic / ny, j = ic - i * ny;
-        Poly P;
-        cell_poly(a.m, i, j, P);
-        const P2 p = find_section(P, mk(a.nx[c][ic], a.ny[c][ic]), a.u[ic]);
+        const P2 p = rect_find_section(make_rect(a.m, i, j), mk(a.nx[c][ic], a.ny[c][ic]), a.u[ic]);
         a.px[c][ic] = p.x;
         a.py[c][ic] = p.y;
     }
@@ -728,7 +829,7 @@ __device__ void adjust_cell(const TrArgs &a, int ic) {
         const P2 pc = mk(a.px[c][ic], a.py[c][ic]);
         const double pp = pc.x * pn.x + pc.y * pn.y;
         const P2 r0 = mk(pp * pn.x, pp * pn.y);
-        P2 ints[2];
+        P2 q0 = mk(0.0, 0.0), q1 = mk(0.0, 0.0);  // the first two section points
         int cnt = 0;
         for (int s = 0; s < 4; ++s) {
             // face vertices (face_nodes2d, indexing.h:279-284) and the neighbour
@@ -769,23 +870,19 @@ __device__ void adjust_cell(const TrArgs &a, int ic) {
                 const double t = cross2(mk(pb.x - v1.x, pb.y - v1.y), l2t) / det;
                 q = mk(v1.x + tau.x * t, v1.y + tau.y * t);
             }
-            if (cnt < 2) ints[cnt] = q;
+            if (cnt == 0) q0 = q;
+            else if (cnt == 1) q1 = q;
             ++cnt;
         }
         if (cnt > 1) {
-            P2 nn = mk(ints[0].y - ints[1].y, ints[1].x - ints[0].x);
+            P2 nn = mk(q0.y - q1.y, q1.x - q0.x);
             if (nn.x * pn.x + nn.y * pn.y < 0.0) nn = mk(nn.x * -1.0, nn.y * -1.0);
             n = normalized(nn);
         }
     }
     P2 p;
-    if (is_zero(n.x, n.y)) {
-        p = mk(a.m.cx[i], a.m.cy[j]);
-    } else {
-        Poly P;
-        cell_poly(a.m, i, j, P);
-        p = find_section(P, n, uc);
-    }
+    if (is_zero(n.x, n.y)) p = mk(a.m.cx[i], a.m.cy[j]);
+    else p = rect_find_section(make_rect(a.m, i, j), n, uc);
     a.nx[o][ic] = n.x;
     a.ny[o][ic] = n.y;
     a.px[o][ic] = p.x;
@@ -865,10 +962,29 @@ void launch_compute_dt(const TrArgs &a, bool advance, double t_end, cudaStream_t
     k_dt<<<g, BLOCK, 0, st>>>(a, advance ? 1 : 0, t_end);
 }
 
-// grid of the work-list kernels: a few resident blocks per SM, striding
-inline unsigned list_blocks(long long n) {
+// Grid of a work-list kernel: the blocks that are resident at once (SMs x
+// blocks per SM at the kernel's register use), striding over the list.
+template <class K>
+unsigned list_blocks(K kernel, long long n) {
+    static thread_local const void *keys[4] = {};
+    static thread_local unsigned vals[4] = {};
+    unsigned resident = 0;
+    int slot = 0;
+    for (; slot < 4 && keys[slot]; ++slot)
+        if (keys[slot] == (const void *)kernel) resident = vals[slot];
+    if (!resident) {
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, 0);
+        resident = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+        if (slot < 4) {
+            keys[slot] = (const void *)kernel;
+            vals[slot] = resident;
+        }
+    }
     const unsigned g = blocks(n);
-    return g < LIST_GRID ? (g ? g : 1u) : LIST_GRID;
+    return g < resident ? (g ? g : 1u) : resident;
 }
 
 void launch_flux(const TrArgs &a, int dir, cudaStream_t st) {
@@ -877,7 +993,7 @@ void launch_flux(const TrArgs &a, int dir, cudaStream_t st) {
     if (nf == 0) return;
     cudaMemsetAsync(a.count + 0, 0, sizeof(int), st);
     k_flux_classify<<<blocks(nf), BLOCK, 0, st>>>(a, dir);
-    if (vof_type(a.method)) k_flux_list<<<list_blocks(nf), BLOCK, 0, st>>>(a, dir);
+    if (vof_type(a.method)) k_flux_list<<<list_blocks(k_flux_list, nf), BLOCK, 0, st>>>(a, dir);
 }
 
 void launch_apply(const TrArgs &a, int dir, cudaStream_t st) {
@@ -888,11 +1004,11 @@ void launch_normals(const TrArgs &a, cudaStream_t st) {
     const long long n = (long long)a.m.nx * a.m.ny;
     cudaMemsetAsync(a.count + 1, 0, sizeof(int), st);
     k_normals<<<blocks(n), BLOCK, 0, st>>>(a);
-    k_sections<<<list_blocks(n), BLOCK, 0, st>>>(a);
+    k_sections<<<list_blocks(k_sections, n), BLOCK, 0, st>>>(a);
 }
 
 void launch_adjust(const TrArgs &a, cudaStream_t st) {
-    k_adjust<<<list_blocks((long long)a.m.nx * a.m.ny), BLOCK, 0, st>>>(a);
+    k_adjust<<<list_blocks(k_adjust, (long long)a.m.nx * a.m.ny), BLOCK, 0, st>>>(a);
 }
 
 void launch_flags(const TrArgs &a, int *flags, cudaStream_t st) {

@@ -1486,6 +1486,7 @@ void tr_update(zg_ctx *c, int dir) {
     const tr::TrArgs &a = c->targs;
     timed(c, ZG_K_TR_FLUX, [&] { tr::launch_flux(a, dir, c->stream); });
     timed(c, ZG_K_TR_UPDATE, [&] { tr::launch_apply(a, dir, c->stream); });
+    std::swap(c->targs.u, c->targs.u_next);
     tr_interface(c, tr::vof_type(c->tpar.method) ? 3 : 0);
 }
 
@@ -1530,12 +1531,13 @@ int zg_tr_configure(zg_ctx *c, const zg_tr_params *p) {
     const size_t n = (size_t)c->n, nx = (size_t)c->mesh.nx, ny = (size_t)c->mesh.ny;
     const size_t nfx = (nx + 1) * ny, nfy = nx * (ny + 1);
     // fields, then the scalars, then the work lists (ints): faces, cells
-    const size_t total = 9 * n + 2 * nfx + 2 * nfy + TR_NSCALAR + (nfx + nfy + n + 1) / 2 + 1;
+    const size_t total = 10 * n + 2 * nfx + 2 * nfy + TR_NSCALAR + (nfx + nfy + n + 1) / 2 + 1 + (n + 7) / 8;
     ZG_CUDA(c, cudaMalloc(&c->d_tr, total * sizeof(double)));
     ZG_CUDA(c, cudaMemsetAsync(c->d_tr, 0, total * sizeof(double), c->stream));
     double *b = c->d_tr;
     a.u = b;
-    b += n;
+    a.u_next = b + n;
+    b += 2 * n;
     for (int k = 0; k < 2; ++k) {
         a.nx[k] = b;
         a.ny[k] = b + n;
@@ -1558,6 +1560,7 @@ int zg_tr_configure(zg_ctx *c, const zg_tr_params *p) {
     a.count = reinterpret_cast<int *>(b + TR_COUNT);
     a.flist = reinterpret_cast<int *>(b + TR_NSCALAR);
     a.clist = a.flist + nfx + nfy;
+    a.zero_np = reinterpret_cast<unsigned char *>(a.clist + n);
     double init[TR_NSCALAR] = {1.0e+300, 0.0, std::numeric_limits<double>::max(), 0.0, 0.0, 0.0, 0.0, 0.0};
     ZG_CUDA(c, cudaMemcpyAsync(b, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));  // dt 1e300 (transfer.cpp:45)
     ZG_CUDA(c, cudaStreamSynchronize(c->stream));
