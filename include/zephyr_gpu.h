@@ -457,6 +457,53 @@ int zg_tr_advance(zg_ctx *ctx, int steps, int split, double t_end, double *time)
 int zg_tr_set_flags(zg_ctx *ctx, int *flags);
 
 /* ------------------------------------------------------------------------
+ * Output: VTU files and PVD series in zephyr's format (io/vtu_file.cpp,
+ * io/pvd_file.cpp): XML header plus raw appended binary, cells written as
+ * quadrilaterals (VtuStructure::fill_adaptive_hex_2D, vtu_file.cpp:186-201).
+ * The arrays are packed from the device buffers on the GPU and written in
+ * one pass; the bytes equal the reference writer's for the same mesh and
+ * variables.  Meshes: zg_mesh_rectangle meshes and adaptive ones.
+ * ------------------------------------------------------------------------ */
+
+/* Sources of cell variables. */
+enum zg_out_source {
+    /* io::Variable's named variables (io/variable.cpp:11-160): */
+    ZG_OUT_LEVEL = 0,   /* Int8 */
+    ZG_OUT_INDEX = 1,   /* Int32, the cell's index */
+    ZG_OUT_RANK = 2,    /* Int32, 0 */
+    ZG_OUT_FLAG = 3,    /* Int8, the last refinement flags (0 before any) */
+    ZG_OUT_B_IDX = 4,   /* Int32 */
+    ZG_OUT_Z_IDX = 5,   /* Int32 */
+    ZG_OUT_CENTER = 6,  /* Float32 x 3 */
+    /* Float64 fields of the device state (`component` selects): */
+    ZG_OUT_SMF = 7,     /* SmFluid: 0 density, 1 velocity x, 2 velocity y, 3 pressure, 4 energy */
+    ZG_OUT_MMF = 8,     /* MmFluid: 0 density, 1 vx, 2 vy, 3 pressure, 4 energy, 5 temperature,
+                           6 + k mass fraction k, 6 + n_materials + k true density k */
+    ZG_OUT_TR = 9,      /* Transfer: 0 u1, 1 n.x, 2 n.y, 3 p.x, 4 p.y; 5 n and 6 p as 3-vectors (z = 0) */
+    ZG_OUT_HOST = 10    /* Float64, a host array of n_cells values (any quantity the caller computes) */
+};
+
+typedef struct zg_out_var {
+    const char *name;    /* the DataArray's Name */
+    int source;          /* zg_out_source */
+    int component;       /* field of ZG_OUT_SMF / MMF / TR */
+    const double *host;  /* ZG_OUT_HOST: n_cells doubles */
+} zg_out_var;
+
+/* VtuFile::save(filename, mesh, variables) (vtu_file.cpp:555-584): creates
+ * the parent directories and writes the file.  Synchronises. */
+int zg_vtu_write(zg_ctx *ctx, const char *filename, const zg_out_var *vars, int n_vars);
+
+/* PvdFile (pvd_file.h:12-89): open(filename, directory) writes the empty
+ * collection (directory relative to the working directory, created if
+ * missing); save writes `<directory>/<filename>_<k>.vtu` and adds it to the
+ * collection at `timestep`. */
+typedef struct zg_pvd zg_pvd;
+int zg_pvd_open(zg_pvd **out, const char *filename, const char *directory);
+int zg_pvd_save(zg_pvd *pvd, zg_ctx *ctx, const zg_out_var *vars, int n_vars, double timestep);
+int zg_pvd_close(zg_pvd *pvd);
+
+/* ------------------------------------------------------------------------
  * Adjoint mode (no counterpart in the reference): the gradient of
  *   J = mean pressure over the cells whose centre lies in a probe box
  * after `steps` Heun steps at a fixed dt, with respect to the initial density

@@ -57,7 +57,7 @@ UNITS = [
 
 # Directories whose every translation unit joins the real-mesh checker, and
 # the units left out: solvers off this path.
-MESH_DIRS = ["zephyr/mesh", "zephyr/geom", "zephyr/math/cfd", "zephyr/math/solver", "zephyr/phys"]
+MESH_DIRS = ["zephyr/mesh", "zephyr/geom", "zephyr/math/cfd", "zephyr/math/solver", "zephyr/phys", "zephyr/io"]
 MESH_FILES = ["zephyr/utils/mpi.cpp", "zephyr/utils/threads.cpp", "zephyr/utils/json.cpp",
               "zephyr/utils/stopwatch.cpp", "zephyr/utils/numpy.cpp", "zephyr/math/funcs.cpp",
               "zephyr/math/random.cpp", "zephyr/math/sle/tridiagonal.cpp", "zephyr/math/calc/integrals.cpp"]

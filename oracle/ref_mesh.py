@@ -50,6 +50,11 @@ def lib():
         L.zm_check.restype = C.c_int
         L.zm_check_refined.argtypes = [C.c_void_p]
         L.zm_check_refined.restype = C.c_int
+        L.zm_vtu.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int]
+        L.zm_pvd_open.restype = C.c_void_p
+        L.zm_pvd_open.argtypes = [C.c_char_p, C.c_char_p]
+        L.zm_pvd_save.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_char_p, C.c_int]
+        L.zm_pvd_close.argtypes = [C.c_void_p]
         L.zm_threads(0)
         _lib = L
     return _lib
@@ -144,6 +149,10 @@ class RefEuMesh:
     def check_refined(self):
         return lib().zm_check_refined(self.h)
 
+    def write_vtu(self, filename, names=("level",), with_state=True):
+        """io::VtuFile::save with the named variables and the SmFluid state."""
+        lib().zm_vtu(self.h, str(filename).encode(), ",".join(names).encode(), int(with_state))
+
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
             _lib.zm_free(self.h)
@@ -156,3 +165,18 @@ def grad_of(mesh: "RefEuMesh"):
     gx, gy = np.empty(4 * n), np.empty(4 * n)
     lib().zm_grad(mesh.h, _dp(gx), _dp(gy))
     return gx.reshape(4, n), gy.reshape(4, n)
+
+
+class RefPvd:
+    """io::PvdFile(filename, directory) saving RefEuMesh instances."""
+
+    def __init__(self, filename, directory):
+        self.h = lib().zm_pvd_open(str(filename).encode(), str(directory).encode())
+
+    def save(self, mesh: RefEuMesh, timestep, names=("level",), with_state=True):
+        lib().zm_pvd_save(self.h, mesh.h, timestep, ",".join(names).encode(), int(with_state))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.zm_pvd_close(self.h)
+            self.h = None

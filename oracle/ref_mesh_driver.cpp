@@ -13,6 +13,8 @@
 #include <vector>
 
 #include <zephyr/geom/generator/rectangle.h>
+#include <zephyr/io/pvd_file.h>
+#include <zephyr/io/vtu_file.h>
 #include <zephyr/math/solver/sm_fluid.h>
 #include <zephyr/mesh/euler/eu_mesh.h>
 #include <zephyr/phys/matter/eos/ideal_gas.h>
@@ -214,5 +216,52 @@ int zm_check(void *p) { return static_cast<RefMesh *>(p)->mesh->check_base() < 0
 // EuMesh::check_refined (eu_mesh.cpp:681-): 0 when an adapted mesh is
 // consistent (hanging faces allowed).
 int zm_check_refined(void *p) { return static_cast<RefMesh *>(p)->mesh->check_refined() < 0 ? -1 : 0; }
+
+// ---- output (io/vtu_file.cpp, io/pvd_file.cpp) ----
+
+namespace {
+// Variables: the named ones of io/variable.cpp (comma-separated, may be
+// empty) and, with `with_state`, the SmFluid state as the single-fluid driver
+// writes it (smf_test_2D.cpp:95-99): density, vel.x, vel.y, pressure, energy.
+io::Variables out_variables(RefMesh *r, const char *names, int with_state) {
+    io::Variables vars;
+    std::string list(names ? names : "");
+    size_t pos = 0;
+    while (pos < list.size()) {
+        size_t comma = list.find(',', pos);
+        if (comma == std::string::npos) comma = list.size();
+        if (comma > pos) vars.append(list.substr(pos, comma - pos));
+        pos = comma + 1;
+    }
+    if (with_state) {
+        auto z = r->part.init;
+        vars += {"density", [z](EuCell &cell) -> double { return cell[z].density; }};
+        vars += {"vel.x", [z](EuCell &cell) -> double { return cell[z].velocity.x(); }};
+        vars += {"vel.y", [z](EuCell &cell) -> double { return cell[z].velocity.y(); }};
+        vars += {"pressure", [z](EuCell &cell) -> double { return cell[z].pressure; }};
+        vars += {"energy", [z](EuCell &cell) -> double { return cell[z].energy; }};
+    }
+    return vars;
+}
+}  // namespace
+
+// VtuFile::save of the mesh with the variables above.
+void zm_vtu(void *p, const char *filename, const char *names, int with_state) {
+    auto *r = static_cast<RefMesh *>(p);
+    io::VtuFile::save(filename, *r->mesh, out_variables(r, names, with_state));
+}
+
+// PvdFile(filename, directory); save(mesh, timestep) with the variables above.
+void *zm_pvd_open(const char *filename, const char *directory) {
+    auto *f = new io::PvdFile();
+    f->open(filename, directory);
+    return f;
+}
+void zm_pvd_save(void *pvd, void *p, double timestep, const char *names, int with_state) {
+    auto *f = static_cast<io::PvdFile *>(pvd);
+    f->variables = out_variables(static_cast<RefMesh *>(p), names, with_state);
+    f->save(*static_cast<RefMesh *>(p)->mesh, timestep);
+}
+void zm_pvd_close(void *pvd) { delete static_cast<io::PvdFile *>(pvd); }
 
 }  // extern "C"

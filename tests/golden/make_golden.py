@@ -240,6 +240,62 @@ def make_trs():
     print("wrote transfer cases")
 
 
+VTU_NAMES = ("level", "index", "center", "rank", "flag", "b_idx", "z_idx")
+
+
+def make_vtu():
+    """The reference's VtuFile::save and PvdFile on a rectangle and on a
+    refined mesh, with the named cell variables and the SmFluid state as the
+    single-fluid driver writes it (density, vel.x, vel.y, pressure, energy).
+    Stores the inputs (state, refine flags) and the files' bytes."""
+    import shutil
+    from oracle import ref_mesh as RME
+    tmp = OUT / "_vtu_tmp"
+    shutil.rmtree(tmp, ignore_errors=True)
+    tmp.mkdir()
+    rng = np.random.default_rng(21)
+    try:
+        # a rectangle with a random state, then a PVD series of two saves
+        nx, ny, box = 6, 4, (0.0, 1.0, 0.0, 0.5)
+        r = RME.RefEuMesh(nx, ny, box=box, bounds=(2, 1, 2, 1))
+        st = [1.0 + rng.random(nx * ny), rng.random(nx * ny) - 0.5, rng.random(nx * ny) - 0.5,
+              1.0 + rng.random(nx * ny), 2.5 + rng.random(nx * ny)]
+        r.set_state(*st)
+        r.write_vtu(tmp / "rect.vtu", names=VTU_NAMES, with_state=True)
+        pvd = RME.RefPvd("series", tmp / "out")
+        pvd.save(r, 0.0, names=("level",), with_state=True)
+        pvd.save(r, 0.125, names=("level",), with_state=True)
+        del pvd
+        np.savez_compressed(OUT / "vtu_rect_6x4.npz", nx=nx, ny=ny, box=np.array(box), bounds=np.array((2, 1, 2, 1)),
+                            state=np.array(st), names=np.array(VTU_NAMES),
+                            vtu=np.frombuffer((tmp / "rect.vtu").read_bytes(), np.uint8),
+                            pvd=np.frombuffer((tmp / "out" / "series.pvd").read_bytes(), np.uint8),
+                            pvd_vtu0=np.frombuffer((tmp / "out" / "series_0.vtu").read_bytes(), np.uint8),
+                            pvd_vtu1=np.frombuffer((tmp / "out" / "series_1.vtu").read_bytes(), np.uint8),
+                            timesteps=np.array([0.0, 0.125]))
+        # an adaptive rectangle after one refine (const distributor)
+        n = 8
+        a = RME.RefEuMesh(n, n, box=(0.0, 1.0, 0.0, 1.0), bounds=(2, 2, 2, 2), max_level=2, distributor="const")
+        st = [1.0 + rng.random(n * n), rng.random(n * n) - 0.5, rng.random(n * n) - 0.5,
+              1.0 + rng.random(n * n), 2.5 + rng.random(n * n)]
+        a.set_state(*st)
+        flags = np.zeros(n * n, np.int32)
+        flags[rng.random(n * n) < 0.3] = 1
+        a.put_flags(flags)
+        a.refine()
+        cells = a.cells()
+        mvx, mvy = a.verts()
+        a.write_vtu(tmp / "amr.vtu", names=VTU_NAMES, with_state=True)
+        np.savez_compressed(OUT / "vtu_amr_8_refined.npz", n=n, state=np.array(st), flags=flags, max_level=2,
+                            names=np.array(VTU_NAMES), map_x=mvx, map_y=mvy, level=cells["level"],
+                            flag=cells["flag"], b_idx=cells["b_idx"], z_idx=cells["z_idx"], cx=cells["cx"],
+                            cy=cells["cy"], state_after=np.array(a.state()),
+                            vtu=np.frombuffer((tmp / "amr.vtu").read_bytes(), np.uint8))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    print("wrote vtu cases")
+
+
 def make_mm_pointwise():
     """Mixture closure, sound speed, mixture HLLC and CRP fluxes of the
     reference on states taken from a running shock / water-column problem,
@@ -321,6 +377,7 @@ def main():
     print("wrote multi-material cases")
     make_amr_cycles()
     make_trs()
+    make_vtu()
 
 
 AMR_CYCLES = {
@@ -338,6 +395,8 @@ def make_amr_cycles():
 if __name__ == "__main__":
     if "--transfer" in sys.argv:
         make_trs()
+    elif "--vtu" in sys.argv:
+        make_vtu()
     elif "--amr-cycle" in sys.argv:
         make_amr_cycles()
     elif "--mm-split" in sys.argv:

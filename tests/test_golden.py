@@ -13,7 +13,7 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 LIM_ID = {"none": 0, "unit": 1, "minmod": 2, "MC": 3, "van Leer": 4, "van Albada 1": 5, "van Albada": 5,
           "van Albada 2": 6, "CHARM": 7, "HCUS": 8, "HQUICK": 9, "Koren": 10, "smart": 11, "superbee": 12}
 CASES = sorted(p.stem for p in GOLDEN.glob("*.npz")
-               if p.stem not in ("pointwise", "isolation_20_mc") and not p.stem.startswith(("amr_", "mm_", "adapt_", "tr_")))
+               if p.stem not in ("pointwise", "isolation_20_mc") and not p.stem.startswith(("amr_", "mm_", "adapt_", "tr_", "vtu_")))
 AMR_CASES = sorted(p.stem for p in GOLDEN.glob("amr_*.npz"))
 
 

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = sorted(p.stem for p in GOLDEN.glob("*.npz")
-               if p.stem not in ("pointwise", "isolation_20_mc") and not p.stem.startswith(("amr_", "mm_", "adapt_", "tr_")))
+               if p.stem not in ("pointwise", "isolation_20_mc") and not p.stem.startswith(("amr_", "mm_", "adapt_", "tr_", "vtu_")))
 AMR_CASES = sorted(p.stem for p in GOLDEN.glob("amr_*.npz"))
 
 

@@ -88,6 +88,11 @@ class TrParams(C.Structure):
     _fields_ = [("method", C.c_int), ("CFL", C.c_double), ("velocity", C.c_int), ("vel", C.c_double * 3)]
 
 
+class OutVar(C.Structure):
+    """zg_out_var"""
+    _fields_ = [("name", C.c_char_p), ("source", C.c_int), ("component", C.c_int), ("host", C.POINTER(C.c_double))]
+
+
 class AdjParams(C.Structure):
     """zg_adj_params"""
     _fields_ = [("gamma", C.c_double), ("dt", C.c_double), ("steps", C.c_int), ("checkpoint_every", C.c_int),
@@ -148,6 +153,10 @@ SIGNATURES = {
     "zg_tr_update": (C.c_int, [_V, C.c_int]),
     "zg_tr_advance": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, _P]),
     "zg_tr_set_flags": (C.c_int, [_V, _I]),
+    "zg_vtu_write": (C.c_int, [_V, C.c_char_p, C.POINTER(OutVar), C.c_int]),
+    "zg_pvd_open": (C.c_int, [C.POINTER(_V), C.c_char_p, C.c_char_p]),
+    "zg_pvd_save": (C.c_int, [_V, _V, C.POINTER(OutVar), C.c_int, C.c_double]),
+    "zg_pvd_close": (C.c_int, [_V]),
     "zg_adj_default_params": (None, [C.POINTER(AdjParams)]),
     "zg_adj_create": (C.c_int, [C.POINTER(_V), C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                 C.c_double]),

@@ -42,6 +42,7 @@ UNITS = {
     "amr_refine.cu": ["-fmad=false"],
     # scalar VOF transport: polygon clipping and sections bit-exact with the reference
     "tr_vof.cu": ["-fmad=false"],
+    "zg_vtu.cu": [],
     "smf_fast.cu": [],
     "smf_slot_fast.cu": [],
     "smf_slot_mixed.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],

@@ -7,7 +7,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <limits>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -18,6 +20,7 @@
 #include "smf_tiled_launch.h"
 #include "smf_types.h"
 #include "tr_types.h"
+#include "vtu_types.h"
 
 using namespace zg;
 
@@ -827,6 +830,7 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     ZG_CUDA(c, cudaMalloc(&c->d_state, nfields * n * sizeof(double)));
     ZG_CUDA(c, cudaMalloc(&c->d_wait, 2 * n * sizeof(int)));
     ZG_CUDA(c, cudaMalloc(&c->d_flags, n * sizeof(int)));
+    ZG_CUDA(c, cudaMemsetAsync(c->d_flags, 0, n * sizeof(int), c->stream));  // cells start unflagged
     ZG_CUDA(c, cudaMalloc(&c->d_dmin, 64));
     c->d_ticket = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dmin) + 8);
     c->d_dt = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_dmin) + 16);
@@ -1688,6 +1692,308 @@ int zg_tr_set_flags(zg_ctx *c, int *flags) {
     cudaFreeAsync(d, c->stream);
     if (e != cudaSuccess) return fail(c, ZG_ERR_CUDA, cudaGetErrorString(e));
     ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Output: VTU files and PVD series (io/vtu_file.cpp, io/pvd_file.cpp)
+
+struct zg_pvd {
+    std::string filename;  // PvdFile::m_filename (the DataSet file prefix)
+    std::string fullname;  // PvdFile::m_fullname (directory / filename)
+    std::vector<double> steps;
+};
+
+namespace {
+
+struct OutVar {
+    std::string name, type;
+    int comps = 1;
+    size_t elem = 8;  // bytes per component
+    int kind = -1;    // vtu::Kind, or -1: a Float64 array copied as is
+    const double *a = nullptr, *b = nullptr;  // device fields
+    const double *host = nullptr;
+};
+
+// The device state field of a source, or null with an error.
+int out_field(zg_ctx *c, const zg_out_var &v, OutVar &o) {
+    const int k = v.component;
+    if (v.source == ZG_OUT_SMF) {
+        if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_vtu_write: no SmFluid state (zg_smf_configure)");
+        int rc = materialize_prim(c);
+        if (rc != ZG_OK) return rc;
+        double *f[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
+        if (k < 0 || k > 4) return fail(c, ZG_ERR_ARG, "zg_vtu_write: SmFluid component 0..4");
+        o.a = f[k];
+        return ZG_OK;
+    }
+    if (v.source == ZG_OUT_MMF) {
+        if (!c->mm_configured) return fail(c, ZG_ERR_STATE, "zg_vtu_write: no MmFluid state (zg_mmf_configure)");
+        const mmf::MmField &z = c->mz;
+        double *f[6 + 2 * mmf::NMAT] = {z.rho, z.vx, z.vy, z.P, z.e, z.T};
+        for (int i = 0; i < mmf::NMAT; ++i) {
+            f[6 + i] = z.b[i];
+            f[6 + mmf::NMAT + i] = z.r[i];
+        }
+        if (k < 0 || k >= 6 + 2 * mmf::NMAT) return fail(c, ZG_ERR_ARG, "zg_vtu_write: MmFluid component out of range");
+        o.a = f[k];
+        return ZG_OK;
+    }
+    if (v.source == ZG_OUT_TR) {
+        if (!c->tr_configured) return fail(c, ZG_ERR_STATE, "zg_vtu_write: no Transfer state (zg_tr_configure)");
+        const tr::TrArgs &t = c->targs;
+        const int q = t.cur;
+        if (k == 5 || k == 6) {
+            o.kind = vtu::K_VEC3;
+            o.comps = 3;
+            o.a = k == 5 ? t.nx[q] : t.px[q];
+            o.b = k == 5 ? t.ny[q] : t.py[q];
+            return ZG_OK;
+        }
+        double *f[5] = {t.u, t.nx[q], t.ny[q], t.px[q], t.py[q]};
+        if (k < 0 || k > 4) return fail(c, ZG_ERR_ARG, "zg_vtu_write: Transfer component 0..6");
+        o.a = f[k];
+        return ZG_OK;
+    }
+    return fail(c, ZG_ERR_ARG, "zg_vtu_write: unknown variable source");
+}
+
+int out_vars(zg_ctx *c, const zg_out_var *vars, int n_vars, std::vector<OutVar> &out) {
+    if (n_vars < 0 || (n_vars > 0 && !vars)) return fail(c, ZG_ERR_ARG, "zg_vtu_write: bad variable list");
+    for (int i = 0; i < n_vars; ++i) {
+        const zg_out_var &v = vars[i];
+        if (!v.name) return fail(c, ZG_ERR_ARG, "zg_vtu_write: variable without a name");
+        OutVar o;
+        o.name = v.name;
+        o.type = "Float64";
+        // io::Variable's named variables: types and sizes of io/variable.cpp
+        switch (v.source) {
+            case ZG_OUT_LEVEL: o.kind = vtu::K_LEVEL; o.type = "Int8"; o.elem = 1; break;
+            case ZG_OUT_INDEX: o.kind = vtu::K_INDEX; o.type = "Int32"; o.elem = 4; break;
+            case ZG_OUT_RANK: o.kind = vtu::K_RANK; o.type = "Int32"; o.elem = 4; break;
+            case ZG_OUT_FLAG: o.kind = vtu::K_FLAG; o.type = "Int8"; o.elem = 1; break;
+            case ZG_OUT_B_IDX: o.kind = vtu::K_BIDX; o.type = "Int32"; o.elem = 4; break;
+            case ZG_OUT_Z_IDX: o.kind = vtu::K_ZIDX; o.type = "Int32"; o.elem = 4; break;
+            case ZG_OUT_CENTER: o.kind = vtu::K_CENTER; o.type = "Float32"; o.elem = 4; o.comps = 3; break;
+            case ZG_OUT_HOST:
+                if (!v.host) return fail(c, ZG_ERR_ARG, "zg_vtu_write: ZG_OUT_HOST without an array");
+                o.host = v.host;
+                break;
+            default: {
+                int rc = out_field(c, v, o);
+                if (rc != ZG_OK) return rc;
+            }
+        }
+        out.push_back(o);
+    }
+    return ZG_OK;
+}
+
+// VtuStructure::write_header + write_primitives + write_cells_data
+// (vtu_file.cpp:439-530) for quadrilateral cells: the header text, then the
+// appended arrays, each behind its uint32 byte count, packed on the device.
+int vtu_write(zg_ctx *c, const std::string &filename, const zg_out_var *vars, int n_vars) {
+    if (!c->have_mesh || (c->slots && !c->amr))
+        return fail(c, ZG_ERR_STATE, "zg_vtu_write: needs a zg_mesh_rectangle mesh (adaptive or not)");
+    DeviceGuard g(c->device);
+    std::vector<OutVar> vs;
+    int rc = out_vars(c, vars, n_vars, vs);
+    if (rc != ZG_OK) return rc;
+    const size_t n = (size_t)c->n, np = 4 * n;
+    if (np > 0xFFFFFFFFull / 24) return fail(c, ZG_ERR_ARG, "zg_vtu_write: mesh too large for 32-bit VTU offsets");
+
+    vtu::MeshSrc m{};
+    m.n = (int)n;
+    if (c->amr) {
+        m.kind = 1;
+        m.mvx = c->av.vx;
+        m.mvy = c->av.vy;
+        m.cx = c->av.cx;
+        m.cy = c->av.cy;
+        m.level = c->av.level;
+        m.b_idx = c->av.b_idx;
+        m.z_idx = c->av.z_idx;
+        m.flag = c->av.flag;
+    } else {
+        m.kind = 0;
+        m.ny = c->mesh.ny;
+        m.X = c->mesh.X;
+        m.Y = c->mesh.Y;
+        m.cxt = c->mesh.cx;
+        m.cyt = c->mesh.cy;
+        m.flag = c->configured ? c->d_flags : nullptr;
+    }
+
+    // header (byte offsets count each array's uint32 size field)
+    std::ostringstream h;
+    h << "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n";
+    h << "  <UnstructuredGrid>\n";
+    h << "    <Piece NumberOfPoints=\"" << np << "\" NumberOfCells=\"" << n << "\">\n";
+    uint64_t off = 0;
+    h << "      <Points>\n";
+    h << "        <DataArray type=\"Float64\" Name=\"Points\" NumberOfComponents=\"3\" format=\"appended\" offset=\""
+      << off << "\"/>\n";
+    h << "      </Points>\n";
+    const size_t b_pts = 24 * np, b_conn = 4 * np, b_off = 4 * n, b_types = n;
+    off += 4 + b_pts;
+    h << "      <Cells>\n";
+    h << "        <DataArray type=\"UInt32\" Name=\"connectivity\" format=\"appended\" offset=\"" << off << "\"/>\n";
+    off += 4 + b_conn;
+    h << "        <DataArray type=\"UInt32\" Name=\"offsets\" format=\"appended\" offset=\"" << off << "\"/>\n";
+    off += 4 + b_off;
+    h << "        <DataArray type=\"UInt8\" Name=\"types\" format=\"appended\" offset=\"" << off << "\"/>\n";
+    off += 4 + b_types;
+    h << "      </Cells>\n";
+    h << "      <CellData>\n";
+    for (const OutVar &v : vs) {
+        h << "        <DataArray type=\"" << v.type << "\" Name=\"" << v.name;
+        if (v.comps >= 2) h << "\" NumberOfComponents=\"" << v.comps;
+        h << "\" format=\"appended\" offset=\"" << off << "\"/>\n";
+        off += 4 + n * v.comps * v.elem;
+    }
+    h << "      </CellData>\n";
+    h << "    </Piece>\n";
+    h << "  </UnstructuredGrid>\n";
+    h << "  <AppendedData encoding=\"raw\">\n";
+    h << "_";
+    if (off > 0xFFFFFFFFull) return fail(c, ZG_ERR_ARG, "zg_vtu_write: file too large for 32-bit VTU offsets");
+    const std::string head = h.str();
+
+    // appended data: the device packs each array, one copy each into a
+    // pinned host image of the file's tail
+    std::vector<size_t> sizes = {b_pts, b_conn, b_off, b_types};
+    for (const OutVar &v : vs) sizes.push_back(n * v.comps * v.elem);
+    size_t total = 0, dev_total = 0;
+    for (size_t sz : sizes) {
+        total += 4 + sz;
+        dev_total += (sz + 255) / 256 * 256;
+    }
+    unsigned char *img = nullptr, *dev = nullptr;
+    ZG_CUDA(c, cudaMallocHost(&img, total));
+    cudaError_t e = cudaMallocAsync(&dev, dev_total, c->stream);
+    if (e != cudaSuccess) {
+        cudaFreeHost(img);
+        return cuda_fail(c, e, "zg_vtu_write: device scratch");
+    }
+    std::vector<unsigned char *> dsec;
+    size_t doff = 0;
+    for (size_t sz : sizes) {
+        dsec.push_back(dev + doff);
+        doff += (sz + 255) / 256 * 256;
+    }
+    vtu::launch_points(m, reinterpret_cast<double *>(dsec[0]), c->stream);
+    vtu::launch_cells((int)n, reinterpret_cast<uint32_t *>(dsec[1]), reinterpret_cast<uint32_t *>(dsec[2]), dsec[3],
+                      c->stream);
+    c->launches += 2;
+    size_t hoff = 0;
+    for (size_t k = 0; k < sizes.size(); ++k) {
+        const uint32_t sz32 = (uint32_t)sizes[k];
+        std::memcpy(img + hoff, &sz32, 4);
+        hoff += 4;
+        const unsigned char *src = dsec[k];
+        if (k >= 4) {
+            const OutVar &v = vs[k - 4];
+            if (v.host) {
+                std::memcpy(img + hoff, v.host, sizes[k]);
+                src = nullptr;
+            } else if (v.kind < 0) {
+                src = reinterpret_cast<const unsigned char *>(v.a);  // a Float64 field: straight from the state
+            } else {
+                vtu::launch_var(m, v.kind, v.a, v.b, dsec[k], c->stream);
+                ++c->launches;
+            }
+        }
+        if (src && sizes[k]) {
+            e = cudaMemcpyAsync(img + hoff, src, sizes[k], cudaMemcpyDeviceToHost, c->stream);
+            if (e != cudaSuccess) break;
+        }
+        hoff += sizes[k];
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFreeAsync(dev, c->stream);
+    if (e != cudaSuccess) {
+        cudaFreeHost(img);
+        return cuda_fail(c, e, "zg_vtu_write: packing");
+    }
+    // create_directories (vtk_type.cpp:13-22), then the file
+    std::error_code ec;
+    const std::filesystem::path path(filename);
+    if (path.has_parent_path()) std::filesystem::create_directories(path.parent_path(), ec);
+    FILE *f = std::fopen(filename.c_str(), "wb");
+    if (!f) {
+        cudaFreeHost(img);
+        return fail(c, ZG_ERR_ARG, "zg_vtu_write: cannot open '" + filename + "'");
+    }
+    const bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size() &&
+                    std::fwrite(img, 1, total, f) == total;
+    std::fclose(f);
+    cudaFreeHost(img);
+    if (!ok) return fail(c, ZG_ERR_ARG, "zg_vtu_write: short write to '" + filename + "'");
+    return ZG_OK;
+}
+
+// The collection file (pvd_file.cpp:150-211): the datasets saved so far.
+bool pvd_rewrite(const zg_pvd *p) {
+    FILE *f = std::fopen((p->fullname + ".pvd").c_str(), "wb");
+    if (!f) return false;
+    std::fputs("<?xml version=\"1.0\"?>\n", f);
+    std::fputs("<VTKFile type=\"Collection\" version=\"0.1\" byte_order=\"LittleEndian\">\n", f);
+    std::fputs("    <Collection>\n", f);
+    for (size_t k = 0; k < p->steps.size(); ++k)
+        std::fprintf(f, "        <DataSet timestep=\"%.15e\" part=\"0\" file=\"%s_%zu.vtu\"/>\n", p->steps[k],
+                     p->filename.c_str(), k);
+    std::fputs("    </Collection>\n", f);
+    std::fputs("</VTKFile>\n", f);
+    return std::fclose(f) == 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zg_vtu_write(zg_ctx *c, const char *filename, const zg_out_var *vars, int n_vars) {
+    if (!c || !filename) return ZG_ERR_ARG;
+    return vtu_write(c, filename, vars, n_vars);
+}
+
+int zg_pvd_open(zg_pvd **out, const char *filename, const char *directory) {
+    if (!out || !filename) return ZG_ERR_ARG;
+    namespace fs = std::filesystem;
+    std::error_code ec;
+    // PvdFile::open (pvd_file.cpp:89-148)
+    fs::path dir = fs::current_path(ec);
+    if (directory && *directory) {
+        fs::path d = directory;
+        dir = d.is_relative() ? dir / d : d;
+    }
+    if (!fs::exists(dir, ec) || !fs::is_directory(dir, ec)) fs::create_directories(dir, ec);
+    auto *p = new zg_pvd();
+    std::string name = filename;
+    p->filename = name;
+    if (name.size() > 4 && name.substr(name.size() - 4) == ".pvd") p->filename = name.substr(name.size() - 4);
+    p->fullname = (dir / name).string();
+    if (!pvd_rewrite(p)) {
+        delete p;
+        return ZG_ERR_ARG;
+    }
+    *out = p;
+    return ZG_OK;
+}
+
+int zg_pvd_save(zg_pvd *p, zg_ctx *c, const zg_out_var *vars, int n_vars, double timestep) {
+    if (!p || !c) return ZG_ERR_ARG;
+    const std::string vtu = p->fullname + "_" + std::to_string(p->steps.size()) + ".vtu";
+    int rc = vtu_write(c, vtu, vars, n_vars);
+    if (rc != ZG_OK) return rc;
+    p->steps.push_back(timestep);
+    if (!pvd_rewrite(p)) return fail(c, ZG_ERR_ARG, "zg_pvd_save: cannot write '" + p->fullname + ".pvd'");
+    return ZG_OK;
+}
+
+int zg_pvd_close(zg_pvd *p) {
+    delete p;
     return ZG_OK;
 }
 
