@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--scheme", choices=["pc", "heun"], default="pc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids: one section alone on a smaller case (not the bench line)
-    ap.add_argument("--only", choices=["amr", "mm", "adjoint", "transfer"], default=None,
+    ap.add_argument("--only", choices=["amr", "mm", "adjoint", "transfer", "vtu"], default=None,
                     help="run one section alone and print its JSON (for ncu captures)")
     ap.add_argument("--amr-base", type=int, default=0, help="AMR base cells per side (default 512)")
     ap.add_argument("--tr-nx", type=int, default=0, help="transport mesh cells along x (default 4096)")
@@ -694,6 +694,58 @@ def transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cp
     return out
 
 
+VTU_SIZE = 1024   # output: cells per side of the mesh written
+
+
+def vtu_variant(torch, local_rank, stream, want_cpu):
+    """VTU output (zg_vtu_write) of a 1024^2 mesh with the level and the five
+    SmFluid state fields as the single-fluid driver writes them: time of the
+    whole call (device packing, copies, file write) into a temporary
+    directory, and the reference's VtuFile::save (oracle/_ref) on the same
+    mesh and values."""
+    import tempfile
+    import zephyr_b200 as Z
+    from zephyr_b200.io import Variables, VtuFile
+    from zephyr_b200.workloads import fourier_smooth
+    w = fourier_smooth(VTU_SIZE)
+    gen = Z.Rectangle(0.0, 1.0, 0.0, 1.0)  # ZOE walls: the reference's adaptive EuMesh rejects periodic axes
+    gen.set_sizes(VTU_SIZE, VTU_SIZE)
+    mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
+    solver = Z.SmFluid(w.eos)
+    solver.add_types(mesh)
+    mesh.set_state(*w.state)
+    names = ("density", "vel.x", "vel.y", "pressure", "energy")
+    v = Variables(["level"])
+    for k, nm in enumerate(names):
+        v.append(nm, ("smf", k))
+    out = {"workload": f"fourier_smooth {VTU_SIZE}x{VTU_SIZE}: level + 5 FP64 state fields, quadrilateral cells"}
+    with tempfile.TemporaryDirectory() as d:
+        f = Path(d) / "out.vtu"
+        times = []
+        for _ in range(4):
+            t0 = time.perf_counter()
+            VtuFile.save(f, mesh, v)
+            times.append(time.perf_counter() - t0)
+        size = f.stat().st_size
+        ms = 1e3 * statistics.median(times[1:])
+        out.update(ms=ms, bytes=size, GBs=size / (ms / 1e3) / 1e9, gpu_launches=4 * (2 + 1))
+        if want_cpu:
+            from oracle import ref_mesh as RME
+            if RME.available():
+                n = VTU_SIZE
+                r = RME.RefEuMesh(n, n, bounds=(2, 2, 2, 2))
+                r.set_state(*w.state)
+                t0 = time.perf_counter()
+                r.write_vtu(Path(d) / "ref.vtu", names=("level",), with_state=True)
+                ref_s = time.perf_counter() - t0
+                same = (Path(d) / "ref.vtu").read_bytes() == f.read_bytes()
+                out["cpu_baseline"] = {"ms": 1e3 * ref_s, "kind": "reference", "cores": 1,
+                                       "sample": "one VtuFile::save of the same mesh and values (oracle/_ref)",
+                                       "same_bytes": same}
+    mesh.close()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import zephyr_b200 as Z
@@ -720,6 +772,8 @@ def run_ours(args, rank, world, local_rank):
             out = amr_variant(torch, lib, dev, stream, local_rank, want_cpu=False, kernels_name=args.amr_kernels,
                               criterion=args.amr_criterion)
             out.pop("final")
+        elif args.only == "vtu":
+            out = vtu_variant(torch, local_rank, stream, want_cpu=True)
         elif args.only == "transfer":
             out = transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False, nx=args.tr_nx)
         elif args.only == "mm":
@@ -795,6 +849,7 @@ def run_ours(args, rank, world, local_rank):
     adjv = adjoint_variant(torch, dev, stream, local_rank)
     trv = transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
                            want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
+    vtuv = vtu_variant(torch, local_rank, stream, want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     # the benchmark's criterion (|grad rho| h / rho) for the FP64 FAST and
     # MIXED forms; the reference's own set_flags for the bit-exact form
     amr = amr_variant(torch, lib, dev, stream, local_rank,
@@ -846,7 +901,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
                             mm["launches"] + mm_mx["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
-                            amr_par["gpu_launches"] + amr_mx["gpu_launches"] + trv["launches"]),
+                            amr_par["gpu_launches"] + amr_mx["gpu_launches"] + trv["launches"] +
+                            vtuv["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 5 * 8 * cells,
                 "d2h_bytes_per_step": 5 * 8 * cells, "steps": e2e_steps,
@@ -879,6 +935,7 @@ def run_ours(args, rank, world, local_rank):
                 **mm_err, "err_after_steps": W + K, "kernels": mm_mx["kernels"],
                 "gpu_launches": int(mm_mx["launches"])},
             "adjoint": adjv,
+            "vtu_write": vtuv,
             "transfer": {
                 "value": world * trv["cells"] * K / (ms_tr / 1e3), "unit": METRIC, "ms_per_step": ms_tr / K,
                 "workload": trv["workload"], "form": trv["form"], "steps": K, "warmup": W,

@@ -98,6 +98,10 @@ struct zg_ctx {
     double *d_tr = nullptr;  // u1, n and p (two buffers), face fluxes, then 8 scalar slots
     tr::TrArgs targs{};
 
+    // output: pinned host image of a VTU file's appended data (grown on demand)
+    unsigned char *out_img = nullptr;
+    size_t out_img_size = 0;
+
     // per-kernel timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -601,6 +605,7 @@ int zg_destroy(zg_ctx *c) {
         free_solver(c);
         free_mesh(c);
         for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+        if (c->out_img) cudaFreeHost(c->out_img);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
     }
     delete c;
@@ -1870,13 +1875,16 @@ int vtu_write(zg_ctx *c, const std::string &filename, const zg_out_var *vars, in
         total += 4 + sz;
         dev_total += (sz + 255) / 256 * 256;
     }
-    unsigned char *img = nullptr, *dev = nullptr;
-    ZG_CUDA(c, cudaMallocHost(&img, total));
-    cudaError_t e = cudaMallocAsync(&dev, dev_total, c->stream);
-    if (e != cudaSuccess) {
-        cudaFreeHost(img);
-        return cuda_fail(c, e, "zg_vtu_write: device scratch");
+    if (c->out_img_size < total) {
+        if (c->out_img) cudaFreeHost(c->out_img);
+        c->out_img = nullptr;
+        c->out_img_size = 0;
+        ZG_CUDA(c, cudaMallocHost(&c->out_img, total));
+        c->out_img_size = total;
     }
+    unsigned char *img = c->out_img, *dev = nullptr;
+    cudaError_t e = cudaMallocAsync(&dev, dev_total, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "zg_vtu_write: device scratch");
     std::vector<unsigned char *> dsec;
     size_t doff = 0;
     for (size_t sz : sizes) {
@@ -1913,23 +1921,16 @@ int vtu_write(zg_ctx *c, const std::string &filename, const zg_out_var *vars, in
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFreeAsync(dev, c->stream);
-    if (e != cudaSuccess) {
-        cudaFreeHost(img);
-        return cuda_fail(c, e, "zg_vtu_write: packing");
-    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "zg_vtu_write: packing");
     // create_directories (vtk_type.cpp:13-22), then the file
     std::error_code ec;
     const std::filesystem::path path(filename);
     if (path.has_parent_path()) std::filesystem::create_directories(path.parent_path(), ec);
     FILE *f = std::fopen(filename.c_str(), "wb");
-    if (!f) {
-        cudaFreeHost(img);
-        return fail(c, ZG_ERR_ARG, "zg_vtu_write: cannot open '" + filename + "'");
-    }
+    if (!f) return fail(c, ZG_ERR_ARG, "zg_vtu_write: cannot open '" + filename + "'");
     const bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size() &&
                     std::fwrite(img, 1, total, f) == total;
     std::fclose(f);
-    cudaFreeHost(img);
     if (!ok) return fail(c, ZG_ERR_ARG, "zg_vtu_write: short write to '" + filename + "'");
     return ZG_OK;
 }
