@@ -351,8 +351,11 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, pre
 AMR_BASE = 512         # quadtree AMR blast: base mesh cells per side
 AMR_LEVELS = 3         # refinement levels above the base
 AMR_CAPACITY = 8 << 20  # device room for cells (live + those held during a refine)
-AMR_WARM_STEPS = 100   # untimed steps (adapting every AMR_EVERY) before the timed window
-AMR_TIMED_STEPS = 400  # steps 100 to 500
+# untimed steps (adapting every AMR_EVERY) before the timed window: by step
+# 7000 the gradient criterion holds 1.1-1.2 M live cells (the 1-3 M window of
+# the configuration; steps 100-500 have about 0.3 M)
+AMR_WARM_STEPS = 7000
+AMR_TIMED_STEPS = 400  # steps 7000 to 7400
 AMR_EVERY = 10         # set_flags + refine every AMR_EVERY steps
 AMR_B_ALG = 160 + 36   # bytes per cell-update: the FP64 two-stage step plus the slot-mesh neighbour indices
 AMR_CELL_BYTES = 600   # bytes of one cell's AmrCells arrays (63 doubles, 22 ints, 16 bytes)
@@ -418,11 +421,12 @@ def amr_cpu_reference(budget_s=12.0):
 
 
 def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None, criterion="reference"):
-    """The quadtree AMR blast: base 512^2, 3 levels, the reference's
-    SmFluid::set_flags criterion and slope distributor, adaptation every 10
-    steps; the FP64 step on the slot mesh with the FAST kernels (derived face
-    geometry) or the PARITY kernels (bit-exact with the reference).  Times
-    steps 100-500 including every set_flags + refine."""
+    """The quadtree AMR blast: base 512^2, 3 levels, the benchmark's
+    |grad rho| h / rho criterion or the reference's SmFluid::set_flags, slope
+    distributor, adaptation every 10 steps; the FP64 step on the slot mesh
+    with the FAST kernels (derived face geometry), the MIXED kernels, or the
+    PARITY kernels (bit-exact with the reference).  Times steps 7000-7400
+    including every set_flags + refine."""
     import zephyr_b200 as Z
     from zephyr_b200._lib import KERNEL_KINDS
     from zephyr_b200.workloads import blast_cell_means
