@@ -45,7 +45,10 @@ enum zg_boundary {
 };
 
 /* Numerical fluxes; values of zephyr's `enum class Fluxes`
- * (math/cfd/flux/num_flux.h:11-21).  HLL and HLLC are implemented. */
+ * (math/cfd/flux/num_flux.h:11-21).  GODUNOV (the exact Riemann solver of
+ * math/solver/riemann.cpp; its rarefaction powers use CUDA's pow, so it
+ * agrees with the reference to a few ulps rather than bit for bit),
+ * RUSANOV, HLL and HLLC are implemented. */
 enum zg_flux {
     ZG_FLUX_GODUNOV = 0,
     ZG_FLUX_RUSANOV = 1,

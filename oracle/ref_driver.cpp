@@ -21,6 +21,7 @@
 #include <zephyr/geom/primitives/quad.h>
 #include <zephyr/math/cfd/flux/hll.h>
 #include <zephyr/math/cfd/flux/hllc.h>
+#include <zephyr/math/cfd/flux/num_flux.h>
 #include <zephyr/math/cfd/limiter.h>
 #include <zephyr/math/solver/sm_fluid.h>
 #include <zephyr/phys/matter/eos/ideal_gas.h>
@@ -211,8 +212,8 @@ void zr_flux(int kind, const double *zL, const double *zR, int eos_kind, double 
     auto eos = make_eos(eos_kind, gamma, P0, e0);
     PState L(zL[0], Vector3d(zL[1], zL[2], zL[3]), zL[4], zL[5]);
     PState R(zR[0], Vector3d(zR[1], zR[2], zR[3]), zR[4], zR[5]);
-    math::smf::Flux F = kind == int(math::Fluxes::HLL) ? math::HLL::calc_flux(L, R, *eos)
-                                                       : math::HLLC::calc_flux(L, R, *eos);
+    // NumFlux::create (num_flux.cpp:6-40): GODUNOV, RUSANOV, HLL, HLLC, ...
+    math::smf::Flux F = math::NumFlux::create(math::Fluxes(kind))->flux(L, R, *eos);
     out[0] = F.density;
     out[1] = F.momentum.x();
     out[2] = F.momentum.y();

@@ -237,8 +237,213 @@ static QState hll(const PState &zL, const PState &zR, const Eos &eos) {
     return F;
 }
 
+// zephyr/math/cfd/flux/rusanov.cpp:15-43  Rusanov::calc_flux (smf)
+static QState rusanov(const PState &zL, const PState &zR, const Eos &eos) {
+    const double u_L = zL.velocity.x;
+    const double u_R = zR.velocity.x;
+    double c_L = eos.sound_speed_rP(zL.density, zL.pressure);
+    double c_R = eos.sound_speed_rP(zR.density, zR.pressure);
+    // std::min / std::max of an initializer list: the first extreme element
+    double S_L = u_L - c_L, S_R = u_L + c_L;
+    if (u_R - c_R < S_L) S_L = u_R - c_R;
+    if (0.0 < S_L) S_L = 0.0;
+    if (S_R < u_R + c_R) S_R = u_R + c_R;
+    if (S_R < 0.0) S_R = 0.0;
+    double S = std::max(std::abs(S_L), S_R);
+    QState Q_L = q_from_p(zL), Q_R = q_from_p(zR);
+    QState F_L = flux_from_p(zL), F_R = flux_from_p(zR);
+    const double *fl = &F_L.density, *fr = &F_R.density, *ql = &Q_L.density, *qr = &Q_R.density;
+    QState F;
+    double *f = &F.density;
+    for (int i = 0; i < 5; ++i) f[i] = 0.5 * (fl[i] + fr[i]) + 0.5 * S * (ql[i] - qr[i]);
+    return F;
+}
+
+// ---------------------------------------------------------------------------
+// Exact Riemann solver for two stiffened gases, zephyr/math/solver/riemann.cpp
+namespace riemann {
+
+static inline double sq(double x) { return x * x; }  // riemann.cpp:12-14
+
+static inline double eos_sound(double rho, double p, double g, double p0) {  // :17-19
+    return std::sqrt(g * (p + p0) / rho);
+}
+static inline double eos_density(double p, double c, double g, double p0) {  // :22-24
+    return g * (p + p0) / sq(c);
+}
+// acoustic initial guess (:32-45); the two-shock and two-rarefaction guesses
+// of :47-61 are the same formula
+static inline double p_init(double rL, double uL, double pL, double cL, double p0L, double rR, double uR, double pR,
+                            double cR, double p0R) {
+    double rcL = rL * cL, rcR = rR * cR;
+    double P = (pL * rcR + pR * rcL + (uL - uR) * rcL * rcR) / (rcL + rcR);
+    double Pmin = -std::min(p0L, p0R) + 1.0e-2 * std::min(pL + p0L, pR + p0R);
+    return std::max(Pmin, P);
+}
+static inline double fK(double P, double rK, double pK, double cK, double gK, double p0K, double AK, double BK,
+                        double GK) {  // :76-84
+    if (P >= pK) return (P - pK) * std::sqrt(AK / (P + BK));
+    return 2.0 * cK / (gK - 1.0) * (std::pow((P + p0K) / (pK + p0K), GK) - 1.0);
+}
+static inline double dfK(double P, double rK, double pK, double cK, double gK, double p0K, double AK, double BK,
+                         double GK) {  // :86-94
+    if (P >= pK) return (1.0 - (P - pK) / (2.0 * (P + BK))) * std::sqrt(AK / (P + BK));
+    return std::pow((P + p0K) / (pK + p0K), GK - 1.0) / (rK * cK);
+}
+
+struct Sol {
+    double rho, Uf, Pf, U, P;
+    bool conv, vacuum, failed;
+};
+
+// contact_p (:118-236): Newton for the contact pressure and velocity
+static void contact(double rL, double uL, double pL, double cL, double gL, double p0L, double rR, double uR,
+                    double pR, double cR, double gR, double p0R, double &P_out, double &U_out, bool &conv,
+                    bool &vacuum, bool &failed) {
+    double AL = 2.0 / ((gL + 1) * rL), AR = 2.0 / ((gR + 1) * rR);
+    double BL = (gL - 1.0) * pL / (gL + 1.0) + 2.0 * gL * p0L / (gL + 1.0);
+    double BR = (gR - 1.0) * pR / (gR + 1.0) + 2.0 * gR * p0R / (gR + 1.0);
+    double GL = (gL - 1.0) / (2.0 * gL), GR = (gR - 1.0) / (2.0 * gR);
+    double p_dno = std::max(-p0L, -p0R);
+    double p_min = std::min(pL, pR);
+    double p_max = std::max(pL, pR);
+    vacuum = failed = false;
+    double f_dno = fK(p_dno, rL, pL, cL, gL, p0L, AL, BL, GL) + fK(p_dno, rR, pR, cR, gR, p0R, AR, BR, GR) + uR - uL;
+    if (f_dno > 0.0) {
+        vacuum = true;
+        P_out = p_dno;
+        U_out = 0.0;
+        conv = true;
+        return;
+    }
+    double P = 0.5 * (pL + pR);
+    double f_min = fK(p_min, rL, pL, cL, gL, p0L, AL, BL, GL) + fK(p_min, rR, pR, cR, gR, p0R, AR, BR, GR) + uR - uL;
+    if (f_min > 0.0) {
+        P = p_init(rL, uL, pL, cL, p0L, rR, uR, pR, cR, p0R);
+    } else {
+        double f_max = fK(p_max, rL, pL, cL, gL, p0L, AL, BL, GL) + fK(p_max, rR, pR, cR, gR, p0R, AR, BR, GR) + uR -
+                       uL;
+        P = p_init(rL, uL, pL, cL, p0L, rR, uR, pR, cR, p0R);
+        (void)f_max;
+    }
+    const int max_iterations = 50;
+    double DP1 = 1.0e-5 * std::abs(pL - pR);
+    double DP2 = 1.0e-12 * std::abs(std::max(pL + p0L, pR + p0R));
+    double DP = std::max(DP1, DP2);
+    double fL = 0.0, fR = 0.0, dfL, dfR, Pn = P;
+    int counter = 0;
+    for (; counter < max_iterations; ++counter) {
+        fL = fK(P, rL, pL, cL, gL, p0L, AL, BL, GL);
+        fR = fK(P, rR, pR, cR, gR, p0R, AR, BR, GR);
+        dfL = dfK(P, rL, pL, cL, gL, p0L, AL, BL, GL);
+        dfR = dfK(P, rR, pR, cR, gR, p0R, AR, BR, GR);
+        Pn = P - (fL + fR + uR - uL) / (dfL + dfR);
+        if (Pn < p_dno) Pn = (p_dno + P) / 2;
+        if (std::abs(Pn - P) < DP) {
+            if (counter > 3) break;
+        }
+        P = Pn;
+    }
+    conv = counter < max_iterations;
+    // the reference throws when a non-converged solve is far off (:224-230)
+    if (!conv && std::abs((P - Pn) / (P + Pn)) > 0.02) failed = true;
+    P_out = P;
+    U_out = 0.5 * (uL + uR + fR - fL);
+}
+
+// RiemannSolver::solve (:366-460): the state on the face x / t = 0
+static Sol solve(double rL, double uL, double pL, double gL, double p0L, double rR, double uR, double pR, double gR,
+                 double p0R) {
+    double cL = eos_sound(rL, pL, gL, p0L);
+    double cR = eos_sound(rR, pR, gR, p0R);
+    Sol s{};
+    double P, U;
+    contact(rL, uL, pL, cL, gL, p0L, rR, uR, pR, cR, gR, p0R, P, U, s.conv, s.vacuum, s.failed);
+    s.U = U;
+    s.P = P;
+    auto set = [&s](double rho, double Uf, double Pf) {
+        s.rho = rho;
+        s.Uf = Uf;
+        s.Pf = Pf;
+    };
+    if (U > 0.0) {
+        if (pL < P) {
+            double D = uL + (P - pL) / (rL * (U - uL));  // shock_wave_speed (:239-241)
+            if (D > 0.0) set(rL, uL, pL);
+            else set(rL * (P - pL) / ((P - pL) - rL * sq(U - uL)), U, P);  // shock_wave_density (:246-248)
+        } else {
+            double DL1 = uL - cL;
+            if (DL1 > 0.0) {
+                set(rL, uL, pL);
+            } else {
+                double cl = cL + 0.5 * (gL - 1.0) * (uL - U);  // rarefaction_sound_L (:254-256)
+                double DL2 = U - cl;
+                if (DL2 < 0.0) {
+                    set(eos_density(P, cl, gL, p0L), U, P);
+                } else {
+                    // the fan on the face, xi = 0 (:280-308)
+                    double base = 2.0 / (gL + 1.0) + ((gL - 1.0) * (uL - 0.0)) / ((gL + 1.0) * cL);
+                    set(rL * std::pow(base, 2.0 / (gL - 1.0)), ((gL - 1.0) * uL + 2.0 * (cL + 0.0)) / (gL + 1.0),
+                        (pL + p0L) * std::pow(base, 2.0 * gL / (gL - 1.0)) - p0L);
+                }
+            }
+        }
+    } else {
+        if (P > pR) {
+            double D = uR + (P - pR) / (rR * (U - uR));
+            if (D < 0.0) set(rR, uR, pR);
+            else set(rR * (P - pR) / ((P - pR) - rR * sq(U - uR)), U, P);
+        } else {
+            double DR2 = uR + cR;
+            if (DR2 < 0.0) {
+                set(rR, uR, pR);
+            } else {
+                double cr = cR - 0.5 * (gR - 1.0) * (uR - U);  // rarefaction_sound_R (:262-264)
+                double DR1 = U + cr;
+                if (DR1 > 0.0) {
+                    set(eos_density(P, cr, gR, p0R), U, P);
+                } else {
+                    double base = 2.0 / (gR + 1.0) - ((gR - 1.0) * (uR - 0.0)) / ((gR + 1.0) * cR);
+                    set(rR * std::pow(base, 2.0 / (gR - 1.0)), ((gR - 1.0) * uR + 2.0 * (0.0 - cR)) / (gR + 1.0),
+                        (pR + p0R) * std::pow(base, 2.0 * gR / (gR - 1.0)) - p0R);
+                }
+            }
+        }
+    }
+    return s;
+}
+
+}  // namespace riemann
+
+// IdealGas::stiffened_gas (ideal_gas.cpp:98-100) and StiffenedGas::
+// stiffened_gas (stiffened_gas.cpp:169-171): the gas's own gamma and P0.
+static inline void local_stiffened(const Eos &eos, double, double, double &g, double &P0) {
+    g = eos.gamma;
+    P0 = eos.kind == EOS_IDEAL ? 0.0 : eos.P0;
+}
+
+// zephyr/math/cfd/flux/godunov.cpp:16-32  Godunov::calc_flux (smf)
+static QState godunov(const PState &zL, const PState &zR, const Eos &eos) {
+    double gL, p0L, gR, p0R;
+    local_stiffened(eos, zL.density, zL.pressure, gL, p0L);
+    local_stiffened(eos, zR.density, zR.pressure, gR, p0R);
+    riemann::Sol s = riemann::solve(zL.density, zL.velocity.x, zL.pressure, gL, p0L, zR.density, zR.velocity.x,
+                                    zR.pressure, gR, p0R);
+    PState z;
+    z.density = s.rho;
+    z.velocity = {s.Uf, s.U > 0.0 ? zL.velocity.y : zR.velocity.y, s.U > 0.0 ? zL.velocity.z : zR.velocity.z};
+    z.pressure = s.Pf;
+    z.energy = eos.energy_rP(s.rho, s.Pf);
+    return flux_from_p(z);
+}
+
 static inline QState num_flux(int kind, const PState &zL, const PState &zR, const Eos &eos) {
-    return kind == FLUX_HLL ? hll(zL, zR, eos) : hllc(zL, zR, eos);
+    switch (kind) {
+        case FLUX_GODUNOV: return godunov(zL, zR, eos);
+        case FLUX_RUSANOV: return rusanov(zL, zR, eos);
+        case FLUX_HLL: return hll(zL, zR, eos);
+        default: return hllc(zL, zR, eos);
+    }
 }
 
 // ---------------------------------------------------------------------------

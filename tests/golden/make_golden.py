@@ -60,6 +60,13 @@ CASES = {
                                0.4, 15, lambda: random_state(256, 11, "water")),
     "superbee_20_zoe": (20, 20, (0, 1, 0, 1), (2, 2, 2, 2), (0, 1.4, 0.0), 3, "superbee", 2, 0.4, 20,
                         lambda: random_state(400, 3)),
+    # the exact-Riemann Godunov flux (shocks, rarefactions and fans across faces) and Rusanov
+    "godunov_riemann3_32_first_order": (32, 32, (0, 1, 0, 1), (2, 2, 2, 2), (0, 1.4, 0.0), 0, "MC", 1, 0.4, 40,
+                                        lambda: riemann2d_case3(32).state),
+    "godunov_stiffened_16_mc": (16, 16, (0.0, 0.1, 0.0, 0.1), (2, 2, 1, 1), (1, 4.4, 6.0e8), 0, "MC", 2, 0.4, 15,
+                                lambda: random_state(256, 12, "water")),
+    "rusanov_fourier_32_vanalbada": (32, 32, (0, 1, 0, 1), (3, 3, 3, 3), (0, 1.4, 0.0), 1, "van Albada", 2, 0.4,
+                                     30, lambda: fourier_smooth(32).state),
 }
 
 
@@ -397,6 +404,9 @@ if __name__ == "__main__":
         make_trs()
     elif "--vtu" in sys.argv:
         make_vtu()
+    elif "--fluxes" in sys.argv:
+        for name in ("godunov_riemann3_32_first_order", "godunov_stiffened_16_mc", "rusanov_fourier_32_vanalbada"):
+            make_case(name, CASES[name])
     elif "--amr-cycle" in sys.argv:
         make_amr_cycles()
     elif "--mm-split" in sys.argv:

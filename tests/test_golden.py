@@ -114,3 +114,34 @@ def test_oracle_matches_reference_build_directly():
         assert np.array_equal(np.array(r.state()), np.array(s.state()))
         gr, go = r.grad(), s.grad()
         assert np.array_equal(gr[0], go[0]) and np.array_equal(gr[1], go[1])
+
+
+def test_oracle_fluxes_match_reference_build_directly():
+    """Godunov (exact Riemann solver) and Rusanov, pointwise, against the
+    reference's own NumFlux on random ideal and stiffened states (shocks,
+    rarefactions, fans on the face, vacuum); NaN where the reference's is."""
+    from oracle import ref as R
+    if not R.available():
+        pytest.skip("reference-source build not present")
+    rng = np.random.default_rng(3)
+    for eos in [(0, 1.4, 0.0, 0.0), (1, 4.4, 6e8, 0.0), (1, 2.0, 1e5, 3.0)]:
+        for kind in (0, 1):
+            for _ in range(800):
+                zs = []
+                for _ in range(2):
+                    if eos[0] == 0:
+                        r, p = 0.1 + 2 * rng.random(), 0.05 + 3 * rng.random()
+                    else:
+                        r = 900 + 200 * rng.random() if eos[2] > 1e6 else 0.5 + rng.random()
+                        p = 1e5 * (0.5 + 10 * rng.random())
+                    u, v = rng.normal() * (100.0 if eos[2] > 1e6 else 1.0), rng.normal()
+                    e = p / ((eos[1] - 1) * r) if eos[0] == 0 else eos[3] + (p + eos[1] * eos[2]) / ((eos[1] - 1) * r)
+                    zs.append(np.array([r, u, v, 0.0, p, e]))
+                zl, zr = zs
+                if rng.random() < 0.1:
+                    zl[1], zr[1] = 5.0, -5.0  # colliding: two shocks
+                elif rng.random() < 0.1:
+                    zl[1], zr[1] = -5.0, 5.0  # receding: rarefactions, vacuum
+                a = np.asarray(O.flux(kind, zl, zr, *eos))
+                b = np.asarray(R.flux(kind, zl, zr, *eos))
+                assert np.array_equal(a, b, equal_nan=True), (kind, eos, zl, zr)

@@ -90,6 +90,9 @@ CASES = [
     ("heun fourier", dict(nx=64, ny=64, bounds=(3, 3, 3, 3), scheme=1), "fourier"),
     ("heun riemann walls", dict(nx=40, ny=40, bounds=(1, 2, 1, 2), scheme=1, lim="MC"), "riemann"),
     ("hll first order", dict(nx=40, ny=40, bounds=(2, 2, 1, 1), acc=1, flux=2), "riemann"),
+    ("godunov first order riemann", dict(nx=48, ny=48, bounds=(2, 2, 2, 2), acc=1, lim="MC", flux=0), "riemann"),
+    ("godunov MC riemann", dict(nx=48, ny=48, bounds=(2, 2, 1, 1), lim="MC", flux=0), "riemann"),
+    ("rusanov fourier periodic", dict(nx=48, ny=48, bounds=(3, 3, 3, 3), flux=1), "fourier"),
 ]
 
 

@@ -15,6 +15,8 @@
 //   rotation       math/cfd/rotate.cpp:7-77 (2-D branch)
 #pragma once
 
+#include <math_constants.h>
+
 #include <cstdint>
 
 namespace zg {
@@ -181,8 +183,176 @@ __device__ inline Cons hll(const Prim &zL, const Prim &zR, const EosD &eos) {
     return F;
 }
 
+// rusanov.cpp:15-43 (std::min / std::max of an initializer list keep the
+// first extreme element)
+__device__ inline Cons rusanov(const Prim &zL, const Prim &zR, const EosD &eos) {
+    double c_L = eos.sound_speed_rP(zL.r, zL.p);
+    double c_R = eos.sound_speed_rP(zR.r, zR.p);
+    double S_L = zL.u - c_L, S_R = zL.u + c_L;
+    if (zR.u - c_R < S_L) S_L = zR.u - c_R;
+    if (0.0 < S_L) S_L = 0.0;
+    if (S_R < zR.u + c_R) S_R = zR.u + c_R;
+    if (S_R < 0.0) S_R = 0.0;
+    const double S = smax(fabs(S_L), S_R), hS = 0.5 * S;
+    Cons QL = q_from_p(zL), QR = q_from_p(zR);
+    Cons FL = flux_from_p(zL), FR = flux_from_p(zR);
+    Cons F;
+    F.r = 0.5 * (FL.r + FR.r) + hS * (QL.r - QR.r);
+    F.mu = 0.5 * (FL.mu + FR.mu) + hS * (QL.mu - QR.mu);
+    F.mv = 0.5 * (FL.mv + FR.mv) + hS * (QL.mv - QR.mv);
+    F.E = 0.5 * (FL.E + FR.E) + hS * (QL.E - QR.E);
+    return F;
+}
+
+// ---------------------------------------------------------------------------
+// Exact Riemann solver for two stiffened gases (math/solver/riemann.cpp) and
+// the Godunov flux of its face state (godunov.cpp:16-32).  The powers of the
+// rarefaction branches use CUDA's pow, so this flux agrees with the
+// reference to a few ulps rather than bit for bit.
+namespace riemann {
+
+__device__ inline double fK(double P, double rK, double pK, double cK, double gK, double p0K, double AK, double BK,
+                            double GK) {  // riemann.cpp:76-84
+    if (P >= pK) return (P - pK) * sqrt(AK / (P + BK));
+    return 2.0 * cK / (gK - 1.0) * (pow((P + p0K) / (pK + p0K), GK) - 1.0);
+}
+__device__ inline double dfK(double P, double rK, double pK, double cK, double gK, double p0K, double AK, double BK,
+                             double GK) {  // riemann.cpp:86-94
+    if (P >= pK) return (1.0 - (P - pK) / (2.0 * (P + BK))) * sqrt(AK / (P + BK));
+    return pow((P + p0K) / (pK + p0K), GK - 1.0) / (rK * cK);
+}
+// the acoustic initial guess (riemann.cpp:32-61: all three cases use it)
+__device__ inline double p_init(double rL, double uL, double pL, double cL, double p0L, double rR, double uR,
+                                double pR, double cR, double p0R) {
+    double rcL = rL * cL, rcR = rR * cR;
+    double P = (pL * rcR + pR * rcL + (uL - uR) * rcL * rcR) / (rcL + rcR);
+    double Pmin = -smin(p0L, p0R) + 1.0e-2 * smin(pL + p0L, pR + p0R);
+    return smax(Pmin, P);
+}
+
+// contact_p (riemann.cpp:118-236): pressure and velocity of the contact.
+// `failed`: the case where the reference throws (no convergence, far off).
+__device__ inline void contact(double rL, double uL, double pL, double cL, double gL, double p0L, double rR,
+                               double uR, double pR, double cR, double gR, double p0R, double &P_out, double &U_out,
+                               bool &failed) {
+    const double AL = 2.0 / ((gL + 1) * rL), AR = 2.0 / ((gR + 1) * rR);
+    const double BL = (gL - 1.0) * pL / (gL + 1.0) + 2.0 * gL * p0L / (gL + 1.0);
+    const double BR = (gR - 1.0) * pR / (gR + 1.0) + 2.0 * gR * p0R / (gR + 1.0);
+    const double GL = (gL - 1.0) / (2.0 * gL), GR = (gR - 1.0) / (2.0 * gR);
+    const double p_dno = smax(-p0L, -p0R);
+    failed = false;
+    const double f_dno =
+        fK(p_dno, rL, pL, cL, gL, p0L, AL, BL, GL) + fK(p_dno, rR, pR, cR, gR, p0R, AR, BR, GR) + uR - uL;
+    if (f_dno > 0.0) {  // vacuum
+        P_out = p_dno;
+        U_out = 0.0;
+        return;
+    }
+    double P = p_init(rL, uL, pL, cL, p0L, rR, uR, pR, cR, p0R);
+    const double DP1 = 1.0e-5 * fabs(pL - pR);
+    const double DP2 = 1.0e-12 * fabs(smax(pL + p0L, pR + p0R));
+    const double DP = smax(DP1, DP2);
+    double fL = 0.0, fR = 0.0, Pn = P;
+    int counter = 0;
+    for (; counter < 50; ++counter) {
+        fL = fK(P, rL, pL, cL, gL, p0L, AL, BL, GL);
+        fR = fK(P, rR, pR, cR, gR, p0R, AR, BR, GR);
+        const double dfL = dfK(P, rL, pL, cL, gL, p0L, AL, BL, GL);
+        const double dfR = dfK(P, rR, pR, cR, gR, p0R, AR, BR, GR);
+        Pn = P - (fL + fR + uR - uL) / (dfL + dfR);
+        if (Pn < p_dno) Pn = (p_dno + P) / 2;
+        if (fabs(Pn - P) < DP && counter > 3) break;
+        P = Pn;
+    }
+    if (counter >= 50 && fabs((P - Pn) / (P + Pn)) > 0.02) failed = true;
+    P_out = P;
+    U_out = 0.5 * (uL + uR + fR - fL);
+}
+
+// RiemannSolver::solve (riemann.cpp:366-460): density, velocity and pressure
+// on the face x / t = 0, and the contact velocity U.
+__device__ inline void solve(double rL, double uL, double pL, double gL, double p0L, double rR, double uR, double pR,
+                             double gR, double p0R, double &rho, double &Uf, double &Pf, double &U, bool &failed) {
+    const double cL = sqrt(gL * (pL + p0L) / rL);
+    const double cR = sqrt(gR * (pR + p0R) / rR);
+    double P;
+    contact(rL, uL, pL, cL, gL, p0L, rR, uR, pR, cR, gR, p0R, P, U, failed);
+    if (U > 0.0) {
+        if (pL < P) {
+            const double D = uL + (P - pL) / (rL * (U - uL));
+            if (D > 0.0) {
+                rho = rL; Uf = uL; Pf = pL;
+            } else {
+                rho = rL * (P - pL) / ((P - pL) - rL * ((U - uL) * (U - uL)));
+                Uf = U; Pf = P;
+            }
+        } else if (uL - cL > 0.0) {
+            rho = rL; Uf = uL; Pf = pL;
+        } else {
+            const double cl = cL + 0.5 * (gL - 1.0) * (uL - U);
+            if (U - cl < 0.0) {
+                rho = gL * (P + p0L) / (cl * cl);
+                Uf = U; Pf = P;
+            } else {
+                const double base = 2.0 / (gL + 1.0) + ((gL - 1.0) * (uL - 0.0)) / ((gL + 1.0) * cL);
+                rho = rL * pow(base, 2.0 / (gL - 1.0));
+                Uf = ((gL - 1.0) * uL + 2.0 * (cL + 0.0)) / (gL + 1.0);
+                Pf = (pL + p0L) * pow(base, 2.0 * gL / (gL - 1.0)) - p0L;
+            }
+        }
+    } else {
+        if (P > pR) {
+            const double D = uR + (P - pR) / (rR * (U - uR));
+            if (D < 0.0) {
+                rho = rR; Uf = uR; Pf = pR;
+            } else {
+                rho = rR * (P - pR) / ((P - pR) - rR * ((U - uR) * (U - uR)));
+                Uf = U; Pf = P;
+            }
+        } else if (uR + cR < 0.0) {
+            rho = rR; Uf = uR; Pf = pR;
+        } else {
+            const double cr = cR - 0.5 * (gR - 1.0) * (uR - U);
+            if (U + cr > 0.0) {
+                rho = gR * (P + p0R) / (cr * cr);
+                Uf = U; Pf = P;
+            } else {
+                const double base = 2.0 / (gR + 1.0) - ((gR - 1.0) * (uR - 0.0)) / ((gR + 1.0) * cR);
+                rho = rR * pow(base, 2.0 / (gR - 1.0));
+                Uf = ((gR - 1.0) * uR + 2.0 * (0.0 - cR)) / (gR + 1.0);
+                Pf = (pR + p0R) * pow(base, 2.0 * gR / (gR - 1.0)) - p0R;
+            }
+        }
+    }
+}
+
+}  // namespace riemann
+
+// Godunov::calc_flux (godunov.cpp:16-32): the gas's own stiffened-gas
+// parameters (IdealGas / StiffenedGas::stiffened_gas: gamma, P0), the exact
+// face state, its physical flux.
+__device__ inline Cons godunov(const Prim &zL, const Prim &zR, const EosD &eos) {
+    const double P0 = eos.kind == EOS_IDEAL ? 0.0 : eos.P0;
+    double rho, Uf, Pf, U;
+    bool failed;
+    riemann::solve(zL.r, zL.u, zL.p, eos.gamma, P0, zR.r, zR.u, zR.p, eos.gamma, P0, rho, Uf, Pf, U, failed);
+    Prim z;
+    z.r = rho;
+    z.u = Uf;
+    z.v = U > 0.0 ? zL.v : zR.v;
+    z.p = Pf;
+    z.e = eos.energy_rP(rho, Pf);
+    if (failed) z.r = CUDART_NAN;  // the reference throws here; the flux becomes NaN instead
+    return flux_from_p(z);
+}
+
 __device__ inline Cons num_flux(int kind, const Prim &zL, const Prim &zR, const EosD &eos) {
-    return kind == FLUX_HLL ? hll(zL, zR, eos) : hllc(zL, zR, eos);
+    switch (kind) {
+        case FLUX_GODUNOV: return godunov(zL, zR, eos);
+        case FLUX_RUSANOV: return rusanov(zL, zR, eos);
+        case FLUX_HLL: return hll(zL, zR, eos);
+        default: return hllc(zL, zR, eos);
+    }
 }
 
 // limiter.cxx binary forms phi(a, b)

@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S2_MINB) k_faces(SmfArgs a, F
         }
         rot_in(nx, ny, zm.u, zm.v);
         rot_in(nx, ny, zp.u, zp.v);
-        C4<R> lf = (robust || a.flux == FLUX_HLL) ? tiled::hll(zm, zp, eos) : tiled::hllc(zm, zp, eos);
+        C4<R> lf = tiled::face_flux(a.flux, robust, zm, zp, eos, a.eos);
         rot_out(nx, ny, lf.mu, lf.mv);
         F[0] += (double)lf.r * g.area;
         F[1] += (double)lf.mu * g.area;

@@ -119,6 +119,44 @@ __device__ inline C4<R> hll(const P5<R> &L, const P5<R> &Rs, const EosR<R> &eos)
     return C4<R>{o[0], o[1], o[2], o[3]};
 }
 
+// rusanov.cpp:15-43 in precision R
+template <typename R>
+__device__ inline C4<R> rusanov(const P5<R> &L, const P5<R> &Rs, const EosR<R> &eos) {
+    R cL = eos.sound(L.r, L.p), cR = eos.sound(Rs.r, Rs.p);
+    R SL = L.u - cL, SR = L.u + cL;
+    if (Rs.u - cR < SL) SL = Rs.u - cR;
+    if (R(0) < SL) SL = R(0);
+    if (SR < Rs.u + cR) SR = Rs.u + cR;
+    if (SR < R(0)) SR = R(0);
+    const R hS = R(0.5) * smax_t(fabs(SL), SR);
+    R EL = L.e + R(0.5) * (L.u * L.u + L.v * L.v);
+    R ER = Rs.e + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v);
+    C4<R> FL = phys_flux(L), FR = phys_flux(Rs);
+    R QL[4] = {L.r, L.r * L.u, L.r * L.v, L.r * EL};
+    R QR[4] = {Rs.r, Rs.r * Rs.u, Rs.r * Rs.v, Rs.r * ER};
+    R fl[4] = {FL.r, FL.mu, FL.mv, FL.E}, fr[4] = {FR.r, FR.mu, FR.mv, FR.E};
+    R o[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o[k] = R(0.5) * (fl[k] + fr[k]) + hS * (QL[k] - QR[k]);
+    return C4<R>{o[0], o[1], o[2], o[3]};
+}
+
+// The selected numerical flux in the face frame (HLL on isolated cells).
+// Godunov's exact Riemann solver runs in FP64 whatever R is.
+template <typename R>
+__device__ inline C4<R> face_flux(int kind, bool robust, const P5<R> &L, const P5<R> &Rs, const EosR<R> &eos,
+                                  const EosD &eosd) {
+    if (robust || kind == FLUX_HLL) return hll(L, Rs, eos);
+    if (kind == FLUX_GODUNOV) {
+        const Prim a{(double)L.r, (double)L.u, (double)L.v, (double)L.p, (double)L.e};
+        const Prim b{(double)Rs.r, (double)Rs.u, (double)Rs.v, (double)Rs.p, (double)Rs.e};
+        const Cons f = godunov(a, b, eosd);
+        return C4<R>{(R)f.r, (R)f.mu, (R)f.mv, (R)f.E};
+    }
+    if (kind == FLUX_RUSANOV) return rusanov(L, Rs, eos);
+    return hllc(L, Rs, eos);
+}
+
 template <typename R>
 __device__ inline R lim2(int kind, R a, R b) {
     switch (kind) {
@@ -622,7 +660,7 @@ __global__ void __launch_bounds__(TX *TY, MINB) k_faces(SmfArgs a, Fields<R> f) 
             }
             to_local(s_own, zm.u, zm.v);
             to_local(s_own, zp.u, zp.v);
-            C4<R> lf = (robust || a.flux == FLUX_HLL) ? hll(zm, zp, eos) : hllc(zm, zp, eos);
+            C4<R> lf = face_flux(a.flux, robust, zm, zp, eos, a.eos);
             to_global(s_own, lf.mu, lf.mv);
             out[0] = sgn * lf.r;
             out[1] = sgn * lf.mu;

@@ -393,7 +393,7 @@ class SmFluid:
         self._push()
 
     def set_method(self, method: Fluxes):  # sm_fluid.cpp:49-51
-        if int(method) not in (Fluxes.HLL, Fluxes.HLLC):
+        if int(method) not in (Fluxes.GODUNOV, Fluxes.RUSANOV, Fluxes.HLL, Fluxes.HLLC):
             raise ZgError(-1, f"numerical flux {Fluxes(method).name} is not implemented on the GPU")
         self.params.flux = int(method)
         self._push()
