@@ -67,6 +67,7 @@ def lib():
         L.zo_mm_set_max_dt.argtypes = [C.c_void_p, C.c_double]
         L.zo_mm_set_threads.argtypes = [C.c_void_p, C.c_int]
         L.zo_mm_set_split.argtypes = [C.c_void_p, C.c_int]
+        L.zo_mm_set_accuracy.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.zo_mm_make_states.argtypes = [C.c_void_p, _P, _P, _P, _P, _P]
         L.zo_mm_set_states.argtypes = [C.c_void_p, _P]
         L.zo_mm_get_states.argtypes = [C.c_void_p, _P]
@@ -277,6 +278,10 @@ class MmSolver:
 
     def set_threads(self, n):
         lib().zo_mm_set_threads(self.h, n)
+
+    def set_accuracy(self, acc, limiter=3):
+        """MmFluid::set_accuracy (mm_fluid.cpp:46-48) and the limiter (default MC)."""
+        lib().zo_mm_set_accuracy(self.h, int(acc), int(limiter))
 
     def set_splitting(self, split):
         """DirSplit: 0 NONE, 1 SIMPLE, 2 STRANG (mm_fluid.cpp:112-137)."""

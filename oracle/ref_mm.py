@@ -30,6 +30,7 @@ def lib():
                                  C.c_double, C.c_int, C.c_int]
         L.zmm_free.argtypes = [C.c_void_p]
         L.zmm_set_split.argtypes = [C.c_void_p, C.c_int]
+        L.zmm_set_limiter.argtypes = [C.c_void_p, C.c_char_p]
         L.zm_threads.argtypes = [C.c_int]
         L.zmm_n_cells.argtypes = [C.c_void_p]
         L.zmm_n_cells.restype = C.c_int
@@ -71,6 +72,9 @@ class RefMmFluid:
         self.h = lib().zmm_create(nx, ny, *box, b.ctypes.data_as(_I), materials.encode(), CFL, accuracy, crp_mode)
         self.n = lib().zmm_n_cells(self.h)
         self.nmat = materials.count(",") + 1
+
+    def set_limiter(self, name):
+        lib().zmm_set_limiter(self.h, name.encode())
 
     def set_splitting(self, split):
         """MmFluid::set_splitting: 0 NONE, 1 SIMPLE, 2 STRANG."""

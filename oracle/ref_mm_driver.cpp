@@ -109,6 +109,9 @@ void *zmm_create(int nx, int ny, double x_min, double x_max, double y_min, doubl
 
 void zmm_free(void *p) { delete static_cast<RefMm *>(p); }
 
+// MmFluid::set_limiter (mm_fluid.cpp:72-74)
+void zmm_set_limiter(void *p, const char *name) { static_cast<RefMm *>(p)->solver->set_limiter(name); }
+
 // MmFluid::set_splitting (mm_fluid.cpp:75-77): 0 NONE, 1 SIMPLE, 2 STRANG
 void zmm_set_split(void *p, int split) {
     static_cast<RefMm *>(p)->solver->set_splitting(math::DirSplit(split));

@@ -1258,6 +1258,12 @@ void zo_mm_set_max_dt(void *p, double dt) { static_cast<zo::mm::MmSolver *>(p)->
 void zo_mm_set_threads(void *p, int n) { static_cast<zo::mm::MmSolver *>(p)->threads = n; }
 // MmFluid::set_splitting (mm_fluid.cpp:75-77): 0 NONE, 1 SIMPLE, 2 STRANG
 void zo_mm_set_split(void *p, int split) { static_cast<zo::mm::MmSolver *>(p)->split = split; }
+// MmFluid::set_accuracy / set_limiter (mm_fluid.cpp:46-48, 72-74)
+void zo_mm_set_accuracy(void *p, int acc, int limiter) {
+    auto *s = static_cast<zo::mm::MmSolver *>(p);
+    s->acc = std::min(std::max(1, acc), 2);
+    s->limiter = limiter;
+}
 // States from (density, velocity, pressure, mass fractions) through the
 // mixture closure, as PState(density, velocity, pressure, Fractions(array),
 // mixture); beta holds 4 fractions per cell and is normalised first.

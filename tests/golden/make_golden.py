@@ -178,7 +178,7 @@ def make_amr_cycle(name, n, bounds, max_level, distributor, acc, limiter, cycles
 MM_MATERIALS = "stiffened:Water,ideal:Air"
 
 
-def make_mm(name, n, crp_mode, steps, split=0):
+def make_mm(name, n, crp_mode, steps, split=0, acc=1, limiter="MC"):
     """The reference's MmFluid (first order, CFL 0.4, direction splitting
     `split`: 0 NONE, 1 SIMPLE, 2 STRANG) on the shock / water column problem
     at n x n: initial states through the reference's mixture closure, the
@@ -187,15 +187,16 @@ def make_mm(name, n, crp_mode, steps, split=0):
     from oracle import ref_mm as RM
     from zephyr_b200.workloads import shock_water_column
     w = shock_water_column(n)
-    r = RM.RefMmFluid(n, n, box=w.box, bounds=w.bounds, materials=MM_MATERIALS, CFL=0.4, accuracy=1,
+    r = RM.RefMmFluid(n, n, box=w.box, bounds=w.bounds, materials=MM_MATERIALS, CFL=0.4, accuracy=acc,
                       crp_mode=crp_mode)
     r.set_splitting(split)
+    r.set_limiter(limiter)
     r.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
     init = r.states()
     nrm, off = r.interface()
     dts = np.array([r.step() for _ in range(steps)])
     np.savez_compressed(OUT / f"{name}.npz", n=n, box=np.array(w.box), bounds=np.array(w.bounds), crp_mode=crp_mode,
-                        split=split, CFL=0.4, steps=steps, inputs=np.stack([w.rho, w.vx, w.vy, w.p]), beta=w.beta, init=init,
+                        split=split, acc=acc, limiter=limiter, CFL=0.4, steps=steps, inputs=np.stack([w.rho, w.vx, w.vy, w.p]), beta=w.beta, init=init,
                         normals=nrm, offsets=off, dts=dts, final=r.states(), flags=r.flags())
 
 
@@ -380,6 +381,9 @@ def main():
     make_mm("mm_shock_column_24_vs", 24, 3, 120)
     make_mm("mm_shock_column_24_strang_plic", 24, 4, 80, split=2)
     make_mm("mm_shock_column_24_simple_vs", 24, 3, 80, split=1)
+    make_mm("mm_shock_column_32_second_order_plic", 32, 4, 60, acc=2, limiter="MC")
+    make_mm("mm_shock_column_24_second_order_hllc_minmod", 24, 0, 50, acc=2, limiter="minmod")
+    make_mm("mm_shock_column_24_second_order_strang_vs", 24, 3, 40, split=2, acc=2, limiter="van Albada")
     make_mm_pointwise()
     print("wrote multi-material cases")
     make_amr_cycles()
@@ -409,6 +413,10 @@ if __name__ == "__main__":
             make_case(name, CASES[name])
     elif "--amr-cycle" in sys.argv:
         make_amr_cycles()
+    elif "--mm2" in sys.argv:
+        make_mm("mm_shock_column_32_second_order_plic", 32, 4, 60, acc=2, limiter="MC")
+        make_mm("mm_shock_column_24_second_order_hllc_minmod", 24, 0, 50, acc=2, limiter="minmod")
+        make_mm("mm_shock_column_24_second_order_strang_vs", 24, 3, 40, split=2, acc=2, limiter="van Albada")
     elif "--mm-split" in sys.argv:
         make_mm("mm_shock_column_24_strang_plic", 24, 4, 80, split=2)
         make_mm("mm_shock_column_24_simple_vs", 24, 3, 80, split=1)

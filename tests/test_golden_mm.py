@@ -12,6 +12,7 @@ from oracle import oracle as O
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = sorted(p.stem for p in GOLDEN.glob("mm_shock_column_*.npz"))
+LIM_ID = {"minmod": 2, "MC": 3, "van Albada": 5}
 
 
 def same(a, b):
@@ -24,6 +25,8 @@ def solver_for(g):
     m = O.Mesh(n, n, *(float(x) for x in g["box"]), bounds=tuple(int(b) for b in g["bounds"]))
     s = O.MmSolver(m, CFL=float(g["CFL"]), crp_mode=int(g["crp_mode"]))
     s.set_splitting(int(g["split"]) if "split" in g.files else 0)
+    if "acc" in g.files:
+        s.set_accuracy(int(g["acc"]), LIM_ID[str(g["limiter"])])
     return m, s
 
 
