@@ -288,6 +288,9 @@ enum zg_kernel_kind {
     ZG_K_TR_UPDATE,   /* transport update of u1 */
     ZG_K_TR_NORMALS,  /* interface normals and sections (InterfaceRecovery compute_normals + find_sections) */
     ZG_K_TR_ADJUST,   /* one smoothing pass (InterfaceRecovery adjust_normals + find_sections) */
+    ZG_K_MM_GRAD,     /* multi-material second order: limited gradients (MmFluid::compute_grad) */
+    ZG_K_MM_STAGE1,   /* multi-material predictor (MmFluid::fluxes_stage1) */
+    ZG_K_MM_STAGE2,   /* multi-material corrector (MmFluid::fluxes_stage2) */
     ZG_K_COUNT
 };
 
@@ -342,14 +345,15 @@ typedef struct zg_mmf_params {
     int n_materials;          /* 2 */
     zg_material materials[4]; /* MixturePT{...}, in order */
     int crp_mode;             /* zg_crp_mode; set_crp_mode / set_method(CRP) */
-    int accuracy;             /* 1 (set_accuracy) */
+    int accuracy;             /* 1 or 2 (set_accuracy) */
     double CFL;               /* clamped to [0, 1] (set_CFL) */
     double max_dt;            /* set_max_dt */
     int split;                /* zg_dir_split (set_splitting) */
     int precision;            /* zg_precision: FP64 (the reference's arithmetic) or MIXED (FP32 face
                                  states, wave speeds and HLLC fluxes of the pure-stencil faces; FP64
                                  accumulation, update, EoS pressure recovery, composite Riemann
-                                 fluxes, PLIC and dt) */
+                                 fluxes, PLIC and dt; first order only) */
+    int limiter;              /* zg_limiter of the second-order gradients (set_limiter; default MC) */
 } zg_mmf_params;
 
 /* MmFluid's constructor defaults (mm_fluid.cpp:16-26): CRP with PLIC,

@@ -45,6 +45,9 @@ def test_gpu_mm_matches_reference_fixture(gpu_lib, name):
     if "split" in g.files:
         from zephyr_b200.mmf import DirSplit
         s.set_splitting(DirSplit(int(g["split"])))
+    if "acc" in g.files:
+        s.set_accuracy(int(g["acc"]))
+        s.set_limiter(str(g["limiter"]))
     rho, vx, vy, p = g["inputs"]
     s.make_states(mesh, rho, vx, vy, p, g["beta"])
     assert same(s.states(mesh), g["init"]), "mixture closure of the initial states differs"
@@ -117,7 +120,7 @@ def test_gpu_mm_rejects_what_it_does_not_build(gpu_lib):
     two = MmFluid(MixturePT([Material.stiffened("Water"), Material.ideal("Air")]))
     two.add_types(mesh)
     with pytest.raises(Z.ZgError):
-        two.set_accuracy(2)
+        two.set_limiter("no-such-limiter")
     mesh.close()
 
 
@@ -152,3 +155,46 @@ def test_gpu_mm_mixed_form_tracks_fp64(gpu_lib):
     # true densities are NaN where a material is absent: at most a few cells
     # next to the interface may hold a trace of the other material in one form only
     assert np.mean(np.any(np.isnan(zmx) != np.isnan(z64), axis=1)) <= 1e-3
+
+
+@pytest.mark.parametrize("crp,split,lim,limid", [(4, 0, "MC", 3), (0, 0, "van Albada", 5), (3, 1, "minmod", 2),
+                                                 (2, 2, "MC", 3)])
+def test_gpu_mm_second_order_matches_oracle(gpu_lib, oracle_mod, crp, split, lim, limid):
+    """MmFluid::set_accuracy(2): limited gradients of the mixture state,
+    predictor with interpolation_update closures, corrector with composite
+    fluxes of the reconstructed states; a fresh size, 60 steps back to back."""
+    Z, O = gpu_lib, oracle_mod
+    from zephyr_b200.mmf import DirSplit
+    from zephyr_b200.workloads import shock_water_column
+    n = 36
+    w = shock_water_column(n)
+    mesh, s = gpu_solver(Z, n, w.box, w.bounds, crp, 0.4)
+    s.set_accuracy(2)
+    s.set_limiter(lim)
+    s.set_splitting(DirSplit(split))
+    s.make_states(mesh, w.rho, w.vx, w.vy, w.p, w.beta)
+    o = O.MmSolver(O.Mesh(n, n, *w.box, bounds=w.bounds), CFL=0.4, crp_mode=crp)
+    o.set_accuracy(2, limid)
+    o.set_splitting(split)
+    o.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
+    s.update(mesh, 60)
+    dts = o.steps(60)
+    assert s.dt() == dts[-1]
+    final, want = s.states(mesh), o.states()
+    bad = ~((final == want) | (np.isnan(final) & np.isnan(want)))
+    assert not bad.any(), f"{np.count_nonzero(bad.any(axis=1))} cells differ"
+    beta = final[:, 6:8]
+    assert ((beta > 0) & (beta < 1)).any(axis=1).sum() > 0  # the shock reached the column
+    mesh.close()
+
+
+def test_gpu_mm_second_order_rejects_mixed_form(gpu_lib):
+    Z = gpu_lib
+    from zephyr_b200 import ZgError
+    from zephyr_b200.workloads import shock_water_column
+    w = shock_water_column(16)
+    mesh, s = gpu_solver(Z, 16, w.box, w.bounds, 4, 0.4)
+    s.set_precision(Z.Precision.MIXED)
+    with pytest.raises(ZgError):
+        s.set_accuracy(2)
+    mesh.close()

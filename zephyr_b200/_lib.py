@@ -80,7 +80,7 @@ class MmfParams(C.Structure):
     """zg_mmf_params"""
     _fields_ = [("n_materials", C.c_int), ("materials", Material * 4), ("crp_mode", C.c_int),
                 ("accuracy", C.c_int), ("CFL", C.c_double), ("max_dt", C.c_double), ("split", C.c_int),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("limiter", C.c_int)]
 
 
 class TrParams(C.Structure):
@@ -174,7 +174,8 @@ SIGNATURES = {
 
 # enum zg_kernel_kind
 KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags", "mm_dt", "mm_recover",
-                "mm_flux", "mm_crp", "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals", "tr_adjust"]
+                "mm_flux", "mm_crp", "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals", "tr_adjust",
+                "mm_grad", "mm_stage1", "mm_stage2"]
 
 _lib = None
 

@@ -343,6 +343,257 @@ __global__ void __launch_bounds__(BLOCK) k_make_states(MmArgs a, const double *r
     store(a.z, ic, state_of_rvp(a.mix, rho[ic], vx[ic], vy[ic], P[ic], b));
 }
 
+// ---------------------------------------------------------------------------
+// Second order (MmFluid::integrate with accuracy 2, mm_fluid.cpp:152-168).
+// The state as an array of NG components; the reference's mmf::PState also
+// carries vz and the unused fraction / density slots, whose gradients are 0
+// and NaN and never reach a result here.
+__device__ __forceinline__ void to_arr(const MSt<NM> &z, double *v) {
+    v[0] = z.rho;
+    v[1] = z.vx;
+    v[2] = z.vy;
+    v[3] = z.P;
+    v[4] = z.e;
+    v[5] = z.T;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        v[6 + i] = z.b.f[i];
+        v[6 + NM + i] = z.r[i];
+    }
+}
+__device__ __forceinline__ MSt<NM> from_arr(const double *v) {
+    MSt<NM> z;
+    z.rho = v[0];
+    z.vx = v[1];
+    z.vy = v[2];
+    z.P = v[3];
+    z.e = v[4];
+    z.T = v[5];
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        z.b.f[i] = v[6 + i];
+        z.r[i] = v[6 + NM + i];
+    }
+    return z;
+}
+
+// boundary_value (mm_fluid.cpp:88-97) of a state for slot geometry g
+__device__ __forceinline__ MSt<NM> ghost(const MSt<NM> &zc, const FaceG &g) {
+    MSt<NM> zn = zc;
+    if (g.flag == BC_WALL) wall_velocity(g, zc.vx, zc.vy, zn.vx, zn.vy);
+    return zn;
+}
+
+// compute_grad (mm_fluid.cpp:439-467): in CRP modes zero gradients in and
+// next to mixed cells; else gradient::LSM and gradient::limiting
+// (gradient.h:226-282, 412-474) on every component, in the 2-D reduction of
+// the 3x3 system (A(i,2), A(2,j) exact zeros, A(2,2) set to 1).
+__global__ void __launch_bounds__(BLOCK) k_grad2(MmArgs a) {
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    StructAcc c(a.mesh, ic);
+    const MSt<NM> zc = load(a.z, ic);
+    bool set_zero = false;
+    if (a.crp != CRP_NONE) {
+        set_zero = frac_index(zc.b) < 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            FaceG g = c.face(s);
+            if (frac_index(load(a.z, g.nb).b) < 0) set_zero = true;
+        }
+    }
+    if (set_zero) {
+#pragma unroll
+        for (int k = 0; k < NG; ++k) {
+            a.gx[k][ic] = 0.0;
+            a.gy[k][ic] = 0.0;
+        }
+        return;
+    }
+    const double pcx = c.cx(), pcy = c.cy();
+    double zcv[NG], dn[4][NG], wv[4], drx[4], dry[4], drnx[4], drny[4];
+    to_arr(zc, zcv);
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
+    double Fx[NG], Fy[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) Fx[k] = Fy[k] = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = c.face(s);
+        double znv[NG];
+        to_arr(!is_boundary(g.flag) ? load(a.z, g.nb) : ghost(zc, g), znv);
+        double ncx, ncy;
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
+        const double rx = ncx - pcx, ry = ncy - pcy;
+        const double d = rx * g.nx + ry * g.ny;
+        const double nxx = d * g.nx, nyy = d * g.ny;
+        const double w = 1.0 * g.area / cube_rn(sqrt(nxx * nxx + nyy * nyy));
+        const double wdx = w * nxx, wdy = w * nyy;
+        A00 += wdx * rx;
+        A01 += wdx * ry;
+        A10 += wdy * rx;
+        A11 += wdy * ry;
+        wv[s] = w;
+        drx[s] = rx;
+        dry[s] = ry;
+        drnx[s] = nxx;
+        drny[s] = nyy;
+#pragma unroll
+        for (int k = 0; k < NG; ++k) {
+            const double dF = znv[k] - zcv[k];
+            dn[s][k] = dF;
+            Fx[k] += w * dF * nxx;
+            Fy[k] += w * dF * nyy;
+        }
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;
+    const double det = A11 * A00 + (-A01) * A10;
+    const double inv = 1.0 / det;
+    const double B00 = A11 * inv, B01 = (-A01) * inv, B10 = (-A10) * inv, B11 = A00 * inv;
+    double Lx[NG], Ly[NG];
+#pragma unroll
+    for (int k = 0; k < NG; ++k) {
+        const double g0x = B00 * Fx[k] + B01 * Fy[k];
+        const double g0y = B10 * Fx[k] + B11 * Fy[k];
+        double lx = 0.0, ly = 0.0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double dF_p = dn[s][k];
+            const double du_n = g0x * drx[s] + g0y * dry[s];
+            const double dF_m = 2.0 * du_n - dF_p;
+            const double dF_lim = limiter2(a.limiter, dF_m, dF_p) * dF_p;
+            lx += wv[s] * dF_lim * drnx[s];
+            ly += wv[s] * dF_lim * drny[s];
+        }
+        Lx[k] = lx;
+        Ly[k] = ly;
+    }
+#pragma unroll
+    for (int k = 0; k < NG; ++k) {
+        a.gx[k][ic] = B00 * Lx[k] + B01 * Ly[k];
+        a.gy[k][ic] = B10 * Lx[k] + B11 * Ly[k];
+    }
+}
+
+// FaceExtra::Direct (face_extra.h:121-171): z shifted along cell o's
+// gradients by (dx, dy)
+__device__ __forceinline__ MSt<NM> shifted(const MmArgs &a, const MSt<NM> &z, int o, double dx, double dy) {
+    double v[NG];
+    to_arr(z, v);
+#pragma unroll
+    for (int k = 0; k < NG; ++k) v[k] = v[k] + (a.gx[k][o] * dx + a.gy[k][o] * dy);
+    return from_arr(v);
+}
+
+// PState::interpolation_update (models.cpp:381-391): fractions normalised,
+// true densities, energy and temperature from (density, pressure) by get_reT
+// with the extrapolated temperature and densities as the guesses
+__device__ __forceinline__ void interp_update(const MixD<NM> &mx, MSt<NM> &z) {
+    normalize(z.b);
+    const int idx = frac_index(z.b);
+    if (idx >= 0) {
+#pragma unroll
+        for (int i = 0; i < NM; ++i) z.r[i] = i == idx ? z.rho : MM_NAN;
+        z.e = m_energy_rP(mx.mat[idx], z.rho, z.P);
+        z.T = m_temperature_rP(mx.mat[idx], z.rho, z.P);
+    } else {
+        RhoSet<NM> rh;
+        double T;
+        double r0[NM];
+#pragma unroll
+        for (int i = 0; i < NM; ++i) r0[i] = z.r[i];
+        z.e = find_reT_rP(mx, z.rho, z.P, z.b, z.T, r0, rh, T, false).val;
+        z.T = T;
+#pragma unroll
+        for (int i = 0; i < NM; ++i) z.r[i] = rh.r[i];
+    }
+}
+
+// fluxes_stage1 (mm_fluid.cpp:521-587): the half step of the cells that are
+// not mixed, from the physical fluxes of their own face values
+__global__ void __launch_bounds__(BLOCK) k_stage1(MmArgs a) {
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    const double dt = a.dt_scale * *a.dt_out;
+    StructAcc c(a.mesh, ic);
+    const MSt<NM> zc = load(a.z, ic);
+    if (frac_index(zc.b) < 0) {
+        store(a.zhalf, ic, zc);
+        return;
+    }
+    const double pcx = c.cx(), pcy = c.cy();
+    QVd<NM> flux = qv_zero<NM>();
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        if (skip_face(a.dir, s)) continue;
+        FaceG g = c.face(s);
+        MSt<NM> zm = shifted(a, zc, ic, g.fcx - pcx, g.fcy - pcy);
+        interp_update(a.mix, zm);
+        to_local(g.nx, g.ny, zm.vx, zm.vy, zm.vx, zm.vy);
+        QVd<NM> lf = f_of(zm);
+        const double mxx = g.nx * lf.a[1] + -g.ny * lf.a[2] + 0.0 * 0.0;
+        const double myy = g.ny * lf.a[1] + g.nx * lf.a[2] + 0.0 * 0.0;
+        lf.a[1] = mxx;
+        lf.a[2] = myy;
+#pragma unroll
+        for (int k = 0; k < 4 + NM; ++k) flux.a[k] += lf.a[k] * g.area;
+    }
+    QVd<NM> q = q_of(zc);
+    const double coef = 0.5 * dt / c.vol();
+#pragma unroll
+    for (int k = 0; k < 4 + NM; ++k) q.a[k] -= coef * flux.a[k];
+    store(a.zhalf, ic, state_of_q(a.mix, q, zc.P, zc.T, zc.r));
+}
+
+// fluxes_stage2 (mm_fluid.cpp:589-680): the step from the half-step face
+// values, extrapolated with the old layer's gradients, through calc_flux
+__global__ void __launch_bounds__(BLOCK) k_stage2(MmArgs a) {
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    const double dt = a.dt_scale * *a.dt_out;
+    StructAcc c(a.mesh, ic);
+    const double pcx = c.cx(), pcy = c.cy(), V_c = c.vol();
+    const MSt<NM> zc = load(a.z, ic);
+    const MSt<NM> zch = load(a.zhalf, ic);
+    QVd<NM> flux = qv_zero<NM>();
+    bool bad = false;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        if (skip_face(a.dir, s)) continue;
+        FaceG g = c.face(s);
+        const bool bnd = is_boundary(g.flag);
+        double ncx, ncy;
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
+        const double V_n = V_c;
+        MSt<NM> zm = shifted(a, zch, ic, g.fcx - pcx, g.fcy - pcy);
+        interp_update(a.mix, zm);
+        MSt<NM> zp;
+        if (!bnd) {
+            zp = shifted(a, load(a.zhalf, g.nb), g.nb, g.fcx - ncx, g.fcy - ncy);
+            interp_update(a.mix, zp);
+        } else {
+            zp = ghost(zm, g);
+        }
+        to_local(g.nx, g.ny, zm.vx, zm.vy, zm.vx, zm.vy);
+        to_local(g.nx, g.ny, zp.vx, zp.vy, zp.vx, zp.vy);
+        const double S = g.area;
+        QVd<NM> lf = calc_flux(a, dt, ic, g, zm, zp, V_c / S, V_n / S, bad);
+        const double mxx = g.nx * lf.a[1] + -g.ny * lf.a[2] + 0.0 * 0.0;
+        const double myy = g.ny * lf.a[1] + g.nx * lf.a[2] + 0.0 * 0.0;
+        lf.a[1] = mxx;
+        lf.a[2] = myy;
+#pragma unroll
+        for (int k = 0; k < 4 + NM; ++k) flux.a[k] += lf.a[k] * S;
+    }
+    QVd<NM> q = q_of(zc);
+    const double coef = dt / V_c;
+#pragma unroll
+    for (int k = 0; k < 4 + NM; ++k) q.a[k] -= coef * flux.a[k];
+    if (q.a[0] < 0.0) bad = true;  // the reference throws (mm_fluid.cpp:670-672)
+    if (bad) atomicOr(a.err, 1);
+    store(a.znext, ic, state_of_q(a.mix, q, zc.P, zc.T, zc.r));
+}
+
 static inline unsigned blocks(const MmArgs &a) { return (unsigned)((a.mesh.n + BLOCK - 1) / BLOCK); }
 
 void launch_dt(const MmArgs &a, void *stream) { k_dt<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
@@ -358,6 +609,9 @@ void launch_flux_crp(const MmArgs &a, void *stream) {
 void launch_closure(const MmArgs &a, void *stream) {
     k_closure<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
+void launch_grad2(const MmArgs &a, void *stream) { k_grad2<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_stage1(const MmArgs &a, void *stream) { k_stage1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_stage2(const MmArgs &a, void *stream) { k_stage2<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
 void launch_flags(const MmArgs &a, int *flags, void *stream) {
     k_flags<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, flags);
 }

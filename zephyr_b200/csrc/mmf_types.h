@@ -9,6 +9,9 @@ namespace zg {
 namespace mmf {
 
 constexpr int NMAT = 2;  // materials per mixture in the compiled kernels
+// second order: components of the state's gradients (density, vx, vy,
+// pressure, energy, temperature, mass fractions, true densities)
+constexpr int NG = 6 + 2 * NMAT;
 
 // Primitive mixture state of every cell, one array per field (structure of
 // arrays): density, velocity, pressure, specific internal energy,
@@ -43,6 +46,11 @@ struct MmArgs {
     int *list_crp, *list_closure;
     double *qbuf;    // (4 + NMAT) doubles per closure-list entry
     double *fbuf;    // (4 + NMAT) doubles per face of every list_crp cell (4 per cell)
+    // second order (MmFluid::set_accuracy(2)): limiter, the half-step state
+    // and the limited gradients (x, y) of the state at the old layer
+    int acc, limiter;
+    MmField zhalf;
+    double *gx[NG], *gy[NG];
 };
 
 void launch_dt(const MmArgs &a, void *stream);
@@ -53,6 +61,10 @@ void launch_flux_pure_fp32(const MmArgs &a, void *stream);  // mmf_mixed.cu
 void launch_flux_crp(const MmArgs &a, void *stream);  // face fluxes, then the cell updates
 void launch_closure(const MmArgs &a, void *stream);
 void launch_flags(const MmArgs &a, int *flags, void *stream);
+// second order: compute_grad, fluxes_stage1, fluxes_stage2 (mm_fluid.cpp:439-680)
+void launch_grad2(const MmArgs &a, void *stream);
+void launch_stage1(const MmArgs &a, void *stream);
+void launch_stage2(const MmArgs &a, void *stream);
 void launch_make_states(const MmArgs &a, const double *rho, const double *vx, const double *vy, const double *P,
                         const double *beta, void *stream);
 

@@ -89,6 +89,7 @@ struct zg_ctx {
     int *d_mm_flags = nullptr;
     int *d_mm_lists = nullptr;     // 8 counters, then the two work lists of the face loop (n each)
     double *d_mm_qbuf = nullptr;   // conservative states of the closure list
+    double *d_mm2 = nullptr;       // second order: half-step state (6 + 2 NMAT fields), then 2 NG gradients
     mmf::MmField mz{}, mznext{};
     double *mnx[mmf::NMAT] = {}, *mny[mmf::NMAT] = {}, *moff[mmf::NMAT] = {};
 
@@ -141,6 +142,8 @@ struct DeviceGuard {
 };
 
 void free_mm(zg_ctx *c) {
+    cudaFree(c->d_mm2);
+    c->d_mm2 = nullptr;
     cudaFree(c->d_mm);
     cudaFree(c->d_mm_scalars);
     cudaFree(c->d_mm_flags);
@@ -1037,7 +1040,7 @@ const char *zg_kernel_name(int kind) {
     static const char *names[ZG_K_COUNT] = {"dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b",
                                             "flags", "mm_dt", "mm_recover", "mm_flux", "mm_crp",
                                             "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals",
-                                            "tr_adjust"};
+                                            "tr_adjust", "mm_grad", "mm_stage1", "mm_stage2"};
     return (kind >= 0 && kind < ZG_K_COUNT) ? names[kind] : "unknown";
 }
 
@@ -1084,6 +1087,28 @@ mmf::MmArgs make_mm_args(const zg_ctx *c) {
     a.list_closure = c->d_mm_lists + 8 + c->n;
     a.qbuf = c->d_mm_qbuf;
     a.fbuf = c->d_mm_qbuf + (4 + mmf::NMAT) * (size_t)c->n;
+    a.acc = c->mpar.accuracy;
+    a.limiter = c->mpar.limiter;
+    if (c->d_mm2) {
+        const size_t n = (size_t)c->n;
+        double *b = c->d_mm2;
+        auto take = [&b, n]() {
+            double *p0 = b;
+            b += n;
+            return p0;
+        };
+        mmf::MmField &h = a.zhalf;
+        h.rho = take();
+        h.vx = take();
+        h.vy = take();
+        h.P = take();
+        h.e = take();
+        h.T = take();
+        for (int i = 0; i < mmf::NMAT; ++i) h.b[i] = take();
+        for (int i = 0; i < mmf::NMAT; ++i) h.r[i] = take();
+        for (int k = 0; k < mmf::NG; ++k) a.gx[k] = take();
+        for (int k = 0; k < mmf::NG; ++k) a.gy[k] = take();
+    }
     return a;
 }
 
@@ -1117,6 +1142,15 @@ int enqueue_mm_step(zg_ctx *c) {
         a.dir = dir;
         a.dt_scale = scale;
         if (sub++ > 0) cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), c->stream);  // empty work lists
+        if (c->mpar.accuracy == 2) {
+            // MmFluid::integrate, second order (mm_fluid.cpp:152-168)
+            timed(c, ZG_K_MM_GRAD, [&] { mmf::launch_grad2(a, st); });
+            if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
+            timed(c, ZG_K_MM_STAGE1, [&] { mmf::launch_stage1(a, st); });
+            timed(c, ZG_K_MM_STAGE2, [&] { mmf::launch_stage2(a, st); });
+            std::swap(c->mz, c->mznext);
+            return;
+        }
         if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
         timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux_pure(a, st); });
         timed(c, ZG_K_MM_CRP, [&] { mmf::launch_flux_crp(a, st); });
@@ -1239,6 +1273,7 @@ void zg_mmf_default_params(zg_mmf_params *p) {
     p->accuracy = 1;
     p->CFL = 0.7;
     p->max_dt = 1.0e+300;
+    p->limiter = ZG_LIM_MC;  // mm_fluid.cpp:20
 }
 
 int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
@@ -1257,11 +1292,21 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown direction splitting");
     if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_PLIC)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown CRP mode");
-    if (std::min(std::max(1, p->accuracy), 2) != 1)
-        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: only the first-order MmFluid step is implemented");
+    const int acc = std::min(std::max(1, p->accuracy), 2);  // mm_fluid.cpp:46-48
+    if (acc == 2 && p->precision != ZG_FP64)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: the mixed form is built for the first-order step");
+    if (p->limiter < ZG_LIM_NONE || p->limiter > ZG_LIM_SUPERBEE)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown limiter");
     DeviceGuard g(c->device);
     c->mpar = *p;
-    c->mpar.accuracy = 1;
+    c->mpar.accuracy = acc;
+    if (acc == 2 && !c->d_mm2) {
+        // half-step state and the limited gradients (x, y) of the state
+        constexpr int NF = 6 + 2 * mmf::NMAT;
+        const size_t n2 = (size_t)c->n;
+        ZG_CUDA(c, cudaMalloc(&c->d_mm2, (NF + 2 * mmf::NG) * n2 * sizeof(double)));
+        ZG_CUDA(c, cudaMemsetAsync(c->d_mm2, 0, (NF + 2 * mmf::NG) * n2 * sizeof(double), c->stream));
+    }
     c->mpar.CFL = std::max(0.0, std::min(p->CFL, 1.0));  // mm_fluid.cpp:43-45
     if (c->mm_configured) return ZG_OK;
     size_t n = (size_t)c->n;

@@ -118,10 +118,14 @@ class MmFluid:
         self._push()
 
     def set_accuracy(self, acc: int):  # mm_fluid.cpp:46-48
-        acc = min(max(1, acc), 2)
-        if acc != 1:
-            raise ZgError(-1, "only the first-order MmFluid step is implemented")
-        self.p.accuracy = acc
+        self.p.accuracy = min(max(1, acc), 2)
+        self._push()
+
+    def set_limiter(self, name: str):  # mm_fluid.cpp:72-74 -> limiter.cxx:163-252
+        k = self._lib.zg_limiter_from_name(name.encode())
+        if k < 0:
+            raise ZgError(-1, f"unknown limiter '{name}'")
+        self.p.limiter = k
         self._push()
 
     def set_method(self, method: Fluxes):  # mm_fluid.cpp:50-61
