@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--amr-base", type=int, default=0, help="AMR base cells per side (default 512)")
     ap.add_argument("--tr-nx", type=int, default=0, help="transport mesh cells along x (default 4096)")
     ap.add_argument("--amr-kernels", choices=["fast", "mixed", "parity"], default="fast")
+    ap.add_argument("--mm-accuracy", type=int, choices=[1, 2], default=1, help="MmFluid order with --only mm")
     ap.add_argument("--amr-criterion", choices=["gradient", "reference"], default="gradient")
     return ap.parse_args()
 
@@ -288,9 +289,10 @@ def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=F
 
 MM_SIZE = 1024     # shock / water-column problem, cells per side
 MM_B_ALG = 160     # bytes per cell and step: 10 FP64 state fields read once and written once
+MM2_B_ALG = 320    # second order: the state read by both stages, the half-step state written and read, the next state written
 
 
-def mm_cpu_reference(w, steps_budget_s=10.0):
+def mm_cpu_reference(w, steps_budget_s=10.0, accuracy=1):
     """The reference's own MmFluid (oracle/_ref) on this host's cores, a few
     steps of the full problem; None when that build is absent."""
     from oracle import ref_mm as RM
@@ -298,7 +300,7 @@ def mm_cpu_reference(w, steps_budget_s=10.0):
         return None
     threads = os.cpu_count() or 1
     r = RM.RefMmFluid(w.nx, w.ny, box=w.box, bounds=w.bounds, materials="stiffened:Water,ideal:Air", CFL=0.4,
-                      accuracy=1, crp_mode=4)
+                      accuracy=accuracy, crp_mode=4)
     r.set_threads(threads)
     r.make_states(w.rho, w.vx, w.vy, w.p, w.beta)
     t0 = time.perf_counter()
@@ -311,13 +313,15 @@ def mm_cpu_reference(w, steps_budget_s=10.0):
     per = (time.perf_counter() - t0) / steps
     return {"value": w.nx * w.ny / per, "unit": METRIC, "cores": threads, "kind": "reference",
             "sample": f"{steps} step(s) of the {w.nx}x{w.ny} problem after 1 untimed step; zephyr's "
-                      f"MmFluid::update compiled from its sources (oracle/_ref); {threads} threads"}
+                      f"MmFluid::update (accuracy {accuracy}) compiled from its sources (oracle/_ref); "
+                      f"{threads} threads"}
 
 
-def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, precision=None):
-    """The multi-material step (MmFluid, first order, CRP + PLIC) on the
-    two-material shock / water-column problem, 1024 x 1024; FP64 (bit-exact)
-    or the mixed form."""
+def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, precision=None, accuracy=1):
+    """The multi-material step (MmFluid, CRP + PLIC) on the two-material
+    shock / water-column problem, 1024 x 1024; first order in FP64
+    (bit-exact) or the mixed form, or second order (FP64, bit-exact, MC
+    limiter)."""
     import zephyr_b200 as Z
     from zephyr_b200.mmf import Material, MixturePT, MmFluid
     from zephyr_b200.workloads import shock_water_column
@@ -328,6 +332,7 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, pre
     mesh = Z.EuMesh(gen, device=local_rank, stream=stream.cuda_stream)
     solver = MmFluid(MixturePT([Material.stiffened("Water"), Material.ideal("Air")]))
     solver.set_CFL(0.4)
+    solver.set_accuracy(accuracy)
     solver.add_types(mesh)
     if precision is not None:
         solver.set_precision(precision)
@@ -339,12 +344,13 @@ def mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu, pre
     cells = w.nx * w.ny
     out = {"workload": f"shock_water_column {w.nx}x{w.ny} (water column in air, planar shock, "
                        "StiffenedGas Water + IdealGas Air)",
-           "form": "FP64, bit-exact with the reference (MmFluid first order, CRP + PLIC, CFL 0.4)",
+           "form": f"FP64, bit-exact with the reference (MmFluid {('first', 'second')[accuracy - 1]} order"
+                   f"{', MC limiter' if accuracy == 2 else ''}, CRP + PLIC, CFL 0.4)",
            "ms": ms, "kernels": kernels, "launches": launches, "cells": cells,
            "final": solver.states(mesh) if precision is not None else None}
     mesh.close()
     if want_cpu:
-        out["cpu_baseline"] = mm_cpu_reference(w)
+        out["cpu_baseline"] = mm_cpu_reference(w, accuracy=accuracy)
     return out
 
 
@@ -782,7 +788,8 @@ def run_ours(args, rank, world, local_rank):
             out = transfer_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False, nx=args.tr_nx)
         elif args.only == "mm":
             out = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
-                             precision=Z.Precision.MIXED if args.amr_kernels == "mixed" else Z.Precision.FP64)
+                             precision=Z.Precision.MIXED if args.amr_kernels == "mixed" else Z.Precision.FP64,
+                             accuracy=args.mm_accuracy)
             out.pop("final")
         else:
             out = adjoint_variant(torch, dev, stream, local_rank)
@@ -847,6 +854,10 @@ def run_ours(args, rank, world, local_rank):
                     want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), precision=Z.Precision.FP64)
     mm_mx = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
                        precision=Z.Precision.MIXED)
+    mm2 = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
+                     want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), precision=Z.Precision.FP64,
+                     accuracy=2)
+    mm2.pop("final")
     z64, zmx = mm.pop("final"), mm_mx.pop("final")
     mm_err = {f"l1_rel_{name}_err_vs_fp64": float(np.sum(np.abs(zmx[:, k] - z64[:, k])) / np.sum(np.abs(z64[:, k])))
               for name, k in (("density", 0), ("pressure", 3))}
@@ -872,8 +883,8 @@ def run_ours(args, rank, world, local_rank):
 
     vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
                                    amr["ms_total"], amr_par["ms_total"], mm_mx["ms"], amr_mx["ms_total"],
-                                   trv["ms"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr = vals
+                                   trv["ms"], mm2["ms"]], dev, world)
+    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr, ms_mm2 = vals
     amr_mx["value"] = world * amr_mx["value"] * amr_mx["ms_total"] / ms_amr_mx
     amr_mx["speedup_vs_fp64"] = ms_amr / ms_amr_mx
     amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
@@ -904,7 +915,7 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
-                            mm["launches"] + mm_mx["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
+                            mm["launches"] + mm_mx["launches"] + mm2["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
                             amr_par["gpu_launches"] + amr_mx["gpu_launches"] + trv["launches"] +
                             vtuv["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
@@ -938,6 +949,13 @@ def run_ours(args, rank, world, local_rank):
                         "PT closure, PLIC and dt",
                 **mm_err, "err_after_steps": W + K, "kernels": mm_mx["kernels"],
                 "gpu_launches": int(mm_mx["launches"])},
+            "multimaterial_second_order": {
+                "value": world * mm2["cells"] * K / (ms_mm2 / 1e3), "unit": METRIC, "ms_per_step": ms_mm2 / K,
+                "workload": mm2["workload"], "form": mm2["form"], "steps": K, "warmup": W,
+                "step_achieved_GBs": MM2_B_ALG * mm2["cells"] * K / (ms_mm2 / 1e3) / 1e9,
+                "step_frac": MM2_B_ALG * mm2["cells"] * K / (ms_mm2 / 1e3) / 1e9 / peak,
+                "algorithmic_bytes_per_cell": MM2_B_ALG, "gpu_launches": int(mm2["launches"]),
+                "kernels": mm2["kernels"], "cpu_baseline": mm2.get("cpu_baseline")},
             "adjoint": adjv,
             "vtu_write": vtuv,
             "transfer": {
