@@ -24,7 +24,9 @@
 // Checkpoints: U is kept every `checkpoint_every` steps during the forward;
 // the reverse sweep recomputes each segment's U^n and U* from its checkpoint
 // and walks it backwards, so memory grows with steps / checkpoint_every plus
-// one segment, not with the number of steps.
+// two segments, not with the number of steps.  The forward keeps the last two
+// segments whole; each earlier one is recomputed on a second stream while
+// the segment after it is swept.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -498,10 +500,15 @@ struct zg_adj {
     double *d_acc = nullptr;           // per-block accumulators: J, gamma
     F4 U0{}, Ua{}, Ub{}, Ustar{}, W{}, gx{}, gy{}, lamA{}, lamB{}, lamS{};
     double *fbx = nullptr, *fby = nullptr;  // face-state cotangents, 8 n each
-    std::vector<F4> ckpt, seg, segstar;
-    // primitive states and slopes of both stages of every step of a segment,
-    // kept from the segment's recomputation for the reverse sweep
-    std::vector<F4> segW, segGx, segGy;
+    std::vector<F4> ckpt;
+    // two sets of segment storage: the states, stage values, primitive states
+    // and slopes of both stages of every step of a segment, kept from the
+    // segment's recomputation for the reverse sweep.  Segment sg lives in set
+    // sg & 1, so the recomputation of segment sg - 1 (on `rstream`) runs while
+    // segment sg is swept backwards (on `stream`).
+    std::vector<F4> seg[2], segstar[2], segW[2], segGx[2], segGy[2];
+    cudaStream_t rstream = nullptr;                                    // segment recomputation
+    cudaEvent_t ev_fwd = nullptr, ev_rec = nullptr, ev_rev = nullptr;  // ordering between the two streams
     long long launches = 0;
 };
 
@@ -541,7 +548,7 @@ int reserve(zg_adj *a, size_t ckpts, size_t seglen) {
     cudaFree(a->d_all);
     a->d_all = nullptr;
     size_t n = (size_t)a->g.n;
-    size_t fields = 10 * 4 + 16 + 4 * ckpts + 4 * (seglen + 1) + 4 * seglen + 3 * 4 * (2 * seglen);
+    size_t fields = 10 * 4 + 16 + 4 * ckpts + 2 * (4 * (seglen + 1) + 4 * seglen + 3 * 4 * (2 * seglen));
     cudaError_t e = cudaMalloc(&a->d_all, fields * n * sizeof(double));
     if (e != cudaSuccess) return afail(a, ZG_ERR_ALLOC, std::string("adjoint storage: ") + cudaGetErrorString(e));
     double *p = a->d_all;
@@ -561,22 +568,24 @@ int reserve(zg_adj *a, size_t ckpts, size_t seglen) {
     take();
     a->ckpt.assign(ckpts, F4{});
     for (auto &c : a->ckpt) c = take();
-    a->seg.assign(seglen + 1, F4{});
-    for (auto &c : a->seg) c = take();
-    a->segstar.assign(seglen, F4{});
-    for (auto &c : a->segstar) c = take();
-    for (auto *v : {&a->segW, &a->segGx, &a->segGy}) {
-        v->assign(2 * seglen, F4{});
-        for (auto &c : *v) c = take();
+    for (int b = 0; b < 2; ++b) {
+        a->seg[b].assign(seglen + 1, F4{});
+        for (auto &c : a->seg[b]) c = take();
+        a->segstar[b].assign(seglen, F4{});
+        for (auto &c : a->segstar[b]) c = take();
+        for (auto *v : {&a->segW[b], &a->segGx[b], &a->segGy[b]}) {
+            v->assign(2 * seglen, F4{});
+            for (auto &c : *v) c = take();
+        }
     }
     a->cap_ckpt = ckpts;
     a->cap_seg = seglen;
     return ZG_OK;
 }
 
-void copy4(zg_adj *a, const F4 &dst, const F4 &src) {
+void copy4(zg_adj *a, cudaStream_t st, const F4 &dst, const F4 &src) {
     for (int k = 0; k < 4; ++k)
-        cudaMemcpyAsync(dst.f[k], src.f[k], (size_t)a->g.n * sizeof(double), cudaMemcpyDeviceToDevice, a->stream);
+        cudaMemcpyAsync(dst.f[k], src.f[k], (size_t)a->g.n * sizeof(double), cudaMemcpyDeviceToDevice, st);
 }
 
 struct WG {  // primitive states and slopes of one stage
@@ -601,29 +610,37 @@ CF4T<S> cas(const F4 &x) {
 }
 
 template <class S>
-void heun_step_t(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
-                 const WG &sb, bool need_out) {
+void heun_step_t(zg_adj *a, cudaStream_t st, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out,
+                 const WG &sa, const WG &sb, bool need_out) {
     unsigned nb = nblocks(a);
-    k_prim_grad<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cf(X), p.gamma, p.limiter_eps, as<S>(sa.W), as<S>(sa.gx),
-                                                as<S>(sa.gy));
-    k_flux_update<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cas<S>(sa.W), cas<S>(sa.gx), cas<S>(sa.gy), p.gamma, cf(X),
-                                                  kNull, 0.0, 1.0, p.dt, star);
-    k_prim_grad<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cf(star), p.gamma, p.limiter_eps, as<S>(sb.W), as<S>(sb.gx),
-                                                as<S>(sb.gy));
+    k_prim_grad<S><<<nb, BLOCK, 0, st>>>(a->g, cf(X), p.gamma, p.limiter_eps, as<S>(sa.W), as<S>(sa.gx),
+                                         as<S>(sa.gy));
+    k_flux_update<S><<<nb, BLOCK, 0, st>>>(a->g, cas<S>(sa.W), cas<S>(sa.gx), cas<S>(sa.gy), p.gamma, cf(X), kNull,
+                                           0.0, 1.0, p.dt, star);
+    k_prim_grad<S><<<nb, BLOCK, 0, st>>>(a->g, cf(star), p.gamma, p.limiter_eps, as<S>(sb.W), as<S>(sb.gx),
+                                         as<S>(sb.gy));
     a->launches += 3;
     if (!need_out) return;
-    k_flux_update<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cas<S>(sb.W), cas<S>(sb.gx), cas<S>(sb.gy), p.gamma,
-                                                  cf(star), cf(X), 0.5, 0.5, p.dt, out);
+    k_flux_update<S><<<nb, BLOCK, 0, st>>>(a->g, cas<S>(sb.W), cas<S>(sb.gx), cas<S>(sb.gy), p.gamma, cf(star),
+                                           cf(X), 0.5, 0.5, p.dt, out);
     ++a->launches;
 }
-void heun_step(zg_adj *a, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out, const WG &sa,
-               const WG &sb, bool need_out = true) {
-    if (p.precision == ZG_MIXED) heun_step_t<float>(a, p, X, star, out, sa, sb, need_out);
-    else heun_step_t<double>(a, p, X, star, out, sa, sb, need_out);
+void heun_step(zg_adj *a, cudaStream_t st, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out,
+               const WG &sa, const WG &sb, bool need_out = true) {
+    if (p.precision == ZG_MIXED) heun_step_t<float>(a, st, p, X, star, out, sa, sb, need_out);
+    else heun_step_t<double>(a, st, p, X, star, out, sa, sb, need_out);
 }
 WG scratch(const zg_adj *a) { return WG{a->W, a->gx, a->gy}; }
-WG seg_stage(const zg_adj *a, int t, int stage) {
-    return WG{a->segW[2 * t + stage], a->segGx[2 * t + stage], a->segGy[2 * t + stage]};
+WG seg_stage(const zg_adj *a, int b, int t, int stage) {
+    return WG{a->segW[b][2 * t + stage], a->segGx[b][2 * t + stage], a->segGy[b][2 * t + stage]};
+}
+// recompute segment sg (len steps from checkpoint sg) into set sg & 1
+void recompute(zg_adj *a, cudaStream_t st, const zg_adj_params &p, int sg, int len) {
+    const int b = sg & 1;
+    copy4(a, st, a->seg[b][0], a->ckpt[sg]);
+    for (int t = 0; t < len; ++t)
+        heun_step(a, st, p, a->seg[b][t], a->segstar[b][t], a->seg[b][t + 1], seg_stage(a, b, t, 0),
+                  seg_stage(a, b, t, 1), t + 1 < len);
 }
 
 // out = base_coef * base + add + L'(X)^T (coef * mu), with X's primitive
@@ -717,6 +734,15 @@ int zg_adj_create(zg_adj **out, int device, int nx, int ny, double x_min, double
         delete a;
         return ZG_ERR_ALLOC;
     }
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);  // lo: the numerically largest, lowest priority
+    if (cudaStreamCreateWithPriority(&a->rstream, cudaStreamNonBlocking, lo) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_fwd, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_rec, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_rev, cudaEventDisableTiming) != cudaSuccess) {
+        zg_adj_destroy(a);
+        return ZG_ERR_CUDA;
+    }
     *out = a;
     return ZG_OK;
 }
@@ -727,6 +753,12 @@ int zg_adj_destroy(zg_adj *a) {
         DevGuard gd(a->device);
         if (a->stream) cudaStreamSynchronize(a->stream);
         else cudaDeviceSynchronize();
+        if (a->rstream) {
+            cudaStreamSynchronize(a->rstream);
+            cudaStreamDestroy(a->rstream);
+        }
+        for (cudaEvent_t e : {a->ev_fwd, a->ev_rec, a->ev_rev})
+            if (e) cudaEventDestroy(e);
         cudaFree(a->d_all);
         cudaFree(a->d_acc);
     }
@@ -763,7 +795,7 @@ int zg_adj_forward(zg_adj *a, const zg_adj_params *p, const double *rho, const d
     ++a->launches;
     F4 cur = a->Ua, nxt = a->Ub;
     for (int s = 0; s < p->steps; ++s) {
-        heun_step(a, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
+        heun_step(a, a->stream, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
         std::swap(cur, nxt);
     }
     cudaMemsetAsync(a->d_acc, 0, 2 * nacc(a) * sizeof(double), a->stream);
@@ -797,23 +829,25 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
     if (np == 0) return afail(a, ZG_ERR_ARG, "no cell centre inside the probe box");
     CF4 w0{{rho, u, v, pr}};
 
-    // forward with checkpoints at steps 0, K, 2K, ...; the last segment keeps
-    // its states and stages for the reverse sweep
-    const int last0 = (nseg - 1) * K;
+    // forward with checkpoints at steps 0, K, 2K, ...; the last two segments
+    // keep their states and stages (one in each set) for the reverse sweep
+    const int stored0 = std::max(0, nseg - 2);  // first segment the forward keeps
+    const int keep0 = stored0 * K;
     k_init<<<nb, BLOCK, 0, a->stream>>>(a->g, w0, p->gamma, a->ckpt[0]);
     ++a->launches;
     F4 cur = a->ckpt[0];
     for (int s = 0; s < N; ++s) {
-        if (s >= last0) {
-            const int t = s - last0;
-            if (t == 0) copy4(a, a->seg[0], cur);
-            heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1], seg_stage(a, t, 0), seg_stage(a, t, 1));
-            cur = a->seg[t + 1];
+        if (s >= keep0) {
+            const int sg = s / K, t = s - sg * K, b = sg & 1;
+            if (t == 0) copy4(a, a->stream, a->seg[b][0], cur);
+            heun_step(a, a->stream, *p, a->seg[b][t], a->segstar[b][t], a->seg[b][t + 1], seg_stage(a, b, t, 0),
+                      seg_stage(a, b, t, 1));
+            cur = a->seg[b][t + 1];
             continue;
         }
         bool keep = (s + 1) % K == 0 && (s + 1) / K < nseg;
         F4 nxt = keep ? a->ckpt[(s + 1) / K] : (cur.f[0] == a->Ua.f[0] ? a->Ub : a->Ua);
-        heun_step(a, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
+        heun_step(a, a->stream, *p, cur, a->Ustar, nxt, scratch(a), scratch(a));
         cur = nxt;
     }
     // J and lambda^N
@@ -824,22 +858,30 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
     ++a->launches;
     double *gacc = a->d_acc + nacc(a);
 
-    // reverse sweep, segment by segment
+    // reverse sweep, segment by segment.  Below the two kept segments, the
+    // recomputation of segment sg - 1 (rstream, set (sg - 1) & 1) overlaps the
+    // sweep of segment sg (stream, set sg & 1); it starts once the checkpoints
+    // exist and the sweep of segment sg + 1, which used the same set, is
+    // done.  Every recomputation is waited for on `stream` before its segment
+    // is swept, so the work of both streams has ended when `stream` has.
+    cudaEventRecord(a->ev_fwd, a->stream);
+    cudaStreamWaitEvent(a->rstream, a->ev_fwd, 0);
     for (int sg = nseg - 1; sg >= 0; --sg) {
-        const int s0 = sg * K, len = std::min(K, N - s0);
-        if (sg != nseg - 1) {  // recompute the segment from its checkpoint
-            copy4(a, a->seg[0], a->ckpt[sg]);
-            for (int t = 0; t < len; ++t)
-                heun_step(a, *p, a->seg[t], a->segstar[t], a->seg[t + 1], seg_stage(a, t, 0), seg_stage(a, t, 1),
-                          t + 1 < len);
+        const int s0 = sg * K, len = std::min(K, N - s0), b = sg & 1;
+        if (sg < stored0) cudaStreamWaitEvent(a->stream, a->ev_rec, 0);  // segment sg recomputed
+        if (sg > 0 && sg - 1 < stored0) {
+            if (sg + 1 < nseg) cudaStreamWaitEvent(a->rstream, a->ev_rev, 0);  // set of sg - 1 free
+            recompute(a, a->rstream, *p, sg - 1, K);
+            cudaEventRecord(a->ev_rec, a->rstream);
         }
         for (int t = len - 1; t >= 0; --t) {
             // stage B: lambda* = 1/2 lambda^{n+1} + L'(U*)^T (dt/2 lambda^{n+1})
-            vjp(a, *p, a->segstar[t], seg_stage(a, t, 1), lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
+            vjp(a, *p, a->segstar[b][t], seg_stage(a, b, t, 1), lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
             // stage A: lambda^n = 1/2 lambda^{n+1} + lambda* + L'(U^n)^T (dt lambda*)
-            vjp(a, *p, a->seg[t], seg_stage(a, t, 0), a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
+            vjp(a, *p, a->seg[b][t], seg_stage(a, b, t, 0), a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
             std::swap(lam, lam_prev);
         }
+        cudaEventRecord(a->ev_rev, a->stream);
     }
     k_seed<<<nb, BLOCK, 0, a->stream>>>(a->g, w0, p->gamma, cf(lam), dJ_drho, gacc);
     ++a->launches;
