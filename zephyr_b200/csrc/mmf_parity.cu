@@ -388,18 +388,50 @@ __device__ __forceinline__ MSt<NM> ghost(const MSt<NM> &zc, const FaceG &g) {
 // next to mixed cells; else gradient::LSM and gradient::limiting
 // (gradient.h:226-282, 412-474) on every component, in the 2-D reduction of
 // the 3x3 system (A(i,2), A(2,j) exact zeros, A(2,2) set to 1).
+// component k of the to_arr order, selected without indexing the parameter
+// block dynamically
+__device__ __forceinline__ double *comp_ptr(const MmField &f, int k) {
+    double *p = f.rho;
+    if (k == 1) p = f.vx;
+    if (k == 2) p = f.vy;
+    if (k == 3) p = f.P;
+    if (k == 4) p = f.e;
+    if (k == 5) p = f.T;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        if (k == 6 + i) p = f.b[i];
+        if (k == 6 + NM + i) p = f.r[i];
+    }
+    return p;
+}
+__device__ __forceinline__ double *grad_ptr(double *const *g, int k) {
+    double *p = g[0];
+#pragma unroll
+    for (int j = 1; j < NG; ++j)
+        if (k == j) p = g[j];
+    return p;
+}
+
+// The face geometry (weights, offsets, the 2x2 system) is formed once; the
+// components then go one at a time through the same least-squares and
+// limiting arithmetic, so only one component's neighbour differences are
+// live at a time.
 __global__ void __launch_bounds__(BLOCK) k_grad2(MmArgs a) {
     const int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= a.mesh.n) return;
     StructAcc c(a.mesh, ic);
-    const MSt<NM> zc = load(a.z, ic);
     bool set_zero = false;
     if (a.crp != CRP_NONE) {
-        set_zero = frac_index(zc.b) < 0;
+        Frac<NM> b;
+#pragma unroll
+        for (int i = 0; i < NM; ++i) b.f[i] = a.z.b[i][ic];
+        set_zero = frac_index(b) < 0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             FaceG g = c.face(s);
-            if (frac_index(load(a.z, g.nb).b) < 0) set_zero = true;
+#pragma unroll
+            for (int i = 0; i < NM; ++i) b.f[i] = a.z.b[i][g.nb];
+            if (frac_index(b) < 0) set_zero = true;
         }
     }
     if (set_zero) {
@@ -411,17 +443,19 @@ __global__ void __launch_bounds__(BLOCK) k_grad2(MmArgs a) {
         return;
     }
     const double pcx = c.cx(), pcy = c.cy();
-    double zcv[NG], dn[4][NG], wv[4], drx[4], dry[4], drnx[4], drny[4];
-    to_arr(zc, zcv);
+    double wv[4], drx[4], dry[4], drnx[4], drny[4], gvx[4], gvy[4];
+    int nb[4];
+    bool bnd[4];
+    const double zvx = a.z.vx[ic], zvy = a.z.vy[ic];
     double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
-    double Fx[NG], Fy[NG];
-#pragma unroll
-    for (int k = 0; k < NG; ++k) Fx[k] = Fy[k] = 0.0;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
         FaceG g = c.face(s);
-        double znv[NG];
-        to_arr(!is_boundary(g.flag) ? load(a.z, g.nb) : ghost(zc, g), znv);
+        nb[s] = g.nb;
+        bnd[s] = is_boundary(g.flag);
+        gvx[s] = zvx;  // boundary_value: the cell's own state, walls reflect the velocity
+        gvy[s] = zvy;
+        if (g.flag == BC_WALL) wall_velocity(g, zvx, zvy, gvx[s], gvy[s]);
         double ncx, ncy;
         neib_center(c, g, s, pcx, pcy, ncx, ncy);
         const double rx = ncx - pcx, ry = ncy - pcy;
@@ -438,40 +472,40 @@ __global__ void __launch_bounds__(BLOCK) k_grad2(MmArgs a) {
         dry[s] = ry;
         drnx[s] = nxx;
         drny[s] = nyy;
-#pragma unroll
-        for (int k = 0; k < NG; ++k) {
-            const double dF = znv[k] - zcv[k];
-            dn[s][k] = dF;
-            Fx[k] += w * dF * nxx;
-            Fy[k] += w * dF * nyy;
-        }
     }
     if (fabs(A11) < 1e-8) A11 = 1.0;
     const double det = A11 * A00 + (-A01) * A10;
     const double inv = 1.0 / det;
     const double B00 = A11 * inv, B01 = (-A01) * inv, B10 = (-A10) * inv, B11 = A00 * inv;
-    double Lx[NG], Ly[NG];
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < NG; ++k) {
-        const double g0x = B00 * Fx[k] + B01 * Fy[k];
-        const double g0y = B10 * Fx[k] + B11 * Fy[k];
+        const double *f = comp_ptr(a.z, k);
+        const double zk = f[ic];
+        double dn[4], Fx = 0.0, Fy = 0.0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            double zn = bnd[s] ? zk : f[nb[s]];
+            if (bnd[s] && k == 1) zn = gvx[s];
+            if (bnd[s] && k == 2) zn = gvy[s];
+            const double dF = zn - zk;
+            dn[s] = dF;
+            Fx += wv[s] * dF * drnx[s];
+            Fy += wv[s] * dF * drny[s];
+        }
+        const double g0x = B00 * Fx + B01 * Fy;
+        const double g0y = B10 * Fx + B11 * Fy;
         double lx = 0.0, ly = 0.0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
-            const double dF_p = dn[s][k];
+            const double dF_p = dn[s];
             const double du_n = g0x * drx[s] + g0y * dry[s];
             const double dF_m = 2.0 * du_n - dF_p;
             const double dF_lim = limiter2(a.limiter, dF_m, dF_p) * dF_p;
             lx += wv[s] * dF_lim * drnx[s];
             ly += wv[s] * dF_lim * drny[s];
         }
-        Lx[k] = lx;
-        Ly[k] = ly;
-    }
-#pragma unroll
-    for (int k = 0; k < NG; ++k) {
-        a.gx[k][ic] = B00 * Lx[k] + B01 * Ly[k];
-        a.gy[k][ic] = B10 * Lx[k] + B11 * Ly[k];
+        grad_ptr(a.gx, k)[ic] = B00 * lx + B01 * ly;
+        grad_ptr(a.gy, k)[ic] = B10 * lx + B11 * ly;
     }
 }
 
@@ -546,38 +580,120 @@ __global__ void __launch_bounds__(BLOCK) k_stage1(MmArgs a) {
 }
 
 // fluxes_stage2 (mm_fluid.cpp:589-680): the step from the half-step face
-// values, extrapolated with the old layer's gradients, through calc_flux
+// values, extrapolated with the old layer's gradients, through calc_flux.
+// One face of cell ic: the flux through face s, in the global frame, times
+// the face area.
+__device__ void face_term2(const MmArgs &a, int ic, int s, double dt, double *out, bool &bad) {
+    StructAcc c(a.mesh, ic);
+    const double pcx = c.cx(), pcy = c.cy(), V_c = c.vol();
+    FaceG g = c.face(s);
+    const bool bnd = is_boundary(g.flag);
+    double ncx, ncy;
+    neib_center(c, g, s, pcx, pcy, ncx, ncy);
+    const double V_n = V_c;
+    MSt<NM> zm = shifted(a, load(a.zhalf, ic), ic, g.fcx - pcx, g.fcy - pcy);
+    interp_update(a.mix, zm);
+    MSt<NM> zp;
+    if (!bnd) {
+        zp = shifted(a, load(a.zhalf, g.nb), g.nb, g.fcx - ncx, g.fcy - ncy);
+        interp_update(a.mix, zp);
+    } else {
+        zp = ghost(zm, g);
+    }
+    to_local(g.nx, g.ny, zm.vx, zm.vy, zm.vx, zm.vy);
+    to_local(g.nx, g.ny, zp.vx, zp.vy, zp.vx, zp.vy);
+    const double S = g.area;
+    QVd<NM> lf = calc_flux(a, dt, ic, g, zm, zp, V_c / S, V_n / S, bad);
+    const double mxx = g.nx * lf.a[1] + -g.ny * lf.a[2] + 0.0 * 0.0;
+    const double myy = g.ny * lf.a[1] + g.nx * lf.a[2] + 0.0 * 0.0;
+    lf.a[1] = mxx;
+    lf.a[2] = myy;
+#pragma unroll
+    for (int k = 0; k < 4 + NM; ++k) out[k] = lf.a[k] * S;
+}
+
+// the update of cell ic from its summed face terms (mm_fluid.cpp:662-679)
+__device__ __forceinline__ void update2(const MmArgs &a, int ic, double dt, const QVd<NM> &flux, bool bad) {
+    const MSt<NM> zc = load(a.z, ic);
+    QVd<NM> q = q_of(zc);
+    const double coef = dt / a.mesh.vol;
+#pragma unroll
+    for (int k = 0; k < 4 + NM; ++k) q.a[k] -= coef * flux.a[k];
+    if (q.a[0] < 0.0) bad = true;  // the reference throws (mm_fluid.cpp:670-672)
+    if (bad) atomicOr(a.err, 1);
+    store(a.znext, ic, state_of_q(a.mix, q, zc.P, zc.T, zc.r));
+}
+
+// Every face of every cell (used without composite fluxes, CRP mode NONE).
 __global__ void __launch_bounds__(BLOCK) k_stage2(MmArgs a) {
     const int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= a.mesh.n) return;
     const double dt = a.dt_scale * *a.dt_out;
+    QVd<NM> flux = qv_zero<NM>();
+    bool bad = false;
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        if (skip_face(a.dir, s)) continue;
+        double term[4 + NM];
+        face_term2(a, ic, s, dt, term, bad);
+#pragma unroll
+        for (int k = 0; k < 4 + NM; ++k) flux.a[k] += term[k];
+    }
+    update2(a, ic, dt, flux, bad);
+}
+
+// interpolation_update of a face value that came out pure (the common case);
+// false, and z untouched past its fractions, when it is mixed
+__device__ __forceinline__ bool interp_pure(const MixD<NM> &mx, MSt<NM> &z) {
+    normalize(z.b);
+    const int idx = frac_index(z.b);
+    if (idx < 0) return false;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) z.r[i] = i == idx ? z.rho : MM_NAN;
+    z.e = m_energy_rP(mx.mat[idx], z.rho, z.P);
+    z.T = m_temperature_rP(mx.mat[idx], z.rho, z.P);
+    return true;
+}
+
+// With composite fluxes (CRP modes): cells all of whose face values come out
+// pure take calc_flux's plain-HLLC branch here, with the same operations as
+// face_term2; a cell with a mixed face value goes to the work list, whose
+// faces k_stage2_faces evaluates one per thread and k_crp_update sums in slot
+// order.  The lean kernel keeps the Newton closures and the composite Riemann
+// solver out of the common path (fewer registers, more resident warps).
+__global__ void __launch_bounds__(BLOCK) k_stage2_pure(MmArgs a) {
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    const double dt = a.dt_scale * *a.dt_out;
     StructAcc c(a.mesh, ic);
-    const double pcx = c.cx(), pcy = c.cy(), V_c = c.vol();
-    const MSt<NM> zc = load(a.z, ic);
+    const double pcx = c.cx(), pcy = c.cy();
     const MSt<NM> zch = load(a.zhalf, ic);
     QVd<NM> flux = qv_zero<NM>();
     bool bad = false;
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < 4; ++s) {
         if (skip_face(a.dir, s)) continue;
         FaceG g = c.face(s);
         const bool bnd = is_boundary(g.flag);
         double ncx, ncy;
         neib_center(c, g, s, pcx, pcy, ncx, ncy);
-        const double V_n = V_c;
         MSt<NM> zm = shifted(a, zch, ic, g.fcx - pcx, g.fcy - pcy);
-        interp_update(a.mix, zm);
+        bool pure = interp_pure(a.mix, zm);
         MSt<NM> zp;
-        if (!bnd) {
+        if (pure && !bnd) {
             zp = shifted(a, load(a.zhalf, g.nb), g.nb, g.fcx - ncx, g.fcy - ncy);
-            interp_update(a.mix, zp);
+            pure = interp_pure(a.mix, zp);
         } else {
             zp = ghost(zm, g);
+        }
+        if (!pure) {
+            a.list_crp[atomicAdd(&a.counts[0], 1)] = ic;
+            return;
         }
         to_local(g.nx, g.ny, zm.vx, zm.vy, zm.vx, zm.vy);
         to_local(g.nx, g.ny, zp.vx, zp.vy, zp.vx, zp.vy);
         const double S = g.area;
-        QVd<NM> lf = calc_flux(a, dt, ic, g, zm, zp, V_c / S, V_n / S, bad);
+        QVd<NM> lf = hllc(a.mix, zm, zp, bad);
         const double mxx = g.nx * lf.a[1] + -g.ny * lf.a[2] + 0.0 * 0.0;
         const double myy = g.ny * lf.a[1] + g.nx * lf.a[2] + 0.0 * 0.0;
         lf.a[1] = mxx;
@@ -585,13 +701,20 @@ __global__ void __launch_bounds__(BLOCK) k_stage2(MmArgs a) {
 #pragma unroll
         for (int k = 0; k < 4 + NM; ++k) flux.a[k] += lf.a[k] * S;
     }
-    QVd<NM> q = q_of(zc);
-    const double coef = dt / V_c;
+    update2(a, ic, dt, flux, bad);
+}
+__global__ void __launch_bounds__(BLOCK) k_stage2_faces(MmArgs a) {
+    const double dt = a.dt_scale * *a.dt_out;
+    const int count = 4 * a.counts[0];
+    for (int t = blockIdx.x * BLOCK + threadIdx.x; t < count; t += gridDim.x * BLOCK) {
+        if (skip_face(a.dir, t & 3)) continue;
+        bool bad = false;
+        double term[4 + NM];
+        face_term2(a, a.list_crp[t >> 2], t & 3, dt, term, bad);
 #pragma unroll
-    for (int k = 0; k < 4 + NM; ++k) q.a[k] -= coef * flux.a[k];
-    if (q.a[0] < 0.0) bad = true;  // the reference throws (mm_fluid.cpp:670-672)
-    if (bad) atomicOr(a.err, 1);
-    store(a.znext, ic, state_of_q(a.mix, q, zc.P, zc.T, zc.r));
+        for (int k = 0; k < 4 + NM; ++k) a.fbuf[(size_t)t * (4 + NM) + k] = term[k];
+        if (bad) atomicOr(a.err, 1);
+    }
 }
 
 static inline unsigned blocks(const MmArgs &a) { return (unsigned)((a.mesh.n + BLOCK - 1) / BLOCK); }
@@ -611,7 +734,16 @@ void launch_closure(const MmArgs &a, void *stream) {
 }
 void launch_grad2(const MmArgs &a, void *stream) { k_grad2<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
 void launch_stage1(const MmArgs &a, void *stream) { k_stage1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
-void launch_stage2(const MmArgs &a, void *stream) { k_stage2<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_stage2(const MmArgs &a, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (a.crp == CRP_NONE) {
+        k_stage2<<<blocks(a), BLOCK, 0, st>>>(a);
+        return;
+    }
+    k_stage2_pure<<<blocks(a), BLOCK, 0, st>>>(a);
+    k_stage2_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, st>>>(a);
+    k_crp_update<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, st>>>(a);
+}
 void launch_flags(const MmArgs &a, int *flags, void *stream) {
     k_flags<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, flags);
 }
