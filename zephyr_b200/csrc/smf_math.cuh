@@ -346,9 +346,15 @@ __device__ inline Cons godunov(const Prim &zL, const Prim &zR, const EosD &eos) 
     return flux_from_p(z);
 }
 
+// The exact solver out of line: inlined, its Newton and fan code raised the
+// register demand of every face kernel and made the HLLC path spill.
+static __device__ __noinline__ Cons godunov_ool(const Prim zL, const Prim zR, const EosD eos) {
+    return godunov(zL, zR, eos);
+}
+
 __device__ inline Cons num_flux(int kind, const Prim &zL, const Prim &zR, const EosD &eos) {
     switch (kind) {
-        case FLUX_GODUNOV: return godunov(zL, zR, eos);
+        case FLUX_GODUNOV: return godunov_ool(zL, zR, eos);
         case FLUX_RUSANOV: return rusanov(zL, zR, eos);
         case FLUX_HLL: return hll(zL, zR, eos);
         default: return hllc(zL, zR, eos);

@@ -150,7 +150,7 @@ __device__ inline C4<R> face_flux(int kind, bool robust, const P5<R> &L, const P
     if (kind == FLUX_GODUNOV) {
         const Prim a{(double)L.r, (double)L.u, (double)L.v, (double)L.p, (double)L.e};
         const Prim b{(double)Rs.r, (double)Rs.u, (double)Rs.v, (double)Rs.p, (double)Rs.e};
-        const Cons f = godunov(a, b, eosd);
+        const Cons f = godunov_ool(a, b, eosd);
         return C4<R>{(R)f.r, (R)f.mu, (R)f.mv, (R)f.E};
     }
     if (kind == FLUX_RUSANOV) return rusanov(L, Rs, eos);
