@@ -56,6 +56,16 @@ void launch_faces(const SmfArgs &a, const Fields<double> &f, int mode, void *str
     dim3 block(TX, TY);
     dim3 grid((a.mesh.ny + TX - 2) / (TX - 1), (a.mesh.nx + TY - 2) / (TY - 1));
     cudaStream_t s = (cudaStream_t)stream;
+    // HLLC and HLL get kernels without the other fluxes' code (registers)
+    if (a.flux == FLUX_HLLC || a.flux == FLUX_HLL) {
+        switch (mode) {
+            case 0: tiled::k_faces<double, false, 0, TX, TY, FMINB, false><<<grid, block, 0, s>>>(a, f); break;
+            case 1: tiled::k_faces<double, false, 1, TX, TY, FMINB, false><<<grid, block, 0, s>>>(a, f); break;
+            case 2: tiled::k_faces<double, false, 2, TX, TY, FMINB, false><<<grid, block, 0, s>>>(a, f); break;
+            default: tiled::k_faces<double, false, 3, TX, TY, FMINB, false><<<grid, block, 0, s>>>(a, f); break;
+        }
+        return;
+    }
     switch (mode) {
         case 0: tiled::k_faces<double, false, 0, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
         case 1: tiled::k_faces<double, false, 1, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;

@@ -142,11 +142,14 @@ __device__ inline C4<R> rusanov(const P5<R> &L, const P5<R> &Rs, const EosR<R> &
 }
 
 // The selected numerical flux in the face frame (HLL on isolated cells).
-// Godunov's exact Riemann solver runs in FP64 whatever R is.
-template <typename R>
+// Godunov's exact Riemann solver runs in FP64 whatever R is.  GEN = false:
+// the kernel was launched for HLLC or HLL only, and carries neither the
+// exact solver's call nor Rusanov.
+template <typename R, bool GEN = true>
 __device__ inline C4<R> face_flux(int kind, bool robust, const P5<R> &L, const P5<R> &Rs, const EosR<R> &eos,
                                   const EosD &eosd) {
     if (robust || kind == FLUX_HLL) return hll(L, Rs, eos);
+    if (!GEN) return hllc(L, Rs, eos);
     if (kind == FLUX_GODUNOV) {
         const Prim a{(double)L.r, (double)L.u, (double)L.v, (double)L.p, (double)L.e};
         const Prim b{(double)Rs.r, (double)Rs.u, (double)Rs.v, (double)Rs.p, (double)Rs.e};
@@ -554,7 +557,7 @@ struct FaceSmem {
     unsigned long long red[TX * TY / 32];
 };
 
-template <typename R, bool MIXED, int MODE, int TX, int TY, int MINB = 1>
+template <typename R, bool MIXED, int MODE, int TX, int TY, int MINB = 1, bool GEN = true>
 __global__ void __launch_bounds__(TX *TY, MINB) k_faces(SmfArgs a, Fields<R> f) {
     __shared__ FaceSmem<R, TX, TY> sm;
     const StructMesh &m = a.mesh;
@@ -660,7 +663,7 @@ __global__ void __launch_bounds__(TX *TY, MINB) k_faces(SmfArgs a, Fields<R> f) 
             }
             to_local(s_own, zm.u, zm.v);
             to_local(s_own, zp.u, zp.v);
-            C4<R> lf = face_flux(a.flux, robust, zm, zp, eos, a.eos);
+            C4<R> lf = face_flux<R, GEN>(a.flux, robust, zm, zp, eos, a.eos);
             to_global(s_own, lf.mu, lf.mv);
             out[0] = sgn * lf.r;
             out[1] = sgn * lf.mu;
