@@ -86,8 +86,13 @@ enum zg_precision { ZG_FP64 = 0, ZG_MIXED = 1 };
 
 /* Kernel family.  PARITY evaluates every face flux from both sides in the
  * reference's order of operations without fused multiply-adds (bit-exact with
- * the reference); FAST computes each face once and lets the compiler fuse. */
-enum zg_kernels { ZG_KERNELS_PARITY = 0, ZG_KERNELS_FAST = 1 };
+ * the reference); FAST computes each face once and lets the compiler fuse.
+ * On a rectangle, FAST runs each second-order stage with HLLC or HLL as ONE
+ * kernel (gradients, predictor, faces and update of a tile in shared
+ * memory); FAST_TWO_PASS keeps the earlier two kernels per stage (gradients
+ * and predictor stored in HBM, then the face pass), for comparison.  The
+ * other fluxes use the two-pass kernels in both FAST families. */
+enum zg_kernels { ZG_KERNELS_PARITY = 0, ZG_KERNELS_FAST = 1, ZG_KERNELS_FAST_TWO_PASS = 2 };
 
 /* Solver configuration: SmFluid(Eos::Ptr) plus its setters
  * (math/solver/sm_fluid.h:41-71; defaults sm_fluid.cpp:16-23). */
@@ -291,6 +296,7 @@ enum zg_kernel_kind {
     ZG_K_MM_GRAD,     /* multi-material second order: limited gradients (MmFluid::compute_grad) */
     ZG_K_MM_STAGE1,   /* multi-material predictor (MmFluid::fluxes_stage1) */
     ZG_K_MM_STAGE2,   /* multi-material corrector (MmFluid::fluxes_stage2) */
+    ZG_K_STEP,        /* fused predictor-corrector step of a rectangle (update in one kernel) */
     ZG_K_COUNT
 };
 

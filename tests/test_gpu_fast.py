@@ -23,13 +23,13 @@ LIMS = {"MC": 3, "van Albada": 5, "minmod": 2, "superbee": 12}
 
 
 def _setup(Z, nx, ny, bounds, box=(0.0, 1.0, 0.0, 1.0), acc=2, lim="van Albada", scheme=0, CFL=0.4, eos=None,
-           precision=None, flux=3):
+           precision=None, flux=3, kernels=None, threads=8):
     eos = eos or Z.IdealGas(1.4)
     gen = Z.Rectangle(*box)
     gen.set_boundaries(Z.Boundaries(*bounds))
     gen.set_sizes(nx, ny)
     mesh = Z.EuMesh(gen)
-    solver = Z.SmFluid(eos, precision=precision or Z.Precision.FP64, kernels=Z.Kernels.FAST)
+    solver = Z.SmFluid(eos, precision=precision or Z.Precision.FP64, kernels=kernels or Z.Kernels.FAST)
     solver.set_accuracy(acc)
     solver.set_CFL(CFL)
     solver.set_limiter(lim)
@@ -37,7 +37,7 @@ def _setup(Z, nx, ny, bounds, box=(0.0, 1.0, 0.0, 1.0), acc=2, lim="van Albada",
     solver.set_scheme(Z.Scheme(scheme))
     solver.add_types(mesh)
     osv = O.Solver(O.Mesh(nx, ny, *box, bounds=bounds), eos_kind=eos.kind, gamma=eos.gamma, P0=eos.P0,
-                   e0=eos.e0, flux=flux, limiter=LIMS[lim], accuracy=acc, scheme=scheme, CFL=CFL, threads=8)
+                   e0=eos.e0, flux=flux, limiter=LIMS[lim], accuracy=acc, scheme=scheme, CFL=CFL, threads=threads)
     return mesh, solver, osv
 
 
@@ -93,6 +93,15 @@ CASES = [
     ("godunov first order riemann", dict(nx=48, ny=48, bounds=(2, 2, 2, 2), acc=1, lim="MC", flux=0), "riemann"),
     ("godunov MC riemann", dict(nx=48, ny=48, bounds=(2, 2, 1, 1), lim="MC", flux=0), "riemann"),
     ("rusanov fourier periodic", dict(nx=48, ny=48, bounds=(3, 3, 3, 3), flux=1), "fourier"),
+    # tile edges of the fused kernels (30 x 14 interior cells per block):
+    # sizes that leave partial tiles, thin periodic axes, mixed boundaries
+    ("tiles periodic 43x61", dict(nx=43, ny=61, bounds=(3, 3, 3, 3)), "random"),
+    ("tiles walls zoe 29x95", dict(nx=29, ny=95, bounds=(1, 2, 2, 1), lim="MC"), "random"),
+    ("tiles thin periodic 3x70", dict(nx=3, ny=70, bounds=(3, 3, 1, 1)), "random"),
+    ("tiles thin periodic 70x2", dict(nx=70, ny=2, bounds=(2, 2, 3, 3), lim="minmod"), "random"),
+    ("tiles hll 31x31", dict(nx=31, ny=31, bounds=(1, 1, 2, 2), flux=2, lim="MC"), "random"),
+    ("tiles heun 57x33 walls", dict(nx=57, ny=33, bounds=(1, 1, 1, 1), scheme=1), "random"),
+    ("tiles heun periodic 15x31", dict(nx=15, ny=31, bounds=(3, 3, 3, 3), scheme=1, lim="superbee"), "random"),
 ]
 
 
@@ -111,11 +120,85 @@ def _state(kind, nx, ny):
     return rho, u, v, p, p / (0.4 * rho)
 
 
+@pytest.mark.parametrize("family", ["FAST", "FAST_TWO_PASS"])
 @pytest.mark.parametrize("name,cfg,kind", CASES, ids=[c[0] for c in CASES])
-def test_fast_within_tolerance_per_step(gpu_lib, name, cfg, kind):
+def test_fast_within_tolerance_per_step(gpu_lib, name, cfg, kind, family):
     Z = gpu_lib
-    mesh, solver, osv = _setup(Z, **cfg)
+    mesh, solver, osv = _setup(Z, **cfg, kernels=Z.Kernels[family])
     _per_step(mesh, solver, osv, _state(kind, cfg["nx"], cfg["ny"]), 12, name)
+
+
+@pytest.mark.parametrize("family", ["FAST", "FAST_TWO_PASS"])
+@pytest.mark.parametrize("scheme", [0, 1], ids=["predictor_corrector", "heun"])
+def test_fast_headline_size_per_step(gpu_lib, family, scheme):
+    """The benchmark's own workload (2048 x 2048 periodic smooth data, van
+    Albada, HLLC, CFL 0.4) through the FAST kernels: each step starts from the
+    oracle's state and must land within 1e-12 of the oracle's next state."""
+    import os
+    Z = gpu_lib
+    from zephyr_b200.workloads import fourier_smooth
+    n = 2048
+    mesh, solver, osv = _setup(Z, n, n, (3, 3, 3, 3), scheme=scheme, kernels=Z.Kernels[family],
+                               threads=max(8, os.cpu_count() or 8))
+    worst = _per_step(mesh, solver, osv, fourier_smooth(n).state, 2, f"2048^2 {family} scheme {scheme}")
+    print(f"2048^2 {family} scheme {scheme}: worst conserved rel diff per step {worst:.3e}")
+
+
+@pytest.mark.parametrize("scheme", [0, 1], ids=["predictor_corrector", "heun"])
+def test_mixed_headline_size_one_step(gpu_lib, scheme):
+    """One mixed-form step of the benchmark's workload from the oracle's
+    state: density within 1e-6 relative of the FP64 oracle's next state (FP32
+    face arithmetic, FP64 update)."""
+    import os
+    Z = gpu_lib
+    from zephyr_b200.workloads import fourier_smooth
+    n = 2048
+    mesh, solver, osv = _setup(Z, n, n, (3, 3, 3, 3), scheme=scheme, precision=Z.Precision.MIXED,
+                               threads=max(8, os.cpu_count() or 8))
+    st = fourier_smooth(n).state
+    mesh.set_state(*st)
+    osv.set_state(*st)
+    solver.update(mesh)
+    dt_o = osv.step()
+    assert abs(solver.dt() - dt_o) <= 1e-12 * dt_o
+    g, o = mesh.get_state(), osv.state()
+    r = float(np.max(np.abs(g[0] - o[0]) / np.abs(o[0])))
+    print(f"2048^2 mixed scheme {scheme}: one-step max rel density difference {r:.3e}")
+    assert r <= 1e-6
+
+
+@pytest.mark.parametrize("scheme", [0, 1], ids=["predictor_corrector", "heun"])
+def test_mixed_l1_at_headline_size_and_horizon(gpu_lib, scheme):
+    """The mixed form over the full configuration: 2048 x 2048 periodic smooth
+    data, 500 steps.  Its density is compared with the FP64 parity form after
+    the same 500 steps (the parity kernels are bit-exact with the reference's
+    step); L1 relative error within 1e-5."""
+    Z = gpu_lib
+    from zephyr_b200.workloads import fourier_smooth
+    n, steps = 2048, 500
+    w = fourier_smooth(n)
+    res = {}
+    for name, prec, kern in (("mixed", Z.Precision.MIXED, Z.Kernels.FAST),
+                             ("parity", Z.Precision.FP64, Z.Kernels.PARITY)):
+        gen = Z.Rectangle(0.0, 1.0, 0.0, 1.0)
+        gen.set_boundaries(Z.Boundaries(3, 3, 3, 3))
+        gen.set_sizes(n, n)
+        mesh = Z.EuMesh(gen)
+        solver = Z.SmFluid(Z.IdealGas(1.4), precision=prec, kernels=kern)
+        solver.set_accuracy(2)
+        solver.set_CFL(0.4)
+        solver.set_limiter("van Albada")
+        solver.set_scheme(Z.Scheme(scheme))
+        solver.add_types(mesh)
+        mesh.set_state(*w.state)
+        solver.update(mesh, steps=steps)
+        res[name] = mesh.get_state()[0]
+        del solver, mesh
+    g, o = res["mixed"], res["parity"]
+    l1 = float(np.sum(np.abs(g - o)) / np.sum(np.abs(o)))
+    linf = float(np.max(np.abs(g - o)) / np.max(np.abs(o)))
+    print(f"mixed scheme={scheme} 2048^2 x {steps}: L1 rel density error {l1:.3e}, Linf {linf:.3e}")
+    assert l1 <= L1_TOL_MIXED
 
 
 def test_fast_stiffened(gpu_lib):

@@ -175,7 +175,7 @@ SIGNATURES = {
 # enum zg_kernel_kind
 KERNEL_KINDS = ["dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b", "flags", "mm_dt", "mm_recover",
                 "mm_flux", "mm_crp", "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals", "tr_adjust",
-                "mm_grad", "mm_stage1", "mm_stage2"]
+                "mm_grad", "mm_stage1", "mm_stage2", "step"]
 
 _lib = None
 

@@ -1,4 +1,5 @@
 // smf_fast.cu -- the tiled FP64 kernels (FAST); multiply-adds may be fused.
+#include "smf_fused.cuh"
 #include "smf_tiled.cuh"
 #include "smf_tiled_launch.h"
 
@@ -72,6 +73,18 @@ void launch_faces(const SmfArgs &a, const Fields<double> &f, int mode, void *str
         case 2: tiled::k_faces<double, false, 2, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
         default: tiled::k_faces<double, false, 3, TX, TY, FMINB><<<grid, block, 0, s>>>(a, f); break;
     }
+}
+
+// Fused single-pass stages (smf_fused.cuh): 30 x FUSED_TH interior cells per
+// block of 32 x (FUSED_TH + 2) threads.
+#ifndef ZG_FAST_FUSED_TH
+#define ZG_FAST_FUSED_TH 14
+#endif
+#ifndef ZG_FAST_FUSED_MINB
+#define ZG_FAST_FUSED_MINB 2
+#endif
+void launch_step(const SmfArgs &a, const Fields<double> &f, int mode, void *stream) {
+    tiled::fused_dispatch<double, false, ZG_FAST_FUSED_TH, ZG_FAST_FUSED_MINB>(a, f, mode, (cudaStream_t)stream);
 }
 
 }  // namespace fast

@@ -1,6 +1,7 @@
 // smf_mixed.cu -- the tiled MIXED kernels: FP32 reconstruction and Riemann
 // fluxes (approximate single-precision division and square root allowed),
 // FP64 conserved state, accumulation, update and dt.
+#include "smf_fused.cuh"
 #include "smf_tiled.cuh"
 #include "smf_tiled_launch.h"
 
@@ -82,6 +83,17 @@ void launch_to_mixed(int n, PrimPtr z, const Fields<float> &f, void *stream) {
 
 void launch_to_prim(int n, const Fields<float> &f, EosD eos, PrimPtr z, void *stream) {
     tiled::k_to_prim<BLOCK><<<blocks(n), BLOCK, 0, (cudaStream_t)stream>>>(n, f, eos, z);
+}
+
+// Fused single-pass stages (smf_fused.cuh).
+#ifndef ZG_MIXED_FUSED_TH
+#define ZG_MIXED_FUSED_TH 14
+#endif
+#ifndef ZG_MIXED_FUSED_MINB
+#define ZG_MIXED_FUSED_MINB 2
+#endif
+void launch_step(const SmfArgs &a, const Fields<float> &f, int mode, void *stream) {
+    tiled::fused_dispatch<float, true, ZG_MIXED_FUSED_TH, ZG_MIXED_FUSED_MINB>(a, f, mode, (cudaStream_t)stream);
 }
 
 }  // namespace mixed

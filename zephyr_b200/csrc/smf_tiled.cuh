@@ -765,7 +765,15 @@ __global__ void __launch_bounds__(BLOCK) k_cfl(SmfArgs a, Fields<R> f) {
     unsigned long long best = 0x7FEFFFFFFFFFFFFFull;
     if (ic < m.n) {
         int i = ic / m.ny, j = ic - i * m.ny;
-        double rho = f.w[0][ic], u = f.w[1][ic], v = f.w[2][ic], p = f.w[3][ic];
+        double rho, u, v, p;
+        if (sizeof(R) == 4) {
+            // MIXED: from the FP64 conserved state (the FP32 mirror only feeds
+            // the face arithmetic)
+            const P5<double> z = prim_of(C4<double>{f.q[0][ic], f.q[1][ic], f.q[2][ic], f.q[3][ic]}, a.eos);
+            rho = z.r, u = z.u, v = z.v, p = z.p;
+        } else {
+            rho = f.w[0][ic], u = f.w[1][ic], v = f.w[2][ic], p = f.w[3][ic];
+        }
         double c = sqrt(a.eos.gamma * (p + a.eos.P0) / rho);
         double dinc = sqrt(smin(m.inc2x[i], m.inc2y[j]));
         double lam = dinc / (sqrt(u * u + v * v) + c);

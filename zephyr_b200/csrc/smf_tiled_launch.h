@@ -14,12 +14,15 @@ namespace fast {
 void launch_cfl(const SmfArgs &a, const tiled::Fields<double> &f, void *stream);
 void launch_grad_predict(const SmfArgs &a, const tiled::Fields<double> &f, bool predict, void *stream);
 void launch_faces(const SmfArgs &a, const tiled::Fields<double> &f, int mode, void *stream);
+// one fused stage: 1 predictor-corrector step, 2 / 3 Heun stage A / B (HLLC, HLL)
+void launch_step(const SmfArgs &a, const tiled::Fields<double> &f, int mode, void *stream);
 }  // namespace fast
 
 namespace mixed {
 void launch_cfl(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
 void launch_grad_predict(const SmfArgs &a, const tiled::Fields<float> &f, bool predict, void *stream);
 void launch_faces(const SmfArgs &a, const tiled::Fields<float> &f, int mode, void *stream);
+void launch_step(const SmfArgs &a, const tiled::Fields<float> &f, int mode, void *stream);
 void launch_to_mixed(int n, PrimPtr z, const tiled::Fields<float> &f, void *stream);
 void launch_to_prim(int n, const tiled::Fields<float> &f, EosD eos, PrimPtr z, void *stream);
 }  // namespace mixed

@@ -439,6 +439,13 @@ int enqueue_tiled_step(zg_ctx *c) {
         if constexpr (MIXED) mixed::launch_faces(a, f, mode, st);
         else fast::launch_faces(a, f, mode, st);
     };
+    auto L_step = [&](const tiled::Fields<R> &f, int mode) {
+        if constexpr (MIXED) mixed::launch_step(a, f, mode, st);
+        else fast::launch_step(a, f, mode, st);
+    };
+    // one kernel per stage (smf_fused.cuh) for HLLC and HLL
+    const bool fused = c->par.kernels != ZG_KERNELS_FAST_TWO_PASS &&
+                       (c->par.flux == ZG_FLUX_HLLC || c->par.flux == ZG_FLUX_HLL);
     tiled::Fields<R> f = fields();
     if (!c->cfl_valid) {
         // Fresh accumulators for this step's minimum and the next one's
@@ -449,6 +456,12 @@ int enqueue_tiled_step(zg_ctx *c) {
     }
     if (c->par.accuracy == 1) {
         timed(c, ZG_K_FLUX1, [&] { L_faces(f, 0); });
+    } else if (fused && c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
+        timed(c, ZG_K_STEP, [&] { L_step(f, 1); });
+        c->wait_cur = 1 - c->wait_cur;
+    } else if (fused) {
+        timed(c, ZG_K_HEUN_A, [&] { L_step(f, 2); });
+        timed(c, ZG_K_HEUN_B, [&] { L_step(f, 3); });
     } else if (c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
         timed(c, ZG_K_STAGE1, [&] { L_grad(f, true); });
         timed(c, ZG_K_STAGE2, [&] { L_faces(f, 1); });
@@ -527,9 +540,10 @@ int enqueue_slot_mixed_step(zg_ctx *c) {
 }
 
 int enqueue_step(zg_ctx *c) {
-    if (c->amr && c->par.precision == ZG_FP64 && c->par.kernels == ZG_KERNELS_FAST) return enqueue_slot_fast_step(c);
+    const bool fast = c->par.kernels != ZG_KERNELS_PARITY;
+    if (c->amr && c->par.precision == ZG_FP64 && fast) return enqueue_slot_fast_step(c);
     if (c->amr && c->par.precision == ZG_MIXED) return enqueue_slot_mixed_step(c);
-    if (c->slots && (c->par.precision == ZG_MIXED || c->par.kernels == ZG_KERNELS_FAST))
+    if (c->slots && (c->par.precision == ZG_MIXED || fast))
         return fail(c, ZG_ERR_STATE,
                     "the MIXED kernels need a rectangle mesh; the FAST kernels a rectangle or an adaptive rectangle");
     if (c->par.precision == ZG_MIXED) {
@@ -539,7 +553,7 @@ int enqueue_step(zg_ctx *c) {
     }
     int rc = convert_state(c, ZG_FP64);
     if (rc != ZG_OK) return rc;
-    if (c->par.kernels == ZG_KERNELS_FAST) return enqueue_tiled_step<double, false>(c);
+    if (fast) return enqueue_tiled_step<double, false>(c);
     return enqueue_parity_step(c);
 }
 
@@ -815,9 +829,9 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown scheme");
     if (p->precision != ZG_FP64 && p->precision != ZG_MIXED)
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown precision");
-    if (p->kernels != ZG_KERNELS_PARITY && p->kernels != ZG_KERNELS_FAST)
+    if (p->kernels != ZG_KERNELS_PARITY && p->kernels != ZG_KERNELS_FAST && p->kernels != ZG_KERNELS_FAST_TWO_PASS)
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown kernel family");
-    if (p->precision == ZG_MIXED && p->kernels != ZG_KERNELS_FAST)
+    if (p->precision == ZG_MIXED && p->kernels == ZG_KERNELS_PARITY)
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: the mixed form uses the FAST kernels");
     if (!(p->gamma > 1.0)) return fail(c, ZG_ERR_ARG, "zg_smf_configure: gamma must exceed 1");
 
@@ -1040,7 +1054,7 @@ const char *zg_kernel_name(int kind) {
     static const char *names[ZG_K_COUNT] = {"dt", "flux1", "grad", "stage1", "stage2", "heun_a", "heun_b",
                                             "flags", "mm_dt", "mm_recover", "mm_flux", "mm_crp",
                                             "mm_closure", "tr_dt", "tr_flux", "tr_update", "tr_normals",
-                                            "tr_adjust", "mm_grad", "mm_stage1", "mm_stage2"};
+                                            "tr_adjust", "mm_grad", "mm_stage1", "mm_stage2", "step"};
     return (kind >= 0 && kind < ZG_K_COUNT) ? names[kind] : "unknown";
 }
 

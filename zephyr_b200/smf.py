@@ -67,6 +67,7 @@ class Precision(enum.IntEnum):
 class Kernels(enum.IntEnum):
     PARITY = 0
     FAST = 1
+    FAST_TWO_PASS = 2
 
 
 @dataclass(frozen=True)
