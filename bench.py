@@ -41,10 +41,15 @@ FALLBACK_HBM_GBS = 6650.0
 # persistent state it needs once and writes its result once; 2-D conserved
 # state = 4 doubles).  Kernels that the model folds into others carry 0.
 B_ALG_KERNEL = {"dt": 0, "flux1": 64, "grad": 0, "stage1": 64, "stage2": 96, "heun_a": 64, "heun_b": 96,
-                "flags": 0}
-# (the FAST predictor pass "stage1" is fused with the gradients; the
-# corrector "stage2" carries the next step's CFL minimum)
+                "flags": 0, "step": 160}
+# (the two-pass predictor "stage1" is fused with the gradients; the corrector
+# "stage2" carries the next step's CFL minimum; the fused FAST/MIXED kernel
+# "step" is the whole predictor-corrector step of a rectangle in one launch,
+# so one launch processes the model's two passes: 160 B per cell)
 B_ALG_STEP = {1: 64, 2: 160}
+# FP64 pipe of B200: 64 FP64 thread-instructions per SM and cycle
+FP64_INST_PER_SM_CYCLE = 64
+N_SM = 148
 
 
 def parse():
@@ -156,14 +161,16 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_cell(kernel):
-    """dram read+write bytes per cell of `kernel` from the committed ncu summary."""
+def traffic_per_cell(kernel, column=1):
+    """dram read+write bytes per cell of `kernel` (column 1), or its FP64
+    thread-instructions per cell (column 2) and FP64 pipe activity in per cent
+    (column 3), from the committed ncu summaries."""
     try:
         for ln in TRAFFIC_FILE.read_text().splitlines():
             parts = ln.split()
-            if len(parts) >= 2 and parts[0] == kernel and not ln.startswith("#"):
-                return float(parts[1])
-    except OSError:
+            if len(parts) > column and parts[0] == kernel and not ln.startswith("#"):
+                return float(parts[column])
+    except (OSError, ValueError):
         pass
     return None
 
@@ -255,14 +262,16 @@ def _solver(Z, w, cfg, args, local_rank, stream, precision, kernels):
     return mesh, solver
 
 
-def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=False):
+def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=False, per_kernel=True):
     """K steps between a barrier + synchronise and CUDA events on the
-    library's stream; returns (ms, per-kernel dict, launches, clocks)."""
+    library's stream; returns (ms, per-kernel dict, launches, clocks).  With
+    per_kernel the library brackets every launch with its own events (the
+    split by kernel); without, the steps run bare."""
     from zephyr_b200._lib import KERNEL_KINDS
     sampler = ClockSampler(torch.cuda.current_device()) if clocks else None
     if sampler:
         sampler.start()
-    lib.zg_set_timing(mesh.ctx, 1)
+    lib.zg_set_timing(mesh.ctx, 1 if per_kernel else 0)
     n0 = mesh.launch_count()
     barrier()
     torch.cuda.synchronize(dev)
@@ -287,6 +296,7 @@ def _timed_steps(torch, lib, mesh, solver, steps, dev, stream, barrier, clocks=F
     return ms, kernels, launches, (sampler.stop() if sampler else None)
 
 
+HORIZON = 500      # steps of the configuration (accuracy of the mixed form over them)
 MM_SIZE = 1024     # shock / water-column problem, cells per side
 MM_B_ALG = 160     # bytes per cell and step: 10 FP64 state fields read once and written once
 MM2_B_ALG = 320    # second order: the state read by both stages, the half-step state written and read, the next state written
@@ -801,11 +811,15 @@ def run_ours(args, rank, world, local_rank):
     cells = w.gen.nx() * w.gen.ny()
 
     # ---- headline: the FP64 step (FAST kernels), inputs resident in HBM ----
+    # timed bare (no per-kernel events); the split by kernel comes from a
+    # second run of K steps with the library's per-launch events
     mesh, solver = _solver(Z, w, cfg, args, local_rank, stream, Z.Precision.FP64, Z.Kernels.FAST)
     solver.update(mesh, steps=W)
     mesh.synchronize()
-    ms, kernels, launches, clocks = _timed_steps(torch, lib, mesh, solver, K, dev, stream, barrier, clocks=True)
+    ms, _, launches, clocks = _timed_steps(torch, lib, mesh, solver, K, dev, stream, barrier, clocks=True,
+                                           per_kernel=False)
     dt_last = solver.dt()
+    _, kernels, _, _ = _timed_steps(torch, lib, mesh, solver, K, dev, stream, barrier)
 
     # ---- end to end through the public API with host buffers ---------------
     pin = [torch.empty(cells, dtype=torch.float64, pin_memory=True) for _ in range(5)]
@@ -832,23 +846,41 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the other forms on the same workload ------------------------------
     variants = {}
-    for name, prec, kern in (("fp64_parity", Z.Precision.FP64, Z.Kernels.PARITY),
-                             ("mixed", Z.Precision.MIXED, Z.Kernels.FAST)):
-        m2, s2 = _solver(Z, w, cfg, args, local_rank, stream, prec, kern)
+    other_scheme = "heun" if args.scheme == "pc" else "pc"
+    for name, prec, kern, scheme in (("fp64_parity", Z.Precision.FP64, Z.Kernels.PARITY, args.scheme),
+                                     ("mixed", Z.Precision.MIXED, Z.Kernels.FAST, args.scheme),
+                                     ("fp64_two_pass", Z.Precision.FP64, Z.Kernels.FAST_TWO_PASS, args.scheme),
+                                     ("fp64_" + other_scheme, Z.Precision.FP64, Z.Kernels.FAST, other_scheme),
+                                     ("mixed_" + other_scheme, Z.Precision.MIXED, Z.Kernels.FAST, other_scheme)):
+        a2 = argparse.Namespace(**{**vars(args), "scheme": scheme})
+        m2, s2 = _solver(Z, w, cfg, a2, local_rank, stream, prec, kern)
         s2.update(m2, steps=W)
         m2.synchronize()
-        v_ms, v_kernels, v_launch, _ = _timed_steps(torch, lib, m2, s2, K, dev, stream, barrier)
-        variants[name] = {"ms": v_ms, "kernels": v_kernels, "launches": v_launch, "mesh": m2, "solver": s2}
+        v_ms, _, v_launch, _ = _timed_steps(torch, lib, m2, s2, K, dev, stream, barrier, per_kernel=False)
+        _, v_kernels, _, _ = _timed_steps(torch, lib, m2, s2, K, dev, stream, barrier)
+        variants[name] = {"ms": v_ms, "kernels": v_kernels, "launches": v_launch, "mesh": m2, "solver": s2,
+                          "scheme": scheme}
 
-    # accuracy of the mixed form: density after W + K steps against the FP64
-    # step run for the same steps from the same initial state
-    m_ref, s_ref = _solver(Z, w, cfg, args, local_rank, stream, Z.Precision.FP64, Z.Kernels.FAST)
-    s_ref.update(m_ref, steps=W + K)
-    rho64 = m_ref.get_state()[0]
-    rho_mx = variants["mixed"]["mesh"].get_state()[0]
-    l1 = float(np.sum(np.abs(rho_mx - rho64)) / np.sum(np.abs(rho64)))
-    linf = float(np.max(np.abs(rho_mx - rho64)) / np.max(np.abs(rho64)))
-    m_ref.close()
+    # accuracy over the configuration's horizon: density after HORIZON steps
+    # of the mixed form (and of the FAST FP64 form) against the bit-exact FP64
+    # parity form run for the same steps from the same initial state
+    acc = {}
+    for scheme in ("pc", "heun"):
+        a2 = argparse.Namespace(**{**vars(args), "scheme": scheme})
+        rho = {}
+        for name, prec, kern in (("parity", Z.Precision.FP64, Z.Kernels.PARITY),
+                                 ("mixed", Z.Precision.MIXED, Z.Kernels.FAST),
+                                 ("fast", Z.Precision.FP64, Z.Kernels.FAST)):
+            m3, s3 = _solver(Z, w, cfg, a2, local_rank, stream, prec, kern)
+            s3.update(m3, steps=HORIZON)
+            rho[name] = m3.get_state()[0]
+            m3.close()
+        o = rho["parity"]
+        acc[scheme] = {f"{k}_{nm}": v for nm in ("mixed", "fast") for k, v in (
+            ("l1_rel_density_err_vs_fp64_parity", float(np.sum(np.abs(rho[nm] - o)) / np.sum(np.abs(o)))),
+            ("linf_rel_density_err_vs_fp64_parity", float(np.max(np.abs(rho[nm] - o)) / np.max(np.abs(o)))))}
+    l1 = acc[args.scheme]["l1_rel_density_err_vs_fp64_parity_mixed"]
+    linf = acc[args.scheme]["linf_rel_density_err_vs_fp64_parity_mixed"]
 
     mm = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
                     want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), precision=Z.Precision.FP64)
@@ -881,10 +913,13 @@ def run_ours(args, rank, world, local_rank):
                                             if same_mesh else None)
     amr_mx["same_mesh_as_fp64"] = same_mesh
 
-    vals = _max_over_ranks(torch, [ms, e2e_ms, variants["fp64_parity"]["ms"], variants["mixed"]["ms"], mm["ms"],
-                                   amr["ms_total"], amr_par["ms_total"], mm_mx["ms"], amr_mx["ms_total"],
-                                   trv["ms"], mm2["ms"]], dev, world)
-    ms, e2e_ms, ms_par, ms_mix, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr, ms_mm2 = vals
+    vnames = list(variants)
+    vals = _max_over_ranks(torch, [ms, e2e_ms, mm["ms"], amr["ms_total"], amr_par["ms_total"], mm_mx["ms"],
+                                   amr_mx["ms_total"], trv["ms"], mm2["ms"]] + [variants[v]["ms"] for v in vnames],
+                           dev, world)
+    ms, e2e_ms, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr, ms_mm2 = vals[:9]
+    vms = dict(zip(vnames, vals[9:]))
+    ms_par, ms_mix = vms["fp64_parity"], vms["mixed"]
     amr_mx["value"] = world * amr_mx["value"] * amr_mx["ms_total"] / ms_amr_mx
     amr_mx["speedup_vs_fp64"] = ms_amr / ms_amr_mx
     amr["value"] = world * amr["value"] * amr["ms_total"] / ms_amr
@@ -907,14 +942,28 @@ def run_ours(args, rank, world, local_rank):
             "algorithmic_bytes_per_launch": balg,
             "step_achieved": B_ALG_STEP[cfg["acc"]] * cells * K / (ms / 1e3) / 1e9}
     roof["step_frac"] = roof["step_achieved"] / peak
+    # the FP64 pipe beside it: FP64 thread-instructions per cell of the top
+    # kernel (ncu, committed summary) at this run's duration, against the
+    # pipe's issue rate at the SM clock sampled during the timed region
+    f64_per_cell = traffic_per_cell(top, 2)
+    if f64_per_cell is not None:
+        mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        f64_peak = FP64_INST_PER_SM_CYCLE * N_SM * mhz * 1e6
+        f64_rate = f64_per_cell * cells / (kernels[top]["ms_avg"] / 1e3)
+        roof["fp64_pipe"] = {"inst_per_cell": f64_per_cell, "achieved_inst_per_s": f64_rate,
+                             "peak_inst_per_s": f64_peak, "frac": f64_rate / f64_peak,
+                             "ncu_pipe_active_pct": traffic_per_cell(top, 3),
+                             "source": "profiles/traffic_per_cell.txt (ncu --set full of the same kernel)"}
     mixed_balg = {1: 64, 2: 144}[cfg["acc"]]
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(config_of(args, w, cfg, world), form="FP64 (FAST kernels: face-once tiles)"),
+        "config": dict(config_of(args, w, cfg, world),
+                       form="FP64 (FAST kernels: one fused kernel per step, face-once tiles in shared memory)",
+                       timing="headline timed without per-kernel events; the kernel split from a second run"),
         "roofline": roof, "kernels": kernels,
-        "gpu_launches": int(launches + variants["fp64_parity"]["launches"] + variants["mixed"]["launches"] +
+        "gpu_launches": int(launches + sum(v["launches"] for v in variants.values()) +
                             mm["launches"] + mm_mx["launches"] + mm2["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
                             amr_par["gpu_launches"] + amr_mx["gpu_launches"] + trv["launches"] +
                             vtuv["gpu_launches"]),
@@ -930,10 +979,31 @@ def run_ours(args, rank, world, local_rank):
             "mixed": {"value": world * cells * K / (ms_mix / 1e3), "ms_per_step": ms_mix / K,
                       "speedup_vs_fp64": ms / ms_mix, "speedup_vs_fp64_parity": ms_par / ms_mix,
                       "l1_rel_density_err_vs_fp64": l1, "linf_rel_density_err_vs_fp64": linf,
-                      "err_after_steps": W + K,
+                      "err_after_steps": HORIZON,
+                      "err_reference": "the bit-exact FP64 parity form after the same steps",
                       "step_achieved_GBs": mixed_balg * cells * K / (ms_mix / 1e3) / 1e9,
                       "step_frac": mixed_balg * cells * K / (ms_mix / 1e3) / 1e9 / peak,
                       "kernels": variants["mixed"]["kernels"]},
+            "fp64_two_pass": {"value": world * cells * K / (vms["fp64_two_pass"] / 1e3),
+                              "ms_per_step": vms["fp64_two_pass"] / K,
+                              "note": "the earlier FAST form: gradients + predictor stored in HBM, then the "
+                                      "face pass", "kernels": variants["fp64_two_pass"]["kernels"]},
+            "fp64_" + other_scheme: {"value": world * cells * K / (vms["fp64_" + other_scheme] / 1e3),
+                                     "ms_per_step": vms["fp64_" + other_scheme] / K,
+                                     "scheme": "heun (extension)" if other_scheme == "heun" else
+                                               "predictor-corrector (reference)",
+                                     "kernels": variants["fp64_" + other_scheme]["kernels"]},
+            "mixed_" + other_scheme: {"value": world * cells * K / (vms["mixed_" + other_scheme] / 1e3),
+                                      "ms_per_step": vms["mixed_" + other_scheme] / K,
+                                      "speedup_vs_fp64": vms["fp64_" + other_scheme] / vms["mixed_" + other_scheme],
+                                      "l1_rel_density_err_vs_fp64": acc[other_scheme][
+                                          "l1_rel_density_err_vs_fp64_parity_mixed"],
+                                      "linf_rel_density_err_vs_fp64": acc[other_scheme][
+                                          "linf_rel_density_err_vs_fp64_parity_mixed"],
+                                      "err_after_steps": HORIZON,
+                                      "kernels": variants["mixed_" + other_scheme]["kernels"]},
+            "accuracy_over_horizon": {"steps": HORIZON, "vs": "FP64 parity form (bit-exact with the reference)",
+                                      "predictor_corrector": acc["pc"], "heun": acc["heun"]},
             "multimaterial": {
                 "value": world * mm["cells"] * K / (ms_mm / 1e3), "unit": METRIC, "ms_per_step": ms_mm / K,
                 "workload": mm["workload"], "form": mm["form"], "steps": K, "warmup": W,

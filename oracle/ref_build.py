@@ -20,7 +20,9 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("ZEPHYR_REFERENCE", "/root/reference"))
+# the zephyr source tree: $ZEPHYR_REFERENCE, else a checkout named
+# "reference" beside this repository
+REF = Path(os.environ.get("ZEPHYR_REFERENCE", str(HERE.parent.parent / "reference")))
 SHIM_COMMON = HERE / "ref_shim" / "common"          # Eigen subset, boost bits, configuration.h
 SHIM_MESH = HERE / "ref_shim" / "mesh_standin"      # plain-array EuMesh for the uniform checker
 OUT_DIR = HERE / "_ref"

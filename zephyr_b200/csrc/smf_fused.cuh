@@ -96,8 +96,9 @@ __device__ __forceinline__ C4<R> flux_x(const FS<R> &z) {
 template <typename R>
 __device__ __forceinline__ C4<R> hllc_fs(const FS<R> &L, const FS<R> &Rs, const EosR<R> &eos) {
     const R cL = sqrt(eos.gamma * (L.p + eos.P0) * L.ri), cR = sqrt(eos.gamma * (Rs.p + eos.P0) * Rs.ri);
-    const R SL = smin_t(L.u - cL, Rs.u - cR);
-    const R SR = smax_t(L.u + cL, Rs.u + cR);
+    // (the states are finite here: a NaN ordering of std::min does not arise)
+    const R SL = fmin(L.u - cL, Rs.u - cR);
+    const R SR = fmax(L.u + cL, Rs.u + cR);
     if (SL >= R(0)) return flux_x(L);
     if (SR <= R(0)) return flux_x(Rs);
     const R aL = L.r * (SL - L.u), aR = Rs.r * (SR - Rs.u);
@@ -127,8 +128,8 @@ __device__ __forceinline__ C4<R> hllc_fs(const FS<R> &L, const FS<R> &Rs, const 
 template <typename R>
 __device__ __forceinline__ C4<R> hll_fs(const FS<R> &L, const FS<R> &Rs, const EosR<R> &eos) {
     const R cL = sqrt(eos.gamma * (L.p + eos.P0) * L.ri), cR = sqrt(eos.gamma * (Rs.p + eos.P0) * Rs.ri);
-    const R SL = smin_t(L.u - cL, smin_t(Rs.u - cR, R(0)));
-    const R SR = smax_t(L.u + cL, smax_t(Rs.u + cR, R(0)));
+    const R SL = fmin(L.u - cL, fmin(Rs.u - cR, R(0)));
+    const R SR = fmax(L.u + cL, fmax(Rs.u + cR, R(0)));
     const C4<R> FL = flux_x(L), FR = flux_x(Rs);
     const R EL = L.e + R(0.5) * (L.u * L.u + L.v * L.v);
     const R ER = Rs.e + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v);
@@ -349,14 +350,14 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
 
     // ---- phase 2: the faces bounding interior cells, each once ---------------
     // face-state source of G cell (gr, gc): the half step, or the Z state
+    // (its reciprocal density is formed only where the state itself is used)
     auto sc = [&](int gr, int gc) {
-        FS<R> z;
-        if (PC) {
-            z = FS<R>{H[0][gr][gc], H[1][gr][gc], H[2][gr][gc], H[3][gr][gc], H[4][gr][gc], R(0)};
-        } else {
-            z = FS<R>{Z[0][gr + 1][gc + 1], Z[1][gr + 1][gc + 1], Z[2][gr + 1][gc + 1], Z[3][gr + 1][gc + 1],
-                      Z[4][gr + 1][gc + 1], R(0)};
-        }
+        if (PC) return FS<R>{H[0][gr][gc], H[1][gr][gc], H[2][gr][gc], H[3][gr][gc], H[4][gr][gc], R(0)};
+        return FS<R>{Z[0][gr + 1][gc + 1], Z[1][gr + 1][gc + 1], Z[2][gr + 1][gc + 1], Z[3][gr + 1][gc + 1],
+                     Z[4][gr + 1][gc + 1], R(0)};
+    };
+    auto sc_ri = [&](int gr, int gc) {
+        FS<R> z = sc(gr, gc);
         z.ri = rcp_r(z.r);
         return z;
     };
@@ -371,7 +372,11 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
                 z.p + G[b + 3][gr][gc] * off, R(0), R(0)};
         o.ri = rcp_r(o.r);
         o.e = energy_ri(eos, o.p, o.ri, igm1);
-        return bad_fs(o, eos.pmin) ? z : o;
+        if (bad_fs(o, eos.pmin)) {
+            o = z;
+            o.ri = rcp_r(z.r);
+        }
+        return o;
     };
 #pragma unroll 1
     for (int dir = 0; dir < 2; ++dir) {
@@ -392,8 +397,8 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
                 s_own = dir == 0 ? 1 : 3;
                 robust = PC && (wt[r][l] || wt[rB][lB]);
                 if (robust) {
-                    zm = sc(r, l);
-                    zp = sc(rB, lB);
+                    zm = sc_ri(r, l);
+                    zp = sc_ri(rB, lB);
                 } else {
                     zm = recon(r, l, dir, true);
                     zp = recon(rB, lB, dir, false);
@@ -405,7 +410,7 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
                 s_own = own_a ? (dir == 0 ? 1 : 3) : (dir == 0 ? 0 : 2);
                 sgn = own_a ? R(1) : R(-1);
                 robust = PC && wt[gr][gc];
-                zm = robust ? sc(gr, gc) : recon(gr, gc, dir, own_a);
+                zm = robust ? sc_ri(gr, gc) : recon(gr, gc, dir, own_a);
                 zp = zm;
                 if (m.bc[s_own] == BC_WALL) {
                     if (dir == 0) zp.u = -zp.u;
