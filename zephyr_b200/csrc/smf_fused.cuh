@@ -39,6 +39,8 @@
 //      pressure recovery, isolation counters, CFL term, block minimum
 #pragma once
 
+#include <type_traits>
+
 #include "smf_tiled.cuh"
 
 namespace zg {
@@ -168,6 +170,32 @@ __device__ __forceinline__ P5<double> prim_ri(const C4<double> &q, const EosD &e
     return z;
 }
 
+// Flux across a boundary face (WALL / ZOE, sm_fluid.cpp:69-79) from the
+// reconstructed state zm of its only cell, whose slot s_own it is: the ghost
+// state reflects the normal velocity at a wall; the flux is returned in the
+// +x / +y direction (negated when the cell lies on the face's high side).
+// Out of line: boundary faces are few, and one copy of the Riemann solver
+// serves all of them.
+template <typename R>
+__device__ __noinline__ C4<R> boundary_flux(FS<R> zm, int s_own, int bc, bool use_hll, EosR<R> eos, bool own_a) {
+    FS<R> zp = zm;
+    if (bc == BC_WALL) {
+        if (s_own < 2) zp.u = -zp.u;
+        else zp.v = -zp.v;
+    }
+    to_local(s_own, zm.u, zm.v);
+    to_local(s_own, zp.u, zp.v);
+    C4<R> lf = use_hll ? hll_fs(zm, zp, eos) : hllc_fs(zm, zp, eos);
+    to_global(s_own, lf.mu, lf.mv);
+    if (!own_a) {
+        lf.r = -lf.r;
+        lf.mu = -lf.mu;
+        lf.mv = -lf.mv;
+        lf.E = -lf.E;
+    }
+    return lf;
+}
+
 template <typename R, int TH, int MODE>
 struct FusedLayout {
     static constexpr int ZR = TH + 4, ZC = 34;  // Z region
@@ -176,9 +204,10 @@ struct FusedLayout {
     static constexpr bool PC = MODE == FUSED_PC;
     static constexpr size_t al(size_t x) { return (x + 15) / 16 * 16; }
     static constexpr size_t z_bytes = al(sizeof(R) * 5 * ZR * ZC);
-    // face fluxes: +x faces of G rows 0..TH, +y faces of G rows 1..TH
-    static constexpr size_t fx_bytes = al(sizeof(R) * 4 * (TH + 1) * GC);
-    static constexpr size_t fy_bytes = al(sizeof(R) * 4 * TH * GC);
+    // face fluxes (widened to FP64 once, where they are computed): +x faces
+    // of G rows 0..TH, +y faces of G rows 1..TH
+    static constexpr size_t fx_bytes = al(sizeof(double) * 4 * (TH + 1) * GC);
+    static constexpr size_t fy_bytes = al(sizeof(double) * 4 * TH * GC);
     // The predictor-corrector reads only the G region after phase 1, so the
     // fluxes may overwrite Z; the Heun stages reconstruct from Z itself.
     static constexpr size_t off_z = 0;
@@ -190,7 +219,10 @@ struct FusedLayout {
     static constexpr size_t g_bytes = al(sizeof(R) * 8 * GR * GC);
     static constexpr size_t off_h = off_g + g_bytes;
     static constexpr size_t h_bytes = PC ? al(sizeof(R) * 5 * GR * GC) : 0;
-    static constexpr size_t off_zin = off_h + h_bytes;
+    // conserved state at t^n of the G cells (predictor-corrector)
+    static constexpr size_t off_q = off_h + h_bytes;
+    static constexpr size_t q_bytes = PC ? al(sizeof(double) * 4 * GR * GC) : 0;
+    static constexpr size_t off_zin = off_q + q_bytes;
     static constexpr size_t zin_bytes = al(ZR * ZC);
     static constexpr size_t off_wt = off_zin + zin_bytes;
     static constexpr size_t wt_bytes = al(GR * GC);
@@ -228,10 +260,11 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
     constexpr bool PC = MODE == FUSED_PC;
     extern __shared__ __align__(16) unsigned char smem[];
     R(*Z)[ZR][ZC] = reinterpret_cast<R(*)[ZR][ZC]>(smem + L::off_z);
-    R(*FX)[TH + 1][GC] = reinterpret_cast<R(*)[TH + 1][GC]>(smem + L::off_fx);
-    R(*FY)[TH][GC] = reinterpret_cast<R(*)[TH][GC]>(smem + L::off_fy);
+    double(*FX)[TH + 1][GC] = reinterpret_cast<double(*)[TH + 1][GC]>(smem + L::off_fx);
+    double(*FY)[TH][GC] = reinterpret_cast<double(*)[TH][GC]>(smem + L::off_fy);
     R(*G)[GR][GC] = reinterpret_cast<R(*)[GR][GC]>(smem + L::off_g);
     R(*H)[GR][GC] = reinterpret_cast<R(*)[GR][GC]>(smem + L::off_h);
+    double(*Q)[GR][GC] = reinterpret_cast<double(*)[GR][GC]>(smem + L::off_q);
     unsigned char(*zin)[ZC] = reinterpret_cast<unsigned char(*)[ZC]>(smem + L::off_zin);
     unsigned char(*wt)[GC] = reinterpret_cast<unsigned char(*)[GC]>(smem + L::off_wt);
     unsigned long long *red = reinterpret_cast<unsigned long long *>(smem + L::off_red);
@@ -273,6 +306,19 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
         if (m.xper) gi = wrap_idx(gi, m.nx);
         if (m.yper) gj = wrap_idx(gj, m.ny);
         const int zr = r + 1, zc = l + 1;
+        // conserved state of the cell at t^n (predictor-corrector): FAST from
+        // the staged primitive state, MIXED from the FP64 fields (loaded here,
+        // ahead of the gradient arithmetic)
+        C4<double> q0{0.0, 0.0, 0.0, 0.0};
+        if (PC) {
+            if (MIXED) {
+                const int g = gi * m.ny + gj;
+                q0 = C4<double>{f.q[0][g], f.q[1][g], f.q[2][g], f.q[3][g]};
+            } else {
+                const double rr = Z[0][zr][zc], u = Z[1][zr][zc], v = Z[2][zr][zc], e = Z[4][zr][zc];
+                q0 = C4<double>{rr, rr * u, rr * v, rr * (e + 0.5 * (u * u + v * v))};
+            }
+        }
         // boundary flags of the four slots (the normals are the axes)
         const int fL = gi > 0 ? BC_INNER : m.bc[0];
         const int fR = gi < m.nx - 1 ? BC_INNER : m.bc[1];
@@ -330,7 +376,7 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
                     F[3] += (double)lf.E * w;
                 }
                 const double coef = 0.5 * dt / m.vol;
-                C4<double> q = q_of<R, MIXED>(f, g);
+                C4<double> q = q0;
                 q.r -= coef * F[0];
                 q.mu -= coef * F[1];
                 q.mv -= coef * F[2];
@@ -344,6 +390,10 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
             H[2][r][l] = hz.v;
             H[3][r][l] = hz.p;
             H[4][r][l] = hz.e;
+            Q[0][r][l] = q0.r;
+            Q[1][r][l] = q0.mu;
+            Q[2][r][l] = q0.mv;
+            Q[3][r][l] = q0.E;
         }
     }
     __syncthreads();
@@ -378,67 +428,65 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
         }
         return o;
     };
-#pragma unroll 1
-    for (int dir = 0; dir < 2; ++dir) {
-        // dir 0: +x face between G cells A = (r, l) and B = (r + 1, l) for the
-        // interior columns; dir 1: +y face between A and B = (r, l + 1) for
-        // the interior rows
-        const bool need = dir == 0 ? (r <= TH && l >= 1 && l <= 30) : (r >= 1 && r <= TH && l <= 30);
-        if (!need) continue;
-        const int rB = r + (dir == 0), lB = l + (dir == 1);
-        const bool inA = zin[r + 1][l + 1], inB = zin[rB + 1][lB + 1];
-        C4<R> lf{R(0), R(0), R(0), R(0)};
-        if (inA || inB) {
-            FS<R> zm, zp;
-            bool robust;
-            int s_own;
-            R sgn = R(1);
-            if (inA && inB) {
-                s_own = dir == 0 ? 1 : 3;
-                robust = PC && (wt[r][l] || wt[rB][lB]);
-                if (robust) {
-                    zm = sc_ri(r, l);
-                    zp = sc_ri(rB, lB);
-                } else {
-                    zm = recon(r, l, dir, true);
-                    zp = recon(rB, lB, dir, false);
-                }
-            } else {
-                // boundary face (WALL / ZOE) seen from its only cell
-                const bool own_a = inA;
-                const int gr = own_a ? r : rB, gc = own_a ? l : lB;
-                s_own = own_a ? (dir == 0 ? 1 : 3) : (dir == 0 ? 0 : 2);
-                sgn = own_a ? R(1) : R(-1);
-                robust = PC && wt[gr][gc];
-                zm = robust ? sc_ri(gr, gc) : recon(gr, gc, dir, own_a);
-                zp = zm;
-                if (m.bc[s_own] == BC_WALL) {
-                    if (dir == 0) zp.u = -zp.u;
-                    else zp.v = -zp.v;
-                }
-            }
-            to_local(s_own, zm.u, zm.v);
-            to_local(s_own, zp.u, zp.v);
-            lf = (robust || a.flux == FLUX_HLL) ? hll_fs(zm, zp, eos) : hllc_fs(zm, zp, eos);
-            to_global(s_own, lf.mu, lf.mv);
-            lf.r *= sgn;
-            lf.mu *= sgn;
-            lf.mv *= sgn;
-            lf.E *= sgn;
-        }
-        // (predictor-corrector: the fluxes overwrite Z, which no thread reads
-        // after phase 1)
-        if (dir == 0) {
-            FX[0][r][l] = lf.r;
-            FX[1][r][l] = lf.mu;
-            FX[2][r][l] = lf.mv;
-            FX[3][r][l] = lf.E;
+    // interior face: the frame of the +x (DIR 0) or +y (DIR 1) normal, where
+    // the rotation of rotate.cpp is the identity or (u, v) -> (v, -u)
+    auto face_interior = [&](auto dirc) {
+        constexpr int DIR = decltype(dirc)::value;
+        const int rB = r + (DIR == 0), lB = l + (DIR == 1);
+        const bool robust = PC && (wt[r][l] || wt[rB][lB]);
+        FS<R> zm, zp;
+        if (robust) {
+            zm = sc_ri(r, l);
+            zp = sc_ri(rB, lB);
         } else {
-            FY[0][r - 1][l] = lf.r;
-            FY[1][r - 1][l] = lf.mu;
-            FY[2][r - 1][l] = lf.mv;
-            FY[3][r - 1][l] = lf.E;
+            zm = recon(r, l, DIR, true);
+            zp = recon(rB, lB, DIR, false);
         }
+        if (DIR == 1) {
+            R t = zm.u;
+            zm.u = zm.v;
+            zm.v = -t;
+            t = zp.u;
+            zp.u = zp.v;
+            zp.v = -t;
+        }
+        C4<R> lf = (robust || a.flux == FLUX_HLL) ? hll_fs(zm, zp, eos) : hllc_fs(zm, zp, eos);
+        if (DIR == 1) {
+            const R t = lf.mu;
+            lf.mu = -lf.mv;
+            lf.mv = t;
+        }
+        return lf;
+    };
+    // boundary face (WALL / ZOE) seen from its only cell (out of line)
+    auto face_boundary = [&](int dir, bool own_a) {
+        const int gr = own_a ? r : r + (dir == 0), gc = own_a ? l : l + (dir == 1);
+        const int s_own = own_a ? (dir == 0 ? 1 : 3) : (dir == 0 ? 0 : 2);
+        const bool robust = PC && wt[gr][gc];
+        const FS<R> zm = robust ? sc_ri(gr, gc) : recon(gr, gc, dir, own_a);
+        return boundary_flux<R>(zm, s_own, m.bc[s_own], robust || a.flux == FLUX_HLL, eos, own_a);
+    };
+    // (predictor-corrector: the fluxes overwrite Z, which no thread reads
+    // after phase 1)
+    if (r <= TH && l >= 1 && l <= 30) {  // +x face between G cells (r, l) and (r + 1, l)
+        const bool inA = zin[r + 1][l + 1], inB = zin[r + 2][l + 1];
+        C4<R> lf{R(0), R(0), R(0), R(0)};
+        if (inA && inB) lf = face_interior(std::integral_constant<int, 0>{});
+        else if (inA || inB) lf = face_boundary(0, inA);
+        FX[0][r][l] = lf.r;
+        FX[1][r][l] = lf.mu;
+        FX[2][r][l] = lf.mv;
+        FX[3][r][l] = lf.E;
+    }
+    if (r >= 1 && r <= TH && l <= 30) {  // +y face between G cells (r, l) and (r, l + 1)
+        const bool inA = zin[r + 1][l + 1], inB = zin[r + 1][l + 2];
+        C4<R> lf{R(0), R(0), R(0), R(0)};
+        if (inA && inB) lf = face_interior(std::integral_constant<int, 1>{});
+        else if (inA || inB) lf = face_boundary(1, inA);
+        FY[0][r - 1][l] = lf.r;
+        FY[1][r - 1][l] = lf.mu;
+        FY[2][r - 1][l] = lf.mv;
+        FY[3][r - 1][l] = lf.E;
     }
     __syncthreads();
 
@@ -451,11 +499,12 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
         double F[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-            F[k] = ((-(double)FX[k][r - 1][l] * hy + (double)FX[k][r][l] * hy) - (double)FY[k][r - 1][l - 1] * hx) +
-                   (double)FY[k][r - 1][l] * hx;
+            F[k] = ((-FX[k][r - 1][l] * hy + FX[k][r][l] * hy) - FY[k][r - 1][l - 1] * hx) + FY[k][r - 1][l] * hx;
         const double coef = dt / m.vol;
         C4<double> q;
-        if (MODE == FUSED_HEUN_B) {
+        if (PC) {
+            q = C4<double>{Q[0][r][l], Q[1][r][l], Q[2][r][l], Q[3][r][l]};
+        } else if (MODE == FUSED_HEUN_B) {
             // Q(z*) of the stage value
             const double rr = Z[0][r + 1][l + 1], u = Z[1][r + 1][l + 1], v = Z[2][r + 1][l + 1],
                          e = Z[4][r + 1][l + 1];
