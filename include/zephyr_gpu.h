@@ -270,6 +270,14 @@ int zg_smf_dt(zg_ctx *ctx, double *dt);
  * SmFluid::set_flags (sm_fluid.cpp:524-559). */
 int zg_smf_set_flags(zg_ctx *ctx, int *flags);
 
+/* Limited gradients of the current state, SmFluid::compute_grad
+ * (sm_fluid.cpp:116-125; gradient.h:226-282, 412-474), computed with the
+ * bit-exact kernels and copied to host arrays of 4 * n_cells doubles each:
+ * d_dx = [d rho/dx | d vx/dx | d vy/dx | d p/dx], d_dy likewise (field-major).
+ * These are the d_dx / d_dy fields that SmFluid::set_flags leaves for the
+ * slope distributor of the next EuMesh::refine (sm_fluid.cpp:404-458). */
+int zg_smf_gradients(zg_ctx *ctx, double *d_dx, double *d_dy);
+
 /* Number of kernels this context has launched (for launch accounting). */
 int zg_launch_count(const zg_ctx *ctx, long long *count);
 

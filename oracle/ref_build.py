@@ -108,6 +108,36 @@ def mesh_units():
     return units + MESH_FILES
 
 
+DROPIN_DIR = HERE.parent / "tests" / "dropin"
+DROPIN_BINS = {"dropin_smf": DROPIN_DIR / "dropin_smf.cpp", "dropin_mmf": DROPIN_DIR / "dropin_mmf.cpp"}
+GPU_LIB_DIR = HERE.parent / "zephyr_b200"
+INCLUDE_DIR = HERE.parent / "include"
+
+
+def build_dropin(force: bool = False, verbose: bool = False) -> list:
+    """The drop-in test drivers: zephyr's problem loops against the
+    reference's own EuMesh / SmFluid / MmFluid (libzref_mesh.so) and the C++
+    drop-ins of include/zephyr/math/solver/*_gpu.h over libzephyr_gpu.so.
+    (The reference's sm_fluid.h and mm_fluid.h cannot share a translation
+    unit: each pulls its own PState into zephyr::math.)"""
+    gpu_lib = GPU_LIB_DIR / "libzephyr_gpu.so"
+    cxx = shutil.which("g++") or "g++"
+    out = []
+    for name, src in DROPIN_BINS.items():
+        binary = OUT_DIR / name
+        out.append(binary)
+        deps = [src, DROPIN_DIR / "dropin_common.h", LIB_MESH, gpu_lib, *INCLUDE_DIR.rglob("*.h")]
+        if not force and binary.exists() and binary.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+            continue
+        cmd = [cxx, *FLAGS, *FORCE, "-I", str(SHIM_COMMON), "-I", str(REF), "-I", str(INCLUDE_DIR), str(src),
+               "-o", str(binary), str(LIB_MESH), str(gpu_lib), "-pthread",
+               "-Wl,-rpath,$ORIGIN:$ORIGIN/../../zephyr_b200"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     """Build both checkers; returns the uniform one's path."""
     if not reference_present():
@@ -140,6 +170,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     with ThreadPoolExecutor(jobs) as ex:
         list(ex.map(lambda so: _compile(cxx, so[0], so[1], inc, force, verbose, newest_shim), zip(srcs, objs)))
     _link(cxx, LIB_MESH, objs, force, verbose)
+    if (GPU_LIB_DIR / "libzephyr_gpu.so").exists():
+        build_dropin(force, verbose)
     return LIB
 
 

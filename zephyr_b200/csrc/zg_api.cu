@@ -1008,6 +1008,25 @@ int zg_smf_set_flags(zg_ctx *c, int *flags) {
     return ZG_OK;
 }
 
+int zg_smf_gradients(zg_ctx *c, double *d_dx, double *d_dy) {
+    if (!c || !d_dx || !d_dy) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_gradients: solver not configured");
+    DeviceGuard g(c->device);
+    int rc = materialize_prim(c);
+    if (rc != ZG_OK) return rc;
+    SmfArgs a = make_args(c);
+    timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, c->slots, (void *)c->stream); });
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "gradient kernel launch");
+    const size_t n = (size_t)c->n;
+    for (int k = 0; k < 4; ++k) {
+        ZG_CUDA(c, cudaMemcpyAsync(d_dx + k * n, c->gx[k], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        ZG_CUDA(c, cudaMemcpyAsync(d_dy + k * n, c->gy[k], n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
 int zg_launch_count(const zg_ctx *c, long long *count) {
     if (!c || !count) return ZG_ERR_ARG;
     *count = c->launches;
