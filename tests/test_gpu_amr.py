@@ -296,3 +296,52 @@ def test_gradient_criterion_flags(gpu_lib):
     mesh.refine()
     assert mesh.n_cells() == n + 3 * int(near.sum())
     mesh.close()
+
+
+def test_adaptation_at_the_blast_configuration_size_side_by_side_with_reference(gpu_lib):
+    """The adaptive configuration at its own size: base mesh 512 x 512,
+    three refinement levels, ZOE sides, the blast data (rho = 1, u = v = 0,
+    p = 1e3 inside r < 0.01 around (0.5, 0.5), 1e-5 outside, at cell centres),
+    slope distributor, van Albada, CFL 0.4.  The initial adaptation loop of
+    smf_test_2D.cpp:112-117 (set the data, set_flags, refine; max_level + 3
+    times), then cycles of set_flags / refine / two steps, on the GPU and in
+    the reference's own EuMesh / SmFluid (oracle/_ref) side by side; every
+    mesh and state array is compared after every call."""
+    if not ref_available():
+        pytest.fail("oracle/_ref/libzref_mesh.so is missing: build it with oracle/ref_build.py")
+    from oracle import ref_mesh as RM
+    n, max_level = 512, 3
+    ref = RM.RefEuMesh(n, n, bounds=(2, 2, 2, 2), accuracy=2, limiter="van Albada", CFL=0.4, max_level=max_level,
+                       distributor="slope")
+    ref_ad = AC.RefAdapter(ref)  # one host thread: the reference's stage-2 counters are then deterministic
+    mesh, solver = gpu_mesh(n, (2, 2, 2, 2), max_level, "slope", 2, "van Albada", 0.4, capacity=1 << 20)
+    gpu_ad = AC.GpuAdapter(mesh, solver)
+
+    def blast(g):
+        r = np.hypot(np.asarray(g["cx"]) - 0.5, np.asarray(g["cy"]) - 0.5)
+        rho = np.ones_like(r)
+        p = np.where(r < 0.01, 1.0e3, 1.0e-5)
+        return rho, np.zeros_like(r), np.zeros_like(r), p, p / (0.4 * rho)
+
+    for k in range(max_level + 3):
+        g = gpu_ad.mesh()
+        ref_ad.set_state(*blast(g))
+        gpu_ad.set_state(*blast(g))
+        assert np.array_equal(ref_ad.set_flags(), gpu_ad.set_flags()), (k, "initial flags")
+        ref_ad.refine()
+        gpu_ad.refine()
+        compare_live(f"init {k}: refine", ref_ad, gpu_ad, gpu_ad.mesh())
+    g = gpu_ad.mesh()
+    ref_ad.set_state(*blast(g))
+    gpu_ad.set_state(*blast(g))
+    levels = np.asarray(g["level"])
+    assert levels.max() == max_level and len(levels) > n * n, (levels.max(), len(levels))
+    for c in range(3):
+        assert np.array_equal(ref_ad.set_flags(), gpu_ad.set_flags()), (c, "flags")
+        ref_ad.refine()
+        gpu_ad.refine()
+        compare_live(f"cycle {c}: refine", ref_ad, gpu_ad, gpu_ad.mesh())
+        for s in range(2):
+            assert ref_ad.step() == gpu_ad.step(), (c, s, "dt")
+            compare_live(f"cycle {c}: step {s}", ref_ad, gpu_ad, gpu_ad.mesh())
+    mesh.close()
