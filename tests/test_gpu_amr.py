@@ -298,6 +298,32 @@ def test_gradient_criterion_flags(gpu_lib):
     mesh.close()
 
 
+def test_gradient_criterion_matches_its_restatement(gpu_lib):
+    """The GPU's |grad rho| h / rho flags against the restatement of the
+    criterion (oracle/gradient_flags.py) on adapted blast meshes, after each
+    of a few adaptations driven by the criterion itself: equal flags on
+    every cell whose criterion is not within rounding of a threshold."""
+    from oracle import gradient_flags as GF
+    from zephyr_b200.workloads import blast_cell_means
+    mesh, solver = gpu_mesh(64, (2, 2, 2, 2), 3, "slope", 2, "van Albada", 0.4)
+    g = mesh.amr_arrays()
+    mesh.set_state(*blast_cell_means(g["vx"], g["vy"]))
+    checked = 0
+    for k in range(6):
+        solver.update(mesh, steps=40)  # the blast moves density about
+        g = mesh.amr_arrays()
+        f = solver.set_flags_gradient(mesh, 0.05, 0.01)
+        rho = mesh.get_state()[0]
+        crit = GF.criterion(g, rho)
+        want = GF.flags(g, rho)
+        clear = (np.abs(crit - 0.05) > 1e-10 * 0.05) & (np.abs(crit - 0.01) > 1e-10 * 0.01)
+        assert np.array_equal(f[clear], want[clear]), (k, int(np.count_nonzero(f[clear] != want[clear])))
+        checked += int(clear.sum())
+        mesh.refine()
+    assert np.asarray(mesh.amr_arrays()["level"]).max() == 3 and checked > 4 * 64 * 64
+    mesh.close()
+
+
 def test_adaptation_at_the_blast_configuration_size_side_by_side_with_reference(gpu_lib):
     """The adaptive configuration at its own size: base mesh 512 x 512,
     three refinement levels, ZOE sides, the blast data (rho = 1, u = v = 0,
