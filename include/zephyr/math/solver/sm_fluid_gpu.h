@@ -29,7 +29,7 @@
 //
 // Errors: a failed call throws std::runtime_error with the library's message,
 // as the reference throws.  Not on the GPU: axial symmetry (set_axial(true)
-// throws) and the fluxes other than Godunov, Rusanov, HLL and HLLC.
+// throws).
 //
 // Build: compile with zephyr's include path and include/ of this repository;
 // link zephyr_b200/libzephyr_gpu.so next to zephyr's own libraries.
@@ -95,8 +95,8 @@ public:
     }
     void set_method(Fluxes method) {
         const int f = static_cast<int>(method);
-        if (f < ZG_FLUX_GODUNOV || f > ZG_FLUX_HLLC)
-            throw std::runtime_error("SmFluidGPU: fluxes GODUNOV, RUSANOV, HLL and HLLC are implemented");
+        if (f < ZG_FLUX_GODUNOV || f > ZG_FLUX_CIR2)
+            throw std::runtime_error("Unknown numerical flux");
         m_par.flux = f;
         reconfigure();
     }

@@ -45,15 +45,21 @@ enum zg_boundary {
 };
 
 /* Numerical fluxes; values of zephyr's `enum class Fluxes`
- * (math/cfd/flux/num_flux.h:11-21).  GODUNOV (the exact Riemann solver of
- * math/solver/riemann.cpp; its rarefaction powers use CUDA's pow, so it
- * agrees with the reference to a few ulps rather than bit for bit),
- * RUSANOV, HLL and HLLC are implemented. */
+ * (math/cfd/flux/num_flux.h:11-21).  All eight of NumFlux::create
+ * (num_flux.cpp:6-35) are implemented.  GODUNOV (the exact Riemann solver of
+ * math/solver/riemann.cpp; its rarefaction powers use CUDA's pow) and HLLC_LM
+ * (its low-Mach factor uses CUDA's sin) agree with the reference to a few
+ * ulps rather than bit for bit.  HLLC_M, HLLC_LM, CIR1 and CIR2 run with the
+ * PARITY kernels only. */
 enum zg_flux {
     ZG_FLUX_GODUNOV = 0,
     ZG_FLUX_RUSANOV = 1,
     ZG_FLUX_HLL = 2,
-    ZG_FLUX_HLLC = 3
+    ZG_FLUX_HLLC = 3,
+    ZG_FLUX_HLLC_M = 4,
+    ZG_FLUX_HLLC_LM = 5,
+    ZG_FLUX_CIR1 = 6,
+    ZG_FLUX_CIR2 = 7
 };
 
 /* Slope limiters of math/cfd/limiter.cxx:15-153 (binary forms). */

@@ -16,6 +16,7 @@ _lib = None
 
 BC_WALL, BC_ZOE, BC_PERIODIC = 1, 2, 3
 FLUX_HLL, FLUX_HLLC = 2, 3
+FLUX_HLLC_M, FLUX_HLLC_LM, FLUX_CIR1, FLUX_CIR2 = 4, 5, 6, 7
 EOS_IDEAL, EOS_STIFFENED = 0, 1
 SCHEME_REF, SCHEME_HEUN = 0, 1
 

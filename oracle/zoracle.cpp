@@ -173,7 +173,10 @@ static inline V3 rot_global(V3 v, V3 no) {
 // ---------------------------------------------------------------------------
 // Numerical fluxes; values follow zephyr's `enum class Fluxes`
 // (zephyr/math/cfd/flux/num_flux.h:11-21).
-enum FluxKind { FLUX_GODUNOV = 0, FLUX_RUSANOV = 1, FLUX_HLL = 2, FLUX_HLLC = 3 };
+enum FluxKind {
+    FLUX_GODUNOV = 0, FLUX_RUSANOV = 1, FLUX_HLL = 2, FLUX_HLLC = 3, FLUX_HLLC_M = 4, FLUX_HLLC_LM = 5,
+    FLUX_CIR1 = 6, FLUX_CIR2 = 7
+};
 
 // zephyr/math/cfd/flux/hllc.cpp:23-83  HLLC::calc_flux (smf)
 static QState hllc(const PState &zL, const PState &zR, const Eos &eos) {
@@ -437,11 +440,205 @@ static QState godunov(const PState &zL, const PState &zR, const Eos &eos) {
     return flux_from_p(z);
 }
 
+// zephyr/math/cfd/flux/hllc.cpp:427-495  HLLC_LM::calc_flux (smf): the
+// HLLC flux whose outer-wave terms are scaled by phi = sin(pi/2 min(Ma / 0.1, 1))
+static QState hllc_lm(const PState &zL, const PState &zR, const Eos &eos) {
+    double c_L = eos.sound_speed_rP(zL.density, zL.pressure);
+    double c_R = eos.sound_speed_rP(zR.density, zR.pressure);
+    double S_L = std::min(zL.velocity.x - c_L, zR.velocity.x - c_R);
+    double S_R = std::max(zL.velocity.x + c_L, zR.velocity.x + c_R);
+    if (S_L >= 0.0) return flux_from_p(zL);
+    if (S_R <= 0.0) return flux_from_p(zR);
+    double a_L = zL.density * (S_L - zL.velocity.x);
+    double a_R = zR.density * (S_R - zR.velocity.x);
+    double S_C = (zL.pressure - zR.pressure + a_R * zR.velocity.x - a_L * zL.velocity.x) / (a_R - a_L);
+    double rho_sL = a_L / (S_L - S_C);
+    double rho_sR = a_R / (S_R - S_C);
+    double E_sL = p_E(zL) + (S_C - zL.velocity.x) * (S_C + zL.pressure / a_L);
+    double E_sR = p_E(zR) + (S_C - zR.velocity.x) * (S_C + zR.pressure / a_R);
+    QState Q_sL{rho_sL, {rho_sL * S_C, rho_sL * zL.velocity.y, rho_sL * zL.velocity.z}, rho_sL * E_sL};
+    QState Q_sR{rho_sR, {rho_sR * S_C, rho_sR * zR.velocity.y, rho_sR * zR.velocity.z}, rho_sR * E_sR};
+    QState Q_L = q_from_p(zL), Q_R = q_from_p(zR);
+    QState F_L = flux_from_p(zL), F_R = flux_from_p(zR);
+    double Ma_local = std::max(std::abs(zL.velocity.x / c_L), std::abs(zR.velocity.x / c_R));
+    double xi = Ma_local / 0.1;
+    double phi = xi > 1.0 ? 1.0 : std::sin(M_PI_2 * xi);
+    const double *fl = &F_L.density, *fr = &F_R.density;
+    const double *qsl = &Q_sL.density, *qsr = &Q_sR.density;
+    const double *ql = &Q_L.density, *qr = &Q_R.density;
+    QState F;
+    double *f = &F.density;
+    double aSC = std::abs(S_C);
+    for (int i = 0; i < 5; ++i) {
+        f[i] = 0.5 * (fl[i] + fr[i] + phi * S_L * (qsl[i] - ql[i]) + aSC * (qsl[i] - qsr[i]) +
+                      phi * S_R * (qsr[i] - qr[i]));
+    }
+    return F;
+}
+
+// zephyr/math/cfd/flux/hllc.cpp:499-570  HLLC_M::calc_flux (smf): the
+// tangential velocities are averaged across the contact too
+static QState hllc_m(const PState &zL, const PState &zR, const Eos &eos) {
+    double c_L = eos.sound_speed_rP(zL.density, zL.pressure);
+    double c_R = eos.sound_speed_rP(zR.density, zR.pressure);
+    double S_L = std::min(zL.velocity.x - c_L, zR.velocity.x - c_R);
+    double S_R = std::max(zL.velocity.x + c_L, zR.velocity.x + c_R);
+    if (S_L >= 0.0) return flux_from_p(zL);
+    if (S_R <= 0.0) return flux_from_p(zR);
+    double a_L = zL.density * (S_L - zL.velocity.x);
+    double a_R = zR.density * (S_R - zR.velocity.x);
+    double S_C = (zL.pressure - zR.pressure + a_R * zR.velocity.x - a_L * zL.velocity.x) / (a_R - a_L);
+    double V_C = (a_R * zR.velocity.y - a_L * zL.velocity.y) / (a_R - a_L);
+    double W_C = (a_R * zR.velocity.z - a_L * zL.velocity.z) / (a_R - a_L);
+    double rho_sL = a_L / (S_L - S_C);
+    double rho_sR = a_R / (S_R - S_C);
+    double E_sL = p_E(zL) + (S_C - zL.velocity.x) * (S_C + zL.pressure / a_L);
+    double E_sR = p_E(zR) + (S_C - zR.velocity.x) * (S_C + zR.pressure / a_R);
+    double v_L2 = std::pow(zL.velocity.y, 2) + std::pow(zL.velocity.z, 2);
+    double v_R2 = std::pow(zR.velocity.y, 2) + std::pow(zR.velocity.z, 2);
+    E_sL += 0.5 * ((a_R * v_R2 - a_L * v_L2) / (a_R - a_L) - v_L2);
+    E_sR += 0.5 * ((a_R * v_R2 - a_L * v_L2) / (a_R - a_L) - v_R2);
+    QState Q_sL{rho_sL, {rho_sL * S_C, rho_sL * V_C, rho_sL * W_C}, rho_sL * E_sL};
+    QState Q_sR{rho_sR, {rho_sR * S_C, rho_sR * V_C, rho_sR * W_C}, rho_sR * E_sR};
+    QState Q_L = q_from_p(zL), Q_R = q_from_p(zR);
+    QState F_L = flux_from_p(zL), F_R = flux_from_p(zR);
+    const double *fl = &F_L.density, *fr = &F_R.density;
+    const double *qsl = &Q_sL.density, *qsr = &Q_sR.density;
+    const double *ql = &Q_L.density, *qr = &Q_R.density;
+    QState F;
+    double *f = &F.density;
+    double aSC = std::abs(S_C);
+    for (int i = 0; i < 5; ++i) {
+        f[i] = 0.5 * (fl[i] + fr[i] + S_L * (qsl[i] - ql[i]) + aSC * (qsl[i] - qsr[i]) +
+                      S_R * (qsr[i] - qr[i]));
+    }
+    return F;
+}
+
+// Dense products in the evaluation order of the Eigen stand-in the reference
+// is built with here: c_ij = a_i0 b_0j, then c_ij += a_ik b_kj for k = 1, 2, ...
+template <int R, int K, int C>
+static void matmul(const double (&a)[R][K], const double (&b)[K][C], double (&c)[R][C]) {
+    for (int i = 0; i < R; ++i)
+        for (int j = 0; j < C; ++j) {
+            double acc = a[i][0] * b[0][j];
+            for (int k = 1; k < K; ++k) acc = acc + a[i][k] * b[k][j];
+            c[i][j] = acc;
+        }
+}
+
+// CIR face state: zE = (zL + zR) / 2 component by component, energy from
+// (density, pressure) (cir.cpp:20-30, 129-137)
+static PState cir_face_state(const PState &zL, const PState &zR, const Eos &eos) {
+    PState zE;
+    zE.density = 0.5 * (zL.density + zR.density);
+    zE.velocity = {0.5 * (zL.velocity.x + zR.velocity.x), 0.5 * (zL.velocity.y + zR.velocity.y),
+                   0.5 * (zL.velocity.z + zR.velocity.z)};
+    zE.pressure = 0.5 * (zL.pressure + zR.pressure);
+    zE.energy = eos.energy_rP(zE.density, zE.pressure);
+    return zE;
+}
+
+// zephyr/math/cfd/flux/cir.cpp:20-125  CIR1::calc_flux: Courant-Isaacson-Rees
+// flux with |A| = R |Lambda| L of the Jacobian at the averaged state
+static QState cir1(const PState &zL, const PState &zR, const Eos &eos) {
+    const PState zE = cir_face_state(zL, zR, eos);
+    double dR, dE;
+    eos.pressure_re_deriv(zE.density, zE.energy, dR, dE);
+    const double rho = zE.density, u = zE.velocity.x, v = zE.velocity.y, w = zE.velocity.z;
+    const double p = zE.pressure, eps = zE.energy;
+    const double u2 = u * u, v2 = v * v, w2 = w * w;
+    const double q2 = u2 + v2 + w2;
+    const double E = rho * (eps + 0.5 * q2);
+    const double c = eos.sound_speed_rP(rho, p);
+    const double c2 = c * c;
+    const double h = (E + p) / rho;
+    const double b = dE / rho;
+    const double T = b * (q2 - h) + c2;
+    const double lam[5] = {std::abs(u - c), std::abs(u), std::abs(u), std::abs(u), std::abs(u + c)};
+    double OmR[5][5] = {{1, 0, 0, 1, 1},
+                        {u - c, 0, 0, u, u + c},
+                        {v, 1, 0, v, v},
+                        {w, 0, 1, w, w},
+                        {h - u * c, v, w, h - c2 / b, h + u * c}};
+    double OmL[5][5] = {{T + u * c, -b * u - c, -b * v, -b * w, b},
+                        {-2 * v * c2, 0, 2 * c2, 0, 0},
+                        {-2 * w * c2, 0, 0, 2 * c2, 0},
+                        {2 * b * (h - q2), 2 * b * u, 2 * b * v, 2 * b * w, -2 * b},
+                        {T - u * c, -b * u + c, -b * v, -b * w, b}};
+    const double den = 2.0 * c2;
+    for (auto &row : OmL)
+        for (double &x : row) x /= den;
+    double RL[5][5], A[5][5];
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) RL[i][j] = OmR[i][j] * lam[j];
+    matmul(RL, OmL, A);
+    const QState qL = q_from_p(zL), qR = q_from_p(zR), fL = flux_from_p(zL), fR = flux_from_p(zR);
+    const double *ql = &qL.density, *qr = &qR.density, *fl = &fL.density, *fr = &fR.density;
+    double dq[5][1], hA[5][5], Adq[5][1];
+    for (int k = 0; k < 5; ++k) dq[k][0] = ql[k] - qr[k];
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 5; ++j) hA[i][j] = 0.5 * A[i][j];
+    matmul(hA, dq, Adq);
+    QState F;
+    double *f = &F.density;
+    for (int k = 0; k < 5; ++k) f[k] = 0.5 * (fl[k] + fr[k]) + Adq[k][0];
+    return F;
+}
+
+// zephyr/math/cfd/flux/cir.cpp:129-234  CIR2::calc_flux: the same with the
+// pressure as a sixth variable (the consistency check of cir.cpp:180-211,
+// which throws when the decomposition is off by more than 1e-10, is not
+// restated)
+static QState cir2(const PState &zL, const PState &zR, const Eos &eos) {
+    const PState zE = cir_face_state(zL, zR, eos);
+    const double rho = zE.density, u = zE.velocity.x, v = zE.velocity.y, w = zE.velocity.z;
+    const double p = zE.pressure, eps = zE.energy;
+    const double u2 = u * u, v2 = v * v, w2 = w * w;
+    const double q2 = u2 + v2 + w2;
+    const double E = rho * (eps + 0.5 * q2);
+    const double c = eos.sound_speed_rP(rho, p);
+    const double c2 = c * c;
+    const double h = (E + p) / rho;
+    const double lam[6] = {std::abs(u - c), std::abs(u), std::abs(u), std::abs(u), std::abs(u + c), std::abs(u)};
+    double OmR[5][6] = {{1, 0, 0, 0, 1, 1},
+                        {u - c, 0, 0, 0, u + c, u},
+                        {v, 1, 0, 0, v, 0},
+                        {w, 0, 1, 0, w, 0},
+                        {h - u * c, 0, 0, 1, h + u * c, 0}};
+    double OmL[6][6] = {{u / (2 * c), -1 / (2 * c), 0, 0, 0, 1 / (2 * c2)},
+                        {0, 0, 1, 0, 0, -v / c2},
+                        {0, 0, 0, 1, 0, -w / c2},
+                        {u2, -u, 0, 0, 1, -h / c2},
+                        {-u / (2 * c), 1 / (2 * c), 0, 0, 0, 1 / (2 * c2)},
+                        {1, 0, 0, 0, 0, -1 / c2}};
+    double RL[5][6], A[5][6];
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 6; ++j) RL[i][j] = OmR[i][j] * lam[j];
+    matmul(RL, OmL, A);
+    const QState qL = q_from_p(zL), qR = q_from_p(zR), fL = flux_from_p(zL), fR = flux_from_p(zR);
+    const double *ql = &qL.density, *qr = &qR.density, *fl = &fL.density, *fr = &fR.density;
+    double dq[6][1], hA[5][6], Adq[5][1];
+    for (int k = 0; k < 5; ++k) dq[k][0] = ql[k] - qr[k];
+    dq[5][0] = zL.pressure - zR.pressure;
+    for (int i = 0; i < 5; ++i)
+        for (int j = 0; j < 6; ++j) hA[i][j] = 0.5 * A[i][j];
+    matmul(hA, dq, Adq);
+    QState F;
+    double *f = &F.density;
+    for (int k = 0; k < 5; ++k) f[k] = 0.5 * (fl[k] + fr[k]) + Adq[k][0];
+    return F;
+}
+
 static inline QState num_flux(int kind, const PState &zL, const PState &zR, const Eos &eos) {
     switch (kind) {
         case FLUX_GODUNOV: return godunov(zL, zR, eos);
         case FLUX_RUSANOV: return rusanov(zL, zR, eos);
         case FLUX_HLL: return hll(zL, zR, eos);
+        case FLUX_HLLC_M: return hllc_m(zL, zR, eos);
+        case FLUX_HLLC_LM: return hllc_lm(zL, zR, eos);
+        case FLUX_CIR1: return cir1(zL, zR, eos);
+        case FLUX_CIR2: return cir2(zL, zR, eos);
         default: return hllc(zL, zR, eos);
     }
 }

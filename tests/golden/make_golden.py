@@ -67,7 +67,20 @@ CASES = {
                                 lambda: random_state(256, 12, "water")),
     "rusanov_fourier_32_vanalbada": (32, 32, (0, 1, 0, 1), (3, 3, 3, 3), (0, 1.4, 0.0), 1, "van Albada", 2, 0.4,
                                      30, lambda: fourier_smooth(32).state),
+    # HLLC_M, HLLC_LM (low Mach numbers: the sine branch), CIR1 and CIR2
+    "hllcm_riemann3_24_mc": (24, 24, (0, 1, 0, 1), (2, 2, 2, 2), (0, 1.4, 0.0), 4, "MC", 2, 0.4, 25,
+                             lambda: riemann2d_case3(24).state),
+    "hllclm_random_24_vanalbada": (24, 24, (0, 1, 0, 1), (1, 1, 3, 3), (0, 1.4, 0.0), 5, "van Albada", 2, 0.4, 25,
+                                   lambda: random_state(576, 21)),
+    "cir1_riemann3_24_first_order": (24, 24, (0, 1, 0, 1), (2, 2, 2, 2), (0, 1.4, 0.0), 6, "MC", 1, 0.4, 30,
+                                     lambda: riemann2d_case3(24).state),
+    "cir1_fourier_24_mc_periodic": (24, 24, (0, 1, 0, 1), (3, 3, 3, 3), (0, 1.4, 0.0), 6, "MC", 2, 0.4, 25,
+                                    lambda: fourier_smooth(24).state),
+    "cir2_stiffened_16_minmod": (16, 16, (0.0, 0.1, 0.0, 0.1), (2, 2, 1, 1), (1, 4.4, 6.0e8), 7, "minmod", 2, 0.4,
+                                 15, lambda: random_state(256, 13, "water")),
 }
+NEW_FLUX_CASES = ("hllcm_riemann3_24_mc", "hllclm_random_24_vanalbada", "cir1_riemann3_24_first_order",
+                  "cir1_fourier_24_mc_periodic", "cir2_stiffened_16_minmod")
 
 
 def make_case(name, spec):
@@ -408,6 +421,10 @@ if __name__ == "__main__":
         make_trs()
     elif "--vtu" in sys.argv:
         make_vtu()
+    elif "--fluxes2" in sys.argv:
+        for name in NEW_FLUX_CASES:
+            make_case(name, CASES[name])
+            print("wrote", name)
     elif "--fluxes" in sys.argv:
         for name in ("godunov_riemann3_32_first_order", "godunov_stiffened_16_mc", "rusanov_fourier_32_vanalbada"):
             make_case(name, CASES[name])

@@ -87,7 +87,7 @@ def test_periodic_pairs():
 def test_unimplemented_flux_is_refused():
     s = Z.SmFluid(Z.IdealGas(1.4))
     with pytest.raises(Z.ZgError):
-        s.set_method(Z.Fluxes.HLLC_M)
+        s.set_method(Z.Fluxes.CRP)  # the multi-material composite flux
     with pytest.raises(Z.ZgError):
         s.set_limiter("no-such-limiter")
 

@@ -116,6 +116,36 @@ def test_oracle_matches_reference_build_directly():
         assert np.array_equal(gr[0], go[0]) and np.array_equal(gr[1], go[1])
 
 
+@pytest.mark.parametrize("kind,name", [(4, "HLLC_M"), (5, "HLLC_LM"), (6, "CIR1"), (7, "CIR2")])
+def test_oracle_more_fluxes_match_reference_build_directly(kind, name):
+    """HLLC_M, HLLC_LM, CIR1 and CIR2 (NumFlux::create, num_flux.cpp:6-35)
+    pointwise against the reference's own classes on random ideal and
+    stiffened states, subsonic and supersonic, with tangential shear and
+    low Mach numbers (HLLC_LM's sine branch); bit for bit."""
+    from oracle import ref as R
+    if not R.available():
+        pytest.skip("reference-source build not present")
+    rng = np.random.default_rng(40 + kind)
+    for eos in [(0, 1.4, 0.0, 0.0), (1, 4.4, 6e8, 0.0), (1, 2.0, 1e5, 3.0)]:
+        for _ in range(600):
+            zs = []
+            for _ in range(2):
+                if eos[0] == 0:
+                    r, p = 0.1 + 2 * rng.random(), 0.05 + 3 * rng.random()
+                    scale = 10.0 ** rng.uniform(-3, 0.5)
+                else:
+                    r = 900 + 200 * rng.random() if eos[2] > 1e6 else 0.5 + rng.random()
+                    p = 1e5 * (0.5 + 10 * rng.random())
+                    scale = (100.0 if eos[2] > 1e6 else 1.0) * 10.0 ** rng.uniform(-3, 0.5)
+                u, v = rng.normal() * scale, rng.normal() * scale
+                e = p / ((eos[1] - 1) * r) if eos[0] == 0 else eos[3] + (p + eos[1] * eos[2]) / ((eos[1] - 1) * r)
+                zs.append(np.array([r, u, v, 0.0, p, e]))
+            zl, zr = zs
+            a = np.asarray(O.flux(kind, zl, zr, *eos))
+            b = np.asarray(R.flux(kind, zl, zr, *eos))
+            assert np.array_equal(a, b, equal_nan=True), (name, eos, zl, zr, a, b)
+
+
 def test_oracle_fluxes_match_reference_build_directly():
     """Godunov (exact Riemann solver) and Rusanov, pointwise, against the
     reference's own NumFlux on random ideal and stiffened states (shocks,

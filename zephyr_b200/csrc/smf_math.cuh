@@ -22,7 +22,10 @@
 namespace zg {
 
 enum : int { EOS_IDEAL = 0, EOS_STIFFENED = 1 };
-enum : int { FLUX_GODUNOV = 0, FLUX_RUSANOV = 1, FLUX_HLL = 2, FLUX_HLLC = 3 };
+enum : int {
+    FLUX_GODUNOV = 0, FLUX_RUSANOV = 1, FLUX_HLL = 2, FLUX_HLLC = 3, FLUX_HLLC_M = 4, FLUX_HLLC_LM = 5,
+    FLUX_CIR1 = 6, FLUX_CIR2 = 7
+};
 enum : int {
     LIM_NONE = 0, LIM_UNIT, LIM_MINMOD, LIM_MC, LIM_VANLEER, LIM_VANALBADA1, LIM_VANALBADA2,
     LIM_CHARM, LIM_HCUS, LIM_HQUICK, LIM_KOREN, LIM_SMART, LIM_SUPERBEE
@@ -352,11 +355,166 @@ static __device__ __noinline__ Cons godunov_ool(const Prim zL, const Prim zR, co
     return godunov(zL, zR, eos);
 }
 
+// The symmetric HLLC sum 0.5 (F_L + F_R + a S_L (Q*L - Q_L) + |S_C| (Q*L - Q*R)
+// + b S_R (Q*R - Q_R)) of hllc.cpp, component by component.
+__device__ inline double hllc_sum(double fl, double fr, double aSL, double ql, double qsl, double aSC, double qsr,
+                                  double bSR, double qr) {
+    return 0.5 * (fl + fr + aSL * (qsl - ql) + aSC * (qsl - qsr) + bSR * (qsr - qr));
+}
+
+// hllc.cpp:427-495 (HLLC_LM): the HLLC flux with the outer-wave terms scaled
+// by phi = sin(pi/2 min(Ma / 0.1, 1)), Ma the larger face Mach number.  The
+// sine is CUDA's: phi, and so the flux, agrees with glibc's to rounding.
+static __device__ __noinline__ Cons hllc_lm(const Prim zL, const Prim zR, const EosD eos) {
+    double c_L = eos.sound_speed_rP(zL.r, zL.p);
+    double c_R = eos.sound_speed_rP(zR.r, zR.p);
+    double S_L = smin(zL.u - c_L, zR.u - c_R);
+    double S_R = smax(zL.u + c_L, zR.u + c_R);
+    if (S_L >= 0.0) return flux_from_p(zL);
+    if (S_R <= 0.0) return flux_from_p(zR);
+    double a_L = zL.r * (S_L - zL.u);
+    double a_R = zR.r * (S_R - zR.u);
+    double S_C = (zL.p - zR.p + a_R * zR.u - a_L * zL.u) / (a_R - a_L);
+    double rho_sL = a_L / (S_L - S_C);
+    double rho_sR = a_R / (S_R - S_C);
+    double E_sL = (zL.e + 0.5 * v2(zL)) + (S_C - zL.u) * (S_C + zL.p / a_L);
+    double E_sR = (zR.e + 0.5 * v2(zR)) + (S_C - zR.u) * (S_C + zR.p / a_R);
+    Cons QsL{rho_sL, rho_sL * S_C, rho_sL * zL.v, rho_sL * E_sL};
+    Cons QsR{rho_sR, rho_sR * S_C, rho_sR * zR.v, rho_sR * E_sR};
+    Cons QL = q_from_p(zL), QR = q_from_p(zR), FL = flux_from_p(zL), FR = flux_from_p(zR);
+    double Ma = smax(fabs(zL.u / c_L), fabs(zR.u / c_R));
+    double xi = Ma / 0.1;
+    double phi = xi > 1.0 ? 1.0 : sin(1.57079632679489661923 * xi);  // M_PI_2
+    double pSL = phi * S_L, pSR = phi * S_R, aSC = fabs(S_C);
+    return Cons{hllc_sum(FL.r, FR.r, pSL, QL.r, QsL.r, aSC, QsR.r, pSR, QR.r),
+                hllc_sum(FL.mu, FR.mu, pSL, QL.mu, QsL.mu, aSC, QsR.mu, pSR, QR.mu),
+                hllc_sum(FL.mv, FR.mv, pSL, QL.mv, QsL.mv, aSC, QsR.mv, pSR, QR.mv),
+                hllc_sum(FL.E, FR.E, pSL, QL.E, QsL.E, aSC, QsR.E, pSR, QR.E)};
+}
+
+// hllc.cpp:499-570 (HLLC_M): the tangential velocity is averaged across the
+// contact as well, with the matching energy correction (v_z = 0 in 2-D;
+// pow(x, 2) is the correctly rounded square x * x).
+static __device__ __noinline__ Cons hllc_m(const Prim zL, const Prim zR, const EosD eos) {
+    double c_L = eos.sound_speed_rP(zL.r, zL.p);
+    double c_R = eos.sound_speed_rP(zR.r, zR.p);
+    double S_L = smin(zL.u - c_L, zR.u - c_R);
+    double S_R = smax(zL.u + c_L, zR.u + c_R);
+    if (S_L >= 0.0) return flux_from_p(zL);
+    if (S_R <= 0.0) return flux_from_p(zR);
+    double a_L = zL.r * (S_L - zL.u);
+    double a_R = zR.r * (S_R - zR.u);
+    double S_C = (zL.p - zR.p + a_R * zR.u - a_L * zL.u) / (a_R - a_L);
+    double V_C = (a_R * zR.v - a_L * zL.v) / (a_R - a_L);
+    double rho_sL = a_L / (S_L - S_C);
+    double rho_sR = a_R / (S_R - S_C);
+    double E_sL = (zL.e + 0.5 * v2(zL)) + (S_C - zL.u) * (S_C + zL.p / a_L);
+    double E_sR = (zR.e + 0.5 * v2(zR)) + (S_C - zR.u) * (S_C + zR.p / a_R);
+    double v_L2 = zL.v * zL.v + 0.0, v_R2 = zR.v * zR.v + 0.0;
+    E_sL += 0.5 * ((a_R * v_R2 - a_L * v_L2) / (a_R - a_L) - v_L2);
+    E_sR += 0.5 * ((a_R * v_R2 - a_L * v_L2) / (a_R - a_L) - v_R2);
+    Cons QsL{rho_sL, rho_sL * S_C, rho_sL * V_C, rho_sL * E_sL};
+    Cons QsR{rho_sR, rho_sR * S_C, rho_sR * V_C, rho_sR * E_sR};
+    Cons QL = q_from_p(zL), QR = q_from_p(zR), FL = flux_from_p(zL), FR = flux_from_p(zR);
+    double aSC = fabs(S_C);
+    return Cons{hllc_sum(FL.r, FR.r, S_L, QL.r, QsL.r, aSC, QsR.r, S_R, QR.r),
+                hllc_sum(FL.mu, FR.mu, S_L, QL.mu, QsL.mu, aSC, QsR.mu, S_R, QR.mu),
+                hllc_sum(FL.mv, FR.mv, S_L, QL.mv, QsL.mv, aSC, QsR.mv, S_R, QR.mv),
+                hllc_sum(FL.E, FR.E, S_L, QL.E, QsL.E, aSC, QsR.E, S_R, QR.E)};
+}
+
+// Courant-Isaacson-Rees fluxes (cir.cpp:20-125 CIR1, 129-234 CIR2):
+// F = (F_L + F_R) / 2 + (|A| / 2) (q_L - q_R) with |A| = R |Lambda| L of the
+// Jacobian at the averaged state.  Vectors carry the reference's five (six)
+// components (density, momentum x, y, z, energy[, pressure]) with z = 0; the
+// dense products sum k in increasing order from the k = 0 term, the order of
+// the Eigen stand-in the reference is built with here.  The consistency
+// check of CIR2 (cir.cpp:180-211, which throws when R Lambda L misses the
+// Jacobian by more than 1e-10) is not made.
+template <int NV>
+__device__ inline Cons cir_flux(const Prim &zL, const Prim &zR, const EosD &eos) {
+    const double rho = 0.5 * (zL.r + zR.r), u = 0.5 * (zL.u + zR.u), v = 0.5 * (zL.v + zR.v), w = 0.5 * (0.0 + 0.0);
+    const double p = 0.5 * (zL.p + zR.p);
+    const double eps = eos.energy_rP(rho, p);
+    const double u2 = u * u, vv = v * v, w2 = w * w;
+    const double q2 = u2 + vv + w2;
+    const double E = rho * (eps + 0.5 * q2);
+    const double c = eos.sound_speed_rP(rho, p);
+    const double c2 = c * c;
+    const double h = (E + p) / rho;
+    double RL[5][NV], L[NV][NV];
+    if (NV == 5) {
+        const double dE = eos.gm1 * rho;  // pressure_re's dP/de (ideal_gas.cpp:32-39, stiffened_gas.cpp:103-110)
+        const double b = dE / rho;
+        const double T = b * (q2 - h) + c2;
+        const double lam[5] = {fabs(u - c), fabs(u), fabs(u), fabs(u), fabs(u + c)};
+        const double R[5][5] = {{1, 0, 0, 1, 1},
+                                {u - c, 0, 0, u, u + c},
+                                {v, 1, 0, v, v},
+                                {w, 0, 1, w, w},
+                                {h - u * c, v, w, h - c2 / b, h + u * c}};
+        const double Lm[5][5] = {{T + u * c, -b * u - c, -b * v, -b * w, b},
+                                 {-2 * v * c2, 0, 2 * c2, 0, 0},
+                                 {-2 * w * c2, 0, 0, 2 * c2, 0},
+                                 {2 * b * (h - q2), 2 * b * u, 2 * b * v, 2 * b * w, -2 * b},
+                                 {T - u * c, -b * u + c, -b * v, -b * w, b}};
+        const double den = 2.0 * c2;
+        for (int i = 0; i < 5; ++i)
+            for (int j = 0; j < 5; ++j) {
+                RL[i][j] = R[i][j] * lam[j];
+                L[i][j] = Lm[i][j] / den;
+            }
+    } else {
+        const double lam[6] = {fabs(u - c), fabs(u), fabs(u), fabs(u), fabs(u + c), fabs(u)};
+        const double R[5][6] = {{1, 0, 0, 0, 1, 1},
+                                {u - c, 0, 0, 0, u + c, u},
+                                {v, 1, 0, 0, v, 0},
+                                {w, 0, 1, 0, w, 0},
+                                {h - u * c, 0, 0, 1, h + u * c, 0}};
+        const double Lm[6][6] = {{u / (2 * c), -1 / (2 * c), 0, 0, 0, 1 / (2 * c2)},
+                                 {0, 0, 1, 0, 0, -v / c2},
+                                 {0, 0, 0, 1, 0, -w / c2},
+                                 {u2, -u, 0, 0, 1, -h / c2},
+                                 {-u / (2 * c), 1 / (2 * c), 0, 0, 0, 1 / (2 * c2)},
+                                 {1, 0, 0, 0, 0, -1 / c2}};
+        for (int i = 0; i < 5; ++i)
+            for (int j = 0; j < NV; ++j) RL[i][j] = R[i][j] * lam[j];
+        for (int i = 0; i < NV; ++i)
+            for (int j = 0; j < NV; ++j) L[i][j] = Lm[i][j];
+    }
+    // |A| / 2 times (q_L - q_R)
+    const Cons qL = q_from_p(zL), qR = q_from_p(zR), fL = flux_from_p(zL), fR = flux_from_p(zR);
+    const double dq[6] = {qL.r - qR.r, qL.mu - qR.mu, qL.mv - qR.mv, 0.0 - 0.0, qL.E - qR.E, zL.p - zR.p};
+    double out[5];
+    for (int i = 0; i < 5; ++i) {
+        double acc = 0.0;
+        for (int j = 0; j < NV; ++j) {
+            double a = RL[i][0] * L[0][j];
+            for (int k = 1; k < NV; ++k) a = a + RL[i][k] * L[k][j];
+            const double term = (0.5 * a) * dq[j];
+            acc = j == 0 ? term : acc + term;
+        }
+        out[i] = acc;
+    }
+    return Cons{0.5 * (fL.r + fR.r) + out[0], 0.5 * (fL.mu + fR.mu) + out[1], 0.5 * (fL.mv + fR.mv) + out[2],
+                0.5 * (fL.E + fR.E) + out[4]};
+}
+static __device__ __noinline__ Cons cir1(const Prim zL, const Prim zR, const EosD eos) {
+    return cir_flux<5>(zL, zR, eos);
+}
+static __device__ __noinline__ Cons cir2(const Prim zL, const Prim zR, const EosD eos) {
+    return cir_flux<6>(zL, zR, eos);
+}
+
 __device__ inline Cons num_flux(int kind, const Prim &zL, const Prim &zR, const EosD &eos) {
     switch (kind) {
         case FLUX_GODUNOV: return godunov_ool(zL, zR, eos);
         case FLUX_RUSANOV: return rusanov(zL, zR, eos);
         case FLUX_HLL: return hll(zL, zR, eos);
+        case FLUX_HLLC_M: return hllc_m(zL, zR, eos);
+        case FLUX_HLLC_LM: return hllc_lm(zL, zR, eos);
+        case FLUX_CIR1: return cir1(zL, zR, eos);
+        case FLUX_CIR2: return cir2(zL, zR, eos);
         default: return hllc(zL, zR, eos);
     }
 }

@@ -821,8 +821,10 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     if (!c->have_mesh) return fail(c, ZG_ERR_STATE, "zg_smf_configure: no mesh");
     if (p->eos_kind != ZG_EOS_IDEAL && p->eos_kind != ZG_EOS_STIFFENED)
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown EoS");
-    if (p->flux < ZG_FLUX_GODUNOV || p->flux > ZG_FLUX_HLLC)
-        return fail(c, ZG_ERR_ARG, "zg_smf_configure: fluxes GODUNOV, RUSANOV, HLL and HLLC are implemented");
+    if (p->flux < ZG_FLUX_GODUNOV || p->flux > ZG_FLUX_CIR2)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown numerical flux");
+    if (p->flux > ZG_FLUX_HLLC && p->kernels != ZG_KERNELS_PARITY)
+        return fail(c, ZG_ERR_ARG, "zg_smf_configure: HLLC_M, HLLC_LM, CIR1 and CIR2 run with the PARITY kernels");
     if (p->limiter < ZG_LIM_NONE || p->limiter > ZG_LIM_SUPERBEE)
         return fail(c, ZG_ERR_ARG, "zg_smf_configure: unknown limiter");
     if (p->scheme != ZG_SCHEME_PREDICTOR_CORRECTOR && p->scheme != ZG_SCHEME_HEUN)

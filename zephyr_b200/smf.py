@@ -393,9 +393,9 @@ class SmFluid:
         self.params.accuracy = min(max(1, int(acc)), 2)
         self._push()
 
-    def set_method(self, method: Fluxes):  # sm_fluid.cpp:49-51
-        if int(method) not in (Fluxes.GODUNOV, Fluxes.RUSANOV, Fluxes.HLL, Fluxes.HLLC):
-            raise ZgError(-1, f"numerical flux {Fluxes(method).name} is not implemented on the GPU")
+    def set_method(self, method: Fluxes):  # sm_fluid.cpp:49-51 -> num_flux.cpp:6-35
+        if not 0 <= int(method) <= int(Fluxes.CIR2):
+            raise ZgError(-1, f"numerical flux {Fluxes(method).name} is not a single-material flux")
         self.params.flux = int(method)
         self._push()
 
