@@ -28,8 +28,7 @@
 // sm_fluid.cpp:372-470).
 //
 // Errors: a failed call throws std::runtime_error with the library's message,
-// as the reference throws.  Not on the GPU: axial symmetry (set_axial(true)
-// throws).
+// as the reference throws.
 //
 // Build: compile with zephyr's include path and include/ of this repository;
 // link zephyr_b200/libzephyr_gpu.so next to zephyr's own libraries.
@@ -90,8 +89,11 @@ public:
 
     void set_CFL(double CFL) { m_par.CFL = std::max(0.0, std::min(CFL, 1.0)); reconfigure(); }
     void set_accuracy(int acc) { m_par.accuracy = std::min(std::max(1, acc), 2); reconfigure(); }
+    /// SmFluid::set_axial (sm_fluid.cpp:45-47): the mesh must come from an
+    /// axisymmetric generator (Rectangle::set_axial), as in the reference.
     void set_axial(bool axial = true) {
-        if (axial) throw std::runtime_error("SmFluidGPU: axial symmetry is not implemented on the GPU");
+        m_axial = axial;
+        m_configured = false;  // the next call uploads the geometry again
     }
     void set_method(Fluxes method) {
         const int f = static_cast<int>(method);
@@ -203,6 +205,15 @@ private:
         zg_mesh_view v{static_cast<int>(n), m_cx.data(), m_cy.data(), m_vol.data(), m_inc.data(), m_fb.data(),
                        m_fn.data(), m_fnx.data(), m_fny.data(), m_fcx.data(), m_fcy.data(), m_fa.data()};
         check(zg_mesh_upload(m_ctx, &v));
+        if (m_axial) {  // AmrCells::volume_alt, AmrFaces::area_alt
+            m_vola.resize(n);
+            m_faa.resize(8 * n);
+            for (size_t ic = 0; ic < n; ++ic) {
+                m_vola[ic] = c.volume_alt[ic];
+                for (int s = 0; s < 8; ++s) m_faa[8 * ic + s] = c.faces.area_alt[c.face_begin[ic] + s];
+            }
+            check(zg_mesh_set_axial(m_ctx, m_vola.data(), m_faa.data()));
+        }
         check(zg_smf_configure(m_ctx, &m_par));
         m_configured = true;
         m_hash = h;
@@ -265,7 +276,8 @@ private:
     mutable size_t m_n = 0;
     mutable std::vector<double> m_cx, m_cy, m_vol, m_inc, m_fnx, m_fny, m_fcx, m_fcy, m_fa;
     mutable std::vector<int> m_fb, m_fn, m_flags, m_w;
-    mutable std::vector<double> m_r, m_u, m_v, m_p, m_e, m_gx, m_gy;
+    mutable std::vector<double> m_r, m_u, m_v, m_p, m_e, m_gx, m_gy, m_vola, m_faa;
+    bool m_axial = false;
 };
 
 }  // namespace zephyr::math

@@ -170,6 +170,18 @@ typedef struct zg_mesh_view {
  * zg_mesh_rectangle. */
 int zg_mesh_upload(zg_ctx *ctx, const zg_mesh_view *mesh);
 
+/* Axial symmetry (SmFluid::set_axial, sm_fluid.cpp:45-47, with a mesh made
+ * by an axisymmetric generator, Rectangle::set_axial): y is the radius; the
+ * fluxes are weighted by the faces' area_alt and the updates divided by the
+ * cells' volume_alt (amr_cells_gen.cpp:267-279), and the radial momentum
+ * gains the pressure source volume / volume_alt * p * dt (sm_fluid.cpp:
+ * 160-170, 236-246, 341-350).  Host arrays: volume_alt (n_cells) and
+ * face_area_alt (8 * n_cells, the slot order of zg_mesh_view); the centres
+ * given to zg_mesh_upload are then the generator's axisymmetric barycentres.
+ * NULL, NULL turns it off.  For a mesh from zg_mesh_upload, after each
+ * upload; the PARITY kernels with first order or the predictor-corrector. */
+int zg_mesh_set_axial(zg_ctx *ctx, const double *volume_alt, const double *face_area_alt);
+
 /* ---- Adaptive mesh on the device ------------------------------------------
  * A rectangle mesh made adaptive keeps zephyr's AmrCells layout on the GPU
  * (9 map points, level, z-index and 8 face slots per cell) with room for

@@ -26,6 +26,10 @@ def lib():
         L.zm_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I, C.c_int,
                                 C.c_double, C.c_double, C.c_double, C.c_int, C.c_char_p, C.c_int, C.c_double,
                                 C.c_int, C.c_char_p]
+        L.zm_create_ax.restype = C.c_void_p
+        L.zm_create_ax.argtypes = L.zm_create.argtypes + [C.c_int]
+        L.zm_axial_geometry.argtypes = [C.c_void_p, _P, _P]
+        L.zm_axial_geometry.restype = C.c_int
         L.zm_free.argtypes = [C.c_void_p]
         L.zm_threads.argtypes = [C.c_int]
         L.zm_n_cells.argtypes = [C.c_void_p]
@@ -72,10 +76,19 @@ class RefEuMesh:
     """zephyr's EuMesh(Rectangle) with an SmFluid on it (the reference's code)."""
 
     def __init__(self, nx, ny, box=(0.0, 1.0, 0.0, 1.0), bounds=(2, 2, 2, 2), eos_kind=0, gamma=1.4, P0=0.0,
-                 e0=0.0, flux=3, limiter="MC", accuracy=1, CFL=0.5, max_level=0, distributor="slope"):
+                 e0=0.0, flux=3, limiter="MC", accuracy=1, CFL=0.5, max_level=0, distributor="slope", axial=False):
         b = np.ascontiguousarray(bounds, dtype=np.int32)
-        self.h = lib().zm_create(nx, ny, *box, _ip(b), eos_kind, gamma, P0, e0, flux, limiter.encode(), accuracy,
-                                 CFL, max_level, distributor.encode())
+        self.h = lib().zm_create_ax(nx, ny, *box, _ip(b), eos_kind, gamma, P0, e0, flux, limiter.encode(),
+                                    accuracy, CFL, max_level, distributor.encode(), int(bool(axial)))
+
+    def axial_geometry(self):
+        """(volume_alt per cell, area_alt per face slot) of an axial mesh."""
+        n = self.n
+        vol = np.empty(n)
+        area = np.empty(8 * n)
+        if lib().zm_axial_geometry(self.h, _dp(vol), _dp(area)) != 0:
+            raise RuntimeError("not a mesh of 8-slot cells")
+        return vol, area
 
     @property
     def n(self):

@@ -45,14 +45,17 @@ extern "C" {
 // Mesh of Rectangle(x_min, x_max, y_min, y_max) with nx by ny cells, boundary
 // flags {left, right, bottom, top}, an SmFluid with the given settings, and
 // AMR up to max_level with the solver's distributor ("slope" or "const").
-void *zm_create(int nx, int ny, double x_min, double x_max, double y_min, double y_max, const int *bounds,
-                int eos_kind, double gamma, double P0, double e0, int flux, const char *limiter, int acc,
-                double CFL, int max_level, const char *distributor) {
+// With axial != 0 the generator and the solver are axisymmetric
+// (Rectangle::set_axial, SmFluid::set_axial: y is the radius).
+void *zm_create_ax(int nx, int ny, double x_min, double x_max, double y_min, double y_max, const int *bounds,
+                   int eos_kind, double gamma, double P0, double e0, int flux, const char *limiter, int acc,
+                   double CFL, int max_level, const char *distributor, int axial) {
     auto *r = new RefMesh();
     geom::generator::Rectangle gen(x_min, x_max, y_min, y_max);
     gen.set_boundaries({.left = Boundary(bounds[0]), .right = Boundary(bounds[1]),
                         .bottom = Boundary(bounds[2]), .top = Boundary(bounds[3])});
     gen.set_sizes(nx, ny);
+    if (axial) gen.set_axial(true);
     r->mesh = std::make_unique<EuMesh>(gen);
     r->eos = eos_kind == 0 ? phys::Eos::Ptr(phys::IdealGas::create(gamma))
                            : phys::Eos::Ptr(phys::StiffenedGas::create(gamma, P0, e0));
@@ -64,7 +67,29 @@ void *zm_create(int nx, int ny, double x_min, double x_max, double y_min, double
     r->part = r->solver->add_types(*r->mesh);
     r->mesh->set_max_level(max_level);
     r->mesh->set_distributor(r->solver->distributor(distributor));
+    if (axial) r->solver->set_axial(true);
     return r;
+}
+
+void *zm_create(int nx, int ny, double x_min, double x_max, double y_min, double y_max, const int *bounds,
+                int eos_kind, double gamma, double P0, double e0, int flux, const char *limiter, int acc,
+                double CFL, int max_level, const char *distributor) {
+    return zm_create_ax(nx, ny, x_min, x_max, y_min, y_max, bounds, eos_kind, gamma, P0, e0, flux, limiter, acc,
+                        CFL, max_level, distributor, 0);
+}
+
+// The axisymmetric geometry of an axial mesh: per cell volume_alt, per face
+// slot (8 per cell) area_alt (AmrCells::volume_alt, AmrFaces::area_alt).
+int zm_axial_geometry(void *p, double *vol_alt, double *area_alt) {
+    auto &c = static_cast<RefMesh *>(p)->mesh->locals();
+    int n = (int)c.size();
+    for (int ic = 0; ic < n; ++ic) {
+        vol_alt[ic] = c.volume_alt[ic];
+        int b = (int)c.face_begin[ic], e = (int)c.face_begin[ic + 1];
+        if (e - b != 8) return -1;
+        for (int s = 0; s < 8; ++s) area_alt[8 * ic + s] = c.faces.area_alt[b + s];
+    }
+    return 0;
 }
 
 void zm_free(void *p) { delete static_cast<RefMesh *>(p); }

@@ -7,7 +7,7 @@
 // (include/zephyr/math/solver/sm_fluid_gpu.h), the solver type being the only
 // difference.  Every cell of the two final meshes is compared bit for bit.
 //
-// Usage: dropin_smf <test> <nx> <max_level> <steps> <accuracy> <limiter> <flux> <CFL>
+// Usage: dropin_smf <test> <nx> <max_level> <steps> <accuracy> <limiter> <flux> <CFL> [axial]
 // Prints one JSON line and exits 0 when the two runs agree bit for bit.
 #include <cstdlib>
 #include <string>
@@ -31,7 +31,8 @@ using mesh::EuMesh;
 namespace {
 
 template <class Solver>
-Snapshot run_smf(int test_case, int nx, int max_level, int steps, int acc, const char *lim, int flux, double CFL) {
+Snapshot run_smf(int test_case, int nx, int max_level, int steps, int acc, const char *lim, int flux, double CFL,
+                 bool axial) {
     using math::smf::PState;
     using math::smf::QState;
     phys::Riemann2D test(test_case);
@@ -40,9 +41,11 @@ Snapshot run_smf(int test_case, int nx, int max_level, int steps, int acc, const
     Rectangle gen(test.xmin(), test.xmax(), test.ymin(), test.ymax());
     gen.set_boundaries(test.boundaries());
     gen.set_nx(nx);
+    if (axial) gen.set_axial(true);
     EuMesh mesh(gen);
 
     Solver solver(eos);
+    if (axial) solver.set_axial(true);
     solver.set_accuracy(acc);
     solver.set_CFL(CFL);
     solver.set_limiter(lim);
@@ -95,13 +98,14 @@ Snapshot run_smf(int test_case, int nx, int max_level, int steps, int acc, const
 }  // namespace
 
 int main(int argc, char **argv) {
-    if (argc != 9) return 2;
+    if (argc != 9 && argc != 10) return 2;
+    const bool axial = argc == 10 && std::string(argv[9]) == "axial";
     try {
         const int test_case = std::atoi(argv[1]), nx = std::atoi(argv[2]), max_level = std::atoi(argv[3]);
         const int steps = std::atoi(argv[4]), acc = std::atoi(argv[5]), flux = std::atoi(argv[7]);
         const double CFL = std::atof(argv[8]);
-        auto ref = run_smf<math::SmFluid>(test_case, nx, max_level, steps, acc, argv[6], flux, CFL);
-        auto gpu = run_smf<math::SmFluidGPU>(test_case, nx, max_level, steps, acc, argv[6], flux, CFL);
+        auto ref = run_smf<math::SmFluid>(test_case, nx, max_level, steps, acc, argv[6], flux, CFL, axial);
+        auto gpu = run_smf<math::SmFluidGPU>(test_case, nx, max_level, steps, acc, argv[6], flux, CFL, axial);
         return dropin::report("smf", ref, gpu);
     } catch (const std::exception &e) {
         std::printf("{\"error\": \"%s\"}\n", e.what());

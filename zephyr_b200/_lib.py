@@ -109,6 +109,7 @@ SIGNATURES = {
     "zg_mesh_rectangle": (C.c_int, [_V, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _I]),
     "zg_mesh_n_cells": (C.c_int, [_V, _I]),
     "zg_mesh_upload": (C.c_int, [_V, C.POINTER(MeshView)]),
+    "zg_mesh_set_axial": (C.c_int, [_V, _P, _P]),
     "zg_amr_enable": (C.c_int, [_V, C.c_int, C.c_int]),
     "zg_amr_set_distributor": (C.c_int, [_V, C.c_int]),
     "zg_amr_put_flags": (C.c_int, [_V, _I]),

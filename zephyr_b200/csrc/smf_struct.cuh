@@ -47,6 +47,11 @@ struct StructAcc {
     __device__ double cx() const { return m.cx[i]; }
     __device__ double cy() const { return m.cy[j]; }
     __device__ double vol() const { return m.vol; }
+    // the flux geometry (SmFluid's face.area(m_axial), cell.volume(m_axial)):
+    // plain on a rectangle
+    static constexpr bool axial() { return false; }
+    __device__ double flux_area(const FaceG &g, int) const { return g.area; }
+    __device__ double flux_vol() const { return m.vol; }
     // incircle diameter (amr_cells.cpp:107-116)
     __device__ double dinc() const { return sqrt(smin(m.inc2x[i], m.inc2y[j])); }
 
@@ -105,6 +110,11 @@ struct SlotAcc {
     __device__ double cy() const { return m.cy[ic]; }
     __device__ double vol() const { return m.vol[ic]; }
     __device__ double dinc() const { return m.inc[ic]; }
+    // the flux geometry: area_alt and volume_alt on an axisymmetric mesh
+    // (sm_fluid.cpp:160-164, 236-240, 341-345)
+    __device__ bool axial() const { return m.vol_alt != nullptr; }
+    __device__ double flux_area(const FaceG &g, int s) const { return m.fa_alt ? m.fa_alt[8 * ic + s] : g.area; }
+    __device__ double flux_vol() const { return m.vol_alt ? m.vol_alt[ic] : m.vol[ic]; }
     __device__ FaceG face(int s) const {
         const int f = 8 * ic + s;
         FaceG g;
@@ -149,6 +159,9 @@ struct SlotFastAcc {
     __device__ double cy() const { return pcy; }
     __device__ double vol() const { return m.vol[ic]; }
     __device__ double dinc() const { return m.inc[ic]; }
+    static constexpr bool axial() { return false; }
+    __device__ double flux_area(const FaceG &g, int) const { return g.area; }
+    __device__ double flux_vol() const { return m.vol[ic]; }
     __device__ FaceG face(int s) const {
         const int f = 8 * ic + s;
         FaceG g;
@@ -330,9 +343,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_flux1(SmfArgs a) {
         rot_local(zp.u, zp.v, cs, sn);
         Cons lf = num_flux(a.flux, zm, zp, a.eos);
         rot_global(lf.mu, lf.mv, cs, sn);
-        add_area(F, lf, g.area);
+        add_area(F, lf, c.flux_area(g, s));
     }
-    update(q, dt / c.vol(), F);
+    update(q, dt / c.flux_vol(), F);
+    if (c.axial()) {  // pressure source of the radial momentum (sm_fluid.cpp:166-169)
+        double coeff = c.vol() / c.flux_vol();
+        q.mv += coeff * zc.p * dt;
+    }
     store_prim(a.znext, ic, p_from_q(q, a.eos));
 }
 
@@ -550,9 +567,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_stage1(SmfArgs a) {
         rot_local(zm.u, zm.v, cs, sn);
         Cons lf = flux_from_p(zm);
         rot_global(lf.mu, lf.mv, cs, sn);
-        add_area(F, lf, g.area);
+        add_area(F, lf, c.flux_area(g, s));
     }
-    update(q, 0.5 * dt / c.vol(), F);
+    update(q, 0.5 * dt / c.flux_vol(), F);
+    if (c.axial()) {  // sm_fluid.cpp:242-245
+        double coeff = c.vol() / c.flux_vol();
+        q.mv += 0.5 * coeff * zc.p * dt;
+    }
     Prim h = p_from_q(q, a.eos);
     if (is_bad(h, a.eos)) h = zc;
     store_prim(a.zhalf, ic, h);
@@ -592,10 +613,11 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &zh, const
     rot_local(zp.u, zp.v, cs, sn);
     Cons lf = robust ? hll(zm, zp, a.eos) : num_flux(a.flux, zm, zp, a.eos);
     rot_global(lf.mu, lf.mv, cs, sn);
-    lf.r *= g.area;
-    lf.mu *= g.area;
-    lf.mv *= g.area;
-    lf.E *= g.area;
+    const double area = c.flux_area(g, s);
+    lf.r *= area;
+    lf.mu *= area;
+    lf.mv *= area;
+    lf.E *= area;
     return lf;
 }
 
@@ -623,7 +645,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_stage2(SmfArgs a) {
         F.mv += lf.mv;
         F.E += lf.E;
     }
-    update(q, dt / c.vol(), F);
+    update(q, dt / c.flux_vol(), F);
+    if (c.axial()) {  // sm_fluid.cpp:347-350, with the half-step pressure
+        double coeff = c.vol() / c.flux_vol();
+        q.mv += coeff * zch.p * dt;
+    }
     Prim n = p_from_q(q, a.eos);
     int wn = wc;
     if (is_bad(n, a.eos)) {

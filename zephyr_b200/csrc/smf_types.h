@@ -34,6 +34,9 @@ struct SlotMesh {
     // level L is hx0 / 2^L by hy0 / 2^L, axis-aligned); null level otherwise
     const int *level;
     double hx0, hy0;
+    // axisymmetric meshes only (y the radius): per cell volume_alt, per slot
+    // area_alt (AmrCells / AmrFaces), null otherwise
+    const double *vol_alt, *fa_alt;
 };
 
 struct PrimPtr {

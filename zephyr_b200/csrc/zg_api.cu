@@ -39,6 +39,7 @@ struct zg_ctx {
     bool slots = false;        // mesh given cell by cell (zg_mesh_upload)
     SlotMesh smesh{};
     void *d_slot = nullptr;    // slot-mesh arrays
+    void *d_axial = nullptr;   // axisymmetric volume_alt / area_alt of a slot mesh
     double *d_geo = nullptr;  // all geometry tables
     double *d_tgeo = nullptr;  // per-axis tables of the tiled kernels, FP64 then FP32
     tiled::AxisGeo<double> ax64{}, ay64{};
@@ -189,6 +190,8 @@ void free_mesh(zg_ctx *c) {
     cudaFree(c->d_geo);
     cudaFree(c->d_tgeo);
     cudaFree(c->d_slot);
+    cudaFree(c->d_axial);
+    c->d_axial = nullptr;
     cudaFree(c->d_amr);
     cudaFree(c->d_amr_scratch);
     c->d_geo = nullptr;
@@ -541,6 +544,9 @@ int enqueue_slot_mixed_step(zg_ctx *c) {
 
 int enqueue_step(zg_ctx *c) {
     const bool fast = c->par.kernels != ZG_KERNELS_PARITY;
+    if (c->smesh.vol_alt && (fast || c->par.precision != ZG_FP64 || (c->par.accuracy == 2 &&
+                                                                        c->par.scheme == ZG_SCHEME_HEUN)))
+        return fail(c, ZG_ERR_STATE, "axial symmetry runs with the PARITY kernels and the reference's schemes");
     if (c->amr && c->par.precision == ZG_FP64 && fast) return enqueue_slot_fast_step(c);
     if (c->amr && c->par.precision == ZG_MIXED) return enqueue_slot_mixed_step(c);
     if (c->slots && (c->par.precision == ZG_MIXED || fast))
@@ -813,6 +819,29 @@ int zg_mesh_upload(zg_ctx *c, const zg_mesh_view *v) {
     c->nx = c->ny = 0;
     c->slots = true;
     c->have_mesh = true;
+    return ZG_OK;
+}
+
+int zg_mesh_set_axial(zg_ctx *c, const double *volume_alt, const double *face_area_alt) {
+    if (!c) return ZG_ERR_ARG;
+    if (!c->have_mesh || !c->slots || c->amr)
+        return fail(c, ZG_ERR_STATE, "zg_mesh_set_axial: axial symmetry needs a mesh given cell by cell (zg_mesh_upload)");
+    if ((volume_alt == nullptr) != (face_area_alt == nullptr))
+        return fail(c, ZG_ERR_ARG, "zg_mesh_set_axial: give both arrays, or neither to turn axial symmetry off");
+    DeviceGuard g(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_axial);
+    c->d_axial = nullptr;
+    c->smesh.vol_alt = nullptr;
+    c->smesh.fa_alt = nullptr;
+    if (!volume_alt) return ZG_OK;
+    const size_t n = (size_t)c->n;
+    ZG_CUDA(c, cudaMalloc(&c->d_axial, 9 * n * sizeof(double)));
+    double *d = static_cast<double *>(c->d_axial);
+    ZG_CUDA(c, cudaMemcpy(d, volume_alt, n * sizeof(double), cudaMemcpyHostToDevice));
+    ZG_CUDA(c, cudaMemcpy(d + n, face_area_alt, 8 * n * sizeof(double), cudaMemcpyHostToDevice));
+    c->smesh.vol_alt = d;
+    c->smesh.fa_alt = d + n;
     return ZG_OK;
 }
 

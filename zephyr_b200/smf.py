@@ -198,11 +198,21 @@ class EuMesh:
                         ip(keep["boundary"]), ip(keep["neib"]), dp(keep["nx"]), dp(keep["ny"]),
                         dp(keep["fx"]), dp(keep["fy"]), dp(keep["area"]))
         check(self.ctx, self._lib.zg_mesh_upload(self.ctx, C.byref(view)))
+        if "vol_alt" in g and "area_alt" in g:
+            self.set_axial(g["vol_alt"], g["area_alt"])
         self.nx = self.ny = 0
         self.gen = None
         self.solver = None
         self._amr = False
         return self
+
+    def set_axial(self, vol_alt, area_alt):
+        """Axisymmetric geometry of a mesh given cell by cell (Rectangle /
+        SmFluid set_axial): volume_alt per cell, area_alt per face slot."""
+        v = np.ascontiguousarray(vol_alt, dtype=np.float64)
+        a = np.ascontiguousarray(area_alt, dtype=np.float64)
+        dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+        check(self.ctx, self._lib.zg_mesh_set_axial(self.ctx, dp(v), dp(a)))
 
     def set_stream(self, stream):
         """Queue all work on `stream` (a cudaStream_t handle as int, or None)."""
