@@ -30,8 +30,11 @@ SMF_CASES = [
     ("riemann7 first order uniform", (7, 32, 0, 40, 1, "MC", 3, 0.4)),
     ("riemann6 van Albada HLL amr3", (6, 16, 3, 20, 2, "vanAlbada1", 2, 0.5)),
     ("riemann7 minmod Rusanov amr1", (7, 20, 1, 25, 2, "minmod", 1, 0.4)),
-    # axial symmetry (Rectangle::set_axial + SmFluid::set_axial), other fluxes
-    ("riemann6 axial MC amr2", (6, 20, 2, 20, 2, "MC", 3, 0.5, "axial")),
+    # axial symmetry (Rectangle::set_axial + SmFluid::set_axial) on unrefined
+    # meshes: the reference's refine computes no volume_alt for new cells
+    # (mesh/amr sets only the split faces' area_alt, faces.h:80), so an
+    # axisymmetric adaptive run is not defined there
+    ("riemann6 axial MC second order uniform", (6, 20, 0, 20, 2, "MC", 3, 0.5, "axial")),
     ("riemann7 axial first order uniform", (7, 24, 0, 30, 1, "MC", 3, 0.4, "axial")),
     ("riemann6 CIR1 amr1", (6, 16, 1, 15, 2, "minmod", 6, 0.4)),
     ("riemann7 HLLC_M uniform", (7, 24, 0, 25, 2, "MC", 4, 0.4)),
