@@ -288,6 +288,22 @@ int zg_smf_dt(zg_ctx *ctx, double *dt);
  * SmFluid::set_flags (sm_fluid.cpp:524-559). */
 int zg_smf_set_flags(zg_ctx *ctx, int *flags);
 
+/* Rows [row0, row0 + nrows) of a rectangle's FP64 state (rows along x:
+ * cell (i, j) at i * ny + j), copied out (put = 0) or in (put = 1): fields
+ * holds 5 blocks of nrows * ny doubles (density, vx, vy, pressure, energy),
+ * wait the isolation counters of the same cells.  Host or device buffers.
+ * The halo exchange of a slab decomposition (zephyr_b200/slabs.py) moves
+ * these rows between ranks; it replaces the reference's mesh.sync of the
+ * layers part.init and part.wait (sm_fluid.cpp:86-97). */
+int zg_state_rows(zg_ctx *ctx, int row0, int nrows, double *fields, int *wait, int put);
+
+/* The CFL quantity of the current state, min over cells of
+ * incircle / (|v| + c), before CFL and max_dt (SmFluid::compute_dt,
+ * sm_fluid.cpp:104-111), with the kernels the configured step uses.  A slab
+ * decomposition takes the minimum over ranks (the reference's mpi::min) and
+ * caps the next step with CFL times it (zg_smf_set_max_dt). */
+int zg_smf_cfl_min(zg_ctx *ctx, double *dmin);
+
 /* Limited gradients of the current state, SmFluid::compute_grad
  * (sm_fluid.cpp:116-125; gradient.h:226-282, 412-474), computed with the
  * bit-exact kernels and copied to host arrays of 4 * n_cells doubles each:

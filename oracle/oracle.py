@@ -50,6 +50,8 @@ def lib():
         L.zo_solver_grad.argtypes = [C.c_void_p, _P, _P]
         L.zo_solver_compute_dt.argtypes = [C.c_void_p]
         L.zo_solver_compute_dt.restype = C.c_double
+        L.zo_solver_cfl_min.argtypes = [C.c_void_p]
+        L.zo_solver_cfl_min.restype = C.c_double
         L.zo_solver_step.argtypes = [C.c_void_p]
         L.zo_solver_step.restype = C.c_double
         L.zo_solver_steps.argtypes = [C.c_void_p, C.c_int, _P]
@@ -195,6 +197,10 @@ class Solver:
 
     def compute_dt(self):
         return lib().zo_solver_compute_dt(self.h)
+
+    def cfl_min(self):
+        """min over cells of incircle / (|v| + c), before CFL and max_dt."""
+        return lib().zo_solver_cfl_min(self.h)
 
     def step(self):
         return lib().zo_solver_step(self.h)

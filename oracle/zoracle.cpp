@@ -1385,6 +1385,19 @@ void zo_solver_grad(void *sp, double *gx, double *gy) {
         }
     }
 }
+// The CFL quantity before CFL and max_dt: min over cells of
+// incircle / (|v| + c) (sm_fluid.cpp:104-111).
+double zo_solver_cfl_min(void *sp) {
+    auto &s = *static_cast<zo::Solver *>(sp);
+    const zo::Mesh &m = *s.mesh;
+    double res = std::numeric_limits<double>::max();
+    for (int ic = 0; ic < m.n_cells; ++ic) {
+        double c = s.eos.sound_speed_rP(s.init[ic].density, s.init[ic].pressure);
+        double v = zo::incircle_diameter(m, ic) / (zo::norm(s.init[ic].velocity) + c);
+        res = std::min(res, v);
+    }
+    return res;
+}
 double zo_solver_compute_dt(void *sp) {
     auto &s = *static_cast<zo::Solver *>(sp);
     s.compute_dt();

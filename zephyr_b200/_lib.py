@@ -128,6 +128,8 @@ SIGNATURES = {
     "zg_smf_dt": (C.c_int, [_V, _P]),
     "zg_smf_set_flags": (C.c_int, [_V, _I]),
     "zg_smf_gradients": (C.c_int, [_V, _P, _P]),
+    "zg_state_rows": (C.c_int, [_V, C.c_int, C.c_int, _P, _I, C.c_int]),
+    "zg_smf_cfl_min": (C.c_int, [_V, _P]),
     "zg_launch_count": (C.c_int, [_V, C.POINTER(C.c_longlong)]),
     "zg_synchronize": (C.c_int, [_V]),
     "zg_set_timing": (C.c_int, [_V, C.c_int]),

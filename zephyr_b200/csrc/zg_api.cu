@@ -1039,6 +1039,64 @@ int zg_smf_set_flags(zg_ctx *c, int *flags) {
     return ZG_OK;
 }
 
+int zg_state_rows(zg_ctx *c, int row0, int nrows, double *fields, int *wait, int put) {
+    if (!c || !fields || !wait || nrows < 0) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_state_rows: solver not configured");
+    if (c->nx <= 0 || c->slots) return fail(c, ZG_ERR_STATE, "zg_state_rows: rows of a rectangle mesh");
+    if (c->par.precision != ZG_FP64) return fail(c, ZG_ERR_STATE, "zg_state_rows: the FP64 forms");
+    if (row0 < 0 || row0 + nrows > c->nx) return fail(c, ZG_ERR_ARG, "zg_state_rows: rows out of range");
+    DeviceGuard g(c->device);
+    const size_t off = (size_t)row0 * c->ny, cnt = (size_t)nrows * c->ny;
+    double *fld[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
+    int *w = c->d_wait + (size_t)c->wait_cur * c->cap;
+    // host or device buffers alike (unified addressing)
+    for (int k = 0; k < 5; ++k) {
+        if (put)
+            ZG_CUDA(c, cudaMemcpyAsync(fld[k] + off, fields + k * cnt, cnt * sizeof(double), cudaMemcpyDefault,
+                                       c->stream));
+        else
+            ZG_CUDA(c, cudaMemcpyAsync(fields + k * cnt, fld[k] + off, cnt * sizeof(double), cudaMemcpyDefault,
+                                       c->stream));
+    }
+    if (put)
+        ZG_CUDA(c, cudaMemcpyAsync(w + off, wait, cnt * sizeof(int), cudaMemcpyDefault, c->stream));
+    else
+        ZG_CUDA(c, cudaMemcpyAsync(wait, w + off, cnt * sizeof(int), cudaMemcpyDefault, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (put) c->cfl_valid = false;  // the next step takes its CFL minimum from the new rows
+    return ZG_OK;
+}
+
+int zg_smf_cfl_min(zg_ctx *c, double *dmin) {
+    if (!c || !dmin) return ZG_ERR_ARG;
+    if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_cfl_min: solver not configured");
+    if (c->par.precision != ZG_FP64) return fail(c, ZG_ERR_STATE, "zg_smf_cfl_min: the FP64 forms");
+    DeviceGuard g(c->device);
+    void *st = (void *)c->stream;
+    if (c->par.kernels != ZG_KERNELS_PARITY && !c->slots) {
+        // the FAST kernels' own CFL pass (the one their step runs after an upload)
+        tiled::Fields<double> f = fast_fields(c);
+        unsigned long long *slot = const_cast<unsigned long long *>(slot_ptr(c, 2));
+        f.slot_cur = slot;
+        cudaMemsetAsync(slot, 0x7F, sizeof(unsigned long long), c->stream);
+        SmfArgs a = make_args(c);
+        timed(c, ZG_K_DT, [&] { fast::launch_cfl(a, f, st); });
+        unsigned long long bits = 0;
+        ZG_CUDA(c, cudaMemcpyAsync(&bits, slot, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+        ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+        std::memcpy(dmin, &bits, sizeof(double));
+        return ZG_OK;
+    }
+    // the parity dt kernel with CFL 1 and no cap: dt = 1 * min = min
+    SmfArgs a = make_args(c);
+    a.CFL = 1.0;
+    a.max_dt = std::numeric_limits<double>::max();
+    timed(c, ZG_K_DT, [&] { parity::launch_dt(a, c->z, c->slots, st); });
+    ZG_CUDA(c, cudaMemcpyAsync(dmin, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ZG_OK;
+}
+
 int zg_smf_gradients(zg_ctx *c, double *d_dx, double *d_dy) {
     if (!c || !d_dx || !d_dy) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_gradients: solver not configured");
