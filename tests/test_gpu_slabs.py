@@ -55,7 +55,7 @@ def test_gpu_slabs_match_the_single_domain(gpu_lib, name, nx, ny, bounds, acc, s
 
     comm = S.LocalComm()
     for r in range(world):
-        slab = S.Slab(nx, ny, (0.0, 1.0, 0.0, 1.0), bounds, world, r)
+        slab = S.Slab(nx, ny, (0.0, 1.0, 0.0, 1.0), bounds, world, r, halo=S.halo_rows(acc, scheme == 1))
         loc = S.GpuSlabSolver(slab, Z.IdealGas(1.4), configure, kernels=Z.Kernels[kern])
         lo, hi = slab.rows
         gl, gh = slab.ghosts

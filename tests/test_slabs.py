@@ -78,7 +78,7 @@ def reference(nx, ny, bounds, acc, lim, steps):
 
 
 def local_slab(nx, ny, bounds, world, rank, acc, lim):
-    slab = S.Slab(nx, ny, (0.0, 1.0, 0.0, 1.0), bounds, world, rank)
+    slab = S.Slab(nx, ny, (0.0, 1.0, 0.0, 1.0), bounds, world, rank, halo=S.halo_rows(acc))
     loc = OracleSlab(slab, acc, lim, 0.4)
     lo, hi = slab.rows
     gl, gh = slab.ghosts

@@ -726,6 +726,31 @@ void launch_flux_pure(const MmArgs &a, void *stream) {
     if (a.fp32_flux) launch_flux_pure_fp32(a, stream);
     else k_flux_pure<double><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
+// The cells whose stencil (the cell and its four neighbours, boundary slots
+// counting as the cell itself) holds a mixed state: the list that
+// k_flux_pure builds, built ahead of it.
+__global__ void __launch_bounds__(BLOCK) k_classify(MmArgs a) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    StructAcc c(a.mesh, ic);
+    const int idx_c = pure_index(a.z, ic);
+    bool pure = idx_c >= 0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = c.face(s);
+        pure = pure && (is_boundary(g.flag) ? idx_c : pure_index(a.z, g.nb)) >= 0;
+    }
+    if (!pure) a.list_crp[atomicAdd(&a.counts[0], 1)] = ic;
+}
+void launch_classify(const MmArgs &a, void *stream) {
+    k_classify<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
+}
+void launch_crp_faces(const MmArgs &a, void *stream) {
+    k_crp_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
+}
+void launch_crp_update(const MmArgs &a, void *stream) {
+    k_crp_update<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
+}
 void launch_flux_crp(const MmArgs &a, void *stream) {
     k_crp_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
     k_crp_update<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);

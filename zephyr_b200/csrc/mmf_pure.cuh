@@ -186,8 +186,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_flux_pure(MmArgs a) {
         pure = pure && idx_n[s] >= 0;
     }
     if (!pure) {  // a mixed state in the stencil: the general path
-        int k = atomicAdd(&a.counts[0], 1);
-        a.list_crp[k] = ic;
+        if (!a.presorted) {
+            int k = atomicAdd(&a.counts[0], 1);
+            a.list_crp[k] = ic;
+        }
         return;
     }
     const double dt = a.dt_scale * *a.dt_out;

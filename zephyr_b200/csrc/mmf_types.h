@@ -44,6 +44,9 @@ struct MmArgs {
     // (Newton closure), with their conservative states.
     int *counts;     // [0] cells in list_crp, [1] cells in list_closure
     int *list_crp, *list_closure;
+    // list_crp filled beforehand (launch_classify): the pure-stencil kernel
+    // only skips the listed cells, so it may run beside the composite faces
+    int presorted;
     double *qbuf;    // (4 + NMAT) doubles per closure-list entry
     double *fbuf;    // (4 + NMAT) doubles per face of every list_crp cell (4 per cell)
     // second order (MmFluid::set_accuracy(2)): limiter, the half-step state
@@ -59,6 +62,11 @@ void launch_recover(const MmArgs &a, void *stream);
 void launch_flux_pure(const MmArgs &a, void *stream);
 void launch_flux_pure_fp32(const MmArgs &a, void *stream);  // mmf_mixed.cu
 void launch_flux_crp(const MmArgs &a, void *stream);  // face fluxes, then the cell updates
+// the same two halves separately, and the list of cells whose stencil holds a
+// mixed state (built before the pure-stencil kernel when the two overlap)
+void launch_classify(const MmArgs &a, void *stream);
+void launch_crp_faces(const MmArgs &a, void *stream);
+void launch_crp_update(const MmArgs &a, void *stream);
 void launch_closure(const MmArgs &a, void *stream);
 void launch_flags(const MmArgs &a, int *flags, void *stream);
 // second order: compute_grad, fluxes_stage1, fluxes_stage2 (mm_fluid.cpp:439-680)

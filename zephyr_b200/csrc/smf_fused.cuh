@@ -549,10 +549,12 @@ __global__ void __launch_bounds__(32 * (TH + 2), MINB) k_step(SmfArgs a, Fields<
                 f.qn[3][ic] = q.E;
             }
             st5(f.wn, ic, down<R>(zn));
-            // CFL term of the new state for the next step (sm_fluid.cpp:104-111)
-            const double c = sqrt(a.eos.gamma * (zn.p + a.eos.P0) * ri);
+            // CFL term of the new state for the next step (sm_fluid.cpp:104-111),
+            // with the arithmetic of k_cfl, which takes the minimum after an
+            // upload or a halo exchange: the same state gives the same dt
+            const double c = sqrt(a.eos.gamma * (zn.p + a.eos.P0) / zn.r);
             const double dinc = sqrt(smin(m.inc2x[i], m.inc2y[j]));
-            const double lam = dinc * rcp_nr(sqrt(zn.u * zn.u + zn.v * zn.v) + c);
+            const double lam = dinc / (sqrt(zn.u * zn.u + zn.v * zn.v) + c);
             if (lam >= 0.0) best = dbits(lam);
         }
     }

@@ -28,6 +28,11 @@ struct zg_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    // a second stream for work that overlaps the main stream's (the
+    // composite Riemann faces beside the pure-stencil cells), with its
+    // fork / join events; created on first use
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     long long launches = 0;
 
@@ -394,6 +399,40 @@ void timed(zg_ctx *c, int kind, F &&launch) {
     c->ev_pending.emplace_back(kind, i0);
 }
 
+// timed() for a launch on another stream of the context (its events are
+// recorded on that stream).
+template <class F>
+void timed_on(zg_ctx *c, int kind, cudaStream_t s, F &&launch) {
+    c->launches += 1;
+    if (!c->timing) {
+        launch();
+        return;
+    }
+    if (c->ev_used + 2 > c->ev_pool.size()) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            c->ev_pool.push_back(e);
+        }
+    }
+    int i0 = (int)c->ev_used;
+    c->ev_used += 2;
+    cudaEventRecord(c->ev_pool[i0], s);
+    launch();
+    cudaEventRecord(c->ev_pool[i0 + 1], s);
+    c->ev_pending.emplace_back(kind, i0);
+}
+
+// The side stream and its events, created on first use on the context's
+// device.
+int ensure_side(zg_ctx *c) {
+    if (c->side) return ZG_OK;
+    ZG_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    return ZG_OK;
+}
+
 // One step of SmFluid::update (sm_fluid.cpp:81-102) as kernel launches.
 int enqueue_parity_step(zg_ctx *c) {
     SmfArgs a = make_args(c);
@@ -630,6 +669,9 @@ int zg_destroy(zg_ctx *c) {
         for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
         if (c->out_img) cudaFreeHost(c->out_img);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
+        if (c->side) cudaStreamDestroy(c->side);
+        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+        if (c->ev_join) cudaEventDestroy(c->ev_join);
     }
     delete c;
     return ZG_OK;
@@ -1254,6 +1296,8 @@ int mm_check_error(zg_ctx *c) {
 // the x and y faces in turn with direction splitting.
 int enqueue_mm_step(zg_ctx *c) {
     void *st = (void *)c->stream;
+    int rc = ensure_side(c);
+    if (rc != ZG_OK) return rc;
     {
         mmf::MmArgs a = make_mm_args(c);
         timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(a, st); });
@@ -1274,8 +1318,18 @@ int enqueue_mm_step(zg_ctx *c) {
             return;
         }
         if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
+        // the cells next to a mixed state are listed first; then their
+        // composite faces (side stream) run beside the pure-stencil cells
+        // (main stream): the two write disjoint data
+        a.presorted = 1;
+        timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_classify(a, st); });
+        cudaEventRecord(c->ev_fork, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        timed_on(c, ZG_K_MM_CRP, c->side, [&] { mmf::launch_crp_faces(a, (void *)c->side); });
         timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux_pure(a, st); });
-        timed(c, ZG_K_MM_CRP, [&] { mmf::launch_flux_crp(a, st); });
+        cudaEventRecord(c->ev_join, c->side);
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        timed(c, ZG_K_MM_CRP, [&] { mmf::launch_crp_update(a, st); });
         timed(c, ZG_K_MM_CLOSURE, [&] { mmf::launch_closure(a, st); });
         std::swap(c->mz, c->mznext);  // MmFluid::swap (mm_fluid.cpp:682-684)
     };

@@ -8,15 +8,17 @@ mesh/euler/tourism.h), and compute_dt takes the minimum over ranks
 rows (rows run along x; cell (i, j) is i * ny + j, so a row block is
 contiguous in memory):
 
-- rank r owns rows [i_lo, i_hi) and keeps `halo` = 2 ghost rows on each side
+- rank r owns rows [i_lo, i_hi) and keeps `halo` ghost rows on each side
   that has a neighbour (both sides on an x-periodic rectangle, the inner
-  sides otherwise); its local rectangle is those rows, with the global
+  sides otherwise): as many rows as one step reads away from a cell
+  (halo_rows: 2 for the predictor-corrector, 4 for Heun's two stages, 1 for
+  first order); its local rectangle is those rows, with the global
   boundary flags on the outer sides and ZOE at the ghost ends (the ghost
   rows' own updates are never used);
 - once per step the ghost rows are refreshed from the neighbours' owned rows
-  (zg_state_rows out, a send / receive, zg_state_rows in): the whole
-  two-stage step reads cells at most two rows away, so one exchange of two
-  rows per step replaces the reference's three syncs of one layer;
+  (zg_state_rows out, a send / receive, zg_state_rows in): one exchange of
+  the step's reach replaces the reference's three syncs of one layer (the
+  ghost rows' own updates are garbage and are never read);
 - dt: every rank computes the CFL minimum of its rows (owned and ghost, all
   current after the exchange; zg_smf_cfl_min), the ranks take the minimum
   (all-reduce MIN), and each local step is capped at CFL times it
@@ -42,6 +44,16 @@ import numpy as np
 HALO = 2
 ZOE = 2
 PERIODIC = 3
+
+
+def halo_rows(accuracy: int, heun: bool = False) -> int:
+    """Ghost rows one exchange per step needs: the rows a step reads away
+    from a cell -- 1 for first order, 2 for the predictor-corrector
+    (gradients, then the corrector's faces), 4 for Heun's two stages of
+    gradients and faces."""
+    if accuracy == 1:
+        return 1
+    return 4 if heun else 2
 
 
 @dataclass(frozen=True)
