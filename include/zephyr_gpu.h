@@ -628,11 +628,13 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *prm, const double *rho, cons
  * GPU that loads the library, held until the process exits).  nx and ny up
  * to ZG_NOALLOC_MAX_AXIS are accepted; larger meshes return
  * ZG_ERR_TOO_LARGE.  Every call resets the scratch it needs on `stream`
- * before use.  The first call on a device looks up that array's address (and
- * may load the library's device code there); make it before any stream
- * capture on that device.  Calls that overlap on one device -- on different
- * streams, or from different host threads -- share the one array and race:
- * serialise them. */
+ * before use.  Every call looks up that array's address on the device (the
+ * first lookup on a device may load the library's device code there; make
+ * the first call before any stream capture on that device).  Calls that
+ * overlap on one device -- on different streams, or from different host
+ * threads -- share the one array and race: serialise them.  Every flux of
+ * zg_flux is accepted.  A CUDA error already pending when the call starts
+ * returns ZG_ERR_CUDA before anything is launched and is left pending. */
 int zg_rect_step_noalloc(int device, int nx, int ny, double x_min, double x_max, double y_min,
                          double y_max, const int bounds[4], const zg_smf_params *p, const double *const in[5],
                          double *const out[5], double *dt, void *stream);

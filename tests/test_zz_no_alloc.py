@@ -17,12 +17,15 @@ pytestmark = pytest.mark.gpu
 TOLERANCE = 0.0  # bit-exact: same kernels, same order of operations
 
 
-def _existing_path(Z, nx, ny, box, bounds, flux, CFL, state, steps):
+WATER = (4.4, 6.0e8, 0.0)  # stiffened gas: gamma, P0, e0
+
+
+def _existing_path(Z, nx, ny, box, bounds, flux, CFL, state, steps, stiff=False):
     gen = Z.Rectangle(*box)
     gen.set_boundaries(Z.Boundaries(*bounds))
     gen.set_sizes(nx, ny)
     mesh = Z.EuMesh(gen)
-    solver = Z.SmFluid(Z.IdealGas(1.4))
+    solver = Z.SmFluid(Z.StiffenedGas(*WATER) if stiff else Z.IdealGas(1.4))
     solver.set_accuracy(1)
     solver.set_CFL(CFL)
     solver.set_method(Z.Fluxes(flux))
@@ -36,13 +39,16 @@ def _existing_path(Z, nx, ny, box, bounds, flux, CFL, state, steps):
     return out
 
 
-def _noalloc_path(Z, nx, ny, box, bounds, flux, CFL, state, steps):
+def _noalloc_path(Z, nx, ny, box, bounds, flux, CFL, state, steps, stiff=False):
     import torch
     from zephyr_b200 import _lib
 
     lib = Z.load()
     p = _lib.SmfParams()
     lib.zg_smf_default_params(C.byref(p))
+    if stiff:
+        p.eos_kind = 1
+        p.gamma, p.P0, p.e0 = WATER
     p.flux = flux
     p.CFL = CFL
     p.accuracy = 1
@@ -68,16 +74,34 @@ CASES = [
     # nx, ny, box, bounds (L, R, B, T), flux, CFL, workload
     (64, 48, (0.0, 1.0, 0.0, 0.75), (2, 2, 1, 1), 3, 0.4, "random"),
     (96, 96, (0.0, 1.0, 0.0, 1.0), (3, 3, 3, 3), 2, 0.5, "fourier"),
+    # the largest axis: the coordinate tables fill the scratch to its end
+    (8192, 4, (0.0, 2.0, 0.0, 0.001), (2, 1, 3, 3), 3, 0.4, "random"),
+    (4, 8192, (0.0, 0.001, 0.0, 2.0), (3, 3, 1, 2), 3, 0.4, "random"),
+    # stiffened gas (P0, e0 and the minimum pressure from the parameters), walls and ZOE
+    (40, 32, (0.0, 0.1, 0.0, 0.08), (1, 2, 2, 1), 3, 0.4, "water"),
+    # the other fluxes of the parity kernels
+    (48, 40, (0.0, 1.0, 0.0, 1.0), (2, 2, 1, 1), 1, 0.4, "random"),
+    (48, 40, (0.0, 1.0, 0.0, 1.0), (3, 3, 2, 2), 6, 0.4, "random"),
 ]
+IDS = ["random_64x48_hllc_walls", "fourier_96_hll_periodic", "random_8192x4_max_x", "random_4x8192_max_y",
+       "water_40x32_walls_zoe", "random_48x40_rusanov", "random_48x40_cir1"]
 
 
-@pytest.mark.parametrize("case", CASES, ids=["random_64x48_hllc_walls", "fourier_96_hll_periodic"])
+@pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_noalloc_step_matches_zg_smf_update(gpu_lib, case):
     Z = gpu_lib
     from zephyr_b200.workloads import fourier_smooth
 
     nx, ny, box, bounds, flux, CFL, kind = case
-    if kind == "random":
+    stiff = kind == "water"
+    if kind == "water":
+        rng = np.random.default_rng(23)
+        n = nx * ny
+        rho = 1000.0 * (1.0 + 0.01 * rng.random(n))
+        u, v = 5.0 * rng.standard_normal(n), 5.0 * rng.standard_normal(n)
+        p = 1.0e5 * (1.0 + rng.random(n))
+        state = (rho, u, v, p, (p + WATER[0] * WATER[1]) / ((WATER[0] - 1.0) * rho))
+    elif kind == "random":
         rng = np.random.default_rng(17)
         n = nx * ny
         rho = 1.0 + 0.3 * rng.random(n)
@@ -86,8 +110,8 @@ def test_noalloc_step_matches_zg_smf_update(gpu_lib, case):
         state = (rho, u, v, p, p / (0.4 * rho))
     else:
         state = tuple(np.asarray(a) for a in fourier_smooth(nx).state)
-    want = _existing_path(Z, nx, ny, box, bounds, flux, CFL, state, 2)
-    got = _noalloc_path(Z, nx, ny, box, bounds, flux, CFL, state, 2)
+    want = _existing_path(Z, nx, ny, box, bounds, flux, CFL, state, 2, stiff)
+    got = _noalloc_path(Z, nx, ny, box, bounds, flux, CFL, state, 2, stiff)
     for (dt_w, st_w), (dt_g, st_g) in zip(want, got):
         assert abs(dt_g - dt_w) <= TOLERANCE * abs(dt_w)
         for a, b in zip(st_g, st_w):

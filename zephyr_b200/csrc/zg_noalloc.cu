@@ -20,7 +20,6 @@
 
 #include <algorithm>
 #include <limits>
-#include <mutex>
 
 #include "../../include/zephyr_gpu.h"
 #include "smf_types.h"
@@ -40,19 +39,16 @@ constexpr size_t kScratchDoubles = kHeader + 8 * (size_t)kMaxAxis + 8;
 static __device__ __align__(256) double g_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double *g_ptr[kMaxDevices] = {};
 
-// Device address of g_scratch on the current device, looked up once per
-// device.  The lookup may load the library's device code on that device.
-int scratch_on(int device, double **out) {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_ptr[device]) {
-        double *p = nullptr;
-        if (cudaGetSymbolAddress((void **)&p, g_scratch) != cudaSuccess || !p) return ZG_ERR_CUDA;
-        g_ptr[device] = p;
-    }
-    *out = g_ptr[device];
+// Device address of g_scratch on the current device.  Looked up on every
+// call (cheap once the module is loaded), so that a context torn down and
+// created again (cudaDeviceReset), which may load the module at another
+// address, is followed.  The first lookup on a device may load the library's
+// device code there.
+int scratch_on(double **out) {
+    double *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_scratch) != cudaSuccess || !p) return ZG_ERR_CUDA;
+    *out = p;
     return ZG_OK;
 }
 
@@ -116,7 +112,7 @@ extern "C" int zg_rect_step_noalloc(int device, int nx, int ny, double x_min, do
             if (out[k] == in[j]) return ZG_ERR_ARG;  // the step reads neighbours of every cell
     }
     if (p->eos_kind != ZG_EOS_IDEAL && p->eos_kind != ZG_EOS_STIFFENED) return ZG_ERR_ARG;
-    if (p->flux != ZG_FLUX_HLLC && p->flux != ZG_FLUX_HLL) return ZG_ERR_ARG;
+    if (p->flux < ZG_FLUX_GODUNOV || p->flux > ZG_FLUX_CIR2) return ZG_ERR_ARG;
     if (!(p->gamma > 1.0)) return ZG_ERR_ARG;
     if (std::min(std::max(1, p->accuracy), 2) != 1 || p->precision != ZG_FP64 || p->kernels != ZG_KERNELS_PARITY)
         return ZG_ERR_ARG;  // first order, FP64, parity kernels only
@@ -126,8 +122,11 @@ extern "C" int zg_rect_step_noalloc(int device, int nx, int ny, double x_min, do
 
     DeviceSwitch sw(device);
     if (!sw.ok) return ZG_ERR_CUDA;
+    // an error left pending by the caller's own earlier work is not this
+    // call's: it is reported, and left pending, before anything is launched
+    if (cudaPeekAtLastError() != cudaSuccess) return ZG_ERR_CUDA;
     double *s = nullptr;
-    int rc = scratch_on(device, &s);
+    int rc = scratch_on(&s);
     if (rc != ZG_OK) return rc;
 
     int bc[4] = {bounds[0], bounds[1], bounds[2], bounds[3]};
@@ -175,7 +174,9 @@ extern "C" int zg_rect_step_noalloc(int device, int nx, int ny, double x_min, do
     cudaStream_t st = (cudaStream_t)stream;
     int span = std::max(nx, ny) + 1;
     k_fill_tables<<<(span + 255) / 256, 256, 0, st>>>(s, nx, ny, x_min, x_max, y_min, y_max);
+    if (cudaGetLastError() != cudaSuccess) return ZG_ERR_CUDA;
     parity::launch_dt(a, a.z, false, stream);
+    if (cudaGetLastError() != cudaSuccess) return ZG_ERR_CUDA;
     parity::launch_flux1(a, false, stream);
     if (cudaGetLastError() != cudaSuccess) return ZG_ERR_CUDA;
     if (dt && cudaMemcpyAsync(dt, s + 2, sizeof(double), cudaMemcpyDefault, st) != cudaSuccess)
