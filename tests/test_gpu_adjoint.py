@@ -146,8 +146,8 @@ def test_adjoint_through_torch_autograd(gpu_lib):
 
 
 def test_mixed_adjoint_tracks_the_fp64_adjoint(gpu_lib):
-    """The mixed adjoint (FP32 primitive states, slopes, HLLC and its reverse;
-    FP64 conserved and adjoint states and sums): J to 1e-8, the gradient to
+    """The mixed adjoint (FP32 slopes from FP64 differences, face states, HLLC
+    and its reverse; FP64 primitive, conserved and adjoint states and sums): J to 1e-8, the gradient to
     1e-4 in the L2 norm against the FP64 adjoint, and directional derivatives
     within 1e-3 of central differences of the FP64 forward."""
     import torch

@@ -60,9 +60,9 @@ struct Grid {
     double hx, hy, vol;
     double x0, y0;
 };
-// four field arrays of element type S (FP64 state and adjoint fields are
-// double; the primitive states, slopes and face cotangents are S = double in
-// the FP64 form and S = float in the mixed form)
+// four field arrays of element type S (FP64 state, adjoint and primitive
+// fields are double; the slopes and face cotangents are S = double in the
+// FP64 form and S = float in the mixed form)
 template <class S>
 struct F4T {
     S *f[4];
@@ -117,11 +117,11 @@ __global__ void k_init(Grid g, CF4 W0, double gamma, F4 U) {
     U.f[3][ic] = p / (gamma - 1.0) + 0.5 * (r * (u * u + v * v));
 }
 
-// primitive state and limited slopes of every cell: the primitive map in
-// FP64, rounded to S; the slopes from the rounded values in S
+// primitive state and limited slopes of every cell: the primitive map and
+// the neighbour differences in FP64, the slopes from the differences in S
 template <class S>
 __global__ void __launch_bounds__(BLOCK, ZG_ADJ_PG_MINB) k_prim_grad(Grid g, CF4 U, double gamma, double eps,
-                                                                     F4T<S> W, F4T<S> gx, F4T<S> gy) {
+                                                                     F4 W, F4T<S> gx, F4T<S> gy) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= g.n) return;
     double wc[4], wl[4], wr[4], wb[4], wt[4];
@@ -134,22 +134,23 @@ __global__ void __launch_bounds__(BLOCK, ZG_ADJ_PG_MINB) k_prim_grad(Grid g, CF4
     const S i2x = S(0.5 / g.hx), i2y = S(0.5 / g.hy), e = S(eps);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        W.f[k][ic] = S(wc[k]);
-        gx.f[k][ic] = slope<S>(S(wl[k]), S(wc[k]), S(wr[k]), i2x, e);
-        gy.f[k][ic] = slope<S>(S(wb[k]), S(wc[k]), S(wt[k]), i2y, e);
+        W.f[k][ic] = wc[k];
+        gx.f[k][ic] = slope<S>(S(wl[k] - wc[k]), S(wr[k] - wc[k]), i2x, e);
+        gy.f[k][ic] = slope<S>(S(wb[k] - wc[k]), S(wt[k] - wc[k]), i2y, e);
     }
 }
 
 // Face states of the face between `lo` and `hi` along an axis, in the face
-// frame (x faces: (rho, u, v, p); y faces: (rho, v, -u, p)).
+// frame (x faces: (rho, u, v, p); y faces: (rho, v, -u, p)): the FP64
+// primitive state rounded to S, plus or minus the slope times h / 2 in S.
 template <class S>
-__device__ __forceinline__ void face_states(const CF4T<S> &W, const CF4T<S> &G, int lo, int hi, S half_h, bool yface,
+__device__ __forceinline__ void face_states(const CF4 &W, const CF4T<S> &G, int lo, int hi, S half_h, bool yface,
                                             S L[4], S R[4]) {
     S a[4], b[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        a[k] = W.f[k][lo] + G.f[k][lo] * half_h;
-        b[k] = W.f[k][hi] - G.f[k][hi] * half_h;
+        a[k] = S(W.f[k][lo]) + G.f[k][lo] * half_h;
+        b[k] = S(W.f[k][hi]) - G.f[k][hi] * half_h;
     }
     if (!yface) {
 #pragma unroll
@@ -178,7 +179,7 @@ __device__ __forceinline__ void flux_global(const S Fl[4], bool yface, S F[4]) {
 
 // out = alpha * base + beta * (X + dt L(X)), L from the face fluxes of W, G
 template <class S>
-__global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, CF4T<S> W, CF4T<S> gx, CF4T<S> gy,
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, CF4 W, CF4T<S> gx, CF4T<S> gy,
                                                                        double gamma, CF4 X, CF4 base, double alpha,
                                                                        double beta, double dt, F4 out) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(BLOCK) k_probe(Grid g, CF4 U, double gamma, do
 // primitive frame, go to fb[face][0..3] and fb[face][4..7]; the faces' gamma
 // parts to gacc.
 template <class S>
-__global__ void __launch_bounds__(BLOCK, ZG_ADJ_VF_MINB) k_vjp_faces(Grid g, CF4T<S> W, CF4T<S> gx, CF4T<S> gy,
+__global__ void __launch_bounds__(BLOCK, ZG_ADJ_VF_MINB) k_vjp_faces(Grid g, CF4 W, CF4T<S> gx, CF4T<S> gy,
                                                                      double gamma, CF4 mu, double coef, S *fbx,
                                                                      S *fby, double *gacc) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
@@ -349,12 +350,13 @@ __device__ __forceinline__ int wrapc(int x, int n) {
 }
 
 // d0 * gb and d2 * gb of a cell's slope along one axis (its contributions to
-// its low and high neighbour), and d1 * gb (its own), for field k, in S
+// its low and high neighbour), and d1 * gb (its own), for field k: the
+// differences in FP64, the partials in S
 template <class S>
-__device__ __forceinline__ void slope_terms(S wm, S w0, S wp, S i2h, S eps, S gb, double &to_lo, double &own,
-                                            double &to_hi) {
+__device__ __forceinline__ void slope_terms(double wm, double w0, double wp, S i2h, S eps, S gb, double &to_lo,
+                                            double &own, double &to_hi) {
     S d[3];
-    slope_partials<S>(wm, w0, wp, i2h, eps, d);
+    slope_partials<S>(S(wm - w0), S(wp - w0), i2h, eps, d);
     to_lo = (double)(d[0] * gb);
     own = (double)(d[1] * gb);
     to_hi = (double)(d[2] * gb);
@@ -362,7 +364,7 @@ __device__ __forceinline__ void slope_terms(S wm, S w0, S wp, S i2h, S eps, S gb
 
 template <class S>
 __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
-    Grid g, CF4 X, CF4T<S> W, double gamma, double eps, const S *fbx, const S *fby, CF4 base, double base_coef,
+    Grid g, CF4 X, CF4 W, double gamma, double eps, const S *fbx, const S *fby, CF4 base, double base_coef,
     CF4 add, F4 out, double *gacc) {
     // contributions of tile positions to their neighbours: x (i) rows -1..VI,
     // y (j) columns -1..VJ
@@ -404,10 +406,10 @@ __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
         const S *fl = fbx + k * n, *fh = fbx + (4 + k) * n, *gl = fby + k * n, *gh = fby + (4 + k) * n;
-        const S *w = W.f[k];
+        const double *w = W.f[k];
         // own position: slope cotangents and partials on both axes
         const S xl_c = fl[c.ic], xh_l = fh[cl.ic], yl_c = gl[c.ic], yh_b = gh[cb.ic];
-        const S w_c = w[c.ic];
+        const double w_c = w[c.ic];
         double ox, oy, lo, hi;
         slope_terms<S>(w[cl.ic], w_c, w[cr.ic], i2x, se, hx2 * (xl_c - xh_l), lo, ox, hi);
         sx_lo[ti + 1][tj] = lo;
@@ -596,8 +598,8 @@ struct WG {  // primitive states and slopes of one stage
 // states and slopes go to sa and sb
 // (need_out = false: the step's result is not wanted, only its stages)
 // the same arrays viewed as element type S (the mixed form keeps its FP32
-// primitive states, slopes and face cotangents in the first half of the
-// FP64-sized buffers)
+// slopes and face cotangents in the first half of the FP64-sized buffers;
+// the primitive states are FP64 in both forms)
 template <class S>
 F4T<S> as(const F4 &x) {
     return F4T<S>{{reinterpret_cast<S *>(x.f[0]), reinterpret_cast<S *>(x.f[1]), reinterpret_cast<S *>(x.f[2]),
@@ -613,15 +615,13 @@ template <class S>
 void heun_step_t(zg_adj *a, cudaStream_t st, const zg_adj_params &p, const F4 &X, const F4 &star, const F4 &out,
                  const WG &sa, const WG &sb, bool need_out) {
     unsigned nb = nblocks(a);
-    k_prim_grad<S><<<nb, BLOCK, 0, st>>>(a->g, cf(X), p.gamma, p.limiter_eps, as<S>(sa.W), as<S>(sa.gx),
-                                         as<S>(sa.gy));
-    k_flux_update<S><<<nb, BLOCK, 0, st>>>(a->g, cas<S>(sa.W), cas<S>(sa.gx), cas<S>(sa.gy), p.gamma, cf(X), kNull,
+    k_prim_grad<S><<<nb, BLOCK, 0, st>>>(a->g, cf(X), p.gamma, p.limiter_eps, sa.W, as<S>(sa.gx), as<S>(sa.gy));
+    k_flux_update<S><<<nb, BLOCK, 0, st>>>(a->g, cf(sa.W), cas<S>(sa.gx), cas<S>(sa.gy), p.gamma, cf(X), kNull,
                                            0.0, 1.0, p.dt, star);
-    k_prim_grad<S><<<nb, BLOCK, 0, st>>>(a->g, cf(star), p.gamma, p.limiter_eps, as<S>(sb.W), as<S>(sb.gx),
-                                         as<S>(sb.gy));
+    k_prim_grad<S><<<nb, BLOCK, 0, st>>>(a->g, cf(star), p.gamma, p.limiter_eps, sb.W, as<S>(sb.gx), as<S>(sb.gy));
     a->launches += 3;
     if (!need_out) return;
-    k_flux_update<S><<<nb, BLOCK, 0, st>>>(a->g, cas<S>(sb.W), cas<S>(sb.gx), cas<S>(sb.gy), p.gamma, cf(star),
+    k_flux_update<S><<<nb, BLOCK, 0, st>>>(a->g, cf(sb.W), cas<S>(sb.gx), cas<S>(sb.gy), p.gamma, cf(star),
                                            cf(X), 0.5, 0.5, p.dt, out);
     ++a->launches;
 }
@@ -650,9 +650,9 @@ void vjp_t(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F
            double base_coef, const CF4 &add, const F4 &out, double *gacc) {
     unsigned nb = nblocks(a);
     S *fbx = reinterpret_cast<S *>(a->fbx), *fby = reinterpret_cast<S *>(a->fby);
-    k_vjp_faces<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cas<S>(wg.W), cas<S>(wg.gx), cas<S>(wg.gy), p.gamma, cf(mu),
+    k_vjp_faces<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cf(wg.W), cas<S>(wg.gx), cas<S>(wg.gy), p.gamma, cf(mu),
                                                 coef, fbx, fby, gacc);
-    k_vjp_cells_tiled<S><<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(X), cas<S>(wg.W), p.gamma,
+    k_vjp_cells_tiled<S><<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(X), cf(wg.W), p.gamma,
                                                                      p.limiter_eps, fbx, fby, cf(base), base_coef,
                                                                      add, out, gacc);
     a->launches += 2;

@@ -55,19 +55,21 @@ __device__ __forceinline__ void prim(const T U[4], const T &gamma, T W[4]) {
     W[3] = (gamma - T(1)) * (U[3] - T(0.5) * ((U[1] * U[1] + U[2] * U[2]) / U[0]));
 }
 
-// limited slope of one field along one axis from its three values:
-//   (phi(-dL, dR) dR - phi(-dR, dL) dL) / (2h)
-// where both limiter values share the denominator dL^2 + dR^2 + eps, so that
-//   = (dL - dR) (2 dL dR - eps) / (dL^2 + dR^2 + eps) / (2h).
+// limited slope of one field along one axis from the differences
+// a = w_{i-1} - w_i and b = w_{i+1} - w_i of its three values:
+//   (phi(-a, b) b - phi(-b, a) a) / (2h)
+// where both limiter values share the denominator a^2 + b^2 + eps, so that
+//   = (a - b) (2 a b - eps) / (a^2 + b^2 + eps) / (2h).
+// The differences are taken by the caller in FP64 (the values are FP64 in
+// both forms): in FP32 the difference of two neighbouring values of a smooth
+// field keeps only the digits their FP32 roundings share.
 template <class T>
-__device__ __forceinline__ T slope(T wm, T w0, T wp, T inv2h, T eps) {
-    T a = wm - w0, b = wp - w0;
+__device__ __forceinline__ T slope(T a, T b, T inv2h, T eps) {
     return inv2h * ((a - b) * (T(2) * a * b - eps)) / (a * a + b * b + eps);
 }
-// its partial derivatives with respect to (wm, w0, wp)
+// its partial derivatives with respect to (w_{i-1}, w_i, w_{i+1})
 template <class T>
-__device__ __forceinline__ void slope_partials(T wm, T w0, T wp, T inv2h, T eps, T d[3]) {
-    T a = wm - w0, b = wp - w0;
+__device__ __forceinline__ void slope_partials(T a, T b, T inv2h, T eps, T d[3]) {
     T q = T(2) * a * b - eps, P = (a - b) * q;
     T iD = T(1) / (a * a + b * b + eps);
     T Pa = q + (a - b) * (T(2) * b), Pb = -q + (a - b) * (T(2) * a);
