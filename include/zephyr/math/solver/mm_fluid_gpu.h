@@ -14,8 +14,11 @@
 // two of them, each IdealGas or StiffenedGas.  update() copies part.init in,
 // runs MmFluid::update (mm_fluid.cpp:112-171) with the bit-exact kernels and
 // copies the new state back; set_flags() gives MmFluid::set_flags
-// (mm_fluid.cpp:836-885).  Not on the GPU: gravity (set_gravity with g != 0
-// throws), CrpMode::MUSCL, fluxes other than HLLC and CRP, refined meshes.
+// (mm_fluid.cpp:836-885).  CrpMode::MUSCL fills part.grad_a as
+// fractions_grad does and, like the reference's assert, throws on a step that
+// reaches a composite face (the reference defines no face fraction for it).
+// Not on the GPU: gravity (set_gravity with g != 0 throws), fluxes other than
+// HLLC and CRP, refined meshes.
 //
 // Errors throw std::runtime_error with the library's message.
 #pragma once
@@ -100,7 +103,6 @@ public:
     }
     void set_crp_mode(CrpMode mode) {
         if (mode == CrpMode::NONE) return;  // mm_fluid.cpp:63-70
-        if (mode == CrpMode::MUSCL) throw std::runtime_error("MmFluidGPU: CrpMode::MUSCL is not implemented on the GPU");
         m_par.crp_mode = static_cast<int>(mode);
         reconfigure();
     }
@@ -125,6 +127,7 @@ public:
         check(zg_mmf_update(m_ctx));
         get_state(mesh);
         check(zg_mmf_dt(m_ctx, &m_dt));
+        if (m_par.crp_mode == ZG_CRP_MUSCL) get_grad_a(mesh);
     }
 
     /// MmFluid::set_flags (mm_fluid.cpp:836-885).
@@ -223,6 +226,20 @@ private:
             }
         }
         check(zg_mmf_state_upload(m_ctx, m_buf.data()));
+    }
+
+    // part.grad_a (CrpMode::MUSCL): the volume-fraction gradients of the step
+    void get_grad_a(EuMesh &mesh) {
+        const size_t n = mesh.n_cells();
+        const int m = m_mix.size();
+        m_buf.resize(2 * m * n);
+        check(zg_mmf_grad_a(m_ctx, m_buf.data()));
+        for (size_t ic = 0; ic < n; ++ic) {
+            EuCell cell = mesh[ic];
+            auto ga = cell[part.grad_a];
+            for (int k = 0; k < m; ++k)
+                ga[k] = Vector3d(m_buf[2 * (m * ic + k)], m_buf[2 * (m * ic + k) + 1], 0.0);
+        }
     }
 
     void get_state(EuMesh &mesh) {

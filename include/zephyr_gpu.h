@@ -376,11 +376,17 @@ typedef struct zg_material {
  * reference evaluates them.  Returns ZG_ERR_ARG for an unknown name. */
 int zg_material_named(int kind, const char *name, zg_material *out);
 
-/* CRP mode: values of the reference's CrpMode (mm_fluid.h:31-37).  NONE
+/* CRP mode: values of the reference's CrpMode (mm_fluid.h:31-41).  NONE
  * uses the plain mixture HLLC flux on every face; V3, V5, VS choose the
  * interface fraction by the heuristics of sections.cpp:50-84; PLIC
- * reconstructs the interface (the default). */
-enum zg_crp_mode { ZG_CRP_NONE = 0, ZG_CRP_V3 = 1, ZG_CRP_V5 = 2, ZG_CRP_VS = 3, ZG_CRP_PLIC = 4 };
+ * reconstructs the interface (the default).  MUSCL computes the limited
+ * volume-fraction gradients of every cell each sub-step (fractions_grad,
+ * mm_fluid.cpp:469-482; zg_mmf_grad_a reads them); the reference gives it no
+ * face fraction (alpha_sigma returns NaN, mm_fluid.cpp:245-250, which
+ * calc_crp_flux's assert rejects, mm_fluid.cpp:276), so a step that reaches
+ * a composite face under MUSCL reports ZG_ERR_NUMERIC; faces whose states
+ * are pure take the plain flux as in the reference. */
+enum zg_crp_mode { ZG_CRP_NONE = 0, ZG_CRP_V3 = 1, ZG_CRP_V5 = 2, ZG_CRP_VS = 3, ZG_CRP_PLIC = 4, ZG_CRP_MUSCL = 5 };
 
 /* MmFluid(MixturePT) and its setters (mm_fluid.h:58-100). */
 /* Direction splitting of the multi-material step, values of DirSplit
@@ -438,6 +444,12 @@ int zg_mmf_dt(zg_ctx *ctx, double *dt);
 
 /* Refinement flags of MmFluid::set_flags (mm_fluid.cpp:836-885). */
 int zg_mmf_set_flags(zg_ctx *ctx, int *flags);
+
+/* CrpMode::MUSCL: the volume-fraction gradients of the last sub-step,
+ * part.grad_a of MmFluid::fractions_grad (mm_fluid.cpp:469-482): per cell
+ * 2 * n_materials doubles, (d alpha_i / dx, d alpha_i / dy) for each
+ * material i.  ZG_ERR_STATE before a MUSCL step.  Synchronises the stream. */
+int zg_mmf_grad_a(zg_ctx *ctx, double *out);
 
 /* The PLIC reconstruction of the current state (interface_recovery,
  * mm_fluid.cpp:484-519): per cell and material the unit normal (x, y) and

@@ -42,6 +42,7 @@ def lib():
         L.zmm_compute_dt.argtypes = [C.c_void_p]
         L.zmm_compute_dt.restype = C.c_double
         L.zmm_interface.argtypes = [C.c_void_p, _P, _P]
+        L.zmm_fractions_grad.argtypes = [C.c_void_p, _P]
         L.zmm_flags.argtypes = [C.c_void_p, _I]
         L.zmm_state_from_q.argtypes = [C.c_void_p, _P, _P, _P]
         L.zmm_sound_speed.argtypes = [C.c_void_p, _P]
@@ -110,6 +111,12 @@ class RefMmFluid:
         off = np.empty((self.n, self.nmat))
         lib().zmm_interface(self.h, _dp(nrm), _dp(off))
         return nrm, off
+
+    def fractions_grad(self):
+        """MmFluid::fractions_grad of the current state: (n, nmat, 2)."""
+        g = np.empty((self.n, self.nmat, 2))
+        lib().zmm_fractions_grad(self.h, _dp(g))
+        return g
 
     def flags(self):
         f = np.empty(self.n, np.int32)

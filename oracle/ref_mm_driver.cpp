@@ -182,6 +182,22 @@ void zmm_interface(void *p, double *nrm /* 2 * nmat per cell */, double *off /* 
     }
 }
 
+// MmFluid::fractions_grad (mm_fluid.cpp:469-482) on the current state; per
+// cell and material the gradient (x, y) of the volume fraction (part.grad_a).
+void zmm_fractions_grad(void *p, double *g /* 2 * nmat per cell */) {
+    auto *r = static_cast<RefMm *>(p);
+    r->solver->fractions_grad(*r->mesh, r->part.init);
+    int n = (int)r->mesh->n_cells(), m = r->mixture.size();
+    for (int i = 0; i < n; ++i) {
+        EuCell cell = (*r->mesh)[i];
+        auto ga = cell[r->part.grad_a];
+        for (int k = 0; k < m; ++k) {
+            g[(size_t)(i * m + k) * 2] = ga[k].x();
+            g[(size_t)(i * m + k) * 2 + 1] = ga[k].y();
+        }
+    }
+}
+
 // MmFluid::set_flags: refinement flags per cell.
 void zmm_flags(void *p, int *flags) {
     auto *r = static_cast<RefMm *>(p);

@@ -234,3 +234,50 @@ def test_gpu_mm_full_size_matches_reference(gpu_lib, acc, steps):
     bad = ~((g == o) | (np.isnan(g) & np.isnan(o)))
     assert not bad.any(), f"{np.count_nonzero(bad.any(axis=1))} of {n * n} cells differ after {steps} steps"
     mesh.close()
+
+
+def test_gpu_mm_muscl_fraction_gradients_match_reference(gpu_lib):
+    """CrpMode::MUSCL.  The reference computes the limited volume-fraction
+    gradients each sub-step (fractions_grad, mm_fluid.cpp:469-482) and gives
+    the mode no face fraction (alpha_sigma returns NaN, mm_fluid.cpp:245-250,
+    which calc_crp_flux's assert rejects).  (a) With pure cells only (a sharp
+    water / air interface at rest, the shock still far away) every face takes
+    the plain flux: five steps bit-exact with the reference's MUSCL steps,
+    and each step's grad_a equal to the reference's fractions_grad of the
+    state it started from.  (b) On the shock / water column (mixed cells) the
+    GPU step's grad_a equals fractions_grad of the initial state and the step
+    reports the missing face fraction (the reference is not stepped there:
+    its assert would end the process)."""
+    from oracle import ref_mm as RM
+    if not RM.available():
+        pytest.fail("oracle/_ref/libzref_mesh.so is missing: build it with oracle/ref_build.py")
+    Z = gpu_lib
+    from zephyr_b200.workloads import shock_water_column
+    n = 40
+    w = shock_water_column(n)
+    water = w.beta[:, 0] >= 0.5
+    sharp_beta = np.stack([water, ~water], axis=1).astype(float)
+    sharp_rho = np.where(water, 1000.0, np.where(w.beta[:, 0] > 0.0, 1.2, w.rho))
+    for case, rho, beta in (("sharp", sharp_rho, sharp_beta), ("column", w.rho, w.beta)):
+        mesh, s = gpu_solver(Z, n, w.box, w.bounds, 5, 0.4)
+        r = RM.RefMmFluid(n, n, box=w.box, bounds=w.bounds, materials="stiffened:Water,ideal:Air", CFL=0.4,
+                          accuracy=1, crp_mode=5)
+        s.make_states(mesh, rho, w.vx, w.vy, w.p, beta)
+        r.make_states(rho, w.vx, w.vy, w.p, beta)
+        assert same(s.states(mesh), r.states())
+        if case == "sharp":
+            for k in range(5):
+                ga_ref = r.fractions_grad()
+                s.update(mesh)
+                dt_r = r.step()
+                assert s.dt() == dt_r, k
+                assert same(s.grad_a(mesh), ga_ref), k
+                assert same(s.states(mesh), r.states()), k
+        else:
+            ga_ref = r.fractions_grad()
+            assert np.abs(ga_ref).max() > 1.0
+            s.update(mesh)
+            assert same(s.grad_a(mesh), ga_ref)
+            with pytest.raises(Z.ZgError, match="MUSCL"):
+                s.dt()
+        mesh.close()

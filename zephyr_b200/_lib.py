@@ -145,6 +145,7 @@ SIGNATURES = {
     "zg_mmf_update_n": (C.c_int, [_V, C.c_int]),
     "zg_mmf_dt": (C.c_int, [_V, _P]),
     "zg_mmf_set_flags": (C.c_int, [_V, _I]),
+    "zg_mmf_grad_a": (C.c_int, [_V, _P]),
     "zg_mmf_interface": (C.c_int, [_V, _P, _P]),
     "zg_tr_default_params": (None, [C.POINTER(TrParams)]),
     "zg_tr_configure": (C.c_int, [_V, C.POINTER(TrParams)]),

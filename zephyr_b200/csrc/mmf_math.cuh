@@ -746,6 +746,14 @@ __device__ __forceinline__ QVd<NM> blend(double a_sig, const QVd<NM> &A, const Q
     return r;
 }
 
+// calc_crp_flux's plain-HLLC case: neither state holds a fraction of
+// material iA strictly between 0 and 1 (mm_fluid.cpp:270-272)
+template <int NM>
+__device__ __forceinline__ bool crp_plain(const MSt<NM> &zL, const MSt<NM> &zR, int iA) {
+    double aL = alpha(zL, iA), aR = alpha(zR, iA);
+    return (aL == 0.0 || aL == 1.0) && (aR == 0.0 || aR == 1.0);
+}
+
 // MmFluid::calc_crp_flux (mm_fluid.cpp:266-345)
 template <int NM>
 __device__ __noinline__ QVd<NM> crp_flux(const MixD<NM> &mx, const MSt<NM> &zL, const MSt<NM> &zR, double hL,
@@ -791,6 +799,102 @@ __device__ __noinline__ QVd<NM> crp_flux(const MixD<NM> &mx, const MSt<NM> &zL, 
         fB = crp_classic(mx, zA, zB, zRB, delta_L, dt, bad);
     }
     return blend(a_sig, fA, fB);
+}
+
+// calc_crp_flux in two parts for two threads of different warps: every
+// composite flux above is blend(a_sig, fA, fB) of two sub-fluxes, one of them
+// a CrpFlux::classic (inverse being classic on mirrored states), the other a
+// plain HLLC or a second classic.  Part 0 computes the classic one, part 1
+// the other; `isA` says whether the result is fA.  The arguments are chosen
+// first and each sub-flux is evaluated at one call site, so the lanes of a
+// warp that need a classic run it together whatever case they are in.  Each
+// sub-flux gets the same arguments as in crp_flux, so blend(a_sig, fA, fB)
+// gives crp_flux's result bit for bit.  Not called when aL and aR are both
+// 0 or 1 (crp_flux's plain HLLC).
+template <int NM>
+__device__ __forceinline__ void mirror(MSt<NM> &z) {
+    z.vx = -z.vx;
+}
+template <int NM>
+__device__ __noinline__ QVd<NM> crp_part(const MixD<NM> &mx, const MSt<NM> &zL, const MSt<NM> &zR, double hL,
+                                         double hR, int iA, double a_sig, double dt, int part, bool &isA, bool &bad) {
+    double aL = alpha(zL, iA), aR = alpha(zR, iA);
+    double delta_L = (aL < a_sig ? aL / a_sig : (1.0 - aL) / (1.0 - a_sig)) * hL;
+    double delta_R = (aR < a_sig ? aR / a_sig : (1.0 - aR) / (1.0 - a_sig)) * hR;
+    // classic(p1, p2, p3, delta), inverted when inv; or hllc(p1, p2)
+    MSt<NM> p1, p2, p3;
+    double delta = 0.0;
+    bool inv = false, plain = false;
+    MSt<NM> zA, zB;
+    if (aL == 0.0 || aL == 1.0) {
+        split(mx, zR, iA, zA, zB);  // zA = zRA, zB = zRB
+        if (aL == 0.0) {
+            // fA = hllc(zL, zA); fB = inverse(zL, zB, zA) = classic(m zA, m zB, m zL), inverted
+            isA = part != 0;
+            if (part == 0) {
+                p1 = zA; p2 = zB; p3 = zL; inv = true; delta = delta_R;
+            } else {
+                p1 = zL; p2 = zA; plain = true;
+            }
+        } else {
+            // fA = inverse(zL, zA, zB) = classic(m zB, m zA, m zL), inverted; fB = hllc(zL, zB)
+            isA = part == 0;
+            if (part == 0) {
+                p1 = zB; p2 = zA; p3 = zL; inv = true; delta = delta_R;
+            } else {
+                p1 = zL; p2 = zB; plain = true;
+            }
+        }
+    } else if (aR == 0.0 || aR == 1.0) {
+        split(mx, zL, iA, zA, zB);  // zA = zLA, zB = zLB
+        if (aR == 0.0) {
+            // fA = hllc(zA, zR); fB = classic(zA, zB, zR)
+            isA = part != 0;
+            if (part == 0) {
+                p1 = zA; p2 = zB; p3 = zR; delta = delta_L;
+            } else {
+                p1 = zA; p2 = zR; plain = true;
+            }
+        } else {
+            // fA = classic(zB, zA, zR); fB = hllc(zB, zR)
+            isA = part == 0;
+            if (part == 0) {
+                p1 = zB; p2 = zA; p3 = zR; delta = delta_L;
+            } else {
+                p1 = zB; p2 = zR; plain = true;
+            }
+        }
+    } else {
+        MSt<NM> zRA, zRB;
+        split(mx, zL, iA, zA, zB);
+        split(mx, zR, iA, zRA, zRB);
+        if (aL < aR) {
+            // fA = classic(zB, zA, zRA); fB = inverse(zB, zRB, zRA) = classic(m zRA, m zRB, m zB), inverted
+            isA = part == 0;
+            if (part == 0) {
+                p1 = zB; p2 = zA; p3 = zRA; delta = delta_L;
+            } else {
+                p1 = zRA; p2 = zRB; p3 = zB; inv = true; delta = delta_R;
+            }
+        } else {
+            // fA = inverse(zA, zRA, zRB) = classic(m zRB, m zRA, m zA), inverted; fB = classic(zA, zB, zRB)
+            isA = part == 0;
+            if (part == 0) {
+                p1 = zRB; p2 = zRA; p3 = zA; inv = true; delta = delta_R;
+            } else {
+                p1 = zA; p2 = zB; p3 = zRB; delta = delta_L;
+            }
+        }
+    }
+    if (plain) return hllc(mx, p1, p2, bad);
+    if (inv) {
+        mirror(p1);
+        mirror(p2);
+        mirror(p3);
+    }
+    QVd<NM> f = crp_classic(mx, p1, p2, p3, delta, dt, bad);
+    if (inv) flux_inverse(f);
+    return f;
 }
 
 // ---------------------------------------------------------------------------
@@ -881,7 +985,7 @@ __device__ __forceinline__ double average_flux(double alpha, double cs, double C
     return heav(P2);
 }
 
-enum : int { CRP_NONE = 0, CRP_V3 = 1, CRP_V5 = 2, CRP_VS = 3, CRP_PLIC = 4 };
+enum : int { CRP_NONE = 0, CRP_V3 = 1, CRP_V5 = 2, CRP_VS = 3, CRP_PLIC = 4, CRP_MUSCL = 5 };
 
 }  // namespace mmf
 }  // namespace zg

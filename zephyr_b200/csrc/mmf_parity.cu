@@ -47,7 +47,7 @@ __device__ __forceinline__ double alpha_rt(const MSt<NM> &z, int idx) {
 // writes dt = min(CFL * min, max_dt) and resets the accumulator.
 __global__ void __launch_bounds__(BLOCK) k_dt(MmArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic == 0) {  // empty work lists for this step's face loop
+    if (ic == 0 && !a.keep_lists) {  // empty work lists for this step's face loop
         a.counts[0] = 0;
         a.counts[1] = 0;
     }
@@ -192,6 +192,8 @@ __device__ QVd<NM> calc_flux(const MmArgs &a, double dt, int ic, const FaceG &g,
         a_sig = face_fraction_v5(a_L, a_R);
     } else if (a.crp == CRP_VS) {
         a_sig = face_fraction_s(a_L, a_R);
+    } else if (a.crp == CRP_MUSCL) {
+        a_sig = MM_NAN;  // alpha_sigma has no face fraction for MUSCL (mm_fluid.cpp:245-250)
     } else {
         double vi = 0.5 * (zm.vx + zp.vx);
         bool upwind = vi > 0.0;
@@ -205,6 +207,10 @@ __device__ QVd<NM> calc_flux(const MmArgs &a, double dt, int ic, const FaceG &g,
         double cs = g.nx * nx + g.ny * ny + 0.0 * 0.0;
         a_sig = between(average_flux(upwind ? a_L : a_R, cs, cfl), a_L, a_R);
     }
+    if (a.crp == CRP_MUSCL && !crp_plain(zm, zp, iA)) {
+        atomicOr(a.err, 2);  // calc_crp_flux's assert on a_sig rejects the NaN (mm_fluid.cpp:276)
+        return qv_zero<NM>();
+    }
     return crp_flux(a.mix, zm, zp, hL, hR, iA, a_sig, dt, bad);
 }
 
@@ -214,10 +220,14 @@ __device__ __forceinline__ void to_local(double cs, double sn, double vx, double
     ox = cs * vx + sn * vy + 0.0 * 0.0;
     oy = -sn * vx + cs * vy + 0.0 * 0.0;
 }
-// One face of the first-order face loop (fluxes, mm_fluid.cpp:385-420):
-// the flux through face s of cell ic, turned back to the global frame and
-// multiplied by the face area.
-__device__ void face_term(const MmArgs &a, int ic, int s, double dt, double *out, bool &bad) {
+// One part of a face of the first-order face loop for two threads: the face
+// flux of calc_flux as face_term computes it, with a composite flux split by
+// crp_part.  Part 0 writes the plain flux (pure states on both sides, or
+// crp_flux's plain-HLLC case) or its part of the composite one, with the
+// face's a_sig and flags (bit 0: composite, bit 1: part 0 is fA); part 1
+// writes the other part of a composite flux.  Rotation to the global frame
+// and the face area follow in k_crp_update_parts.
+__device__ void face_part(const MmArgs &a, int ic, int s, int f, int part, double dt, bool &bad) {
     StructAcc c(a.mesh, ic);
     const double V_c = c.vol();
     MSt<NM> zc = load(a.z, ic);
@@ -235,33 +245,125 @@ __device__ void face_term(const MmArgs &a, int ic, int s, double dt, double *out
     to_local(cs, sn, zc.vx, zc.vy, zm.vx, zm.vy);
     to_local(cs, sn, zn.vx, zn.vy, zp.vx, zp.vy);
     const double S = g.area;
-    QVd<NM> lf = calc_flux(a, dt, ic, g, zm, zp, V_c / S, V_n / S, bad);
-    // Rotate::to_global of the momentum (rotate.cpp:43-77)
-    double mx = cs * lf.a[1] + -sn * lf.a[2] + 0.0 * 0.0;
-    double my = sn * lf.a[1] + cs * lf.a[2] + 0.0 * 0.0;
-    lf.a[1] = mx;
-    lf.a[2] = my;
+    const double hL = V_c / S, hR = V_n / S;
+    // calc_flux (mm_fluid.cpp:347-371): the plain-HLLC cases
+    bool plain = a.crp == CRP_NONE || (frac_index(zm.b) >= 0 && frac_index(zp.b) >= 0);
+    int iA = 0;
+    double a_sig = 0.0;
+    if (!plain) {
+        iA = master_component(zm, zp);
+        double a_L = alpha_rt(zm, iA), a_R = alpha_rt(zp, iA);
+        if (a.crp == CRP_V3) {
+            a_sig = face_fraction_v3(a_L, a_R);
+        } else if (a.crp == CRP_V5) {
+            a_sig = face_fraction_v5(a_L, a_R);
+        } else if (a.crp == CRP_VS) {
+            a_sig = face_fraction_s(a_L, a_R);
+        } else if (a.crp == CRP_MUSCL) {
+            a_sig = MM_NAN;  // alpha_sigma has no face fraction for MUSCL (mm_fluid.cpp:245-250)
+        } else {
+            double vi = 0.5 * (zm.vx + zp.vx);
+            bool upwind = vi > 0.0;
+            double cfl = dt * fabs(vi) / (upwind ? hL : hR);
+            int owner = upwind ? ic : g.nb;
+            double nx = normal_of(a.nrm_x, iA, owner), ny = normal_of(a.nrm_y, iA, owner);
+            if (!upwind) {
+                nx = -nx;
+                ny = -ny;
+            }
+            double csn = g.nx * nx + g.ny * ny + 0.0 * 0.0;
+            a_sig = between(average_flux(upwind ? a_L : a_R, csn, cfl), a_L, a_R);
+        }
+        plain = crp_plain(zm, zp, iA);
+    }
+    double *out = a.fbuf + ((size_t)f * 2 + part) * (4 + NM);
+    QVd<NM> lf;
+    if (!plain && a.crp == CRP_MUSCL) {
+        atomicOr(a.err, 2);  // calc_crp_flux's assert on a_sig rejects the NaN (mm_fluid.cpp:276)
+        if (part == 0) a.fflag[f] = 0;
+        lf = qv_zero<NM>();
+    } else if (plain) {
+        if (part != 0) return;
+        lf = hllc(a.mix, zm, zp, bad);
+        a.fflag[f] = 0;
+    } else {
+        bool isA = true;
+        lf = crp_part(a.mix, zm, zp, hL, hR, iA, a_sig, dt, part, isA, bad);
+        if (part == 0) {
+            a.fsig[f] = a_sig;
+            a.fflag[f] = 1 | (isA ? 2 : 0);
+        }
+    }
 #pragma unroll
-    for (int k = 0; k < 4 + NM; ++k) out[k] = lf.a[k] * S;
+    for (int k = 0; k < 4 + NM; ++k) out[k] = lf.a[k];
 }
 
 // --- work lists ------------------------------------------------------------
 constexpr int LIST_BLOCKS = 148 * 4;
 
-// Cells next to a mixed state: one thread per face (the faces of a cell are
-// independent), then one per cell summing its four face terms in slot order
-// as the reference's loop does, updating and closing the state.
-__global__ void __launch_bounds__(BLOCK) k_crp_faces(MmArgs a) {
+// Cells next to a mixed state, first order: two threads per face, in
+// different warps (warp 2w + p takes part p of the faces of warp pair w), so
+// the two sub-fluxes of a composite flux run side by side.
+__global__ void __launch_bounds__(BLOCK) k_crp_parts(MmArgs a) {
     const double dt = a.dt_scale * *a.dt_out;
-    const int count = 4 * a.counts[0];
-    for (int t = blockIdx.x * BLOCK + threadIdx.x; t < count; t += gridDim.x * BLOCK) {
-        if (skip_face(a.dir, t & 3)) continue;
+    const int faces = 4 * a.counts[0];
+    const int tasks = 2 * ((faces + 31) & ~31);
+    for (int t = blockIdx.x * BLOCK + threadIdx.x; t < tasks; t += gridDim.x * BLOCK) {
+        const int w = t >> 5, part = w & 1, f = ((w >> 1) << 5) + (t & 31);
+        if (f >= faces || skip_face(a.dir, f & 3)) continue;
         bool bad = false;
-        double term[4 + NM];
-        face_term(a, a.list_crp[t >> 2], t & 3, dt, term, bad);
-#pragma unroll
-        for (int k = 0; k < 4 + NM; ++k) a.fbuf[(size_t)t * (4 + NM) + k] = term[k];
+        face_part(a, a.list_crp[f >> 2], f & 3, f, part, dt, bad);
         if (bad) atomicOr(a.err, 1);
+    }
+}
+// Per listed cell: each face's flux from its parts (blend(a_sig, fA, fB) of
+// calc_crp_flux, mm_fluid.cpp:266-345), turned back to the global frame and
+// multiplied by the area as face_term does, summed in slot order; update
+// and closure as in k_crp_update.
+__global__ void __launch_bounds__(BLOCK) k_crp_update_parts(MmArgs a) {
+    const double dt = a.dt_scale * *a.dt_out;
+    const int count = a.counts[0];
+    for (int k = blockIdx.x * BLOCK + threadIdx.x; k < count; k += gridDim.x * BLOCK) {
+        int ic = a.list_crp[k];
+        StructAcc c(a.mesh, ic);
+        MSt<NM> zc = load(a.z, ic);
+        QVd<NM> flux = qv_zero<NM>();
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (skip_face(a.dir, s)) continue;
+            const int f = 4 * k + s;
+            const double *p0 = a.fbuf + (size_t)f * 2 * (4 + NM), *p1 = p0 + (4 + NM);
+            const int fl = a.fflag[f];
+            QVd<NM> lf;
+            if (fl & 1) {
+                QVd<NM> fA, fB;
+#pragma unroll
+                for (int j = 0; j < 4 + NM; ++j) {
+                    fA.a[j] = (fl & 2) ? p0[j] : p1[j];
+                    fB.a[j] = (fl & 2) ? p1[j] : p0[j];
+                }
+                lf = blend(a.fsig[f], fA, fB);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4 + NM; ++j) lf.a[j] = p0[j];
+            }
+            const FaceG g = c.face(s);
+            const double cs = g.nx, sn = g.ny;
+            // Rotate::to_global of the momentum (rotate.cpp:43-77)
+            double mx = cs * lf.a[1] + -sn * lf.a[2] + 0.0 * 0.0;
+            double my = sn * lf.a[1] + cs * lf.a[2] + 0.0 * 0.0;
+            lf.a[1] = mx;
+            lf.a[2] = my;
+            const double S = g.area;
+#pragma unroll
+            for (int j = 0; j < 4 + NM; ++j) flux.a[j] += lf.a[j] * S;
+        }
+        QVd<NM> q = q_of(zc);
+        double coef = dt / a.mesh.vol;
+#pragma unroll
+        for (int j = 0; j < 4 + NM; ++j) q.a[j] -= coef * flux.a[j];
+        if (q.a[0] < 0.0) atomicOr(a.err, 1);  // the reference throws (mm_fluid.cpp:431-433)
+        store(a.znext, ic, state_of_q(a.mix, q, zc.P, zc.T, zc.r));
     }
 }
 __global__ void __launch_bounds__(BLOCK) k_crp_update(MmArgs a) {
@@ -509,6 +611,88 @@ __global__ void __launch_bounds__(BLOCK) k_grad2(MmArgs a) {
     }
 }
 
+// MmFluid::fractions_grad (mm_fluid.cpp:469-482), the volume-fraction
+// gradients of CrpMode::MUSCL: gradient::LSM and gradient::limiting
+// (gradient.h:226-282, 412-474) of PState::volume_fractions (models.cpp:
+// 239-249: beta_i rho / rho_i where beta_i > 0, else 0) with
+// boundary_value_a, the cell's own fractions (mm_fluid.cpp:108-110); the
+// geometry and arithmetic of k_grad2.  Output ga[2 i] = d alpha_i / dx,
+// ga[2 i + 1] = d alpha_i / dy.
+__device__ __forceinline__ double vol_frac(const MmField &z, int i, int ic) {
+    double b = z.b[0][ic], r = z.r[0][ic];
+#pragma unroll
+    for (int k = 1; k < NM; ++k)
+        if (k == i) {
+            b = z.b[k][ic];
+            r = z.r[k][ic];
+        }
+    return b > 0.0 ? b * z.rho[ic] / r : 0.0;
+}
+__global__ void __launch_bounds__(BLOCK) k_grad_a(MmArgs a) {
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.mesh.n) return;
+    StructAcc c(a.mesh, ic);
+    const double pcx = c.cx(), pcy = c.cy();
+    double wv[4], drx[4], dry[4], drnx[4], drny[4];
+    int nb[4];
+    bool bnd[4];
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        FaceG g = c.face(s);
+        nb[s] = g.nb;
+        bnd[s] = is_boundary(g.flag);
+        double ncx, ncy;
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
+        const double rx = ncx - pcx, ry = ncy - pcy;
+        const double d = rx * g.nx + ry * g.ny;
+        const double nxx = d * g.nx, nyy = d * g.ny;
+        const double w = 1.0 * g.area / cube_rn(sqrt(nxx * nxx + nyy * nyy));
+        const double wdx = w * nxx, wdy = w * nyy;
+        A00 += wdx * rx;
+        A01 += wdx * ry;
+        A10 += wdy * rx;
+        A11 += wdy * ry;
+        wv[s] = w;
+        drx[s] = rx;
+        dry[s] = ry;
+        drnx[s] = nxx;
+        drny[s] = nyy;
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;
+    const double det = A11 * A00 + (-A01) * A10;
+    const double inv = 1.0 / det;
+    const double B00 = A11 * inv, B01 = (-A01) * inv, B10 = (-A10) * inv, B11 = A00 * inv;
+    const size_t n = (size_t)a.mesh.n;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) {
+        const double zk = vol_frac(a.z, i, ic);
+        double dn[4], Fx = 0.0, Fy = 0.0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double zn = bnd[s] ? zk : vol_frac(a.z, i, nb[s]);
+            const double dF = zn - zk;
+            dn[s] = dF;
+            Fx += wv[s] * dF * drnx[s];
+            Fy += wv[s] * dF * drny[s];
+        }
+        const double g0x = B00 * Fx + B01 * Fy;
+        const double g0y = B10 * Fx + B11 * Fy;
+        double lx = 0.0, ly = 0.0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double dF_p = dn[s];
+            const double du_n = g0x * drx[s] + g0y * dry[s];
+            const double dF_m = 2.0 * du_n - dF_p;
+            const double dF_lim = limiter2(a.limiter, dF_m, dF_p) * dF_p;
+            lx += wv[s] * dF_lim * drnx[s];
+            ly += wv[s] * dF_lim * drny[s];
+        }
+        a.grad_a[(2 * i) * n + ic] = B00 * lx + B01 * ly;
+        a.grad_a[(2 * i + 1) * n + ic] = B10 * lx + B11 * ly;
+    }
+}
+
 // FaceExtra::Direct (face_extra.h:121-171): z shifted along cell o's
 // gradients by (dx, dy)
 __device__ __forceinline__ MSt<NM> shifted(const MmArgs &a, const MSt<NM> &z, int o, double dx, double dy) {
@@ -746,19 +930,16 @@ void launch_classify(const MmArgs &a, void *stream) {
     k_classify<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
 void launch_crp_faces(const MmArgs &a, void *stream) {
-    k_crp_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
+    k_crp_parts<<<std::min<unsigned>(8 * blocks(a), 2 * LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
 void launch_crp_update(const MmArgs &a, void *stream) {
-    k_crp_update<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
-}
-void launch_flux_crp(const MmArgs &a, void *stream) {
-    k_crp_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
-    k_crp_update<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
+    k_crp_update_parts<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
 void launch_closure(const MmArgs &a, void *stream) {
     k_closure<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
 void launch_grad2(const MmArgs &a, void *stream) { k_grad2<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
+void launch_grad_a(const MmArgs &a, void *stream) { k_grad_a<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
 void launch_stage1(const MmArgs &a, void *stream) { k_stage1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a); }
 void launch_stage2(const MmArgs &a, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;

@@ -47,13 +47,24 @@ struct MmArgs {
     // list_crp filled beforehand (launch_classify): the pure-stencil kernel
     // only skips the listed cells, so it may run beside the composite faces
     int presorted;
+    // dt kernel: leave the work lists alone (they are emptied on another
+    // stream while it runs)
+    int keep_lists;
     double *qbuf;    // (4 + NMAT) doubles per closure-list entry
-    double *fbuf;    // (4 + NMAT) doubles per face of every list_crp cell (4 per cell)
+    // face fluxes of the list_crp cells (4 faces per cell): first order, two
+    // parts of (4 + NMAT) doubles per face with the face's a_sig and flags
+    // (k_crp_parts); second order, one face term of (4 + NMAT) doubles
+    double *fbuf;
+    double *fsig;
+    int *fflag;
     // second order (MmFluid::set_accuracy(2)): limiter, the half-step state
     // and the limited gradients (x, y) of the state at the old layer
     int acc, limiter;
     MmField zhalf;
     double *gx[NG], *gy[NG];
+    // CrpMode::MUSCL: volume-fraction gradients, x and y per material
+    // (2 NMAT arrays of n doubles)
+    double *grad_a;
 };
 
 void launch_dt(const MmArgs &a, void *stream);
@@ -61,13 +72,13 @@ void launch_recover(const MmArgs &a, void *stream);
 // the face loop: pure stencils, then the two work lists
 void launch_flux_pure(const MmArgs &a, void *stream);
 void launch_flux_pure_fp32(const MmArgs &a, void *stream);  // mmf_mixed.cu
-void launch_flux_crp(const MmArgs &a, void *stream);  // face fluxes, then the cell updates
 // the same two halves separately, and the list of cells whose stencil holds a
 // mixed state (built before the pure-stencil kernel when the two overlap)
 void launch_classify(const MmArgs &a, void *stream);
 void launch_crp_faces(const MmArgs &a, void *stream);
 void launch_crp_update(const MmArgs &a, void *stream);
 void launch_closure(const MmArgs &a, void *stream);
+void launch_grad_a(const MmArgs &a, void *stream);  // CrpMode::MUSCL
 void launch_flags(const MmArgs &a, int *flags, void *stream);
 // second order: compute_grad, fluxes_stage1, fluxes_stage2 (mm_fluid.cpp:439-680)
 void launch_grad2(const MmArgs &a, void *stream);

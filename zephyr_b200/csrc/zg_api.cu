@@ -29,10 +29,11 @@ struct zg_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     // a second stream for work that overlaps the main stream's (the
-    // composite Riemann faces beside the pure-stencil cells), with its
-    // fork / join events; created on first use
+    // interface reconstruction and the work list beside dt, the composite
+    // Riemann faces beside the pure-stencil cells), with its events; created
+    // on first use
     cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_cleared = nullptr, ev_dt = nullptr;
     std::string err;
     long long launches = 0;
 
@@ -96,6 +97,8 @@ struct zg_ctx {
     int *d_mm_lists = nullptr;     // 8 counters, then the two work lists of the face loop (n each)
     double *d_mm_qbuf = nullptr;   // conservative states of the closure list
     double *d_mm2 = nullptr;       // second order: half-step state (6 + 2 NMAT fields), then 2 NG gradients
+    double *d_mm_grad_a = nullptr;  // CrpMode::MUSCL: volume-fraction gradients, 2 NMAT fields
+    bool mm_grad_a_valid = false;
     mmf::MmField mz{}, mznext{};
     double *mnx[mmf::NMAT] = {}, *mny[mmf::NMAT] = {}, *moff[mmf::NMAT] = {};
 
@@ -150,6 +153,9 @@ struct DeviceGuard {
 void free_mm(zg_ctx *c) {
     cudaFree(c->d_mm2);
     c->d_mm2 = nullptr;
+    cudaFree(c->d_mm_grad_a);
+    c->d_mm_grad_a = nullptr;
+    c->mm_grad_a_valid = false;
     cudaFree(c->d_mm);
     cudaFree(c->d_mm_scalars);
     cudaFree(c->d_mm_flags);
@@ -430,6 +436,8 @@ int ensure_side(zg_ctx *c) {
     ZG_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_cleared, cudaEventDisableTiming));
+    ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_dt, cudaEventDisableTiming));
     return ZG_OK;
 }
 
@@ -670,8 +678,8 @@ int zg_destroy(zg_ctx *c) {
         if (c->out_img) cudaFreeHost(c->out_img);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
         if (c->side) cudaStreamDestroy(c->side);
-        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-        if (c->ev_join) cudaEventDestroy(c->ev_join);
+        for (cudaEvent_t e : {c->ev_fork, c->ev_join, c->ev_cleared, c->ev_dt})
+            if (e) cudaEventDestroy(e);
     }
     delete c;
     return ZG_OK;
@@ -1251,8 +1259,11 @@ mmf::MmArgs make_mm_args(const zg_ctx *c) {
     a.list_closure = c->d_mm_lists + 8 + c->n;
     a.qbuf = c->d_mm_qbuf;
     a.fbuf = c->d_mm_qbuf + (4 + mmf::NMAT) * (size_t)c->n;
+    a.fsig = a.fbuf + 8 * (4 + mmf::NMAT) * (size_t)c->n;
+    a.fflag = reinterpret_cast<int *>(a.fsig + 4 * (size_t)c->n);
     a.acc = c->mpar.accuracy;
     a.limiter = c->mpar.limiter;
+    a.grad_a = c->d_mm_grad_a;
     if (c->d_mm2) {
         const size_t n = (size_t)c->n;
         double *b = c->d_mm2;
@@ -1286,6 +1297,10 @@ int mm_check_error(zg_ctx *c) {
     int err = 0;
     ZG_CUDA(c, cudaMemcpyAsync(&err, c->d_mm_scalars + 3, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (err & 2)
+        return fail(c, ZG_ERR_NUMERIC, "MmFluid: CrpMode::MUSCL reached a composite face; the reference has no face "
+                                       "fraction for it (alpha_sigma returns NaN, mm_fluid.cpp:245-250, and "
+                                       "calc_crp_flux's assert rejects it, mm_fluid.cpp:276)");
     if (err) return fail(c, ZG_ERR_NUMERIC, "MmFluid: negative density, NaN flux or an unsupported composite "
                                             "Riemann configuration (the reference throws here)");
     return ZG_OK;
@@ -1298,7 +1313,8 @@ int enqueue_mm_step(zg_ctx *c) {
     void *st = (void *)c->stream;
     int rc = ensure_side(c);
     if (rc != ZG_OK) return rc;
-    {
+    const bool first_order = c->mpar.accuracy == 1;
+    if (!first_order) {
         mmf::MmArgs a = make_mm_args(c);
         timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(a, st); });
     }
@@ -1307,24 +1323,43 @@ int enqueue_mm_step(zg_ctx *c) {
         mmf::MmArgs a = make_mm_args(c);
         a.dir = dir;
         a.dt_scale = scale;
-        if (sub++ > 0) cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), c->stream);  // empty work lists
+        if (!first_order && sub++ > 0) cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), c->stream);  // empty work lists
         if (c->mpar.accuracy == 2) {
             // MmFluid::integrate, second order (mm_fluid.cpp:152-168)
             timed(c, ZG_K_MM_GRAD, [&] { mmf::launch_grad2(a, st); });
+            if (c->mpar.crp_mode == ZG_CRP_MUSCL) timed(c, ZG_K_MM_GRAD, [&] { mmf::launch_grad_a(a, st); });
             if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
             timed(c, ZG_K_MM_STAGE1, [&] { mmf::launch_stage1(a, st); });
             timed(c, ZG_K_MM_STAGE2, [&] { mmf::launch_stage2(a, st); });
             std::swap(c->mz, c->mznext);
             return;
         }
-        if (c->mpar.crp_mode == ZG_CRP_PLIC) timed(c, ZG_K_MM_RECOVER, [&] { mmf::launch_recover(a, st); });
-        // the cells next to a mixed state are listed first; then their
-        // composite faces (side stream) run beside the pure-stencil cells
-        // (main stream): the two write disjoint data
+        // First order, on two streams.  Side: empty the work lists, then
+        // MmFluid::integrate's preparation (mm_fluid.cpp:139-150: the
+        // volume-fraction gradients for MUSCL, the interface reconstruction
+        // for PLIC) and the list of cells next to a mixed state, beside dt
+        // (first sub-step; it leaves the lists alone here) on the main
+        // stream.  Then the composite faces of the listed cells (side) beside
+        // the pure-stencil cells (main); the two write disjoint data, and the
+        // cell updates follow on the main stream once both are done.
         a.presorted = 1;
-        timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_classify(a, st); });
         cudaEventRecord(c->ev_fork, c->stream);
         cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        cudaMemsetAsync(a.counts, 0, 2 * sizeof(int), c->side);
+        cudaEventRecord(c->ev_cleared, c->side);
+        if (c->mpar.crp_mode == ZG_CRP_MUSCL)
+            timed_on(c, ZG_K_MM_GRAD, c->side, [&] { mmf::launch_grad_a(a, (void *)c->side); });
+        if (c->mpar.crp_mode == ZG_CRP_PLIC)
+            timed_on(c, ZG_K_MM_RECOVER, c->side, [&] { mmf::launch_recover(a, (void *)c->side); });
+        timed_on(c, ZG_K_MM_FLUX, c->side, [&] { mmf::launch_classify(a, (void *)c->side); });
+        if (sub++ == 0) {
+            mmf::MmArgs d = a;
+            d.keep_lists = 1;
+            timed(c, ZG_K_MM_DT, [&] { mmf::launch_dt(d, st); });
+        }
+        cudaStreamWaitEvent(c->stream, c->ev_cleared, 0);  // the pure-stencil kernel appends to a list
+        cudaEventRecord(c->ev_dt, c->stream);
+        cudaStreamWaitEvent(c->side, c->ev_dt, 0);
         timed_on(c, ZG_K_MM_CRP, c->side, [&] { mmf::launch_crp_faces(a, (void *)c->side); });
         timed(c, ZG_K_MM_FLUX, [&] { mmf::launch_flux_pure(a, st); });
         cudaEventRecord(c->ev_join, c->side);
@@ -1343,6 +1378,7 @@ int enqueue_mm_step(zg_ctx *c) {
     } else {
         integrate(0, 1.0);
     }
+    if (c->mpar.crp_mode == ZG_CRP_MUSCL) c->mm_grad_a_valid = true;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     return ZG_OK;
@@ -1466,7 +1502,7 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown precision");
     if (p->split < ZG_SPLIT_NONE || p->split > ZG_SPLIT_STRANG)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown direction splitting");
-    if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_PLIC)
+    if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_MUSCL)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown CRP mode");
     const int acc = std::min(std::max(1, p->accuracy), 2);  // mm_fluid.cpp:46-48
     if (acc == 2 && p->precision != ZG_FP64)
@@ -1483,6 +1519,8 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
         ZG_CUDA(c, cudaMalloc(&c->d_mm2, (NF + 2 * mmf::NG) * n2 * sizeof(double)));
         ZG_CUDA(c, cudaMemsetAsync(c->d_mm2, 0, (NF + 2 * mmf::NG) * n2 * sizeof(double), c->stream));
     }
+    if (p->crp_mode == ZG_CRP_MUSCL && !c->d_mm_grad_a)
+        ZG_CUDA(c, cudaMalloc(&c->d_mm_grad_a, 2 * mmf::NMAT * (size_t)c->n * sizeof(double)));
     c->mpar.CFL = std::max(0.0, std::min(p->CFL, 1.0));  // mm_fluid.cpp:43-45
     if (c->mm_configured) return ZG_OK;
     size_t n = (size_t)c->n;
@@ -1491,7 +1529,8 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
     ZG_CUDA(c, cudaMalloc(&c->d_mm_scalars, 64));
     ZG_CUDA(c, cudaMalloc(&c->d_mm_flags, n * sizeof(int)));
     ZG_CUDA(c, cudaMalloc(&c->d_mm_lists, (2 * n + 8) * sizeof(int)));
-    ZG_CUDA(c, cudaMalloc(&c->d_mm_qbuf, 5 * (4 + mmf::NMAT) * n * sizeof(double)));  // closure q, face terms
+    // closure q; two face parts per face (4 per cell); a_sig and flags per face
+    ZG_CUDA(c, cudaMalloc(&c->d_mm_qbuf, (9 * (4 + mmf::NMAT) + 4 + 2) * n * sizeof(double)));
     ZG_CUDA(c, cudaMemsetAsync(c->d_mm_lists, 0, (2 * n + 8) * sizeof(int), c->stream));
     double *b = c->d_mm;
     auto take = [&b, n]() {
@@ -1570,6 +1609,23 @@ int zg_mmf_state_download(zg_ctx *c, double *cells) {
         }
     }
     return rc;
+}
+
+int zg_mmf_grad_a(zg_ctx *c, double *out) {
+    int rc = mm_ready(c, "zg_mmf_grad_a");
+    if (rc != ZG_OK) return rc;
+    if (!out) return fail(c, ZG_ERR_ARG, "zg_mmf_grad_a: null array");
+    if (c->mpar.crp_mode != ZG_CRP_MUSCL || !c->mm_grad_a_valid)
+        return fail(c, ZG_ERR_STATE, "zg_mmf_grad_a: computed by the steps of CrpMode::MUSCL only");
+    DeviceGuard g(c->device);
+    const size_t n = (size_t)c->n;
+    std::vector<double> soa(2 * mmf::NMAT * n);
+    ZG_CUDA(c, cudaMemcpyAsync(soa.data(), c->d_mm_grad_a, soa.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream));
+    ZG_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 2 * mmf::NMAT; ++k) out[2 * mmf::NMAT * i + k] = soa[k * n + i];
+    return ZG_OK;
 }
 
 int zg_mmf_make_states(zg_ctx *c, const double *rho, const double *vx, const double *vy, const double *p,

@@ -138,8 +138,10 @@ class MmFluid:
         self._push()
 
     def set_crp_mode(self, mode: CrpMode):  # mm_fluid.cpp:63-69
-        if mode == CrpMode.MUSCL:
-            raise ZgError(-1, "CrpMode::MUSCL is unfinished in the reference (alpha_sigma returns NAN)")
+        """CrpMode::MUSCL computes the volume-fraction gradients (grad_a); the
+        reference defines no face fraction for it, so a step that reaches a
+        composite face raises ZgError (ZG_ERR_NUMERIC) where the reference's
+        assert fails (mm_fluid.cpp:245-250, 276)."""
         if mode != CrpMode.NONE:
             self.p.crp_mode = mode
             self._push()
@@ -195,6 +197,15 @@ class MmFluid:
         f = np.empty(mesh.n_cells(), np.int32)
         check(mesh.ctx, self._lib.zg_mmf_set_flags(mesh.ctx, f.ctypes.data_as(C.POINTER(C.c_int))))
         return f
+
+    def grad_a(self, mesh: EuMesh):
+        """part.grad_a of the last MUSCL sub-step (fractions_grad,
+        mm_fluid.cpp:469-482): (n, n_materials, 2) volume-fraction gradients."""
+        self._require(mesh)
+        n, nm = mesh.n_cells(), self.p.n_materials
+        g = np.empty((n, nm, 2))
+        check(mesh.ctx, self._lib.zg_mmf_grad_a(mesh.ctx, g.ctypes.data_as(C.POINTER(C.c_double))))
+        return g
 
     def interface(self, mesh: EuMesh):
         """interface_recovery of the current state: normals (n, nm, 2), offsets (n, nm)."""
