@@ -45,6 +45,7 @@ UNITS = {
     "zg_vtu.cu": [],
     "smf_fast.cu": [],
     "smf_slot_fast.cu": [],
+    "smf_slot_order.cu": [],
     "smf_slot_mixed.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "adj.cu": [],
     # FP32 face arithmetic: approximate single-precision division and square

@@ -79,6 +79,25 @@ void launch_stage1(const SmfArgs &a, void *stream);
 void launch_stage2(const SmfArgs &a, void *stream);
 void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream);
 void launch_grad_flags(const SmfArgs &a, int *flags, double refine, double coarsen, void *stream);
+
+// Morton order of the cells for the FAST step (smf_slot_order.cu): device
+// buffers of `cap` cells (keys 2 cap), cub scratch of tmp_bytes
+struct OrderBuffers {
+    int cap;
+    unsigned long long *keys;
+    int *idx, *perm, *inv;
+    void *tmp;
+    size_t tmp_bytes;
+    double *cx, *cy, *vol, *inc;
+    int *level, *fb, *fn;
+};
+size_t order_scratch_bytes(int cap);
+// fills b.perm (position -> cell), b.inv and the reordered mesh arrays, and
+// `out`, the mesh view over them; 0 on success
+int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, OrderBuffers &b,
+                SlotMesh &out, void *stream);
+void gather_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream);
+void scatter_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream);
 }  // namespace slotfast
 
 }  // namespace zg

@@ -61,6 +61,16 @@ struct zg_ctx {
     size_t amr_scratch_size = 0;
     amr::View av{};                 // mesh arrays; state pointers set per refine
     zg_amr_stats amr_last{};
+    long long mesh_version = 0;     // bumped whenever the cell set changes
+    // FAST step on the adaptive mesh: the cells in Morton order for the step
+    // (smf_slot_order.cu): order buffers, the reordered mesh arrays, three
+    // states and two counter sets in that order (capacity cells)
+    void *d_ord = nullptr;
+    slotfast::OrderBuffers ord{};
+    SlotMesh ord_mesh{};
+    PrimPtr oz{}, ozhalf{}, oznext{};
+    int *ow[2] = {};
+    long long ord_version = -1;
 
     // solver
     bool configured = false;
@@ -205,6 +215,10 @@ void free_mesh(zg_ctx *c) {
     c->d_axial = nullptr;
     cudaFree(c->d_amr);
     cudaFree(c->d_amr_scratch);
+    cudaFree(c->d_ord);
+    c->d_ord = nullptr;
+    c->ord = slotfast::OrderBuffers{};
+    c->ord_version = -1;
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
     c->d_slot = nullptr;
@@ -430,10 +444,16 @@ void timed_on(zg_ctx *c, int kind, cudaStream_t s, F &&launch) {
 }
 
 // The side stream and its events, created on first use on the context's
-// device.
+// device.  The side stream has the highest priority: its kernels (the
+// composite faces: few blocks, long latency chains) are placed first, and
+// the pure-stencil kernel fills the rest of the GPU around them (measured
+// on the two-material 1024^2 step: 0.267 ms per step against 0.294-0.301
+// ms with default priority).
 int ensure_side(zg_ctx *c) {
     if (c->side) return ZG_OK;
-    ZG_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    int lo = 0, hi = 0;
+    ZG_CUDA(c, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    ZG_CUDA(c, cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi));
     ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     ZG_CUDA(c, cudaEventCreateWithFlags(&c->ev_cleared, cudaEventDisableTiming));
@@ -534,25 +554,92 @@ int enqueue_tiled_step(zg_ctx *c) {
     return ZG_OK;
 }
 
+// The buffers of the Morton order (capacity cells), allocated on first use.
+int ensure_order(zg_ctx *c) {
+    if (c->d_ord) return ZG_OK;
+    const size_t cap = (size_t)c->cap;
+    const size_t tmp = slotfast::order_scratch_bytes(c->cap);
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t bytes = al(2 * cap * 8) + 3 * al(cap * 4) + al(tmp) + 4 * al(cap * 8) + al(cap * 4) +
+                         2 * al(8 * cap * 4) + 15 * al(cap * 8) + 2 * al(cap * 4);
+    ZG_CUDA(c, cudaMalloc(&c->d_ord, bytes));
+    char *p = static_cast<char *>(c->d_ord);
+    auto take = [&p, &al](size_t b) {
+        char *q = p;
+        p += al(b);
+        return q;
+    };
+    slotfast::OrderBuffers &o = c->ord;
+    o.cap = c->cap;
+    o.keys = reinterpret_cast<unsigned long long *>(take(2 * cap * 8));
+    o.idx = reinterpret_cast<int *>(take(cap * 4));
+    o.perm = reinterpret_cast<int *>(take(cap * 4));
+    o.inv = reinterpret_cast<int *>(take(cap * 4));
+    o.tmp = take(tmp);
+    o.tmp_bytes = tmp;
+    o.cx = reinterpret_cast<double *>(take(cap * 8));
+    o.cy = reinterpret_cast<double *>(take(cap * 8));
+    o.vol = reinterpret_cast<double *>(take(cap * 8));
+    o.inc = reinterpret_cast<double *>(take(cap * 8));
+    o.level = reinterpret_cast<int *>(take(cap * 4));
+    o.fb = reinterpret_cast<int *>(take(8 * cap * 4));
+    o.fn = reinterpret_cast<int *>(take(8 * cap * 4));
+    for (PrimPtr *z : {&c->oz, &c->ozhalf, &c->oznext}) {
+        z->r = reinterpret_cast<double *>(take(cap * 8));
+        z->u = reinterpret_cast<double *>(take(cap * 8));
+        z->v = reinterpret_cast<double *>(take(cap * 8));
+        z->p = reinterpret_cast<double *>(take(cap * 8));
+        z->e = reinterpret_cast<double *>(take(cap * 8));
+    }
+    c->ow[0] = reinterpret_cast<int *>(take(cap * 4));
+    c->ow[1] = reinterpret_cast<int *>(take(cap * 4));
+    c->ord_version = -1;
+    return ZG_OK;
+}
+
 // The FAST step on an adaptive rectangle: the gather-form kernels of the
-// parity step over derived face geometry, with fused multiply-adds.
+// parity step over derived face geometry, with fused multiply-adds, run on
+// the cells in Morton order (the state gathered into it and scattered back;
+// the same results as in the mesh's own order).
 int enqueue_slot_fast_step(zg_ctx *c) {
-    SmfArgs a = make_args(c);
     void *st = (void *)c->stream;
-    timed(c, ZG_K_DT, [&] { slotfast::launch_dt(a, c->z, st); });
+    int rc = ensure_order(c);
+    if (rc != ZG_OK) return rc;
+    if (c->ord_version != c->mesh_version) {
+        const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
+        if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
+            return cuda_fail(c, cudaGetLastError(), "cell order");
+        c->launches += 4;
+        c->ord_version = c->mesh_version;
+    }
+    const bool pc = c->par.accuracy == 2 && c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR;
+    SmfArgs a = make_args(c);
+    const PrimPtr znext_mesh = c->znext;
+    int *const wout_mesh = a.wait_out;
+    slotfast::gather_state(c->ord.perm, c->n, c->z, c->oz, pc ? a.wait_in : nullptr, c->ow[0], st);
+    ++c->launches;
+    a.smesh = c->ord_mesh;
+    a.z = c->oz;
+    a.zhalf = c->ozhalf;
+    a.znext = c->oznext;
+    a.wait_in = c->ow[0];
+    a.wait_out = c->ow[1];
+    timed(c, ZG_K_DT, [&] { slotfast::launch_dt(a, a.z, st); });
     if (c->par.accuracy == 1) {
         timed(c, ZG_K_FLUX1, [&] { slotfast::launch_flux1(a, st); });
-    } else if (c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR) {
-        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->z, st); });
+    } else if (pc) {
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
         timed(c, ZG_K_STAGE1, [&] { slotfast::launch_stage1(a, st); });
         timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2(a, st); });
         c->wait_cur = 1 - c->wait_cur;
     } else {
-        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->z, st); });
-        timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun(a, c->z, c->zhalf, false, st); });
-        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->zhalf, st); });
-        timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun(a, c->zhalf, c->znext, true, st); });
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
+        timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun(a, a.z, a.zhalf, false, st); });
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.zhalf, st); });
+        timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun(a, a.zhalf, a.znext, true, st); });
     }
+    slotfast::scatter_state(c->ord.perm, c->n, c->oznext, znext_mesh, pc ? c->ow[1] : nullptr, wout_mesh, st);
+    ++c->launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     std::swap(c->z, c->znext);
@@ -2336,6 +2423,7 @@ void amr_carve(zg_ctx *c, size_t cap) {
 }
 
 void amr_set_n(zg_ctx *c, int n) {
+    ++c->mesh_version;
     c->n = n;
     c->smesh.n = n;
     c->mesh = StructMesh{};
