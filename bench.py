@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--scheme", choices=["pc", "heun"], default="pc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # profiling aids: one section alone on a smaller case (not the bench line)
-    ap.add_argument("--only", choices=["amr", "mm", "adjoint", "transfer", "vtu"], default=None,
+    ap.add_argument("--only", choices=["forms", "amr", "mm", "adjoint", "transfer", "vtu"], default=None,
                     help="run one section alone and print its JSON (for ncu captures)")
     ap.add_argument("--amr-base", type=int, default=0, help="AMR base cells per side (default 512)")
     ap.add_argument("--tr-nx", type=int, default=0, help="transport mesh cells along x (default 4096)")
@@ -851,7 +851,7 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.barrier()
 
     K, W = args.steps, max(args.warmup, 3)
-    if args.only:
+    if args.only and args.only != "forms":
         global AMR_BASE, AMR_CAPACITY
         if args.amr_base:
             AMR_BASE = args.amr_base
@@ -928,6 +928,14 @@ def run_ours(args, rank, world, local_rank):
         _, v_kernels, _, _ = _timed_steps(torch, lib, m2, s2, K, dev, stream, barrier)
         variants[name] = {"ms": v_ms, "kernels": v_kernels, "launches": v_launch, "mesh": m2, "solver": s2,
                           "scheme": scheme}
+    if args.only == "forms":  # the step's forms on the 2048^2 workload alone
+        for v in variants.values():
+            v["mesh"].close()
+        if rank == 0:
+            print(json.dumps({"only": "forms", "headline_ms_per_step": ms / K, "headline_kernels": kernels,
+                              **{n: {"ms_per_step": v["ms"] / K, "kernels": v["kernels"]}
+                                 for n, v in variants.items()}}), flush=True)
+        return
 
     # accuracy over the configuration's horizon: density after HORIZON steps
     # of the mixed form (and of the FAST FP64 form) against the bit-exact FP64
@@ -957,7 +965,11 @@ def run_ours(args, rank, world, local_rank):
     mm2 = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank,
                      want_cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline), precision=Z.Precision.FP64,
                      accuracy=2)
-    mm2.pop("final")
+    mm2_mx = mm_variant(torch, lib, dev, stream, barrier, K, W, local_rank, want_cpu=False,
+                        precision=Z.Precision.MIXED, accuracy=2)
+    z2, z2mx = mm2.pop("final"), mm2_mx.pop("final")
+    mm2_err = {f"l1_rel_{name}_err_vs_fp64": float(np.sum(np.abs(z2mx[:, k] - z2[:, k])) / np.sum(np.abs(z2[:, k])))
+               for name, k in (("density", 0), ("pressure", 3))}
     z64, zmx = mm.pop("final"), mm_mx.pop("final")
     mm_err = {f"l1_rel_{name}_err_vs_fp64": float(np.sum(np.abs(zmx[:, k] - z64[:, k])) / np.sum(np.abs(z64[:, k])))
               for name, k in (("density", 0), ("pressure", 3))}
@@ -983,10 +995,10 @@ def run_ours(args, rank, world, local_rank):
 
     vnames = list(variants)
     vals = _max_over_ranks(torch, [ms, e2e_ms, mm["ms"], amr["ms_total"], amr_par["ms_total"], mm_mx["ms"],
-                                   amr_mx["ms_total"], trv["ms"], mm2["ms"]] + [variants[v]["ms"] for v in vnames],
-                           dev, world)
-    ms, e2e_ms, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr, ms_mm2 = vals[:9]
-    vms = dict(zip(vnames, vals[9:]))
+                                   amr_mx["ms_total"], trv["ms"], mm2["ms"], mm2_mx["ms"]] +
+                           [variants[v]["ms"] for v in vnames], dev, world)
+    ms, e2e_ms, ms_mm, ms_amr, ms_amr_par, ms_mm_mx, ms_amr_mx, ms_tr, ms_mm2, ms_mm2_mx = vals[:10]
+    vms = dict(zip(vnames, vals[10:]))
     ms_par, ms_mix = vms["fp64_parity"], vms["mixed"]
     amr_mx["value"] = world * amr_mx["value"] * amr_mx["ms_total"] / ms_amr_mx
     amr_mx["speedup_vs_fp64"] = ms_amr / ms_amr_mx
@@ -1032,7 +1044,8 @@ def run_ours(args, rank, world, local_rank):
                        timing="headline timed without per-kernel events; the kernel split from a second run"),
         "roofline": roof, "kernels": kernels,
         "gpu_launches": int(launches + sum(v["launches"] for v in variants.values()) +
-                            mm["launches"] + mm_mx["launches"] + mm2["launches"] + adjv["gpu_launches"] + amr["gpu_launches"] +
+                            mm["launches"] + mm_mx["launches"] + mm2["launches"] + mm2_mx["launches"] +
+                            adjv["gpu_launches"] + amr["gpu_launches"] +
                             amr_par["gpu_launches"] + amr_mx["gpu_launches"] + trv["launches"] +
                             vtuv["gpu_launches"]),
         "gpu_launches_headline": int(launches), "clocks": clocks,
@@ -1094,6 +1107,13 @@ def run_ours(args, rank, world, local_rank):
                 "step_frac": MM2_B_ALG * mm2["cells"] * K / (ms_mm2 / 1e3) / 1e9 / peak,
                 "algorithmic_bytes_per_cell": MM2_B_ALG, "gpu_launches": int(mm2["launches"]),
                 "kernels": mm2["kernels"], "cpu_baseline": mm2.get("cpu_baseline")},
+            "multimaterial_second_order_mixed": {
+                "value": world * mm2_mx["cells"] * K / (ms_mm2_mx / 1e3), "unit": METRIC,
+                "ms_per_step": ms_mm2_mx / K, "speedup_vs_fp64": ms_mm2 / ms_mm2_mx,
+                "form": "FP32 HLLC of the faces whose reconstructed states stay pure; FP64 reconstruction and "
+                        "closures, composite Riemann fluxes, sums, update, PLIC and dt",
+                **mm2_err, "err_after_steps": W + 2 * K, "kernels": mm2_mx["kernels"],
+                "gpu_launches": int(mm2_mx["launches"])},
             "adjoint": adjv,
             "vtu_write": vtuv,
             "transfer": {

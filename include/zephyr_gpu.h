@@ -404,9 +404,11 @@ typedef struct zg_mmf_params {
     double max_dt;            /* set_max_dt */
     int split;                /* zg_dir_split (set_splitting) */
     int precision;            /* zg_precision: FP64 (the reference's arithmetic) or MIXED (FP32 face
-                                 states, wave speeds and HLLC fluxes of the pure-stencil faces; FP64
-                                 accumulation, update, EoS pressure recovery, composite Riemann
-                                 fluxes, PLIC and dt; first order only) */
+                                 states, wave speeds and HLLC fluxes of the pure faces: pure-stencil
+                                 faces in first order, faces whose reconstructed states stay pure in
+                                 second order (with a CRP mode); FP64 accumulation, update, EoS
+                                 pressure recovery, reconstruction and its closures, composite
+                                 Riemann fluxes, PLIC and dt) */
     int limiter;              /* zg_limiter of the second-order gradients (set_limiter; default MC) */
 } zg_mmf_params;
 

@@ -846,6 +846,22 @@ __device__ __forceinline__ bool interp_pure(const MixD<NM> &mx, MSt<NM> &z) {
 // order.  The lean kernel keeps the Newton closures and the composite Riemann
 // solver out of the common path (fewer registers, more resident warps).
 // (four resident blocks: 128 registers, measured 9 % faster than three)
+// R = double: the reference's arithmetic.  R = float: the mixed form -- the
+// reconstruction and its closures in FP64, the HLLC flux of the two pure
+// face states in FP32 (hllc_pure), widened to FP64 for the sums.
+__device__ __forceinline__ PureSt<float> pure_f(const MSt<NM> &z) {
+    PureSt<float> o;
+    o.rho = (float)z.rho;
+    o.vx = (float)z.vx;
+    o.vy = (float)z.vy;
+    o.P = (float)z.P;
+    o.e = (float)z.e;
+#pragma unroll
+    for (int i = 0; i < NM; ++i) o.b[i] = (float)z.b.f[i];
+    o.idx = frac_index(z.b);
+    return o;
+}
+template <typename R>
 __global__ void __launch_bounds__(BLOCK, 4) k_stage2_pure(MmArgs a) {
     const int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= a.mesh.n) return;
@@ -878,7 +894,15 @@ __global__ void __launch_bounds__(BLOCK, 4) k_stage2_pure(MmArgs a) {
         to_local(g.nx, g.ny, zm.vx, zm.vy, zm.vx, zm.vy);
         to_local(g.nx, g.ny, zp.vx, zp.vy, zp.vx, zp.vy);
         const double S = g.area;
-        QVd<NM> lf = hllc(a.mix, zm, zp, bad);
+        QVd<NM> lf;
+        if constexpr (sizeof(R) == 8) {
+            lf = hllc(a.mix, zm, zp, bad);
+        } else {
+            float F[4 + NM];
+            hllc_pure<float>(a.mix, pure_f(zm), pure_f(zp), F, bad);
+#pragma unroll
+            for (int k = 0; k < 4 + NM; ++k) lf.a[k] = (double)F[k];
+        }
         const double mxx = g.nx * lf.a[1] + -g.ny * lf.a[2] + 0.0 * 0.0;
         const double myy = g.ny * lf.a[1] + g.nx * lf.a[2] + 0.0 * 0.0;
         lf.a[1] = mxx;
@@ -947,7 +971,8 @@ void launch_stage2(const MmArgs &a, void *stream) {
         k_stage2<<<blocks(a), BLOCK, 0, st>>>(a);
         return;
     }
-    k_stage2_pure<<<blocks(a), BLOCK, 0, st>>>(a);
+    if (a.fp32_flux) k_stage2_pure<float><<<blocks(a), BLOCK, 0, st>>>(a);
+    else k_stage2_pure<double><<<blocks(a), BLOCK, 0, st>>>(a);
     k_stage2_faces<<<std::min<unsigned>(4 * blocks(a), LIST_BLOCKS), BLOCK, 0, st>>>(a);
     k_crp_update<<<std::min<unsigned>(blocks(a), LIST_BLOCKS), BLOCK, 0, st>>>(a);
 }

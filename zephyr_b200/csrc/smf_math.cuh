@@ -519,6 +519,16 @@ __device__ inline Cons num_flux(int kind, const Prim &zL, const Prim &zR, const 
     }
 }
 
+// The flux of a kernel instantiated for one flux family: FX = FLUX_HLLC or
+// FLUX_HLL calls that flux directly (the kernel then carries none of the
+// other fluxes' code or registers); FX = -1 takes the run-time switch.
+template <int FX>
+__device__ inline Cons flux_fx(int kind, const Prim &zL, const Prim &zR, const EosD &eos) {
+    if constexpr (FX == FLUX_HLLC) return hllc(zL, zR, eos);
+    else if constexpr (FX == FLUX_HLL) return hll(zL, zR, eos);
+    else return num_flux(kind, zL, zR, eos);
+}
+
 // limiter.cxx binary forms phi(a, b)
 __device__ inline double lim_MC1(double r) {
     if (isnan(r)) return 0.0;

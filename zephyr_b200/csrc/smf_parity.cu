@@ -29,19 +29,44 @@ void launch_dt(const SmfArgs &a, PrimPtr z, bool slots, void *stream) {
     b.z = z;
     ZG_DISPATCH(k_dt, b);
 }
-void launch_flux1(const SmfArgs &a, bool slots, void *stream) { ZG_DISPATCH(k_flux1, a); }
-void launch_grad(const SmfArgs &a, PrimPtr z, bool slots, void *stream) { ZG_DISPATCH(k_grad, a, z); }
-void launch_stage1(const SmfArgs &a, bool slots, void *stream) { ZG_DISPATCH(k_stage1, a); }
-void launch_stage2(const SmfArgs &a, bool slots, void *stream) { ZG_DISPATCH(k_stage2, a); }
-void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, bool slots, void *stream) {
+// The kernels that evaluate face fluxes, instantiated per flux family: HLLC
+// and HLL without the other fluxes' code (the run-time switch over the
+// eight fluxes of NumFlux::create costs registers and spills), the general
+// switch for the rest.  The same operations either way.
+template <int FX>
+static void flux1_fx(const SmfArgs &a, bool slots, void *stream) {
+    if (slots) k_flux1<SlotAcc, BLOCK, 1, FX><<<blocks(a, true), BLOCK, 0, (cudaStream_t)stream>>>(a);
+    else k_flux1<StructAcc, BLOCK, 1, FX><<<blocks(a, false), BLOCK, 0, (cudaStream_t)stream>>>(a);
+}
+template <int FX>
+static void stage2_fx(const SmfArgs &a, bool slots, void *stream) {
+    if (slots) k_stage2<SlotAcc, BLOCK, 1, FX><<<blocks(a, true), BLOCK, 0, (cudaStream_t)stream>>>(a);
+    else k_stage2<StructAcc, BLOCK, 1, FX><<<blocks(a, false), BLOCK, 0, (cudaStream_t)stream>>>(a);
+}
+template <int FX>
+static void heun_fx(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, bool slots, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (slots) {
-        if (final) k_heun<SlotAcc, BLOCK, true><<<blocks(a, true), BLOCK, 0, st>>>(a, zin, zout);
-        else k_heun<SlotAcc, BLOCK, false><<<blocks(a, true), BLOCK, 0, st>>>(a, zin, zout);
+        if (final) k_heun<SlotAcc, BLOCK, true, 1, FX><<<blocks(a, true), BLOCK, 0, st>>>(a, zin, zout);
+        else k_heun<SlotAcc, BLOCK, false, 1, FX><<<blocks(a, true), BLOCK, 0, st>>>(a, zin, zout);
     } else {
-        if (final) k_heun<StructAcc, BLOCK, true><<<blocks(a, false), BLOCK, 0, st>>>(a, zin, zout);
-        else k_heun<StructAcc, BLOCK, false><<<blocks(a, false), BLOCK, 0, st>>>(a, zin, zout);
+        if (final) k_heun<StructAcc, BLOCK, true, 1, FX><<<blocks(a, false), BLOCK, 0, st>>>(a, zin, zout);
+        else k_heun<StructAcc, BLOCK, false, 1, FX><<<blocks(a, false), BLOCK, 0, st>>>(a, zin, zout);
     }
+}
+#define ZG_FLUX_FAMILY(FN, ...)                                        \
+    do {                                                               \
+        if (a.flux == FLUX_HLLC) FN<FLUX_HLLC>(__VA_ARGS__);           \
+        else if (a.flux == FLUX_HLL) FN<FLUX_HLL>(__VA_ARGS__);        \
+        else FN<-1>(__VA_ARGS__);                                      \
+    } while (0)
+
+void launch_flux1(const SmfArgs &a, bool slots, void *stream) { ZG_FLUX_FAMILY(flux1_fx, a, slots, stream); }
+void launch_grad(const SmfArgs &a, PrimPtr z, bool slots, void *stream) { ZG_DISPATCH(k_grad, a, z); }
+void launch_stage1(const SmfArgs &a, bool slots, void *stream) { ZG_DISPATCH(k_stage1, a); }
+void launch_stage2(const SmfArgs &a, bool slots, void *stream) { ZG_FLUX_FAMILY(stage2_fx, a, slots, stream); }
+void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, bool slots, void *stream) {
+    ZG_FLUX_FAMILY(heun_fx, a, zin, zout, final, slots, stream);
 }
 void launch_flags(const SmfArgs &a, int *flags, bool slots, void *stream) { ZG_DISPATCH(k_flags, a, flags); }
 

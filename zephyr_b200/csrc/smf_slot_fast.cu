@@ -31,22 +31,38 @@ void launch_dt(const SmfArgs &a, PrimPtr z, void *stream) {
     b.z = z;
     k_dt<SlotFastAcc, BLOCK><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(b);
 }
-void launch_flux1(const SmfArgs &a, void *stream) {
-    k_flux1<SlotFastAcc, BLOCK, S2M><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
+// the face-flux kernels per flux family (HLLC, HLL, the general switch)
+#define ZG_FLUX_FAMILY(FN, ...)                                        \
+    do {                                                               \
+        if (a.flux == FLUX_HLLC) FN<FLUX_HLLC>(__VA_ARGS__);           \
+        else if (a.flux == FLUX_HLL) FN<FLUX_HLL>(__VA_ARGS__);        \
+        else FN<-1>(__VA_ARGS__);                                      \
+    } while (0)
+template <int FX>
+static void flux1_fx(const SmfArgs &a, void *stream) {
+    k_flux1<SlotFastAcc, BLOCK, S2M, FX><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
+template <int FX>
+static void stage2_fx(const SmfArgs &a, void *stream) {
+    k_stage2<SlotFastAcc, BLOCK, S2M, FX><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
+}
+template <int FX>
+static void heun_fx(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (final) k_heun<SlotFastAcc, BLOCK, true, S2M, FX><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
+    else k_heun<SlotFastAcc, BLOCK, false, S2M, FX><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
+}
+
+void launch_flux1(const SmfArgs &a, void *stream) { ZG_FLUX_FAMILY(flux1_fx, a, stream); }
 void launch_grad(const SmfArgs &a, PrimPtr z, void *stream) {
     k_grad<SlotFastAcc, BLOCK, GM><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, z);
 }
 void launch_stage1(const SmfArgs &a, void *stream) {
     k_stage1<SlotFastAcc, BLOCK, S1M><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
-void launch_stage2(const SmfArgs &a, void *stream) {
-    k_stage2<SlotFastAcc, BLOCK, S2M><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
-}
+void launch_stage2(const SmfArgs &a, void *stream) { ZG_FLUX_FAMILY(stage2_fx, a, stream); }
 void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream) {
-    cudaStream_t st = (cudaStream_t)stream;
-    if (final) k_heun<SlotFastAcc, BLOCK, true, S2M><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
-    else k_heun<SlotFastAcc, BLOCK, false, S2M><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
+    ZG_FLUX_FAMILY(heun_fx, a, zin, zout, final, stream);
 }
 
 // Refinement flags by the density-gradient criterion |grad rho| h / rho (h =

@@ -322,7 +322,7 @@ __device__ inline void update(Cons &q, double coef, const Cons &F) {
 
 // ---------------------------------------------------------------------------
 // K2: first-order step (sm_fluid.cpp:127-174).
-template <class Acc, int BLOCK, int MINB = 1>
+template <class Acc, int BLOCK, int MINB = 1, int FX = -1>
 __global__ void __launch_bounds__(BLOCK, MINB) k_flux1(SmfArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_flux1(SmfArgs a) {
         Prim zm = zc, zp = zn;
         rot_local(zm.u, zm.v, cs, sn);
         rot_local(zp.u, zp.v, cs, sn);
-        Cons lf = num_flux(a.flux, zm, zp, a.eos);
+        Cons lf = flux_fx<FX>(a.flux, zm, zp, a.eos);
         rot_global(lf.mu, lf.mv, cs, sn);
         add_area(F, lf, c.flux_area(g, s));
     }
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_stage1(SmfArgs a) {
 // Face flux of the corrector (sm_fluid.cpp:271-341): reconstruct with the
 // gradients of z at the states zh and solve the Riemann problem; returned
 // multiplied by the face area.
-template <class Acc>
+template <int FX, class Acc>
 __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &zh, const int *wt, const Acc &c, int s,
                                       const FaceG &g, const Prim &zch, double pcx, double pcy, int wc) {
     const int ic = c.ic;
@@ -611,7 +611,7 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &zh, const
     frame<Acc>(g, cs, sn);
     rot_local(zm.u, zm.v, cs, sn);
     rot_local(zp.u, zp.v, cs, sn);
-    Cons lf = robust ? hll(zm, zp, a.eos) : num_flux(a.flux, zm, zp, a.eos);
+    Cons lf = robust ? hll(zm, zp, a.eos) : flux_fx<FX>(a.flux, zm, zp, a.eos);
     rot_global(lf.mu, lf.mv, cs, sn);
     const double area = c.flux_area(g, s);
     lf.r *= area;
@@ -623,7 +623,7 @@ __device__ inline Cons corrector_face(const SmfArgs &a, const PrimPtr &zh, const
 
 // K5: corrector with the isolation bit (sm_fluid.cpp:255-366).  `wait` is
 // read from the previous step's array and written to the other one.
-template <class Acc, int BLOCK, int MINB = 1>
+template <class Acc, int BLOCK, int MINB = 1, int FX = -1>
 __global__ void __launch_bounds__(BLOCK, MINB) k_stage2(SmfArgs a) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
@@ -639,7 +639,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_stage2(SmfArgs a) {
     for (int s = 0; s < Acc::NSLOT; ++s) {
         FaceG g = c.face(s);
         if (g.flag == BC_UNDEFINED) continue;
-        Cons lf = corrector_face(a, a.zhalf, a.wait_in, c, s, g, zch, pcx, pcy, wc);
+        Cons lf = corrector_face<FX>(a, a.zhalf, a.wait_in, c, s, g, zch, pcx, pcy, wc);
         F.r += lf.r;
         F.mu += lf.mu;
         F.mv += lf.mv;
@@ -667,7 +667,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_stage2(SmfArgs a) {
 // corrector with z_half = z, no isolation):
 //   stage A: z* = P(Q(z^n) - dt/V * sum F(z^n))
 //   stage B: z^{n+1} = P(0.5 * (Q(z^n) + Q(z*) - dt/V * sum F(z*)))
-template <class Acc, int BLOCK, bool FINAL, int MINB = 1>
+template <class Acc, int BLOCK, bool FINAL, int MINB = 1, int FX = -1>
 __global__ void __launch_bounds__(BLOCK, MINB) k_heun(SmfArgs a, PrimPtr zin, PrimPtr zout) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= Acc::n(a)) return;
@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_heun(SmfArgs a, PrimPtr zin, Pr
     for (int s = 0; s < Acc::NSLOT; ++s) {
         FaceG g = c.face(s);
         if (g.flag == BC_UNDEFINED) continue;
-        Cons lf = corrector_face(a, zin, nullptr, c, s, g, zc, pcx, pcy, 0);
+        Cons lf = corrector_face<FX>(a, zin, nullptr, c, s, g, zc, pcx, pcy, 0);
         F.r += lf.r;
         F.mu += lf.mu;
         F.mv += lf.mv;

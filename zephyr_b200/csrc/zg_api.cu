@@ -1592,8 +1592,9 @@ int zg_mmf_configure(zg_ctx *c, const zg_mmf_params *p) {
     if (p->crp_mode < ZG_CRP_NONE || p->crp_mode > ZG_CRP_MUSCL)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown CRP mode");
     const int acc = std::min(std::max(1, p->accuracy), 2);  // mm_fluid.cpp:46-48
-    if (acc == 2 && p->precision != ZG_FP64)
-        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: the mixed form is built for the first-order step");
+    if (acc == 2 && p->precision != ZG_FP64 && p->crp_mode == ZG_CRP_NONE)
+        return fail(c, ZG_ERR_ARG, "zg_mmf_configure: the mixed second-order form runs with a CRP mode (its "
+                                   "FP32 faces are those whose reconstructed states stay pure)");
     if (p->limiter < ZG_LIM_NONE || p->limiter > ZG_LIM_SUPERBEE)
         return fail(c, ZG_ERR_ARG, "zg_mmf_configure: unknown limiter");
     DeviceGuard g(c->device);

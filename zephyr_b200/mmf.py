@@ -109,7 +109,9 @@ class MmFluid:
 
     def set_precision(self, precision: int):
         """Precision.FP64 (the reference's arithmetic) or Precision.MIXED (FP32
-        face arithmetic of the pure-stencil faces, FP64 elsewhere)."""
+        HLLC of the pure faces -- pure-stencil faces in first order, faces
+        whose reconstructed states stay pure in second order -- FP64
+        elsewhere; second order with a CRP mode only)."""
         self.p.precision = int(precision)
         self._push()
 
