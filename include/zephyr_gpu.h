@@ -467,11 +467,17 @@ int zg_mmf_interface(zg_ctx *ctx, double *normals, double *offsets);
  * instead of by overriding Transfer::velocity.
  * ------------------------------------------------------------------------ */
 
-/* Transfer::Method values (transfer.h:25-51) with kernels: the CRP family and
- * VOF / VOF_CRP (swept-polygon fluxes with the PLIC reconstruction). */
+/* Transfer::Method values (transfer.h:25-51) with kernels: the CRP family,
+ * VOF / VOF_CRP (swept-polygon fluxes with the PLIC reconstruction) and the
+ * MUSCL family (compute_slopes and fluxes_MUSCL, transfer.cpp:345-469:
+ * MUSCLd least-squares slopes, MUSCLn slopes from the interface planes,
+ * MUSCL_MC limited slopes, and their CRP-limited forms) and WENO, WENO_CRP
+ * (update_WENO, transfer.cpp:541-666: five-cell WENO stencils with the mesh's
+ * periodic index wrap; at least 3 cells per axis). */
 enum zg_tr_method {
     ZG_TR_CRP_V3 = 0, ZG_TR_CRP_V5 = 1, ZG_TR_CRP_SE = 2, ZG_TR_CRP_N1 = 3, ZG_TR_CRP_N2 = 4,
-    ZG_TR_VOF = 5, ZG_TR_VOF_CRP = 6
+    ZG_TR_VOF = 5, ZG_TR_VOF_CRP = 6, ZG_TR_MUSCLD = 7, ZG_TR_MUSCLN = 8, ZG_TR_MUSCLD_CRP = 9,
+    ZG_TR_MUSCLN_CRP = 10, ZG_TR_MUSCL_MC = 11, ZG_TR_MUSCL_MC_CRP = 12, ZG_TR_WENO = 13, ZG_TR_WENO_CRP = 14
 };
 enum zg_tr_velocity { ZG_TR_TRANSLATION = 0, ZG_TR_ROTATION = 1 };
 /* Face directions of one update (mesh::Direction, amr_faces.h:75-80). */

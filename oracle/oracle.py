@@ -362,7 +362,9 @@ def mm_average_flux(alpha, cos, CFL):
 
 
 # Transfer::Method values (transfer.h:25-51) that the restatement covers
-TR_METHODS = {"CRP_V3": 0, "CRP_V5": 1, "CRP_SE": 2, "CRP_N1": 3, "CRP_N2": 4, "VOF": 5, "VOF_CRP": 6}
+TR_METHODS = {"CRP_V3": 0, "CRP_V5": 1, "CRP_SE": 2, "CRP_N1": 3, "CRP_N2": 4, "VOF": 5, "VOF_CRP": 6,
+              "MUSCLd": 7, "MUSCLn": 8, "MUSCLd_CRP": 9, "MUSCLn_CRP": 10, "MUSCL_MC": 11, "MUSCL_MC_CRP": 12,
+              "WENO": 13, "WENO_CRP": 14}
 
 
 class TrSolver:

@@ -711,6 +711,7 @@ enum Boundary { B_UNDEFINED = -1, B_INNER = 0, B_WALL = 1, B_ZOE = 2, B_PERIODIC
 
 struct Mesh {
     int n_cells = 0;
+    int nx = 0, ny = 0;  // a rectangle's cells per axis (0 for meshes built from arrays)
     // cells
     std::vector<V3> center;
     std::vector<double> volume;
@@ -751,6 +752,8 @@ static void make_rectangle(Mesh &m, int nx, int ny, double x_min, double x_max, 
 
     const int N = nx * ny;
     m.n_cells = N;
+    m.nx = nx;
+    m.ny = ny;
     m.center.resize(N);
     m.volume.resize(N);
     m.verts.resize(9 * (size_t)N);

@@ -228,6 +228,17 @@ TR_CASES = {
     "tr_disk_30x21_crpv3_rotation_split": (30, 21, "CRP_V3", TR_ROTATION, True, 20),
     "tr_disk_30x21_crpv5_translation_split": (30, 21, "CRP_V5", TR_TRANSLATION, True, 20),
 }
+# the MUSCL and WENO families (make_golden.py --transfer-high-order)
+TR_HIGH_ORDER_CASES = {
+    "tr_disk_32x22_muscld_rotation_split": (32, 22, "MUSCLd", TR_ROTATION, True, 25),
+    "tr_disk_32x22_muscln_translation_any": (32, 22, "MUSCLn", TR_TRANSLATION, False, 25),
+    "tr_disk_30x21_muscldcrp_translation_split": (30, 21, "MUSCLd_CRP", TR_TRANSLATION, True, 20),
+    "tr_disk_30x21_musclncrp_rotation_any": (30, 21, "MUSCLn_CRP", TR_ROTATION, False, 20),
+    "tr_disk_30x21_musclmc_rotation_split": (30, 21, "MUSCL_MC", TR_ROTATION, True, 20),
+    "tr_disk_30x21_musclmccrp_translation_any": (30, 21, "MUSCL_MC_CRP", TR_TRANSLATION, False, 20),
+    "tr_disk_30x21_weno_rotation_split": (30, 21, "WENO", TR_ROTATION, True, 20),
+    "tr_disk_30x21_wenocrp_translation_any": (30, 21, "WENO_CRP", TR_TRANSLATION, False, 20),
+}
 
 
 def make_tr(name, nx, ny, method, vel, split, steps):
@@ -240,7 +251,7 @@ def make_tr(name, nx, ny, method, vel, split, steps):
     r = RT.RefTransfer(nx, ny, box=box, bounds=(2, 2, 2, 2), method=method, CFL=0.5, vel=vel)
     u0 = r.disk(0.15, 0.5, 0.1)
     r.set_u(u0)
-    r.update_interface(3 if method.startswith("VOF") else 0)
+    r.update_interface(3 if method.startswith(("VOF", "MUSCL", "WENO")) else 0)
     _, n0, p0 = r.get()
     dts = []
     for _ in range(steps):
@@ -255,8 +266,8 @@ def make_tr(name, nx, ny, method, vel, split, steps):
                         CFL=0.5, u0=u0, n0=n0, p0=p0, dts=np.array(dts), u=u, n=n, p=p, flags=r.flags())
 
 
-def make_trs():
-    for name, spec in TR_CASES.items():
+def make_trs(cases=TR_CASES):
+    for name, spec in cases.items():
         make_tr(name, *spec)
     print("wrote transfer cases")
 
@@ -417,7 +428,9 @@ def make_amr_cycles():
 
 
 if __name__ == "__main__":
-    if "--transfer" in sys.argv:
+    if "--transfer-high-order" in sys.argv:
+        make_trs(TR_HIGH_ORDER_CASES)
+    elif "--transfer" in sys.argv:
         make_trs()
     elif "--vtu" in sys.argv:
         make_vtu()

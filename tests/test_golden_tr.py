@@ -34,7 +34,7 @@ def test_oracle_transfer_matches_reference(name):
     m = O.Mesh(nx, ny, *map(float, g["box"]), bounds=tuple(int(b) for b in g["bounds"]))
     s = O.TrSolver(m, method=method, CFL=float(g["CFL"]), vel=vel_of(g))
     s.set_u(g["u0"])
-    s.update_interface(3 if method.startswith("VOF") else 0)
+    s.update_interface(3 if method.startswith(("VOF", "MUSCL", "WENO")) else 0)
     _, n0, p0 = s.get()
     assert same(n0, g["n0"]) and same(p0, g["p0"]), "initial reconstruction differs"
     dirs = (1, 2) if bool(g["split"]) else (0,)
@@ -68,7 +68,7 @@ def test_oracle_transfer_matches_reference_build_directly():
                 u0 = r.disk(0.3, 0.4, 0.15)
                 r.set_u(u0)
                 s.set_u(u0)
-                sm = 3 if method.startswith("VOF") else 0
+                sm = 3 if method.startswith(("VOF", "MUSCL", "WENO")) else 0
                 r.update_interface(sm)
                 s.update_interface(sm)
                 for _ in range(6):

@@ -9,9 +9,15 @@ namespace zg {
 namespace tr {
 
 // Transfer::Method values (transfer.h:25-51) with GPU kernels.
-enum Method { CRP_V3 = 0, CRP_V5 = 1, CRP_SE = 2, CRP_N1 = 3, CRP_N2 = 4, VOF = 5, VOF_CRP = 6 };
+enum Method {
+    CRP_V3 = 0, CRP_V5 = 1, CRP_SE = 2, CRP_N1 = 3, CRP_N2 = 4, VOF = 5, VOF_CRP = 6,
+    MUSCLd = 7, MUSCLn = 8, MUSCLd_CRP = 9, MUSCLn_CRP = 10, MUSCL_MC = 11, MUSCL_MC_CRP = 12, WENO = 13,
+    WENO_CRP = 14
+};
 
 __host__ __device__ inline bool vof_type(int m) { return m == VOF || m == VOF_CRP; }
+__host__ __device__ inline bool muscl_type(int m) { return m >= MUSCLd && m <= MUSCL_MC_CRP; }  // transfer.cpp:29-36
+__host__ __device__ inline bool weno_type(int m) { return m == WENO || m == WENO_CRP; }         // transfer.cpp:38-41
 
 // Uniform non-periodic rectangle, cell ic = i * ny + j; geometry tables with
 // the reference's formulas (filled by zg_mesh_rectangle).
@@ -50,6 +56,8 @@ struct TrArgs {
     int *flist;                // faces whose VOF flux clips polygons (index over the update's faces)
     int *clist;                // cells with a non-zero interface normal
     unsigned char *zero_np;    // 1: both n / p buffers of the cell hold n = (+0, +0) and p = its centre
+    double *gx, *gy;           // the MUSCL slopes du_dx, du_dy per cell
+    int limiter;               // m_limiter of MUSCL_MC (transfer.cpp:47: MC)
 };
 
 // Transfer::compute_dt (transfer.cpp:88-105) into *a.dt.  With `advance`
@@ -57,9 +65,16 @@ struct TrArgs {
 // transfer problem's time loop does (problems/transfer.cpp:213-232).
 void launch_compute_dt(const TrArgs &a, bool advance, double t_end, cudaStream_t st);
 
+// Transfer::compute_slopes (transfer.cpp:404-469) of the MUSCL methods.
+void launch_slopes(const TrArgs &a, cudaStream_t st);
+
 // Fluxes through the interior faces of direction dir (0 ANY, 1 X, 2 Y):
-// swept polygons (VOF, VOF_CRP) or the CRP formulas.
+// swept polygons (VOF, VOF_CRP), the CRP formulas, or the MUSCL face values.
 void launch_flux(const TrArgs &a, int dir, cudaStream_t st);
+
+// Transfer::update_WENO's fluxes and update (transfer.cpp:541-666) into
+// u_next; the caller swaps u and u_next.
+void launch_weno(const TrArgs &a, int dir, cudaStream_t st);
 
 // u_next <- between(u1 - sum of face fluxes / volume, 0, 1); the caller
 // swaps u and u_next.

@@ -2,7 +2,8 @@
 // (math/solver/transfer.cpp) on a uniform non-periodic rectangle: the VOF
 // and VOF_CRP fluxes from swept polygons (flux_VOF, transfer.cpp:250-292),
 // the CRP family (CRP_V3, CRP_V5, CRP_SE, CRP_N1, CRP_N2; transfer.cpp:
-// 109-248), the interface reconstruction InterfaceRecovery
+// 109-248), the MUSCL family (transfer.cpp:345-469), the interface
+// reconstruction InterfaceRecovery
 // (geom/interface_recovery.cpp) with the polygon clipping and Newton section
 // search of geom/primitives/polygon.cpp, and the CFL time step.
 //
@@ -12,8 +13,9 @@
 // evaluated once: the reference evaluates it from both cells, and the two
 // results are exact negatives except where the normal velocity is exactly 0
 // (both cells then take the other one as upwind) and for CRP_N2 (whose
-// neighbour plane differs); those cases are evaluated from each side.  Each
-// cell sums its faces in slot order L, R, B, T as the reference does.
+// neighbour plane differs); those cases are evaluated from each side, and so
+// is every face of the MUSCL family.  Each cell sums its faces in slot order
+// L, R, B, T as the reference does.
 //
 // Arithmetic follows the reference term by term (compiled with -fmad=false).
 // The reference's vectors carry a z component that is +-0 throughout the
@@ -457,6 +459,13 @@ __device__ __forceinline__ double flux_2D(double a1, double a2, double S, double
     return sgn(vn) * between(gamma * as, F_min, F_max);
 }
 
+// limiters::vanAlbada2(a, b) (limiter.cxx:92-96)
+__device__ __forceinline__ double van_albada2(double a, double b) {
+    if (a * b <= 0.0) return 0.0;
+    const double eps = 10e-6;
+    return (2.0 * a * b + eps) / (a * a + b * b + eps);
+}
+
 // best_face_fraction + flux_CRP (transfer.cpp:179-206)
 __device__ __forceinline__ double flux_crp(double a1, double a2, double S, double V1, double V2, double vn, double dt,
                                            double Flux) {
@@ -622,11 +631,62 @@ __device__ double face_crp_side(const TrArgs &a, int ic, int id, P2 v1, P2 v2, P
     return flux_2D(a1, a2, S, a.m.vol, a.m.vol, a_sig, vn, dt);
 }
 
+// Transfer::fluxes_MUSCL for one face seen from cell c (i, j) with neighbour
+// d (di, dj) (transfer.cpp:345-402); fn is the normal out of c.  The face
+// value is FaceExtra::Direct for MUSCL_MC (face_extra.h:121-171, limited to
+// the two cells' values) and FaceExtra::ATvL otherwise (face_extra.h:
+// 264-350, van Albada 2); the CRP forms then pass the flux through
+// flux_CRP.  The two cells' views of a face are not exact negatives (the
+// ATvL value is formed from each side's geometry), so each is evaluated.
+__device__ double face_muscl_side(const TrArgs &a, int ci, int cj, int di, int dj, P2 fc, P2 fn, double S,
+                                  double dt) {
+    const int ic = ci * a.m.ny + cj, id = di * a.m.ny + dj;
+    const P2 V = velocity(a.vel, fc.x, fc.y);
+    const double vn = V.x * fn.x + V.y * fn.y;
+    const double uc = a.u[ic], un = a.u[id];
+    const double ccx = a.m.cx[ci], ccy = a.m.cy[cj], ncx = a.m.cx[di], ncy = a.m.cy[dj];
+    double a_sig;
+    if (a.method == MUSCL_MC || a.method == MUSCL_MC_CRP) {
+        const double duc = a.gx[ic] * (fc.x - ccx) + a.gy[ic] * (fc.y - ccy) + 0.0 * 0.0;
+        const double dun = a.gx[id] * (fc.x - ncx) + a.gy[id] * (fc.y - ncy) + 0.0 * 0.0;
+        a_sig = vn > 0.0 ? uc + duc : un + dun;
+        a_sig = between(a_sig, uc, un);
+    } else {
+        const double rcx = fc.x - ccx, rcy = fc.y - ccy, rnx = ncx - fc.x, rny = ncy - fc.y;
+        const double dx_c = sqrt(rcx * rcx + rcy * rcy), dx_n = sqrt(rnx * rnx + rny * rny);
+        const double dx = dx_c + dx_n;
+        if (vn > 0.0) {  // m(u_c)
+            const double du_c = (a.gx[ic] * rcx + a.gy[ic] * rcy + 0.0 * 0.0) / dx_c;
+            const double delta = dx_c / dx;
+            const double eta = (12.0 * delta * delta - 1.0) / 24.0;
+            const double dzp = un - uc;
+            const double dzm = 2.0 * du_c * dx - dzp;
+            const double s = van_albada2(dzm, dzp);
+            a_sig = uc + s * ((0.5 * delta - s * eta) * dzm + (0.5 * delta + s * eta) * dzp);
+        } else {  // p(u_n)
+            const double du_n = (a.gx[id] * rnx + a.gy[id] * rny + 0.0 * 0.0) / dx_n;
+            const double delta = dx_n / dx;
+            const double eta = (12.0 * delta * delta - 1.0) / 24.0;
+            const double dzm = un - uc;
+            const double dzp = 2.0 * du_n * dx - dzm;
+            const double s = van_albada2(dzm, dzp);
+            a_sig = un - s * ((0.5 * delta + s * eta) * dzm + (0.5 * delta - s * eta) * dzp);
+        }
+    }
+    double Flux = a_sig * vn * dt * S;
+    if (a.method == MUSCLd_CRP || a.method == MUSCLn_CRP || a.method == MUSCL_MC_CRP)
+        Flux = flux_crp(uc, un, S, a.m.vol, a.m.vol, vn, dt, Flux);
+    return Flux;
+}
+
 template <bool POLY>
 __device__ __forceinline__ void face_fluxes(const TrArgs &a, const Face &f, int dir, double &fa, double &fb) {
     const double dt = *a.dt;
     if (vof_type(a.method)) {
         face_vof<POLY>(a, f, dir, dt, fa, fb);
+    } else if (muscl_type(a.method)) {
+        fa = face_muscl_side(a, f.iA, f.jA, f.iB, f.jB, f.fc, f.fn, f.S, dt);
+        fb = face_muscl_side(a, f.iB, f.jB, f.iA, f.jA, f.fc, mk(-f.fn.x, -f.fn.y), f.S, dt);
     } else {
         const int icA = f.iA * a.m.ny + f.jA, icB = f.iB * a.m.ny + f.jB;
         fa = face_crp_side(a, icA, icB, f.v1, f.v2, f.fc, f.fn, f.S, dt);
@@ -953,7 +1013,193 @@ __global__ void __launch_bounds__(BLOCK) k_flags(TrArgs a, int *flags) {
 
 inline unsigned blocks(long long n) { return (unsigned)((n + BLOCK - 1) / BLOCK); }
 
+// Transfer::compute_slopes (transfer.cpp:404-469), one thread per cell,
+// faces in slot order L, R, B, T with the reference's normals (signed zeros
+// included).  MUSCLn, MUSCLn_CRP: the part of each face under the cell's
+// interface plane, sum a_sig S n / V.  The others: gradient::LSM of u1
+// (gradient.h:226-282; boundary faces take the cell's own value at the
+// mirrored centre), limited (gradient.h:412-474) for MUSCL_MC, with the
+// 2-D reduction of the 3x3 system that the single-material kernels use.
+__global__ void __launch_bounds__(BLOCK) k_slopes(TrArgs a) {
+    const int nx = a.m.nx, ny = a.m.ny;
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= nx * ny) return;
+    const int i = ic / ny, j = ic - i * ny;
+    const double fnx[4] = {-1.0, 1.0, -0.0, 0.0}, fny[4] = {-0.0, 0.0, -1.0, 1.0};
+    const double S[4] = {a.m.hy, a.m.hy, a.m.hx, a.m.hx};
+    if (a.method == MUSCLn || a.method == MUSCLn_CRP) {
+        const int c = a.cur;
+        const double pnx = a.nx[c][ic], pny = a.ny[c][ic];
+        const double pp = a.px[c][ic] * pnx + a.py[c][ic] * pny;
+        // face vertices (face_nodes2d): L, R from bottom to top; B, T from left to right
+        const double xl = a.m.X[i], xr = a.m.X[i + 1], yb = a.m.Y[j], yt = a.m.Y[j + 1];
+        const P2 vs1[4] = {mk(xl, yb), mk(xr, yb), mk(xl, yb), mk(xl, yt)};
+        const P2 vs2[4] = {mk(xl, yt), mk(xr, yt), mk(xr, yb), mk(xr, yt)};
+        double gx = 0.0, gy = 0.0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const P2 v1 = vs1[s], v2 = vs2[s];
+            const bool in1 = v1.x * pnx + v1.y * pny < pp, in2 = v2.x * pnx + v2.y * pny < pp;
+            double a_sig;
+            if (in1 && in2) {
+                a_sig = 1.0;
+            } else if (!in1 && !in2) {
+                a_sig = 0.0;
+            } else {
+                // find_fast(plane, seg): line {v2, v2 - v1} (intersection.cpp:63-70)
+                const double tx = v2.x - v1.x, ty = v2.y - v1.y;
+                const double t = (pp - (pnx * v2.x + pny * v2.y)) / (pnx * tx + pny * ty);
+                const double qx = v2.x + t * tx, qy = v2.y + t * ty;
+                const double len = sqrt(tx * tx + ty * ty);
+                a_sig = in1 ? sqrt((qx - v1.x) * (qx - v1.x) + (qy - v1.y) * (qy - v1.y)) / len
+                            : sqrt((qx - v2.x) * (qx - v2.x) + (qy - v2.y) * (qy - v2.y)) / len;
+            }
+            gx += a_sig * S[s] * fnx[s];
+            gy += a_sig * S[s] * fny[s];
+        }
+        a.gx[ic] = gx / a.m.vol;
+        a.gy[ic] = gy / a.m.vol;
+        return;
+    }
+    const double uc = a.u[ic], pcx = a.m.cx[i], pcy = a.m.cy[j];
+    double wv[4], drx[4], dry[4], drnx[4], drny[4], dn[4];
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0, Fx = 0.0, Fy = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const bool bnd = (s == 0 && i == 0) || (s == 1 && i == nx - 1) || (s == 2 && j == 0) || (s == 3 && j == ny - 1);
+        const int nb = s == 0 ? ic - ny : s == 1 ? ic + ny : s == 2 ? ic - 1 : ic + 1;
+        double ncx, ncy;
+        if (!bnd) {
+            ncx = s < 2 ? a.m.cx[s == 0 ? i - 1 : i + 1] : pcx;
+            ncy = s < 2 ? pcy : a.m.cy[s == 2 ? j - 1 : j + 1];
+        } else {  // symm_point (amr_faces.h:197-199)
+            const double fcx = s < 2 ? a.m.X[s == 0 ? i : i + 1] : a.m.fxm[i];
+            const double fcy = s < 2 ? a.m.fym[j] : a.m.Y[s == 2 ? j : j + 1];
+            const double d2 = 2.0 * ((fcx - pcx) * fnx[s] + (fcy - pcy) * fny[s]);
+            ncx = pcx + d2 * fnx[s];
+            ncy = pcy + d2 * fny[s];
+        }
+        const double un = bnd ? uc : a.u[nb];
+        const double rx = ncx - pcx, ry = ncy - pcy;
+        const double d = rx * fnx[s] + ry * fny[s];
+        const double nxx = d * fnx[s], nyy = d * fny[s];
+        const double w = 1.0 * S[s] / cube_rn(sqrt(nxx * nxx + nyy * nyy));
+        const double wdx = w * nxx, wdy = w * nyy;
+        A00 += wdx * rx;
+        A01 += wdx * ry;
+        A10 += wdy * rx;
+        A11 += wdy * ry;
+        const double dF = un - uc;
+        Fx += w * dF * nxx;
+        Fy += w * dF * nyy;
+        wv[s] = w;
+        drx[s] = rx;
+        dry[s] = ry;
+        drnx[s] = nxx;
+        drny[s] = nyy;
+        dn[s] = dF;
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;
+    const double det = A11 * A00 + (-A01) * A10;
+    const double inv = 1.0 / det;
+    const double B00 = A11 * inv, B01 = (-A01) * inv, B10 = (-A10) * inv, B11 = A00 * inv;
+    const double g0x = B00 * Fx + B01 * Fy, g0y = B10 * Fx + B11 * Fy;
+    if (a.method != MUSCL_MC && a.method != MUSCL_MC_CRP) {
+        a.gx[ic] = g0x;
+        a.gy[ic] = g0y;
+        return;
+    }
+    double lx = 0.0, ly = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        const double dF_p = dn[s];
+        const double du_n = g0x * drx[s] + g0y * dry[s];
+        const double dF_m = 2.0 * du_n - dF_p;
+        const double dF_lim = limiter2(a.limiter, dF_m, dF_p) * dF_p;
+        lx += wv[s] * dF_lim * drnx[s];
+        ly += wv[s] * dF_lim * drny[s];
+    }
+    a.gx[ic] = B00 * lx + B01 * ly;
+    a.gy[ic] = B10 * lx + B11 * ly;
+}
+
+// WENO5 (math/calc/weno.h:113-169) on the five values q[0..4] centred on
+// q[2]: the value at the centre cell's right face (p) or left face (m)
+__device__ __forceinline__ double weno_beta(int kind, const double *q) {  // weno.h:88-107
+    const double d2 = q[0] - 2.0 * q[1] + q[2];
+    const double d1 = kind == 2 ? q[0] - 4.0 * q[1] + 3.0 * q[2] : (kind == 1 ? q[0] - q[2] : 3.0 * q[0] - 4.0 * q[1] + q[2]);
+    return 13.0 / 12.0 * d2 * d2 + 1.0 / 4.0 * d1 * d1;
+}
+__device__ double weno5(const double u[5], bool right) {
+    const double *s2 = u, *s1 = u + 1, *s0 = u + 2;
+    const double b0 = weno_beta(0, s0), b1 = weno_beta(1, s1), b2 = weno_beta(2, s2);
+    double d0_c, d1_c, d2_c, e0, e1, e2;
+    if (right) {
+        d0_c = 3.0 / 10.0, d1_c = 6.0 / 10.0, d2_c = 1.0 / 10.0;
+        e0 = +1.0 / 3.0 * s0[0] + +5.0 / 6.0 * s0[1] + -1.0 / 6.0 * s0[2];
+        e1 = -1.0 / 6.0 * s1[0] + +5.0 / 6.0 * s1[1] + +1.0 / 3.0 * s1[2];
+        e2 = +1.0 / 3.0 * s2[0] + -7.0 / 6.0 * s2[1] + 11.0 / 6.0 * s2[2];
+    } else {
+        d0_c = 1.0 / 10.0, d1_c = 6.0 / 10.0, d2_c = 3.0 / 10.0;
+        e0 = 11.0 / 6.0 * s0[0] + -7.0 / 6.0 * s0[1] + +1.0 / 3.0 * s0[2];
+        e1 = +1.0 / 3.0 * s1[0] + +5.0 / 6.0 * s1[1] + -1.0 / 6.0 * s1[2];
+        e2 = -1.0 / 6.0 * s2[0] + +5.0 / 6.0 * s2[1] + +1.0 / 3.0 * s2[2];
+    }
+    const double d0 = d0_c / ((1.0e-8 + b0) * (1.0e-8 + b0));
+    const double d1 = d1_c / ((1.0e-8 + b1) * (1.0e-8 + b1));
+    const double d2 = d2_c / ((1.0e-8 + b2) * (1.0e-8 + b2));
+    const double w0 = d0 / (d0 + d1 + d2);
+    const double w1 = d1 / (d0 + d1 + d2);
+    const double w2 = d2 / (d0 + d1 + d2);
+    return w0 * e0 + w1 * e1 + w2 * e2;
+}
+
+// Transfer::update_WENO's face loop and update (transfer.cpp:541-666), one
+// thread per cell: every face of the direction, boundary faces included
+// (their neighbour is the cell itself), each with the five-cell stencil of
+// its upwind cell taken through EuMesh::operator()(i, j)'s periodic index
+// wrap (eu_mesh.cpp:826-830); faces in slot order L, R, B, T, then
+// u_next = between(u1 - sum / V, 0, 1).
+__global__ void __launch_bounds__(BLOCK) k_weno(TrArgs a, int dir) {
+    const int nx = a.m.nx, ny = a.m.ny;
+    const int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= nx * ny) return;
+    const int i = ic / ny, j = ic - i * ny;
+    const double dt = *a.dt;
+    const double fnx[4] = {-1.0, 1.0, -0.0, 0.0}, fny[4] = {-0.0, 0.0, -1.0, 1.0};
+    double fluxes = 0.0;
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+        if ((s < 2 && dir == 2) || (s >= 2 && dir == 1)) continue;
+        const P2 fc = s < 2 ? mk(a.m.X[s == 0 ? i : i + 1], a.m.fym[j]) : mk(a.m.fxm[i], a.m.Y[s == 2 ? j : j + 1]);
+        const double S = s < 2 ? a.m.hy : a.m.hx;
+        const bool bnd = (s == 0 && i == 0) || (s == 1 && i == nx - 1) || (s == 2 && j == 0) || (s == 3 && j == ny - 1);
+        const int nb = bnd ? ic : (s == 0 ? ic - ny : s == 1 ? ic + ny : s == 2 ? ic - 1 : ic + 1);
+        const P2 V = velocity(a.vel, fc.x, fc.y);
+        const double vn = V.x * fnx[s] + V.y * fny[s];
+        const bool low = s == 0 || s == 2;
+        const int K = (s < 2 ? i : j) + (vn > 0.0 ? 0 : (low ? -1 : 1));
+        double st[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            const int q = K - 2 + k;
+            st[k] = s < 2 ? a.u[(size_t)ny * ((q + nx) % nx) + j] : a.u[(size_t)ny * i + (q + ny) % ny];
+        }
+        const double a_sig = between(weno5(st, vn > 0.0 ? !low : low), 0.0, 1.0);
+        double Flux = a_sig * vn * dt * S;
+        if (a.method == WENO_CRP) Flux = flux_crp(a.u[ic], a.u[nb], S, a.m.vol, a.m.vol, vn, dt, Flux);
+        fluxes += Flux;
+    }
+    const double u2 = a.u[ic] - fluxes / a.m.vol;
+    a.u_next[ic] = dmax(0.0, dmin(u2, 1.0));
+}
+
 }  // namespace
+
+void launch_weno(const TrArgs &a, int dir, cudaStream_t st) {
+    const int n = a.m.nx * a.m.ny;
+    k_weno<<<(n + BLOCK - 1) / BLOCK, BLOCK, 0, st>>>(a, dir);
+}
 
 void launch_compute_dt(const TrArgs &a, bool advance, double t_end, cudaStream_t st) {
     const long long n = (long long)a.m.nx * a.m.ny;
@@ -985,6 +1231,11 @@ unsigned list_blocks(K kernel, long long n) {
     }
     const unsigned g = blocks(n);
     return g < resident ? (g ? g : 1u) : resident;
+}
+
+void launch_slopes(const TrArgs &a, cudaStream_t st) {
+    const int n = a.m.nx * a.m.ny;
+    k_slopes<<<(n + BLOCK - 1) / BLOCK, BLOCK, 0, st>>>(a);
 }
 
 void launch_flux(const TrArgs &a, int dir, cudaStream_t st) {

@@ -1854,14 +1854,21 @@ void tr_interface(zg_ctx *c, int smoothing) {
     }
 }
 
-// Transfer::update (transfer.cpp:471-537): fluxes, update, reconstruction
-// (three smoothing passes for the VOF methods, none for CRP).
+// Transfer::update (transfer.cpp:471-666): the MUSCL slopes, fluxes,
+// update (one kernel for WENO), reconstruction (three smoothing passes for
+// the VOF, MUSCL and WENO methods, none for CRP).
 void tr_update(zg_ctx *c, int dir) {
     const tr::TrArgs &a = c->targs;
-    timed(c, ZG_K_TR_FLUX, [&] { tr::launch_flux(a, dir, c->stream); });
-    timed(c, ZG_K_TR_UPDATE, [&] { tr::launch_apply(a, dir, c->stream); });
+    const int m = c->tpar.method;
+    if (tr::weno_type(m)) {
+        timed(c, ZG_K_TR_FLUX, [&] { tr::launch_weno(a, dir, c->stream); });
+    } else {
+        if (tr::muscl_type(m)) timed(c, ZG_K_TR_FLUX, [&] { tr::launch_slopes(a, c->stream); });
+        timed(c, ZG_K_TR_FLUX, [&] { tr::launch_flux(a, dir, c->stream); });
+        timed(c, ZG_K_TR_UPDATE, [&] { tr::launch_apply(a, dir, c->stream); });
+    }
     std::swap(c->targs.u, c->targs.u_next);
-    tr_interface(c, tr::vof_type(c->tpar.method) ? 3 : 0);
+    tr_interface(c, tr::vof_type(m) || tr::muscl_type(m) || tr::weno_type(m) ? 3 : 0);
 }
 
 void tr_dt(zg_ctx *c, bool advance, double t_end) {
@@ -1879,8 +1886,11 @@ int zg_tr_configure(zg_ctx *c, const zg_tr_params *p) {
     if (c->mesh.xper || c->mesh.yper)
         return fail(c, ZG_ERR_ARG, "zg_tr_configure: periodic boundaries are not supported (the reference clips "
                                    "the upwind cell's polygon across the domain there)");
-    if (p->method < ZG_TR_CRP_V3 || p->method > ZG_TR_VOF_CRP)
-        return fail(c, ZG_ERR_ARG, "zg_tr_configure: method without GPU kernels (MUSCL and WENO families)");
+    if (p->method < ZG_TR_CRP_V3 || p->method > ZG_TR_WENO_CRP)
+        return fail(c, ZG_ERR_ARG, "zg_tr_configure: unknown method");
+    if (tr::weno_type(p->method) && (c->mesh.nx < 3 || c->mesh.ny < 3))
+        return fail(c, ZG_ERR_ARG, "zg_tr_configure: WENO needs at least 3 cells per axis (its stencil wraps "
+                                   "indices once, as EuMesh::operator() does)");
     if (p->velocity != ZG_TR_TRANSLATION && p->velocity != ZG_TR_ROTATION)
         return fail(c, ZG_ERR_ARG, "zg_tr_configure: unknown velocity field");
     DeviceGuard g(c->device);
@@ -1900,12 +1910,13 @@ int zg_tr_configure(zg_ctx *c, const zg_tr_params *p) {
     }
     a.method = p->method;
     a.CFL = c->tpar.CFL;
+    a.limiter = LIM_MC;  // Transfer's m_limiter (transfer.cpp:47)
     if (c->tr_configured) return ZG_OK;
 
     const size_t n = (size_t)c->n, nx = (size_t)c->mesh.nx, ny = (size_t)c->mesh.ny;
     const size_t nfx = (nx + 1) * ny, nfy = nx * (ny + 1);
     // fields, then the scalars, then the work lists (ints): faces, cells
-    const size_t total = 10 * n + 2 * nfx + 2 * nfy + TR_NSCALAR + (nfx + nfy + n + 1) / 2 + 1 + (n + 7) / 8;
+    const size_t total = 12 * n + 2 * nfx + 2 * nfy + TR_NSCALAR + (nfx + nfy + n + 1) / 2 + 1 + (n + 7) / 8;
     ZG_CUDA(c, cudaMalloc(&c->d_tr, total * sizeof(double)));
     ZG_CUDA(c, cudaMemsetAsync(c->d_tr, 0, total * sizeof(double), c->stream));
     double *b = c->d_tr;
@@ -1920,6 +1931,9 @@ int zg_tr_configure(zg_ctx *c, const zg_tr_params *p) {
         b += 4 * n;
     }
     a.cur = 0;
+    a.gx = b;
+    a.gy = b + n;
+    b += 2 * n;
     a.fxa = b;
     a.fxb = b + nfx;
     b += 2 * nfx;

@@ -29,7 +29,7 @@ _P = C.POINTER(C.c_double)
 
 
 class Method(enum.IntEnum):
-    """Transfer::Method (transfer.h:25-51); the MUSCL and WENO families have no kernels."""
+    """Transfer::Method (transfer.h:25-51)."""
     CRP_V3 = 0
     CRP_V5 = 1
     CRP_SE = 2
@@ -87,8 +87,6 @@ class Transfer:
         return Method(self.p.method)
 
     def set_method(self, method: Method):  # transfer.cpp:73-75
-        if int(method) > Method.VOF_CRP:
-            raise ZgError(-1, f"{Method(method).name}: the MUSCL and WENO families have no GPU kernels")
         self.p.method = int(method)
         self._push()
 
