@@ -93,8 +93,14 @@ __device__ __forceinline__ C4<R> flux_x(const FS<R> &z) {
     return C4<R>{ru, ru * z.u + z.p, ru * z.v, (z.r * (z.e + R(0.5) * (z.u * z.u + z.v * z.v)) + z.p) * z.u};
 }
 
-// HLLC (hllc.cpp:23-83) in the face frame, the divisions sharing reciprocals:
-// 1/(a_R - a_L), 1/((S_L - S_C)(S_R - S_C)) and 1/(a_L a_R).
+// HLLC (hllc.cpp:23-83) in the face frame.  hllc.cpp writes the flux in its
+// symmetric form 1/2 (F_L + F_R + S_L (Q*_L - Q_L) + |S_C| (Q*_L - Q*_R) +
+// S_R (Q*_R - Q_R)); through the Rankine-Hugoniot relations that define the
+// star states this is the star flux on the side of the contact the face
+// lies on: F_L + S_L (Q*_L - Q_L) for S_C >= 0, F_R + S_R (Q*_R - Q_R)
+// otherwise.  The kernel evaluates that one side (the two forms agree to
+// rounding), with the side's state chosen before the arithmetic so that a
+// warp runs one path.
 template <typename R>
 __device__ __forceinline__ C4<R> hllc_fs(const FS<R> &L, const FS<R> &Rs, const EosR<R> &eos) {
     const R cL = sqrt(eos.gamma * (L.p + eos.P0) * L.ri), cR = sqrt(eos.gamma * (Rs.p + eos.P0) * Rs.ri);
@@ -105,25 +111,25 @@ __device__ __forceinline__ C4<R> hllc_fs(const FS<R> &L, const FS<R> &Rs, const 
     if (SR <= R(0)) return flux_x(Rs);
     const R aL = L.r * (SL - L.u), aR = Rs.r * (SR - Rs.u);
     const R SC = (L.p - Rs.p + aR * Rs.u - aL * L.u) * rcp_r(aR - aL);
-    const R dl = SL - SC, dr = SR - SC;
-    const R i1 = rcp_r(dl * dr), i2 = rcp_r(aL * aR);
-    const R rsL = aL * dr * i1, rsR = aR * dl * i1;
-    const R EL = L.e + R(0.5) * (L.u * L.u + L.v * L.v);
-    const R ER = Rs.e + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v);
-    const R EsL = EL + (SC - L.u) * (SC + L.p * aR * i2);
-    const R EsR = ER + (SC - Rs.u) * (SC + Rs.p * aL * i2);
-    const C4<R> FL = flux_x(L), FR = flux_x(Rs);
-    const R QL[4] = {L.r, L.r * L.u, L.r * L.v, L.r * EL};
-    const R QR[4] = {Rs.r, Rs.r * Rs.u, Rs.r * Rs.v, Rs.r * ER};
-    const R QsL[4] = {rsL, rsL * SC, rsL * L.v, rsL * EsL};
-    const R QsR[4] = {rsR, rsR * SC, rsR * Rs.v, rsR * EsR};
-    const R fl[4] = {FL.r, FL.mu, FL.mv, FL.E}, fr[4] = {FR.r, FR.mu, FR.mv, FR.E};
-    const R aSC = fabs(SC);
-    R o[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-        o[k] = R(0.5) * (fl[k] + fr[k] + SL * (QsL[k] - QL[k]) + aSC * (QsL[k] - QsR[k]) + SR * (QsR[k] - QR[k]));
-    return C4<R>{o[0], o[1], o[2], o[3]};
+    const bool left = SC >= R(0);
+    FS<R> X;
+    X.r = left ? L.r : Rs.r;
+    X.u = left ? L.u : Rs.u;
+    X.v = left ? L.v : Rs.v;
+    X.p = left ? L.p : Rs.p;
+    X.e = left ? L.e : Rs.e;
+    const R SX = left ? SL : SR, aX = left ? aL : aR;
+    const R rs = aX * rcp_r(SX - SC);
+    const R EX = X.e + R(0.5) * (X.u * X.u + X.v * X.v);
+    const R Es = EX + (SC - X.u) * (SC + X.p * rcp_r(aX));
+    const R ru = X.r * X.u;
+    const R rE = X.r * EX;
+    C4<R> f;
+    f.r = ru + SX * (rs - X.r);
+    f.mu = ru * X.u + X.p + SX * (rs * SC - ru);
+    f.mv = ru * X.v + SX * (rs * X.v - X.r * X.v);
+    f.E = (rE + X.p) * X.u + SX * (rs * Es - rE);
+    return f;
 }
 
 // HLL (hll.cpp:23-57) in the face frame (isolated cells, and the HLL method)
