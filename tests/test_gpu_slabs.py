@@ -1,7 +1,7 @@
 """Slab decomposition on the GPU (zg_state_rows, zg_smf_cfl_min): several
 slabs of one rectangle, each with its own context on the same GPU, joined by
 the in-process communicator (LocalComm: the exchange copies rows through host
-buffers, no kernel waits on another), against the single-domain GPU step
+buffers or device tensors, no kernel waits on another), against the single-domain GPU step
 with the same kernels.  Dyadic cell size: every owned cell and every dt bit
 for bit."""
 import numpy as np
@@ -30,9 +30,10 @@ def initial(nx, ny, seed=5):
     return rho, u, v, p, p / (0.4 * rho)
 
 
+@pytest.mark.parametrize("device_rows", [False, True], ids=["host rows", "device rows"])
 @pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("name,nx,ny,bounds,acc,scheme,kern", CASES, ids=[c[0] for c in CASES])
-def test_gpu_slabs_match_the_single_domain(gpu_lib, name, nx, ny, bounds, acc, scheme, kern, world):
+def test_gpu_slabs_match_the_single_domain(gpu_lib, name, nx, ny, bounds, acc, scheme, kern, world, device_rows):
     Z = gpu_lib
     steps = 8
 
@@ -56,7 +57,7 @@ def test_gpu_slabs_match_the_single_domain(gpu_lib, name, nx, ny, bounds, acc, s
     comm = S.LocalComm()
     for r in range(world):
         slab = S.Slab(nx, ny, (0.0, 1.0, 0.0, 1.0), bounds, world, r, halo=S.halo_rows(acc, scheme == 1))
-        loc = S.GpuSlabSolver(slab, Z.IdealGas(1.4), configure, kernels=Z.Kernels[kern])
+        loc = S.GpuSlabSolver(slab, Z.IdealGas(1.4), configure, kernels=Z.Kernels[kern], device_rows=device_rows)
         lo, hi = slab.rows
         gl, gh = slab.ghosts
         idx = np.concatenate([np.arange((i % nx) * ny, (i % nx + 1) * ny) for i in range(lo - gl, hi + gh)])

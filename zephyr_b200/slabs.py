@@ -179,9 +179,10 @@ class TorchComm:
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
+        device_rows = getattr(stepper.local, "device_rows", False) and self.device.type == "cuda"
         inbox = {}
         for src, rf, rw in recvs:  # in posting order: messages of one peer stay in the order sent
-            inbox.setdefault(src, []).append((rf.cpu().numpy(), rw.cpu().numpy()))
+            inbox.setdefault(src, []).append((rf, rw) if device_rows else (rf.cpu().numpy(), rw.cpu().numpy()))
         stepper.incoming(inbox)
 
     def min_all(self, value: float) -> float:
@@ -251,9 +252,11 @@ class SlabStepper:
         self.dt = self.local.dt()
 
     def owned_state(self):
-        """(fields (5, rows * ny), wait) of the owned rows."""
+        """(fields (5, rows * ny), wait) of the owned rows, in host memory."""
         first, last = self.slab.owned_local()
         f, w = self.local.get_rows(first, last - first)
+        if hasattr(f, "cpu"):
+            f, w = f.cpu().numpy(), w.cpu().numpy()
         return np.asarray(f).reshape(5, -1), np.asarray(w)
 
 
@@ -268,9 +271,15 @@ def step_all(comm: LocalComm):
 class GpuSlabSolver:
     """The local solver of a slab on one GPU, through the C ABI (FP64 FAST or
     PARITY kernels): a rectangle of the slab's local rows, zg_state_rows for
-    the ghost rows, zg_smf_cfl_min, zg_smf_set_max_dt."""
+    the ghost rows, zg_smf_cfl_min, zg_smf_set_max_dt.
 
-    def __init__(self, slab: Slab, eos, configure, precision=None, kernels=None, device=0, stream=None):
+    device_rows: the rows leave and enter as torch tensors on the slab's GPU
+    (zg_state_rows copies device to device), so a TorchComm on that device
+    sends them with NCCL without a host round trip; otherwise they are numpy
+    arrays in host memory."""
+
+    def __init__(self, slab: Slab, eos, configure, precision=None, kernels=None, device=0, stream=None,
+                 device_rows=False):
         from . import smf as Z
         gen = Z.Rectangle(*slab.local_box)
         gen.set_boundaries(Z.Boundaries(*slab.local_bounds))
@@ -282,6 +291,8 @@ class GpuSlabSolver:
         configure(self.solver)
         self.solver.add_types(self.mesh)
         self.ny = slab.ny
+        self.device = device
+        self.device_rows = device_rows
 
     def set_state(self, rho, u, v, p, e, wait=None):
         self.mesh.set_state(rho, u, v, p, e)
@@ -290,21 +301,47 @@ class GpuSlabSolver:
 
     def get_rows(self, row0, nrows):
         n = nrows * self.ny
-        f = np.empty(5 * n)
-        w = np.empty(n, np.int32)
+        if self.device_rows:
+            import torch
+            dev = torch.device("cuda", self.device)
+            f = torch.empty(5 * n, dtype=torch.float64, device=dev)
+            w = torch.empty(n, dtype=torch.int32, device=dev)
+        else:
+            f = np.empty(5 * n)
+            w = np.empty(n, np.int32)
         self._rows(row0, nrows, f, w, 0)
         return f, w
 
     def put_rows(self, row0, f, w):
-        f = np.ascontiguousarray(f, dtype=np.float64)
-        w = np.ascontiguousarray(w, dtype=np.int32)
-        self._rows(row0, len(w) // self.ny, f, w, 1)
+        if hasattr(f, "data_ptr"):  # torch tensors (device or host)
+            f = f.to(dtype=self._torch().float64).contiguous()
+            w = w.to(dtype=self._torch().int32).contiguous()
+            nrows = w.numel() // self.ny
+        else:
+            f = np.ascontiguousarray(f, dtype=np.float64)
+            w = np.ascontiguousarray(w, dtype=np.int32)
+            nrows = len(w) // self.ny
+        self._rows(row0, nrows, f, w, 1)
+
+    @staticmethod
+    def _torch():
+        import torch
+        return torch
 
     def _rows(self, row0, nrows, f, w, put):
         from ._lib import check
-        check(self.mesh.ctx, self.mesh._lib.zg_state_rows(self.mesh.ctx, int(row0), int(nrows),
-                                                          f.ctypes.data_as(C.POINTER(C.c_double)),
-                                                          w.ctypes.data_as(C.POINTER(C.c_int)), int(put)))
+        if hasattr(f, "data_ptr"):
+            # the copies run on the library's stream; the tensors must be
+            # complete on torch's stream first (zg_state_rows synchronises
+            # its own stream before it returns)
+            if f.is_cuda:
+                self._torch().cuda.current_stream(f.device).synchronize()
+            fp = C.cast(C.c_void_p(f.data_ptr()), C.POINTER(C.c_double))
+            wp = C.cast(C.c_void_p(w.data_ptr()), C.POINTER(C.c_int))
+        else:
+            fp = f.ctypes.data_as(C.POINTER(C.c_double))
+            wp = w.ctypes.data_as(C.POINTER(C.c_int))
+        check(self.mesh.ctx, self.mesh._lib.zg_state_rows(self.mesh.ctx, int(row0), int(nrows), fp, wp, int(put)))
 
     def cfl_min(self):
         from ._lib import check
