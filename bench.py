@@ -639,7 +639,7 @@ def adjoint_variant(torch, dev, stream, local_rank):
     n0 = adj.launch_count()
     ms_f, J = timed(lambda: adj.forward(prm, r, u, v, p))
     ms_g, (J2, dg) = timed(lambda: adj.gradient(prm, r, u, v, p, grad))
-    # the mixed form: FP32 slopes, face states, HLLC and its reverse
+    # the mixed form: FP64 primal, FP32 slopes and reverse-sweep face arithmetic
     pmx = Adjoint.params(steps=100, checkpoint_every=10, dt=dt, precision=1)
     gmx = torch.empty_like(r)
     adj.forward(pmx, r, u, v, p)
@@ -665,9 +665,9 @@ def adjoint_variant(torch, dev, stream, local_rank):
             "checkpoint_every": 10, "J": J, "dJ_dgamma": dg,
             "fd_rel_err_max": max(errs), "fd_rel_err_median": float(np.median(errs)), "fd_directions": 16,
             "fd_rel_err_gamma": abs(fd_g - dg) / abs(dg), "gpu_launches": int(launches),
-            "mixed": {"form": "FP32 slopes (from FP64 neighbour differences), face states, HLLC and its reverse; "
-                              "FP64 primitive states, conserved "
-                              "and adjoint states, flux and cotangent sums, primitive map and gamma",
+            "mixed": {"form": "FP64 primal step with FP32 slopes (from FP64 neighbour differences); reverse "
+                              "sweep with FP32 slope partials, face states, HLLC reverse and face cotangents, "
+                              "FP64 adjoint states, cotangent sums, primitive map and gamma",
                       "forward_ms": ms_fm, "gradient_ms": ms_gm, "adjoint_over_forward": ms_gm / ms_fm,
                       "gradient_speedup_vs_fp64": ms_g / ms_gm, "J_rel_err_vs_fp64": abs(Jm - J) / abs(J),
                       "grad_l2_rel_err_vs_fp64": float(torch.linalg.norm(gmx - grad) / torch.linalg.norm(grad)),

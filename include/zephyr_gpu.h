@@ -598,10 +598,11 @@ typedef struct zg_adj_params {
     int checkpoint_every;  /* steps between stored states */
     double limiter_eps;    /* eps of the smooth limiter (default 1e-8) */
     double probe[4];       /* x_min, x_max, y_min, y_max of the probe box */
-    int precision;         /* zg_precision: FP64, or MIXED (slopes and their partials from FP64
-                              neighbour differences, face states, HLLC and its reverse in FP32;
-                              conserved states, adjoint states, primitive states, flux and
-                              cotangent sums, the primitive map and gamma in FP64) */
+    int precision;         /* zg_precision: FP64, or MIXED (an FP64 primal step with FP32
+                              slopes from FP64 neighbour differences; a reverse sweep with the
+                              slopes' partials, face states, HLLC reverse and face cotangents
+                              in FP32 and the adjoint states, their sums, the primitive map
+                              and gamma in FP64) */
 } zg_adj_params;
 
 /* gamma 1.4, 100 steps, checkpoints every 10, eps 1e-8, probe [0.6,0.7]^2. */

@@ -21,6 +21,17 @@
 // and the primitive map's partials to U and gamma.  HLLC branches and the
 // limiter are differentiated on the side the forward took.
 //
+// Precision.  The FP64 form is FP64 throughout.  The mixed form keeps the
+// primal step (face states, HLLC fluxes, states) in FP64 and stores the
+// slopes in FP32 (computed in FP32 from FP64 neighbour differences); its
+// reverse sweep evaluates the slopes' partials, the face states, the HLLC
+// reverse and the face cotangents in FP32, with the adjoint states, their
+// sums, the primitive map and gamma in FP64.  The primal stays FP64 because
+// its rounding noise reaches the gradient through the limiter's partials
+// (FP32 fluxes: gradient 1.6e-5 from the FP64 one in L2 on the 1024^2,
+// 100-step problem; FP64 reverse arithmetic alone left that unchanged);
+// the reverse's own FP32 arithmetic costs 1e-6.
+//
 // Checkpoints: U is kept every `checkpoint_every` steps during the forward;
 // the reverse sweep recomputes each segment's U^n and U* from its checkpoint
 // and walks it backwards, so memory grows with steps / checkpoint_every plus
@@ -192,10 +203,33 @@ __global__ void __launch_bounds__(BLOCK, ZG_ADJ_FU_MINB) k_flux_update(Grid g, C
         const bool yface = s >= 2, high = (s & 1) == 1;
         const int lo = high ? ic : nb[s], hi = high ? nb[s] : ic;
         const double half_h = 0.5 * (yface ? g.hy : g.hx), A = yface ? g.hx : g.hy;
-        S L[4], R[4], Fl[4], F[4];
-        face_states<S>(W, yface ? gy : gx, lo, hi, S(half_h), yface, L, R);
-        hllc<S>(L, R, S(gamma), Fl);
-        flux_global<S>(Fl, yface, F);
+        // face states and HLLC in FP64 in both forms (the slopes are FP32 in
+        // the mixed form): FP32 fluxes carry rounding errors of ~1e-7 of the
+        // flux, ~1e-4 of the flux difference across a cell of a smooth
+        // field, and the limiter's partials, which depend on neighbour
+        // differences, carry that noise of the trajectory into the gradient
+        double L[4], R[4], Fl[4], F[4];
+        {
+            const CF4T<S> &G = yface ? gy : gx;
+            double a_[4], b_[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                a_[k] = W.f[k][lo] + (double)G.f[k][lo] * half_h;
+                b_[k] = W.f[k][hi] - (double)G.f[k][hi] * half_h;
+            }
+            if (!yface) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    L[k] = a_[k];
+                    R[k] = b_[k];
+                }
+            } else {
+                L[0] = a_[0]; L[1] = a_[2]; L[2] = -a_[1]; L[3] = a_[3];
+                R[0] = b_[0]; R[1] = b_[2]; R[2] = -b_[1]; R[3] = b_[3];
+            }
+        }
+        hllc<double>(L, R, gamma, Fl);
+        flux_global<double>(Fl, yface, F);
         const double sgn = high ? A : -A;  // outward flux of this cell
 #pragma unroll
         for (int k = 0; k < 4; ++k) sum[k] += sgn * (double)F[k];
@@ -364,12 +398,12 @@ __device__ __forceinline__ void slope_terms(double wm, double w0, double wp, S i
 
 template <class S>
 __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
-    Grid g, CF4 X, CF4 W, double gamma, double eps, const S *fbx, const S *fby, CF4 base, double base_coef,
-    CF4 add, F4 out, double *gacc) {
-    // contributions of tile positions to their neighbours: x (i) rows -1..VI,
-    // y (j) columns -1..VJ
-    __shared__ double sx_lo[VI + 2][VJ], sx_hi[VI + 2][VJ];
-    __shared__ double sy_lo[VI][VJ + 2], sy_hi[VI][VJ + 2];
+    Grid g, CF4 W, double gamma, double eps, const S *fbx, const S *fby, CF4 base, double base_coef, CF4 add,
+    F4 out, double *gacc) {
+    // contributions of tile positions to their neighbours, for two fields at
+    // a time: x (i) rows -1..VI, y (j) columns -1..VJ
+    __shared__ double sx_lo[2][VI + 2][VJ], sx_hi[2][VI + 2][VJ];
+    __shared__ double sy_lo[2][VI][VJ + 2], sy_hi[2][VI][VJ + 2];
     __shared__ double red[VJ * VI / 32];
     const int tj = threadIdx.x, ti = threadIdx.y, tid = ti * VJ + tj;
     const int i0 = blockIdx.y * VI, j0 = blockIdx.x * VJ;
@@ -402,56 +436,60 @@ __global__ void __launch_bounds__(VJ *VI, ZG_ADJ_VT_MINB) k_vjp_cells_tiled(
         hm = ym(g, hc);
         hp = yp(g, hc);
     }
-    double wt[4];
-#pragma unroll 1
-    for (int k = 0; k < 4; ++k) {
-        const S *fl = fbx + k * n, *fh = fbx + (4 + k) * n, *gl = fby + k * n, *gh = fby + (4 + k) * n;
-        const double *w = W.f[k];
-        // own position: slope cotangents and partials on both axes
-        const S xl_c = fl[c.ic], xh_l = fh[cl.ic], yl_c = gl[c.ic], yh_b = gh[cb.ic];
-        const double w_c = w[c.ic];
-        double ox, oy, lo, hi;
-        slope_terms<S>(w[cl.ic], w_c, w[cr.ic], i2x, se, hx2 * (xl_c - xh_l), lo, ox, hi);
-        sx_lo[ti + 1][tj] = lo;
-        sx_hi[ti + 1][tj] = hi;
-        slope_terms<S>(w[cb.ic], w_c, w[ct.ic], i2y, se, hy2 * (yl_c - yh_b), lo, oy, hi);
-        sy_lo[ti][tj + 1] = lo;
-        sy_hi[ti][tj + 1] = hi;
-        if (h_axis == 0) {
-            const S gb = hx2 * (fl[hc.ic] - fh[hm.ic]);
-            double o;
-            slope_terms<S>(w[hm.ic], w[hc.ic], w[hp.ic], i2x, se, gb, lo, o, hi);
-            if (h_side == 0) sx_hi[0][h_pos] = hi;
-            else sx_lo[VI + 1][h_pos] = lo;
-        } else if (h_axis == 1) {
-            const S gb = hy2 * (gl[hc.ic] - gh[hm.ic]);
-            double o;
-            slope_terms<S>(w[hm.ic], w[hc.ic], w[hp.ic], i2y, se, gb, lo, o, hi);
-            if (h_side == 0) sy_hi[h_pos][0] = hi;
-            else sy_lo[h_pos][VJ + 1] = lo;
+    // two fields per pair of barriers: their loads are in flight together
+    double wt[4], wc[4];
+#pragma unroll
+    for (int k0 = 0; k0 < 4; k0 += 2) {
+        double part[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int k = k0 + q;
+            const S *fl = fbx + k * n, *fh = fbx + (4 + k) * n, *gl = fby + k * n, *gh = fby + (4 + k) * n;
+            const double *w = W.f[k];
+            // own position: slope cotangents and partials on both axes
+            const S xl_c = fl[c.ic], xh_l = fh[cl.ic], yl_c = gl[c.ic], yh_b = gh[cb.ic];
+            const double w_c = w[c.ic];
+            wc[k] = w_c;
+            double ox, oy, lo, hi;
+            slope_terms<S>(w[cl.ic], w_c, w[cr.ic], i2x, se, hx2 * (xl_c - xh_l), lo, ox, hi);
+            sx_lo[q][ti + 1][tj] = lo;
+            sx_hi[q][ti + 1][tj] = hi;
+            slope_terms<S>(w[cb.ic], w_c, w[ct.ic], i2y, se, hy2 * (yl_c - yh_b), lo, oy, hi);
+            sy_lo[q][ti][tj + 1] = lo;
+            sy_hi[q][ti][tj + 1] = hi;
+            part[q] = (double)xl_c + (double)xh_l + (double)yl_c + (double)yh_b + ox + oy;
+            if (h_axis == 0) {
+                const S gb = hx2 * (fl[hc.ic] - fh[hm.ic]);
+                double o;
+                slope_terms<S>(w[hm.ic], w[hc.ic], w[hp.ic], i2x, se, gb, lo, o, hi);
+                if (h_side == 0) sx_hi[q][0][h_pos] = hi;
+                else sx_lo[q][VI + 1][h_pos] = lo;
+            } else if (h_axis == 1) {
+                const S gb = hy2 * (gl[hc.ic] - gh[hm.ic]);
+                double o;
+                slope_terms<S>(w[hm.ic], w[hc.ic], w[hp.ic], i2y, se, gb, lo, o, hi);
+                if (h_side == 0) sy_hi[q][h_pos][0] = hi;
+                else sy_lo[q][h_pos][VJ + 1] = lo;
+            }
         }
         __syncthreads();
-        double acc = (double)xl_c + (double)xh_l + (double)yl_c + (double)yh_b;
-        acc += sx_hi[ti][tj];      // the left cell's slope (this cell is its high neighbour)
-        acc += ox;                 // own slope
-        acc += sx_lo[ti + 2][tj];  // the right cell's slope
-        acc += sy_hi[ti][tj];
-        acc += oy;
-        acc += sy_lo[ti][tj + 2];
-        wt[k] = acc;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)  // the low neighbours' slopes (this cell is their high neighbour), the high ones'
+            wt[k0 + q] = part[q] + sx_hi[q][ti][tj] + sx_lo[q][ti + 2][tj] + sy_hi[q][ti][tj] + sy_lo[q][ti][tj + 2];
         __syncthreads();
     }
     double gpart = 0.0;
     if (live) {
         const int ic = c.ic;
-        const double rho = X.f[0][ic], mx = X.f[1][ic], my = X.f[2][ic], E = X.f[3][ic];
-        const double ir = 1.0 / rho, u = mx * ir, v = my * ir, gm1 = gamma - 1.0;
+        // the primitive map's partials at the stage's primitive state
+        // (rho, u, v, p): E - rho |v|^2 / 2 = p / (gamma - 1)
+        const double ir = 1.0 / wc[0], u = wc[1], v = wc[2], gm1 = gamma - 1.0;
         double ub[4];
         ub[0] = wt[0] - wt[1] * u * ir - wt[2] * v * ir + wt[3] * gm1 * 0.5 * (u * u + v * v);
         ub[1] = wt[1] * ir - wt[3] * gm1 * u;
         ub[2] = wt[2] * ir - wt[3] * gm1 * v;
         ub[3] = wt[3] * gm1;
-        gpart = wt[3] * (E - 0.5 * ((mx * mx + my * my) * ir));
+        gpart = wt[3] * (wc[3] / gm1);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             double vv = ub[k];
@@ -644,23 +682,23 @@ void recompute(zg_adj *a, cudaStream_t st, const zg_adj_params &p, int sg, int l
 }
 
 // out = base_coef * base + add + L'(X)^T (coef * mu), with X's primitive
-// states and slopes in wg
+// states and slopes in wg (X itself is not read: the primitive map's partials
+// are taken at its primitive state)
 template <class S>
-void vjp_t(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F4 &mu, double coef, const F4 &base,
+void vjp_t(zg_adj *a, const zg_adj_params &p, const WG &wg, const F4 &mu, double coef, const F4 &base,
            double base_coef, const CF4 &add, const F4 &out, double *gacc) {
     unsigned nb = nblocks(a);
     S *fbx = reinterpret_cast<S *>(a->fbx), *fby = reinterpret_cast<S *>(a->fby);
     k_vjp_faces<S><<<nb, BLOCK, 0, a->stream>>>(a->g, cf(wg.W), cas<S>(wg.gx), cas<S>(wg.gy), p.gamma, cf(mu),
                                                 coef, fbx, fby, gacc);
-    k_vjp_cells_tiled<S><<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(X), cf(wg.W), p.gamma,
-                                                                     p.limiter_eps, fbx, fby, cf(base), base_coef,
-                                                                     add, out, gacc);
+    k_vjp_cells_tiled<S><<<vtiles(a), dim3(VJ, VI), 0, a->stream>>>(a->g, cf(wg.W), p.gamma, p.limiter_eps, fbx,
+                                                                     fby, cf(base), base_coef, add, out, gacc);
     a->launches += 2;
 }
-void vjp(zg_adj *a, const zg_adj_params &p, const F4 &X, const WG &wg, const F4 &mu, double coef, const F4 &base,
+void vjp(zg_adj *a, const zg_adj_params &p, const WG &wg, const F4 &mu, double coef, const F4 &base,
          double base_coef, const CF4 &add, const F4 &out, double *gacc) {
-    if (p.precision == ZG_MIXED) vjp_t<float>(a, p, X, wg, mu, coef, base, base_coef, add, out, gacc);
-    else vjp_t<double>(a, p, X, wg, mu, coef, base, base_coef, add, out, gacc);
+    if (p.precision == ZG_MIXED) vjp_t<float>(a, p, wg, mu, coef, base, base_coef, add, out, gacc);
+    else vjp_t<double>(a, p, wg, mu, coef, base, base_coef, add, out, gacc);
 }
 
 int check_params(zg_adj *a, const zg_adj_params *p) {
@@ -876,9 +914,9 @@ int zg_adj_gradient(zg_adj *a, const zg_adj_params *p, const double *rho, const 
         }
         for (int t = len - 1; t >= 0; --t) {
             // stage B: lambda* = 1/2 lambda^{n+1} + L'(U*)^T (dt/2 lambda^{n+1})
-            vjp(a, *p, a->segstar[b][t], seg_stage(a, b, t, 1), lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
+            vjp(a, *p, seg_stage(a, b, t, 1), lam, 0.5 * p->dt, lam, 0.5, kNull, a->lamS, gacc);
             // stage A: lambda^n = 1/2 lambda^{n+1} + lambda* + L'(U^n)^T (dt lambda*)
-            vjp(a, *p, a->seg[b][t], seg_stage(a, b, t, 0), a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
+            vjp(a, *p, seg_stage(a, b, t, 0), a->lamS, p->dt, lam, 0.5, cf(a->lamS), lam_prev, gacc);
             std::swap(lam, lam_prev);
         }
         cudaEventRecord(a->ev_rev, a->stream);
