@@ -377,6 +377,7 @@ AMR_CAPACITY = 8 << 20  # device room for cells (live + those held during a refi
 AMR_WARM_STEPS = 7000
 AMR_TIMED_STEPS = 400  # steps 7000 to 7400
 AMR_EVERY = 10         # set_flags + refine every AMR_EVERY steps
+AMR_SPLIT_STEPS = 100  # steps after the timed window that give the per-kernel split
 AMR_B_ALG = 160 + 36   # bytes per cell-update: the FP64 two-stage step plus the slot-mesh neighbour indices
 AMR_CELL_BYTES = 600   # bytes of one cell's AmrCells arrays (63 doubles, 22 ints, 16 bytes)
 AMR_KERNELS = "fast"   # kernel family of the AMR step: "fast" (slot FAST) or "parity" (bit-exact)
@@ -477,7 +478,6 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
             _amr_flags(solver, mesh, criterion)
             mesh.refine()
     torch.cuda.synchronize(dev)
-    lib.zg_set_timing(mesh.ctx, 1)
     n0 = mesh.launch_count()
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     e0, e1 = ev(), ev()
@@ -501,6 +501,14 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
     ms = e0.elapsed_time(e1)
     adapt_ms = [a.elapsed_time(b) for a, b in adapt_ev]
     launches = mesh.launch_count() - n0
+    # the per-kernel split from the AMR_SPLIT_STEPS steps after the window,
+    # with an event pair around every launch
+    lib.zg_set_timing(mesh.ctx, 1)
+    for s in range(AMR_SPLIT_STEPS):
+        solver.update(mesh)
+        if (s + 1) % AMR_EVERY == 0:
+            _amr_flags(solver, mesh, criterion)
+            mesh.refine()
     kms = (C.c_double * len(KERNEL_KINDS))()
     kcount = (C.c_longlong * len(KERNEL_KINDS))()
     lib.zg_kernel_times(mesh.ctx, kms, kcount)
@@ -537,7 +545,9 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
                              "(all cell and face arrays read once, new arrays written once)",
         "algorithmic_bytes_per_cell_update": AMR_B_ALG,
         "step_achieved_GBs": AMR_B_ALG * updates / (step_ms / 1e3) / 1e9,
-        "gpu_launches": int(launches), "kernels": kernels, "final": final,
+        "gpu_launches": int(launches), "kernels": kernels,
+        "kernels_window": f"the {AMR_SPLIT_STEPS} steps after the timed window, with per-launch events",
+        "final": final,
     }
     if want_cpu:
         out["cpu_baseline"] = amr_cpu_reference()

@@ -24,6 +24,10 @@
 
 using namespace zg;
 
+// state_mode of a state held in the Morton order of the FAST step on an
+// adaptive rectangle (FP64 primitive, in the order buffers)
+constexpr int STATE_ORDERED = 100;
+
 struct zg_ctx {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -71,6 +75,7 @@ struct zg_ctx {
     PrimPtr oz{}, ozhalf{}, oznext{};
     int *ow[2] = {};
     long long ord_version = -1;
+    bool ord_waits = false;  // ow[0] holds the current isolation counters (predictor-corrector)
 
     // solver
     bool configured = false;
@@ -91,7 +96,7 @@ struct zg_ctx {
     unsigned long long *d_slots = nullptr;  // three rotating CFL accumulators
     int slot_k = 0;
     bool cfl_valid = false;
-    int state_mode = ZG_FP64;  // representation of the current state
+    int state_mode = ZG_FP64;  // representation of the current state (zg_precision, or STATE_ORDERED)
     double *d_mq = nullptr;    // MIXED conserved state, two sets of 4 fields
     float *d_mf = nullptr;     // MIXED FP32 fields: two state mirrors (5), stage (5), gradients (8)
     double *mq[2][4] = {};
@@ -219,6 +224,7 @@ void free_mesh(zg_ctx *c) {
     c->d_ord = nullptr;
     c->ord = slotfast::OrderBuffers{};
     c->ord_version = -1;
+    if (c->state_mode == STATE_ORDERED) c->state_mode = ZG_FP64;  // the state goes with the mesh
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
     c->d_slot = nullptr;
@@ -310,9 +316,25 @@ tiled::Fields<float> mixed_fields(const zg_ctx *c) {
     return f;
 }
 
+// Bring a state held in the Morton order of the FAST adaptive step back to
+// the mesh's own order (FP64 primitive in c->z, counters in the current
+// counter buffer); a no-op in the other representations.
+int leave_order(zg_ctx *c) {
+    if (c->state_mode != STATE_ORDERED) return ZG_OK;
+    int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
+    slotfast::scatter_state(c->ord.perm, c->n, c->oz, c->z, c->ord_waits ? c->ow[0] : nullptr, wait,
+                            (void *)c->stream);
+    ++c->launches;
+    c->state_mode = ZG_FP64;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "state order");
+}
+
 // Move the current state into the representation `mode` (FP64 primitive or
 // MIXED) on the device.
 int convert_state(zg_ctx *c, int mode) {
+    int rc = leave_order(c);
+    if (rc != ZG_OK) return rc;
     if (mode == c->state_mode) return ZG_OK;
     if (mode == ZG_MIXED) {
         tiled::Fields<float> f = mixed_fields(c);
@@ -333,6 +355,8 @@ int convert_state(zg_ctx *c, int mode) {
 // changing the representation the steps use (MIXED keeps its FP64 conserved
 // variables, so no conversion round trip enters the solution).
 int materialize_prim(zg_ctx *c) {
+    int rc = leave_order(c);
+    if (rc != ZG_OK) return rc;
     if (c->state_mode != ZG_MIXED) return ZG_OK;
     mixed::launch_to_prim(c->n, mixed_fields(c), c->eos, c->z, (void *)c->stream);
     c->launches += 1;
@@ -599,25 +623,37 @@ int ensure_order(zg_ctx *c) {
 
 // The FAST step on an adaptive rectangle: the gather-form kernels of the
 // parity step over derived face geometry, with fused multiply-adds, run on
-// the cells in Morton order (the state gathered into it and scattered back;
-// the same results as in the mesh's own order).
+// the cells in Morton order.  The state is gathered into that order by the
+// first step after it was in the mesh's order and stays there between steps
+// (state_mode STATE_ORDERED); every other entry point that reads or writes
+// the state, or changes the mesh, first scatters it back (leave_order).  The
+// results are the same as in the mesh's own order.
 int enqueue_slot_fast_step(zg_ctx *c) {
     void *st = (void *)c->stream;
     int rc = ensure_order(c);
     if (rc != ZG_OK) return rc;
-    if (c->ord_version != c->mesh_version) {
-        const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
-        if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
-            return cuda_fail(c, cudaGetLastError(), "cell order");
-        c->launches += 4;
-        c->ord_version = c->mesh_version;
-    }
     const bool pc = c->par.accuracy == 2 && c->par.scheme == ZG_SCHEME_PREDICTOR_CORRECTOR;
+    if (c->state_mode == STATE_ORDERED && (c->ord_version != c->mesh_version || c->ord_waits != pc)) {
+        rc = leave_order(c);  // not reached through the API: the mesh and the scheme change after leave_order
+        if (rc != ZG_OK) return rc;
+    }
+    if (c->state_mode != STATE_ORDERED) {
+        rc = convert_state(c, ZG_FP64);
+        if (rc != ZG_OK) return rc;
+        if (c->ord_version != c->mesh_version) {
+            const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
+            if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
+                return cuda_fail(c, cudaGetLastError(), "cell order");
+            c->launches += 4;
+            c->ord_version = c->mesh_version;
+        }
+        int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
+        slotfast::gather_state(c->ord.perm, c->n, c->z, c->oz, pc ? wait : nullptr, c->ow[0], st);
+        ++c->launches;
+        c->ord_waits = pc;
+        c->state_mode = STATE_ORDERED;
+    }
     SmfArgs a = make_args(c);
-    const PrimPtr znext_mesh = c->znext;
-    int *const wout_mesh = a.wait_out;
-    slotfast::gather_state(c->ord.perm, c->n, c->z, c->oz, pc ? a.wait_in : nullptr, c->ow[0], st);
-    ++c->launches;
     a.smesh = c->ord_mesh;
     a.z = c->oz;
     a.zhalf = c->ozhalf;
@@ -631,18 +667,16 @@ int enqueue_slot_fast_step(zg_ctx *c) {
         timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
         timed(c, ZG_K_STAGE1, [&] { slotfast::launch_stage1(a, st); });
         timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2(a, st); });
-        c->wait_cur = 1 - c->wait_cur;
+        std::swap(c->ow[0], c->ow[1]);
     } else {
         timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
         timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun(a, a.z, a.zhalf, false, st); });
         timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.zhalf, st); });
         timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun(a, a.zhalf, a.znext, true, st); });
     }
-    slotfast::scatter_state(c->ord.perm, c->n, c->oznext, znext_mesh, pc ? c->ow[1] : nullptr, wout_mesh, st);
-    ++c->launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
-    std::swap(c->z, c->znext);
+    std::swap(c->oz, c->oznext);
     c->cfl_valid = false;
     c->stepped = true;
     return ZG_OK;
@@ -1004,6 +1038,8 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     if (!(p->gamma > 1.0)) return fail(c, ZG_ERR_ARG, "zg_smf_configure: gamma must exceed 1");
 
     DeviceGuard g(c->device);
+    int rc = leave_order(c);  // the new parameters may take the step off the ordered path
+    if (rc != ZG_OK) return rc;
     c->par = *p;
     c->par.accuracy = std::min(std::max(1, p->accuracy), 2);        // sm_fluid.cpp:41-43
     c->par.CFL = std::max(0.0, std::min(p->CFL, 1.0));               // sm_fluid.cpp:37-39
@@ -1081,6 +1117,8 @@ int zg_state_upload(zg_ctx *c, const double *rho, const double *vx, const double
     if (!c || !rho || !vx || !vy || !p || !e) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_state_upload: solver not configured");
     DeviceGuard g(c->device);
+    int rc = leave_order(c);  // the counters held in the cell order come back with it
+    if (rc != ZG_OK) return rc;
     size_t bytes = (size_t)c->n * sizeof(double);
     const double *src[5] = {rho, vx, vy, p, e};
     double *dst[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
@@ -1111,6 +1149,8 @@ int zg_wait_upload(zg_ctx *c, const int *wait) {
     if (!c || !wait) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_wait_upload: solver not configured");
     DeviceGuard g(c->device);
+    int rc = leave_order(c);
+    if (rc != ZG_OK) return rc;
     ZG_CUDA(c, cudaMemcpyAsync(c->d_wait + (size_t)c->wait_cur * c->cap, wait, (size_t)c->n * sizeof(int),
                                cudaMemcpyHostToDevice, c->stream));
     return ZG_OK;
@@ -1120,6 +1160,8 @@ int zg_wait_download(zg_ctx *c, int *wait) {
     if (!c || !wait) return ZG_ERR_ARG;
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_wait_download: solver not configured");
     DeviceGuard g(c->device);
+    int rc = leave_order(c);
+    if (rc != ZG_OK) return rc;
     ZG_CUDA(c, cudaMemcpyAsync(wait, c->d_wait + (size_t)c->wait_cur * c->cap, (size_t)c->n * sizeof(int),
                                cudaMemcpyDeviceToHost, c->stream));
     ZG_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1183,6 +1225,8 @@ int zg_state_rows(zg_ctx *c, int row0, int nrows, double *fields, int *wait, int
     if (c->par.precision != ZG_FP64) return fail(c, ZG_ERR_STATE, "zg_state_rows: the FP64 forms");
     if (row0 < 0 || row0 + nrows > c->nx) return fail(c, ZG_ERR_ARG, "zg_state_rows: rows out of range");
     DeviceGuard g(c->device);
+    int rc = leave_order(c);
+    if (rc != ZG_OK) return rc;
     const size_t off = (size_t)row0 * c->ny, cnt = (size_t)nrows * c->ny;
     double *fld[5] = {c->z.r, c->z.u, c->z.v, c->z.p, c->z.e};
     int *w = c->d_wait + (size_t)c->wait_cur * c->cap;
@@ -1209,6 +1253,8 @@ int zg_smf_cfl_min(zg_ctx *c, double *dmin) {
     if (!c->configured) return fail(c, ZG_ERR_STATE, "zg_smf_cfl_min: solver not configured");
     if (c->par.precision != ZG_FP64) return fail(c, ZG_ERR_STATE, "zg_smf_cfl_min: the FP64 forms");
     DeviceGuard g(c->device);
+    int rc = leave_order(c);
+    if (rc != ZG_OK) return rc;
     void *st = (void *)c->stream;
     if (c->par.kernels != ZG_KERNELS_PARITY && !c->slots) {
         // the FAST kernels' own CFL pass (the one their step runs after an upload)
