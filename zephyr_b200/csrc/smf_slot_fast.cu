@@ -1,8 +1,9 @@
 // smf_slot_fast.cu -- the FAST form of the step on an adaptive rectangle: the
-// gather-form kernels of smf_struct.cuh over SlotFastAcc (face geometry from
-// the cell's centre and level instead of five stored arrays per slot),
-// compiled with fused multiply-adds and register caps.  Results match the
-// parity form to rounding (not bit for bit).
+// kernels of smf_struct.cuh over SlotFastAcc (face geometry from the cell's
+// centre and level instead of five stored arrays per slot), compiled with
+// fused multiply-adds and register caps, with the corrector and the Heun
+// stages face-once.  Results match the parity form to rounding (not bit for
+// bit).
 #include <cuda_runtime.h>
 
 #include "smf_struct.cuh"
@@ -42,16 +43,6 @@ template <int FX>
 static void flux1_fx(const SmfArgs &a, void *stream) {
     k_flux1<SlotFastAcc, BLOCK, S2M, FX><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
-template <int FX>
-static void stage2_fx(const SmfArgs &a, void *stream) {
-    k_stage2<SlotFastAcc, BLOCK, S2M, FX><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
-}
-template <int FX>
-static void heun_fx(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream) {
-    cudaStream_t st = (cudaStream_t)stream;
-    if (final) k_heun<SlotFastAcc, BLOCK, true, S2M, FX><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
-    else k_heun<SlotFastAcc, BLOCK, false, S2M, FX><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout);
-}
 
 void launch_flux1(const SmfArgs &a, void *stream) { ZG_FLUX_FAMILY(flux1_fx, a, stream); }
 void launch_grad(const SmfArgs &a, PrimPtr z, void *stream) {
@@ -60,9 +51,112 @@ void launch_grad(const SmfArgs &a, PrimPtr z, void *stream) {
 void launch_stage1(const SmfArgs &a, void *stream) {
     k_stage1<SlotFastAcc, BLOCK, S1M><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
 }
-void launch_stage2(const SmfArgs &a, void *stream) { ZG_FLUX_FAMILY(stage2_fx, a, stream); }
-void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream) {
-    ZG_FLUX_FAMILY(heun_fx, a, zin, zout, final, stream);
+
+// --- face-once corrector / Heun stages --------------------------------------
+// One thread per face of the list (computes_face in smf_struct.cuh decides
+// which cell evaluates a face): the corrector's face flux into the slot.
+template <int FX, bool HEUN>
+__global__ void __launch_bounds__(BLOCK, S2M) k_faces_once(SmfArgs a, PrimPtr zin, FaceFlux ff) {
+    int t = blockIdx.x * BLOCK + threadIdx.x;
+    if (t >= ff.nfaces) return;
+    const int f = ff.list[t], ic = f >> 3, s = f & 7;
+    SlotFastAcc c(a, ic);
+    const FaceG g = c.face(s);
+    const Prim zc = load_prim(zin, ic);
+    const int wc = HEUN ? 0 : a.wait_in[ic];
+    Cons lf = corrector_face<FX>(a, zin, HEUN ? nullptr : a.wait_in, c, s, g, zc, c.cx(), c.cy(), wc);
+    ff.r[f] = lf.r;
+    ff.mu[f] = lf.mu;
+    ff.mv[f] = lf.mv;
+    ff.E[f] = lf.E;
+}
+
+// the face fluxes of cell ic summed in slot order
+__device__ __forceinline__ Cons sum_faces(const SlotMesh &m, int ic, const FaceFlux &ff) {
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int f = 8 * ic + s, flag = m.fb[f];
+        if (flag == BC_UNDEFINED) continue;
+        const int nb = m.fn[f];
+        if (computes_face(m, ic, s, flag, nb)) {
+            F.r += ff.r[f];
+            F.mu += ff.mu[f];
+            F.mv += ff.mv[f];
+            F.E += ff.E[f];
+        } else {
+            const int o = 8 * nb + ((s & 3) ^ 1);
+            F.r -= ff.r[o];
+            F.mu -= ff.mu[o];
+            F.mv -= ff.mv[o];
+            F.E -= ff.E[o];
+        }
+    }
+    return F;
+}
+
+// k_stage2's update (sm_fluid.cpp:342-366) from the summed face fluxes
+__global__ void __launch_bounds__(BLOCK) k_stage2_sum(SmfArgs a, FaceFlux ff) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    const double dt = finalize_dt(a);
+    const Prim zc = load_prim(a.z, ic);
+    const int wc = a.wait_in[ic];
+    Cons q = q_from_p(zc);
+    const Cons F = sum_faces(a.smesh, ic, ff);
+    update(q, dt / a.smesh.vol[ic], F);
+    Prim n = p_from_q(q, a.eos);
+    int wn = wc;
+    if (is_bad(n, a.eos)) {
+        n = zc;
+        wn = 3;
+    } else if (wn > 0) {
+        --wn;
+    }
+    store_prim(a.znext, ic, n);
+    a.wait_out[ic] = wn;
+}
+
+// k_heun's update from the summed face fluxes
+template <bool FINAL>
+__global__ void __launch_bounds__(BLOCK) k_heun_sum(SmfArgs a, PrimPtr zin, PrimPtr zout, FaceFlux ff) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    const double dt = finalize_dt(a);
+    Cons q = q_from_p(load_prim(zin, ic));
+    const Cons F = sum_faces(a.smesh, ic, ff);
+    update(q, dt / a.smesh.vol[ic], F);
+    if (FINAL) {
+        Cons q0 = q_from_p(load_prim(a.z, ic));
+        q.r = 0.5 * (q0.r + q.r);
+        q.mu = 0.5 * (q0.mu + q.mu);
+        q.mv = 0.5 * (q0.mv + q.mv);
+        q.E = 0.5 * (q0.E + q.E);
+    }
+    store_prim(zout, ic, p_from_q(q, a.eos));
+}
+
+template <int FX>
+static void faces_fx(const SmfArgs &a, PrimPtr zin, FaceFlux ff, bool heun, void *stream) {
+    if (ff.nfaces <= 0) return;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned nb = (unsigned)((ff.nfaces + BLOCK - 1) / BLOCK);
+    if (heun) k_faces_once<FX, true><<<nb, BLOCK, 0, st>>>(a, zin, ff);
+    else k_faces_once<FX, false><<<nb, BLOCK, 0, st>>>(a, zin, ff);
+}
+void launch_stage2_faces(const SmfArgs &a, FaceFlux ff, void *stream) {
+    ZG_FLUX_FAMILY(faces_fx, a, a.zhalf, ff, false, stream);
+}
+void launch_stage2_sum(const SmfArgs &a, FaceFlux ff, void *stream) {
+    k_stage2_sum<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, ff);
+}
+void launch_heun_faces(const SmfArgs &a, PrimPtr zin, FaceFlux ff, void *stream) {
+    ZG_FLUX_FAMILY(faces_fx, a, zin, ff, true, stream);
+}
+void launch_heun_sum(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, FaceFlux ff, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (final) k_heun_sum<true><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout, ff);
+    else k_heun_sum<false><<<blocks(a), BLOCK, 0, st>>>(a, zin, zout, ff);
 }
 
 // Refinement flags by the density-gradient criterion |grad rho| h / rho (h =

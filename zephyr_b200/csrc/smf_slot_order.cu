@@ -13,7 +13,9 @@
 
 #include <cub/cub.cuh>
 
-#include "smf_types.h"
+#include <algorithm>
+
+#include "smf_struct.cuh"
 
 namespace zg {
 namespace slotfast {
@@ -87,11 +89,39 @@ __global__ void k_scatter(const int *perm, int n, PrimPtr src, PrimPtr dst, cons
     if (wsrc) wdst[ic] = wsrc[p];
 }
 
+// the face list of the face-once kernels: the slots whose face each cell
+// evaluates (computes_face), counted, offset by an exclusive scan, listed
+__global__ void k_own_count(SlotMesh m, int n, int *cnt) {
+    int p = blockIdx.x * OBLOCK + threadIdx.x;
+    if (p > n) return;
+    int k = 0;
+    if (p < n) {
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            const int flag = m.fb[8 * p + s];
+            if (flag != BC_UNDEFINED && computes_face(m, p, s, flag, m.fn[8 * p + s])) ++k;
+        }
+    }
+    cnt[p] = k;  // cnt[n] = 0: the scan's last entry is the total
+}
+
+__global__ void k_own_list(SlotMesh m, int n, const int *off, int *list) {
+    int p = blockIdx.x * OBLOCK + threadIdx.x;
+    if (p >= n) return;
+    int o = off[p];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int flag = m.fb[8 * p + s];
+        if (flag != BC_UNDEFINED && computes_face(m, p, s, flag, m.fn[8 * p + s])) list[o++] = 8 * p + s;
+    }
+}
+
 size_t order_scratch_bytes(int cap) {
-    size_t bytes = 0;
+    size_t bytes = 0, scan = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr,
                                     (unsigned long long *)nullptr, (const int *)nullptr, (int *)nullptr, cap, 0, 42);
-    return bytes;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan, (const int *)nullptr, (int *)nullptr, cap + 1);
+    return std::max(bytes, scan);
 }
 
 int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, OrderBuffers &b,
@@ -117,6 +147,14 @@ int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, doubl
     out.fn = b.fn;
     // the stored per-slot geometry is not read by the FAST kernels
     out.fnx = out.fny = out.fcx = out.fcy = out.fa = nullptr;
+    k_own_count<<<oblocks(n + 1), OBLOCK, 0, st>>>(out, n, b.fcnt);
+    size_t scan = b.tmp_bytes;
+    if (cub::DeviceScan::ExclusiveSum(b.tmp, scan, b.fcnt, b.foff, n + 1, st) != cudaSuccess) return -1;
+    k_own_list<<<oblocks(n), OBLOCK, 0, st>>>(out, n, b.foff, b.flist);
+    // the face count sizes the face kernels' grids (one copy per mesh change)
+    if (cudaMemcpyAsync(&b.nfaces, b.foff + n, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return -1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -194,6 +194,20 @@ struct SlotFastAcc {
     }
 };
 
+// The face-once form's choice of the cell that evaluates a face (slot s of
+// cell ic, flag, neighbour nb): a boundary face its cell; a face between a
+// coarse and a fine cell the fine one (its full face is the coarse cell's
+// half face, with the same centre and area); a face between cells of one
+// level the cell on its low side (the face is that cell's x-high or y-high
+// slot).  The other cell reads the flux from the neighbour's slot of the
+// opposite side, which is a full slot (< 4) in both cases.
+__device__ __forceinline__ bool computes_face(const SlotMesh &m, int ic, int s, int flag, int nb) {
+    if (is_boundary(flag)) return true;
+    const int ln = m.level[nb], lc = m.level[ic];
+    if (ln != lc) return ln < lc;
+    return (s & 1) == 1;
+}
+
 // Centre of the neighbour across slot s, or the mirror of the cell centre in
 // the face (sm_fluid.cpp:211-212; amr_faces.h:197-199 symm_point).
 template <class Acc>

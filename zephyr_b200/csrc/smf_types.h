@@ -76,9 +76,23 @@ void launch_dt(const SmfArgs &a, PrimPtr z, void *stream);
 void launch_flux1(const SmfArgs &a, void *stream);
 void launch_grad(const SmfArgs &a, PrimPtr z, void *stream);
 void launch_stage1(const SmfArgs &a, void *stream);
-void launch_stage2(const SmfArgs &a, void *stream);
-void launch_heun(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, void *stream);
 void launch_grad_flags(const SmfArgs &a, int *flags, double refine, double coarsen, void *stream);
+
+// Face-once form of the corrector and of the Heun stages: each face's flux
+// (times its area, outward from the cell that computes it) is evaluated once,
+// by one of its two cells, into the slot of that cell (8 slots per cell, one
+// array per conserved component), and every cell then sums its slots in slot
+// order, taking a face it does not compute from the neighbour's slot with
+// the opposite sign.
+struct FaceFlux {
+    double *r, *mu, *mv, *E;  // 8 n each
+    const int *list;          // the slots 8 ic + s whose face cell ic computes, in cell order
+    int nfaces;               // entries of `list`
+};
+void launch_stage2_faces(const SmfArgs &a, FaceFlux ff, void *stream);
+void launch_stage2_sum(const SmfArgs &a, FaceFlux ff, void *stream);
+void launch_heun_faces(const SmfArgs &a, PrimPtr zin, FaceFlux ff, void *stream);
+void launch_heun_sum(const SmfArgs &a, PrimPtr zin, PrimPtr zout, bool final, FaceFlux ff, void *stream);
 
 // Morton order of the cells for the FAST step (smf_slot_order.cu): device
 // buffers of `cap` cells (keys 2 cap), cub scratch of tmp_bytes
@@ -90,6 +104,9 @@ struct OrderBuffers {
     size_t tmp_bytes;
     double *cx, *cy, *vol, *inc;
     int *level, *fb, *fn;
+    int *fcnt, *foff;  // faces each cell computes, their exclusive prefix sum (cap + 1 each)
+    int *flist;        // FaceFlux::list (8 cap)
+    int nfaces;
 };
 size_t order_scratch_bytes(int cap);
 // fills b.perm (position -> cell), b.inv and the reordered mesh arrays, and

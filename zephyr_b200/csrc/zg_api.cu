@@ -74,6 +74,7 @@ struct zg_ctx {
     SlotMesh ord_mesh{};
     PrimPtr oz{}, ozhalf{}, oznext{};
     int *ow[2] = {};
+    slotfast::FaceFlux oflux{};  // face-once fluxes, 8 slots per cell
     long long ord_version = -1;
     bool ord_waits = false;  // ow[0] holds the current isolation counters (predictor-corrector)
 
@@ -585,7 +586,8 @@ int ensure_order(zg_ctx *c) {
     const size_t tmp = slotfast::order_scratch_bytes(c->cap);
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t bytes = al(2 * cap * 8) + 3 * al(cap * 4) + al(tmp) + 4 * al(cap * 8) + al(cap * 4) +
-                         2 * al(8 * cap * 4) + 15 * al(cap * 8) + 2 * al(cap * 4);
+                         2 * al(8 * cap * 4) + 15 * al(cap * 8) + 2 * al(cap * 4) + 4 * al(8 * cap * 8) +
+                         2 * al((cap + 1) * 4) + al(8 * cap * 4);
     ZG_CUDA(c, cudaMalloc(&c->d_ord, bytes));
     char *p = static_cast<char *>(c->d_ord);
     auto take = [&p, &al](size_t b) {
@@ -617,13 +619,20 @@ int ensure_order(zg_ctx *c) {
     }
     c->ow[0] = reinterpret_cast<int *>(take(cap * 4));
     c->ow[1] = reinterpret_cast<int *>(take(cap * 4));
+    for (double **f : {&c->oflux.r, &c->oflux.mu, &c->oflux.mv, &c->oflux.E})
+        *f = reinterpret_cast<double *>(take(8 * cap * 8));
+    o.fcnt = reinterpret_cast<int *>(take((cap + 1) * 4));
+    o.foff = reinterpret_cast<int *>(take((cap + 1) * 4));
+    o.flist = reinterpret_cast<int *>(take(8 * cap * 4));
+    o.nfaces = 0;
     c->ord_version = -1;
     return ZG_OK;
 }
 
-// The FAST step on an adaptive rectangle: the gather-form kernels of the
-// parity step over derived face geometry, with fused multiply-adds, run on
-// the cells in Morton order.  The state is gathered into that order by the
+// The FAST step on an adaptive rectangle: the kernels of the parity step
+// over derived face geometry, with fused multiply-adds, the corrector (and
+// the Heun stages) face-once over a face list, run on the cells in Morton
+// order.  The state is gathered into that order by the
 // first step after it was in the mesh's order and stays there between steps
 // (state_mode STATE_ORDERED); every other entry point that reads or writes
 // the state, or changes the mesh, first scatters it back (leave_order).  The
@@ -644,7 +653,7 @@ int enqueue_slot_fast_step(zg_ctx *c) {
             const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
             if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
                 return cuda_fail(c, cudaGetLastError(), "cell order");
-            c->launches += 4;
+            c->launches += 7;
             c->ord_version = c->mesh_version;
         }
         int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
@@ -653,6 +662,8 @@ int enqueue_slot_fast_step(zg_ctx *c) {
         c->ord_waits = pc;
         c->state_mode = STATE_ORDERED;
     }
+    c->oflux.list = c->ord.flist;
+    c->oflux.nfaces = c->ord.nfaces;
     SmfArgs a = make_args(c);
     a.smesh = c->ord_mesh;
     a.z = c->oz;
@@ -666,13 +677,17 @@ int enqueue_slot_fast_step(zg_ctx *c) {
     } else if (pc) {
         timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
         timed(c, ZG_K_STAGE1, [&] { slotfast::launch_stage1(a, st); });
-        timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2(a, st); });
+        // the corrector face-once: the listed faces, then every cell's sum
+        timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2_faces(a, c->oflux, st); });
+        timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2_sum(a, c->oflux, st); });
         std::swap(c->ow[0], c->ow[1]);
     } else {
         timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
-        timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun(a, a.z, a.zhalf, false, st); });
+        timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun_faces(a, a.z, c->oflux, st); });
+        timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun_sum(a, a.z, a.zhalf, false, c->oflux, st); });
         timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.zhalf, st); });
-        timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun(a, a.zhalf, a.znext, true, st); });
+        timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun_faces(a, a.zhalf, c->oflux, st); });
+        timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun_sum(a, a.zhalf, a.znext, true, c->oflux, st); });
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
