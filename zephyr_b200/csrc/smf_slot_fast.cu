@@ -65,31 +65,27 @@ __global__ void __launch_bounds__(BLOCK, S2M) k_faces_once(SmfArgs a, PrimPtr zi
     const Prim zc = load_prim(zin, ic);
     const int wc = HEUN ? 0 : a.wait_in[ic];
     Cons lf = corrector_face<FX>(a, zin, HEUN ? nullptr : a.wait_in, c, s, g, zc, c.cx(), c.cy(), wc);
-    ff.r[f] = lf.r;
-    ff.mu[f] = lf.mu;
-    ff.mv[f] = lf.mv;
-    ff.E[f] = lf.E;
+    ff.f[t] = make_double4(lf.r, lf.mu, lf.mv, lf.E);
 }
 
 // the face fluxes of cell ic summed in slot order
-__device__ __forceinline__ Cons sum_faces(const SlotMesh &m, int ic, const FaceFlux &ff) {
+__device__ __forceinline__ Cons sum_faces(int ic, const FaceFlux &ff) {
     Cons F{0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        const int f = 8 * ic + s, flag = m.fb[f];
-        if (flag == BC_UNDEFINED) continue;
-        const int nb = m.fn[f];
-        if (computes_face(m, ic, s, flag, nb)) {
-            F.r += ff.r[f];
-            F.mu += ff.mu[f];
-            F.mv += ff.mv[f];
-            F.E += ff.E[f];
+        const int x = ff.fidx[8 * ic + s];
+        if (x == FACE_NONE) continue;
+        const double4 v = ff.f[x >= 0 ? x : -x - 1];
+        if (x >= 0) {
+            F.r += v.x;
+            F.mu += v.y;
+            F.mv += v.z;
+            F.E += v.w;
         } else {
-            const int o = 8 * nb + ((s & 3) ^ 1);
-            F.r -= ff.r[o];
-            F.mu -= ff.mu[o];
-            F.mv -= ff.mv[o];
-            F.E -= ff.E[o];
+            F.r -= v.x;
+            F.mu -= v.y;
+            F.mv -= v.z;
+            F.E -= v.w;
         }
     }
     return F;
@@ -103,7 +99,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage2_sum(SmfArgs a, FaceFlux ff) {
     const Prim zc = load_prim(a.z, ic);
     const int wc = a.wait_in[ic];
     Cons q = q_from_p(zc);
-    const Cons F = sum_faces(a.smesh, ic, ff);
+    const Cons F = sum_faces(ic, ff);
     update(q, dt / a.smesh.vol[ic], F);
     Prim n = p_from_q(q, a.eos);
     int wn = wc;
@@ -124,7 +120,7 @@ __global__ void __launch_bounds__(BLOCK) k_heun_sum(SmfArgs a, PrimPtr zin, Prim
     if (ic >= a.smesh.n) return;
     const double dt = finalize_dt(a);
     Cons q = q_from_p(load_prim(zin, ic));
-    const Cons F = sum_faces(a.smesh, ic, ff);
+    const Cons F = sum_faces(ic, ff);
     update(q, dt / a.smesh.vol[ic], F);
     if (FINAL) {
         Cons q0 = q_from_p(load_prim(a.z, ic));

@@ -116,6 +116,37 @@ __global__ void k_own_list(SlotMesh m, int n, const int *off, int *list) {
     }
 }
 
+// position of slot s among the slots cell p computes (its face list entry
+// minus the cell's offset)
+__device__ __forceinline__ int own_rank(const SlotMesh &m, int p, int s) {
+    int k = 0;
+    for (int q = 0; q < s; ++q) {
+        const int flag = m.fb[8 * p + q];
+        if (flag != BC_UNDEFINED && computes_face(m, p, q, flag, m.fn[8 * p + q])) ++k;
+    }
+    return k;
+}
+
+__global__ void k_face_index(SlotMesh m, int n, const int *off, int *fidx) {
+    int p = blockIdx.x * OBLOCK + threadIdx.x;
+    if (p >= n) return;
+    int o = off[p];
+    for (int s = 0; s < 8; ++s) {
+        const int flag = m.fb[8 * p + s];
+        int x = FACE_NONE;
+        if (flag != BC_UNDEFINED) {
+            const int nb = m.fn[8 * p + s];
+            if (computes_face(m, p, s, flag, nb)) {
+                x = o++;
+            } else {
+                const int q = (s & 3) ^ 1;  // the neighbour's full slot of the opposite side
+                x = -(off[nb] + own_rank(m, nb, q)) - 1;
+            }
+        }
+        fidx[8 * p + s] = x;
+    }
+}
+
 size_t order_scratch_bytes(int cap) {
     size_t bytes = 0, scan = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr,
@@ -151,6 +182,7 @@ int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, doubl
     size_t scan = b.tmp_bytes;
     if (cub::DeviceScan::ExclusiveSum(b.tmp, scan, b.fcnt, b.foff, n + 1, st) != cudaSuccess) return -1;
     k_own_list<<<oblocks(n), OBLOCK, 0, st>>>(out, n, b.foff, b.flist);
+    k_face_index<<<oblocks(n), OBLOCK, 0, st>>>(out, n, b.foff, b.fidx);
     // the face count sizes the face kernels' grids (one copy per mesh change)
     if (cudaMemcpyAsync(&b.nfaces, b.foff + n, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)

@@ -85,10 +85,13 @@ void launch_grad_flags(const SmfArgs &a, int *flags, double refine, double coars
 // order, taking a face it does not compute from the neighbour's slot with
 // the opposite sign.
 struct FaceFlux {
-    double *r, *mu, *mv, *E;  // 8 n each
-    const int *list;          // the slots 8 ic + s whose face cell ic computes, in cell order
-    int nfaces;               // entries of `list`
+    double4 *f;        // per face of `list`: (rho, rho u, rho v, rho E) flux times area
+    const int *list;   // the slots 8 ic + s whose face cell ic computes, in cell order
+    const int *fidx;   // per slot 8 ic + s: t >= 0, the face list entry it computes; -(t + 1), the
+                       // neighbour's entry it takes with the opposite sign; FACE_NONE, no face
+    int nfaces;        // entries of `list`
 };
+constexpr int FACE_NONE = -2147483647 - 1;
 void launch_stage2_faces(const SmfArgs &a, FaceFlux ff, void *stream);
 void launch_stage2_sum(const SmfArgs &a, FaceFlux ff, void *stream);
 void launch_heun_faces(const SmfArgs &a, PrimPtr zin, FaceFlux ff, void *stream);
@@ -106,6 +109,7 @@ struct OrderBuffers {
     int *level, *fb, *fn;
     int *fcnt, *foff;  // faces each cell computes, their exclusive prefix sum (cap + 1 each)
     int *flist;        // FaceFlux::list (8 cap)
+    int *fidx;         // FaceFlux::fidx (8 cap)
     int nfaces;
 };
 size_t order_scratch_bytes(int cap);

@@ -587,7 +587,7 @@ int ensure_order(zg_ctx *c) {
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t bytes = al(2 * cap * 8) + 3 * al(cap * 4) + al(tmp) + 4 * al(cap * 8) + al(cap * 4) +
                          2 * al(8 * cap * 4) + 15 * al(cap * 8) + 2 * al(cap * 4) + 4 * al(8 * cap * 8) +
-                         2 * al((cap + 1) * 4) + al(8 * cap * 4);
+                         2 * al((cap + 1) * 4) + 2 * al(8 * cap * 4);
     ZG_CUDA(c, cudaMalloc(&c->d_ord, bytes));
     char *p = static_cast<char *>(c->d_ord);
     auto take = [&p, &al](size_t b) {
@@ -619,11 +619,11 @@ int ensure_order(zg_ctx *c) {
     }
     c->ow[0] = reinterpret_cast<int *>(take(cap * 4));
     c->ow[1] = reinterpret_cast<int *>(take(cap * 4));
-    for (double **f : {&c->oflux.r, &c->oflux.mu, &c->oflux.mv, &c->oflux.E})
-        *f = reinterpret_cast<double *>(take(8 * cap * 8));
+    c->oflux.f = reinterpret_cast<double4 *>(take(4 * 8 * cap * 8));
     o.fcnt = reinterpret_cast<int *>(take((cap + 1) * 4));
     o.foff = reinterpret_cast<int *>(take((cap + 1) * 4));
     o.flist = reinterpret_cast<int *>(take(8 * cap * 4));
+    o.fidx = reinterpret_cast<int *>(take(8 * cap * 4));
     o.nfaces = 0;
     c->ord_version = -1;
     return ZG_OK;
@@ -653,7 +653,7 @@ int enqueue_slot_fast_step(zg_ctx *c) {
             const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
             if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
                 return cuda_fail(c, cudaGetLastError(), "cell order");
-            c->launches += 7;
+            c->launches += 8;
             c->ord_version = c->mesh_version;
         }
         int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
@@ -663,6 +663,7 @@ int enqueue_slot_fast_step(zg_ctx *c) {
         c->state_mode = STATE_ORDERED;
     }
     c->oflux.list = c->ord.flist;
+    c->oflux.fidx = c->ord.fidx;
     c->oflux.nfaces = c->ord.nfaces;
     SmfArgs a = make_args(c);
     a.smesh = c->ord_mesh;
