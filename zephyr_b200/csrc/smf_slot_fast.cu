@@ -15,15 +15,12 @@ constexpr int BLOCK = 128;
 // Minimum resident blocks per SM: register caps chosen by timing the AMR
 // blast (512^2, 3 levels) over a sweep on a B200 (-D overrides)
 #ifndef ZG_SLOT_GRAD_MINB
-#define ZG_SLOT_GRAD_MINB 5
-#endif
-#ifndef ZG_SLOT_S1_MINB
-#define ZG_SLOT_S1_MINB 6
+#define ZG_SLOT_GRAD_MINB 6
 #endif
 #ifndef ZG_SLOT_S2_MINB
 #define ZG_SLOT_S2_MINB 5
 #endif
-constexpr int GM = ZG_SLOT_GRAD_MINB, S1M = ZG_SLOT_S1_MINB, S2M = ZG_SLOT_S2_MINB;
+constexpr int GM = ZG_SLOT_GRAD_MINB, S2M = ZG_SLOT_S2_MINB;
 
 static inline unsigned blocks(const SmfArgs &a) { return (unsigned)((a.smesh.n + BLOCK - 1) / BLOCK); }
 
@@ -48,8 +45,164 @@ void launch_flux1(const SmfArgs &a, void *stream) { ZG_FLUX_FAMILY(flux1_fx, a, 
 void launch_grad(const SmfArgs &a, PrimPtr z, void *stream) {
     k_grad<SlotFastAcc, BLOCK, GM><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, z);
 }
-void launch_stage1(const SmfArgs &a, void *stream) {
-    k_stage1<SlotFastAcc, BLOCK, S1M><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a);
+
+// --- least-squares gradients over precomputed geometry ------------------------
+// lsm_limited_2pass (smf_struct.cuh, gradient.h:226-282 with the limiting of
+// sm_fluid.cpp:143-174) with the slot geometry, its weights and the inverse
+// matrix computed once per mesh change instead of in both passes of every
+// gradient evaluation.
+__global__ void __launch_bounds__(BLOCK) k_grad_geometry(SmfArgs a, double4 *sg, double4 *bm) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    SlotFastAcc c(a, ic);
+    const double pcx = c.cx(), pcy = c.cy();
+    double A00 = 0.0, A01 = 0.0, A10 = 0.0, A11 = 0.0;
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        const FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) {
+            sg[8 * ic + s] = make_double4(0.0, 0.0, 0.0, 0.0);
+            continue;
+        }
+        double ncx, ncy;
+        neib_center(c, g, s, pcx, pcy, ncx, ncy);
+        const double rx = ncx - pcx, ry = ncy - pcy;
+        const double d = rx * g.nx + ry * g.ny, nxx = d * g.nx, nyy = d * g.ny;
+        const double w = g.area / cube_rn(sqrt(nxx * nxx + nyy * nyy));
+        const double wdx = w * nxx, wdy = w * nyy;
+        A00 += wdx * rx;
+        A01 += wdx * ry;
+        A10 += wdy * rx;
+        A11 += wdy * ry;
+        sg[8 * ic + s] = make_double4(rx, ry, wdx, wdy);
+    }
+    if (fabs(A11) < 1e-8) A11 = 1.0;  // 1-D case (gradient.h:270-272)
+    const double det = A11 * A00 + (-A01) * A10, inv = 1.0 / det;
+    bm[ic] = make_double4(A11 * inv, (-A01) * inv, (-A10) * inv, A00 * inv);
+}
+
+// the neighbour's (or the boundary's) primitive values across slot s
+__device__ __forceinline__ void slot_values(const SmfArgs &a, const PrimPtr &z, const Prim &zc, int ic, int s,
+                                            int flag, double zn[4]) {
+    Prim p;
+    if (!is_boundary(flag)) {
+        const int nb = a.smesh.fn[8 * ic + s];
+        zn[0] = z.r[nb];
+        zn[1] = z.u[nb];
+        zn[2] = z.v[nb];
+        zn[3] = z.p[nb];
+        return;
+    }
+    const int side = s & 3;  // the axis normal of the side (SlotFastAcc::face)
+    const double nx = side == 0 ? -1.0 : (side == 1 ? 1.0 : (side == 2 ? -0.0 : 0.0));
+    const double ny = side == 0 ? -0.0 : (side == 1 ? 0.0 : (side == 2 ? -1.0 : 1.0));
+    p = boundary_value(zc, nx, ny, flag);
+    zn[0] = p.r;
+    zn[1] = p.u;
+    zn[2] = p.v;
+    zn[3] = p.p;
+}
+
+// PRED: the predictor of the predictor-corrector scheme (k_stage1,
+// sm_fluid.cpp:176-253) follows in the same thread from the gradients just
+// computed, into a.zhalf.
+template <bool PRED>
+__global__ void __launch_bounds__(BLOCK, GM) k_grad_pre(SmfArgs a, PrimPtr z, const double4 *sg, const double4 *bm) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    if (ic >= a.smesh.n) return;
+    const Prim zc = load_prim(z, ic);
+    const double zcv[4] = {zc.r, zc.u, zc.v, zc.p};
+    double Fx[4] = {0.0, 0.0, 0.0, 0.0}, Fy[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        const int flag = a.smesh.fb[8 * ic + s];
+        if (flag == BC_UNDEFINED) continue;
+        double zn[4];
+        slot_values(a, z, zc, ic, s, flag, zn);
+        const double4 G = sg[8 * ic + s];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double dF = zn[k] - zcv[k];
+            Fx[k] += G.z * dF;
+            Fy[k] += G.w * dF;
+        }
+    }
+    const double4 B = bm[ic];
+    double g0x[4], g0y[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        g0x[k] = B.x * Fx[k] + B.y * Fy[k];
+        g0y[k] = B.z * Fx[k] + B.w * Fy[k];
+    }
+    double Lx[4] = {0.0, 0.0, 0.0, 0.0}, Ly[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        const int flag = a.smesh.fb[8 * ic + s];
+        if (flag == BC_UNDEFINED) continue;
+        double zn[4];
+        slot_values(a, z, zc, ic, s, flag, zn);
+        const double4 G = sg[8 * ic + s];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double dF_p = zn[k] - zcv[k];
+            const double du_n = g0x[k] * G.x + g0y[k] * G.y;
+            const double dF_m = 2.0 * du_n - dF_p;
+            const double dF_lim = limiter2(a.limiter, dF_m, dF_p) * dF_p;
+            Lx[k] += G.z * dF_lim;
+            Ly[k] += G.w * dF_lim;
+        }
+    }
+    double gx[4], gy[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        gx[k] = B.x * Lx[k] + B.y * Ly[k];
+        gy[k] = B.z * Lx[k] + B.w * Ly[k];
+        a.gx[k][ic] = gx[k];
+        a.gy[k][ic] = gy[k];
+    }
+    if constexpr (PRED) {
+        if (a.wait_in[ic] > 0) {
+            store_prim(a.zhalf, ic, zc);
+            return;
+        }
+        SlotFastAcc c(a, ic);
+        const double dt = finalize_dt(a), pcx = c.cx(), pcy = c.cy();
+        Cons q = q_from_p(zc);
+        Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int s = 0; s < 8; ++s) {
+            const FaceG g = c.face(s);
+            if (g.flag == BC_UNDEFINED) continue;
+            const double dx = g.fcx - pcx, dy = g.fcy - pcy;
+            Prim zm;  // extrap (face_extra.h:135-163)
+            zm.r = zc.r + (gx[0] * dx + gy[0] * dy);
+            zm.u = zc.u + (gx[1] * dx + gy[1] * dy);
+            zm.v = zc.v + (gx[2] * dx + gy[2] * dy);
+            zm.p = zc.p + (gx[3] * dx + gy[3] * dy);
+            zm.e = a.eos.energy_rP(zm.r, zm.p);
+            if (is_bad(zm, a.eos)) zm = zc;
+            double cs, sn;
+            frame<SlotFastAcc>(g, cs, sn);
+            rot_local(zm.u, zm.v, cs, sn);
+            Cons lf = flux_from_p(zm);
+            rot_global(lf.mu, lf.mv, cs, sn);
+            add_area(F, lf, g.area);
+        }
+        update(q, 0.5 * dt / c.vol(), F);
+        Prim h = p_from_q(q, a.eos);
+        if (is_bad(h, a.eos)) h = zc;
+        store_prim(a.zhalf, ic, h);
+    }
+}
+
+void launch_grad_geometry(const SmfArgs &a, double4 *sg, double4 *bm, void *stream) {
+    k_grad_geometry<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, sg, bm);
+}
+void launch_grad_pre(const SmfArgs &a, PrimPtr z, const double4 *sg, const double4 *bm, bool predictor,
+                     void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (predictor) k_grad_pre<true><<<blocks(a), BLOCK, 0, st>>>(a, z, sg, bm);
+    else k_grad_pre<false><<<blocks(a), BLOCK, 0, st>>>(a, z, sg, bm);
 }
 
 // --- face-once corrector / Heun stages --------------------------------------
@@ -91,45 +244,57 @@ __device__ __forceinline__ Cons sum_faces(int ic, const FaceFlux &ff) {
     return F;
 }
 
-// k_stage2's update (sm_fluid.cpp:342-366) from the summed face fluxes
+// k_stage2's update (sm_fluid.cpp:342-366) from the summed face fluxes.
+// With ff.dt_next, every thread of the block (those past the last cell with
+// the neutral value) reaches the one block-wide CFL minimum at the end.
 __global__ void __launch_bounds__(BLOCK) k_stage2_sum(SmfArgs a, FaceFlux ff) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= a.smesh.n) return;
-    const double dt = finalize_dt(a);
-    const Prim zc = load_prim(a.z, ic);
-    const int wc = a.wait_in[ic];
-    Cons q = q_from_p(zc);
-    const Cons F = sum_faces(ic, ff);
-    update(q, dt / a.smesh.vol[ic], F);
-    Prim n = p_from_q(q, a.eos);
-    int wn = wc;
-    if (is_bad(n, a.eos)) {
-        n = zc;
-        wn = 3;
-    } else if (wn > 0) {
-        --wn;
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
+    if (ic < a.smesh.n) {
+        const double dt = finalize_dt(a);
+        const Prim zc = load_prim(a.z, ic);
+        const int wc = a.wait_in[ic];
+        Cons q = q_from_p(zc);
+        const Cons F = sum_faces(ic, ff);
+        update(q, dt / a.smesh.vol[ic], F);
+        Prim n = p_from_q(q, a.eos);
+        int wn = wc;
+        if (is_bad(n, a.eos)) {
+            n = zc;
+            wn = 3;
+        } else if (wn > 0) {
+            --wn;
+        }
+        store_prim(a.znext, ic, n);
+        a.wait_out[ic] = wn;
+        if (ff.dt_next) best = cfl_bits(a, a.smesh.inc[ic], n.r, n.u, n.v, n.p);
     }
-    store_prim(a.znext, ic, n);
-    a.wait_out[ic] = wn;
+    if (ff.dt_next) commit_cfl_min<BLOCK>(a, best, ff.dt_next);
 }
 
-// k_heun's update from the summed face fluxes
+// k_heun's update from the summed face fluxes (the final stage with
+// ff.dt_next: the CFL minimum as in k_stage2_sum)
 template <bool FINAL>
 __global__ void __launch_bounds__(BLOCK) k_heun_sum(SmfArgs a, PrimPtr zin, PrimPtr zout, FaceFlux ff) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= a.smesh.n) return;
-    const double dt = finalize_dt(a);
-    Cons q = q_from_p(load_prim(zin, ic));
-    const Cons F = sum_faces(ic, ff);
-    update(q, dt / a.smesh.vol[ic], F);
-    if (FINAL) {
-        Cons q0 = q_from_p(load_prim(a.z, ic));
-        q.r = 0.5 * (q0.r + q.r);
-        q.mu = 0.5 * (q0.mu + q.mu);
-        q.mv = 0.5 * (q0.mv + q.mv);
-        q.E = 0.5 * (q0.E + q.E);
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;
+    if (ic < a.smesh.n) {
+        const double dt = finalize_dt(a);
+        Cons q = q_from_p(load_prim(zin, ic));
+        const Cons F = sum_faces(ic, ff);
+        update(q, dt / a.smesh.vol[ic], F);
+        if (FINAL) {
+            Cons q0 = q_from_p(load_prim(a.z, ic));
+            q.r = 0.5 * (q0.r + q.r);
+            q.mu = 0.5 * (q0.mu + q.mu);
+            q.mv = 0.5 * (q0.mv + q.mv);
+            q.E = 0.5 * (q0.E + q.E);
+        }
+        const Prim n = p_from_q(q, a.eos);
+        store_prim(zout, ic, n);
+        if (FINAL && ff.dt_next) best = cfl_bits(a, a.smesh.inc[ic], n.r, n.u, n.v, n.p);
     }
-    store_prim(zout, ic, p_from_q(q, a.eos));
+    if (FINAL && ff.dt_next) commit_cfl_min<BLOCK>(a, best, ff.dt_next);
 }
 
 template <int FX>

@@ -273,21 +273,26 @@ __device__ inline void frame(const FaceG &g, double &c, double &s) {
 
 // ---------------------------------------------------------------------------
 // K1: CFL minimum over cells (sm_fluid.cpp:104-114, amr_cells.cpp:107-116).
-template <class Acc, int BLOCK, int MINB = 1>
-__global__ void __launch_bounds__(BLOCK, MINB) k_dt(SmfArgs a) {
-    int ic = blockIdx.x * BLOCK + threadIdx.x;
-    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
-    if (ic < Acc::n(a)) {
-        Acc c(a, ic);
-        double rho = a.z.r[ic], u = a.z.u[ic], v = a.z.v[ic], p = a.z.p[ic];
-        double cs = a.eos.sound_speed_rP(rho, p);
-        double lam = c.dinc() / (sqrt(u * u + v * v) + cs);
-        // std::min skips a NaN in its second slot; NaN bits sort above all
-        // finite positives, so the unsigned minimum skips it too.
-        unsigned long long b = dbits(lam);
-        if (!(lam >= 0.0)) b = 0x7FEFFFFFFFFFFFFFull;
-        best = b;
-    }
+// The CFL bound of one cell, incircle / (|v| + c), as the bits of a
+// non-negative double (compute_dt, sm_fluid.cpp:104-116).  std::min skips a
+// NaN in its second slot; NaN bits sort above all finite positives, so the
+// unsigned minimum skips it too.
+__device__ inline unsigned long long cfl_bits(const SmfArgs &a, double dinc, double rho, double u, double v,
+                                              double p) {
+    double cs = a.eos.sound_speed_rP(rho, p);
+    double lam = dinc / (sqrt(u * u + v * v) + cs);
+    unsigned long long b = dbits(lam);
+    if (!(lam >= 0.0)) b = 0x7FEFFFFFFFFFFFFFull;
+    return b;
+}
+
+// Block minimum of `best`, then the grid minimum through a.dmin_bits: the
+// last block to finish turns it into dt = min(CFL * min, max_dt)
+// (sm_fluid.cpp:112) at *dst and resets the accumulator for the next use.
+// No block waits for another.  Every thread of the block calls it, from one
+// call site (it holds a block barrier).
+template <int BLOCK>
+__device__ inline void commit_cfl_min(const SmfArgs &a, unsigned long long best, double *dst) {
     for (int o = 16; o > 0; o >>= 1) {
         unsigned long long t = __shfl_xor_sync(0xffffffffu, best, o);
         best = t < best ? t : best;
@@ -303,21 +308,29 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_dt(SmfArgs a) {
         }
         if (threadIdx.x == 0) {
             atomicMin(a.dmin_bits, best);
-            // The last block to finish turns the minimum into
-            // dt = min(CFL * min, max_dt) (sm_fluid.cpp:112) and resets the
-            // accumulator for the next step.  No block waits for another.
             __threadfence();
             unsigned int ticket = atomicAdd(a.dt_ticket, 1u);
             if (ticket == gridDim.x - 1) {
                 unsigned long long bits = atomicMin(a.dmin_bits, 0x7FEFFFFFFFFFFFFFull);
                 double dmin = __longlong_as_double((long long)bits);
-                *a.dt_out = smin(a.CFL * dmin, a.max_dt);
+                *dst = smin(a.CFL * dmin, a.max_dt);
                 *a.dmin_bits = 0x7FEFFFFFFFFFFFFFull;
                 *a.dt_ticket = 0u;
                 __threadfence();
             }
         }
     }
+}
+
+template <class Acc, int BLOCK, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_dt(SmfArgs a) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
+    if (ic < Acc::n(a)) {
+        Acc c(a, ic);
+        best = cfl_bits(a, c.dinc(), a.z.r[ic], a.z.u[ic], a.z.v[ic], a.z.p[ic]);
+    }
+    commit_cfl_min<BLOCK>(a, best, a.dt_out);
 }
 
 __device__ inline void add_area(Cons &F, const Cons &lf, double area) {

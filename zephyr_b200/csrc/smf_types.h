@@ -75,7 +75,6 @@ namespace slotfast {
 void launch_dt(const SmfArgs &a, PrimPtr z, void *stream);
 void launch_flux1(const SmfArgs &a, void *stream);
 void launch_grad(const SmfArgs &a, PrimPtr z, void *stream);
-void launch_stage1(const SmfArgs &a, void *stream);
 void launch_grad_flags(const SmfArgs &a, int *flags, double refine, double coarsen, void *stream);
 
 // Face-once form of the corrector and of the Heun stages: each face's flux
@@ -90,8 +89,17 @@ struct FaceFlux {
     const int *fidx;   // per slot 8 ic + s: t >= 0, the face list entry it computes; -(t + 1), the
                        // neighbour's entry it takes with the opposite sign; FACE_NONE, no face
     int nfaces;        // entries of `list`
+    double *dt_next;   // non-null: the cell sums also give the next step's dt (of the state they write) here
 };
 constexpr int FACE_NONE = -2147483647 - 1;
+// The limited least-squares gradients over per-slot geometry built once per
+// mesh change: sg[8 ic + s] = (rx, ry, w nx^, w ny^) (the centre offset and
+// the weighted normal projections of gradient.h:251-275), bm[ic] = the
+// inverse of the cell's 2x2 least-squares matrix (B00, B01, B10, B11).
+void launch_grad_geometry(const SmfArgs &a, double4 *sg, double4 *bm, void *stream);
+// predictor: the predictor stage (k_stage1) fused after the gradients
+void launch_grad_pre(const SmfArgs &a, PrimPtr z, const double4 *sg, const double4 *bm, bool predictor,
+                     void *stream);
 void launch_stage2_faces(const SmfArgs &a, FaceFlux ff, void *stream);
 void launch_stage2_sum(const SmfArgs &a, FaceFlux ff, void *stream);
 void launch_heun_faces(const SmfArgs &a, PrimPtr zin, FaceFlux ff, void *stream);
@@ -111,6 +119,7 @@ struct OrderBuffers {
     int *flist;        // FaceFlux::list (8 cap)
     int *fidx;         // FaceFlux::fidx (8 cap)
     int nfaces;
+    double4 *sg, *bm;  // gradient geometry (8 cap, cap)
 };
 size_t order_scratch_bytes(int cap);
 // fills b.perm (position -> cell), b.inv and the reordered mesh arrays, and

@@ -86,7 +86,9 @@ struct zg_ctx {
     int *d_wait = nullptr;      // two isolation-counter buffers
     unsigned long long *d_dmin = nullptr;
     unsigned int *d_ticket = nullptr;
-    double *d_dt = nullptr;
+    double *d_dt = nullptr;     // dt of the last step
+    double *d_dt2 = nullptr;    // the other dt slot: the next step's dt when dt_next_ready
+    bool dt_next_ready = false; // the FAST adaptive step's cell sums left the next dt in d_dt2
     int *d_flags = nullptr;
     PrimPtr z{}, zhalf{}, znext{};
     double *gx[4] = {}, *gy[4] = {};
@@ -208,6 +210,8 @@ void free_solver(zg_ctx *c) {
     c->d_dmin = nullptr;
     c->d_ticket = nullptr;
     c->d_dt = nullptr;
+    c->d_dt2 = nullptr;
+    c->dt_next_ready = false;
     c->d_flags = nullptr;
     c->configured = false;
     c->stepped = false;
@@ -321,6 +325,7 @@ tiled::Fields<float> mixed_fields(const zg_ctx *c) {
 // the mesh's own order (FP64 primitive in c->z, counters in the current
 // counter buffer); a no-op in the other representations.
 int leave_order(zg_ctx *c) {
+    c->dt_next_ready = false;  // the state may change before the next step
     if (c->state_mode != STATE_ORDERED) return ZG_OK;
     int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
     slotfast::scatter_state(c->ord.perm, c->n, c->oz, c->z, c->ord_waits ? c->ow[0] : nullptr, wait,
@@ -587,7 +592,7 @@ int ensure_order(zg_ctx *c) {
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t bytes = al(2 * cap * 8) + 3 * al(cap * 4) + al(tmp) + 4 * al(cap * 8) + al(cap * 4) +
                          2 * al(8 * cap * 4) + 15 * al(cap * 8) + 2 * al(cap * 4) + 4 * al(8 * cap * 8) +
-                         2 * al((cap + 1) * 4) + 2 * al(8 * cap * 4);
+                         2 * al((cap + 1) * 4) + 2 * al(8 * cap * 4) + al(8 * cap * 32) + al(cap * 32);
     ZG_CUDA(c, cudaMalloc(&c->d_ord, bytes));
     char *p = static_cast<char *>(c->d_ord);
     auto take = [&p, &al](size_t b) {
@@ -624,6 +629,8 @@ int ensure_order(zg_ctx *c) {
     o.foff = reinterpret_cast<int *>(take((cap + 1) * 4));
     o.flist = reinterpret_cast<int *>(take(8 * cap * 4));
     o.fidx = reinterpret_cast<int *>(take(8 * cap * 4));
+    o.sg = reinterpret_cast<double4 *>(take(8 * cap * 32));
+    o.bm = reinterpret_cast<double4 *>(take(cap * 32));
     o.nfaces = 0;
     c->ord_version = -1;
     return ZG_OK;
@@ -653,7 +660,10 @@ int enqueue_slot_fast_step(zg_ctx *c) {
             const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
             if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
                 return cuda_fail(c, cudaGetLastError(), "cell order");
-            c->launches += 8;
+            SmfArgs ga = make_args(c);
+            ga.smesh = c->ord_mesh;
+            slotfast::launch_grad_geometry(ga, c->ord.sg, c->ord.bm, st);
+            c->launches += 9;
             c->ord_version = c->mesh_version;
         }
         int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
@@ -665,6 +675,13 @@ int enqueue_slot_fast_step(zg_ctx *c) {
     c->oflux.list = c->ord.flist;
     c->oflux.fidx = c->ord.fidx;
     c->oflux.nfaces = c->ord.nfaces;
+    // second order: the corrector's (or the final Heun stage's) cell sums
+    // also take the CFL minimum of the state they write, so the next step
+    // starts with its dt (in the other dt slot) and launches no dt kernel
+    const bool fuse_dt = c->par.accuracy == 2;
+    const bool have_dt = c->dt_next_ready;
+    if (have_dt) std::swap(c->d_dt, c->d_dt2);
+    c->oflux.dt_next = fuse_dt ? c->d_dt2 : nullptr;
     SmfArgs a = make_args(c);
     a.smesh = c->ord_mesh;
     a.z = c->oz;
@@ -672,27 +689,28 @@ int enqueue_slot_fast_step(zg_ctx *c) {
     a.znext = c->oznext;
     a.wait_in = c->ow[0];
     a.wait_out = c->ow[1];
-    timed(c, ZG_K_DT, [&] { slotfast::launch_dt(a, a.z, st); });
+    if (!have_dt) timed(c, ZG_K_DT, [&] { slotfast::launch_dt(a, a.z, st); });
     if (c->par.accuracy == 1) {
         timed(c, ZG_K_FLUX1, [&] { slotfast::launch_flux1(a, st); });
     } else if (pc) {
-        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
-        timed(c, ZG_K_STAGE1, [&] { slotfast::launch_stage1(a, st); });
+        // gradients and the predictor in one pass
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad_pre(a, a.z, c->ord.sg, c->ord.bm, true, st); });
         // the corrector face-once: the listed faces, then every cell's sum
         timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2_faces(a, c->oflux, st); });
         timed(c, ZG_K_STAGE2, [&] { slotfast::launch_stage2_sum(a, c->oflux, st); });
         std::swap(c->ow[0], c->ow[1]);
     } else {
-        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.z, st); });
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad_pre(a, a.z, c->ord.sg, c->ord.bm, false, st); });
         timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun_faces(a, a.z, c->oflux, st); });
         timed(c, ZG_K_HEUN_A, [&] { slotfast::launch_heun_sum(a, a.z, a.zhalf, false, c->oflux, st); });
-        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, a.zhalf, st); });
+        timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad_pre(a, a.zhalf, c->ord.sg, c->ord.bm, false, st); });
         timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun_faces(a, a.zhalf, c->oflux, st); });
         timed(c, ZG_K_HEUN_B, [&] { slotfast::launch_heun_sum(a, a.zhalf, a.znext, true, c->oflux, st); });
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     std::swap(c->oz, c->oznext);
+    c->dt_next_ready = fuse_dt;
     c->cfl_valid = false;
     c->stepped = true;
     return ZG_OK;
@@ -1076,6 +1094,8 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
     ZG_CUDA(c, cudaMalloc(&c->d_dmin, 64));
     c->d_ticket = reinterpret_cast<unsigned int *>(reinterpret_cast<char *>(c->d_dmin) + 8);
     c->d_dt = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_dmin) + 16);
+    c->d_dt2 = reinterpret_cast<double *>(reinterpret_cast<char *>(c->d_dmin) + 48);
+    c->dt_next_ready = false;
     c->d_slots = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(c->d_dmin) + 24);
     ZG_CUDA(c, cudaMalloc(&c->d_mq, 8 * n * sizeof(double)));
     ZG_CUDA(c, cudaMalloc(&c->d_mf, 23 * n * sizeof(float)));
@@ -1125,6 +1145,7 @@ int zg_smf_configure(zg_ctx *c, const zg_smf_params *p) {
 int zg_smf_set_max_dt(zg_ctx *c, double max_dt) {
     if (!c) return ZG_ERR_ARG;
     c->par.max_dt = max_dt;
+    c->dt_next_ready = false;  // a dt taken with the old cap
     return ZG_OK;
 }
 
