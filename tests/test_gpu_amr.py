@@ -210,13 +210,14 @@ def test_fast_kernels_on_the_adaptive_mesh_match_parity(gpu_lib, acc, scheme):
     mesh.close()
 
 
-@pytest.mark.parametrize("acc,scheme", [(2, "pc"), (2, "heun"), (1, "pc")])
-def test_fast_state_order_between_steps(gpu_lib, acc, scheme):
-    """The FAST adaptive step keeps the state in its Morton cell order
-    between steps and every other entry point brings it back: steps run
-    back to back (state held in that order, set_flags and refine between
-    them) give the same bits, counters included, as the same schedule read
-    out after every step."""
+@pytest.mark.parametrize("acc,scheme,form", [(2, "pc", "fast"), (2, "heun", "fast"), (1, "pc", "fast"),
+                                             (2, "pc", "mixed"), (1, "pc", "mixed")])
+def test_fast_state_order_between_steps(gpu_lib, acc, scheme, form):
+    """The FAST and MIXED adaptive steps keep the state in the Morton cell
+    order between steps and every other entry point brings it back: steps
+    run back to back (state held in that order, set_flags and refine
+    between them) give the same bits, counters included, as the same
+    schedule read out after every step."""
     import zephyr_b200 as Z
 
     def run(read_each_step):
@@ -228,6 +229,8 @@ def test_fast_state_order_between_steps(gpu_lib, acc, scheme):
         fast = Z.SmFluid(Z.IdealGas(1.4), kernels=Z.Kernels.FAST)
         fast.params = solver.params
         fast.params.kernels = int(Z.Kernels.FAST)
+        if form == "mixed":
+            fast.params.precision = int(Z.Precision.MIXED)
         fast.add_types(mesh)
         seen = []
         for _ in range(3):

@@ -147,6 +147,19 @@ __global__ void k_face_index(SlotMesh m, int n, const int *off, int *fidx) {
     }
 }
 
+template <bool GATHER>
+__global__ void k_permute_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst) {
+    int p = blockIdx.x * OBLOCK + threadIdx.x;
+    if (p >= n) return;
+    const int ic = perm[p];
+    const int from = GATHER ? ic : p, to = GATHER ? p : ic;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) dst.q[k][to] = src.q[k][from];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) dst.w[k][to] = src.w[k][from];
+    if (wsrc) wdst[to] = wsrc[from];
+}
+
 size_t order_scratch_bytes(int cap) {
     size_t bytes = 0, scan = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr,
@@ -192,6 +205,13 @@ int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, doubl
 
 void gather_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream) {
     if (n > 0) k_gather<<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst, wsrc, wdst);
+}
+void gather_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst, void *stream) {
+    if (n > 0) k_permute_mixed<true><<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst, wsrc, wdst);
+}
+void scatter_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst,
+                   void *stream) {
+    if (n > 0) k_permute_mixed<false><<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst, wsrc, wdst);
 }
 void scatter_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream) {
     if (n > 0) k_scatter<<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst, wsrc, wdst);

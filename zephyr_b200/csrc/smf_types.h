@@ -127,6 +127,15 @@ size_t order_scratch_bytes(int cap);
 int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, OrderBuffers &b,
                 SlotMesh &out, void *stream);
 void gather_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream);
+// the MIXED representation (FP64 conserved, FP32 primitive mirror) and the
+// counters, into and out of the order
+struct MixedState {
+    double *q[4];
+    float *w[5];
+};
+void gather_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst, void *stream);
+void scatter_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst,
+                   void *stream);
 void scatter_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream);
 }  // namespace slotfast
 

@@ -24,9 +24,11 @@
 
 using namespace zg;
 
-// state_mode of a state held in the Morton order of the FAST step on an
-// adaptive rectangle (FP64 primitive, in the order buffers)
+// state_mode of a state held in the Morton order of the steps on an
+// adaptive rectangle: FP64 primitive in the order buffers (FAST), or the
+// MIXED representation in its own double buffers (MIXED)
 constexpr int STATE_ORDERED = 100;
+constexpr int STATE_ORDERED_MIXED = 101;
 
 struct zg_ctx {
     int device = 0;
@@ -230,6 +232,7 @@ void free_mesh(zg_ctx *c) {
     c->ord = slotfast::OrderBuffers{};
     c->ord_version = -1;
     if (c->state_mode == STATE_ORDERED) c->state_mode = ZG_FP64;  // the state goes with the mesh
+    if (c->state_mode == STATE_ORDERED_MIXED) c->state_mode = ZG_MIXED;
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
     c->d_slot = nullptr;
@@ -324,8 +327,27 @@ tiled::Fields<float> mixed_fields(const zg_ctx *c) {
 // Bring a state held in the Morton order of the FAST adaptive step back to
 // the mesh's own order (FP64 primitive in c->z, counters in the current
 // counter buffer); a no-op in the other representations.
+slotfast::MixedState mixed_set(const zg_ctx *c, int set) {
+    slotfast::MixedState m{};
+    for (int k = 0; k < 4; ++k) m.q[k] = c->mq[set][k];
+    for (int k = 0; k < 5; ++k) m.w[k] = c->mw[set][k];
+    return m;
+}
+
 int leave_order(zg_ctx *c) {
     c->dt_next_ready = false;  // the state may change before the next step
+    if (c->state_mode == STATE_ORDERED_MIXED) {
+        // from the current set (cell order) into the other (mesh order)
+        int *wsrc = c->d_wait + (size_t)c->wait_cur * c->cap, *wdst = c->d_wait + (size_t)(1 - c->wait_cur) * c->cap;
+        slotfast::scatter_mixed(c->ord.perm, c->n, mixed_set(c, c->mcur), mixed_set(c, 1 - c->mcur), wsrc, wdst,
+                                (void *)c->stream);
+        ++c->launches;
+        c->mcur = 1 - c->mcur;
+        c->wait_cur = 1 - c->wait_cur;
+        c->state_mode = ZG_MIXED;
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "state order");
+    }
     if (c->state_mode != STATE_ORDERED) return ZG_OK;
     int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
     slotfast::scatter_state(c->ord.perm, c->n, c->oz, c->z, c->ord_waits ? c->ow[0] : nullptr, wait,
@@ -636,6 +658,24 @@ int ensure_order(zg_ctx *c) {
     return ZG_OK;
 }
 
+// The cell order, the ordered mesh arrays, the face list and the gradient
+// geometry of the current mesh (rebuilt after a mesh change).
+int order_current(zg_ctx *c) {
+    int rc = ensure_order(c);
+    if (rc != ZG_OK) return rc;
+    if (c->ord_version == c->mesh_version) return ZG_OK;
+    void *st = (void *)c->stream;
+    const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
+    if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
+        return cuda_fail(c, cudaGetLastError(), "cell order");
+    SmfArgs ga = make_args(c);
+    ga.smesh = c->ord_mesh;
+    slotfast::launch_grad_geometry(ga, c->ord.sg, c->ord.bm, st);
+    c->launches += 9;
+    c->ord_version = c->mesh_version;
+    return ZG_OK;
+}
+
 // The FAST step on an adaptive rectangle: the kernels of the parity step
 // over derived face geometry, with fused multiply-adds, the corrector (and
 // the Heun stages) face-once over a face list, run on the cells in Morton
@@ -656,16 +696,8 @@ int enqueue_slot_fast_step(zg_ctx *c) {
     if (c->state_mode != STATE_ORDERED) {
         rc = convert_state(c, ZG_FP64);
         if (rc != ZG_OK) return rc;
-        if (c->ord_version != c->mesh_version) {
-            const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
-            if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
-                return cuda_fail(c, cudaGetLastError(), "cell order");
-            SmfArgs ga = make_args(c);
-            ga.smesh = c->ord_mesh;
-            slotfast::launch_grad_geometry(ga, c->ord.sg, c->ord.bm, st);
-            c->launches += 9;
-            c->ord_version = c->mesh_version;
-        }
+        rc = order_current(c);
+        if (rc != ZG_OK) return rc;
         int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
         slotfast::gather_state(c->ord.perm, c->n, c->z, c->oz, pc ? wait : nullptr, c->ow[0], st);
         ++c->launches;
@@ -722,11 +754,30 @@ int enqueue_slot_mixed_step(zg_ctx *c) {
     if (c->par.accuracy == 2 && c->par.scheme != ZG_SCHEME_PREDICTOR_CORRECTOR)
         return fail(c, ZG_ERR_STATE,
                     "the MIXED form on an adaptive mesh runs first order or the predictor-corrector scheme");
-    int rc = convert_state(c, ZG_MIXED);
-    if (rc != ZG_OK) return rc;
-    SmfArgs a = make_args(c);
-    tiled::Fields<float> f = mixed_fields(c);
+    // the state in the cell order of the FAST step (smf_slot_order.cu), kept
+    // there between steps like the FAST step's: gathered from the current
+    // set of the MIXED buffers into the other, with the counters
     void *st = (void *)c->stream;
+    int rc = ZG_OK;
+    if (c->state_mode == STATE_ORDERED_MIXED && c->ord_version != c->mesh_version) {
+        rc = leave_order(c);  // not reached through the API: the mesh changes after leave_order
+        if (rc != ZG_OK) return rc;
+    }
+    if (c->state_mode != STATE_ORDERED_MIXED) {
+        rc = convert_state(c, ZG_MIXED);
+        if (rc != ZG_OK) return rc;
+        rc = order_current(c);
+        if (rc != ZG_OK) return rc;
+        int *wsrc = c->d_wait + (size_t)c->wait_cur * c->cap, *wdst = c->d_wait + (size_t)(1 - c->wait_cur) * c->cap;
+        slotfast::gather_mixed(c->ord.perm, c->n, mixed_set(c, c->mcur), mixed_set(c, 1 - c->mcur), wsrc, wdst, st);
+        ++c->launches;
+        c->mcur = 1 - c->mcur;
+        c->wait_cur = 1 - c->wait_cur;
+        c->state_mode = STATE_ORDERED_MIXED;
+    }
+    SmfArgs a = make_args(c);
+    a.smesh = c->ord_mesh;
+    tiled::Fields<float> f = mixed_fields(c);
     timed(c, ZG_K_DT, [&] { slotmixed::launch_dt(a, f, st); });
     if (c->par.accuracy == 1) {
         timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_faces(a, f, 0, st); });
