@@ -221,29 +221,6 @@ __global__ void __launch_bounds__(BLOCK, S2M) k_faces_once(SmfArgs a, PrimPtr zi
     ff.f[t] = make_double4(lf.r, lf.mu, lf.mv, lf.E);
 }
 
-// the face fluxes of cell ic summed in slot order
-__device__ __forceinline__ Cons sum_faces(int ic, const FaceFlux &ff) {
-    Cons F{0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const int x = ff.fidx[8 * ic + s];
-        if (x == FACE_NONE) continue;
-        const double4 v = ff.f[x >= 0 ? x : -x - 1];
-        if (x >= 0) {
-            F.r += v.x;
-            F.mu += v.y;
-            F.mv += v.z;
-            F.E += v.w;
-        } else {
-            F.r -= v.x;
-            F.mu -= v.y;
-            F.mv -= v.z;
-            F.E -= v.w;
-        }
-    }
-    return F;
-}
-
 // k_stage2's update (sm_fluid.cpp:342-366) from the summed face fluxes.
 // With ff.dt_next, every thread of the block (those past the last cell with
 // the neutral value) reaches the one block-wide CFL minimum at the end.

@@ -248,75 +248,95 @@ __global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S1_MINB) k_stage1(SmfArgs a, 
     stw(f.h, ic, tiled::bad64(hz, a.eos) ? zc : tiled::down<R>(hz));
 }
 
-// Face loop and update.  MODE 0: first order (faces from the state,
-// sm_fluid.cpp:127-174); MODE 1: corrector of the predictor-corrector scheme
-// with the isolation counters (sm_fluid.cpp:255-366).
+// Face-once form over the FAST step's face list (slotfast::FaceFlux): one
+// thread per face, the face flux of k_faces times the face's area into the
+// face's FP64 record; then per cell the records in slot order and the update
+// of k_faces, with the CFL minimum of the new state for the next step's dt
+// (ff.dt_next).
 template <int MODE>
-__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S2_MINB) k_faces(SmfArgs a, Fields<R> f) {
-    int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= a.smesh.n) return;
+__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S2_MINB) k_faces_once(SmfArgs a, Fields<R> f,
+                                                                          slotfast::FaceFlux ff) {
+    int t = blockIdx.x * BLOCK + threadIdx.x;
+    if (t >= ff.nfaces) return;
+    const int fi = ff.list[t], ic = fi >> 3, s = fi & 7;
     SlotFastAcc c(a, ic);
+    const FaceG g = c.face(s);
     const EosR<R> eos = tiled::eos_as<R>(a.eos);
     const R *const *src = MODE == 1 ? const_cast<const R *const *>(f.h) : f.w;
     const P5<R> zch = ldw(src, ic);
     const int wc = MODE == 1 ? f.wait_in[ic] : 0;
-    R gx[4], gy[4];
-    if (MODE == 1) ldg(f, ic, gx, gy);
-    double F[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-    for (int s = 0; s < 8; ++s) {
-        FaceG g = c.face(s);
-        if (g.flag == BC_UNDEFINED) continue;
-        const bool bnd = is_boundary(g.flag);
-        const R nx = (R)g.nx, ny = (R)g.ny;
-        const P5<R> z_nh = bnd ? wall_of(zch, nx, ny, g.flag) : ldw(src, g.nb);
-        const bool robust = MODE == 1 && (wc > 0 || f.wait_in[g.nb] > 0);
-        P5<R> zm = zch, zp = z_nh;
-        if (MODE == 1 && !robust) {
-            double ncx, ncy;
-            neib_center(c, g, s, c.cx(), c.cy(), ncx, ncy);
-            zm = recon(zch, gx, gy, (R)(g.fcx - c.cx()), (R)(g.fcy - c.cy()), eos);
-            if (!bnd) {
-                R hx[4], hy[4];
-                ldg(f, g.nb, hx, hy);
-                zp = recon(z_nh, hx, hy, (R)(g.fcx - ncx), (R)(g.fcy - ncy), eos);
-            } else {
-                zp = wall_of(zm, nx, ny, g.flag);
+    const bool bnd = is_boundary(g.flag);
+    const R nx = (R)g.nx, ny = (R)g.ny;
+    const P5<R> z_nh = bnd ? wall_of(zch, nx, ny, g.flag) : ldw(src, g.nb);
+    const bool robust = MODE == 1 && (wc > 0 || f.wait_in[g.nb] > 0);
+    P5<R> zm = zch, zp = z_nh;
+    if (MODE == 1 && !robust) {
+        R gx[4], gy[4];
+        ldg(f, ic, gx, gy);
+        double ncx, ncy;
+        neib_center(c, g, s, c.cx(), c.cy(), ncx, ncy);
+        zm = recon(zch, gx, gy, (R)(g.fcx - c.cx()), (R)(g.fcy - c.cy()), eos);
+        if (!bnd) {
+            R hx[4], hy[4];
+            ldg(f, g.nb, hx, hy);
+            zp = recon(z_nh, hx, hy, (R)(g.fcx - ncx), (R)(g.fcy - ncy), eos);
+        } else {
+            zp = wall_of(zm, nx, ny, g.flag);
+        }
+    }
+    rot_in(nx, ny, zm.u, zm.v);
+    rot_in(nx, ny, zp.u, zp.v);
+    C4<R> lf = tiled::face_flux(a.flux, robust, zm, zp, eos, a.eos);
+    rot_out(nx, ny, lf.mu, lf.mv);
+    ff.f[t] = make_double4((double)lf.r * g.area, (double)lf.mu * g.area, (double)lf.mv * g.area,
+                           (double)lf.E * g.area);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(BLOCK) k_sum(SmfArgs a, Fields<R> f, slotfast::FaceFlux ff) {
+    int ic = blockIdx.x * BLOCK + threadIdx.x;
+    unsigned long long best = 0x7FEFFFFFFFFFFFFFull;  // bits of DBL_MAX
+    if (ic < a.smesh.n) {
+        const Cons F = sum_faces(ic, ff);
+        const double coef = (*a.dt_out) / a.smesh.vol[ic];
+        const C4<double> q0 = ldq(f, ic);
+        C4<double> q = q0;
+        q.r -= coef * F.r;
+        q.mu -= coef * F.mu;
+        q.mv -= coef * F.mv;
+        q.E -= coef * F.E;
+        P5<double> zn = tiled::prim_of(q, a.eos);
+        if (MODE == 1) {
+            const int wc = f.wait_in[ic];
+            int wn = wc;
+            if (tiled::bad64(zn, a.eos)) {  // isolation: keep the old state
+                q = q0;
+                zn = tiled::prim_of(q0, a.eos);
+                wn = 3;
+            } else if (wn > 0) {
+                --wn;
             }
+            f.wait_out[ic] = wn;
         }
-        rot_in(nx, ny, zm.u, zm.v);
-        rot_in(nx, ny, zp.u, zp.v);
-        C4<R> lf = tiled::face_flux(a.flux, robust, zm, zp, eos, a.eos);
-        rot_out(nx, ny, lf.mu, lf.mv);
-        F[0] += (double)lf.r * g.area;
-        F[1] += (double)lf.mu * g.area;
-        F[2] += (double)lf.mv * g.area;
-        F[3] += (double)lf.E * g.area;
+        f.qn[0][ic] = q.r;
+        f.qn[1][ic] = q.mu;
+        f.qn[2][ic] = q.mv;
+        f.qn[3][ic] = q.E;
+        stw(f.wn, ic, tiled::down<R>(zn));
+        if (ff.dt_next) best = cfl_bits(a, a.smesh.inc[ic], zn.r, zn.u, zn.v, zn.p);
     }
-    const double coef = (*a.dt_out) / c.vol();
-    const C4<double> q0 = ldq(f, ic);
-    C4<double> q = q0;
-    q.r -= coef * F[0];
-    q.mu -= coef * F[1];
-    q.mv -= coef * F[2];
-    q.E -= coef * F[3];
-    P5<double> zn = tiled::prim_of(q, a.eos);
-    if (MODE == 1) {
-        int wn = wc;
-        if (tiled::bad64(zn, a.eos)) {  // isolation: keep the old state
-            q = q0;
-            zn = tiled::prim_of(q0, a.eos);
-            wn = 3;
-        } else if (wn > 0) {
-            --wn;
-        }
-        f.wait_out[ic] = wn;
-    }
-    f.qn[0][ic] = q.r;
-    f.qn[1][ic] = q.mu;
-    f.qn[2][ic] = q.mv;
-    f.qn[3][ic] = q.E;
-    stw(f.wn, ic, tiled::down<R>(zn));
+    if (ff.dt_next) commit_cfl_min<BLOCK>(a, best, ff.dt_next);  // every thread, one call site
+}
+
+void launch_faces_once(const SmfArgs &a, const Fields<R> &f, int mode, const slotfast::FaceFlux &ff, void *stream) {
+    if (ff.nfaces <= 0) return;
+    const unsigned nb = (unsigned)((ff.nfaces + BLOCK - 1) / BLOCK);
+    if (mode == 0) k_faces_once<0><<<nb, BLOCK, 0, (cudaStream_t)stream>>>(a, f, ff);
+    else k_faces_once<1><<<nb, BLOCK, 0, (cudaStream_t)stream>>>(a, f, ff);
+}
+void launch_sum(const SmfArgs &a, const Fields<R> &f, int mode, const slotfast::FaceFlux &ff, void *stream) {
+    if (mode == 0) k_sum<0><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f, ff);
+    else k_sum<1><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f, ff);
 }
 
 void launch_dt(const SmfArgs &a, const Fields<R> &f, void *stream) {
@@ -333,10 +353,6 @@ void launch_grad(const SmfArgs &a, const Fields<R> &f, void *stream) {
 }
 void launch_stage1(const SmfArgs &a, const Fields<R> &f, void *stream) {
     k_stage1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
-}
-void launch_faces(const SmfArgs &a, const Fields<R> &f, int mode, void *stream) {
-    if (mode == 0) k_faces<0><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
-    else k_faces<1><<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
 }
 
 }  // namespace slotmixed

@@ -208,6 +208,30 @@ __device__ __forceinline__ bool computes_face(const SlotMesh &m, int ic, int s, 
     return (s & 1) == 1;
 }
 
+// The face-once fluxes of cell ic (slotfast::FaceFlux records, signed by
+// the slot index) summed in slot order.
+__device__ __forceinline__ Cons sum_faces(int ic, const slotfast::FaceFlux &ff) {
+    Cons F{0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int x = ff.fidx[8 * ic + s];
+        if (x == slotfast::FACE_NONE) continue;
+        const double4 v = ff.f[x >= 0 ? x : -x - 1];
+        if (x >= 0) {
+            F.r += v.x;
+            F.mu += v.y;
+            F.mv += v.z;
+            F.E += v.w;
+        } else {
+            F.r -= v.x;
+            F.mu -= v.y;
+            F.mv -= v.z;
+            F.E -= v.w;
+        }
+    }
+    return F;
+}
+
 // Centre of the neighbour across slot s, or the mirror of the cell centre in
 // the face (sm_fluid.cpp:211-212; amr_faces.h:197-199 symm_point).
 template <class Acc>

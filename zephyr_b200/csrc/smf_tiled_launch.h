@@ -34,6 +34,11 @@ namespace slotmixed {
 void launch_dt(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
 void launch_grad(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
 void launch_stage1(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
-void launch_faces(const SmfArgs &a, const tiled::Fields<float> &f, int mode, void *stream);
+// face-once (mode 0 first order, 1 corrector): the listed faces, then the
+// cell sums (and the next dt with ff.dt_next)
+void launch_faces_once(const SmfArgs &a, const tiled::Fields<float> &f, int mode, const slotfast::FaceFlux &ff,
+                       void *stream);
+void launch_sum(const SmfArgs &a, const tiled::Fields<float> &f, int mode, const slotfast::FaceFlux &ff,
+                void *stream);
 }  // namespace slotmixed
 }  // namespace zg

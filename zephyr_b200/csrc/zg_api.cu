@@ -775,21 +775,32 @@ int enqueue_slot_mixed_step(zg_ctx *c) {
         c->wait_cur = 1 - c->wait_cur;
         c->state_mode = STATE_ORDERED_MIXED;
     }
+    // the faces once over the face list, the cell sums taking the next dt
+    // (as in the FAST step)
+    c->oflux.list = c->ord.flist;
+    c->oflux.fidx = c->ord.fidx;
+    c->oflux.nfaces = c->ord.nfaces;
+    const bool have_dt = c->dt_next_ready;
+    if (have_dt) std::swap(c->d_dt, c->d_dt2);
+    c->oflux.dt_next = c->d_dt2;
     SmfArgs a = make_args(c);
     a.smesh = c->ord_mesh;
     tiled::Fields<float> f = mixed_fields(c);
-    timed(c, ZG_K_DT, [&] { slotmixed::launch_dt(a, f, st); });
+    if (!have_dt) timed(c, ZG_K_DT, [&] { slotmixed::launch_dt(a, f, st); });
     if (c->par.accuracy == 1) {
-        timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_faces(a, f, 0, st); });
+        timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_faces_once(a, f, 0, c->oflux, st); });
+        timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_sum(a, f, 0, c->oflux, st); });
     } else {
         timed(c, ZG_K_GRAD, [&] { slotmixed::launch_grad(a, f, st); });
         timed(c, ZG_K_STAGE1, [&] { slotmixed::launch_stage1(a, f, st); });
-        timed(c, ZG_K_STAGE2, [&] { slotmixed::launch_faces(a, f, 1, st); });
+        timed(c, ZG_K_STAGE2, [&] { slotmixed::launch_faces_once(a, f, 1, c->oflux, st); });
+        timed(c, ZG_K_STAGE2, [&] { slotmixed::launch_sum(a, f, 1, c->oflux, st); });
         c->wait_cur = 1 - c->wait_cur;
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     c->mcur = 1 - c->mcur;
+    c->dt_next_ready = true;
     c->cfl_valid = false;
     c->stepped = true;
     return ZG_OK;
