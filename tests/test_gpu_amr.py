@@ -253,6 +253,40 @@ def test_fast_state_order_between_steps(gpu_lib, acc, scheme, form):
     assert np.array_equal(w0, w1)
 
 
+def test_refine_after_fast_steps_splits_with_the_last_steps_gradients(gpu_lib):
+    """A refine with the slope distributor right after steps, with flags put
+    by the caller and no gradient pass between, splits with the gradients of
+    the last step (the cells' stored gradients the reference's distributor
+    reads).  The FAST steps keep their gradients in the cell order and bring
+    them back with the state; against the parity steps on the same schedule
+    the refined states agree to the FAST form's rounding."""
+    import zephyr_b200 as Z
+    outs = []
+    for kern in (Z.Kernels.PARITY, Z.Kernels.FAST):
+        mesh, solver = gpu_mesh(24, (2, 1, 1, 2), 3, "slope", 2, "MC", 0.4)
+        g = mesh.amr_arrays()
+        mesh.set_state(*AC.init_state(g["cx"], g["cy"]))
+        for _ in range(2):
+            solver.set_flags(mesh)
+            mesh.refine()
+        s = Z.SmFluid(Z.IdealGas(1.4), kernels=kern)
+        s.params = solver.params
+        s.params.kernels = int(kern)
+        s.add_types(mesh)
+        s.update(mesh, 3)
+        flags = np.zeros(mesh.n_cells(), dtype=np.int32)
+        flags[::3] = 1
+        mesh.put_flags(flags)
+        mesh.refine()
+        outs.append((mesh.get_state(), mesh.amr_arrays()["level"]))
+        mesh.close()
+    (za, la), (zb, lb) = outs
+    assert np.array_equal(la, lb) and (la == 3).any()
+    for k in range(4):  # rho, u, v, p
+        a, b = za[k], zb[k]
+        assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(a)), (k, np.max(np.abs(a - b)))
+
+
 def _adapted(acc=2, distributor="slope", bounds=(2, 1, 1, 2), rounds=4):
     mesh, solver = gpu_mesh(24, bounds, 3, distributor, acc, "MC", 0.4)
     g = mesh.amr_arrays()

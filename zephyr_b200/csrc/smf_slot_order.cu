@@ -160,6 +160,14 @@ __global__ void k_permute_mixed(const int *perm, int n, MixedState src, MixedSta
     if (wsrc) wdst[to] = wsrc[from];
 }
 
+__global__ void k_scatter8(const int *perm, int n, Fields8 src, Fields8 dst) {
+    int p = blockIdx.x * OBLOCK + threadIdx.x;
+    if (p >= n) return;
+    const int ic = perm[p];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dst.f[k][ic] = src.f[k][p];
+}
+
 size_t order_scratch_bytes(int cap) {
     size_t bytes = 0, scan = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr,
@@ -212,6 +220,9 @@ void gather_mixed(const int *perm, int n, MixedState src, MixedState dst, const 
 void scatter_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst,
                    void *stream) {
     if (n > 0) k_permute_mixed<false><<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst, wsrc, wdst);
+}
+void scatter_fields8(const int *perm, int n, Fields8 src, Fields8 dst, void *stream) {
+    if (n > 0) k_scatter8<<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst);
 }
 void scatter_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream) {
     if (n > 0) k_scatter<<<oblocks(n), OBLOCK, 0, (cudaStream_t)stream>>>(perm, n, src, dst, wsrc, wdst);

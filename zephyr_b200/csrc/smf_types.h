@@ -134,6 +134,11 @@ struct MixedState {
     float *w[5];
 };
 void gather_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst, void *stream);
+// eight fields of n doubles (the gradients) from the order back to the mesh's
+struct Fields8 {
+    double *f[8];
+};
+void scatter_fields8(const int *perm, int n, Fields8 src, Fields8 dst, void *stream);
 void scatter_mixed(const int *perm, int n, MixedState src, MixedState dst, const int *wsrc, int *wdst,
                    void *stream);
 void scatter_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream);

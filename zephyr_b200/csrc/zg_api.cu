@@ -79,6 +79,7 @@ struct zg_ctx {
     slotfast::FaceFlux oflux{};  // face-once fluxes, 8 slots per cell
     long long ord_version = -1;
     bool ord_waits = false;  // ow[0] holds the current isolation counters (predictor-corrector)
+    bool grad_ordered = false;  // gx / gy hold the last FAST adaptive step's gradients in the cell order
 
     // solver
     bool configured = false;
@@ -232,6 +233,7 @@ void free_mesh(zg_ctx *c) {
     c->ord = slotfast::OrderBuffers{};
     c->ord_version = -1;
     if (c->state_mode == STATE_ORDERED) c->state_mode = ZG_FP64;  // the state goes with the mesh
+    c->grad_ordered = false;
     if (c->state_mode == STATE_ORDERED_MIXED) c->state_mode = ZG_MIXED;
     c->d_geo = nullptr;
     c->d_tgeo = nullptr;
@@ -349,13 +351,37 @@ int leave_order(zg_ctx *c) {
         return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "state order");
     }
     if (c->state_mode != STATE_ORDERED) return ZG_OK;
+    cudaStream_t st = c->stream;
     int *wait = c->d_wait + (size_t)c->wait_cur * c->cap;
-    slotfast::scatter_state(c->ord.perm, c->n, c->oz, c->z, c->ord_waits ? c->ow[0] : nullptr, wait,
-                            (void *)c->stream);
+    slotfast::scatter_state(c->ord.perm, c->n, c->oz, c->z, c->ord_waits ? c->ow[0] : nullptr, wait, (void *)st);
     ++c->launches;
     c->state_mode = ZG_FP64;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "state order");
+}
+
+// The last FAST adaptive step's limited gradients back in the mesh's order,
+// for a refine's slope distributor when no gradient computation came between
+// (sm_fluid.cpp:372-470 reads the cells' stored gradients): copied into the
+// order buffers the state has left, then scattered.  Call after
+// leave_order, before the mesh changes.
+int unorder_gradients(zg_ctx *c) {
+    if (!c->grad_ordered) return ZG_OK;
+    cudaStream_t st = c->stream;
+    const size_t bytes = (size_t)c->n * sizeof(double);
+    double *tmp[8] = {c->oz.r, c->oz.u, c->oz.v, c->oz.p, c->oz.e, c->ozhalf.r, c->ozhalf.u, c->ozhalf.v};
+    slotfast::Fields8 src{}, dst{};
+    for (int k = 0; k < 8; ++k) {
+        double *g = k < 4 ? c->gx[k] : c->gy[k - 4];
+        ZG_CUDA(c, cudaMemcpyAsync(tmp[k], g, bytes, cudaMemcpyDeviceToDevice, st));
+        src.f[k] = tmp[k];
+        dst.f[k] = g;
+    }
+    slotfast::scatter_fields8(c->ord.perm, c->n, src, dst, (void *)st);
+    ++c->launches;
+    c->grad_ordered = false;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? ZG_OK : cuda_fail(c, e, "gradient order");
 }
 
 // Move the current state into the representation `mode` (FP64 primitive or
@@ -515,6 +541,7 @@ int ensure_side(zg_ctx *c) {
 
 // One step of SmFluid::update (sm_fluid.cpp:81-102) as kernel launches.
 int enqueue_parity_step(zg_ctx *c) {
+    if (c->par.accuracy == 2) c->grad_ordered = false;  // this step's gradients, in the mesh's order
     SmfArgs a = make_args(c);
     void *st = (void *)c->stream;
     timed(c, ZG_K_DT, [&] { parity::launch_dt(a, c->z, c->slots, st); });
@@ -742,6 +769,7 @@ int enqueue_slot_fast_step(zg_ctx *c) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "kernel launch");
     std::swap(c->oz, c->oznext);
+    if (c->par.accuracy == 2) c->grad_ordered = true;
     c->dt_next_ready = fuse_dt;
     c->cfl_valid = false;
     c->stepped = true;
@@ -1308,6 +1336,7 @@ int zg_smf_set_flags(zg_ctx *c, int *flags) {
     // the slope distributor of the next refine uses (compute_grad,
     // sm_fluid.cpp:521-522)
     if (c->amr) timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, true, (void *)c->stream); });
+    if (c->amr) c->grad_ordered = false;  // gradients of the current state in the mesh's order
     timed(c, ZG_K_FLAGS, [&] { parity::launch_flags(a, dflags, c->slots, (void *)c->stream); });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "flags kernel launch");
@@ -1387,6 +1416,7 @@ int zg_smf_gradients(zg_ctx *c, double *d_dx, double *d_dy) {
     if (rc != ZG_OK) return rc;
     SmfArgs a = make_args(c);
     timed(c, ZG_K_GRAD, [&] { parity::launch_grad(a, c->z, c->slots, (void *)c->stream); });
+    c->grad_ordered = false;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "gradient kernel launch");
     const size_t n = (size_t)c->n;
@@ -2687,6 +2717,7 @@ int zg_amr_set_flags_gradient(zg_ctx *c, double refine_above, double coarsen_bel
     SmfArgs a = make_args(c);
     void *st = (void *)c->stream;
     timed(c, ZG_K_GRAD, [&] { slotfast::launch_grad(a, c->z, st); });
+    c->grad_ordered = false;
     timed(c, ZG_K_FLAGS, [&] { slotfast::launch_grad_flags(a, c->av.flag, refine_above, coarsen_below, st); });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "flags kernel launch");
@@ -2712,6 +2743,7 @@ int zg_amr_refine(zg_ctx *c) {
     DeviceGuard g(c->device);
     // the refine moves and splits the FP64 primitive state
     int rc0 = convert_state(c, ZG_FP64);
+    if (rc0 == ZG_OK) rc0 = unorder_gradients(c);
     if (rc0 != ZG_OK) return rc0;
     const int n0 = c->n;
     amr::RefineResult res = amr::refine(amr_view(c), c->n, c->cap, c->amr_max_level, c->d_amr_scratch,
