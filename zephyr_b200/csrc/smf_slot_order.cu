@@ -176,13 +176,15 @@ size_t order_scratch_bytes(int cap) {
     return std::max(bytes, scan);
 }
 
-int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, OrderBuffers &b,
-                SlotMesh &out, void *stream) {
+int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, int key_bits,
+                OrderBuffers &b, SlotMesh &out, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (n <= 0) return 0;
     k_keys<<<oblocks(n), OBLOCK, 0, st>>>(m.cx, m.cy, n, x0, y0, 1.0 / hx, 1.0 / hy, b.keys, b.idx);
     size_t bytes = b.tmp_bytes;
-    if (cub::DeviceRadixSort::SortPairs(b.tmp, bytes, b.keys, b.keys + b.cap, b.idx, b.perm, n, 0, 42, st) !=
+    // the keys use 2 key_bits bits: one radix pass per 8 of them
+    const int end_bit = std::min(42, std::max(2, 2 * key_bits));
+    if (cub::DeviceRadixSort::SortPairs(b.tmp, bytes, b.keys, b.keys + b.cap, b.idx, b.perm, n, 0, end_bit, st) !=
         cudaSuccess)
         return -1;
     k_inverse<<<oblocks(n), OBLOCK, 0, st>>>(b.perm, n, b.inv);

@@ -123,9 +123,10 @@ struct OrderBuffers {
 };
 size_t order_scratch_bytes(int cap);
 // fills b.perm (position -> cell), b.inv and the reordered mesh arrays, and
-// `out`, the mesh view over them; 0 on success
-int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, OrderBuffers &b,
-                SlotMesh &out, void *stream);
+// `out`, the mesh view over them; key_bits: bits of a finest-cell index per
+// axis (at most 21); 0 on success
+int build_order(const SlotMesh &m, int n, double x0, double y0, double hx, double hy, int key_bits,
+                OrderBuffers &b, SlotMesh &out, void *stream);
 void gather_state(const int *perm, int n, PrimPtr src, PrimPtr dst, const int *wsrc, int *wdst, void *stream);
 // the MIXED representation (FP64 conserved, FP32 primitive mirror) and the
 // counters, into and out of the order

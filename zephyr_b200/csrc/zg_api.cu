@@ -693,7 +693,12 @@ int order_current(zg_ctx *c) {
     if (c->ord_version == c->mesh_version) return ZG_OK;
     void *st = (void *)c->stream;
     const double hx = ldexp(c->smesh.hx0, -c->amr_max_level), hy = ldexp(c->smesh.hy0, -c->amr_max_level);
-    if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, c->ord, c->ord_mesh, st) != 0)
+    // finest cells per axis: the rectangle's extent in cells of the deepest level
+    const double finest = std::max((c->box[1] - c->box[0]) / hx, (c->box[3] - c->box[2]) / hy);
+    int key_bits = 1;
+    while (key_bits < 21 && (double)(1LL << key_bits) <= finest - 0.5) ++key_bits;  // indices < 2^key_bits
+    if (slotfast::build_order(c->smesh, c->n, c->box[0], c->box[2], hx, hy, key_bits, c->ord, c->ord_mesh, st) !=
+        0)
         return cuda_fail(c, cudaGetLastError(), "cell order");
     SmfArgs ga = make_args(c);
     ga.smesh = c->ord_mesh;
