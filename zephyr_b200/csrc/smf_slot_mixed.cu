@@ -24,9 +24,6 @@ constexpr int BLOCK = 128;
 #ifndef ZG_SLOTMX_GRAD_MINB
 #define ZG_SLOTMX_GRAD_MINB 8
 #endif
-#ifndef ZG_SLOTMX_S1_MINB
-#define ZG_SLOTMX_S1_MINB 8
-#endif
 #ifndef ZG_SLOTMX_S2_MINB
 #define ZG_SLOTMX_S2_MINB 6
 #endif
@@ -152,9 +149,46 @@ __device__ __forceinline__ void slot_terms(const SlotFastAcc &c, const Fields<R>
     t.dF[3] = zn.p - zc.p;
 }
 
+// Predictor (sm_fluid.cpp:176-253): half step with the physical flux of the
+// reconstructed face states from the cell's gradients gx, gy; FP64 sums,
+// update and pressure recovery.
+__device__ __forceinline__ void predictor(const SmfArgs &a, const Fields<R> &f, const SlotFastAcc &c, int ic,
+                                          const P5<R> &zc, const R gx[4], const R gy[4]) {
+    if (f.wait_in[ic] > 0) {
+        stw(f.h, ic, zc);
+        return;
+    }
+    const EosR<R> eos = tiled::eos_as<R>(a.eos);
+    double F[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int s = 0; s < 8; ++s) {
+        FaceG g = c.face(s);
+        if (g.flag == BC_UNDEFINED) continue;
+        const R nx = (R)g.nx, ny = (R)g.ny;
+        P5<R> zm = recon(zc, gx, gy, (R)(g.fcx - c.cx()), (R)(g.fcy - c.cy()), eos);
+        rot_in(nx, ny, zm.u, zm.v);
+        C4<R> lf = tiled::phys_flux(zm);
+        rot_out(nx, ny, lf.mu, lf.mv);
+        F[0] += (double)lf.r * g.area;
+        F[1] += (double)lf.mu * g.area;
+        F[2] += (double)lf.mv * g.area;
+        F[3] += (double)lf.E * g.area;
+    }
+    const double coef = 0.5 * (*a.dt_out) / c.vol();
+    C4<double> q = ldq(f, ic);
+    q.r -= coef * F[0];
+    q.mu -= coef * F[1];
+    q.mv -= coef * F[2];
+    q.E -= coef * F[3];
+    P5<double> hz = tiled::prim_of(q, a.eos);
+    stw(f.h, ic, tiled::bad64(hz, a.eos) ? zc : tiled::down<R>(hz));
+}
+
 // Limited least-squares gradients of the FP32 state (two passes over the
 // slots; gradient.h:226-282 and 412-474).
-template <int LIM>
+// PRED: the predictor (k_stage1) follows in the same thread from the
+// gradients just computed.
+template <int LIM, bool PRED>
 __global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad(SmfArgs a, Fields<R> f) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= a.smesh.n) return;
@@ -202,50 +236,15 @@ __global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad(SmfArgs a, 
             Ly[k] += t.w * dl * t.nyy;
         }
     }
+    R gx[4], gy[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        f.gx[k][ic] = B00 * Lx[k] + B01 * Ly[k];
-        f.gy[k][ic] = B10 * Lx[k] + B11 * Ly[k];
+        gx[k] = B00 * Lx[k] + B01 * Ly[k];
+        gy[k] = B10 * Lx[k] + B11 * Ly[k];
+        f.gx[k][ic] = gx[k];
+        f.gy[k][ic] = gy[k];
     }
-}
-
-// Predictor (sm_fluid.cpp:176-253): half step with the physical flux of the
-// reconstructed face states; FP64 sums, update and pressure recovery.
-__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_S1_MINB) k_stage1(SmfArgs a, Fields<R> f) {
-    int ic = blockIdx.x * BLOCK + threadIdx.x;
-    if (ic >= a.smesh.n) return;
-    SlotFastAcc c(a, ic);
-    const P5<R> zc = ldw(f.w, ic);
-    if (f.wait_in[ic] > 0) {
-        stw(f.h, ic, zc);
-        return;
-    }
-    const EosR<R> eos = tiled::eos_as<R>(a.eos);
-    R gx[4], gy[4];
-    ldg(f, ic, gx, gy);
-    double F[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-    for (int s = 0; s < 8; ++s) {
-        FaceG g = c.face(s);
-        if (g.flag == BC_UNDEFINED) continue;
-        const R nx = (R)g.nx, ny = (R)g.ny;
-        P5<R> zm = recon(zc, gx, gy, (R)(g.fcx - c.cx()), (R)(g.fcy - c.cy()), eos);
-        rot_in(nx, ny, zm.u, zm.v);
-        C4<R> lf = tiled::phys_flux(zm);
-        rot_out(nx, ny, lf.mu, lf.mv);
-        F[0] += (double)lf.r * g.area;
-        F[1] += (double)lf.mu * g.area;
-        F[2] += (double)lf.mv * g.area;
-        F[3] += (double)lf.E * g.area;
-    }
-    const double coef = 0.5 * (*a.dt_out) / c.vol();
-    C4<double> q = ldq(f, ic);
-    q.r -= coef * F[0];
-    q.mu -= coef * F[1];
-    q.mv -= coef * F[2];
-    q.E -= coef * F[3];
-    P5<double> hz = tiled::prim_of(q, a.eos);
-    stw(f.h, ic, tiled::bad64(hz, a.eos) ? zc : tiled::down<R>(hz));
+    if constexpr (PRED) predictor(a, f, c, ic, zc, gx, gy);
 }
 
 // Face-once form over the FAST step's face list (slotfast::FaceFlux): one
@@ -342,17 +341,18 @@ void launch_sum(const SmfArgs &a, const Fields<R> &f, int mode, const slotfast::
 void launch_dt(const SmfArgs &a, const Fields<R> &f, void *stream) {
     k_dt<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
 }
-void launch_grad(const SmfArgs &a, const Fields<R> &f, void *stream) {
-    cudaStream_t s = (cudaStream_t)stream;
+template <bool PRED>
+static void grad_pred(const SmfArgs &a, const Fields<R> &f, cudaStream_t s) {
     switch (a.limiter) {  // the common limiters compiled in, the others at run time
-        case LIM_VANALBADA1: k_grad<LIM_VANALBADA1><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
-        case LIM_MC: k_grad<LIM_MC><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
-        case LIM_MINMOD: k_grad<LIM_MINMOD><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
-        default: k_grad<-1><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        case LIM_VANALBADA1: k_grad<LIM_VANALBADA1, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        case LIM_MC: k_grad<LIM_MC, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        case LIM_MINMOD: k_grad<LIM_MINMOD, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        default: k_grad<-1, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
     }
 }
-void launch_stage1(const SmfArgs &a, const Fields<R> &f, void *stream) {
-    k_stage1<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
+void launch_grad(const SmfArgs &a, const Fields<R> &f, bool predictor, void *stream) {
+    if (predictor) grad_pred<true>(a, f, (cudaStream_t)stream);
+    else grad_pred<false>(a, f, (cudaStream_t)stream);
 }
 
 }  // namespace slotmixed

@@ -28,12 +28,12 @@ void launch_to_prim(int n, const tiled::Fields<float> &f, EosD eos, PrimPtr z, v
 }  // namespace mixed
 
 // MIXED kernels on an adaptive rectangle (smf_slot_mixed.cu): dt from the FP64
-// conserved state, FP32 gradients, predictor, and the face loop (mode 0 first
-// order, 1 corrector).
+// conserved state, FP32 gradients with the predictor, and the face-once face
+// loop (mode 0 first order, 1 corrector).
 namespace slotmixed {
 void launch_dt(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
-void launch_grad(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
-void launch_stage1(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
+// predictor: the predictor stage (sm_fluid.cpp:176-253) fused after the gradients
+void launch_grad(const SmfArgs &a, const tiled::Fields<float> &f, bool predictor, void *stream);
 // face-once (mode 0 first order, 1 corrector): the listed faces, then the
 // cell sums (and the next dt with ff.dt_next)
 void launch_faces_once(const SmfArgs &a, const tiled::Fields<float> &f, int mode, const slotfast::FaceFlux &ff,
