@@ -81,6 +81,34 @@ __global__ void __launch_bounds__(BLOCK) k_grad_geometry(SmfArgs a, double4 *sg,
     bm[ic] = make_double4(A11 * inv, (-A01) * inv, (-A10) * inv, A00 * inv);
 }
 
+// 1/x: Newton-Raphson (y <- y + y (1 - x y), two steps; P. Markstein, IBM
+// J. Res. Dev. 34(1), 1990) from the hardware's approximate reciprocal
+// (PTX rcp.approx.ftz.f64); within 2 ulp of 1/x for normal finite x
+__device__ __forceinline__ double rcp2(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+// limiter2 (limiter.cxx binary forms) with its divisions as reciprocals for
+// the common limiters, the others as limiter2
+__device__ __forceinline__ double limiter_rcp(int kind, double a, double b) {
+    switch (kind) {
+        case LIM_VANALBADA1:
+            if (a * b <= 0.0) return 0.0;
+            if (b == 0.0) return 1.0;
+            return a * (a + b) * rcp2(a * a + b * b);
+        case LIM_MC:
+            return b == 0.0 ? limiter2(kind, a, b) : lim_MC1(a * rcp2(b));
+        case LIM_MINMOD:
+            if (a * b <= 0.0) return 0.0;
+            return smin(a * rcp2(b), 1.0);
+        default: return limiter2(kind, a, b);
+    }
+}
+
 // the neighbour's (or the boundary's) primitive values across slot s
 __device__ __forceinline__ void slot_values(const SmfArgs &a, const PrimPtr &z, const Prim &zc, int ic, int s,
                                             int flag, double zn[4]) {
@@ -147,7 +175,7 @@ __global__ void __launch_bounds__(BLOCK, GM) k_grad_pre(SmfArgs a, PrimPtr z, co
             const double dF_p = zn[k] - zcv[k];
             const double du_n = g0x[k] * G.x + g0y[k] * G.y;
             const double dF_m = 2.0 * du_n - dF_p;
-            const double dF_lim = limiter2(a.limiter, dF_m, dF_p) * dF_p;
+            const double dF_lim = limiter_rcp(a.limiter, dF_m, dF_p) * dF_p;
             Lx[k] += G.z * dF_lim;
             Ly[k] += G.w * dF_lim;
         }
