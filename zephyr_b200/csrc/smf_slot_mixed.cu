@@ -122,33 +122,6 @@ __global__ void __launch_bounds__(BLOCK) k_dt(SmfArgs a, Fields<R> f) {
     }
 }
 
-// One slot's least-squares terms: neighbour difference, centre offset, the
-// normal part of the offset and the weight (gradient.h:226-282), offsets in
-// FP64 rounded once to FP32.
-struct Terms {
-    R w, rx, ry, nxx, nyy, dF[4];
-};
-__device__ __forceinline__ void slot_terms(const SlotFastAcc &c, const Fields<R> &f, const FaceG &g, int s,
-                                           const P5<R> &zc, Terms &t) {
-    const R nx = (R)g.nx, ny = (R)g.ny;
-    P5<R> zn = !is_boundary(g.flag) ? ldw(f.w, g.nb) : wall_of(zc, nx, ny, g.flag);
-    double ncx, ncy;
-    neib_center(c, g, s, c.cx(), c.cy(), ncx, ncy);
-    const double rx = ncx - c.cx(), ry = ncy - c.cy();
-    const double d = rx * g.nx + ry * g.ny;
-    const double nxx = d * g.nx, nyy = d * g.ny;
-    const double an = sqrt(nxx * nxx + nyy * nyy);
-    t.w = (R)(g.area / (an * an * an));
-    t.rx = (R)rx;
-    t.ry = (R)ry;
-    t.nxx = (R)nxx;
-    t.nyy = (R)nyy;
-    t.dF[0] = zn.r - zc.r;
-    t.dF[1] = zn.u - zc.u;
-    t.dF[2] = zn.v - zc.v;
-    t.dF[3] = zn.p - zc.p;
-}
-
 // Predictor (sm_fluid.cpp:176-253): half step with the physical flux of the
 // reconstructed face states from the cell's gradients gx, gy; FP64 sums,
 // update and pressure recovery.
@@ -184,37 +157,54 @@ __device__ __forceinline__ void predictor(const SmfArgs &a, const Fields<R> &f, 
     stw(f.h, ic, tiled::bad64(hz, a.eos) ? zc : tiled::down<R>(hz));
 }
 
+
 // Limited least-squares gradients of the FP32 state (two passes over the
-// slots; gradient.h:226-282 and 412-474).
-// PRED: the predictor (k_stage1) follows in the same thread from the
-// gradients just computed.
+// slots; gradient.h:226-282 and 412-474) over the slot geometry built once
+// per mesh change for the FAST step (slotfast::launch_grad_geometry: sg =
+// (rx, ry, w nx^, w ny^) per slot, bm = the inverse least-squares matrix per
+// cell) in FP64, rounded to FP32 here.  PRED: the predictor follows in the
+// same thread from the gradients just computed.
 template <int LIM, bool PRED>
-__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad(SmfArgs a, Fields<R> f) {
+__global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad_pre(SmfArgs a, Fields<R> f, const double4 *sg,
+                                                                         const double4 *bm) {
     int ic = blockIdx.x * BLOCK + threadIdx.x;
     if (ic >= a.smesh.n) return;
-    SlotFastAcc c(a, ic);
     const P5<R> zc = ldw(f.w, ic);
-    R A00 = 0, A01 = 0, A10 = 0, A11 = 0, Fx[4] = {0, 0, 0, 0}, Fy[4] = {0, 0, 0, 0};
+    const R zcv[4] = {zc.r, zc.u, zc.v, zc.p};
+    // the neighbour's (or the wall's) FP32 values across slot s
+    auto values = [&](int s, int flag, R zn[4]) {
+        P5<R> z;
+        if (!is_boundary(flag)) {
+            z = ldw(f.w, a.smesh.fn[8 * ic + s]);
+        } else {
+            const int side = s & 3;  // the axis normal of the side (SlotFastAcc::face)
+            const R nx = side == 0 ? R(-1) : (side == 1 ? R(1) : R(0));
+            const R ny = side == 2 ? R(-1) : (side == 3 ? R(1) : R(0));
+            z = wall_of(zc, nx, ny, flag);
+        }
+        zn[0] = z.r;
+        zn[1] = z.u;
+        zn[2] = z.v;
+        zn[3] = z.p;
+    };
+    R Fx[4] = {0, 0, 0, 0}, Fy[4] = {0, 0, 0, 0};
 #pragma unroll 1
     for (int s = 0; s < 8; ++s) {
-        FaceG g = c.face(s);
-        if (g.flag == BC_UNDEFINED) continue;
-        Terms t;
-        slot_terms(c, f, g, s, zc, t);
-        R wdx = t.w * t.nxx, wdy = t.w * t.nyy;
-        A00 += wdx * t.rx;
-        A01 += wdx * t.ry;
-        A10 += wdy * t.rx;
-        A11 += wdy * t.ry;
+        const int flag = a.smesh.fb[8 * ic + s];
+        if (flag == BC_UNDEFINED) continue;
+        R zn[4];
+        values(s, flag, zn);
+        const double4 G = sg[8 * ic + s];
+        const R wdx = (R)G.z, wdy = (R)G.w;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            Fx[k] += t.w * t.dF[k] * t.nxx;
-            Fy[k] += t.w * t.dF[k] * t.nyy;
+            const R dF = zn[k] - zcv[k];
+            Fx[k] += wdx * dF;
+            Fy[k] += wdy * dF;
         }
     }
-    if (fabsf(A11) < R(1e-8)) A11 = R(1);  // 1-D case (gradient.h:270-272)
-    const R inv = R(1) / (A11 * A00 - A01 * A10);
-    const R B00 = A11 * inv, B01 = -A01 * inv, B10 = -A10 * inv, B11 = A00 * inv;
+    const double4 Bd = bm[ic];
+    const R B00 = (R)Bd.x, B01 = (R)Bd.y, B10 = (R)Bd.z, B11 = (R)Bd.w;
     R g0x[4], g0y[4], Lx[4] = {0, 0, 0, 0}, Ly[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -223,17 +213,19 @@ __global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad(SmfArgs a, 
     }
 #pragma unroll 1
     for (int s = 0; s < 8; ++s) {
-        FaceG g = c.face(s);
-        if (g.flag == BC_UNDEFINED) continue;
-        Terms t;
-        slot_terms(c, f, g, s, zc, t);
+        const int flag = a.smesh.fb[8 * ic + s];
+        if (flag == BC_UNDEFINED) continue;
+        R zn[4];
+        values(s, flag, zn);
+        const double4 G = sg[8 * ic + s];
+        const R rx = (R)G.x, ry = (R)G.y, wdx = (R)G.z, wdy = (R)G.w;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            R dF_p = t.dF[k];
-            R dF_m = R(2) * (g0x[k] * t.rx + g0y[k] * t.ry) - dF_p;
-            R dl = tiled::limit<LIM, R>(a.limiter, dF_m, dF_p) * dF_p;
-            Lx[k] += t.w * dl * t.nxx;
-            Ly[k] += t.w * dl * t.nyy;
+            const R dF_p = zn[k] - zcv[k];
+            const R dF_m = R(2) * (g0x[k] * rx + g0y[k] * ry) - dF_p;
+            const R dl = tiled::limit<LIM, R>(a.limiter, dF_m, dF_p) * dF_p;
+            Lx[k] += wdx * dl;
+            Ly[k] += wdy * dl;
         }
     }
     R gx[4], gy[4];
@@ -244,7 +236,10 @@ __global__ void __launch_bounds__(BLOCK, ZG_SLOTMX_GRAD_MINB) k_grad(SmfArgs a, 
         f.gx[k][ic] = gx[k];
         f.gy[k][ic] = gy[k];
     }
-    if constexpr (PRED) predictor(a, f, c, ic, zc, gx, gy);
+    if constexpr (PRED) {
+        SlotFastAcc c(a, ic);
+        predictor(a, f, c, ic, zc, gx, gy);
+    }
 }
 
 // Face-once form over the FAST step's face list (slotfast::FaceFlux): one
@@ -342,17 +337,18 @@ void launch_dt(const SmfArgs &a, const Fields<R> &f, void *stream) {
     k_dt<<<blocks(a), BLOCK, 0, (cudaStream_t)stream>>>(a, f);
 }
 template <bool PRED>
-static void grad_pred(const SmfArgs &a, const Fields<R> &f, cudaStream_t s) {
+static void grad_pred(const SmfArgs &a, const Fields<R> &f, const double4 *sg, const double4 *bm, cudaStream_t s) {
     switch (a.limiter) {  // the common limiters compiled in, the others at run time
-        case LIM_VANALBADA1: k_grad<LIM_VANALBADA1, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
-        case LIM_MC: k_grad<LIM_MC, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
-        case LIM_MINMOD: k_grad<LIM_MINMOD, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
-        default: k_grad<-1, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f); break;
+        case LIM_VANALBADA1: k_grad_pre<LIM_VANALBADA1, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f, sg, bm); break;
+        case LIM_MC: k_grad_pre<LIM_MC, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f, sg, bm); break;
+        case LIM_MINMOD: k_grad_pre<LIM_MINMOD, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f, sg, bm); break;
+        default: k_grad_pre<-1, PRED><<<blocks(a), BLOCK, 0, s>>>(a, f, sg, bm); break;
     }
 }
-void launch_grad(const SmfArgs &a, const Fields<R> &f, bool predictor, void *stream) {
-    if (predictor) grad_pred<true>(a, f, (cudaStream_t)stream);
-    else grad_pred<false>(a, f, (cudaStream_t)stream);
+void launch_grad(const SmfArgs &a, const Fields<R> &f, const double4 *sg, const double4 *bm, bool predictor,
+                 void *stream) {
+    if (predictor) grad_pred<true>(a, f, sg, bm, (cudaStream_t)stream);
+    else grad_pred<false>(a, f, sg, bm, (cudaStream_t)stream);
 }
 
 }  // namespace slotmixed

@@ -32,8 +32,10 @@ void launch_to_prim(int n, const tiled::Fields<float> &f, EosD eos, PrimPtr z, v
 // loop (mode 0 first order, 1 corrector).
 namespace slotmixed {
 void launch_dt(const SmfArgs &a, const tiled::Fields<float> &f, void *stream);
-// predictor: the predictor stage (sm_fluid.cpp:176-253) fused after the gradients
-void launch_grad(const SmfArgs &a, const tiled::Fields<float> &f, bool predictor, void *stream);
+// the gradients over the FAST step's slot geometry (sg, bm); predictor: the
+// predictor stage (sm_fluid.cpp:176-253) fused after them
+void launch_grad(const SmfArgs &a, const tiled::Fields<float> &f, const double4 *sg, const double4 *bm,
+                 bool predictor, void *stream);
 // face-once (mode 0 first order, 1 corrector): the listed faces, then the
 // cell sums (and the next dt with ff.dt_next)
 void launch_faces_once(const SmfArgs &a, const tiled::Fields<float> &f, int mode, const slotfast::FaceFlux &ff,

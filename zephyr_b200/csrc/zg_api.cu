@@ -824,7 +824,7 @@ int enqueue_slot_mixed_step(zg_ctx *c) {
         timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_faces_once(a, f, 0, c->oflux, st); });
         timed(c, ZG_K_FLUX1, [&] { slotmixed::launch_sum(a, f, 0, c->oflux, st); });
     } else {
-        timed(c, ZG_K_GRAD, [&] { slotmixed::launch_grad(a, f, true, st); });
+        timed(c, ZG_K_GRAD, [&] { slotmixed::launch_grad(a, f, c->ord.sg, c->ord.bm, true, st); });
         timed(c, ZG_K_STAGE2, [&] { slotmixed::launch_faces_once(a, f, 1, c->oflux, st); });
         timed(c, ZG_K_STAGE2, [&] { slotmixed::launch_sum(a, f, 1, c->oflux, st); });
         c->wait_cur = 1 - c->wait_cur;
