@@ -525,9 +525,10 @@ def amr_variant(torch, lib, dev, stream, local_rank, want_cpu, kernels_name=None
         "workload": f"AMR blast, base {AMR_BASE}x{AMR_BASE}, max_level {AMR_LEVELS}, ZOE; rho = 1, u = v = 0, "
                     f"p = 1e-5 except p = 1e3 for r < 0.01 at (0.5, 0.5), 20x20 sub-sampled cell means",
         "form": {"fast": "FP64 FAST kernels on the slot mesh (face geometry from centre and level, fused "
-                         "multiply-adds; within 1e-12 of the parity form per step)",
+                         "multiply-adds, cells in Morton order, face-once corrector; within 1e-12 of the parity "
+                         "form per step)",
                  "mixed": "MIXED kernels on the slot mesh (FP32 states, gradients and fluxes; FP64 conserved "
-                          "sums, update, pressure recovery and dt)",
+                          "sums, update, pressure recovery and dt; cells in Morton order, face-once corrector)",
                  "parity": "FP64 PARITY kernels on the slot mesh, bit-exact with the reference"}[kernels_name] +
                 " -- SmFluid second order, predictor-corrector, HLLC, van Albada 1, CFL 0.4; set_flags criterion; "
                 "slope distributor",
